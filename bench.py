@@ -1,0 +1,311 @@
+#!/usr/bin/env python
+"""Benchmark: FWI shot-gradients/s of the B200 acoustic propagator (forward + exact adjoint).
+
+One step = one full FWI gradient of the 512^2 workload: 16 Ricker shots (10 Hz) over a seeded
+layered model, 4000 leapfrog steps, order-4 stencil, 20-cell sponge, full wavefield history in HBM,
+misfit 1/2 ||F(c) - d||^2 with its gradient w.r.t. c reduced over shots in float64.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Rank 0 prints one JSON line. Under torchrun every rank runs its own 16 shots (weak scaling) and the
+float64 gradient is summed with one NCCL all-reduce per step. ``--impl reference`` times the CPU
+restatement of the reference algorithm (the oracle, float32, all host threads) on a bounded sample.
+"""
+
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+import torch
+
+ROOT = Path(__file__).resolve().parent
+METRIC = "FWI shot-gradients/s & Gcell-updates/s at 1e-4 grad err vs FP64; plain vs batched"
+UNIT = "shot-gradients/s"
+CPU_SAMPLE_SHOTS, CPU_SAMPLE_STEPS = 8, 300
+
+
+def peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def workload_desc(w) -> dict:
+    P = w.n + 2 * w.absorb_cells
+    return {"workload": f"{w.name}: {w.n}x{w.n} FP32 grid h={w.h:g} m, seeded layered model "
+                        f"(6-10 layers 1500-4500 m/s + 4 anomalies), {len(w.sources)} Ricker shots "
+                        f"{w.f0:g} Hz, {len(w.receivers)} receivers, {w.n_steps} steps, Courant "
+                        f"{w.courant_number}, order {w.order}, {w.absorb_cells}-cell sponge, full history in HBM",
+            "grid_padded": [P, P], "shots_per_gpu": len(w.sources), "n_steps": w.n_steps,
+            "l2": "256 MiB buffer written between timed steps; working set (history) far above L2"}
+
+
+# ------------------------------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ------------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.proc = None
+        self.path = Path(tempfile.mkstemp(suffix=".csv")[1])
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(gpu_index)], stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        rows = [r.split(",") for r in self.path.read_text().strip().splitlines() if r.count(",") >= 8]
+        self.path.unlink(missing_ok=True)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if "Active" in v and "Not" not in v})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].strip().replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max(float(r[3]) for r in rows if r[3].strip().replace(".", "").isdigit())}
+
+
+# ------------------------------------------------------------------------------------------------
+# CPU baseline: the oracle (float32, all host threads) on a bounded sample of the workload
+# ------------------------------------------------------------------------------------------------
+def cpu_sample(w, n_shots=CPU_SAMPLE_SHOTS, n_steps=CPU_SAMPLE_STEPS) -> tuple[float, dict]:
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle  # noqa: E402  (the checker, used here only as the timed CPU baseline)
+
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    kw = w.operator_kwargs()
+    kw["n_t"] = n_steps + 1
+    L = w.n * w.h
+    orc = oracle.OracleWave((w.n, w.n), ((0.0, L), (0.0, L)), w.receivers, sources=w.sources[:n_shots],
+                            **{k: v for k, v in kw.items()})
+    g = np.random.default_rng(1).standard_normal((n_shots, len(w.receivers), n_steps + 1)).astype(np.float32)
+    t0 = time.perf_counter()
+    orc.fwi(w.c, g, dtype=np.float32)
+    t = time.perf_counter() - t0
+    per_shot_full = t / n_shots * (w.n_steps / n_steps)
+    info = {"cores": min(threads, n_shots), "sample": f"{n_shots} shots x {n_steps} of {w.n_steps} steps "
+            f"(forward + adjoint, full {w.n + 2 * w.absorb_cells}^2 padded grid), float32; "
+            f"extrapolated linearly in steps", "seconds": t,
+            "gcell_updates_per_s": 2 * w.padded_cells() * n_steps * n_shots / t / 1e9}
+    return 1.0 / per_shot_full, info
+
+
+def run_reference(args) -> None:
+    from nefi_b200 import workloads
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w = workloads.WORKLOADS[args.workload]()
+    vals, info = [], {}
+    for i in range(args.warmup + args.steps):
+        v, info = cpu_sample(w)
+        if i >= args.warmup:
+            vals.append(v)
+    v = statistics.median(vals)
+    out = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * len(w.sources) / v,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic (seeded)", "config": {**workload_desc(w), "parallelism": "cpu threads"},
+           "cpu_baseline": {"value": v, "unit": UNIT, "cores": info["cores"], "kind": "port",
+                            "sample": info["sample"]},
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "gcell_updates_per_s": info["gcell_updates_per_s"]}
+    print(json.dumps(out), flush=True)
+
+
+# ------------------------------------------------------------------------------------------------
+# the GPU arm
+# ------------------------------------------------------------------------------------------------
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--workload", default="fwi_512")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch.distributed as dist
+
+    from nefi_b200 import WaveOperatorB200, _lib, workloads
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+
+    w = workloads.WORKLOADS[args.workload]()
+    op = WaveOperatorB200(w.domain, w.sources, w.receivers, grad_mode="autograd", **w.operator_kwargs())
+    c = torch.tensor(w.c, dtype=torch.float32, device=dev)
+    # observed data: traces of a smoothed model (the misfit of a typical early FWI iteration)
+    with torch.no_grad():
+        c_true = torch.tensor(w.c, dtype=torch.float32, device=dev)
+        d = op({"c": torch.nn.functional.avg_pool2d(c_true[None, None], 9, 1, 4,
+                                                    count_include_pad=False)[0, 0].contiguous()})
+    flush = torch.empty(64 * 2**20, dtype=torch.float32, device=dev)
+    lib = _lib.load()
+
+    def step(cc, dd, events=None):
+        loss, g = op.misfit_gradient(cc, dd, events=events)
+        if world > 1:
+            dist.all_reduce(g)
+        return loss, g
+
+    for _ in range(args.warmup):
+        step(c, d)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+
+    sampler = ClockSampler(dev.index if "CUDA_VISIBLE_DEVICES" not in os.environ else local)
+    times, fwd_ms, adj_ms = [], [], []
+    launches0 = lib.nw_launch_count()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    for _ in range(args.steps):
+        flush.zero_()
+        ev = {}
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        step(c, d, ev)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+        fwd_ms.append(ev["fwd0"].elapsed_time(ev["fwd1"]))
+        adj_ms.append(ev["adj0"].elapsed_time(ev["adj1"]))
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches = lib.nw_launch_count() - launches0
+    clocks = sampler.stop()
+    total_ms = sum(times)
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t)
+    S = len(w.sources)
+    ms_per_step = total_ms / args.steps
+    value = S * world / (ms_per_step / 1000.0)
+    cells = w.padded_cells()
+    gcells = 2 * cells * w.n_steps * S * world / (ms_per_step / 1000.0) / 1e9
+
+    # roofline of the dominant stencil kernel: 16 B per cell-update, per launch = cells * shots
+    peak, peak_kind = peaks()
+    alg_bytes = 16.0 * cells * S
+    fwd_launch_ms = statistics.median(fwd_ms) / w.n_steps
+    adj_launch_ms = statistics.median(adj_ms) / w.n_steps
+    kern = "adj2d" if adj_launch_ms >= fwd_launch_ms else "fwd2d"
+    launch_ms = max(adj_launch_ms, fwd_launch_ms)
+    achieved = alg_bytes / (launch_ms * 1e-3) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "traffic.json"
+    if tf.exists():
+        tj = json.loads(tf.read_text())
+        if kern in tj:
+            traffic = tj[kern]["bytes_per_launch_full"]
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": kern, "peak_source": peak_kind,
+                "algorithmic_bytes_per_launch": alg_bytes,
+                "per_kernel_GBps": {"fwd2d": alg_bytes / (fwd_launch_ms * 1e-3) / 1e9,
+                                    "adj2d_with_injection": alg_bytes / (adj_launch_ms * 1e-3) / 1e9}}
+
+    # end to end through the public API: H2D of c and d from pinned memory, D2H of loss and gradient
+    c_h = c.cpu().pin_memory()
+    d_h = d.cpu().pin_memory()
+    g_h = torch.empty(c.shape, dtype=torch.float64).pin_memory()
+    l_h = torch.empty((), dtype=torch.float64).pin_memory()
+    e2e_ms = []
+    for i in range(1 + args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        cd = c_h.to(dev, non_blocking=True)
+        dd = d_h.to(dev, non_blocking=True)
+        loss, g = step(cd, dd)
+        g_h.copy_(g, non_blocking=True)
+        l_h.copy_(loss, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        if i > 0:
+            e2e_ms.append(e0.elapsed_time(e1))
+    e2e_total = sum(e2e_ms)
+    if world > 1:
+        t = torch.tensor([e2e_total], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t)
+    e2e_val = S * world / (e2e_total / len(e2e_ms) / 1000.0)
+    h2d = c_h.numel() * c_h.element_size() + d_h.numel() * d_h.element_size()
+    d2h = g_h.numel() * 8 + 8
+
+    accuracy = None
+    if not args.no_accuracy and rank == 0:
+        # float32 gradient against a float64 device run of the same step (checkpointed, exact snapshots)
+        _, g32 = op.misfit_gradient(c, d)
+        op64 = WaveOperatorB200(w.domain, w.sources, w.receivers, grad_mode="checkpoint", **w.operator_kwargs())
+        _, g64 = op64.misfit_gradient(c.double(), d.double())
+        accuracy = {"grad_rel_l2_fp32_vs_fp64": float((g32 - g64).norm() / g64.norm())}
+        del op64
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, info = cpu_sample(w)
+        cpu = {"value": v, "unit": UNIT, "cores": info["cores"], "kind": "port", "sample": info["sample"],
+               "gcell_updates_per_s": info["gcell_updates_per_s"]}
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f32",
+               "data": "synthetic (seeded layered model; observed data from a smoothed model)",
+               "config": {**workload_desc(w), "method": "plain (per-step launches, full history)",
+                          "parallelism": f"shots sharded over {world} GPU(s), fp64 gradient all-reduce"},
+               "gcell_updates_per_s": gcells, "roofline": roofline, "cpu_baseline": cpu,
+               "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+               "clocks": clocks, "gpu_launches": int(launches), "accuracy": accuracy}
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,235 @@
+/*
+ * nefi_wave.h — C ABI of the B200 (sm_100a) acoustic leapfrog propagator and its exact adjoint.
+ *
+ * The library replaces the time loop of NEFI's wave operators: the leapfrog step
+ * `_LeapfrogBase._step_fn` (nefi/physics/wave.py:520-554), the loop driver `run_timestepping`
+ * (nefi/physics/timestep.py:78-169), receiver sampling `_sample` (nefi/physics/wave.py:321-324),
+ * source injection (nefi/physics/wave.py:715-721), and the reverse-mode autodiff of all of them
+ * (the discrete adjoint NEFI obtains from torch.autograd, nefi/physics/wave.py:46-49).
+ *
+ * Conventions
+ *  - Every pointer is a device pointer unless stated otherwise; sizes are element counts.
+ *  - Nothing is allocated by the library: the caller passes every buffer, sized by the
+ *    nw_*_bytes() queries. The library never frees caller memory.
+ *  - All work is enqueued on `stream` (a cudaStream_t passed as void*); calls are asynchronous
+ *    unless they say otherwise. Calls on distinct streams with distinct buffers may overlap.
+ *  - Return value: NW_OK or an NW_ERR_* code; nw_last_error() gives a message for the calling
+ *    thread's last failure.
+ *  - Grid arrays ("fields") use the ghost layout described by nw_grid: the padded simulation grid
+ *    (P0[,P1],Pl), last axis contiguous, surrounded by zero cells so that every stencil read is in
+ *    bounds and reads zero outside the grid (the reference's zero-padded convolution,
+ *    nefi/physics/wave.py:144-168). The library writes only interior cells, so the ghost cells of
+ *    a buffer that started zeroed stay zero.
+ */
+#ifndef NEFI_WAVE_H
+#define NEFI_WAVE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NW_ABI_VERSION 1
+
+/* scalar type of a computation */
+enum { NW_F32 = 0, NW_F64 = 1 };
+/* absorbing layer kind (nefi/physics/wave.py:80, 469-501) */
+enum { NW_ABS_NONE = 0, NW_ABS_SPONGE = 1, NW_ABS_CERJAN = 2 };
+/* snapshot encodings for checkpointed gradients */
+enum { NW_SNAP_EXACT = 0, NW_SNAP_F16 = 1, NW_SNAP_BF16 = 2 };
+/* status codes */
+enum {
+  NW_OK = 0,
+  NW_ERR_ARG = 1,         /* invalid argument (the message names it) */
+  NW_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+  NW_ERR_UNSUPPORTED = 3, /* valid but not built (dimension/order/absorbing combination) */
+  NW_ERR_NONFINITE = 4,   /* a snapshot block held a non-finite value or scale */
+  NW_ERR_TIMEOUT = 5      /* a bounded device-side wait gave up */
+};
+
+/*
+ * Geometry of one padded grid. The caller fills ndim, order, dtype, absorbing, n[], core_lo[],
+ * core_hi[] and the stencil weights; nw_grid_layout() fills the layout fields.
+ * Replaces WaveGrid (nefi/physics/wave.py:195-318) and laplacian_kernel (wave.py:125-141).
+ */
+typedef struct nw_grid {
+  int32_t ndim;       /* 2 or 3 */
+  int32_t order;      /* 2 or 4: spatial accuracy of the Laplacian */
+  int32_t dtype;      /* NW_F32 or NW_F64 */
+  int32_t absorbing;  /* NW_ABS_* */
+  int32_t n[3];       /* padded extents P per axis; the last used axis is contiguous */
+  int32_t core_lo[3]; /* cells with lo <= i < hi on every axis are outside the layer */
+  int32_t core_hi[3];
+  double w_center;    /* Laplacian weights: centre, +-1 and +-2 neighbours per axis */
+  double w1[3];
+  double w2[3];
+  /* --- filled by nw_grid_layout --- */
+  int32_t radius;      /* stencil radius: order / 2 */
+  int32_t reserved;
+  int64_t stride[3];   /* element strides per axis in the ghost layout */
+  int64_t origin;      /* element offset of cell (0,..,0) */
+  int64_t field_elems; /* elements per field buffer, ghosts included */
+} nw_grid;
+
+/* Fills radius/stride/origin/field_elems of `g`. Host only, no CUDA call. */
+int nw_grid_layout(nw_grid* g);
+
+/*
+ * Point stencils of one acquisition. Sources: one multilinear stencil per shot, injected as
+ * weight[k] * wavelet[n] into cell corner + bits(k) every step n (nefi/physics/wave.py:312-318,
+ * 715-721). Receivers: one multilinear stencil per receiver, shared by all shots, sampled at
+ * every record step (nefi/physics/wave.py:272-300, 321-324, 723-729).
+ * The adjoint of the receiver sampling is given as a cell-major table (CSR over the cells the
+ * receivers touch) so that the adjoint injection sums each cell in a fixed order.
+ */
+typedef struct nw_acquisition {
+  int32_t n_shots;
+  int32_t has_source;          /* 0 for the initial-value (photoacoustic) operator */
+  const int32_t* src_corner;   /* (n_shots, ndim) lower corner cell */
+  const void* src_weight;      /* (n_shots, 2^ndim) dtype: w / cell_volume * dt^2 */
+  const void* wavelet;         /* (n_steps,) dtype: source time function at t = n dt */
+  int32_t n_rec;
+  int32_t n_cells;             /* cells touched by the receiver stencils */
+  const int64_t* rec_index;    /* (n_rec, 2^ndim) ghost-layout offsets */
+  const void* rec_weight;      /* (n_rec, 2^ndim) dtype */
+  const int64_t* cell_index;   /* (n_cells,) ghost-layout offsets, ascending */
+  const int32_t* cell_ptr;     /* (n_cells + 1,) CSR row pointers into cell_rec/cell_weight */
+  const int32_t* cell_rec;     /* receiver id per entry */
+  const void* cell_weight;     /* dtype weight per entry */
+} nw_acquisition;
+
+/* The medium: c^2 dt^2 on the padded grid and the absorbing coefficients. */
+typedef struct nw_medium {
+  const void* c2dt2;  /* field (ghost layout) */
+  const void* coef_a; /* field: A = 1/(1 + sigma dt/2) (sponge) or the Cerjan taper; NULL if none */
+  const void* coef_b; /* field: B = 1 - sigma dt/2 (sponge) or the Cerjan taper; NULL if none */
+} nw_medium;
+
+/* Time axis: n_steps = (n_t - 1) * substeps; trace sample j is the state after j*substeps steps. */
+typedef struct nw_time {
+  int32_t n_steps;
+  int32_t substeps;
+  int32_t n_t;
+  int32_t first_b_one; /* 1: the first step uses B = 1 on p^-1 (Cerjan, nefi/physics/wave.py:550-551) */
+} nw_time;
+
+/*
+ * Wavefield storage for the gradient.
+ *  history != NULL: every level p^-1..p^N is kept, level n at history + (n+1)*level_stride
+ *    (level_stride = n_shots * field_elems). Matches grad_mode="autograd".
+ *  history == NULL and snap != NULL: checkpointing (grad_mode="checkpoint",
+ *    nefi/physics/timestep.py:141-169): the pair (p^{n0-1}, p^{n0}) is encoded into snapshot
+ *    j = n0 / segment for every segment start n0; the adjoint recomputes each segment into
+ *    `segbuf` (segment + 1 levels). snap_kind selects exact copies or 16-bit values with one
+ *    power-of-two scale per block of NW_SNAP_BLOCK elements.
+ *  both NULL: forward only; `ring` holds three levels.
+ */
+#define NW_SNAP_BLOCK 1024
+typedef struct nw_storage {
+  void* history;
+  void* ring;          /* 3 levels, used when history == NULL */
+  void* snap;          /* snapshot pool, nw_snapshot_bytes() bytes */
+  void* segbuf;        /* (segment + 1) levels, used when snap != NULL */
+  int32_t segment;     /* steps per checkpoint segment */
+  int32_t snap_kind;   /* NW_SNAP_* */
+} nw_storage;
+
+/* Bytes of one snapshot pool for `n_snap` snapshots of n_shots shots (both levels). */
+size_t nw_snapshot_bytes(const nw_grid* g, int32_t n_shots, int32_t n_snap, int32_t snap_kind);
+
+/*
+ * Prepare the medium: c (physical grid, contiguous, dtype) -> c2dt2 = pad_replicate(c)^2 * dt2
+ * in the ghost layout (nefi/physics/wave.py:222-240, 718). `n_abs` is the layer width per axis.
+ */
+int nw_prepare_medium(const nw_grid* g, const int32_t* n_abs, const void* c, double dt2,
+                      void* c2dt2, void* stream);
+
+/*
+ * Copy per-shot physical fields (n_shots, n...) into ghost-layout levels with a zero layer
+ * (WaveGrid.pad(.., "zeros"), nefi/physics/wave.py:226-230) and form
+ * p^-1 = p^0 + 1/2 c2dt2 * Lap p^0 (nefi/physics/wave.py:849-850).
+ * Writes level p^0 into `p0_level` and p^-1 into `pm1_level` (each n_shots fields).
+ */
+int nw_initial_state(const nw_grid* g, const int32_t* n_abs, const nw_medium* m, int32_t n_shots,
+                     const void* p0, void* pm1_level, void* p0_level, void* stream);
+
+/*
+ * Forward run of steps [n_begin, n_end) for all shots. Levels are addressed through `st`
+ * (history, or the ring when no history is given). Receiver samples of every recorded level
+ * n in [n_begin, n_end] go to traces (n_shots, n_rec, n_t); with checkpointing, snapshots of
+ * every segment start in [n_begin, n_end) are encoded. On entry levels n_begin-1 and n_begin
+ * must be in place. Replaces WaveOperator.simulate / run_timestepping
+ * (nefi/physics/wave.py:699-740, nefi/physics/timestep.py:144-149).
+ */
+int nw_forward(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, const nw_time* t,
+               const nw_storage* st, int32_t n_begin, int32_t n_end, void* traces, void* stream);
+
+/*
+ * Adjoint run for all shots: from trace cotangents `grad_traces` (n_shots, n_rec, n_t) computes
+ *  - grad_c2dt2: per-shot accumulators (n_shots fields, dtype; zeroed by the call)
+ *    of sum_n mu^{n+1} * Lap p^n, and
+ *  - lambda0 / mu1 (n_shots fields each, may be NULL): the sensitivities of p^0 and A*p^1
+ *    needed by the initial-value operator.
+ * `work` holds three adjoint levels (3 * n_shots fields). Uses the history or recomputes
+ * segments from the snapshots in `st`. This is the discrete adjoint torch.autograd derives from
+ * nefi/physics/wave.py:529-552 and nefi/physics/timestep.py:151-169.
+ */
+int nw_adjoint(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, const nw_time* t,
+               const nw_storage* st, const void* grad_traces, void* work, void* grad_c2dt2,
+               void* lambda0, void* mu1, void* stream);
+
+/*
+ * Reduce per-shot c2dt2 gradients over shots in float64 and apply the chain rule of
+ * c2dt2 = pad_replicate(c)^2 dt^2: grad_c (physical grid, float64) =
+ * pad_replicate^T(2 c_pad dt2 * sum_shots g) (nefi/physics/wave.py:231-240, 718).
+ * `accumulate` != 0 adds into grad_c instead of overwriting it.
+ */
+int nw_reduce_grad_c(const nw_grid* g, const int32_t* n_abs, const void* c, double dt2,
+                     int32_t n_shots, const void* grad_c2dt2, int32_t accumulate, double* grad_c,
+                     void* stream);
+
+/*
+ * Gradient of the initial-value operator w.r.t. p0 (n_shots physical fields, dtype):
+ * lambda^0 + lambda^-1 + Lap(1/2 c2dt2 lambda^-1) cropped to the physical grid, with
+ * lambda^-1 = -B0 mu^1 (B0 = 1 when time.first_b_one). If grad_c2dt2 != NULL also adds
+ * 1/2 lambda^-1 * Lap p^0 to it (the c-dependence of p^-1, nefi/physics/wave.py:850).
+ */
+int nw_initial_state_adjoint(const nw_grid* g, const int32_t* n_abs, const nw_medium* m,
+                             const nw_time* t, int32_t n_shots, const void* lambda0,
+                             const void* mu1, const void* p0_level, void* grad_p0,
+                             void* grad_c2dt2, void* stream);
+
+/*
+ * Zero only the ghost cells of `n_fields` consecutive fields (e.g. a freshly allocated history),
+ * leaving interior cells untouched: the stencils then read zero outside the grid without a
+ * full memset of storage whose interior every step overwrites anyway.
+ */
+int nw_zero_ghosts(const nw_grid* g, void* fields, int64_t n_fields, void* stream);
+
+/* Number of kernels this library has enqueued since it was loaded (all threads). Host only. */
+uint64_t nw_launch_count(void);
+
+/* Receiver samples of one level (n_shots fields) into traces[:, :, j]. */
+int nw_sample(const nw_grid* g, const nw_acquisition* a, int32_t n_t, const void* level,
+              int32_t j, void* traces, void* stream);
+
+/*
+ * Synchronises `stream`, then returns and clears the device status word that kernels set on a
+ * detected failure (a non-finite snapshot block: NW_ERR_NONFINITE). The word is shared by all
+ * streams of the current device. NEFI raises OperatorError/SolverError for such failures
+ * (nefi/physics/wave.py:561-569, nefi/errors.py:22-27).
+ */
+int nw_status(void* stream);
+
+/* Message of the calling thread's last error ("" if none). Host only. */
+const char* nw_last_error(void);
+/* Library ABI version (NW_ABI_VERSION) and the CUDA architecture it was built for (e.g. 1000). */
+int nw_abi_version(void);
+int nw_built_arch(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NEFI_WAVE_H */

@@ -1,0 +1,16 @@
+"""nefi_b200 — B200-native acoustic leapfrog propagator and exact adjoint for NEFI.
+
+Public API:
+
+* :class:`WaveOperatorB200` — FWI operator, drop-in for ``nefi.physics.wave.WaveOperator``.
+* :class:`WaveInitialConditionOperatorB200` — photoacoustic operator, drop-in for
+  ``nefi.physics.wave.WaveInitialConditionOperator``.
+
+The compute path is the in-tree CUDA library ``libnefiwave.so`` (C ABI in
+``include/nefi_wave.h``); build it with ``python -m nefi_b200.build``.
+"""
+
+from .operators import WaveInitialConditionOperatorB200, WaveOperatorB200
+
+__all__ = ["WaveInitialConditionOperatorB200", "WaveOperatorB200"]
+__version__ = "0.1.0"

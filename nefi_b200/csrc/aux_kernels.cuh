@@ -1,0 +1,303 @@
+// aux_kernels.cuh — preparation, reduction and snapshot kernels of the leapfrog propagator.
+#pragma once
+#include "kernels.cuh"
+
+namespace nw {
+
+// Physical-grid index helpers: a padded cell (x, y, z) maps to the physical cell
+// clamp(x - a, 0, n - 1) per axis under replicate padding (nefi/physics/wave.py:231-240).
+struct PadMap {
+  int a0, a1, a2;  // layer widths
+  int m0, m1, m2;  // physical extents (m2 = 1 in 2-D)
+};
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// c2dt2[cell] = c[pad_replicate(cell)]^2 * dt2 over all padded cells (2-D: n2 = 1).
+template <typename T>
+__global__ void medium_kernel(KGrid<T> g, PadMap pm, const T* __restrict__ c, T dt2, int ndim,
+                              T* __restrict__ out) {
+  const long long cells = (long long)g.n0 * g.n1 * g.n2;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < cells;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int z = (int)(t % g.n2);
+    const int y = (int)((t / g.n2) % g.n1);
+    const int x = (int)(t / ((long long)g.n2 * g.n1));
+    long long src, dst;
+    if (ndim == 2) {  // (x, y) are the two axes, z == 0
+      const int i = clampi(x - pm.a0, 0, pm.m0 - 1), j = clampi(y - pm.a1, 0, pm.m1 - 1);
+      src = (long long)i * pm.m1 + j;
+      dst = g.origin + (long long)x * g.s0 + y;
+    } else {
+      const int i = clampi(x - pm.a0, 0, pm.m0 - 1), j = clampi(y - pm.a1, 0, pm.m1 - 1),
+                k = clampi(z - pm.a2, 0, pm.m2 - 1);
+      src = ((long long)i * pm.m1 + j) * pm.m2 + k;
+      dst = g.origin + (long long)x * g.s0 + (long long)y * g.s1 + z;
+    }
+    const T cv = c[src];
+    const T c2 = cv * cv;
+    out[dst] = c2 * dt2;
+  }
+}
+
+// Zero-padded copy of per-shot physical fields into ghost-layout levels.
+template <typename T>
+__global__ void pad_zero_kernel(KGrid<T> g, PadMap pm, int ndim, const T* __restrict__ p0,
+                                T* __restrict__ lvl) {
+  const int s = blockIdx.y;
+  const long long cells = (long long)pm.m0 * pm.m1 * pm.m2;
+  const T* src = p0 + (long long)s * cells;
+  T* dst = lvl + (long long)s * g.field;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < cells;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(t % pm.m2);
+    const int j = (int)((t / pm.m2) % pm.m1);
+    const int i = (int)(t / ((long long)pm.m2 * pm.m1));
+    long long d;
+    if (ndim == 2) d = g.origin + (long long)(i + pm.a0) * g.s0 + (j + pm.a1);
+    else d = g.origin + (long long)(i + pm.a0) * g.s0 + (long long)(j + pm.a1) * g.s1 + (k + pm.a2);
+    dst[d] = src[t];
+  }
+}
+
+template <typename T, int R>
+__device__ __forceinline__ T lap_at(const KGrid<T>& g, const T* __restrict__ p, long long i, int ndim) {
+  T l;
+  if (ndim == 2) {
+    l = g.wc * p[i] + g.w1a * (p[i - g.s0] + p[i + g.s0]) + g.w1b * (p[i - 1] + p[i + 1]);
+    if (R == 2) l += g.w2a * (p[i - 2 * g.s0] + p[i + 2 * g.s0]) + g.w2b * (p[i - 2] + p[i + 2]);
+  } else {
+    l = g.wc * p[i] + g.w1a * (p[i - g.s0] + p[i + g.s0]) + g.w1b * (p[i - g.s1] + p[i + g.s1]) +
+        g.w1c * (p[i - 1] + p[i + 1]);
+    if (R == 2)
+      l += g.w2a * (p[i - 2 * g.s0] + p[i + 2 * g.s0]) + g.w2b * (p[i - 2 * g.s1] + p[i + 2 * g.s1]) +
+           g.w2c * (p[i - 2] + p[i + 2]);
+  }
+  return l;
+}
+
+__device__ __forceinline__ bool cell_of(long long t, int n0, int n1, int n2, int ndim, int& x, int& y,
+                                        int& z) {
+  z = (int)(t % n2);
+  y = (int)((t / n2) % n1);
+  x = (int)(t / ((long long)n2 * n1));
+  return true;
+}
+
+template <typename T>
+__device__ __forceinline__ long long ghost_index(const KGrid<T>& g, int ndim, int x, int y, int z) {
+  return ndim == 2 ? g.origin + (long long)x * g.s0 + y
+                   : g.origin + (long long)x * g.s0 + (long long)y * g.s1 + z;
+}
+
+// p^-1 = p^0 + (0.5 c2dt2) * Lap p^0 over all padded cells (nefi/physics/wave.py:850).
+template <typename T, int R>
+__global__ void initial_prev_kernel(KGrid<T> g, int ndim, const T* __restrict__ C,
+                                    const T* __restrict__ p0, T* __restrict__ pm1) {
+  const int s = blockIdx.y;
+  const long long cells = (long long)g.n0 * g.n1 * g.n2;
+  const T* p = p0 + (long long)s * g.field;
+  T* out = pm1 + (long long)s * g.field;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < cells;
+       t += (long long)gridDim.x * blockDim.x) {
+    int x, y, z;
+    cell_of(t, g.n0, g.n1, g.n2, ndim, x, y, z);
+    const long long i = ghost_index(g, ndim, x, y, z);
+    const T h = T(0.5) * C[i];
+    out[i] = p[i] + h * lap_at<T, R>(g, p, i, ndim);
+  }
+}
+
+// Adjoint of the initial state: lambda^-1 = -B0 mu^1,
+// grad_p0p = lambda^0 + lambda^-1 + Lap(0.5 C lambda^-1), cropped to the physical grid;
+// optionally grad_C += 0.5 lambda^-1 Lap p^0.
+template <typename T, int R>
+__global__ void initial_adjoint_kernel(KGrid<T> g, PadMap pm, int ndim, const T* __restrict__ C,
+                                       const T* __restrict__ B, int b_one,
+                                       const T* __restrict__ lam0, const T* __restrict__ mu1,
+                                       const T* __restrict__ p0, T* __restrict__ grad_p0,
+                                       T* __restrict__ grad_c) {
+  const int s = blockIdx.y;
+  const long long cells = (long long)g.n0 * g.n1 * g.n2;
+  const long long so = (long long)s * g.field;
+  const T* m = mu1 + so;
+  const long long pcells = (long long)pm.m0 * pm.m1 * pm.m2;
+  auto lm1 = [&](long long i) -> T {
+    const T b = (b_one || B == nullptr) ? T(1) : B[i];
+    return -(b * m[i]);
+  };
+  auto hl = [&](long long i) -> T { return (T(0.5) * C[i]) * lm1(i); };
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < cells;
+       t += (long long)gridDim.x * blockDim.x) {
+    int x, y, z;
+    cell_of(t, g.n0, g.n1, g.n2, ndim, x, y, z);
+    const long long i = ghost_index(g, ndim, x, y, z);
+    const T l = lm1(i);
+    if (grad_c) grad_c[so + i] += (T(0.5) * l) * lap_at<T, R>(g, p0 + so, i, ndim);
+    int pi, pj, pk;
+    if (ndim == 2) { pi = x - pm.a0; pj = y - pm.a1; pk = 0; }
+    else { pi = x - pm.a0; pj = y - pm.a1; pk = z - pm.a2; }
+    if (pi < 0 || pi >= pm.m0 || pj < 0 || pj >= pm.m1 || pk < 0 || pk >= pm.m2) continue;
+    T lh;
+    if (ndim == 2) {
+      lh = g.wc * hl(i) + g.w1a * (hl(i - g.s0) + hl(i + g.s0)) + g.w1b * (hl(i - 1) + hl(i + 1));
+      if (R == 2) lh += g.w2a * (hl(i - 2 * g.s0) + hl(i + 2 * g.s0)) + g.w2b * (hl(i - 2) + hl(i + 2));
+    } else {
+      lh = g.wc * hl(i) + g.w1a * (hl(i - g.s0) + hl(i + g.s0)) + g.w1b * (hl(i - g.s1) + hl(i + g.s1)) +
+           g.w1c * (hl(i - 1) + hl(i + 1));
+      if (R == 2)
+        lh += g.w2a * (hl(i - 2 * g.s0) + hl(i + 2 * g.s0)) + g.w2b * (hl(i - 2 * g.s1) + hl(i + 2 * g.s1)) +
+              g.w2c * (hl(i - 2) + hl(i + 2));
+    }
+    const long long pidx = ((long long)pi * pm.m1 + pj) * pm.m2 + pk;
+    grad_p0[(long long)s * pcells + pidx] = (lam0[so + i] + l) + lh;
+  }
+}
+
+// grad_c[phys] (+)= 2 c dt2 * sum_shots sum_{padded cells -> phys} g_s[cell], in float64.
+template <typename T>
+__global__ void reduce_grad_kernel(KGrid<T> g, PadMap pm, int ndim, const T* __restrict__ c,
+                                   double dt2, int n_shots, const T* __restrict__ gs,
+                                   int accumulate, double* __restrict__ out) {
+  const long long pcells = (long long)pm.m0 * pm.m1 * pm.m2;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < pcells;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(t % pm.m2);
+    const int j = (int)((t / pm.m2) % pm.m1);
+    const int i = (int)(t / ((long long)pm.m2 * pm.m1));
+    // padded range mapping onto physical index i along an axis of width m with layer a
+    auto lo = [](int i, int a, int m) { return i == 0 ? 0 : i + a; };
+    auto hi = [](int i, int a, int m) { return i == m - 1 ? m + 2 * a - 1 : i + a; };
+    const int x0 = lo(i, pm.a0, pm.m0), x1 = hi(i, pm.a0, pm.m0);
+    const int y0 = lo(j, pm.a1, pm.m1), y1 = hi(j, pm.a1, pm.m1);
+    const int z0 = ndim == 3 ? lo(k, pm.a2, pm.m2) : 0, z1 = ndim == 3 ? hi(k, pm.a2, pm.m2) : 0;
+    double acc = 0.0;
+    for (int s = 0; s < n_shots; ++s) {
+      const T* gp = gs + (long long)s * g.field;
+      for (int x = x0; x <= x1; ++x)
+        for (int y = y0; y <= y1; ++y)
+          for (int z = z0; z <= z1; ++z) acc += (double)gp[ghost_index(g, ndim, x, y, z)];
+    }
+    const double v = 2.0 * (double)c[t] * dt2 * acc;
+    out[t] = accumulate ? out[t] + v : v;
+  }
+}
+
+// Zero the ghost cells of n_fields consecutive fields (a warp per storage row): whole rows
+// outside the grid and the tail [n_last, ld) of every data row. Interior cells are untouched.
+template <typename T>
+__global__ void zero_ghosts_kernel(T* __restrict__ base, long long field, long long n_rows,
+                                   int ld, int n_last, int ndim, int r, int n0, int n1,
+                                   int rows_per_plane, long long n_fields) {
+  const long long warps = (long long)gridDim.x * (blockDim.x / 32);
+  const int lane = threadIdx.x & 31;
+  for (long long w = (long long)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; w < n_rows * n_fields;
+       w += warps) {
+    const long long f = w / n_rows, row = w % n_rows;
+    bool ghost_row;
+    if (ndim == 2) {
+      ghost_row = row < r || row >= r + n0;
+    } else {
+      const long long plane = row / rows_per_plane, y = row % rows_per_plane;
+      ghost_row = plane < r || plane >= r + n0 || y >= n1;
+    }
+    T* p = base + f * field + row * ld;
+    for (int z = ghost_row ? lane : n_last + lane; z < ld; z += 32) p[z] = T(0);
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Snapshot codec: blocks of SNAP_BLOCK contiguous elements of one field, each stored as
+// 16-bit values with one power-of-two float scale (block floating point).
+// ------------------------------------------------------------------------------------------
+constexpr int SNAP_BLOCK = 1024;
+
+template <typename H>
+struct Half16;
+template <>
+struct Half16<__half> {
+  static __device__ __forceinline__ __half enc(float v) { return __float2half_rn(v); }
+  static __device__ __forceinline__ float dec(__half v) { return __half2float(v); }
+  static constexpr int kExpMax = 15;  // |v / scale| <= 2^15 < 65504
+};
+template <>
+struct Half16<__nv_bfloat16> {
+  static __device__ __forceinline__ __nv_bfloat16 enc(float v) { return __float2bfloat16_rn(v); }
+  static __device__ __forceinline__ float dec(__nv_bfloat16 v) { return __bfloat162float(v); }
+  static constexpr int kExpMax = 0;
+};
+
+__device__ int g_status;  // sticky device status word (NW_ERR_* or 0)
+
+// One CTA of 256 threads per block; grid.x = blocks per field, grid.y = fields.
+template <typename T, typename H>
+__global__ void __launch_bounds__(256) snap_encode(const T* __restrict__ src, long long field,
+                                                   int nblk, H* __restrict__ vals,
+                                                   float* __restrict__ scales) {
+  const int b = blockIdx.x, f = blockIdx.y;
+  const long long off = (long long)b * SNAP_BLOCK;
+  const T* p = src + (long long)f * field + off;
+  const long long n = min((long long)SNAP_BLOCK, field - off);
+  float v[4];
+  float mx = 0.f;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int e = threadIdx.x + 256 * k;
+    v[k] = e < n ? (float)p[e] : 0.f;
+    mx = fmaxf(mx, fabsf(v[k]));
+    if (!(fabsf(v[k]) <= 3.0e38f)) mx = __int_as_float(0x7fc00000);  // NaN/Inf poisons the block
+  }
+  __shared__ float red[8];
+  for (int o = 16; o > 0; o >>= 1) {
+    const float other = __shfl_xor_sync(0xffffffffu, mx, o);
+    mx = (isnan(other) || isnan(mx)) ? __int_as_float(0x7fc00000) : fmaxf(mx, other);
+  }
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    float m = threadIdx.x < 8 ? red[threadIdx.x] : 0.f;
+    for (int o = 4; o > 0; o >>= 1) {
+      const float other = __shfl_xor_sync(0xffffffffu, m, o);
+      m = (isnan(other) || isnan(m)) ? __int_as_float(0x7fc00000) : fmaxf(m, other);
+    }
+    if (threadIdx.x == 0) red[0] = m;
+  }
+  __syncthreads();
+  mx = red[0];
+  float scale = 1.f;
+  if (isnan(mx)) {
+    scale = mx;
+    if (threadIdx.x == 0) atomicExch(&g_status, 4);
+  } else if (mx > 0.f) {
+    int e;
+    frexpf(mx, &e);  // mx <= 2^e
+    scale = ldexpf(1.f, e - Half16<H>::kExpMax);
+  }
+  const float inv = isnan(scale) ? 0.f : 1.f / scale;  // exact: scale is a power of two
+  H* q = vals + ((long long)f * nblk + b) * SNAP_BLOCK;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) q[threadIdx.x + 256 * k] = Half16<H>::enc(v[k] * inv);
+  if (threadIdx.x == 0) scales[(long long)f * nblk + b] = scale;
+}
+
+template <typename T, typename H>
+__global__ void __launch_bounds__(256) snap_decode(const H* __restrict__ vals,
+                                                   const float* __restrict__ scales, int nblk,
+                                                   long long field, T* __restrict__ dst) {
+  const int b = blockIdx.x, f = blockIdx.y;
+  const long long off = (long long)b * SNAP_BLOCK;
+  const long long n = min((long long)SNAP_BLOCK, field - off);
+  const float scale = scales[(long long)f * nblk + b];
+  if (!(fabsf(scale) <= 3.0e38f) || !(scale > 0.f)) {
+    if (threadIdx.x == 0) atomicExch(&g_status, 4);
+  }
+  const H* q = vals + ((long long)f * nblk + b) * SNAP_BLOCK;
+  T* p = dst + (long long)f * field + off;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int e = threadIdx.x + 256 * k;
+    if (e < n) p[e] = (T)(Half16<H>::dec(q[e]) * scale);
+  }
+}
+
+}  // namespace nw

@@ -1,0 +1,630 @@
+// wave_capi.cu — host drivers and the extern "C" entry points declared in include/nefi_wave.h.
+//
+// The drivers run whole time loops on the caller's stream (one kernel launch per leapfrog step,
+// plus the receiver/adjoint-source kernels), so a forward or adjoint sweep costs one call from
+// the host language. No device memory is allocated here: every buffer comes from the caller.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/nefi_wave.h"
+#include "aux_kernels.cuh"
+#include "kernels.cuh"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define NW_CUDA(expr)                                                                  \
+  do {                                                                                 \
+    cudaError_t e_ = (expr);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return fail(NW_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_));    \
+  } while (0)
+
+// Kernels enqueued by this library since load (host-side count, all threads).
+std::atomic<unsigned long long> g_launches{0};
+
+#define NW_LAUNCHED()                                                                  \
+  do {                                                                                 \
+    g_launches.fetch_add(1, std::memory_order_relaxed);                                \
+    cudaError_t e_ = cudaGetLastError();                                               \
+    if (e_ != cudaSuccess)                                                             \
+      return fail(NW_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+int check_grid(const nw_grid* g) {
+  if (!g) return fail(NW_ERR_ARG, "grid is NULL");
+  if (g->ndim != 2 && g->ndim != 3) return fail(NW_ERR_UNSUPPORTED, "ndim must be 2 or 3");
+  if (g->order != 2 && g->order != 4) return fail(NW_ERR_ARG, "order must be 2 or 4");
+  if (g->dtype != NW_F32 && g->dtype != NW_F64) return fail(NW_ERR_ARG, "dtype must be NW_F32 or NW_F64");
+  if (g->absorbing < NW_ABS_NONE || g->absorbing > NW_ABS_CERJAN)
+    return fail(NW_ERR_UNSUPPORTED, "absorbing kind not built");
+  for (int a = 0; a < g->ndim; ++a)
+    if (g->n[a] < 2) return fail(NW_ERR_ARG, "every padded extent must be >= 2");
+  if (g->field_elems <= 0 || g->radius != g->order / 2)
+    return fail(NW_ERR_ARG, "grid layout not initialised (call nw_grid_layout)");
+  return NW_OK;
+}
+
+template <typename T>
+nw::KGrid<T> kgrid(const nw_grid* g) {
+  nw::KGrid<T> k;
+  k.n0 = g->n[0];
+  k.n1 = g->n[1];
+  k.n2 = g->ndim == 3 ? g->n[2] : 1;
+  k.lo0 = g->core_lo[0]; k.lo1 = g->core_lo[1]; k.lo2 = g->ndim == 3 ? g->core_lo[2] : 0;
+  k.hi0 = g->core_hi[0]; k.hi1 = g->core_hi[1]; k.hi2 = g->ndim == 3 ? g->core_hi[2] : 1;
+  k.s0 = g->stride[0];
+  k.s1 = g->stride[1];
+  k.origin = g->origin;
+  k.field = g->field_elems;
+  k.wc = (T)g->w_center;
+  k.w1a = (T)g->w1[0]; k.w1b = (T)g->w1[1]; k.w1c = (T)g->w1[2];
+  k.w2a = (T)g->w2[0]; k.w2b = (T)g->w2[1]; k.w2c = (T)g->w2[2];
+  return k;
+}
+
+nw::PadMap padmap(const nw_grid* g, const int32_t* n_abs) {
+  nw::PadMap p;
+  p.a0 = n_abs[0]; p.a1 = n_abs[1]; p.a2 = g->ndim == 3 ? n_abs[2] : 0;
+  p.m0 = g->n[0] - 2 * p.a0; p.m1 = g->n[1] - 2 * p.a1;
+  p.m2 = g->ndim == 3 ? g->n[2] - 2 * p.a2 : 1;
+  return p;
+}
+
+constexpr int kRX = 4;  // rows (2-D) or planes (3-D) per thread
+
+// Launch shape of the stencil kernels: 32 x 8 threads, each owning kRX cells along axis 0.
+struct Shape {
+  dim3 grid, block;
+};
+Shape stencil_shape(const nw_grid* g, int n_shots) {
+  Shape s;
+  s.block = dim3(32, 8, 1);
+  if (g->ndim == 2) {
+    s.grid = dim3((g->n[1] + 31) / 32, (g->n[0] + 8 * kRX - 1) / (8 * kRX), n_shots);
+  } else {
+    const unsigned zt = (g->n[2] + 31) / 32, yt = (g->n[1] + 7) / 8;
+    s.grid = dim3(zt * yt, (g->n[0] + kRX - 1) / kRX, n_shots);
+  }
+  return s;
+}
+
+template <typename T>
+int launch_fwd(const nw_grid* g, const nw::KGrid<T>& kg, const nw::FwdStep<T>& st, int n_shots,
+               bool ab, cudaStream_t s) {
+  Shape sh = stencil_shape(g, n_shots);
+  const int r = g->radius;
+#define NW_FWD(D, R, AB) nw::fwd##D##d<T, R, AB, kRX><<<sh.grid, sh.block, 0, s>>>(kg, st)
+  if (g->ndim == 2) {
+    if (r == 1) { if (ab) NW_FWD(2, 1, true); else NW_FWD(2, 1, false); }
+    else        { if (ab) NW_FWD(2, 2, true); else NW_FWD(2, 2, false); }
+  } else {
+    if (r == 1) { if (ab) NW_FWD(3, 1, true); else NW_FWD(3, 1, false); }
+    else        { if (ab) NW_FWD(3, 2, true); else NW_FWD(3, 2, false); }
+  }
+#undef NW_FWD
+  NW_LAUNCHED();
+  return NW_OK;
+}
+
+template <typename T>
+int launch_adj(const nw_grid* g, const nw::KGrid<T>& kg, const nw::AdjStep<T>& st, int n_shots,
+               bool ab, cudaStream_t s) {
+  Shape sh = stencil_shape(g, n_shots);
+  const int r = g->radius;
+#define NW_ADJ(D, R, AB) nw::adj##D##d<T, R, AB, kRX><<<sh.grid, sh.block, 0, s>>>(kg, st)
+  if (g->ndim == 2) {
+    if (r == 1) { if (ab) NW_ADJ(2, 1, true); else NW_ADJ(2, 1, false); }
+    else        { if (ab) NW_ADJ(2, 2, true); else NW_ADJ(2, 2, false); }
+  } else {
+    if (r == 1) { if (ab) NW_ADJ(3, 1, true); else NW_ADJ(3, 1, false); }
+    else        { if (ab) NW_ADJ(3, 2, true); else NW_ADJ(3, 2, false); }
+  }
+#undef NW_ADJ
+  NW_LAUNCHED();
+  return NW_OK;
+}
+
+template <typename T>
+int launch_sample(const nw_grid* g, const nw_acquisition* a, int n_t, const T* lvl, int j, T* traces,
+                  cudaStream_t s) {
+  if (a->n_rec <= 0) return NW_OK;
+  dim3 grid((a->n_rec + 127) / 128, a->n_shots);
+  if (g->ndim == 2)
+    nw::sample_kernel<T, 4><<<grid, 128, 0, s>>>(lvl, g->field_elems, traces, a->rec_index,
+                                                 (const T*)a->rec_weight, a->n_rec, n_t, j);
+  else
+    nw::sample_kernel<T, 8><<<grid, 128, 0, s>>>(lvl, g->field_elems, traces, a->rec_index,
+                                                 (const T*)a->rec_weight, a->n_rec, n_t, j);
+  NW_LAUNCHED();
+  return NW_OK;
+}
+
+// ---- snapshot pool layout: per snapshot, 2 levels x n_shots fields ------------------------
+struct SnapLayout {
+  int nblk;             // blocks per field
+  size_t vals_bytes;    // 16-bit payload of one snapshot
+  size_t scale_bytes;   // scales of one snapshot
+  size_t exact_bytes;   // exact copy of one snapshot
+  size_t per_snap(int kind) const {
+    return kind == NW_SNAP_EXACT ? exact_bytes : ((vals_bytes + scale_bytes + 255) / 256) * 256;
+  }
+};
+SnapLayout snap_layout(const nw_grid* g, int n_shots) {
+  SnapLayout L;
+  const size_t esz = g->dtype == NW_F64 ? 8 : 4;
+  L.nblk = (int)((g->field_elems + nw::SNAP_BLOCK - 1) / nw::SNAP_BLOCK);
+  const size_t fields = 2 * (size_t)n_shots;
+  L.vals_bytes = fields * L.nblk * nw::SNAP_BLOCK * 2;
+  L.scale_bytes = fields * L.nblk * sizeof(float);
+  L.exact_bytes = fields * g->field_elems * esz;
+  return L;
+}
+
+// Encodes levels (lm1, l0) (each n_shots fields, contiguous) into snapshot j.
+template <typename T>
+int snap_store(const nw_grid* g, const nw_storage* st, int n_shots, const T* lm1, const T* l0, int j,
+               cudaStream_t s) {
+  SnapLayout L = snap_layout(g, n_shots);
+  char* base = (char*)st->snap + (size_t)j * L.per_snap(st->snap_kind);
+  const size_t lvl_bytes = (size_t)n_shots * g->field_elems * sizeof(T);
+  if (st->snap_kind == NW_SNAP_EXACT) {
+    NW_CUDA(cudaMemcpyAsync(base, lm1, lvl_bytes, cudaMemcpyDeviceToDevice, s));
+    NW_CUDA(cudaMemcpyAsync(base + lvl_bytes, l0, lvl_bytes, cudaMemcpyDeviceToDevice, s));
+    return NW_OK;
+  }
+  float* scales = (float*)(base + L.vals_bytes);
+  const size_t half_fields = (size_t)n_shots * L.nblk * nw::SNAP_BLOCK;
+  dim3 grid(L.nblk, n_shots);
+  for (int lv = 0; lv < 2; ++lv) {
+    const T* src = lv == 0 ? lm1 : l0;
+    float* sc = scales + (size_t)lv * n_shots * L.nblk;
+    if (st->snap_kind == NW_SNAP_F16) {
+      __half* v = (__half*)base + lv * half_fields;
+      nw::snap_encode<T, __half><<<grid, 256, 0, s>>>(src, g->field_elems, L.nblk, v, sc);
+    } else {
+      __nv_bfloat16* v = (__nv_bfloat16*)base + lv * half_fields;
+      nw::snap_encode<T, __nv_bfloat16><<<grid, 256, 0, s>>>(src, g->field_elems, L.nblk, v, sc);
+    }
+    NW_LAUNCHED();
+  }
+  return NW_OK;
+}
+
+template <typename T>
+int snap_load(const nw_grid* g, const nw_storage* st, int n_shots, int j, T* lm1, T* l0,
+              cudaStream_t s) {
+  SnapLayout L = snap_layout(g, n_shots);
+  const char* base = (const char*)st->snap + (size_t)j * L.per_snap(st->snap_kind);
+  const size_t lvl_bytes = (size_t)n_shots * g->field_elems * sizeof(T);
+  if (st->snap_kind == NW_SNAP_EXACT) {
+    NW_CUDA(cudaMemcpyAsync(lm1, base, lvl_bytes, cudaMemcpyDeviceToDevice, s));
+    NW_CUDA(cudaMemcpyAsync(l0, base + lvl_bytes, lvl_bytes, cudaMemcpyDeviceToDevice, s));
+    return NW_OK;
+  }
+  const float* scales = (const float*)(base + L.vals_bytes);
+  const size_t half_fields = (size_t)n_shots * L.nblk * nw::SNAP_BLOCK;
+  dim3 grid(L.nblk, n_shots);
+  for (int lv = 0; lv < 2; ++lv) {
+    T* dst = lv == 0 ? lm1 : l0;
+    const float* sc = scales + (size_t)lv * n_shots * L.nblk;
+    if (st->snap_kind == NW_SNAP_F16)
+      nw::snap_decode<T, __half><<<grid, 256, 0, s>>>((const __half*)base + lv * half_fields, sc,
+                                                      L.nblk, g->field_elems, dst);
+    else
+      nw::snap_decode<T, __nv_bfloat16><<<grid, 256, 0, s>>>(
+          (const __nv_bfloat16*)base + lv * half_fields, sc, L.nblk, g->field_elems, dst);
+    NW_LAUNCHED();
+  }
+  return NW_OK;
+}
+
+// ---- forward driver ---------------------------------------------------------------------
+template <typename T>
+struct Levels {  // address of time level n (n >= -1) in history, ring or segment buffer
+  T* base;
+  long long level_elems;
+  int mode;  // 0 history, 1 ring, 2 segment (offset n0)
+  int n0;
+  T* at(int n) const {
+    if (mode == 0) return base + (long long)(n + 1) * level_elems;
+    if (mode == 1) return base + (long long)((n + 1) % 3) * level_elems;
+    return base + (long long)(n - n0 + 1) * level_elems;
+  }
+};
+
+template <typename T>
+nw::FwdStep<T> fwd_step_args(const nw_grid* g, const nw_medium* m, const nw_acquisition* a,
+                             const nw_time* t, const Levels<T>& L, int n, T* traces) {
+  nw::FwdStep<T> st;
+  st.prev = L.at(n - 1);
+  st.cur = L.at(n);
+  st.next = L.at(n + 1);
+  st.C = (const T*)m->c2dt2;
+  st.A = (const T*)m->coef_a;
+  st.B = (const T*)m->coef_b;
+  st.b_one = (n == 0 && t->first_b_one) ? 1 : 0;
+  st.src_corner = a->has_source ? a->src_corner : nullptr;
+  st.src_w = (const T*)a->src_weight;
+  st.wavelet = (const T*)a->wavelet;
+  st.n = n;
+  const bool rec = traces && a->n_rec > 0 && (n % t->substeps) == 0;
+  st.traces = rec ? traces : nullptr;
+  st.rec_idx = a->rec_index;
+  st.rec_w = (const T*)a->rec_weight;
+  st.n_rec = a->n_rec;
+  st.n_t = t->n_t;
+  st.j = n / t->substeps;
+  return st;
+}
+
+template <typename T>
+int forward_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, const nw_time* t,
+                 const nw_storage* st, int n_begin, int n_end, T* traces, cudaStream_t s) {
+  const long long LE = (long long)a->n_shots * g->field_elems;
+  Levels<T> L;
+  L.level_elems = LE;
+  L.n0 = 0;
+  if (st->history) { L.base = (T*)st->history; L.mode = 0; }
+  else if (st->ring) { L.base = (T*)st->ring; L.mode = 1; }
+  else return fail(NW_ERR_ARG, "storage needs a history or a ring buffer");
+  const bool ckpt = !st->history && st->snap;
+  if (ckpt && st->segment < 1) return fail(NW_ERR_ARG, "segment must be >= 1");
+  const nw::KGrid<T> kg = kgrid<T>(g);
+  const bool ab = m->coef_a != nullptr;
+  for (int n = n_begin; n < n_end; ++n) {
+    if (ckpt && n % st->segment == 0) {
+      int rc = snap_store<T>(g, st, a->n_shots, L.at(n - 1), L.at(n), n / st->segment, s);
+      if (rc) return rc;
+    }
+    int rc = launch_fwd<T>(g, kg, fwd_step_args<T>(g, m, a, t, L, n, traces), a->n_shots, ab, s);
+    if (rc) return rc;
+  }
+  if (traces && n_end == t->n_steps && t->n_steps % t->substeps == 0) {
+    int rc = launch_sample<T>(g, a, t->n_t, L.at(n_end), n_end / t->substeps, traces, s);
+    if (rc) return rc;
+  }
+  return NW_OK;
+}
+
+// ---- adjoint driver ---------------------------------------------------------------------
+template <typename T>
+int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, const nw_time* t,
+                 const nw_storage* st, const T* gtr, T* work, T* grad, T* lambda0, T* mu1,
+                 cudaStream_t s) {
+  const int N = t->n_steps, M = t->substeps, S = a->n_shots;
+  const long long LE = (long long)S * g->field_elems;
+  const size_t lvl_bytes = (size_t)LE * sizeof(T);
+  const nw::KGrid<T> kg = kgrid<T>(g);
+  const bool ab = m->coef_a != nullptr;
+  NW_CUDA(cudaMemsetAsync(work, 0, 3 * lvl_bytes, s));
+  NW_CUDA(cudaMemsetAsync(grad, 0, lvl_bytes, s));
+  auto mu = [&](int n) { return work + (long long)(n % 3) * LE; };
+  const bool hist = st->history != nullptr;
+  const bool ckpt = !hist && st->snap != nullptr;
+  if (!hist && !ckpt && N > 0) return fail(NW_ERR_ARG, "adjoint needs a history or snapshots");
+  const int K = ckpt ? st->segment : 0;
+  Levels<T> H;
+  H.level_elems = LE;
+  H.mode = 0;
+  H.n0 = 0;
+  H.base = hist ? (T*)st->history : nullptr;
+  Levels<T> SEG;
+  SEG.level_elems = LE;
+  SEG.mode = 2;
+  SEG.base = ckpt ? (T*)st->segbuf : nullptr;
+  SEG.n0 = -1;
+  const int n_stop = lambda0 ? 0 : 1;
+  dim3 ig(((a->n_cells > 0 ? a->n_cells : 1) + 127) / 128, S);
+  auto inject = [&](int n) -> int {
+    if (a->n_cells <= 0 || n % M != 0) return NW_OK;
+    nw::inject_kernel<T><<<ig, 128, 0, s>>>(mu(n), g->field_elems, (const T*)m->coef_a, n >= 1 ? 1 : 0,
+                                            gtr, a->n_rec, t->n_t, n / M, a->n_cells, a->cell_index,
+                                            a->cell_ptr, a->cell_rec, (const T*)a->cell_weight);
+    NW_LAUNCHED();
+    return NW_OK;
+  };
+  // level N: mu^N = A R^T g_N (the buffers start at zero)
+  if (N >= n_stop) {
+    int rc = inject(N);
+    if (rc) return rc;
+  }
+  for (int n = N - 1; n >= n_stop; --n) {
+    const T* pn;
+    if (hist) {
+      pn = H.at(n);
+    } else {
+      const int n0 = (n / K) * K;
+      if (SEG.n0 != n0) {  // entering a segment from its end: recompute p^{n0..n1-1}
+        const int n1 = std::min(n0 + K, N);
+        SEG.n0 = n0;
+        int rc = snap_load<T>(g, st, S, n0 / K, SEG.at(n0 - 1), SEG.at(n0), s);
+        if (rc) return rc;
+        for (int k = n0; k < n1 - 1; ++k) {
+          rc = launch_fwd<T>(g, kg, fwd_step_args<T>(g, m, a, t, SEG, k, nullptr), S, ab, s);
+          if (rc) return rc;
+        }
+      }
+      pn = SEG.at(n);
+    }
+    nw::AdjStep<T> as;
+    as.mu1 = mu(n + 1);
+    as.mu2 = mu(n + 2);
+    as.out = mu(n);
+    as.C = (const T*)m->c2dt2;
+    as.A = (const T*)m->coef_a;
+    as.B = (const T*)m->coef_b;
+    as.apply_a = n >= 1 ? 1 : 0;
+    as.p = pn;
+    as.grad = grad;
+    int rc = launch_adj<T>(g, kg, as, S, ab, s);
+    if (rc) return rc;
+    rc = inject(n);
+    if (rc) return rc;
+  }
+  if (lambda0) {
+    if (N == 0) {  // no step: lambda^0 = R^T g_0, mu^1 = 0
+      NW_CUDA(cudaMemcpyAsync(lambda0, mu(0), lvl_bytes, cudaMemcpyDeviceToDevice, s));
+      if (mu1) NW_CUDA(cudaMemsetAsync(mu1, 0, lvl_bytes, s));
+    } else {
+      NW_CUDA(cudaMemcpyAsync(lambda0, mu(0), lvl_bytes, cudaMemcpyDeviceToDevice, s));
+      if (mu1) NW_CUDA(cudaMemcpyAsync(mu1, mu(1), lvl_bytes, cudaMemcpyDeviceToDevice, s));
+    }
+  }
+  return NW_OK;
+}
+
+int grid_blocks(long long work, int threads) {
+  long long b = (work + threads - 1) / threads;
+  return (int)std::max(1LL, std::min(b, 148LL * 32));
+}
+
+}  // namespace
+
+// =============================================================================================
+extern "C" {
+
+int nw_abi_version(void) { return NW_ABI_VERSION; }
+int nw_built_arch(void) { return 1000; }
+const char* nw_last_error(void) { return g_err.c_str(); }
+
+int nw_grid_layout(nw_grid* g) {
+  if (!g) return fail(NW_ERR_ARG, "grid is NULL");
+  if (g->ndim != 2 && g->ndim != 3) return fail(NW_ERR_UNSUPPORTED, "ndim must be 2 or 3");
+  if (g->order != 2 && g->order != 4) return fail(NW_ERR_ARG, "order must be 2 or 4");
+  const int r = g->order / 2;
+  g->radius = r;
+  const int last = g->ndim - 1;
+  const long long ld = ((long long)g->n[last] + r + 31) / 32 * 32;
+  if (g->ndim == 2) {
+    g->stride[0] = ld;
+    g->stride[1] = 1;
+    g->stride[2] = 0;
+    g->origin = (long long)r * ld;
+    g->field_elems = ((long long)g->n[0] + 2 * r) * ld;
+  } else {
+    const long long rows = (long long)g->n[1] + r;
+    g->stride[0] = rows * ld;
+    g->stride[1] = ld;
+    g->stride[2] = 1;
+    g->origin = (long long)r * rows * ld;
+    g->field_elems = ((long long)g->n[0] + 2 * r) * rows * ld;
+  }
+  return NW_OK;
+}
+
+size_t nw_snapshot_bytes(const nw_grid* g, int32_t n_shots, int32_t n_snap, int32_t snap_kind) {
+  if (!g || n_shots < 1 || n_snap < 0) return 0;
+  return snap_layout(g, n_shots).per_snap(snap_kind) * (size_t)n_snap;
+}
+
+int nw_prepare_medium(const nw_grid* g, const int32_t* n_abs, const void* c, double dt2, void* c2dt2,
+                      void* stream) {
+  int rc = check_grid(g);
+  if (rc) return rc;
+  if (!c || !c2dt2 || !n_abs) return fail(NW_ERR_ARG, "NULL pointer");
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t esz = g->dtype == NW_F64 ? 8 : 4;
+  NW_CUDA(cudaMemsetAsync(c2dt2, 0, g->field_elems * esz, s));
+  const nw::PadMap pm = padmap(g, n_abs);
+  const long long cells = (long long)g->n[0] * g->n[1] * (g->ndim == 3 ? g->n[2] : 1);
+  const int blocks = grid_blocks(cells, 256);
+  if (g->dtype == NW_F32)
+    nw::medium_kernel<float><<<blocks, 256, 0, s>>>(kgrid<float>(g), pm, (const float*)c, (float)dt2,
+                                                    g->ndim, (float*)c2dt2);
+  else
+    nw::medium_kernel<double><<<blocks, 256, 0, s>>>(kgrid<double>(g), pm, (const double*)c, dt2,
+                                                     g->ndim, (double*)c2dt2);
+  NW_LAUNCHED();
+  return NW_OK;
+}
+
+int nw_initial_state(const nw_grid* g, const int32_t* n_abs, const nw_medium* m, int32_t n_shots,
+                     const void* p0, void* pm1_level, void* p0_level, void* stream) {
+  int rc = check_grid(g);
+  if (rc) return rc;
+  if (!m || !p0 || !pm1_level || !p0_level || !n_abs || n_shots < 1)
+    return fail(NW_ERR_ARG, "invalid initial-state arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t esz = g->dtype == NW_F64 ? 8 : 4;
+  const size_t lvl = (size_t)n_shots * g->field_elems * esz;
+  NW_CUDA(cudaMemsetAsync(p0_level, 0, lvl, s));
+  NW_CUDA(cudaMemsetAsync(pm1_level, 0, lvl, s));
+  const nw::PadMap pm = padmap(g, n_abs);
+  const long long pcells = (long long)pm.m0 * pm.m1 * pm.m2;
+  const long long cells = (long long)g->n[0] * g->n[1] * (g->ndim == 3 ? g->n[2] : 1);
+  dim3 gp(grid_blocks(pcells, 256), n_shots), gc(grid_blocks(cells, 256), n_shots);
+  if (g->dtype == NW_F32) {
+    auto kg = kgrid<float>(g);
+    nw::pad_zero_kernel<float><<<gp, 256, 0, s>>>(kg, pm, g->ndim, (const float*)p0, (float*)p0_level);
+    if (g->radius == 1)
+      nw::initial_prev_kernel<float, 1><<<gc, 256, 0, s>>>(kg, g->ndim, (const float*)m->c2dt2,
+                                                          (const float*)p0_level, (float*)pm1_level);
+    else
+      nw::initial_prev_kernel<float, 2><<<gc, 256, 0, s>>>(kg, g->ndim, (const float*)m->c2dt2,
+                                                          (const float*)p0_level, (float*)pm1_level);
+  } else {
+    auto kg = kgrid<double>(g);
+    nw::pad_zero_kernel<double><<<gp, 256, 0, s>>>(kg, pm, g->ndim, (const double*)p0, (double*)p0_level);
+    if (g->radius == 1)
+      nw::initial_prev_kernel<double, 1><<<gc, 256, 0, s>>>(kg, g->ndim, (const double*)m->c2dt2,
+                                                           (const double*)p0_level, (double*)pm1_level);
+    else
+      nw::initial_prev_kernel<double, 2><<<gc, 256, 0, s>>>(kg, g->ndim, (const double*)m->c2dt2,
+                                                           (const double*)p0_level, (double*)pm1_level);
+  }
+  g_launches.fetch_add(1, std::memory_order_relaxed);  // pad_zero_kernel
+  NW_LAUNCHED();
+  return NW_OK;
+}
+
+static int check_run(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, const nw_time* t,
+                     const nw_storage* st) {
+  int rc = check_grid(g);
+  if (rc) return rc;
+  if (!m || !a || !t || !st) return fail(NW_ERR_ARG, "NULL descriptor");
+  if (!m->c2dt2) return fail(NW_ERR_ARG, "medium.c2dt2 is NULL");
+  if ((g->absorbing != NW_ABS_NONE) != (m->coef_a != nullptr) || (m->coef_a == nullptr) != (m->coef_b == nullptr))
+    return fail(NW_ERR_ARG, "absorbing coefficients must be given exactly when absorbing != none");
+  if (a->n_shots < 1) return fail(NW_ERR_ARG, "n_shots must be >= 1");
+  if (a->n_shots > 65535) return fail(NW_ERR_ARG, "n_shots must be <= 65535");
+  if (a->has_source && (!a->src_corner || !a->src_weight || !a->wavelet))
+    return fail(NW_ERR_ARG, "source arrays are NULL");
+  if (a->n_rec > 0 && (!a->rec_index || !a->rec_weight)) return fail(NW_ERR_ARG, "receiver arrays are NULL");
+  if (t->substeps < 1 || t->n_t < 1 || t->n_steps != (t->n_t - 1) * t->substeps)
+    return fail(NW_ERR_ARG, "inconsistent time axis");
+  return NW_OK;
+}
+
+int nw_forward(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, const nw_time* t,
+               const nw_storage* st, int32_t n_begin, int32_t n_end, void* traces, void* stream) {
+  int rc = check_run(g, m, a, t, st);
+  if (rc) return rc;
+  if (n_begin < 0 || n_end < n_begin || n_end > t->n_steps) return fail(NW_ERR_ARG, "step range out of bounds");
+  if (g->dtype == NW_F32)
+    return forward_impl<float>(g, m, a, t, st, n_begin, n_end, (float*)traces, (cudaStream_t)stream);
+  return forward_impl<double>(g, m, a, t, st, n_begin, n_end, (double*)traces, (cudaStream_t)stream);
+}
+
+int nw_adjoint(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, const nw_time* t,
+               const nw_storage* st, const void* grad_traces, void* work, void* grad_c2dt2,
+               void* lambda0, void* mu1, void* stream) {
+  int rc = check_run(g, m, a, t, st);
+  if (rc) return rc;
+  if (!grad_traces || !work || !grad_c2dt2) return fail(NW_ERR_ARG, "NULL adjoint buffer");
+  if (a->n_cells > 0 && (!a->cell_index || !a->cell_ptr || !a->cell_rec || !a->cell_weight))
+    return fail(NW_ERR_ARG, "receiver adjoint table is NULL");
+  if (!st->history && st->snap && !st->segbuf) return fail(NW_ERR_ARG, "checkpointing needs segbuf");
+  if (g->dtype == NW_F32)
+    return adjoint_impl<float>(g, m, a, t, st, (const float*)grad_traces, (float*)work,
+                               (float*)grad_c2dt2, (float*)lambda0, (float*)mu1, (cudaStream_t)stream);
+  return adjoint_impl<double>(g, m, a, t, st, (const double*)grad_traces, (double*)work,
+                              (double*)grad_c2dt2, (double*)lambda0, (double*)mu1, (cudaStream_t)stream);
+}
+
+int nw_reduce_grad_c(const nw_grid* g, const int32_t* n_abs, const void* c, double dt2,
+                     int32_t n_shots, const void* grad_c2dt2, int32_t accumulate, double* grad_c,
+                     void* stream) {
+  int rc = check_grid(g);
+  if (rc) return rc;
+  if (!n_abs || !c || !grad_c2dt2 || !grad_c || n_shots < 1) return fail(NW_ERR_ARG, "invalid reduce arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  const nw::PadMap pm = padmap(g, n_abs);
+  const long long pcells = (long long)pm.m0 * pm.m1 * pm.m2;
+  const int blocks = grid_blocks(pcells, 128);
+  if (g->dtype == NW_F32)
+    nw::reduce_grad_kernel<float><<<blocks, 128, 0, s>>>(kgrid<float>(g), pm, g->ndim, (const float*)c, dt2,
+                                                         n_shots, (const float*)grad_c2dt2, accumulate, grad_c);
+  else
+    nw::reduce_grad_kernel<double><<<blocks, 128, 0, s>>>(kgrid<double>(g), pm, g->ndim, (const double*)c,
+                                                          dt2, n_shots, (const double*)grad_c2dt2, accumulate,
+                                                          grad_c);
+  NW_LAUNCHED();
+  return NW_OK;
+}
+
+int nw_initial_state_adjoint(const nw_grid* g, const int32_t* n_abs, const nw_medium* m,
+                             const nw_time* t, int32_t n_shots, const void* lambda0,
+                             const void* mu1, const void* p0_level, void* grad_p0,
+                             void* grad_c2dt2, void* stream) {
+  int rc = check_grid(g);
+  if (rc) return rc;
+  if (!m || !t || !n_abs || !lambda0 || !mu1 || !p0_level || !grad_p0 || n_shots < 1)
+    return fail(NW_ERR_ARG, "invalid initial-state adjoint arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  const nw::PadMap pm = padmap(g, n_abs);
+  const long long cells = (long long)g->n[0] * g->n[1] * (g->ndim == 3 ? g->n[2] : 1);
+  dim3 gc(grid_blocks(cells, 256), n_shots);
+  const int b_one = t->first_b_one;
+#define NW_IA(T, R)                                                                                   \
+  nw::initial_adjoint_kernel<T, R><<<gc, 256, 0, s>>>(kgrid<T>(g), pm, g->ndim, (const T*)m->c2dt2,   \
+                                                      (const T*)m->coef_b, b_one, (const T*)lambda0,  \
+                                                      (const T*)mu1, (const T*)p0_level, (T*)grad_p0, \
+                                                      (T*)grad_c2dt2)
+  if (g->dtype == NW_F32) { if (g->radius == 1) NW_IA(float, 1); else NW_IA(float, 2); }
+  else { if (g->radius == 1) NW_IA(double, 1); else NW_IA(double, 2); }
+#undef NW_IA
+  NW_LAUNCHED();
+  return NW_OK;
+}
+
+int nw_sample(const nw_grid* g, const nw_acquisition* a, int32_t n_t, const void* level, int32_t j,
+              void* traces, void* stream) {
+  int rc = check_grid(g);
+  if (rc) return rc;
+  if (!a || !level || !traces || j < 0 || j >= n_t) return fail(NW_ERR_ARG, "invalid sample arguments");
+  if (g->dtype == NW_F32)
+    return launch_sample<float>(g, a, n_t, (const float*)level, j, (float*)traces, (cudaStream_t)stream);
+  return launch_sample<double>(g, a, n_t, (const double*)level, j, (double*)traces, (cudaStream_t)stream);
+}
+
+int nw_zero_ghosts(const nw_grid* g, void* fields, int64_t n_fields, void* stream) {
+  int rc = check_grid(g);
+  if (rc) return rc;
+  if (!fields || n_fields < 0) return fail(NW_ERR_ARG, "invalid zero_ghosts arguments");
+  if (n_fields == 0) return NW_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int last = g->ndim - 1;
+  const int ld = (int)g->stride[last - 1];
+  const long long n_rows = g->field_elems / ld;
+  const int rows_per_plane = g->ndim == 3 ? (int)(g->stride[0] / g->stride[1]) : 1;
+  const int blocks = grid_blocks(n_rows * n_fields * 32, 256);
+  if (g->dtype == NW_F32)
+    nw::zero_ghosts_kernel<float><<<blocks, 256, 0, s>>>((float*)fields, g->field_elems, n_rows, ld, g->n[last],
+                                                         g->ndim, g->radius, g->n[0], g->n[1], rows_per_plane,
+                                                         n_fields);
+  else
+    nw::zero_ghosts_kernel<double><<<blocks, 256, 0, s>>>((double*)fields, g->field_elems, n_rows, ld, g->n[last],
+                                                          g->ndim, g->radius, g->n[0], g->n[1], rows_per_plane,
+                                                          n_fields);
+  NW_LAUNCHED();
+  return NW_OK;
+}
+
+uint64_t nw_launch_count(void) { return g_launches.load(); }
+
+// Synchronises `stream`, returns and clears the sticky device status word (NW_OK if clean).
+int nw_status(void* stream) {
+  NW_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+  int v = 0;
+  NW_CUDA(cudaMemcpyFromSymbol(&v, nw::g_status, sizeof(int)));
+  if (v) {
+    const int zero = 0;
+    NW_CUDA(cudaMemcpyToSymbol(nw::g_status, &zero, sizeof(int)));
+    return fail(v, "a snapshot block held a non-finite value or scale");
+  }
+  return NW_OK;
+}
+
+}  // extern "C"

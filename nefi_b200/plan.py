@@ -1,0 +1,189 @@
+"""Device-side tables of one operator at one (device, dtype): the ``nw_*`` descriptors.
+
+A :class:`DevicePlan` owns the constant device tensors (absorbing coefficients in the ghost layout,
+source/receiver stencils, the adjoint receiver table, the wavelet) and the ctypes descriptors that
+point at them. It is built once per operator, device and dtype and reused by every call, so a
+forward or adjoint sweep does no host-side geometry work.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import torch
+
+from . import _lib
+from ._compat import ConfigError
+from .geometry import PaddedGrid, cerjan_taper, sponge_coefficients, stencil_weights
+
+
+def ghost_layout(grid_struct: _lib.Grid) -> _lib.Grid:
+    _lib.check(_lib.load().nw_grid_layout(C.byref(grid_struct)))
+    return grid_struct
+
+
+def make_grid(grid: PaddedGrid, order: int, dtype: torch.dtype, absorbing: str) -> _lib.Grid:
+    g = _lib.Grid()
+    g.ndim = grid.d
+    g.order = order
+    g.dtype = _lib.dtype_code(dtype)
+    g.absorbing = {"none": _lib.NW_ABS_NONE, "sponge": _lib.NW_ABS_SPONGE,
+                   "cerjan": _lib.NW_ABS_CERJAN}[absorbing if any(grid.n_abs) else "none"]
+    for ax in range(3):
+        if ax < grid.d:
+            g.n[ax] = grid.padded_shape[ax]
+            g.core_lo[ax] = grid.n_abs[ax]
+            g.core_hi[ax] = grid.n_abs[ax] + grid.shape[ax]
+        else:
+            g.n[ax], g.core_lo[ax], g.core_hi[ax] = 1, 0, 1
+    wc, w1, w2 = stencil_weights(grid.spacing, order)
+    g.w_center = wc
+    for ax in range(3):
+        g.w1[ax] = w1[ax] if ax < grid.d else 0.0
+        g.w2[ax] = w2[ax] if ax < grid.d else 0.0
+    return ghost_layout(g)
+
+
+def to_ghost(g: _lib.Grid, dense: torch.Tensor, fill: float = 0.0) -> torch.Tensor:
+    """Place a padded-grid array ``(*P)`` into a flat ghost-layout buffer (host or device)."""
+    out = torch.full((g.field_elems,), fill, dtype=dense.dtype, device=dense.device)
+    view = ghost_view(g, out)
+    view.copy_(dense)
+    return out
+
+
+def ghost_view(g: _lib.Grid, flat: torch.Tensor) -> torch.Tensor:
+    """Strided view ``(..., *P)`` of the interior cells of ghost-layout field(s) in ``flat``."""
+    lead = flat.shape[:-1]
+    r = g.radius
+    if g.ndim == 2:
+        rows = flat.shape[-1] // g.stride[0]
+        v = flat.view(*lead, rows, g.stride[0])
+        return v[..., r:r + g.n[0], : g.n[1]]
+    planes = flat.shape[-1] // g.stride[0]
+    v = flat.view(*lead, planes, g.stride[0] // g.stride[1], g.stride[1])
+    return v[..., r:r + g.n[0], : g.n[1], : g.n[2]]
+
+
+def ghost_offsets(g: _lib.Grid, corner: torch.Tensor) -> torch.Tensor:
+    """Ghost-layout offsets ``(n, 2^d)`` of the stencil corners (same ordering as the weights)."""
+    d = g.ndim
+    out = torch.full((corner.shape[0], 1), int(g.origin), dtype=torch.long)
+    for ax in range(d):
+        hi = (corner[:, ax] + 1).clamp(max=g.n[ax] - 1)
+        pair = torch.stack([corner[:, ax], hi], 1) * int(g.stride[ax])
+        out = (out[:, :, None] + pair[:, None, :]).flatten(1)
+    return out
+
+
+class DevicePlan:
+    """Constant device tables of one operator (``op``) for ``device`` and ``dtype``."""
+
+    def __init__(self, op, device: torch.device, dtype: torch.dtype) -> None:
+        self.device, self.dtype = device, dtype
+        grid: PaddedGrid = op.grid
+        self.pgrid = grid
+        self.g = make_grid(grid, op.order, dtype, op.absorbing)
+        self.n_abs = (C.c_int32 * 3)(*(list(grid.n_abs) + [0] * (3 - grid.d)))
+        self.field = int(self.g.field_elems)
+        cast = {"device": device, "dtype": dtype}
+        # absorbing coefficients (interior cells are exactly 1, ghost cells 0)
+        self.A = self.B = None
+        if self.g.absorbing == _lib.NW_ABS_SPONGE:
+            a, b = sponge_coefficients(grid, op.c_max, op.absorb_R, op.dt)
+            self.A = to_ghost(self.g, a.to(dtype)).to(device)
+            self.B = to_ghost(self.g, b.to(dtype)).to(device)
+        elif self.g.absorbing == _lib.NW_ABS_CERJAN:
+            tp = cerjan_taper(grid, op.cerjan_gamma)
+            self.A = to_ghost(self.g, tp.to(dtype)).to(device)
+            self.B = self.A
+        self.first_b_one = 1 if self.g.absorbing == _lib.NW_ABS_CERJAN else 0
+        # receivers
+        corner, w = grid.point_stencils(op.receivers)
+        self.n_rec = int(corner.shape[0])
+        idx = ghost_offsets(self.g, corner)
+        self.rec_index = idx.to(device)
+        self.rec_weight = w.to(**cast)
+        # adjoint table: cells touched by receiver stencils, entries in (receiver, corner) order
+        flat = idx.reshape(-1)
+        rec_of = torch.arange(self.n_rec).repeat_interleave(idx.shape[1])
+        order = torch.argsort(flat, stable=True)
+        cells, counts = torch.unique_consecutive(flat[order], return_counts=True)
+        self.n_cells = int(cells.numel())
+        self.cell_index = cells.to(device)
+        ptr = torch.zeros(self.n_cells + 1, dtype=torch.int32)
+        ptr[1:] = torch.cumsum(counts, 0).to(torch.int32)
+        self.cell_ptr = ptr.to(device)
+        self.cell_rec = rec_of[order].to(torch.int32).to(device)
+        self.cell_weight = w.reshape(-1)[order].to(**cast)
+        # sources (FWI only)
+        self.has_source = hasattr(op, "sources")
+        if self.has_source:
+            sc, sw = grid.point_stencils(op.sources)
+            self.src_corner = sc.to(torch.int32).to(device)
+            self.src_weight = (sw / grid.cell_volume * op.dt**2).to(**cast)
+            self.wavelet = op.wavelet().to(**cast)
+        self.time = _lib.Time(op.n_steps, op.substeps, op.n_t, self.first_b_one)
+
+    # -- descriptors ------------------------------------------------------------------------
+    def medium(self, c2dt2: torch.Tensor) -> _lib.Medium:
+        return _lib.Medium(c2dt2.data_ptr(), _lib.ptr(self.A), _lib.ptr(self.B))
+
+    def acquisition(self, n_shots: int, shot0: int = 0) -> _lib.Acquisition:
+        a = _lib.Acquisition()
+        a.n_shots = n_shots
+        a.has_source = 1 if self.has_source else 0
+        if self.has_source:
+            a.src_corner = self.src_corner[shot0:].data_ptr()
+            a.src_weight = self.src_weight[shot0:].data_ptr()
+            a.wavelet = self.wavelet.data_ptr()
+        a.n_rec = self.n_rec
+        a.n_cells = self.n_cells
+        a.rec_index = self.rec_index.data_ptr()
+        a.rec_weight = self.rec_weight.data_ptr()
+        a.cell_index = self.cell_index.data_ptr()
+        a.cell_ptr = self.cell_ptr.data_ptr()
+        a.cell_rec = self.cell_rec.data_ptr()
+        a.cell_weight = self.cell_weight.data_ptr()
+        return a
+
+    def empty_levels(self, n_levels: int, n_shots: int, zero: bool = True) -> torch.Tensor:
+        fn = torch.zeros if zero else torch.empty
+        return fn((n_levels, n_shots, self.field), device=self.device, dtype=self.dtype)
+
+    def level_bytes(self, n_shots: int) -> int:
+        return n_shots * self.field * torch.finfo(self.dtype).bits // 8
+
+    def snapshot_bytes(self, n_shots: int, n_snap: int, kind: int) -> int:
+        return int(_lib.load().nw_snapshot_bytes(C.byref(self.g), n_shots, n_snap, kind))
+
+
+def plan_storage(plan: DevicePlan, n_shots: int, n_steps: int, grad_mode: str,
+                 checkpoint_every: int | None, snapshot: str, budget: int | None):
+    """Choose the wavefield storage of a gradient run: ``("history",)`` or ``("checkpoint", K)``.
+
+    ``grad_mode="autograd"`` keeps every level when it fits ``budget`` bytes and otherwise falls
+    back to checkpointing; ``"checkpoint"`` uses segments of ``checkpoint_every`` steps (default
+    ``ceil(sqrt(n_steps))``, the reference's choice) or the shortest segment whose pool fits the
+    budget.
+    """
+    lvl = plan.level_bytes(n_shots)
+    hist = (n_steps + 2) * lvl
+    if grad_mode == "autograd" and (budget is None or hist <= budget):
+        return ("history", None)
+    kind = _lib.SNAP_KINDS[snapshot]
+    if checkpoint_every:
+        return ("checkpoint", max(1, int(checkpoint_every)))
+    k = max(1, int(math.ceil(math.sqrt(max(1, n_steps)))))
+    if budget is not None:
+        def cost(k_):
+            return plan.snapshot_bytes(n_shots, -(-n_steps // k_), kind) + (k_ + 4) * lvl
+        best = min(range(1, n_steps + 1), key=cost) if n_steps < 20000 else k
+        if cost(k) > budget:
+            k = best
+        if cost(k) > budget:
+            raise ConfigError(
+                f"checkpointed gradient needs {cost(k) / 2**30:.1f} GiB, above the budget "
+                f"{budget / 2**30:.1f} GiB; lower source_batch or use fp16/bf16 snapshots")
+    return ("checkpoint", k)

@@ -1,0 +1,165 @@
+"""Generate golden vectors for the wave propagator by running the reference NEFI package itself.
+
+Run where the reference checkout is available (it is not needed anywhere else):
+
+    python tests/golden/make_golden.py [/path/to/reference]
+
+Every case stores its inputs, the operator arguments (JSON) and the reference's outputs in float64
+and float32: traces of ``op(fields)`` and the gradient of ``sum(traces * g)`` for a seeded
+cotangent ``g``, taken with ``torch.autograd`` through the reference's unrolled loop (grad_mode
+"autograd"). For the photoacoustic operator the gradient w.r.t. the (frozen) sound speed is taken
+through the reference's own internals, the same calls its ``simulate`` makes
+(nefi/physics/wave.py:840-867).
+"""
+
+from __future__ import annotations
+
+import json
+import math
+import sys
+from pathlib import Path
+
+import numpy as np
+import torch
+
+HERE = Path(__file__).resolve().parent
+REF = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+sys.path.insert(0, str(REF))
+
+from nefi.domain import Domain  # noqa: E402
+from nefi.physics.timestep import run_timestepping  # noqa: E402
+from nefi.physics.wave import WaveInitialConditionOperator, WaveOperator, laplacian  # noqa: E402
+
+F64, F32 = torch.float64, torch.float32
+
+
+def cotangent(shape, seed):
+    """Seeded trace cotangent g (regenerated by the tests from the stored seed)."""
+    return torch.randn(tuple(shape), generator=torch.Generator().manual_seed(seed), dtype=F64)
+
+
+def fwi_case(name, shape, extent, sources, receivers, c, kw, seed, rec_stride=1):
+    dom = Domain(shape, extent)
+    out = {"kind": "fwi", "shape": list(shape), "extent": [list(e) for e in extent],
+           "sources": np.asarray(sources, dtype=np.float64), "receivers": np.asarray(receivers, dtype=np.float64),
+           "c": c.numpy(), "kw": kw, "seed": seed, "rec_stride": rec_stride}
+    for dt, tag in ((F64, "f64"), (F32, "f32")):
+        op = WaveOperator(dom, sources, receivers, grad_mode="autograd", **kw)
+        x = c.to(dt).clone().requires_grad_(True)
+        tr = op({"c": x})
+        gtr = cotangent(tr.shape, seed)
+        (gc,) = torch.autograd.grad((tr * gtr.to(dt)).sum(), x)
+        out[f"traces_{tag}"] = tr.detach()[:, ::rec_stride].numpy()
+        out[f"grad_c_{tag}"] = gc.numpy()
+        out["meta"] = {"substeps": op.substeps, "n_steps": op.n_steps, "dt": op.dt,
+                       "padded": list(op.grid.padded_shape), "n_abs": list(op.grid.n_abs)}
+    save(name, out)
+
+
+def pat_case(name, shape, extent, receivers, p0, c, kw, seed):
+    dom = Domain(shape, extent)
+    out = {"kind": "pat", "shape": list(shape), "extent": [list(e) for e in extent],
+           "receivers": np.asarray(receivers, dtype=np.float64), "p0": p0.numpy(), "c": c.numpy(), "kw": kw,
+           "seed": seed, "rec_stride": 1}
+    for dt, tag in ((F64, "f64"), (F32, "f32")):
+        op = WaveInitialConditionOperator(dom, receivers, c=c, grad_mode="autograd", **kw)
+        x = p0.to(dt).clone().requires_grad_(True)
+        tr = op({"p0": x})
+        gtr = cotangent(tr.shape, seed)
+        (gp,) = torch.autograd.grad((tr * gtr.to(dt)).sum(), x)
+        out[f"traces_{tag}"] = tr.detach().numpy()
+        out[f"grad_p0_{tag}"] = gp.numpy()
+        # gradient w.r.t. the sound speed through the reference's own step function; like the
+        # operator (nefi/physics/wave.py:814-820) c2dt2 is formed in float64 and then cast
+        st = op._static(torch.device("cpu"), dt)
+        cl = c.clone().requires_grad_(True)
+        c2dt2 = (op.grid.pad(cl, "replicate") ** 2 * op.dt**2).to(dt)
+        p0p = op.grid.pad(p0.to(dt).reshape(-1, *shape), "zeros")
+        pm1 = p0p + 0.5 * c2dt2 * laplacian(p0p, op.grid.spacing, op.order, st["kernel"])
+        ridx, rw = st["rec_idx"], st["rec_w"]
+        d = len(shape)
+
+        def observe(s, n):
+            return (s[1].reshape(*s[1].shape[:-d], -1)[..., ridx] * rw).sum(-1)
+
+        _, obs = run_timestepping(op._step_fn(st, None), op._initial_state(pm1, p0p), (c2dt2,),
+                                  op.n_steps, op.dt, observe, record=op.record)
+        yc = torch.stack(obs, -1).reshape(tr.shape)
+        assert float((yc.detach() - tr.detach()).abs().max()) == 0.0
+        (gc,) = torch.autograd.grad((yc * gtr.to(dt)).sum(), cl)
+        out[f"grad_c_{tag}"] = gc.numpy()
+        out["meta"] = {"substeps": op.substeps, "n_steps": op.n_steps, "dt": op.dt,
+                       "padded": list(op.grid.padded_shape), "n_abs": list(op.grid.n_abs)}
+    save(name, out)
+
+
+def save(name, out):
+    arrays = {k: v for k, v in out.items() if isinstance(v, np.ndarray)}
+    meta = {k: v for k, v in out.items() if not isinstance(v, np.ndarray)}
+    for k, v in list(arrays.items()):
+        if v.dtype == np.float64 and k.endswith("_f32"):
+            arrays[k] = v.astype(np.float32)
+    np.savez_compressed(HERE / f"{name}.npz", meta=json.dumps(meta), **arrays)
+    print(name, {k: v.shape for k, v in arrays.items()}, meta.get("meta"))
+
+
+def main():
+    torch.manual_seed(0)
+    # small FWI cases, 2-D (the geometry of the reference's own adjoint checks)
+    c = (2.0 + 0.2 * torch.randn(20, 24, dtype=F64)).clamp(1.6, 2.4)
+    src = [[0.3, 0.2], [0.6, 0.5]]
+    rec = [[0.8, y] for y in (0.2, 0.5, 0.9)]
+    base = dict(n_t=30, dt_obs=0.012, f0=6.0, c_max=2.5)
+    ext = ((0.0, 1.0), (0.0, 1.2))
+    fwi_case("fwi_o4_sponge", (20, 24), ext, src, rec, c, {**base, "order": 4, "absorbing": "sponge",
+                                                             "absorb_width": 0.2}, 1)
+    fwi_case("fwi_o2_none", (20, 24), ext, src, rec, c, {**base, "order": 2, "absorbing": "none"}, 2)
+    fwi_case("fwi_o4_cerjan", (20, 24), ext, src, rec, c, {**base, "order": 4, "absorbing": "cerjan",
+                                                             "absorb_width": 0.2, "cerjan_gamma": 0.5}, 3)
+    c2 = (2.0 + 0.2 * torch.randn(18, 30, dtype=F64)).clamp(1.6, 2.4)
+    fwi_case("fwi_o2_sponge_aniso", (18, 30), ((0.0, 0.9), (0.0, 1.2)), [[0.45, 0.1]],
+             [[0.1 + 0.1 * i, 1.0] for i in range(7)], c2,
+             {**base, "n_t": 25, "order": 2, "absorbing": "sponge", "absorb_width": 0.16, "courant": 0.8}, 4)
+    # 128^2, h = 10 m, 2000 m/s + two +-300 m/s Gaussian anomalies (sigma 8 cells),
+    # 20-cell sponge, one 15 Hz Ricker at top centre, 128 receivers on row 2, 1000 steps at CFL 0.4.
+    n, h = 128, 10.0
+    rng = torch.Generator().manual_seed(0)
+    xs = (torch.arange(n, dtype=F64) + 0.5) * h
+    X, Z = torch.meshgrid(xs, xs, indexing="ij")
+    cc = torch.full((n, n), 2000.0, dtype=F64)
+    for s in (1.0, -1.0):
+        ctr = torch.rand(2, generator=rng, dtype=F64) * n * h * 0.5 + n * h * 0.25
+        cc = cc + s * 300.0 * torch.exp(-((X - ctr[0]) ** 2 + (Z - ctr[1]) ** 2) / (2 * (8 * h) ** 2))
+    cmax = float(cc.max())
+    dt = 0.4 * h / cmax
+    fwi_case("cfg1_128_o4_sponge", (n, n), ((0.0, n * h), (0.0, n * h)), [[n * h / 2, 1.5 * h]],
+             [[(i + 0.5) * h, 2.5 * h] for i in range(n)], cc,
+             dict(n_t=1001, dt_obs=dt, f0=15.0, c_max=cmax, order=4, absorbing="sponge",
+                  absorb_width=20 * h, courant=1.0), 5, rec_stride=4)
+    # photoacoustic, 2-D ring of receivers, known heterogeneous speed
+    torch.manual_seed(1)
+    n2 = 24
+    th = 2 * math.pi * torch.arange(32, dtype=F64) / 32
+    ring = torch.stack([0.85 * torch.cos(th), 0.85 * torch.sin(th)], 1)
+    p0 = torch.rand(2, n2, n2, dtype=F64)
+    cpat = 1.0 + 0.05 * torch.rand(n2, n2, dtype=F64)
+    pat_case("pat2d_o4_sponge", (n2, n2), ((-1.0, 1.0), (-1.0, 1.0)), ring, p0, cpat,
+             dict(n_t=50, dt_obs=0.03, order=4, absorbing="sponge", absorb_width=0.25), 6)
+    pat_case("pat2d_o2_cerjan", (n2, n2), ((-1.0, 1.0), (-1.0, 1.0)), ring, p0[0], cpat,
+             dict(n_t=40, dt_obs=0.03, order=2, absorbing="cerjan", absorb_width=0.25), 7)
+    # photoacoustic, 3-D slab with a planar sensor array on the top face
+    xs3 = (torch.arange(4, dtype=F64) + 0.5) * 0.75
+    Xs, Ys = torch.meshgrid(xs3, xs3, indexing="ij")
+    sens = torch.stack([Xs.ravel(), Ys.ravel(), torch.zeros(16, dtype=F64)], -1)
+    p03 = torch.rand(12, 12, 8, dtype=F64)
+    c3 = 1.5 * (1.0 + 0.05 * torch.rand(12, 12, 8, dtype=F64))
+    pat_case("pat3d_o2_sponge", (12, 12, 8), ((0.0, 3.0), (0.0, 3.0), (0.0, 2.0)), sens, p03, c3,
+             dict(n_t=30, dt_obs=0.1, order=2, absorbing="sponge", absorb_width=0.75), 8)
+    sens_in = sens * 0.8
+    sens_in[:, 2] = 0.125  # first cell centre: without a layer the sensors must sit inside the grid
+    pat_case("pat3d_o4_none", (10, 9, 8), ((0.0, 2.5), (0.0, 2.25), (0.0, 2.0)), sens_in, p03[:10, :9],
+             c3[:10, :9], dict(n_t=20, dt_obs=0.08, order=4, absorbing="none"), 9)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,100 @@
+"""The C-ABI library loads, exports every function include/nefi_wave.h declares, and its host-only
+entry points (layout, sizes, errors) behave; no CUDA device is needed."""
+
+from __future__ import annotations
+
+import ctypes as C
+import re
+from pathlib import Path
+
+import pytest
+
+from nefi_b200 import _lib
+from nefi_b200.build import build
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "nefi_wave.h"
+
+
+def declared_functions(header: Path = HEADER) -> list[str]:
+    text = re.sub(r"/\*.*?\*/", "", header.read_text(), flags=re.S)
+    return sorted(set(re.findall(r"\b(nw_[a-z0-9_]+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    build()
+    return _lib.load()
+
+
+def test_every_declared_symbol_is_exported_and_bound(lib):
+    names = declared_functions()
+    assert len(names) >= 12
+    for n in names:
+        assert hasattr(lib, n), n
+    assert sorted(_lib.EXPORTED) == names
+
+
+def test_abi_version_and_arch(lib):
+    assert lib.nw_abi_version() == 1
+    assert lib.nw_built_arch() == 1000
+
+
+@pytest.mark.parametrize("ndim,order", [(2, 2), (2, 4), (3, 2), (3, 4)])
+def test_ghost_layout_keeps_every_stencil_read_in_bounds(lib, ndim, order):
+    g = _lib.Grid()
+    g.ndim, g.order, g.dtype = ndim, order, _lib.NW_F32
+    n = (13, 7, 37)[:ndim]
+    for ax in range(3):
+        g.n[ax] = n[ax] if ax < ndim else 1
+    _lib.check(lib.nw_grid_layout(C.byref(g)))
+    r = order // 2
+    assert g.radius == r
+    ld = g.stride[ndim - 2]  # row pitch of the contiguous axis
+    assert ld % 32 == 0 and ld >= n[-1] + r
+    # the lowest and highest neighbour reads (one axis at a time) stay inside [0, field_elems)
+    reach = max(r * g.stride[ax] for ax in range(ndim))
+    last = [k - 1 for k in n]
+    hi_cell = g.origin + sum(last[ax] * g.stride[ax] for ax in range(ndim))
+    assert g.origin - reach >= 0 and hi_cell + reach < g.field_elems
+    # a neighbour outside the grid along one axis never aliases an interior cell
+    interior = set()
+    import itertools
+
+    for idx in itertools.product(*[range(k) for k in n]):
+        interior.add(g.origin + sum(i * g.stride[ax] for ax, i in enumerate(idx)))
+    for idx in itertools.product(*[range(k) for k in n]):
+        base = g.origin + sum(i * g.stride[ax] for ax, i in enumerate(idx))
+        for ax in range(ndim):
+            for o in range(1, r + 1):
+                for sgn in (-1, 1):
+                    j = idx[ax] + sgn * o
+                    if not 0 <= j < n[ax]:
+                        assert base + sgn * o * g.stride[ax] not in interior
+
+
+def test_invalid_arguments_report_errors(lib):
+    g = _lib.Grid()
+    g.ndim, g.order = 1, 2
+    rc = lib.nw_grid_layout(C.byref(g))
+    assert rc == _lib.NW_ERR_UNSUPPORTED
+    assert b"ndim" in lib.nw_last_error()
+    g.ndim, g.order = 2, 6
+    assert lib.nw_grid_layout(C.byref(g)) == _lib.NW_ERR_ARG
+    with pytest.raises(_lib.LibraryError, match="order"):
+        _lib.check(lib.nw_grid_layout(C.byref(g)))
+
+
+def test_snapshot_pool_sizes(lib):
+    g = _lib.Grid()
+    g.ndim, g.order, g.dtype = 2, 4, _lib.NW_F32
+    g.n[0], g.n[1], g.n[2] = 552, 552, 1
+    _lib.check(lib.nw_grid_layout(C.byref(g)))
+    exact = lib.nw_snapshot_bytes(C.byref(g), 16, 10, _lib.NW_SNAP_EXACT)
+    half = lib.nw_snapshot_bytes(C.byref(g), 16, 10, _lib.NW_SNAP_F16)
+    assert exact == 10 * 2 * 16 * g.field_elems * 4
+    assert 0.49 * exact < half < 0.53 * exact
+
+
+def test_missing_library_fails_loudly(tmp_path):
+    with pytest.raises(_lib.LibraryError, match="missing"):
+        _lib.load(tmp_path / "libnefiwave.so")

@@ -1,0 +1,252 @@
+"""GPU parity of the CUDA propagator (through the C ABI) against the reference's golden vectors
+and the CPU oracle.
+
+Tolerances (relative L2):
+  float64 device run vs reference float64: traces 1e-11, gradients 1e-10 (rounding only);
+  float32 device run vs reference float32: traces 1e-5, gradients 1e-4 (the stated FP32 bar);
+  float32 device run vs the float64 oracle: traces 1e-5, gradients 1e-4.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import cotangent, full_trace_shape, golden_names, load_golden, oracle_for, rel_l2
+from nefi_b200 import WaveInitialConditionOperatorB200, WaveOperatorB200
+from nefi_b200._compat import Domain, OperatorError, SolverError
+
+pytestmark = pytest.mark.gpu
+
+FWI = golden_names("fwi")
+PAT = golden_names("pat")
+
+
+def make_op(case, **over):
+    dom = Domain(tuple(case["shape"]), tuple(tuple(e) for e in case["extent"]))
+    kw = {**case["kw"], "grad_mode": "autograd", **over}
+    if case["kind"] == "fwi":
+        return WaveOperatorB200(dom, case["sources"], case["receivers"], **kw)
+    return WaveInitialConditionOperatorB200(dom, case["receivers"], c=torch.tensor(case["c"]), **kw)
+
+
+def run_fwi(case, dtype, dev, **over):
+    op = make_op(case, **over)
+    c = torch.tensor(case["c"], dtype=dtype, device=dev, requires_grad=True)
+    tr = op({"c": c})
+    g = torch.tensor(cotangent(tr.shape, case["seed"]), dtype=dtype, device=dev)
+    (gc,) = torch.autograd.grad((tr * g).sum(), c)
+    return tr.detach()[:, :: case["rec_stride"]].cpu().numpy(), gc.cpu().numpy()
+
+
+def run_pat(case, dtype, dev, with_c=False, **over):
+    op = make_op(case, **over)
+    p0 = torch.tensor(case["p0"], dtype=dtype, device=dev, requires_grad=True)
+    if with_c:
+        c = torch.tensor(case["c"], dtype=dtype, device=dev, requires_grad=True)
+        tr = op.with_speed(p0, c)
+    else:
+        tr = op({"p0": p0})
+    g = torch.tensor(cotangent(tr.shape, case["seed"]), dtype=dtype, device=dev)
+    if with_c:
+        gp, gc = torch.autograd.grad((tr * g).sum(), (p0, c))
+        return tr.detach().cpu().numpy(), gp.cpu().numpy(), gc.cpu().numpy()
+    (gp,) = torch.autograd.grad((tr * g).sum(), p0)
+    return tr.detach().cpu().numpy(), gp.cpu().numpy(), None
+
+
+@pytest.mark.parametrize("name", FWI)
+def test_fwi_float64_matches_reference(name, cuda_device):
+    case = load_golden(name)
+    tr, gc = run_fwi(case, torch.float64, cuda_device)
+    assert rel_l2(tr, case["traces_f64"]) < 1e-11
+    assert rel_l2(gc, case["grad_c_f64"]) < 1e-10
+
+
+@pytest.mark.parametrize("name", FWI)
+def test_fwi_float32_matches_reference_float32(name, cuda_device):
+    case = load_golden(name)
+    tr, gc = run_fwi(case, torch.float32, cuda_device)
+    assert rel_l2(tr, case["traces_f32"]) < 1e-5
+    assert rel_l2(gc, case["grad_c_f32"]) < 1e-4
+    # and against the float64 oracle
+    assert rel_l2(tr, case["traces_f64"]) < 1e-5
+    assert rel_l2(gc, case["grad_c_f64"]) < 1e-4
+
+
+@pytest.mark.parametrize("name", PAT)
+def test_pat_float64_matches_reference(name, cuda_device):
+    case = load_golden(name)
+    tr, gp, _ = run_pat(case, torch.float64, cuda_device)
+    assert rel_l2(tr, case["traces_f64"]) < 1e-11
+    assert rel_l2(gp, case["grad_p0_f64"]) < 1e-10
+    tr2, gp2, gc = run_pat(case, torch.float64, cuda_device, with_c=True)
+    assert rel_l2(tr2, case["traces_f64"]) < 1e-11
+    assert rel_l2(gp2, case["grad_p0_f64"]) < 1e-10
+    assert rel_l2(gc, case["grad_c_f64"]) < 1e-10
+
+
+@pytest.mark.parametrize("name", PAT)
+def test_pat_float32_matches_reference_float32(name, cuda_device):
+    case = load_golden(name)
+    tr, gp, _ = run_pat(case, torch.float32, cuda_device)
+    assert rel_l2(tr, case["traces_f32"]) < 1e-5
+    assert rel_l2(gp, case["grad_p0_f32"]) < 1e-4
+    _, _, gc = run_pat(case, torch.float32, cuda_device, with_c=True)
+    assert rel_l2(gc, case["grad_c_f32"]) < 1e-4
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+@pytest.mark.parametrize("name", ["fwi_o4_sponge", "fwi_o4_cerjan", "pat3d_o2_sponge"])
+def test_checkpointed_gradient_is_identical_to_full_history(name, dtype, cuda_device):
+    case = load_golden(name)
+    if case["kind"] == "fwi":
+        ref = run_fwi(case, dtype, cuda_device)
+        for k in (5, None):
+            got = run_fwi(case, dtype, cuda_device, grad_mode="checkpoint", checkpoint_every=k)
+            assert np.array_equal(got[0], ref[0]) and np.array_equal(got[1], ref[1])
+    else:
+        ref = run_pat(case, dtype, cuda_device)
+        got = run_pat(case, dtype, cuda_device, grad_mode="checkpoint", checkpoint_every=7)
+        assert np.array_equal(got[0], ref[0]) and np.array_equal(got[1], ref[1])
+
+
+@pytest.mark.parametrize("snapshot,tol", [("fp16", 2e-3), ("bf16", 2e-2)])
+def test_reduced_precision_snapshots_error_is_bounded(snapshot, tol, cuda_device):
+    case = load_golden("cfg1_128_o4_sponge")
+    tr, gc = run_fwi(case, torch.float32, cuda_device, grad_mode="checkpoint", checkpoint_every=40,
+                     snapshot=snapshot)
+    assert rel_l2(tr, case["traces_f64"]) < 1e-5  # the forward never reads a snapshot
+    assert rel_l2(gc, case["grad_c_f64"]) < tol
+
+
+def test_runs_are_bitwise_deterministic(cuda_device):
+    case = load_golden("fwi_o4_sponge")
+    a = run_fwi(case, torch.float32, cuda_device)
+    b = run_fwi(case, torch.float32, cuda_device)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def test_central_finite_differences_float64(cuda_device):
+    """The reference's own check (tests/test_physics_wave.py:145-165), on the device."""
+    torch.manual_seed(0)
+    dom = Domain((16, 16), ((0.0, 1.0), (0.0, 1.0)))
+    c = (2.0 + 0.2 * torch.randn(16, 16, dtype=torch.float64)).clamp(1.6, 2.4).to(cuda_device)
+    kw = dict(n_t=40, dt_obs=0.01, f0=5.0, c_max=2.5, absorb_width=0.2, absorbing="sponge")
+    src, rec = [[0.2, 0.3], [0.2, 0.7]], [[0.8, y] for y in (0.2, 0.4, 0.6, 0.8)]
+    w = torch.randn(2, 4, 40, dtype=torch.float64).to(cuda_device)
+    grads = []
+    for mode, ck in (("autograd", None), ("checkpoint", 5), ("checkpoint", None)):
+        op = WaveOperatorB200(dom, src, rec, grad_mode=mode, checkpoint_every=ck, **kw)
+        x = c.clone().requires_grad_(True)
+        (g,) = torch.autograd.grad((op({"c": x}) * w).sum(), x)
+        grads.append(g)
+    for g in grads[1:]:
+        assert float((g - grads[0]).norm() / grads[0].norm()) < 1e-6
+    op = WaveOperatorB200(dom, src, rec, grad_mode="autograd", **kw)
+    for seed in range(4):
+        e = torch.randn(16, 16, dtype=torch.float64, generator=torch.Generator().manual_seed(seed)).to(cuda_device)
+        eps = 1e-6
+        fd = float((op({"c": c + eps * e}) * w).sum()) - float((op({"c": c - eps * e}) * w).sum())
+        fd /= 2 * eps
+        assert abs(fd - float((grads[0] * e).sum())) < 1e-6 * max(1.0, abs(fd))
+
+
+def test_pat_adjoint_identity_and_linearity_float64(cuda_device):
+    """<A a, y> = <a, A^T y> (tests/test_photoacoustic3d.py:49-59), on the device."""
+    case = load_golden("pat3d_o2_sponge")
+    op = make_op(case)
+    dev, F = cuda_device, torch.float64
+    g = torch.Generator().manual_seed(0)
+    a = torch.rand(12, 12, 8, dtype=F, generator=g).to(dev)
+    b = torch.rand(12, 12, 8, dtype=F, generator=g).to(dev)
+    ya, yb = op({"p0": a}), op({"p0": b})
+    assert torch.allclose(op({"p0": 2 * a - 0.5 * b}), 2 * ya - 0.5 * yb, atol=1e-10)
+    y = torch.randn(ya.shape, dtype=F, generator=g).to(dev)
+    x = torch.zeros(12, 12, 8, dtype=F, device=dev, requires_grad=True)
+    (adj,) = torch.autograd.grad((op({"p0": x}) * y).sum(), x)
+    assert float((ya * y).sum()) == pytest.approx(float((a * adj).sum()), rel=1e-9)
+
+
+def test_source_batching_and_speed_check(cuda_device):
+    """tests/test_physics_wave.py:168-189 on the device."""
+    dom = Domain((32, 32), ((0.0, 1.0), (0.0, 1.0)))
+    src = [[0.1, 0.3], [0.1, 0.5], [0.1, 0.7]]
+    rec = [[0.9, y] for y in torch.linspace(0.1, 0.9, 6).tolist()]
+    kw = dict(n_t=60, dt_obs=0.016, f0=3.0, c_max=2.5, absorb_width=0.25, absorbing="sponge")
+    op = WaveOperatorB200(dom, src, rec, **kw)
+    x = dom.physical_coords(dtype=torch.float64)
+    c = (2.0 + 0.2 * torch.exp(-((x - 0.5) ** 2).sum(-1) / 0.02)).to(cuda_device)
+    y = op({"c": c})
+    assert y.shape == (3, 6, 60)
+    batched = WaveOperatorB200(dom, src, rec, source_batch=2, **kw)
+    assert torch.allclose(batched({"c": c}), y, atol=1e-12)
+    with pytest.raises(OperatorError, match="exceeds"):
+        op({"c": torch.full((32, 32), 3.0, dtype=torch.float64, device=cuda_device)})
+
+
+def test_energy_is_conserved_without_absorption(cuda_device):
+    """tests/test_physics_wave.py:100-118 through the per-step observe path."""
+    dom = Domain((40, 40), ((0.0, 1.0), (0.0, 1.0)))
+    c = torch.full((40, 40), 1.0, dtype=torch.float64)
+    c[20:, :] = 1.5
+    c = c.to(cuda_device)
+    op = WaveOperatorB200(dom, [[0.5, 0.5]], [[0.2, 0.2]], n_t=150, dt_obs=0.01, f0=8.0, c_max=1.5,
+                          order=4, grad_mode="autograd", absorbing="none")
+    rec = list(range(80, 1 + 149 * 2, 20))
+    from nefi_b200.geometry import stencil_weights
+
+    wc, w1, w2 = stencil_weights(op.grid.spacing, 4)
+
+    def lap(p):  # order-4 Laplacian, zero outside the grid
+        out = wc * p
+        for ax in (0, 1):
+            for o, w in ((1, w1[ax]), (2, w2[ax])):
+                out = out + w * (_shift(p, o, -2 + ax) + _shift(p, -o, -2 + ax))
+        return out
+
+    def energy(state, n):
+        pp, p = state
+        kin = (p - pp) ** 2 / (c**2 * op.dt**2)
+        return 0.5 * (kin - p * lap(pp)).sum()
+
+    _, e = op.simulate(c, observe=energy, record=rec)
+    e = torch.stack(e)
+    assert float((e.max() - e.min()) / e.mean()) < 1e-9
+
+
+def _shift(p, o, dim):
+    out = torch.zeros_like(p)
+    n = p.shape[dim]
+    if o > 0:
+        out.narrow(dim, o, n - o).copy_(p.narrow(dim, 0, n - o))
+    else:
+        out.narrow(dim, 0, n + o).copy_(p.narrow(dim, -o, n + o))
+    return out
+
+
+def test_corrupted_snapshot_raises(cuda_device):
+    """Host-side fault injection: a NaN written into the snapshot pool between the forward and the
+    backward sweep must surface as SolverError, not as a silent gradient."""
+    case = load_golden("fwi_o4_sponge")
+    op = make_op(case, grad_mode="checkpoint", checkpoint_every=10, snapshot="fp16")
+    c = torch.tensor(case["c"], dtype=torch.float32, device=cuda_device, requires_grad=True)
+    tr = op({"c": c})
+    ctx_run = tr.grad_fn.run  # the _Run object saved on the autograd context
+    ctx_run.snap.view(torch.float32).fill_(float("nan"))  # poison every block and scale
+    with pytest.raises(SolverError, match="non-finite"):
+        tr.sum().backward()
+    # the context stays usable afterwards
+    tr2 = op({"c": c.detach()})
+    assert torch.isfinite(tr2).all()
+
+
+def test_oracle_agrees_with_device_float32_on_cfg1(cuda_device):
+    case = load_golden("cfg1_128_o4_sponge")
+    tr, gc = run_fwi(case, torch.float32, cuda_device)
+    orc = oracle_for(case)
+    g = cotangent(full_trace_shape(case), case["seed"])
+    otr, ogc = orc.fwi(case["c"], g, dtype=np.float64)
+    assert rel_l2(tr, otr[:, :: case["rec_stride"]]) < 1e-5
+    assert rel_l2(gc, ogc) < 1e-4

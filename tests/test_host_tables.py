@@ -1,0 +1,139 @@
+"""Host-side logic on the CPU: the operators' geometry and the device tables they build reproduce the
+reference's results when the kernels' semantics are replayed in numpy (tests/kernel_model.py)."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import cotangent, full_trace_shape, golden_names, load_golden, rel_l2
+from kernel_model import GhostModel
+from nefi_b200 import WaveInitialConditionOperatorB200, WaveOperatorB200
+from nefi_b200._compat import ConfigError, Domain, OperatorError, ShapeError
+
+SMALL_FWI = [n for n in golden_names("fwi") if not n.startswith("cfg1")]
+PAT = golden_names("pat")
+CPU = torch.device("cpu")
+
+
+def make_op(case):
+    dom = Domain(tuple(case["shape"]), tuple(tuple(e) for e in case["extent"]))
+    if case["kind"] == "fwi":
+        return WaveOperatorB200(dom, case["sources"], case["receivers"], grad_mode="autograd", **case["kw"])
+    return WaveInitialConditionOperatorB200(dom, case["receivers"], c=torch.tensor(case["c"]),
+                                            grad_mode="autograd", **case["kw"])
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_time_axis_and_padding_match_reference(name):
+    case = load_golden(name)
+    op = make_op(case)
+    meta = case["meta"]
+    assert op.substeps == meta["substeps"] and op.n_steps == meta["n_steps"]
+    assert op.dt == pytest.approx(meta["dt"], rel=1e-15)
+    assert list(op.grid.padded_shape) == meta["padded"] and list(op.grid.n_abs) == meta["n_abs"]
+
+
+@pytest.mark.parametrize("name", SMALL_FWI)
+def test_fwi_tables_reproduce_reference(name):
+    case = load_golden(name)
+    op = make_op(case)
+    model = GhostModel(op._plan(CPU, torch.float64))
+    C = model.medium(case["c"], op.dt**2)
+    g = cotangent(full_trace_shape(case), case["seed"])
+    tr, gC, _, _ = model.run(C, op.n_steps, op.substeps, op.n_t, list(range(op.n_sources)), grad_traces=g)
+    assert rel_l2(tr, case["traces_f64"]) < 1e-12
+    assert rel_l2(model.fold_grad(case["c"], op.dt**2, gC), case["grad_c_f64"]) < 1e-11
+
+
+@pytest.mark.parametrize("name", PAT)
+def test_pat_tables_reproduce_reference(name):
+    case = load_golden(name)
+    op = make_op(case)
+    plan = op._plan(CPU, torch.float64)
+    model = GhostModel(plan)
+    d = len(case["shape"])
+    p0 = case["p0"].reshape(-1, *case["shape"])
+    S = p0.shape[0]
+    C = np.zeros(model.F)
+    c2 = op.grid.pad(torch.tensor(case["c"]), "replicate").numpy() ** 2 * op.dt**2
+    C[model.I] = c2.reshape(-1)
+    cur = np.zeros((S, model.F))
+    padded = np.pad(p0, [(0, 0)] + [(a, a) for a in op.grid.n_abs])
+    cur[:, model.I] = padded.reshape(S, -1)
+    prev = np.zeros((S, model.F))
+    for s in range(S):
+        prev[s, model.I] = cur[s, model.I] + (0.5 * C[model.I]) * model.lap(cur[s])
+    g = cotangent(full_trace_shape(case), case["seed"]).reshape(S, plan.n_rec, op.n_t)
+    tr, gC, lam0, mu1 = model.run(C, op.n_steps, op.substeps, op.n_t, list(range(S)), init=(prev, cur),
+                                  grad_traces=g)
+    assert rel_l2(tr.reshape(case["traces_f64"].shape), case["traces_f64"]) < 1e-12
+    b0 = 1.0 if (model.B is None or plan.first_b_one) else model.B
+    gp = np.zeros((S, *case["shape"]))
+    for s in range(S):
+        lm1 = -(b0 * mu1[s])
+        full = (lam0[s] + lm1)[model.I] + model.lap(0.5 * C * lm1)
+        dense = full.reshape(model.P)
+        sl = tuple(slice(a, a + n) for a, n in zip(op.grid.n_abs, case["shape"]))
+        gp[s] = dense[sl]
+        gC[s, model.I] += (0.5 * lm1[model.I]) * model.lap(cur[s])
+    assert rel_l2(gp.reshape(case["grad_p0_f64"].shape), case["grad_p0_f64"]) < 1e-11
+    gc = model.fold_grad(case["c"], op.dt**2, gC)
+    assert rel_l2(gc, case["grad_c_f64"]) < 1e-11
+    assert d in (2, 3)
+
+
+def test_adjoint_table_is_cell_major_and_complete():
+    case = load_golden("fwi_o4_sponge")
+    plan = make_op(case)._plan(CPU, torch.float64)
+    cells = plan.cell_index.numpy()
+    assert np.all(np.diff(cells) > 0)
+    ptr = plan.cell_ptr.numpy()
+    assert ptr[0] == 0 and ptr[-1] == plan.rec_index.numel()
+    # every (receiver, corner) pair appears exactly once
+    pairs = sorted(zip(plan.cell_rec.numpy().tolist(), plan.cell_weight.numpy().tolist()))
+    ref = sorted((r, w) for r in range(plan.n_rec) for w in plan.rec_weight[r].tolist())
+    assert pairs == ref
+
+
+def test_reference_errors_are_raised_on_the_host():
+    dom = Domain((16, 16), ((0.0, 1.0), (0.0, 1.0)))
+    kw = dict(n_t=10, dt_obs=0.01, f0=5.0, c_max=2.5, absorbing="sponge")
+    with pytest.raises(ConfigError):
+        WaveOperatorB200(dom, [[0.5, 0.5]], [[0.5, 0.5]], **{**kw, "absorbing": "bogus"})
+    with pytest.raises(ConfigError):
+        WaveOperatorB200(dom, [[0.5, 0.5]], [[0.5, 0.5]], **{**kw, "order": 6})
+    with pytest.raises(ConfigError):
+        WaveOperatorB200(dom, [[0.5, 0.5]], [[0.5, 0.5]], **kw, grad_mode="other")
+    with pytest.raises(ConfigError):  # outside the padded grid
+        WaveOperatorB200(dom, [[5.0, 0.5]], [[0.5, 0.5]], **kw)
+    op = WaveOperatorB200(dom, [[0.5, 0.5]], [[0.5, 0.5]], **kw)
+    with pytest.raises(ShapeError):
+        op({"c": torch.ones(8, 8, dtype=torch.float64)})
+    with pytest.raises(ConfigError, match="CUDA"):  # no CPU path
+        op({"c": torch.full((16, 16), 2.0, dtype=torch.float64)})
+    with pytest.raises(OperatorError):
+        op._check_speed(torch.full((16, 16), 3.0))
+    with pytest.raises(ConfigError):
+        WaveInitialConditionOperatorB200(Domain((4, 4, 4), ((0, 1),) * 3), [[0.5, 0.5, 0.5]], n_t=3,
+                                         dt_obs=0.1, absorbing="pml")
+
+
+def test_attributes_mirror_reference_operator():
+    dom = Domain((32, 32), ((0.0, 1.0), (0.0, 1.0)))
+    src = [[0.1, 0.3], [0.1, 0.5], [0.1, 0.7]]
+    rec = [[0.9, y] for y in torch.linspace(0.1, 0.9, 6).tolist()]
+    op = WaveOperatorB200(dom, src, rec, n_t=60, dt_obs=0.016, f0=3.0, c_max=2.5, absorb_width=0.25,
+                          absorbing="sponge")
+    assert op.output_shape((32, 32)) == (3, 6, 60)
+    assert op.fidelity_tag == "wave-leapfrog-o4-sponge" and op.homogeneity is None
+    assert op.traceable is False and op.batchable is False and op.primary == "c"
+    coarse = op.at_resolution((16, 16))
+    assert coarse is op.at_resolution((16, 16)) and coarse.grid.shape == (16, 16)
+    assert coarse.fidelity_tag == op.fidelity_tag
+    assert op.record == [j * op.substeps for j in range(60)]
+    assert op.times.shape == (60,) and op.wavelet().shape == (op.n_steps,)
+    pat = WaveInitialConditionOperatorB200(dom, rec, n_t=20, dt_obs=0.01, absorbing="sponge")
+    assert pat.homogeneity == 1.0 and pat.fidelity_tag == "wave-leapfrog-ic-o4-sponge"
+    assert pat.output_shape((32, 32)) == (6, 20)

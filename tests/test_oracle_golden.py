@@ -1,0 +1,70 @@
+"""Pin the CPU oracle to the reference: its float64 results must reproduce the golden vectors the
+reference produced (tests/golden/make_golden.py) to rounding, and its float32 results must stay
+within single-precision distance of the reference's float32 results."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import cotangent, full_trace_shape, golden_names, load_golden, oracle_for, rel_l2
+
+FWI = golden_names("fwi")
+PAT = golden_names("pat")
+
+
+def _fwi(case, dtype):
+    orc = oracle_for(case)
+    g = cotangent(full_trace_shape(case), case["seed"])
+    tr, gc = orc.fwi(case["c"], g, dtype=dtype)
+    return tr[:, :: case["rec_stride"]], gc
+
+
+def _pat(case, dtype):
+    orc = oracle_for(case)
+    g = cotangent(full_trace_shape(case), case["seed"])
+    return orc.pat(case["p0"], case["c"], g, dtype=dtype)
+
+
+@pytest.mark.parametrize("name", FWI)
+def test_oracle_fwi_float64_matches_reference(name):
+    case = load_golden(name)
+    tr, gc = _fwi(case, np.float64)
+    assert rel_l2(tr, case["traces_f64"]) < 1e-12
+    assert rel_l2(gc, case["grad_c_f64"]) < 1e-11
+
+
+@pytest.mark.parametrize("name", PAT)
+def test_oracle_pat_float64_matches_reference(name):
+    case = load_golden(name)
+    tr, gp, gc = _pat(case, np.float64)
+    assert rel_l2(tr, case["traces_f64"]) < 1e-12
+    assert rel_l2(gp, case["grad_p0_f64"]) < 1e-11
+    assert rel_l2(gc, case["grad_c_f64"]) < 1e-11
+
+
+@pytest.mark.parametrize("name", FWI)
+def test_oracle_fwi_float32_close_to_reference_float32(name):
+    case = load_golden(name)
+    tr, gc = _fwi(case, np.float32)
+    assert rel_l2(tr, case["traces_f32"]) < 1e-5
+    assert rel_l2(gc, case["grad_c_f32"]) < 1e-4
+
+
+@pytest.mark.parametrize("name", PAT)
+def test_oracle_pat_float32_close_to_reference_float32(name):
+    case = load_golden(name)
+    tr, gp, gc = _pat(case, np.float32)
+    assert rel_l2(tr, case["traces_f32"]) < 1e-5
+    assert rel_l2(gp, case["grad_p0_f32"]) < 1e-4
+    assert rel_l2(gc, case["grad_c_f32"]) < 1e-4
+
+
+def test_oracle_detects_a_planted_error():
+    """A perturbed oracle (sponge damping 5 % too strong) must fail the float64 pin."""
+    case = load_golden("fwi_o4_sponge")
+    orc = oracle_for(case)
+    orc.B = 1.0 - (1.0 - orc.B) * 1.05
+    g = cotangent(full_trace_shape(case), case["seed"])
+    tr, gc = orc.fwi(case["c"], g)
+    assert rel_l2(gc, case["grad_c_f64"]) > 1e-9
