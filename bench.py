@@ -119,13 +119,24 @@ def cpu_sample(w, n_shots=CPU_SAMPLE_SHOTS, n_steps=CPU_SAMPLE_STEPS) -> tuple[f
     return 1.0 / per_shot_full, info
 
 
+def make_workload(args):
+    from nefi_b200 import workloads
+
+    kw = {}
+    if getattr(args, "n_steps", None):
+        kw["n_steps"] = args.n_steps
+    if getattr(args, "shots", None):
+        kw["n_shots"] = args.shots
+    return workloads.WORKLOADS[args.workload](**kw)
+
+
 def run_reference(args) -> None:
     from nefi_b200 import workloads
 
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    w = workloads.WORKLOADS[args.workload]()
+    w = make_workload(args)
     vals, info = [], {}
     for i in range(args.warmup + args.steps):
         v, info = cpu_sample(w)
@@ -155,6 +166,8 @@ def main() -> None:
     ap.add_argument("--workload", default="fwi_512")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--n-steps", type=int, default=None, help="override the leapfrog steps (profiling cases)")
+    ap.add_argument("--shots", type=int, default=None, help="override the shots per GPU (profiling cases)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -172,7 +185,7 @@ def main() -> None:
     if world > 1:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
 
-    w = workloads.WORKLOADS[args.workload]()
+    w = make_workload(args)
     op = WaveOperatorB200(w.domain, w.sources, w.receivers, grad_mode="autograd", **w.operator_kwargs())
     c = torch.tensor(w.c, dtype=torch.float32, device=dev)
     # observed data: traces of a smoothed model (the misfit of a typical early FWI iteration)

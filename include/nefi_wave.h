@@ -31,14 +31,14 @@
 extern "C" {
 #endif
 
-#define NW_ABI_VERSION 1
+#define NW_ABI_VERSION 2
 
 /* scalar type of a computation */
 enum { NW_F32 = 0, NW_F64 = 1 };
 /* absorbing layer kind (nefi/physics/wave.py:80, 469-501) */
 enum { NW_ABS_NONE = 0, NW_ABS_SPONGE = 1, NW_ABS_CERJAN = 2 };
 /* snapshot encodings for checkpointed gradients */
-enum { NW_SNAP_EXACT = 0, NW_SNAP_F16 = 1, NW_SNAP_BF16 = 2 };
+enum { NW_SNAP_EXACT = 0, NW_SNAP_F16 = 1, NW_SNAP_BF16 = 2, NW_SNAP_I16 = 3 };
 /* status codes */
 enum {
   NW_OK = 0,
@@ -67,14 +67,34 @@ typedef struct nw_grid {
   double w2[3];
   /* --- filled by nw_grid_layout --- */
   int32_t radius;      /* stencil radius: order / 2 */
-  int32_t reserved;
+  int32_t guard;       /* zero elements before the first storage row (keeps 16-byte tile copies
+                          that start left of column 0 inside the buffer) */
   int64_t stride[3];   /* element strides per axis in the ghost layout */
   int64_t origin;      /* element offset of cell (0,..,0) */
-  int64_t field_elems; /* elements per field buffer, ghosts included */
+  int64_t field_elems; /* elements per field buffer, ghosts included (a multiple of 32) */
 } nw_grid;
 
-/* Fills radius/stride/origin/field_elems of `g`. Host only, no CUDA call. */
+/* Fills radius/guard/stride/origin/field_elems of `g`. Host only, no CUDA call. */
 int nw_grid_layout(nw_grid* g);
+
+/*
+ * Launch shape of the 2-D tiled kernels. A CTA owns a tile of 8*rx rows by 32*vz columns and
+ * loops over shots_per_cta shots. Zero fields take the library's defaults. 3-D grids ignore it.
+ */
+typedef struct nw_tuning {
+  int32_t vz;                /* columns per thread: 2 or 4 (float32), 2 (float64) */
+  int32_t rx;                /* rows per thread: 2, 4 or 8 */
+  int32_t shots_per_cta;     /* forward steps: shots per CTA, >= 1 */
+  int32_t adj_shots_per_cta; /* adjoint steps: shots per CTA, >= 1 (one float64 gradient
+                                accumulator per group of this many shots) */
+  int32_t reserved[4];
+} nw_tuning;
+
+/* Resolves the defaults of `t` for grid `g` in place and reports the tile (tx rows, tz columns). */
+int nw_tile_shape(const nw_grid* g, nw_tuning* t, int32_t* tx, int32_t* tz);
+
+/* Number of float64 gradient accumulator fields nw_adjoint fills for n_shots shots. */
+int nw_adjoint_groups(const nw_grid* g, const nw_tuning* t, int32_t n_shots);
 
 /*
  * Point stencils of one acquisition. Sources: one multilinear stencil per shot, injected as
@@ -83,6 +103,7 @@ int nw_grid_layout(nw_grid* g);
  * every record step (nefi/physics/wave.py:272-300, 321-324, 723-729).
  * The adjoint of the receiver sampling is given as a cell-major table (CSR over the cells the
  * receivers touch) so that the adjoint injection sums each cell in a fixed order.
+ * For 2-D grids the per-tile tables index the same data by the tile shape nw_tile_shape reports.
  */
 typedef struct nw_acquisition {
   int32_t n_shots;
@@ -98,6 +119,15 @@ typedef struct nw_acquisition {
   const int32_t* cell_ptr;     /* (n_cells + 1,) CSR row pointers into cell_rec/cell_weight */
   const int32_t* cell_rec;     /* receiver id per entry */
   const void* cell_weight;     /* dtype weight per entry */
+  /* 2-D per-tile tables (tiles in row-major order, tiles_z along the contiguous axis) */
+  int32_t tiles_z;
+  int32_t tile_rows, tile_cols;    /* tile shape the tables were built for */
+  const int32_t* rec_corner;       /* (n_rec, 2) corner cell of each receiver stencil */
+  const int32_t* tile_rec_ptr;     /* (n_tiles + 1): receivers whose corner lies in the tile */
+  const int32_t* tile_rec_list;
+  const int32_t* tile_cell_ptr;    /* (n_tiles + 1): touched cells of the tile */
+  const int32_t* tile_cell_local;  /* (x - x0) * tile_cols + (z - z0) */
+  const int32_t* tile_cell_gid;    /* row in cell_index / cell_ptr */
 } nw_acquisition;
 
 /* The medium: c^2 dt^2 on the padded grid and the absorbing coefficients. */
@@ -123,10 +153,12 @@ typedef struct nw_time {
  *    nefi/physics/timestep.py:141-169): the pair (p^{n0-1}, p^{n0}) is encoded into snapshot
  *    j = n0 / segment for every segment start n0; the adjoint recomputes each segment into
  *    `segbuf` (segment + 1 levels). snap_kind selects exact copies or 16-bit values with one
- *    power-of-two scale per block of NW_SNAP_BLOCK elements.
+ *    float scale per block of NW_SNAP_BLOCK elements: fp16 / bf16 with a power-of-two scale,
+ *    or int16 mantissas scaled by the block maximum (NW_SNAP_I16, block floating point). The
+ *    16-bit kinds store p^{n0} and p^{n0} - p^{n0-1}.
  *  both NULL: forward only; `ring` holds three levels.
  */
-#define NW_SNAP_BLOCK 1024
+#define NW_SNAP_BLOCK 32
 typedef struct nw_storage {
   void* history;
   void* ring;          /* 3 levels, used when history == NULL */
@@ -141,7 +173,7 @@ size_t nw_snapshot_bytes(const nw_grid* g, int32_t n_shots, int32_t n_snap, int3
 
 /*
  * Prepare the medium: c (physical grid, contiguous, dtype) -> c2dt2 = pad_replicate(c)^2 * dt2
- * in the ghost layout (nefi/physics/wave.py:222-240, 718). `n_abs` is the layer width per axis.
+ * in the ghost layout (nefi/physics/wave.py:222-240, 718). `n_abs` (host) is the layer width per axis.
  */
 int nw_prepare_medium(const nw_grid* g, const int32_t* n_abs, const void* c, double dt2,
                       void* c2dt2, void* stream);
@@ -158,18 +190,20 @@ int nw_initial_state(const nw_grid* g, const int32_t* n_abs, const nw_medium* m,
 /*
  * Forward run of steps [n_begin, n_end) for all shots. Levels are addressed through `st`
  * (history, or the ring when no history is given). Receiver samples of every recorded level
- * n in [n_begin, n_end] go to traces (n_shots, n_rec, n_t); with checkpointing, snapshots of
- * every segment start in [n_begin, n_end) are encoded. On entry levels n_begin-1 and n_begin
- * must be in place. Replaces WaveOperator.simulate / run_timestepping
- * (nefi/physics/wave.py:699-740, nefi/physics/timestep.py:144-149).
+ * n in [n_begin, n_end) go to traces (n_shots, n_rec, n_t), and of level n_end when it is the last
+ * step; with checkpointing, snapshots of every segment start in [n_begin, n_end) are encoded.
+ * On entry levels n_begin-1 and n_begin must be in place. `tune` may be NULL.
+ * Replaces WaveOperator.simulate / run_timestepping (nefi/physics/wave.py:699-740,
+ * nefi/physics/timestep.py:144-149).
  */
 int nw_forward(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, const nw_time* t,
-               const nw_storage* st, int32_t n_begin, int32_t n_end, void* traces, void* stream);
+               const nw_storage* st, const nw_tuning* tune, int32_t n_begin, int32_t n_end,
+               void* traces, void* stream);
 
 /*
  * Adjoint run for all shots: from trace cotangents `grad_traces` (n_shots, n_rec, n_t) computes
- *  - grad_c2dt2: per-shot accumulators (n_shots fields, dtype; zeroed by the call)
- *    of sum_n mu^{n+1} * Lap p^n, and
+ *  - grad_acc: nw_adjoint_groups() float64 fields (zeroed by the call) whose sum is
+ *    sum_shots sum_n mu^{n+1} * Lap p^n, the gradient w.r.t. c2dt2, and
  *  - lambda0 / mu1 (n_shots fields each, may be NULL): the sensitivities of p^0 and A*p^1
  *    needed by the initial-value operator.
  * `work` holds three adjoint levels (3 * n_shots fields). Uses the history or recomputes
@@ -177,29 +211,30 @@ int nw_forward(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, co
  * nefi/physics/wave.py:529-552 and nefi/physics/timestep.py:151-169.
  */
 int nw_adjoint(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, const nw_time* t,
-               const nw_storage* st, const void* grad_traces, void* work, void* grad_c2dt2,
-               void* lambda0, void* mu1, void* stream);
+               const nw_storage* st, const nw_tuning* tune, const void* grad_traces, void* work,
+               double* grad_acc, void* lambda0, void* mu1, void* stream);
 
 /*
- * Reduce per-shot c2dt2 gradients over shots in float64 and apply the chain rule of
+ * Reduce gradient accumulators (n_acc float64 fields) and apply the chain rule of
  * c2dt2 = pad_replicate(c)^2 dt^2: grad_c (physical grid, float64) =
- * pad_replicate^T(2 c_pad dt2 * sum_shots g) (nefi/physics/wave.py:231-240, 718).
+ * pad_replicate^T(2 c_pad dt2 * sum_acc g) (nefi/physics/wave.py:231-240, 718).
  * `accumulate` != 0 adds into grad_c instead of overwriting it.
  */
 int nw_reduce_grad_c(const nw_grid* g, const int32_t* n_abs, const void* c, double dt2,
-                     int32_t n_shots, const void* grad_c2dt2, int32_t accumulate, double* grad_c,
+                     int32_t n_acc, const double* grad_acc, int32_t accumulate, double* grad_c,
                      void* stream);
 
 /*
  * Gradient of the initial-value operator w.r.t. p0 (n_shots physical fields, dtype):
  * lambda^0 + lambda^-1 + Lap(1/2 c2dt2 lambda^-1) cropped to the physical grid, with
- * lambda^-1 = -B0 mu^1 (B0 = 1 when time.first_b_one). If grad_c2dt2 != NULL also adds
- * 1/2 lambda^-1 * Lap p^0 to it (the c-dependence of p^-1, nefi/physics/wave.py:850).
+ * lambda^-1 = -B0 mu^1 (B0 = 1 when time.first_b_one). If grad_acc != NULL also adds
+ * 1/2 lambda^-1 * Lap p^0 of shot s to accumulator s / shots_per_acc (the c-dependence of p^-1,
+ * nefi/physics/wave.py:850).
  */
 int nw_initial_state_adjoint(const nw_grid* g, const int32_t* n_abs, const nw_medium* m,
                              const nw_time* t, int32_t n_shots, const void* lambda0,
                              const void* mu1, const void* p0_level, void* grad_p0,
-                             void* grad_c2dt2, void* stream);
+                             double* grad_acc, int32_t shots_per_acc, void* stream);
 
 /*
  * Zero only the ghost cells of `n_fields` consecutive fields (e.g. a freshly allocated history),

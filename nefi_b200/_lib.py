@@ -13,14 +13,16 @@ from pathlib import Path
 import torch
 
 LIB_PATH = Path(__file__).resolve().parent / "libnefiwave.so"
+ABI_VERSION = 2
 
 NW_F32, NW_F64 = 0, 1
 NW_ABS_NONE, NW_ABS_SPONGE, NW_ABS_CERJAN = 0, 1, 2
 NW_SNAP_EXACT, NW_SNAP_F16, NW_SNAP_BF16 = 0, 1, 2
 NW_OK, NW_ERR_ARG, NW_ERR_CUDA, NW_ERR_UNSUPPORTED, NW_ERR_NONFINITE, NW_ERR_TIMEOUT = range(6)
-NW_SNAP_BLOCK = 1024
+NW_SNAP_BLOCK = 32
 
-SNAP_KINDS = {"exact": NW_SNAP_EXACT, "fp16": NW_SNAP_F16, "bf16": NW_SNAP_BF16}
+NW_SNAP_I16 = 3
+SNAP_KINDS = {"exact": NW_SNAP_EXACT, "fp16": NW_SNAP_F16, "bf16": NW_SNAP_BF16, "fixed16": NW_SNAP_I16}
 
 
 class Grid(C.Structure):
@@ -28,9 +30,14 @@ class Grid(C.Structure):
         ("ndim", C.c_int32), ("order", C.c_int32), ("dtype", C.c_int32), ("absorbing", C.c_int32),
         ("n", C.c_int32 * 3), ("core_lo", C.c_int32 * 3), ("core_hi", C.c_int32 * 3),
         ("w_center", C.c_double), ("w1", C.c_double * 3), ("w2", C.c_double * 3),
-        ("radius", C.c_int32), ("reserved", C.c_int32),
+        ("radius", C.c_int32), ("guard", C.c_int32),
         ("stride", C.c_int64 * 3), ("origin", C.c_int64), ("field_elems", C.c_int64),
     ]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("vz", C.c_int32), ("rx", C.c_int32), ("shots_per_cta", C.c_int32),
+                ("adj_shots_per_cta", C.c_int32), ("reserved", C.c_int32 * 4)]
 
 
 class Acquisition(C.Structure):
@@ -41,6 +48,9 @@ class Acquisition(C.Structure):
         ("rec_index", C.c_void_p), ("rec_weight", C.c_void_p),
         ("cell_index", C.c_void_p), ("cell_ptr", C.c_void_p), ("cell_rec", C.c_void_p),
         ("cell_weight", C.c_void_p),
+        ("tiles_z", C.c_int32), ("tile_rows", C.c_int32), ("tile_cols", C.c_int32),
+        ("rec_corner", C.c_void_p), ("tile_rec_ptr", C.c_void_p), ("tile_rec_list", C.c_void_p),
+        ("tile_cell_ptr", C.c_void_p), ("tile_cell_local", C.c_void_p), ("tile_cell_gid", C.c_void_p),
     ]
 
 
@@ -68,13 +78,15 @@ _SIGNATURES = {
     "nw_snapshot_bytes": (C.c_size_t, [P(Grid), C.c_int32, C.c_int32, C.c_int32]),
     "nw_prepare_medium": (C.c_int, [P(Grid), VP, VP, C.c_double, VP, VP]),
     "nw_initial_state": (C.c_int, [P(Grid), VP, P(Medium), C.c_int32, VP, VP, VP, VP]),
-    "nw_forward": (C.c_int, [P(Grid), P(Medium), P(Acquisition), P(Time), P(Storage), C.c_int32,
-                             C.c_int32, VP, VP]),
-    "nw_adjoint": (C.c_int, [P(Grid), P(Medium), P(Acquisition), P(Time), P(Storage), VP, VP, VP,
-                             VP, VP, VP]),
+    "nw_tile_shape": (C.c_int, [P(Grid), P(Tuning), P(C.c_int32), P(C.c_int32)]),
+    "nw_adjoint_groups": (C.c_int, [P(Grid), P(Tuning), C.c_int32]),
+    "nw_forward": (C.c_int, [P(Grid), P(Medium), P(Acquisition), P(Time), P(Storage), P(Tuning),
+                             C.c_int32, C.c_int32, VP, VP]),
+    "nw_adjoint": (C.c_int, [P(Grid), P(Medium), P(Acquisition), P(Time), P(Storage), P(Tuning), VP,
+                             VP, VP, VP, VP, VP]),
     "nw_reduce_grad_c": (C.c_int, [P(Grid), VP, VP, C.c_double, C.c_int32, VP, C.c_int32, VP, VP]),
     "nw_initial_state_adjoint": (C.c_int, [P(Grid), VP, P(Medium), P(Time), C.c_int32, VP, VP, VP,
-                                           VP, VP, VP]),
+                                           VP, VP, C.c_int32, VP]),
     "nw_sample": (C.c_int, [P(Grid), P(Acquisition), C.c_int32, VP, C.c_int32, VP, VP]),
     "nw_status": (C.c_int, [VP]),
     "nw_zero_ghosts": (C.c_int, [P(Grid), VP, C.c_int64, VP]),
@@ -106,7 +118,7 @@ def load(path: Path | None = None) -> C.CDLL:
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    if lib.nw_abi_version() != 1:
+    if lib.nw_abi_version() != ABI_VERSION:
         raise LibraryError(-1, f"ABI version mismatch: {lib.nw_abi_version()}")
     if path is None:
         _lib = lib

@@ -110,54 +110,59 @@ __global__ void initial_prev_kernel(KGrid<T> g, int ndim, const T* __restrict__ 
 
 // Adjoint of the initial state: lambda^-1 = -B0 mu^1,
 // grad_p0p = lambda^0 + lambda^-1 + Lap(0.5 C lambda^-1), cropped to the physical grid;
-// optionally grad_C += 0.5 lambda^-1 Lap p^0.
+// optionally acc[s / spa] += 0.5 lambda^-1 Lap p^0. blockIdx.y is an accumulator group whose
+// shots a thread visits in order, so no two threads add into the same accumulator cell.
 template <typename T, int R>
 __global__ void initial_adjoint_kernel(KGrid<T> g, PadMap pm, int ndim, const T* __restrict__ C,
-                                       const T* __restrict__ B, int b_one,
+                                       const T* __restrict__ B, int b_one, int n_shots, int spa,
                                        const T* __restrict__ lam0, const T* __restrict__ mu1,
                                        const T* __restrict__ p0, T* __restrict__ grad_p0,
-                                       T* __restrict__ grad_c) {
-  const int s = blockIdx.y;
+                                       double* __restrict__ acc) {
+  const int grp = blockIdx.y;
   const long long cells = (long long)g.n0 * g.n1 * g.n2;
-  const long long so = (long long)s * g.field;
-  const T* m = mu1 + so;
   const long long pcells = (long long)pm.m0 * pm.m1 * pm.m2;
-  auto lm1 = [&](long long i) -> T {
-    const T b = (b_one || B == nullptr) ? T(1) : B[i];
-    return -(b * m[i]);
-  };
-  auto hl = [&](long long i) -> T { return (T(0.5) * C[i]) * lm1(i); };
+  double* ga = acc ? acc + (long long)grp * g.field : nullptr;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < cells;
        t += (long long)gridDim.x * blockDim.x) {
     int x, y, z;
     cell_of(t, g.n0, g.n1, g.n2, ndim, x, y, z);
     const long long i = ghost_index(g, ndim, x, y, z);
-    const T l = lm1(i);
-    if (grad_c) grad_c[so + i] += (T(0.5) * l) * lap_at<T, R>(g, p0 + so, i, ndim);
     int pi, pj, pk;
     if (ndim == 2) { pi = x - pm.a0; pj = y - pm.a1; pk = 0; }
     else { pi = x - pm.a0; pj = y - pm.a1; pk = z - pm.a2; }
-    if (pi < 0 || pi >= pm.m0 || pj < 0 || pj >= pm.m1 || pk < 0 || pk >= pm.m2) continue;
-    T lh;
-    if (ndim == 2) {
-      lh = g.wc * hl(i) + g.w1a * (hl(i - g.s0) + hl(i + g.s0)) + g.w1b * (hl(i - 1) + hl(i + 1));
-      if (R == 2) lh += g.w2a * (hl(i - 2 * g.s0) + hl(i + 2 * g.s0)) + g.w2b * (hl(i - 2) + hl(i + 2));
-    } else {
-      lh = g.wc * hl(i) + g.w1a * (hl(i - g.s0) + hl(i + g.s0)) + g.w1b * (hl(i - g.s1) + hl(i + g.s1)) +
-           g.w1c * (hl(i - 1) + hl(i + 1));
-      if (R == 2)
-        lh += g.w2a * (hl(i - 2 * g.s0) + hl(i + 2 * g.s0)) + g.w2b * (hl(i - 2 * g.s1) + hl(i + 2 * g.s1)) +
-              g.w2c * (hl(i - 2) + hl(i + 2));
+    const bool phys = !(pi < 0 || pi >= pm.m0 || pj < 0 || pj >= pm.m1 || pk < 0 || pk >= pm.m2);
+    for (int s = grp * spa; s < min(n_shots, (grp + 1) * spa); ++s) {
+      const long long so = (long long)s * g.field;
+      const T* m = mu1 + so;
+      auto lm1 = [&](long long k) -> T {
+        const T b = (b_one || B == nullptr) ? T(1) : B[k];
+        return -(b * m[k]);
+      };
+      auto hl = [&](long long k) -> T { return (T(0.5) * C[k]) * lm1(k); };
+      const T l = lm1(i);
+      if (ga) ga[i] += (double)((T(0.5) * l) * lap_at<T, R>(g, p0 + so, i, ndim));
+      if (!phys) continue;
+      T lh;
+      if (ndim == 2) {
+        lh = g.wc * hl(i) + g.w1a * (hl(i - g.s0) + hl(i + g.s0)) + g.w1b * (hl(i - 1) + hl(i + 1));
+        if (R == 2) lh += g.w2a * (hl(i - 2 * g.s0) + hl(i + 2 * g.s0)) + g.w2b * (hl(i - 2) + hl(i + 2));
+      } else {
+        lh = g.wc * hl(i) + g.w1a * (hl(i - g.s0) + hl(i + g.s0)) + g.w1b * (hl(i - g.s1) + hl(i + g.s1)) +
+             g.w1c * (hl(i - 1) + hl(i + 1));
+        if (R == 2)
+          lh += g.w2a * (hl(i - 2 * g.s0) + hl(i + 2 * g.s0)) + g.w2b * (hl(i - 2 * g.s1) + hl(i + 2 * g.s1)) +
+                g.w2c * (hl(i - 2) + hl(i + 2));
+      }
+      const long long pidx = ((long long)pi * pm.m1 + pj) * pm.m2 + pk;
+      grad_p0[(long long)s * pcells + pidx] = (lam0[so + i] + l) + lh;
     }
-    const long long pidx = ((long long)pi * pm.m1 + pj) * pm.m2 + pk;
-    grad_p0[(long long)s * pcells + pidx] = (lam0[so + i] + l) + lh;
   }
 }
 
-// grad_c[phys] (+)= 2 c dt2 * sum_shots sum_{padded cells -> phys} g_s[cell], in float64.
+// grad_c[phys] (+)= 2 c dt2 * sum_acc sum_{padded cells -> phys} g_acc[cell], in float64.
 template <typename T>
 __global__ void reduce_grad_kernel(KGrid<T> g, PadMap pm, int ndim, const T* __restrict__ c,
-                                   double dt2, int n_shots, const T* __restrict__ gs,
+                                   double dt2, int n_acc, const double* __restrict__ gs,
                                    int accumulate, double* __restrict__ out) {
   const long long pcells = (long long)pm.m0 * pm.m1 * pm.m2;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < pcells;
@@ -172,11 +177,11 @@ __global__ void reduce_grad_kernel(KGrid<T> g, PadMap pm, int ndim, const T* __r
     const int y0 = lo(j, pm.a1, pm.m1), y1 = hi(j, pm.a1, pm.m1);
     const int z0 = ndim == 3 ? lo(k, pm.a2, pm.m2) : 0, z1 = ndim == 3 ? hi(k, pm.a2, pm.m2) : 0;
     double acc = 0.0;
-    for (int s = 0; s < n_shots; ++s) {
-      const T* gp = gs + (long long)s * g.field;
+    for (int s = 0; s < n_acc; ++s) {
+      const double* gp = gs + (long long)s * g.field;
       for (int x = x0; x <= x1; ++x)
         for (int y = y0; y <= y1; ++y)
-          for (int z = z0; z <= z1; ++z) acc += (double)gp[ghost_index(g, ndim, x, y, z)];
+          for (int z = z0; z <= z1; ++z) acc += gp[ghost_index(g, ndim, x, y, z)];
     }
     const double v = 2.0 * (double)c[t] * dt2 * acc;
     out[t] = accumulate ? out[t] + v : v;
@@ -186,7 +191,7 @@ __global__ void reduce_grad_kernel(KGrid<T> g, PadMap pm, int ndim, const T* __r
 // Zero the ghost cells of n_fields consecutive fields (a warp per storage row): whole rows
 // outside the grid and the tail [n_last, ld) of every data row. Interior cells are untouched.
 template <typename T>
-__global__ void zero_ghosts_kernel(T* __restrict__ base, long long field, long long n_rows,
+__global__ void zero_ghosts_kernel(T* __restrict__ base, long long field, int guard, long long n_rows,
                                    int ld, int n_last, int ndim, int r, int n0, int n1,
                                    int rows_per_plane, long long n_fields) {
   const long long warps = (long long)gridDim.x * (blockDim.x / 32);
@@ -201,103 +206,111 @@ __global__ void zero_ghosts_kernel(T* __restrict__ base, long long field, long l
       const long long plane = row / rows_per_plane, y = row % rows_per_plane;
       ghost_row = plane < r || plane >= r + n0 || y >= n1;
     }
-    T* p = base + f * field + row * ld;
+    if (row == 0)
+      for (int z = lane; z < guard; z += 32) base[f * field + z] = T(0);
+    T* p = base + f * field + guard + row * ld;
     for (int z = ghost_row ? lane : n_last + lane; z < ld; z += 32) p[z] = T(0);
   }
 }
 
 // ------------------------------------------------------------------------------------------
-// Snapshot codec: blocks of SNAP_BLOCK contiguous elements of one field, each stored as
-// 16-bit values with one power-of-two float scale (block floating point).
+// Snapshot codec: blocks of SNAP_BLOCK = 32 contiguous elements of one field (one warp), each
+// stored as 16-bit values with one float scale per block:
+//   fp16 / bf16: power-of-two scale (exact to apply), 11- / 8-bit mantissas;
+//   fixed16:     int16 mantissas with scale = block max / 32767 (block floating point), whose
+//                absolute error is 2^-16 of the block maximum.
 // ------------------------------------------------------------------------------------------
-constexpr int SNAP_BLOCK = 1024;
+constexpr int SNAP_BLOCK = 32;
+constexpr int CODEC_F16 = 1, CODEC_BF16 = 2, CODEC_I16 = 3;
 
-template <typename H>
-struct Half16;
+template <int K>
+struct Codec;
 template <>
-struct Half16<__half> {
-  static __device__ __forceinline__ __half enc(float v) { return __float2half_rn(v); }
-  static __device__ __forceinline__ float dec(__half v) { return __half2float(v); }
-  static constexpr int kExpMax = 15;  // |v / scale| <= 2^15 < 65504
+struct Codec<CODEC_F16> {
+  using H = __half;
+  static __device__ __forceinline__ float scale(float mx) {
+    int e;
+    frexpf(mx, &e);  // mx <= 2^e; |v / scale| <= 2^15 < 65504
+    return ldexpf(1.f, max(-126, min(127, e - 15)));
+  }
+  static __device__ __forceinline__ H enc(float v, float inv) { return __float2half_rn(v * inv); }
+  static __device__ __forceinline__ float dec(H q, float s) { return __half2float(q) * s; }
 };
 template <>
-struct Half16<__nv_bfloat16> {
-  static __device__ __forceinline__ __nv_bfloat16 enc(float v) { return __float2bfloat16_rn(v); }
-  static __device__ __forceinline__ float dec(__nv_bfloat16 v) { return __bfloat162float(v); }
-  static constexpr int kExpMax = 0;
+struct Codec<CODEC_BF16> {
+  using H = __nv_bfloat16;
+  static __device__ __forceinline__ float scale(float mx) {
+    int e;
+    frexpf(mx, &e);
+    return ldexpf(1.f, max(-126, min(127, e)));
+  }
+  static __device__ __forceinline__ H enc(float v, float inv) { return __float2bfloat16_rn(v * inv); }
+  static __device__ __forceinline__ float dec(H q, float s) { return __bfloat162float(q) * s; }
+};
+template <>
+struct Codec<CODEC_I16> {
+  using H = short;
+  static __device__ __forceinline__ float scale(float mx) { return fmaxf(mx / 32767.f, 1.17549435e-38f); }
+  static __device__ __forceinline__ H enc(float v, float inv) {
+    return (short)fminf(32767.f, fmaxf(-32767.f, rintf(v * inv)));
+  }
+  static __device__ __forceinline__ float dec(H q, float s) { return (float)q * s; }
 };
 
 __device__ int g_status;  // sticky device status word (NW_ERR_* or 0)
 
-// One CTA of 256 threads per block; grid.x = blocks per field, grid.y = fields.
-template <typename T, typename H>
-__global__ void __launch_bounds__(256) snap_encode(const T* __restrict__ src, long long field,
-                                                   int nblk, H* __restrict__ vals,
+// Encodes src (or src - sub when sub != nullptr: the level difference, whose small magnitude
+// would be lost if both levels were rounded to 16 bits separately). One warp per block;
+// grid.x covers the blocks of one field, grid.y the fields.
+template <typename T, int K>
+__global__ void __launch_bounds__(256) snap_encode(const T* __restrict__ src, const T* __restrict__ sub,
+                                                   long long field, int nblk,
+                                                   typename Codec<K>::H* __restrict__ vals,
                                                    float* __restrict__ scales) {
-  const int b = blockIdx.x, f = blockIdx.y;
-  const long long off = (long long)b * SNAP_BLOCK;
-  const T* p = src + (long long)f * field + off;
-  const long long n = min((long long)SNAP_BLOCK, field - off);
-  float v[4];
-  float mx = 0.f;
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const int e = threadIdx.x + 256 * k;
-    v[k] = e < n ? (float)p[e] : 0.f;
-    mx = fmaxf(mx, fabsf(v[k]));
-    if (!(fabsf(v[k]) <= 3.0e38f)) mx = __int_as_float(0x7fc00000);  // NaN/Inf poisons the block
+  const int f = blockIdx.y;
+  const long long b = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (b >= nblk) return;
+  const int lane = threadIdx.x & 31;
+  const long long e = b * SNAP_BLOCK + lane;
+  float v = 0.f;
+  if (e < field) {
+    const long long i = (long long)f * field + e;
+    v = (float)(sub ? src[i] - sub[i] : src[i]);
   }
-  __shared__ float red[8];
-  for (int o = 16; o > 0; o >>= 1) {
-    const float other = __shfl_xor_sync(0xffffffffu, mx, o);
-    mx = (isnan(other) || isnan(mx)) ? __int_as_float(0x7fc00000) : fmaxf(mx, other);
-  }
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    float m = threadIdx.x < 8 ? red[threadIdx.x] : 0.f;
-    for (int o = 4; o > 0; o >>= 1) {
-      const float other = __shfl_xor_sync(0xffffffffu, m, o);
-      m = (isnan(other) || isnan(m)) ? __int_as_float(0x7fc00000) : fmaxf(m, other);
-    }
-    if (threadIdx.x == 0) red[0] = m;
-  }
-  __syncthreads();
-  mx = red[0];
-  float scale = 1.f;
-  if (isnan(mx)) {
-    scale = mx;
-    if (threadIdx.x == 0) atomicExch(&g_status, 4);
+  const bool bad = !(fabsf(v) <= 3.0e38f);  // NaN or Inf
+  float mx = fabsf(v);
+  for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  const bool any_bad = __any_sync(0xffffffffu, bad);
+  float s = 1.f;
+  if (any_bad) {
+    s = __int_as_float(0x7fc00000);
+    if (lane == 0) atomicExch(&g_status, 4);
   } else if (mx > 0.f) {
-    int e;
-    frexpf(mx, &e);  // mx <= 2^e
-    scale = ldexpf(1.f, e - Half16<H>::kExpMax);
+    s = Codec<K>::scale(mx);
   }
-  const float inv = isnan(scale) ? 0.f : 1.f / scale;  // exact: scale is a power of two
-  H* q = vals + ((long long)f * nblk + b) * SNAP_BLOCK;
-#pragma unroll
-  for (int k = 0; k < 4; ++k) q[threadIdx.x + 256 * k] = Half16<H>::enc(v[k] * inv);
-  if (threadIdx.x == 0) scales[(long long)f * nblk + b] = scale;
+  const float inv = any_bad ? 0.f : 1.f / s;
+  vals[(long long)f * nblk * SNAP_BLOCK + b * SNAP_BLOCK + lane] = Codec<K>::enc(v, inv);
+  if (lane == 0) scales[(long long)f * nblk + b] = s;
 }
 
-template <typename T, typename H>
-__global__ void __launch_bounds__(256) snap_decode(const H* __restrict__ vals,
+// Decodes into dst (or dst = minuend - decoded when minuend != nullptr, undoing the difference
+// encoding of snap_encode).
+template <typename T, int K>
+__global__ void __launch_bounds__(256) snap_decode(const typename Codec<K>::H* __restrict__ vals,
                                                    const float* __restrict__ scales, int nblk,
-                                                   long long field, T* __restrict__ dst) {
-  const int b = blockIdx.x, f = blockIdx.y;
-  const long long off = (long long)b * SNAP_BLOCK;
-  const long long n = min((long long)SNAP_BLOCK, field - off);
-  const float scale = scales[(long long)f * nblk + b];
-  if (!(fabsf(scale) <= 3.0e38f) || !(scale > 0.f)) {
-    if (threadIdx.x == 0) atomicExch(&g_status, 4);
-  }
-  const H* q = vals + ((long long)f * nblk + b) * SNAP_BLOCK;
-  T* p = dst + (long long)f * field + off;
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const int e = threadIdx.x + 256 * k;
-    if (e < n) p[e] = (T)(Half16<H>::dec(q[e]) * scale);
-  }
+                                                   long long field, const T* __restrict__ minuend,
+                                                   T* __restrict__ dst) {
+  const int f = blockIdx.y;
+  const long long b = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (b >= nblk) return;
+  const int lane = threadIdx.x & 31;
+  const float s = scales[(long long)f * nblk + b];
+  if (!(s > 0.f && s <= 3.0e38f) && lane == 0) atomicExch(&g_status, 4);
+  const long long e = b * SNAP_BLOCK + lane;
+  if (e >= field) return;
+  const long long i = (long long)f * field + e;
+  const T v = (T)Codec<K>::dec(vals[(long long)f * nblk * SNAP_BLOCK + b * SNAP_BLOCK + lane], s);
+  dst[i] = minuend ? minuend[i] - v : v;
 }
 
 }  // namespace nw

@@ -60,7 +60,7 @@ struct AdjStep {
   const T* __restrict__ B;
   int apply_a;
   const T* __restrict__ p;      // p^n (nullptr: no gradient term)
-  T* __restrict__ grad;         // per-shot dJ/dC accumulators
+  double* __restrict__ grad;    // per-shot float64 dJ/dC accumulators
 };
 
 __device__ __forceinline__ long long global_thread_in_shot() {
@@ -84,129 +84,7 @@ __device__ __forceinline__ void gather_receivers(const T* __restrict__ lvl, T* _
 }
 
 // ------------------------------------------------------------------------------------------
-// 2-D forward step. Thread (tx, ty) owns column z = bx*32 + tx and RX rows starting at
-// x0 = (by*blockDim.y + ty)*RX; the x-neighbours come from a register window, the
-// z-neighbours from L1.
-// ------------------------------------------------------------------------------------------
-template <typename T, int R, bool AB, int RX>
-__global__ void __launch_bounds__(256) fwd2d(KGrid<T> g, FwdStep<T> a) {
-  const int s = blockIdx.z;
-  const long long so = (long long)s * g.field;
-  const T* __restrict__ pc = a.cur + so;
-  if (a.traces) gather_receivers<T, 4>(pc, a.traces, a.rec_idx, a.rec_w, a.n_rec, a.n_t, a.j, s);
-
-  const int z = blockIdx.x * blockDim.x + threadIdx.x;
-  const int x0 = (blockIdx.y * blockDim.y + threadIdx.y) * RX;
-  if (z >= g.n1 || x0 >= g.n0) return;
-  const long long base = g.origin + (long long)x0 * g.s0 + z;
-
-  T col[RX + 2 * R];
-#pragma unroll
-  for (int k = 0; k < RX + 2 * R; ++k) {
-    const int xr = x0 - R + k;
-    col[k] = (xr < g.n0 + R) ? pc[base + (long long)(k - R) * g.s0] : T(0);
-  }
-  int bx = -4, bz = -4;
-  T sw0 = 0, sw1 = 0, sw2 = 0, sw3 = 0, wn = 0;
-  if (a.src_corner) {
-    bx = a.src_corner[2 * s];
-    bz = a.src_corner[2 * s + 1];
-    if (bz <= z && z <= bz + 1 && bx + 1 >= x0 && bx <= x0 + RX - 1) {
-      const T* sw = a.src_w + 4 * s;
-      sw0 = sw[0]; sw1 = sw[1]; sw2 = sw[2]; sw3 = sw[3];
-      wn = a.wavelet[a.n];
-    } else {
-      bx = -4;
-    }
-  }
-#pragma unroll
-  for (int k = 0; k < RX; ++k) {
-    const int x = x0 + k;
-    if (x < g.n0) {
-      const long long i = base + (long long)k * g.s0;
-      const T c = col[k + R];
-      T lap = g.wc * c + g.w1a * (col[k + R - 1] + col[k + R + 1]) + g.w1b * (pc[i - 1] + pc[i + 1]);
-      if (R == 2) lap += g.w2a * (col[k] + col[k + 4]) + g.w2b * (pc[i - 2] + pc[i + 2]);
-      const T pp = a.prev[so + i];
-      T av = T(1), bv = T(1);
-      bool layer = false;
-      if (AB) {
-        layer = x < g.lo0 || x >= g.hi0 || z < g.lo1 || z >= g.hi1;
-        if (layer) {
-          av = a.A[i];
-          bv = a.b_one ? T(1) : a.B[i];
-        }
-      }
-      T rhs = (T(2) * c - bv * pp) + a.C[i] * lap;
-      const int dx = x - bx, dz = z - bz;
-      if (dx >= 0 && dx <= 1 && dz >= 0 && dz <= 1) {
-        const T w = (dx == 0) ? (dz == 0 ? sw0 : sw1) : (dz == 0 ? sw2 : sw3);
-        rhs += w * wn;
-      }
-      a.next[so + i] = layer ? av * rhs : rhs;
-    }
-  }
-}
-
-// 2-D adjoint step (see the header comment).
-template <typename T, int R, bool AB, int RX>
-__global__ void __launch_bounds__(256) adj2d(KGrid<T> g, AdjStep<T> a) {
-  const int s = blockIdx.z;
-  const long long so = (long long)s * g.field;
-  const int z = blockIdx.x * blockDim.x + threadIdx.x;
-  const int x0 = (blockIdx.y * blockDim.y + threadIdx.y) * RX;
-  if (z >= g.n1 || x0 >= g.n0) return;
-  const long long base = g.origin + (long long)x0 * g.s0 + z;
-  const T* __restrict__ m1 = a.mu1 + so;
-  const T* __restrict__ C = a.C;
-
-  T q[RX + 2 * R];   // C * mu^{n+1} along x
-  T m[RX];           // mu^{n+1} at the owned cells
-#pragma unroll
-  for (int k = 0; k < RX + 2 * R; ++k) {
-    const int xr = x0 - R + k;
-    const long long i = base + (long long)(k - R) * g.s0;
-    T mv = (xr < g.n0 + R) ? m1[i] : T(0);
-    q[k] = (xr < g.n0 + R) ? C[i] * mv : T(0);
-    if (k >= R && k < R + RX) m[k - R] = mv;
-  }
-  T pw[RX + 2 * R];  // p^n along x
-  const T* __restrict__ pn = a.p ? a.p + so : nullptr;
-  if (pn) {
-#pragma unroll
-    for (int k = 0; k < RX + 2 * R; ++k) {
-      const int xr = x0 - R + k;
-      pw[k] = (xr < g.n0 + R) ? pn[base + (long long)(k - R) * g.s0] : T(0);
-    }
-  }
-#pragma unroll
-  for (int k = 0; k < RX; ++k) {
-    const int x = x0 + k;
-    if (x < g.n0) {
-      const long long i = base + (long long)k * g.s0;
-      T lq = g.wc * q[k + R] + g.w1a * (q[k + R - 1] + q[k + R + 1]) +
-             g.w1b * (C[i - 1] * m1[i - 1] + C[i + 1] * m1[i + 1]);
-      if (R == 2)
-        lq += g.w2a * (q[k] + q[k + 4]) + g.w2b * (C[i - 2] * m1[i - 2] + C[i + 2] * m1[i + 2]);
-      T av = T(1), bv = T(1);
-      bool layer = false;
-      if (AB) {
-        layer = x < g.lo0 || x >= g.hi0 || z < g.lo1 || z >= g.hi1;
-        if (layer) { av = a.A[i]; bv = a.B[i]; }
-      }
-      T lam = (T(2) * m[k] + lq) - bv * a.mu2[so + i];
-      a.out[so + i] = (layer && a.apply_a) ? av * lam : lam;
-      if (pn) {
-        T lp = g.wc * pw[k + R] + g.w1a * (pw[k + R - 1] + pw[k + R + 1]) + g.w1b * (pn[i - 1] + pn[i + 1]);
-        if (R == 2) lp += g.w2a * (pw[k] + pw[k + 4]) + g.w2b * (pn[i - 2] + pn[i + 2]);
-        a.grad[so + i] += m[k] * lp;
-      }
-    }
-  }
-}
-
-// ------------------------------------------------------------------------------------------
-// 3-D variants: thread (tx, ty) owns (y, z) = (by*blockDim.y + ty, bz*32 + tx) and RX planes
+// 3-D kernels: thread (tx, ty) owns (y, z) = (by*blockDim.y + ty, bz*32 + tx) and RX planes
 // along x starting at x0 = blockIdx.y*RX; blockIdx.x enumerates (y-tile, z-tile).
 // ------------------------------------------------------------------------------------------
 struct Tile3 {
@@ -331,7 +209,7 @@ __global__ void __launch_bounds__(256) adj3d(KGrid<T> g, AdjStep<T> a) {
         if (R == 2)
           lp += g.w2a * (pw[k] + pw[k + 4]) + g.w2b * (pn[i - 2 * sy] + pn[i + 2 * sy]) +
                 g.w2c * (pn[i - 2] + pn[i + 2]);
-        a.grad[so + i] += m[k] * lp;
+        a.grad[so + i] += (double)(m[k] * lp);
       }
     }
   }

@@ -1,0 +1,535 @@
+// stencil2d.cuh — tiled 2-D leapfrog kernels for sm_100a.
+//
+// One CTA (8 warps) owns a tile of TX = 8*RX rows by TZ = 32*VZ columns and loops over a group
+// of shots. For every shot the input tiles (p^n or mu^{n+1} with an R-row and 16-byte-column halo,
+// and the core of p^{n-1} or mu^{n+2}) are staged in shared memory by cp.async, double buffered
+// so that the copies of shot s+1 overlap the arithmetic of shot s. Each thread computes the
+// shared/global offsets of the 16-byte chunks it copies once per CTA; per shot it only adds the
+// shot's base address. A thread owns VZ adjacent columns and RX rows: it slides a (2R+1)-row
+// register window down its columns, reading each row once as a VZ-wide vector plus two halo
+// vectors, so every shared-memory access is a conflict-free 8- or 16-byte load. Coefficients
+// (c^2 dt^2 and the absorbing A/B) are read per row from global memory; they are the same for
+// every shot of the CTA and stay in L1.
+//
+// Receivers are gathered and adjoint sources injected inside the same kernels, from per-tile
+// tables built on the host (the receivers whose stencil corner lies in the tile; the cells of the
+// tile that receiver stencils touch), in a fixed order, so results are bitwise reproducible.
+#pragma once
+#include <type_traits>
+
+#include "kernels.cuh"
+
+namespace nw {
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Vector of N elements of T loaded/stored as one 8- or 16-byte access.
+template <typename T, int N>
+__device__ __forceinline__ void vload(const T* p, T (&o)[N]) {
+  static_assert(sizeof(T) * N == 8 || sizeof(T) * N == 16, "vector width");
+  if constexpr (sizeof(T) * N == 16) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    const T* q = reinterpret_cast<const T*>(&t);
+#pragma unroll
+    for (int i = 0; i < N; ++i) o[i] = q[i];
+  } else {
+    const float2 t = *reinterpret_cast<const float2*>(p);
+    const T* q = reinterpret_cast<const T*>(&t);
+#pragma unroll
+    for (int i = 0; i < N; ++i) o[i] = q[i];
+  }
+}
+// Read-only global load through the non-coherent (L1) path.
+template <typename T, int N>
+__device__ __forceinline__ void vldg(const T* p, T (&o)[N]) {
+  if constexpr (sizeof(T) * N == 16) {
+    const float4 t = __ldg(reinterpret_cast<const float4*>(p));
+    const T* q = reinterpret_cast<const T*>(&t);
+#pragma unroll
+    for (int i = 0; i < N; ++i) o[i] = q[i];
+  } else {
+    const float2 t = __ldg(reinterpret_cast<const float2*>(p));
+    const T* q = reinterpret_cast<const T*>(&t);
+#pragma unroll
+    for (int i = 0; i < N; ++i) o[i] = q[i];
+  }
+}
+template <typename T, int N>
+__device__ __forceinline__ void vstore(T* p, const T (&o)[N]) {
+  if constexpr (sizeof(T) * N == 16) {
+    float4 t;
+    T* q = reinterpret_cast<T*>(&t);
+#pragma unroll
+    for (int i = 0; i < N; ++i) q[i] = o[i];
+    *reinterpret_cast<float4*>(p) = t;
+  } else {
+    float2 t;
+    T* q = reinterpret_cast<T*>(&t);
+#pragma unroll
+    for (int i = 0; i < N; ++i) q[i] = o[i];
+    *reinterpret_cast<float2*>(p) = t;
+  }
+}
+
+// Per-tile tables, built on the host for one tile shape (TX, TZ).
+struct TileTables {
+  int tiles_z;                        // tiles along the contiguous axis (gridDim.x)
+  const int* __restrict__ rec_ptr;    // (n_tiles + 1): receivers whose stencil corner is in the tile
+  const int* __restrict__ rec_list;   // receiver ids
+  const int* __restrict__ rec_corner; // (n_rec, 2) corner cell (x, z)
+  const int* __restrict__ cell_ptr;   // (n_tiles + 1): receiver-touched cells of the tile
+  const int* __restrict__ cell_local; // (x - x0) * TZ + (z - z0)
+  const int* __restrict__ cell_gid;   // row of the cell in the global cell table
+  const int* __restrict__ gcell_ptr;  // global cell table: entries of each touched cell
+  const int* __restrict__ gcell_rec;
+};
+
+template <typename T>
+struct FwdTiled {
+  const T* __restrict__ prev;
+  const T* __restrict__ cur;
+  T* __restrict__ next;
+  const T* __restrict__ C;
+  const T* __restrict__ A;
+  const T* __restrict__ B;
+  int b_one;
+  const int* __restrict__ src_corner;
+  const T* __restrict__ src_w;
+  const T* __restrict__ wavelet;
+  int n;
+  int n_shots, shots_per_cta;
+  T* __restrict__ traces;  // non-null on record steps
+  const T* __restrict__ rec_w;
+  int n_rec, n_t, j;
+  TileTables tt;
+};
+
+template <typename T>
+struct AdjTiled {
+  const T* __restrict__ mu1;
+  const T* __restrict__ mu2;
+  T* __restrict__ out;
+  const T* __restrict__ C;
+  const T* __restrict__ A;
+  const T* __restrict__ B;
+  int apply_a;
+  const T* __restrict__ p;      // p^n, nullptr: no gradient term
+  double* __restrict__ gacc;    // (n_groups, field) float64 accumulators of dJ/dC
+  int n_shots, shots_per_cta;
+  const T* __restrict__ gtr;    // trace cotangents (n_shots, n_rec, n_t); non-null on record steps
+  const T* __restrict__ gcell_w;
+  int n_rec, n_t, j;
+  TileTables tt;
+};
+
+template <typename T, int VZ, int RX, int R>
+struct Tile2Shape {
+  static constexpr int TZ = 32 * VZ;
+  static constexpr int TX = 8 * RX;
+  static constexpr int HL = 16 / (int)sizeof(T);  // halo columns per side (one 16-byte chunk)
+  static constexpr int SW = TZ + 2 * HL;          // shared row width of halo tiles
+  static constexpr int EPC = 16 / (int)sizeof(T); // elements per 16-byte chunk
+  static constexpr int HR = TX + 2 * R;           // rows of a halo tile
+  static constexpr int PS = HR * SW;              // elements of a halo tile
+  static constexpr int QS = TX * TZ;              // elements of a core tile
+  static constexpr int NCH = (HR * (SW / EPC) + 255) / 256;  // halo chunks per thread
+  static constexpr int NCC = (TX * (TZ / EPC) + 255) / 256;  // core chunks per thread
+};
+
+// The chunks one thread copies for one tile region: shared and global element offsets (the
+// global offset relative to a field's base; -1 marks a chunk outside the stored rows).
+template <int NC>
+struct CopyPlan {
+  int soff[NC];
+  int goff[NC];
+};
+
+// Halo tile: rows [x0 - R, x0 + TX + R) x columns [z0 - HL, z0 + TZ + HL), row pitch SW.
+// Rows past the last ghost row and chunks past the row pitch are not stored.
+template <typename T, int VZ, int RX, int R>
+__device__ __forceinline__ CopyPlan<Tile2Shape<T, VZ, RX, R>::NCH> plan_halo(const KGrid<T>& g, int x0, int z0) {
+  using S = Tile2Shape<T, VZ, RX, R>;
+  constexpr int CPR = S::SW / S::EPC;
+  CopyPlan<S::NCH> p;
+#pragma unroll
+  for (int i = 0; i < S::NCH; ++i) {
+    const int c = threadIdx.x + 256 * i;
+    const int row = c / CPR, ch = c - row * CPR;
+    const int x = x0 - R + row;
+    const int z = z0 - S::HL + ch * S::EPC;
+    p.soff[i] = row * S::SW + ch * S::EPC;
+    p.goff[i] = (c < S::HR * CPR && x < g.n0 + R && z < (int)g.s0) ? (int)(g.origin + (long long)x * g.s0 + z) : -1;
+  }
+  return p;
+}
+// Core tile: rows [x0, x0 + TX) x columns [z0, z0 + TZ), row pitch TZ.
+template <typename T, int VZ, int RX, int R>
+__device__ __forceinline__ CopyPlan<Tile2Shape<T, VZ, RX, R>::NCC> plan_core(const KGrid<T>& g, int x0, int z0) {
+  using S = Tile2Shape<T, VZ, RX, R>;
+  constexpr int CPR = S::TZ / S::EPC;
+  CopyPlan<S::NCC> p;
+#pragma unroll
+  for (int i = 0; i < S::NCC; ++i) {
+    const int c = threadIdx.x + 256 * i;
+    const int row = c / CPR, ch = c - row * CPR;
+    const int x = x0 + row;
+    const int z = z0 + ch * S::EPC;
+    p.soff[i] = row * S::TZ + ch * S::EPC;
+    p.goff[i] = (c < S::TX * CPR && x < g.n0 && z < (int)g.s0) ? (int)(g.origin + (long long)x * g.s0 + z) : -1;
+  }
+  return p;
+}
+template <typename T, int NC>
+__device__ __forceinline__ void issue(const CopyPlan<NC>& p, const T* __restrict__ field, T* dst) {
+#pragma unroll
+  for (int i = 0; i < NC; ++i)
+    if (p.goff[i] >= 0) cp_async16(dst + p.soff[i], field + p.goff[i]);
+}
+
+// Row loader of the sliding window: own VZ vector and the two neighbouring vectors.
+template <typename T, int VZ>
+struct Row3 {
+  T l[VZ], c[VZ], r[VZ];
+};
+template <typename T, int VZ>
+__device__ __forceinline__ T zval(const Row3<T, VZ>& w, int u) {  // column u in [-VZ, 2VZ)
+  return u < 0 ? w.l[VZ + u] : (u >= VZ ? w.r[u - VZ] : w.c[u]);
+}
+
+template <typename T, int VZ>
+__device__ __forceinline__ void store_row(T* dst, const T (&o)[VZ], int zc, int n1) {
+  if (zc + VZ <= n1) {
+    vstore<T, VZ>(dst, o);
+  } else {
+#pragma unroll
+    for (int v = 0; v < VZ; ++v)
+      if (zc + v < n1) dst[v] = o[v];
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// forward step
+// ------------------------------------------------------------------------------------------
+template <typename T, int R, int VZ, int RX, bool AB>
+__global__ void __launch_bounds__(256, 3) fwd2d_tiled(KGrid<T> g, FwdTiled<T> a) {
+  using S = Tile2Shape<T, VZ, RX, R>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sp = reinterpret_cast<T*>(smem_raw);  // [2][PS] p^n
+  T* sq = sp + 2 * S::PS;                  // [2][QS] p^{n-1}
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int z0 = blockIdx.x * S::TZ, x0 = blockIdx.y * S::TX;
+  const int tile = blockIdx.y * a.tt.tiles_z + blockIdx.x;
+  const int sb = blockIdx.z * a.shots_per_cta;
+  const int se = min(sb + a.shots_per_cta, a.n_shots);
+  const int zc = z0 + lane * VZ;  // first owned column
+  const int xr = x0 + warp * RX;  // first owned row
+  const int lrow = warp * RX;     // first owned row inside the tile
+  const bool own_cols = zc < g.n1;
+
+  const CopyPlan<S::NCH> ph = plan_halo<T, VZ, RX, R>(g, x0, z0);
+  const CopyPlan<S::NCC> pc = plan_core<T, VZ, RX, R>(g, x0, z0);
+  issue(ph, a.cur + (long long)sb * g.field, sp);
+  issue(pc, a.prev + (long long)sb * g.field, sq);
+  cp_async_commit();
+
+  const bool layer_tile = AB && (x0 < g.lo0 || x0 + S::TX > g.hi0 || z0 < g.lo1 || z0 + S::TZ > g.hi1);
+  const T wc = g.wc, w1x = g.w1a, w1z = g.w1b, w2x = g.w2a, w2z = g.w2b;
+  const long long cbase = g.origin + (long long)xr * g.s0 + zc;  // owned cells of row k: + k*s0
+
+  for (int s = sb; s < se; ++s) {
+    const int buf = (s - sb) & 1;
+    if (s + 1 < se) {
+      issue(ph, a.cur + (long long)(s + 1) * g.field, sp + (buf ^ 1) * S::PS);
+      issue(pc, a.prev + (long long)(s + 1) * g.field, sq + (buf ^ 1) * S::QS);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const T* P = sp + buf * S::PS;
+    const T* Q = sq + buf * S::QS;
+
+    if (a.traces) {  // receiver samples of p^n from the staged tile
+      const int e0 = a.tt.rec_ptr[tile], e1 = a.tt.rec_ptr[tile + 1];
+      for (int e = e0 + threadIdx.x; e < e1; e += 256) {
+        const int r = a.tt.rec_list[e];
+        const int row = a.tt.rec_corner[2 * r] - x0 + R, col = a.tt.rec_corner[2 * r + 1] - z0 + S::HL;
+        const T* w = a.rec_w + 4 * r;
+        T acc = T(0);
+        acc += w[0] * P[row * S::SW + col];
+        acc += w[1] * P[row * S::SW + col + 1];
+        acc += w[2] * P[(row + 1) * S::SW + col];
+        acc += w[3] * P[(row + 1) * S::SW + col + 1];
+        a.traces[((long long)s * a.n_rec + r) * a.n_t + a.j] = acc;
+      }
+    }
+    // the shot's source stencil, if it touches this tile (a CTA-uniform test)
+    int bx = 0, bz = 0;
+    bool src_tile = false;
+    T sw0 = 0, sw1 = 0, sw2 = 0, sw3 = 0;
+    if (a.src_corner) {
+      bx = a.src_corner[2 * s];
+      bz = a.src_corner[2 * s + 1];
+      src_tile = bx + 1 >= x0 && bx < x0 + S::TX && bz + 1 >= z0 && bz < z0 + S::TZ;
+      if (src_tile) {
+        const T wn = a.wavelet[a.n];
+        sw0 = a.src_w[4 * s] * wn; sw1 = a.src_w[4 * s + 1] * wn;
+        sw2 = a.src_w[4 * s + 2] * wn; sw3 = a.src_w[4 * s + 3] * wn;
+      }
+    }
+
+    // sliding window: wv[q] holds tile row (lrow + k + q - R) (own columns only)
+    T wv[2 * R + 1][VZ];
+#pragma unroll
+    for (int q = 0; q < 2 * R; ++q) vload<T, VZ>(P + (lrow + q) * S::SW + S::HL + lane * VZ, wv[q]);
+    T* nx = a.next + (long long)s * g.field;
+#pragma unroll
+    for (int k = 0; k < RX; ++k) {
+      const int prow = lrow + k + R;  // shared row of the output row
+      vload<T, VZ>(P + (prow + R) * S::SW + S::HL + lane * VZ, wv[2 * R]);
+      Row3<T, VZ> rw;
+      vload<T, VZ>(P + prow * S::SW + S::HL + lane * VZ - VZ, rw.l);
+#pragma unroll
+      for (int v = 0; v < VZ; ++v) rw.c[v] = wv[R][v];
+      vload<T, VZ>(P + prow * S::SW + S::HL + lane * VZ + VZ, rw.r);
+      T pp[VZ];
+      vload<T, VZ>(Q + (lrow + k) * S::TZ + lane * VZ, pp);
+      const int x = xr + k;
+      const bool ok = own_cols && x < g.n0;
+      T cc[VZ], ca[VZ], cb[VZ];
+#pragma unroll
+      for (int v = 0; v < VZ; ++v) { cc[v] = T(0); ca[v] = T(1); cb[v] = T(1); }
+      if (ok) vldg<T, VZ>(a.C + cbase + (long long)k * g.s0, cc);
+      if (layer_tile && ok) {
+        vldg<T, VZ>(a.A + cbase + (long long)k * g.s0, ca);
+        if (!a.b_one) vldg<T, VZ>(a.B + cbase + (long long)k * g.s0, cb);
+      }
+      T o[VZ];
+#pragma unroll
+      for (int v = 0; v < VZ; ++v) {
+        const T c = wv[R][v];
+        T lap = wc * c + w1x * (wv[R - 1][v] + wv[R + 1][v]) + w1z * (zval(rw, v - 1) + zval(rw, v + 1));
+        if (R == 2) lap += w2x * (wv[0][v] + wv[4][v]) + w2z * (zval(rw, v - 2) + zval(rw, v + 2));
+        o[v] = (T(2) * c - cb[v] * pp[v]) + cc[v] * lap;
+      }
+      if (src_tile) {
+#pragma unroll
+        for (int v = 0; v < VZ; ++v) {
+          const int dx = x - bx, dz = zc + v - bz;
+          if (dx >= 0 && dx <= 1 && dz >= 0 && dz <= 1)
+            o[v] += (dx == 0) ? (dz == 0 ? sw0 : sw1) : (dz == 0 ? sw2 : sw3);
+        }
+      }
+      if (layer_tile) {
+#pragma unroll
+        for (int v = 0; v < VZ; ++v) o[v] = ca[v] * o[v];
+      }
+      if (ok) store_row<T, VZ>(nx + cbase + (long long)k * g.s0, o, zc, g.n1);
+#pragma unroll
+      for (int q = 0; q < 2 * R; ++q)
+#pragma unroll
+        for (int v = 0; v < VZ; ++v) wv[q][v] = wv[q + 1][v];
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// adjoint step: mu^n = A (R^T g_n + 2 mu1 + Lap(C mu1) - B mu2), grad += mu1 Lap(p^n)
+// ------------------------------------------------------------------------------------------
+template <typename T, int R, int VZ, int RX, bool AB>
+__global__ void __launch_bounds__(256, 2) adj2d_tiled(KGrid<T> g, AdjTiled<T> a) {
+  using S = Tile2Shape<T, VZ, RX, R>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sc = reinterpret_cast<T*>(smem_raw);  // [PS] C with halo
+  T* sm = sc + S::PS;                      // [2][PS] mu^{n+1} with halo
+  T* sn = sm + 2 * S::PS;                  // [2][PS] p^n with halo
+  T* s2 = sn + 2 * S::PS;                  // [2][QS] mu^{n+2}
+  T* sj = s2 + 2 * S::QS;                  // [QS] adjoint source of the current shot
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int z0 = blockIdx.x * S::TZ, x0 = blockIdx.y * S::TX;
+  const int tile = blockIdx.y * a.tt.tiles_z + blockIdx.x;
+  const int sb = blockIdx.z * a.shots_per_cta;
+  const int se = min(sb + a.shots_per_cta, a.n_shots);
+  const int zc = z0 + lane * VZ;
+  const int xr = x0 + warp * RX;
+  const int lrow = warp * RX;
+  const bool own_cols = zc < g.n1;
+  const bool grad = a.p != nullptr;
+
+  const CopyPlan<S::NCH> ph = plan_halo<T, VZ, RX, R>(g, x0, z0);
+  const CopyPlan<S::NCC> pc = plan_core<T, VZ, RX, R>(g, x0, z0);
+  issue(ph, a.C, sc);
+  issue(ph, a.mu1 + (long long)sb * g.field, sm);
+  if (grad) issue(ph, a.p + (long long)sb * g.field, sn);
+  issue(pc, a.mu2 + (long long)sb * g.field, s2);
+  cp_async_commit();
+
+  const int c0 = a.gtr ? a.tt.cell_ptr[tile] : 0, c1 = a.gtr ? a.tt.cell_ptr[tile + 1] : 0;
+  const bool inject = c1 > c0;  // uniform
+  if (inject) {
+    for (int i = threadIdx.x; i < S::QS; i += 256) sj[i] = T(0);
+    __syncthreads();  // zeroing completes before any thread writes a source value
+  }
+
+  const bool layer_tile = AB && (x0 < g.lo0 || x0 + S::TX > g.hi0 || z0 < g.lo1 || z0 + S::TZ > g.hi1);
+  const bool use_a = layer_tile && a.apply_a;
+  const T wc = g.wc, w1x = g.w1a, w1z = g.w1b, w2x = g.w2a, w2z = g.w2b;
+  const long long cbase = g.origin + (long long)xr * g.s0 + zc;
+  // per-cell sum over this CTA's shots: float for float fields, double for double fields
+  using Acc = typename std::conditional<sizeof(T) == 8, double, float>::type;
+  Acc gsum[RX][VZ];
+#pragma unroll
+  for (int k = 0; k < RX; ++k)
+#pragma unroll
+    for (int v = 0; v < VZ; ++v) gsum[k][v] = Acc(0);
+
+  for (int s = sb; s < se; ++s) {
+    const int buf = (s - sb) & 1;
+    if (s + 1 < se) {
+      issue(ph, a.mu1 + (long long)(s + 1) * g.field, sm + (buf ^ 1) * S::PS);
+      if (grad) issue(ph, a.p + (long long)(s + 1) * g.field, sn + (buf ^ 1) * S::PS);
+      issue(pc, a.mu2 + (long long)(s + 1) * g.field, s2 + (buf ^ 1) * S::QS);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    if (inject) {  // adjoint source of shot s: each touched cell summed in table order
+      const T* gs = a.gtr + (long long)s * a.n_rec * a.n_t + a.j;
+      for (int e = c0 + threadIdx.x; e < c1; e += 256) {
+        const int gid = a.tt.cell_gid[e];
+        T acc = T(0);
+        for (int q = a.tt.gcell_ptr[gid]; q < a.tt.gcell_ptr[gid + 1]; ++q)
+          acc += a.gcell_w[q] * gs[(long long)a.tt.gcell_rec[q] * a.n_t];
+        sj[a.tt.cell_local[e]] = acc;
+      }
+    }
+    __syncthreads();
+    const T* M = sm + buf * S::PS;
+    const T* PN = sn + buf * S::PS;
+    const T* M2 = s2 + buf * S::QS;
+
+    T qv[2 * R + 1][VZ];  // C * mu1, own columns
+    T pv[2 * R + 1][VZ];  // p^n, own columns
+#pragma unroll
+    for (int q = 0; q < 2 * R; ++q) {
+      T tm[VZ], tc[VZ];
+      const int off = (lrow + q) * S::SW + S::HL + lane * VZ;
+      vload<T, VZ>(M + off, tm);
+      vload<T, VZ>(sc + off, tc);
+#pragma unroll
+      for (int v = 0; v < VZ; ++v) qv[q][v] = tc[v] * tm[v];
+      if (grad) vload<T, VZ>(PN + off, pv[q]);
+    }
+    T* ob = a.out + (long long)s * g.field;
+#pragma unroll
+    for (int k = 0; k < RX; ++k) {
+      const int prow = lrow + k + R;
+      {
+        T tm[VZ], tc[VZ];
+        const int off = (prow + R) * S::SW + S::HL + lane * VZ;
+        vload<T, VZ>(M + off, tm);
+        vload<T, VZ>(sc + off, tc);
+#pragma unroll
+        for (int v = 0; v < VZ; ++v) qv[2 * R][v] = tc[v] * tm[v];
+        if (grad) vload<T, VZ>(PN + off, pv[2 * R]);
+      }
+      const int coff = prow * S::SW + S::HL + lane * VZ;
+      Row3<T, VZ> qw;
+      T mc[VZ];
+      {
+        T tm[VZ], tc[VZ];
+        vload<T, VZ>(M + coff - VZ, tm);
+        vload<T, VZ>(sc + coff - VZ, tc);
+#pragma unroll
+        for (int v = 0; v < VZ; ++v) qw.l[v] = tc[v] * tm[v];
+        vload<T, VZ>(M + coff + VZ, tm);
+        vload<T, VZ>(sc + coff + VZ, tc);
+#pragma unroll
+        for (int v = 0; v < VZ; ++v) qw.r[v] = tc[v] * tm[v];
+        vload<T, VZ>(M + coff, mc);
+#pragma unroll
+        for (int v = 0; v < VZ; ++v) qw.c[v] = qv[R][v];
+      }
+      Row3<T, VZ> pw;
+      if (grad) {
+        vload<T, VZ>(PN + coff - VZ, pw.l);
+        vload<T, VZ>(PN + coff + VZ, pw.r);
+#pragma unroll
+        for (int v = 0; v < VZ; ++v) pw.c[v] = pv[R][v];
+      }
+      T m2[VZ];
+      vload<T, VZ>(M2 + (lrow + k) * S::TZ + lane * VZ, m2);
+      const int x = xr + k;
+      const bool ok = own_cols && x < g.n0;
+      T ca[VZ], cb[VZ];
+#pragma unroll
+      for (int v = 0; v < VZ; ++v) { ca[v] = T(1); cb[v] = T(1); }
+      if (layer_tile && ok) {
+        vldg<T, VZ>(a.A + cbase + (long long)k * g.s0, ca);
+        vldg<T, VZ>(a.B + cbase + (long long)k * g.s0, cb);
+      }
+      T o[VZ];
+#pragma unroll
+      for (int v = 0; v < VZ; ++v) {
+        T lq = wc * qv[R][v] + w1x * (qv[R - 1][v] + qv[R + 1][v]) + w1z * (zval(qw, v - 1) + zval(qw, v + 1));
+        if (R == 2) lq += w2x * (qv[0][v] + qv[4][v]) + w2z * (zval(qw, v - 2) + zval(qw, v + 2));
+        o[v] = (T(2) * mc[v] + lq) - cb[v] * m2[v];
+      }
+      if (inject) {
+        T inj[VZ];
+        vload<T, VZ>(sj + (lrow + k) * S::TZ + lane * VZ, inj);
+#pragma unroll
+        for (int v = 0; v < VZ; ++v) o[v] = inj[v] + o[v];
+      }
+      if (use_a) {
+#pragma unroll
+        for (int v = 0; v < VZ; ++v) o[v] = ca[v] * o[v];
+      }
+      if (grad) {
+#pragma unroll
+        for (int v = 0; v < VZ; ++v) {
+          T lp = wc * pv[R][v] + w1x * (pv[R - 1][v] + pv[R + 1][v]) + w1z * (zval(pw, v - 1) + zval(pw, v + 1));
+          if (R == 2) lp += w2x * (pv[0][v] + pv[4][v]) + w2z * (zval(pw, v - 2) + zval(pw, v + 2));
+          gsum[k][v] += (Acc)(mc[v] * lp);
+        }
+      }
+      if (ok) store_row<T, VZ>(ob + cbase + (long long)k * g.s0, o, zc, g.n1);
+#pragma unroll
+      for (int q = 0; q < 2 * R; ++q)
+#pragma unroll
+        for (int v = 0; v < VZ; ++v) {
+          qv[q][v] = qv[q + 1][v];
+          if (grad) pv[q][v] = pv[q + 1][v];
+        }
+    }
+    __syncthreads();
+    if (inject)  // the same threads clear the cells they set, before the next shot sets them again
+      for (int e = c0 + threadIdx.x; e < c1; e += 256) sj[a.tt.cell_local[e]] = T(0);
+  }
+  if (grad && own_cols) {
+    double* gp = a.gacc + (long long)blockIdx.z * g.field;
+#pragma unroll
+    for (int k = 0; k < RX; ++k) {
+      if (xr + k >= g.n0) continue;
+      double* dst = gp + cbase + (long long)k * g.s0;
+#pragma unroll
+      for (int v = 0; v < VZ; ++v)
+        if (zc + v < g.n1) dst[v] += (double)gsum[k][v];
+    }
+  }
+}
+
+}  // namespace nw

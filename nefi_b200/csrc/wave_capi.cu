@@ -14,6 +14,7 @@
 #include "../../include/nefi_wave.h"
 #include "aux_kernels.cuh"
 #include "kernels.cuh"
+#include "stencil2d.cuh"
 
 namespace {
 
@@ -51,6 +52,7 @@ int check_grid(const nw_grid* g) {
     return fail(NW_ERR_UNSUPPORTED, "absorbing kind not built");
   for (int a = 0; a < g->ndim; ++a)
     if (g->n[a] < 2) return fail(NW_ERR_ARG, "every padded extent must be >= 2");
+  if (g->field_elems >= (1LL << 31)) return fail(NW_ERR_ARG, "a field must hold fewer than 2^31 elements");
   if (g->field_elems <= 0 || g->radius != g->order / 2)
     return fail(NW_ERR_ARG, "grid layout not initialised (call nw_grid_layout)");
   return NW_OK;
@@ -82,7 +84,8 @@ nw::PadMap padmap(const nw_grid* g, const int32_t* n_abs) {
   return p;
 }
 
-constexpr int kRX = 4;  // rows (2-D) or planes (3-D) per thread
+constexpr int kRX = 4;     // rows (2-D) or planes (3-D) per thread
+constexpr int kGuard = 32; // zero elements in front of every field (see nw_grid.guard)
 
 // Launch shape of the stencil kernels: 32 x 8 threads, each owning kRX cells along axis 0.
 struct Shape {
@@ -98,42 +101,6 @@ Shape stencil_shape(const nw_grid* g, int n_shots) {
     s.grid = dim3(zt * yt, (g->n[0] + kRX - 1) / kRX, n_shots);
   }
   return s;
-}
-
-template <typename T>
-int launch_fwd(const nw_grid* g, const nw::KGrid<T>& kg, const nw::FwdStep<T>& st, int n_shots,
-               bool ab, cudaStream_t s) {
-  Shape sh = stencil_shape(g, n_shots);
-  const int r = g->radius;
-#define NW_FWD(D, R, AB) nw::fwd##D##d<T, R, AB, kRX><<<sh.grid, sh.block, 0, s>>>(kg, st)
-  if (g->ndim == 2) {
-    if (r == 1) { if (ab) NW_FWD(2, 1, true); else NW_FWD(2, 1, false); }
-    else        { if (ab) NW_FWD(2, 2, true); else NW_FWD(2, 2, false); }
-  } else {
-    if (r == 1) { if (ab) NW_FWD(3, 1, true); else NW_FWD(3, 1, false); }
-    else        { if (ab) NW_FWD(3, 2, true); else NW_FWD(3, 2, false); }
-  }
-#undef NW_FWD
-  NW_LAUNCHED();
-  return NW_OK;
-}
-
-template <typename T>
-int launch_adj(const nw_grid* g, const nw::KGrid<T>& kg, const nw::AdjStep<T>& st, int n_shots,
-               bool ab, cudaStream_t s) {
-  Shape sh = stencil_shape(g, n_shots);
-  const int r = g->radius;
-#define NW_ADJ(D, R, AB) nw::adj##D##d<T, R, AB, kRX><<<sh.grid, sh.block, 0, s>>>(kg, st)
-  if (g->ndim == 2) {
-    if (r == 1) { if (ab) NW_ADJ(2, 1, true); else NW_ADJ(2, 1, false); }
-    else        { if (ab) NW_ADJ(2, 2, true); else NW_ADJ(2, 2, false); }
-  } else {
-    if (r == 1) { if (ab) NW_ADJ(3, 1, true); else NW_ADJ(3, 1, false); }
-    else        { if (ab) NW_ADJ(3, 2, true); else NW_ADJ(3, 2, false); }
-  }
-#undef NW_ADJ
-  NW_LAUNCHED();
-  return NW_OK;
 }
 
 template <typename T>
@@ -172,63 +139,180 @@ SnapLayout snap_layout(const nw_grid* g, int n_shots) {
   return L;
 }
 
-// Encodes levels (lm1, l0) (each n_shots fields, contiguous) into snapshot j.
-template <typename T>
-int snap_store(const nw_grid* g, const nw_storage* st, int n_shots, const T* lm1, const T* l0, int j,
-               cudaStream_t s) {
-  SnapLayout L = snap_layout(g, n_shots);
-  char* base = (char*)st->snap + (size_t)j * L.per_snap(st->snap_kind);
-  const size_t lvl_bytes = (size_t)n_shots * g->field_elems * sizeof(T);
-  if (st->snap_kind == NW_SNAP_EXACT) {
-    NW_CUDA(cudaMemcpyAsync(base, lm1, lvl_bytes, cudaMemcpyDeviceToDevice, s));
-    NW_CUDA(cudaMemcpyAsync(base + lvl_bytes, l0, lvl_bytes, cudaMemcpyDeviceToDevice, s));
-    return NW_OK;
-  }
+// Encodes levels (lm1, l0) (each n_shots fields, contiguous) into snapshot j. The 16-bit kinds
+// store p^{n0} and the difference p^{n0} - p^{n0-1}, each block-scaled, so the small level
+// difference (the discrete time derivative) keeps 16-bit relative precision.
+template <typename T, int K>
+int snap_codec(const nw_grid* g, const SnapLayout& L, int n_shots, char* base, const T* lm1, T* lm1_out,
+               const T* l0, T* l0_out, bool encode, cudaStream_t s) {
+  using H = typename nw::Codec<K>::H;
   float* scales = (float*)(base + L.vals_bytes);
   const size_t half_fields = (size_t)n_shots * L.nblk * nw::SNAP_BLOCK;
-  dim3 grid(L.nblk, n_shots);
-  for (int lv = 0; lv < 2; ++lv) {
-    const T* src = lv == 0 ? lm1 : l0;
+  dim3 grid((L.nblk + 7) / 8, n_shots);
+  for (int lv = 0; lv < 2; ++lv) {  // slot 0: p^{n0}; slot 1: p^{n0} - p^{n0-1}
+    H* v = (H*)base + lv * half_fields;
     float* sc = scales + (size_t)lv * n_shots * L.nblk;
-    if (st->snap_kind == NW_SNAP_F16) {
-      __half* v = (__half*)base + lv * half_fields;
-      nw::snap_encode<T, __half><<<grid, 256, 0, s>>>(src, g->field_elems, L.nblk, v, sc);
-    } else {
-      __nv_bfloat16* v = (__nv_bfloat16*)base + lv * half_fields;
-      nw::snap_encode<T, __nv_bfloat16><<<grid, 256, 0, s>>>(src, g->field_elems, L.nblk, v, sc);
-    }
+    if (encode)
+      nw::snap_encode<T, K><<<grid, 256, 0, s>>>(l0, lv == 0 ? nullptr : lm1, g->field_elems, L.nblk, v, sc);
+    else  // p^{n0} first, then p^{n0-1} = p^{n0} - difference
+      nw::snap_decode<T, K><<<grid, 256, 0, s>>>(v, sc, L.nblk, g->field_elems, lv == 0 ? nullptr : l0_out,
+                                                 lv == 0 ? l0_out : lm1_out);
     NW_LAUNCHED();
   }
   return NW_OK;
 }
 
 template <typename T>
+int snap_store(const nw_grid* g, const nw_storage* st, int n_shots, const T* lm1, const T* l0, int j,
+               cudaStream_t s) {
+  SnapLayout L = snap_layout(g, n_shots);
+  char* base = (char*)st->snap + (size_t)j * L.per_snap(st->snap_kind);
+  const size_t lvl_bytes = (size_t)n_shots * g->field_elems * sizeof(T);
+  switch (st->snap_kind) {
+    case NW_SNAP_EXACT:
+      NW_CUDA(cudaMemcpyAsync(base, lm1, lvl_bytes, cudaMemcpyDeviceToDevice, s));
+      NW_CUDA(cudaMemcpyAsync(base + lvl_bytes, l0, lvl_bytes, cudaMemcpyDeviceToDevice, s));
+      return NW_OK;
+    case NW_SNAP_F16: return snap_codec<T, nw::CODEC_F16>(g, L, n_shots, base, lm1, nullptr, l0, nullptr, true, s);
+    case NW_SNAP_BF16: return snap_codec<T, nw::CODEC_BF16>(g, L, n_shots, base, lm1, nullptr, l0, nullptr, true, s);
+    case NW_SNAP_I16: return snap_codec<T, nw::CODEC_I16>(g, L, n_shots, base, lm1, nullptr, l0, nullptr, true, s);
+  }
+  return fail(NW_ERR_ARG, "unknown snapshot kind");
+}
+
+template <typename T>
 int snap_load(const nw_grid* g, const nw_storage* st, int n_shots, int j, T* lm1, T* l0,
               cudaStream_t s) {
   SnapLayout L = snap_layout(g, n_shots);
-  const char* base = (const char*)st->snap + (size_t)j * L.per_snap(st->snap_kind);
+  char* base = (char*)st->snap + (size_t)j * L.per_snap(st->snap_kind);
   const size_t lvl_bytes = (size_t)n_shots * g->field_elems * sizeof(T);
-  if (st->snap_kind == NW_SNAP_EXACT) {
-    NW_CUDA(cudaMemcpyAsync(lm1, base, lvl_bytes, cudaMemcpyDeviceToDevice, s));
-    NW_CUDA(cudaMemcpyAsync(l0, base + lvl_bytes, lvl_bytes, cudaMemcpyDeviceToDevice, s));
-    return NW_OK;
+  switch (st->snap_kind) {
+    case NW_SNAP_EXACT:
+      NW_CUDA(cudaMemcpyAsync(lm1, base, lvl_bytes, cudaMemcpyDeviceToDevice, s));
+      NW_CUDA(cudaMemcpyAsync(l0, base + lvl_bytes, lvl_bytes, cudaMemcpyDeviceToDevice, s));
+      return NW_OK;
+    case NW_SNAP_F16: return snap_codec<T, nw::CODEC_F16>(g, L, n_shots, base, nullptr, lm1, nullptr, l0, false, s);
+    case NW_SNAP_BF16: return snap_codec<T, nw::CODEC_BF16>(g, L, n_shots, base, nullptr, lm1, nullptr, l0, false, s);
+    case NW_SNAP_I16: return snap_codec<T, nw::CODEC_I16>(g, L, n_shots, base, nullptr, lm1, nullptr, l0, false, s);
   }
-  const float* scales = (const float*)(base + L.vals_bytes);
-  const size_t half_fields = (size_t)n_shots * L.nblk * nw::SNAP_BLOCK;
-  dim3 grid(L.nblk, n_shots);
-  for (int lv = 0; lv < 2; ++lv) {
-    T* dst = lv == 0 ? lm1 : l0;
-    const float* sc = scales + (size_t)lv * n_shots * L.nblk;
-    if (st->snap_kind == NW_SNAP_F16)
-      nw::snap_decode<T, __half><<<grid, 256, 0, s>>>((const __half*)base + lv * half_fields, sc,
-                                                      L.nblk, g->field_elems, dst);
-    else
-      nw::snap_decode<T, __nv_bfloat16><<<grid, 256, 0, s>>>(
-          (const __nv_bfloat16*)base + lv * half_fields, sc, L.nblk, g->field_elems, dst);
-    NW_LAUNCHED();
-  }
+  return fail(NW_ERR_ARG, "unknown snapshot kind");
+}
+
+// ---- launch shapes ------------------------------------------------------------------------
+struct Tune {
+  int vz, rx, spc, adj_spc;
+};
+
+int resolve_tune(const nw_grid* g, const nw_tuning* t, Tune* out) {
+  Tune r;
+  // defaults: the best combined forward + adjoint time of a sweep on a 552^2 x 16-shot grid
+  r.vz = (t && t->vz) ? t->vz : 2;
+  r.rx = (t && t->rx) ? t->rx : 4;
+  r.spc = (t && t->shots_per_cta) ? t->shots_per_cta : 2;
+  r.adj_spc = (t && t->adj_shots_per_cta) ? t->adj_shots_per_cta : 4;
+  if (g->ndim == 3) r.spc = r.adj_spc = 1;
+  if (g->dtype == NW_F32 && r.vz != 2 && r.vz != 4) return fail(NW_ERR_ARG, "tuning.vz must be 2 or 4 for float32");
+  if (g->dtype == NW_F64 && r.vz != 2) return fail(NW_ERR_ARG, "tuning.vz must be 2 for float64");
+  if (r.rx != 2 && r.rx != 4 && r.rx != 8) return fail(NW_ERR_ARG, "tuning.rx must be 2, 4 or 8");
+  if (r.spc < 1 || r.adj_spc < 1) return fail(NW_ERR_ARG, "tuning shots per CTA must be >= 1");
+  *out = r;
   return NW_OK;
 }
+
+int n_groups(const nw_grid* g, const Tune& t, int n_shots) {
+  return g->ndim == 3 ? n_shots : (n_shots + t.adj_spc - 1) / t.adj_spc;
+}
+
+template <typename T, int R, int VZ, int RX>
+constexpr size_t fwd2_smem() {
+  using S = nw::Tile2Shape<T, VZ, RX, R>;
+  return (2 * S::PS + 2 * S::QS) * sizeof(T);
+}
+template <typename T, int R, int VZ, int RX>
+constexpr size_t adj2_smem() {
+  using S = nw::Tile2Shape<T, VZ, RX, R>;
+  return (5 * S::PS + 3 * S::QS) * sizeof(T);
+}
+constexpr size_t kMaxSmem = 227 * 1024;  // opt-in shared memory per CTA on sm_100a
+
+// Opt a kernel into more than 48 KB of dynamic shared memory (once per instantiation).
+template <typename K>
+int allow_smem(K kernel, size_t bytes, bool* done) {
+  if (*done || bytes <= 48 * 1024) return NW_OK;
+  NW_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  *done = true;
+  return NW_OK;
+}
+
+nw::TileTables tile_tables(const nw_acquisition* a) {
+  nw::TileTables tt;
+  tt.tiles_z = a->tiles_z;
+  tt.rec_ptr = a->tile_rec_ptr;
+  tt.rec_list = a->tile_rec_list;
+  tt.rec_corner = a->rec_corner;
+  tt.cell_ptr = a->tile_cell_ptr;
+  tt.cell_local = a->tile_cell_local;
+  tt.cell_gid = a->tile_cell_gid;
+  tt.gcell_ptr = a->cell_ptr;
+  tt.gcell_rec = a->cell_rec;
+  return tt;
+}
+
+template <typename T, int R, int VZ, int RX, bool AB>
+int launch_fwd2_v(const nw_grid* g, const nw::KGrid<T>& kg, const nw::FwdTiled<T>& st, const Tune& t,
+                  cudaStream_t s) {
+  using S = nw::Tile2Shape<T, VZ, RX, R>;
+  constexpr size_t smem = fwd2_smem<T, R, VZ, RX>();
+  if (smem > kMaxSmem) return fail(NW_ERR_ARG, "tile too large for shared memory (lower tuning.rx)");
+  static bool done = false;
+  int rc = allow_smem(nw::fwd2d_tiled<T, R, VZ, RX, AB>, smem, &done);
+  if (rc) return rc;
+  dim3 grid((g->n[1] + S::TZ - 1) / S::TZ, (g->n[0] + S::TX - 1) / S::TX, (st.n_shots + t.spc - 1) / t.spc);
+  nw::fwd2d_tiled<T, R, VZ, RX, AB><<<grid, 256, smem, s>>>(kg, st);
+  NW_LAUNCHED();
+  return NW_OK;
+}
+template <typename T, int R, int VZ, int RX, bool AB>
+int launch_adj2_v(const nw_grid* g, const nw::KGrid<T>& kg, const nw::AdjTiled<T>& st, const Tune& t,
+                  cudaStream_t s) {
+  using S = nw::Tile2Shape<T, VZ, RX, R>;
+  constexpr size_t smem = adj2_smem<T, R, VZ, RX>();
+  if (smem > kMaxSmem) return fail(NW_ERR_ARG, "tile too large for shared memory (lower tuning.rx)");
+  static bool done = false;
+  int rc = allow_smem(nw::adj2d_tiled<T, R, VZ, RX, AB>, smem, &done);
+  if (rc) return rc;
+  dim3 grid((g->n[1] + S::TZ - 1) / S::TZ, (g->n[0] + S::TX - 1) / S::TX, (st.n_shots + t.adj_spc - 1) / t.adj_spc);
+  nw::adj2d_tiled<T, R, VZ, RX, AB><<<grid, 256, smem, s>>>(kg, st);
+  NW_LAUNCHED();
+  return NW_OK;
+}
+
+// Runtime (radius, vz, rx, absorbing) -> template instantiation.
+#define NW_DISPATCH2(FN, T, TU, ...)                                                                   \
+  [&]() -> int {                                                                                   \
+    const int r_ = g->radius;                                                                      \
+    const bool ab_ = m->coef_a != nullptr;                                                         \
+    if constexpr (sizeof(T) == 4) {                                                                \
+      if (TU.vz == 4) {                                                                             \
+        if (r_ == 2) {                                                                             \
+          if (TU.rx == 2) return ab_ ? FN<T, 2, 4, 2, true>(__VA_ARGS__) : FN<T, 2, 4, 2, false>(__VA_ARGS__); \
+          if (TU.rx == 4) return ab_ ? FN<T, 2, 4, 4, true>(__VA_ARGS__) : FN<T, 2, 4, 4, false>(__VA_ARGS__); \
+          return ab_ ? FN<T, 2, 4, 8, true>(__VA_ARGS__) : FN<T, 2, 4, 8, false>(__VA_ARGS__);     \
+        }                                                                                          \
+        if (TU.rx == 2) return ab_ ? FN<T, 1, 4, 2, true>(__VA_ARGS__) : FN<T, 1, 4, 2, false>(__VA_ARGS__); \
+        if (TU.rx == 4) return ab_ ? FN<T, 1, 4, 4, true>(__VA_ARGS__) : FN<T, 1, 4, 4, false>(__VA_ARGS__); \
+        return ab_ ? FN<T, 1, 4, 8, true>(__VA_ARGS__) : FN<T, 1, 4, 8, false>(__VA_ARGS__);       \
+      }                                                                                            \
+    }                                                                                              \
+    if (r_ == 2) {                                                                                 \
+      if (TU.rx == 2) return ab_ ? FN<T, 2, 2, 2, true>(__VA_ARGS__) : FN<T, 2, 2, 2, false>(__VA_ARGS__); \
+      if (TU.rx == 4) return ab_ ? FN<T, 2, 2, 4, true>(__VA_ARGS__) : FN<T, 2, 2, 4, false>(__VA_ARGS__); \
+      return ab_ ? FN<T, 2, 2, 8, true>(__VA_ARGS__) : FN<T, 2, 2, 8, false>(__VA_ARGS__);         \
+    }                                                                                              \
+    if (TU.rx == 2) return ab_ ? FN<T, 1, 2, 2, true>(__VA_ARGS__) : FN<T, 1, 2, 2, false>(__VA_ARGS__); \
+    if (TU.rx == 4) return ab_ ? FN<T, 1, 2, 4, true>(__VA_ARGS__) : FN<T, 1, 2, 4, false>(__VA_ARGS__); \
+    return ab_ ? FN<T, 1, 2, 8, true>(__VA_ARGS__) : FN<T, 1, 2, 8, false>(__VA_ARGS__);           \
+  }()
 
 // ---- forward driver ---------------------------------------------------------------------
 template <typename T>
@@ -244,9 +328,34 @@ struct Levels {  // address of time level n (n >= -1) in history, ring or segmen
   }
 };
 
+// One forward step n for all shots (traces != NULL: also sample level n if it is a record step).
 template <typename T>
-nw::FwdStep<T> fwd_step_args(const nw_grid* g, const nw_medium* m, const nw_acquisition* a,
-                             const nw_time* t, const Levels<T>& L, int n, T* traces) {
+int forward_step(const nw_grid* g, const nw::KGrid<T>& kg, const nw_medium* m, const nw_acquisition* a,
+                 const nw_time* t, const Tune& tu, const Levels<T>& L, int n, T* traces, cudaStream_t s) {
+  const bool rec = traces && a->n_rec > 0 && (n % t->substeps) == 0;
+  if (g->ndim == 2) {
+    nw::FwdTiled<T> st;
+    st.prev = L.at(n - 1);
+    st.cur = L.at(n);
+    st.next = L.at(n + 1);
+    st.C = (const T*)m->c2dt2;
+    st.A = (const T*)m->coef_a;
+    st.B = (const T*)m->coef_b;
+    st.b_one = (n == 0 && t->first_b_one) ? 1 : 0;
+    st.src_corner = a->has_source ? a->src_corner : nullptr;
+    st.src_w = (const T*)a->src_weight;
+    st.wavelet = (const T*)a->wavelet;
+    st.n = n;
+    st.n_shots = a->n_shots;
+    st.shots_per_cta = tu.spc;
+    st.traces = rec ? traces : nullptr;
+    st.rec_w = (const T*)a->rec_weight;
+    st.n_rec = a->n_rec;
+    st.n_t = t->n_t;
+    st.j = n / t->substeps;
+    st.tt = tile_tables(a);
+    return NW_DISPATCH2(launch_fwd2_v, T, tu, g, kg, st, tu, s);
+  }
   nw::FwdStep<T> st;
   st.prev = L.at(n - 1);
   st.cur = L.at(n);
@@ -259,19 +368,28 @@ nw::FwdStep<T> fwd_step_args(const nw_grid* g, const nw_medium* m, const nw_acqu
   st.src_w = (const T*)a->src_weight;
   st.wavelet = (const T*)a->wavelet;
   st.n = n;
-  const bool rec = traces && a->n_rec > 0 && (n % t->substeps) == 0;
   st.traces = rec ? traces : nullptr;
   st.rec_idx = a->rec_index;
   st.rec_w = (const T*)a->rec_weight;
   st.n_rec = a->n_rec;
   st.n_t = t->n_t;
   st.j = n / t->substeps;
-  return st;
+  Shape sh = stencil_shape(g, a->n_shots);
+  const bool ab = m->coef_a != nullptr;
+  if (g->radius == 1) {
+    if (ab) nw::fwd3d<T, 1, true, kRX><<<sh.grid, sh.block, 0, s>>>(kg, st);
+    else nw::fwd3d<T, 1, false, kRX><<<sh.grid, sh.block, 0, s>>>(kg, st);
+  } else {
+    if (ab) nw::fwd3d<T, 2, true, kRX><<<sh.grid, sh.block, 0, s>>>(kg, st);
+    else nw::fwd3d<T, 2, false, kRX><<<sh.grid, sh.block, 0, s>>>(kg, st);
+  }
+  NW_LAUNCHED();
+  return NW_OK;
 }
 
 template <typename T>
 int forward_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, const nw_time* t,
-                 const nw_storage* st, int n_begin, int n_end, T* traces, cudaStream_t s) {
+                 const nw_storage* st, const Tune& tu, int n_begin, int n_end, T* traces, cudaStream_t s) {
   const long long LE = (long long)a->n_shots * g->field_elems;
   Levels<T> L;
   L.level_elems = LE;
@@ -282,13 +400,12 @@ int forward_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
   const bool ckpt = !st->history && st->snap;
   if (ckpt && st->segment < 1) return fail(NW_ERR_ARG, "segment must be >= 1");
   const nw::KGrid<T> kg = kgrid<T>(g);
-  const bool ab = m->coef_a != nullptr;
   for (int n = n_begin; n < n_end; ++n) {
     if (ckpt && n % st->segment == 0) {
       int rc = snap_store<T>(g, st, a->n_shots, L.at(n - 1), L.at(n), n / st->segment, s);
       if (rc) return rc;
     }
-    int rc = launch_fwd<T>(g, kg, fwd_step_args<T>(g, m, a, t, L, n, traces), a->n_shots, ab, s);
+    int rc = forward_step<T>(g, kg, m, a, t, tu, L, n, traces, s);
     if (rc) return rc;
   }
   if (traces && n_end == t->n_steps && t->n_steps % t->substeps == 0) {
@@ -301,15 +418,15 @@ int forward_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
 // ---- adjoint driver ---------------------------------------------------------------------
 template <typename T>
 int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, const nw_time* t,
-                 const nw_storage* st, const T* gtr, T* work, T* grad, T* lambda0, T* mu1,
-                 cudaStream_t s) {
+                 const nw_storage* st, const Tune& tu, const T* gtr, T* work, double* gacc, T* lambda0,
+                 T* mu1, cudaStream_t s) {
   const int N = t->n_steps, M = t->substeps, S = a->n_shots;
   const long long LE = (long long)S * g->field_elems;
   const size_t lvl_bytes = (size_t)LE * sizeof(T);
   const nw::KGrid<T> kg = kgrid<T>(g);
   const bool ab = m->coef_a != nullptr;
   NW_CUDA(cudaMemsetAsync(work, 0, 3 * lvl_bytes, s));
-  NW_CUDA(cudaMemsetAsync(grad, 0, lvl_bytes, s));
+  NW_CUDA(cudaMemsetAsync(gacc, 0, (size_t)n_groups(g, tu, S) * g->field_elems * sizeof(double), s));
   auto mu = [&](int n) { return work + (long long)(n % 3) * LE; };
   const bool hist = st->history != nullptr;
   const bool ckpt = !hist && st->snap != nullptr;
@@ -327,7 +444,7 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
   SEG.n0 = -1;
   const int n_stop = lambda0 ? 0 : 1;
   dim3 ig(((a->n_cells > 0 ? a->n_cells : 1) + 127) / 128, S);
-  auto inject = [&](int n) -> int {
+  auto inject3 = [&](int n) -> int {  // 3-D: separate adjoint-source kernel
     if (a->n_cells <= 0 || n % M != 0) return NW_OK;
     nw::inject_kernel<T><<<ig, 128, 0, s>>>(mu(n), g->field_elems, (const T*)m->coef_a, n >= 1 ? 1 : 0,
                                             gtr, a->n_rec, t->n_t, n / M, a->n_cells, a->cell_index,
@@ -335,9 +452,29 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
     NW_LAUNCHED();
     return NW_OK;
   };
-  // level N: mu^N = A R^T g_N (the buffers start at zero)
-  if (N >= n_stop) {
-    int rc = inject(N);
+  auto step2 = [&](int n, const T* pn) -> int {  // 2-D: one fused tiled launch
+    nw::AdjTiled<T> as;
+    as.mu1 = mu(n + 1);
+    as.mu2 = mu(n + 2);
+    as.out = mu(n);
+    as.C = (const T*)m->c2dt2;
+    as.A = (const T*)m->coef_a;
+    as.B = (const T*)m->coef_b;
+    as.apply_a = n >= 1 ? 1 : 0;
+    as.p = pn;
+    as.gacc = gacc;
+    as.n_shots = S;
+    as.shots_per_cta = tu.adj_spc;
+    as.gtr = (a->n_cells > 0 && n % M == 0) ? gtr : nullptr;
+    as.gcell_w = (const T*)a->cell_weight;
+    as.n_rec = a->n_rec;
+    as.n_t = t->n_t;
+    as.j = n / M;
+    as.tt = tile_tables(a);
+    return NW_DISPATCH2(launch_adj2_v, T, tu, g, kg, as, tu, s);
+  };
+  if (N >= n_stop) {  // level N: mu^N = A R^T g_N (mu^{N+1} = mu^{N+2} = 0)
+    int rc = g->ndim == 2 ? step2(N, nullptr) : inject3(N);
     if (rc) return rc;
   }
   for (int n = N - 1; n >= n_stop; --n) {
@@ -352,11 +489,16 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
         int rc = snap_load<T>(g, st, S, n0 / K, SEG.at(n0 - 1), SEG.at(n0), s);
         if (rc) return rc;
         for (int k = n0; k < n1 - 1; ++k) {
-          rc = launch_fwd<T>(g, kg, fwd_step_args<T>(g, m, a, t, SEG, k, nullptr), S, ab, s);
+          rc = forward_step<T>(g, kg, m, a, t, tu, SEG, k, nullptr, s);
           if (rc) return rc;
         }
       }
       pn = SEG.at(n);
+    }
+    if (g->ndim == 2) {
+      int rc = step2(n, pn);
+      if (rc) return rc;
+      continue;
     }
     nw::AdjStep<T> as;
     as.mu1 = mu(n + 1);
@@ -367,19 +509,24 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
     as.B = (const T*)m->coef_b;
     as.apply_a = n >= 1 ? 1 : 0;
     as.p = pn;
-    as.grad = grad;
-    int rc = launch_adj<T>(g, kg, as, S, ab, s);
-    if (rc) return rc;
-    rc = inject(n);
+    as.grad = gacc;
+    Shape sh = stencil_shape(g, S);
+    if (g->radius == 1) {
+      if (ab) nw::adj3d<T, 1, true, kRX><<<sh.grid, sh.block, 0, s>>>(kg, as);
+      else nw::adj3d<T, 1, false, kRX><<<sh.grid, sh.block, 0, s>>>(kg, as);
+    } else {
+      if (ab) nw::adj3d<T, 2, true, kRX><<<sh.grid, sh.block, 0, s>>>(kg, as);
+      else nw::adj3d<T, 2, false, kRX><<<sh.grid, sh.block, 0, s>>>(kg, as);
+    }
+    NW_LAUNCHED();
+    int rc = inject3(n);
     if (rc) return rc;
   }
   if (lambda0) {
-    if (N == 0) {  // no step: lambda^0 = R^T g_0, mu^1 = 0
-      NW_CUDA(cudaMemcpyAsync(lambda0, mu(0), lvl_bytes, cudaMemcpyDeviceToDevice, s));
-      if (mu1) NW_CUDA(cudaMemsetAsync(mu1, 0, lvl_bytes, s));
-    } else {
-      NW_CUDA(cudaMemcpyAsync(lambda0, mu(0), lvl_bytes, cudaMemcpyDeviceToDevice, s));
-      if (mu1) NW_CUDA(cudaMemcpyAsync(mu1, mu(1), lvl_bytes, cudaMemcpyDeviceToDevice, s));
+    NW_CUDA(cudaMemcpyAsync(lambda0, mu(0), lvl_bytes, cudaMemcpyDeviceToDevice, s));
+    if (mu1) {
+      if (N == 0) NW_CUDA(cudaMemsetAsync(mu1, 0, lvl_bytes, s));
+      else NW_CUDA(cudaMemcpyAsync(mu1, mu(1), lvl_bytes, cudaMemcpyDeviceToDevice, s));
     }
   }
   return NW_OK;
@@ -405,21 +552,22 @@ int nw_grid_layout(nw_grid* g) {
   if (g->order != 2 && g->order != 4) return fail(NW_ERR_ARG, "order must be 2 or 4");
   const int r = g->order / 2;
   g->radius = r;
+  g->guard = kGuard;
   const int last = g->ndim - 1;
   const long long ld = ((long long)g->n[last] + r + 31) / 32 * 32;
   if (g->ndim == 2) {
     g->stride[0] = ld;
     g->stride[1] = 1;
     g->stride[2] = 0;
-    g->origin = (long long)r * ld;
-    g->field_elems = ((long long)g->n[0] + 2 * r) * ld;
+    g->origin = kGuard + (long long)r * ld;
+    g->field_elems = kGuard + ((long long)g->n[0] + 2 * r) * ld;
   } else {
     const long long rows = (long long)g->n[1] + r;
     g->stride[0] = rows * ld;
     g->stride[1] = ld;
     g->stride[2] = 1;
-    g->origin = (long long)r * rows * ld;
-    g->field_elems = ((long long)g->n[0] + 2 * r) * rows * ld;
+    g->origin = kGuard + (long long)r * rows * ld;
+    g->field_elems = kGuard + ((long long)g->n[0] + 2 * r) * rows * ld;
   }
   return NW_OK;
 }
@@ -490,7 +638,7 @@ int nw_initial_state(const nw_grid* g, const int32_t* n_abs, const nw_medium* m,
 }
 
 static int check_run(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, const nw_time* t,
-                     const nw_storage* st) {
+                     const nw_storage* st, const Tune& tu) {
   int rc = check_grid(g);
   if (rc) return rc;
   if (!m || !a || !t || !st) return fail(NW_ERR_ARG, "NULL descriptor");
@@ -504,52 +652,93 @@ static int check_run(const nw_grid* g, const nw_medium* m, const nw_acquisition*
   if (a->n_rec > 0 && (!a->rec_index || !a->rec_weight)) return fail(NW_ERR_ARG, "receiver arrays are NULL");
   if (t->substeps < 1 || t->n_t < 1 || t->n_steps != (t->n_t - 1) * t->substeps)
     return fail(NW_ERR_ARG, "inconsistent time axis");
+  if (g->ndim == 2) {
+    const int tx = 8 * tu.rx, tz = 32 * tu.vz;
+    if (a->tile_rows != tx || a->tile_cols != tz)
+      return fail(NW_ERR_ARG, "per-tile tables were built for another tile shape (see nw_tile_shape)");
+    if (a->tiles_z != (g->n[1] + tz - 1) / tz || !a->tile_rec_ptr || !a->tile_cell_ptr || !a->rec_corner ||
+        (a->n_cells > 0 && (!a->tile_cell_local || !a->tile_cell_gid)) || (a->n_rec > 0 && !a->tile_rec_list))
+      return fail(NW_ERR_ARG, "2-D grids need the per-tile receiver tables");
+  }
   return NW_OK;
 }
 
+int nw_tile_shape(const nw_grid* g, nw_tuning* t, int32_t* tx, int32_t* tz) {
+  int rc = check_grid(g);
+  if (rc) return rc;
+  Tune tu;
+  rc = resolve_tune(g, t, &tu);
+  if (rc) return rc;
+  if (t) {
+    t->vz = tu.vz;
+    t->rx = tu.rx;
+    t->shots_per_cta = tu.spc;
+    t->adj_shots_per_cta = tu.adj_spc;
+  }
+  if (tx) *tx = 8 * tu.rx;
+  if (tz) *tz = 32 * tu.vz;
+  return NW_OK;
+}
+
+int nw_adjoint_groups(const nw_grid* g, const nw_tuning* t, int32_t n_shots) {
+  Tune tu;
+  if (check_grid(g) || resolve_tune(g, t, &tu) || n_shots < 1) return -1;
+  return n_groups(g, tu, n_shots);
+}
+
 int nw_forward(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, const nw_time* t,
-               const nw_storage* st, int32_t n_begin, int32_t n_end, void* traces, void* stream) {
-  int rc = check_run(g, m, a, t, st);
+               const nw_storage* st, const nw_tuning* tune, int32_t n_begin, int32_t n_end, void* traces,
+               void* stream) {
+  int rc = check_grid(g);
+  if (rc) return rc;
+  Tune tu;
+  rc = resolve_tune(g, tune, &tu);
+  if (rc) return rc;
+  rc = check_run(g, m, a, t, st, tu);
   if (rc) return rc;
   if (n_begin < 0 || n_end < n_begin || n_end > t->n_steps) return fail(NW_ERR_ARG, "step range out of bounds");
   if (g->dtype == NW_F32)
-    return forward_impl<float>(g, m, a, t, st, n_begin, n_end, (float*)traces, (cudaStream_t)stream);
-  return forward_impl<double>(g, m, a, t, st, n_begin, n_end, (double*)traces, (cudaStream_t)stream);
+    return forward_impl<float>(g, m, a, t, st, tu, n_begin, n_end, (float*)traces, (cudaStream_t)stream);
+  return forward_impl<double>(g, m, a, t, st, tu, n_begin, n_end, (double*)traces, (cudaStream_t)stream);
 }
 
 int nw_adjoint(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, const nw_time* t,
-               const nw_storage* st, const void* grad_traces, void* work, void* grad_c2dt2,
-               void* lambda0, void* mu1, void* stream) {
-  int rc = check_run(g, m, a, t, st);
+               const nw_storage* st, const nw_tuning* tune, const void* grad_traces, void* work,
+               double* grad_acc, void* lambda0, void* mu1, void* stream) {
+  int rc = check_grid(g);
   if (rc) return rc;
-  if (!grad_traces || !work || !grad_c2dt2) return fail(NW_ERR_ARG, "NULL adjoint buffer");
+  Tune tu;
+  rc = resolve_tune(g, tune, &tu);
+  if (rc) return rc;
+  rc = check_run(g, m, a, t, st, tu);
+  if (rc) return rc;
+  if (!grad_traces || !work || !grad_acc) return fail(NW_ERR_ARG, "NULL adjoint buffer");
   if (a->n_cells > 0 && (!a->cell_index || !a->cell_ptr || !a->cell_rec || !a->cell_weight))
     return fail(NW_ERR_ARG, "receiver adjoint table is NULL");
   if (!st->history && st->snap && !st->segbuf) return fail(NW_ERR_ARG, "checkpointing needs segbuf");
   if (g->dtype == NW_F32)
-    return adjoint_impl<float>(g, m, a, t, st, (const float*)grad_traces, (float*)work,
-                               (float*)grad_c2dt2, (float*)lambda0, (float*)mu1, (cudaStream_t)stream);
-  return adjoint_impl<double>(g, m, a, t, st, (const double*)grad_traces, (double*)work,
-                              (double*)grad_c2dt2, (double*)lambda0, (double*)mu1, (cudaStream_t)stream);
+    return adjoint_impl<float>(g, m, a, t, st, tu, (const float*)grad_traces, (float*)work, grad_acc,
+                               (float*)lambda0, (float*)mu1, (cudaStream_t)stream);
+  return adjoint_impl<double>(g, m, a, t, st, tu, (const double*)grad_traces, (double*)work, grad_acc,
+                              (double*)lambda0, (double*)mu1, (cudaStream_t)stream);
 }
 
 int nw_reduce_grad_c(const nw_grid* g, const int32_t* n_abs, const void* c, double dt2,
-                     int32_t n_shots, const void* grad_c2dt2, int32_t accumulate, double* grad_c,
+                     int32_t n_acc, const double* grad_acc, int32_t accumulate, double* grad_c,
                      void* stream) {
   int rc = check_grid(g);
   if (rc) return rc;
-  if (!n_abs || !c || !grad_c2dt2 || !grad_c || n_shots < 1) return fail(NW_ERR_ARG, "invalid reduce arguments");
+  if (!n_abs || !c || !grad_acc || !grad_c || n_acc < 1) return fail(NW_ERR_ARG, "invalid reduce arguments");
   cudaStream_t s = (cudaStream_t)stream;
   const nw::PadMap pm = padmap(g, n_abs);
   const long long pcells = (long long)pm.m0 * pm.m1 * pm.m2;
   const int blocks = grid_blocks(pcells, 128);
   if (g->dtype == NW_F32)
     nw::reduce_grad_kernel<float><<<blocks, 128, 0, s>>>(kgrid<float>(g), pm, g->ndim, (const float*)c, dt2,
-                                                         n_shots, (const float*)grad_c2dt2, accumulate, grad_c);
+                                                         n_acc, grad_acc, accumulate, grad_c);
   else
     nw::reduce_grad_kernel<double><<<blocks, 128, 0, s>>>(kgrid<double>(g), pm, g->ndim, (const double*)c,
-                                                          dt2, n_shots, (const double*)grad_c2dt2, accumulate,
-                                                          grad_c);
+                                                          dt2, n_acc, grad_acc, accumulate, grad_c);
   NW_LAUNCHED();
   return NW_OK;
 }
@@ -557,21 +746,22 @@ int nw_reduce_grad_c(const nw_grid* g, const int32_t* n_abs, const void* c, doub
 int nw_initial_state_adjoint(const nw_grid* g, const int32_t* n_abs, const nw_medium* m,
                              const nw_time* t, int32_t n_shots, const void* lambda0,
                              const void* mu1, const void* p0_level, void* grad_p0,
-                             void* grad_c2dt2, void* stream) {
+                             double* grad_acc, int32_t shots_per_acc, void* stream) {
   int rc = check_grid(g);
   if (rc) return rc;
-  if (!m || !t || !n_abs || !lambda0 || !mu1 || !p0_level || !grad_p0 || n_shots < 1)
+  if (!m || !t || !n_abs || !lambda0 || !mu1 || !p0_level || !grad_p0 || n_shots < 1 || shots_per_acc < 1)
     return fail(NW_ERR_ARG, "invalid initial-state adjoint arguments");
   cudaStream_t s = (cudaStream_t)stream;
   const nw::PadMap pm = padmap(g, n_abs);
   const long long cells = (long long)g->n[0] * g->n[1] * (g->ndim == 3 ? g->n[2] : 1);
-  dim3 gc(grid_blocks(cells, 256), n_shots);
+  const int groups = (n_shots + shots_per_acc - 1) / shots_per_acc;
+  dim3 gc(grid_blocks(cells, 256), groups);
   const int b_one = t->first_b_one;
-#define NW_IA(T, R)                                                                                   \
-  nw::initial_adjoint_kernel<T, R><<<gc, 256, 0, s>>>(kgrid<T>(g), pm, g->ndim, (const T*)m->c2dt2,   \
-                                                      (const T*)m->coef_b, b_one, (const T*)lambda0,  \
-                                                      (const T*)mu1, (const T*)p0_level, (T*)grad_p0, \
-                                                      (T*)grad_c2dt2)
+#define NW_IA(T, R)                                                                                       \
+  nw::initial_adjoint_kernel<T, R><<<gc, 256, 0, s>>>(kgrid<T>(g), pm, g->ndim, (const T*)m->c2dt2,       \
+                                                      (const T*)m->coef_b, b_one, n_shots, shots_per_acc, \
+                                                      (const T*)lambda0, (const T*)mu1, (const T*)p0_level, \
+                                                      (T*)grad_p0, grad_acc)
   if (g->dtype == NW_F32) { if (g->radius == 1) NW_IA(float, 1); else NW_IA(float, 2); }
   else { if (g->radius == 1) NW_IA(double, 1); else NW_IA(double, 2); }
 #undef NW_IA
@@ -597,17 +787,17 @@ int nw_zero_ghosts(const nw_grid* g, void* fields, int64_t n_fields, void* strea
   cudaStream_t s = (cudaStream_t)stream;
   const int last = g->ndim - 1;
   const int ld = (int)g->stride[last - 1];
-  const long long n_rows = g->field_elems / ld;
+  const long long n_rows = (g->field_elems - g->guard) / ld;
   const int rows_per_plane = g->ndim == 3 ? (int)(g->stride[0] / g->stride[1]) : 1;
   const int blocks = grid_blocks(n_rows * n_fields * 32, 256);
   if (g->dtype == NW_F32)
-    nw::zero_ghosts_kernel<float><<<blocks, 256, 0, s>>>((float*)fields, g->field_elems, n_rows, ld, g->n[last],
-                                                         g->ndim, g->radius, g->n[0], g->n[1], rows_per_plane,
-                                                         n_fields);
+    nw::zero_ghosts_kernel<float><<<blocks, 256, 0, s>>>((float*)fields, g->field_elems, g->guard, n_rows, ld,
+                                                         g->n[last], g->ndim, g->radius, g->n[0], g->n[1],
+                                                         rows_per_plane, n_fields);
   else
-    nw::zero_ghosts_kernel<double><<<blocks, 256, 0, s>>>((double*)fields, g->field_elems, n_rows, ld, g->n[last],
-                                                          g->ndim, g->radius, g->n[0], g->n[1], rows_per_plane,
-                                                          n_fields);
+    nw::zero_ghosts_kernel<double><<<blocks, 256, 0, s>>>((double*)fields, g->field_elems, g->guard, n_rows, ld,
+                                                          g->n[last], g->ndim, g->radius, g->n[0], g->n[1],
+                                                          rows_per_plane, n_fields);
   NW_LAUNCHED();
   return NW_OK;
 }

@@ -49,7 +49,7 @@ from .plan import DevicePlan, ghost_view, plan_storage, to_ghost
 
 log = logging.getLogger("nefi_b200")
 
-SNAPSHOTS = ("exact", "fp16", "bf16")
+SNAPSHOTS = ("exact", "fixed16", "fp16", "bf16")
 
 
 class _LeapfrogB200(Operator):
@@ -214,7 +214,8 @@ def _forward_sweep(plan: DevicePlan, medium, acq, run: _Run, n_begin: int, n_end
                    traces: torch.Tensor | None, stream: int) -> None:
     lib = _lib.load()
     _lib.check(lib.nw_forward(C.byref(plan.g), C.byref(medium), C.byref(acq), C.byref(plan.time),
-                              C.byref(run.storage), n_begin, n_end, _lib.ptr(traces), stream))
+                              C.byref(run.storage), C.byref(plan.tuning), n_begin, n_end,
+                              _lib.ptr(traces), stream))
 
 
 def _adjoint_sweep(plan: DevicePlan, medium, acq, run: _Run, grad_traces: torch.Tensor,
@@ -222,14 +223,14 @@ def _adjoint_sweep(plan: DevicePlan, medium, acq, run: _Run, grad_traces: torch.
     lib = _lib.load()
     S = run.n_shots
     work = plan.empty_levels(3, S, zero=False)
-    gC = plan.empty_levels(1, S, zero=False)[0]
+    gC = torch.empty(plan.n_acc(S), plan.field, device=plan.device, dtype=torch.float64)
     lam0 = mu1 = None
     if want_initial:
         lam0 = plan.empty_levels(1, S, zero=False)[0]
         mu1 = plan.empty_levels(1, S, zero=False)[0]
     _lib.check(lib.nw_adjoint(C.byref(plan.g), C.byref(medium), C.byref(acq), C.byref(plan.time),
-                              C.byref(run.storage), grad_traces.data_ptr(), work.data_ptr(),
-                              gC.data_ptr(), _lib.ptr(lam0), _lib.ptr(mu1), stream))
+                              C.byref(run.storage), C.byref(plan.tuning), grad_traces.data_ptr(),
+                              work.data_ptr(), gC.data_ptr(), _lib.ptr(lam0), _lib.ptr(mu1), stream))
     if run.storage.snap and run.storage.snap_kind != _lib.NW_SNAP_EXACT:
         # encoded snapshots carry a validity check; reading the status synchronises the stream
         rc = lib.nw_status(stream)
@@ -282,7 +283,7 @@ class _FWIFunction(torch.autograd.Function):
         gC, _, _ = _adjoint_sweep(plan, medium, acq, run, gtr, False, stream)
         grad64 = torch.empty(c.shape, device=c.device, dtype=torch.float64)
         _lib.check(_lib.load().nw_reduce_grad_c(C.byref(plan.g), plan.n_abs, c.data_ptr(), op.dt**2,
-                                                ctx.n_shots, gC.data_ptr(), 0, grad64.data_ptr(),
+                                                gC.shape[0], gC.data_ptr(), 0, grad64.data_ptr(),
                                                 stream))
         run.release()
         ctx.run = None
@@ -410,8 +411,8 @@ class WaveOperatorB200(_LeapfrogB200):
                 tm["adj0"] = torch.cuda.Event(enable_timing=True)
                 tm["adj0"].record()
             gC, _, _ = _adjoint_sweep(plan, medium, acq, run, resid.contiguous(), False, stream)
-            _lib.check(lib.nw_reduce_grad_c(C.byref(plan.g), plan.n_abs, c.data_ptr(), self.dt**2, S,
-                                            gC.data_ptr(), 1, grad.data_ptr(), stream))
+            _lib.check(lib.nw_reduce_grad_c(C.byref(plan.g), plan.n_abs, c.data_ptr(), self.dt**2,
+                                            gC.shape[0], gC.data_ptr(), 1, grad.data_ptr(), stream))
             if tm is not None:
                 tm["adj1"] = torch.cuda.Event(enable_timing=True)
                 tm["adj1"].record()
@@ -520,12 +521,13 @@ class _PATFunction(torch.autograd.Function):
         _lib.check(lib.nw_initial_state_adjoint(C.byref(plan.g), plan.n_abs, C.byref(medium),
                                                 C.byref(plan.time), S, lam0.data_ptr(), mu1.data_ptr(),
                                                 p0l.data_ptr(), grad_p0.data_ptr(),
-                                                gC.data_ptr() if need_c else None, stream))
+                                                gC.data_ptr() if need_c else None, plan.shots_per_acc,
+                                                stream))
         grad_c = None
         if need_c:
             g64 = torch.empty(c.shape, device=dev, dtype=torch.float64)
             _lib.check(lib.nw_reduce_grad_c(C.byref(plan.g), plan.n_abs, c.contiguous().data_ptr(),
-                                            op.dt**2, S, gC.data_ptr(), 0, g64.data_ptr(), stream))
+                                            op.dt**2, gC.shape[0], gC.data_ptr(), 0, g64.data_ptr(), stream))
             grad_c = g64.to(c.dtype)
         run.release()
         ctx.run = None

@@ -57,12 +57,13 @@ def ghost_view(g: _lib.Grid, flat: torch.Tensor) -> torch.Tensor:
     """Strided view ``(..., *P)`` of the interior cells of ghost-layout field(s) in ``flat``."""
     lead = flat.shape[:-1]
     r = g.radius
+    body = flat[..., g.guard:]
     if g.ndim == 2:
-        rows = flat.shape[-1] // g.stride[0]
-        v = flat.view(*lead, rows, g.stride[0])
+        rows = body.shape[-1] // g.stride[0]
+        v = body.view(*lead, rows, g.stride[0])
         return v[..., r:r + g.n[0], : g.n[1]]
-    planes = flat.shape[-1] // g.stride[0]
-    v = flat.view(*lead, planes, g.stride[0] // g.stride[1], g.stride[1])
+    planes = body.shape[-1] // g.stride[0]
+    v = body.view(*lead, planes, g.stride[0] // g.stride[1], g.stride[1])
     return v[..., r:r + g.n[0], : g.n[1], : g.n[2]]
 
 
@@ -125,6 +126,65 @@ class DevicePlan:
             self.src_weight = (sw / grid.cell_volume * op.dt**2).to(**cast)
             self.wavelet = op.wavelet().to(**cast)
         self.time = _lib.Time(op.n_steps, op.substeps, op.n_t, self.first_b_one)
+        self._corner = corner
+        self._cells = cells
+        self.set_tuning(*(getattr(op, "tuning", None) or ()))
+
+    def set_tuning(self, vz: int = 0, rx: int = 0, shots_per_cta: int = 0, adj_shots_per_cta: int = 0) -> None:
+        """Choose the 2-D launch shape (0 = library default) and build the per-tile tables."""
+        t = _lib.Tuning(int(vz), int(rx), int(shots_per_cta), int(adj_shots_per_cta))
+        tx, tz = C.c_int32(), C.c_int32()
+        _lib.check(_lib.load().nw_tile_shape(C.byref(self.g), C.byref(t), C.byref(tx), C.byref(tz)))
+        self.tuning = t
+        self.tile = (tx.value, tz.value)
+        self.tiles_z = 0
+        self.rec_corner = self.tile_rec_ptr = self.tile_rec_list = None
+        self.tile_cell_ptr = self.tile_cell_local = self.tile_cell_gid = None
+        if self.g.ndim == 2:
+            self._build_tile_tables()
+
+    def _build_tile_tables(self) -> None:
+        """Per-tile receiver and adjoint-source tables for the 2-D tiled kernels.
+
+        A receiver belongs to the tile holding its stencil's lower corner (its other corners lie
+        in that tile's one-cell halo); a receiver-touched cell belongs to the tile containing it.
+        Lists keep ascending receiver / cell order inside each tile.
+        """
+        TX, TZ = self.tile
+        g = self.g
+        tiles_z = -(-g.n[1] // TZ)
+        n_tiles = tiles_z * -(-g.n[0] // TX)
+        corner = self._corner
+        tile_of = (corner[:, 0] // TX) * tiles_z + corner[:, 1] // TZ
+        order = torch.argsort(tile_of, stable=True)
+        rptr = torch.zeros(n_tiles + 1, dtype=torch.int64)
+        rptr[1:] = torch.cumsum(torch.bincount(tile_of, minlength=n_tiles), 0)
+        rel = self._cells - int(g.origin)
+        x, z = rel // int(g.stride[0]), rel % int(g.stride[0])
+        ctile = (x // TX) * tiles_z + z // TZ
+        corder = torch.argsort(ctile, stable=True)
+        cptr = torch.zeros(n_tiles + 1, dtype=torch.int64)
+        cptr[1:] = torch.cumsum(torch.bincount(ctile, minlength=n_tiles), 0)
+        local = (x % TX) * TZ + z % TZ
+        dev, i32 = self.device, torch.int32
+        self.tiles_z = tiles_z
+        self.rec_corner = corner.to(i32).contiguous().to(dev)
+        self.tile_rec_ptr = rptr.to(i32).to(dev)
+        self.tile_rec_list = order.to(i32).to(dev)
+        self.tile_cell_ptr = cptr.to(i32).to(dev)
+        self.tile_cell_local = local[corder].to(i32).to(dev)
+        self.tile_cell_gid = corder.to(i32).to(dev)
+
+    def n_acc(self, n_shots: int) -> int:
+        """Float64 gradient accumulators the adjoint sweep fills for ``n_shots`` shots."""
+        n = _lib.load().nw_adjoint_groups(C.byref(self.g), C.byref(self.tuning), n_shots)
+        if n < 1:
+            raise _lib.LibraryError(_lib.NW_ERR_ARG, "invalid adjoint group query")
+        return n
+
+    @property
+    def shots_per_acc(self) -> int:
+        return int(self.tuning.adj_shots_per_cta) if self.g.ndim == 2 else 1
 
     # -- descriptors ------------------------------------------------------------------------
     def medium(self, c2dt2: torch.Tensor) -> _lib.Medium:
@@ -146,6 +206,15 @@ class DevicePlan:
         a.cell_ptr = self.cell_ptr.data_ptr()
         a.cell_rec = self.cell_rec.data_ptr()
         a.cell_weight = self.cell_weight.data_ptr()
+        if self.g.ndim == 2:
+            a.tiles_z = self.tiles_z
+            a.tile_rows, a.tile_cols = self.tile
+            a.rec_corner = self.rec_corner.data_ptr()
+            a.tile_rec_ptr = self.tile_rec_ptr.data_ptr()
+            a.tile_rec_list = self.tile_rec_list.data_ptr()
+            a.tile_cell_ptr = self.tile_cell_ptr.data_ptr()
+            a.tile_cell_local = self.tile_cell_local.data_ptr()
+            a.tile_cell_gid = self.tile_cell_gid.data_ptr()
         return a
 
     def empty_levels(self, n_levels: int, n_shots: int, zero: bool = True) -> torch.Tensor:

@@ -35,7 +35,7 @@ def test_every_declared_symbol_is_exported_and_bound(lib):
 
 
 def test_abi_version_and_arch(lib):
-    assert lib.nw_abi_version() == 1
+    assert lib.nw_abi_version() == _lib.ABI_VERSION == 2
     assert lib.nw_built_arch() == 1000
 
 
@@ -90,9 +90,11 @@ def test_snapshot_pool_sizes(lib):
     g.n[0], g.n[1], g.n[2] = 552, 552, 1
     _lib.check(lib.nw_grid_layout(C.byref(g)))
     exact = lib.nw_snapshot_bytes(C.byref(g), 16, 10, _lib.NW_SNAP_EXACT)
-    half = lib.nw_snapshot_bytes(C.byref(g), 16, 10, _lib.NW_SNAP_F16)
     assert exact == 10 * 2 * 16 * g.field_elems * 4
-    assert 0.49 * exact < half < 0.53 * exact
+    for kind in (_lib.NW_SNAP_F16, _lib.NW_SNAP_BF16, _lib.NW_SNAP_I16):
+        half = lib.nw_snapshot_bytes(C.byref(g), 16, 10, kind)
+        # 2 bytes per element plus one float scale per 32-element block
+        assert 0.53 * exact < half < 0.54 * exact
 
 
 def test_missing_library_fails_loudly(tmp_path):

@@ -97,6 +97,37 @@ def test_adjoint_table_is_cell_major_and_complete():
     assert pairs == ref
 
 
+@pytest.mark.parametrize("tuning", [(0, 0, 0), (2, 2, 1), (4, 8, 3), (2, 4, 16)])
+@pytest.mark.parametrize("name", ["fwi_o4_sponge", "cfg1_128_o4_sponge", "pat2d_o4_sponge"])
+def test_tile_tables_partition_receivers_and_cells(name, tuning):
+    """Every receiver is owned by exactly the tile holding its stencil corner, and every
+    receiver-touched cell appears once, in its own tile, at the right local index."""
+    case = load_golden(name)
+    plan = make_op(case)._plan(CPU, torch.float32)
+    plan.set_tuning(*tuning)
+    TX, TZ = plan.tile
+    assert TX == 8 * plan.tuning.rx and TZ == 32 * plan.tuning.vz
+    tz = plan.tiles_z
+    rptr, rlist = plan.tile_rec_ptr.numpy(), plan.tile_rec_list.numpy()
+    corner = plan.rec_corner.numpy()
+    assert sorted(rlist.tolist()) == list(range(plan.n_rec))
+    for t in range(len(rptr) - 1):
+        for r in rlist[rptr[t]:rptr[t + 1]]:
+            assert (corner[r, 0] // TX) * tz + corner[r, 1] // TZ == t
+    cptr = plan.tile_cell_ptr.numpy()
+    gid, local = plan.tile_cell_gid.numpy(), plan.tile_cell_local.numpy()
+    assert sorted(gid.tolist()) == list(range(plan.n_cells))
+    cells = plan.cell_index.numpy() - plan.g.origin
+    ld = plan.g.stride[0]
+    for t in range(len(cptr) - 1):
+        x0, z0 = (t // tz) * TX, (t % tz) * TZ
+        for e in range(cptr[t], cptr[t + 1]):
+            x, z = divmod(int(cells[gid[e]]), ld)
+            assert x0 <= x < x0 + TX and z0 <= z < z0 + TZ
+            assert local[e] == (x - x0) * TZ + (z - z0)
+    assert plan.n_acc(16) == (-(-16 // plan.tuning.adj_shots_per_cta))
+
+
 def test_reference_errors_are_raised_on_the_host():
     dom = Domain((16, 16), ((0.0, 1.0), (0.0, 1.0)))
     kw = dict(n_t=10, dt_obs=0.01, f0=5.0, c_max=2.5, absorbing="sponge")
