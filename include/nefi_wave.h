@@ -237,6 +237,34 @@ int nw_initial_state_adjoint(const nw_grid* g, const int32_t* n_abs, const nw_me
                              double* grad_acc, int32_t shots_per_acc, void* stream);
 
 /*
+ * Allocation-free gradient: the work of nw_adjoint followed by nw_reduce_grad_c (overwriting
+ * grad_c), with the adjoint's scratch -- three adjoint levels and the float64 accumulators -- taken
+ * from one fixed array that the library holds in device memory instead of from caller buffers.
+ * This entry point has no counterpart in the reference; it exists for callers that cannot allocate
+ * device memory themselves: a host runtime that reaches this library only through the C ABI and
+ * owns no CUDA allocator (a JVM or Go service binding it through JNI or cgo), a service that
+ * reserves its device memory at start-up and may not allocate afterwards, or a latency-bound loop
+ * that must not call cudaMalloc, which synchronises the device. The caller still passes every
+ * input and the output grad_c (physical grid, float64).
+ *  - Limit: 3 * n_shots * field_elems * sizeof(dtype), rounded up to 256 bytes, plus
+ *    nw_adjoint_groups() * field_elems * 8 bytes must not exceed NW_NOALLOC_SCRATCH_BYTES (64 MiB);
+ *    e.g. 8 float32 shots on a 552^2 padded grid fit, 16 do not. Larger requests return
+ *    NW_ERR_ARG with a message giving the size needed; use nw_adjoint then.
+ *  - Every GPU that loads the library holds the 64 MiB array until the process exits.
+ *  - The first call on a device looks up the array's device address (with that device current) and
+ *    caches it; make that first call before any stream capture begins.
+ *  - All calls share the one array and it keeps the last call's contents; each call clears what it
+ *    uses before use, but two calls whose GPU work overlaps (different streams or host threads)
+ *    race on it, so serialise them.
+ *  - No cudaMalloc, cudaFree or other allocating routine is called.
+ */
+#define NW_NOALLOC_SCRATCH_BYTES (64u * 1024u * 1024u)
+int nw_adjoint_grad_c_noalloc(const nw_grid* g, const int32_t* n_abs, const nw_medium* m,
+                              const nw_acquisition* a, const nw_time* t, const nw_storage* st,
+                              const nw_tuning* tune, const void* c, double dt2,
+                              const void* grad_traces, double* grad_c, void* stream);
+
+/*
  * Zero only the ghost cells of `n_fields` consecutive fields (e.g. a freshly allocated history),
  * leaving interior cells untouched: the stencils then read zero outside the grid without a
  * full memset of storage whose interior every step overwrites anyway.

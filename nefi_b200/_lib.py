@@ -90,6 +90,8 @@ _SIGNATURES = {
     "nw_sample": (C.c_int, [P(Grid), P(Acquisition), C.c_int32, VP, C.c_int32, VP, VP]),
     "nw_status": (C.c_int, [VP]),
     "nw_zero_ghosts": (C.c_int, [P(Grid), VP, C.c_int64, VP]),
+    "nw_adjoint_grad_c_noalloc": (C.c_int, [P(Grid), VP, P(Medium), P(Acquisition), P(Time), P(Storage),
+                                            P(Tuning), VP, C.c_double, VP, VP, VP]),
     "nw_launch_count": (C.c_uint64, []),
 }
 EXPORTED = tuple(_SIGNATURES)

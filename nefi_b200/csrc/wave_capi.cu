@@ -9,6 +9,7 @@
 #include <atomic>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "../../include/nefi_wave.h"
@@ -818,3 +819,86 @@ int nw_status(void* stream) {
 }
 
 }  // extern "C"
+
+// =============================================================================================
+// Allocation-free adjoint gradient: nw_adjoint + nw_reduce_grad_c with their scratch (the three
+// adjoint levels and the float64 accumulators) carved out of a fixed array in device memory
+// instead of caller buffers. The array is module-scope device storage, so every GPU that loads
+// this library holds NW_NOALLOC_SCRATCH_BYTES of it until the process exits.
+// =============================================================================================
+namespace {
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[NW_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kMaxDevices = 128;
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kMaxDevices] = {};
+
+// Device address of the scratch array on the current device. The host symbol is only a
+// stand-in, so the address is looked up once per device (with that device current) and cached.
+int noalloc_scratch(void** out) {
+  int dev = 0;
+  NW_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return fail(NW_ERR_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    NW_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return NW_OK;
+}
+
+template <typename T>
+int noalloc_gradient(const nw_grid* g, const int32_t* n_abs, const nw_medium* m, const nw_acquisition* a,
+                     const nw_time* t, const nw_storage* st, const Tune& tu, const void* c, double dt2,
+                     const T* gtr, double* grad_c, cudaStream_t s) {
+  const size_t work_bytes = 3 * (size_t)a->n_shots * g->field_elems * sizeof(T);
+  const size_t acc_off = (work_bytes + 255) / 256 * 256;
+  const int n_acc = n_groups(g, tu, a->n_shots);
+  const size_t need = acc_off + (size_t)n_acc * g->field_elems * sizeof(double);
+  if (need > NW_NOALLOC_SCRATCH_BYTES)
+    return fail(NW_ERR_ARG, "nw_adjoint_grad_c_noalloc needs " + std::to_string(need) +
+                                " bytes of scratch, above its fixed " + std::to_string(NW_NOALLOC_SCRATCH_BYTES) +
+                                "-byte array; use nw_adjoint with caller-allocated buffers or fewer shots per call");
+  void* base = nullptr;
+  int rc = noalloc_scratch(&base);
+  if (rc) return rc;
+  T* work = reinterpret_cast<T*>(base);
+  double* acc = reinterpret_cast<double*>(reinterpret_cast<char*>(base) + acc_off);
+  // adjoint_impl clears the work levels and the accumulators on `s` before using them, so the
+  // previous call's contents never leak into this one.
+  rc = adjoint_impl<T>(g, m, a, t, st, tu, gtr, work, acc, nullptr, nullptr, s);
+  if (rc) return rc;
+  const nw::PadMap pm = padmap(g, n_abs);
+  const long long pcells = (long long)pm.m0 * pm.m1 * pm.m2;
+  nw::reduce_grad_kernel<T><<<grid_blocks(pcells, 128), 128, 0, s>>>(kgrid<T>(g), pm, g->ndim, (const T*)c, dt2,
+                                                                     n_acc, acc, 0, grad_c);
+  NW_LAUNCHED();
+  return NW_OK;
+}
+
+}  // namespace
+
+extern "C" int nw_adjoint_grad_c_noalloc(const nw_grid* g, const int32_t* n_abs, const nw_medium* m,
+                                         const nw_acquisition* a, const nw_time* t, const nw_storage* st,
+                                         const nw_tuning* tune, const void* c, double dt2,
+                                         const void* grad_traces, double* grad_c, void* stream) {
+  int rc = check_grid(g);
+  if (rc) return rc;
+  Tune tu;
+  rc = resolve_tune(g, tune, &tu);
+  if (rc) return rc;
+  rc = check_run(g, m, a, t, st, tu);
+  if (rc) return rc;
+  if (!n_abs || !c || !grad_traces || !grad_c) return fail(NW_ERR_ARG, "NULL argument");
+  if (a->n_cells > 0 && (!a->cell_index || !a->cell_ptr || !a->cell_rec || !a->cell_weight))
+    return fail(NW_ERR_ARG, "receiver adjoint table is NULL");
+  if (!st->history && st->snap && !st->segbuf) return fail(NW_ERR_ARG, "checkpointing needs segbuf");
+  if (g->dtype == NW_F32)
+    return noalloc_gradient<float>(g, n_abs, m, a, t, st, tu, c, dt2, (const float*)grad_traces, grad_c,
+                                   (cudaStream_t)stream);
+  return noalloc_gradient<double>(g, n_abs, m, a, t, st, tu, c, dt2, (const double*)grad_traces, grad_c,
+                                  (cudaStream_t)stream);
+}
