@@ -146,24 +146,27 @@ typedef struct nw_time {
 } nw_time;
 
 /*
- * Wavefield storage for the gradient.
- *  history != NULL: every level p^-1..p^N is kept, level n at history + (n+1)*level_stride
- *    (level_stride = n_shots * field_elems). Matches grad_mode="autograd".
+ * Wavefield storage. The pressure always advances through `ring`: three levels, level n at
+ * ring + ((n+1) % 3) * level_stride (level_stride = n_shots * field_elems). What the gradient
+ * needs of the forward run is Lap p^n for n = 0..N-1, the factor of the velocity term
+ * mu^{n+1} * Lap p^n; it is kept in one of two ways.
+ *  history != NULL: the forward step n stores Lap p^n at history + n*level_stride (N levels,
+ *    grad_mode="autograd").
  *  history == NULL and snap != NULL: checkpointing (grad_mode="checkpoint",
  *    nefi/physics/timestep.py:141-169): the pair (p^{n0-1}, p^{n0}) is encoded into snapshot
- *    j = n0 / segment for every segment start n0; the adjoint recomputes each segment into
- *    `segbuf` (segment + 1 levels). snap_kind selects exact copies or 16-bit values with one
- *    float scale per block of NW_SNAP_BLOCK elements: fp16 / bf16 with a power-of-two scale,
- *    or int16 mantissas scaled by the block maximum (NW_SNAP_I16, block floating point). The
- *    16-bit kinds store p^{n0} and p^{n0} - p^{n0-1}.
- *  both NULL: forward only; `ring` holds three levels.
+ *    j = n0 / segment for every segment start n0; the adjoint decodes it into the ring and
+ *    recomputes Lap p^{n0..n0+segment-1} into `segbuf` (segment levels). snap_kind selects exact
+ *    copies or 16-bit values with one float scale per block of NW_SNAP_BLOCK elements: fp16 /
+ *    bf16 with a power-of-two scale, or int16 mantissas scaled by the block maximum (NW_SNAP_I16,
+ *    block floating point). The 16-bit kinds store p^{n0} and p^{n0} - p^{n0-1}.
+ *  both NULL: forward only.
  */
 #define NW_SNAP_BLOCK 32
 typedef struct nw_storage {
-  void* history;
-  void* ring;          /* 3 levels, used when history == NULL */
+  void* history;       /* N levels of Lap p^n, or NULL */
+  void* ring;          /* 3 levels of p, always required */
   void* snap;          /* snapshot pool, nw_snapshot_bytes() bytes */
-  void* segbuf;        /* (segment + 1) levels, used when snap != NULL */
+  void* segbuf;        /* `segment` levels of Lap p^n, used when snap != NULL */
   int32_t segment;     /* steps per checkpoint segment */
   int32_t snap_kind;   /* NW_SNAP_* */
 } nw_storage;
@@ -188,11 +191,11 @@ int nw_initial_state(const nw_grid* g, const int32_t* n_abs, const nw_medium* m,
                      const void* p0, void* pm1_level, void* p0_level, void* stream);
 
 /*
- * Forward run of steps [n_begin, n_end) for all shots. Levels are addressed through `st`
- * (history, or the ring when no history is given). Receiver samples of every recorded level
+ * Forward run of steps [n_begin, n_end) for all shots through the ring of `st`; with a history,
+ * step n also stores Lap p^n there. Receiver samples of every recorded level
  * n in [n_begin, n_end) go to traces (n_shots, n_rec, n_t), and of level n_end when it is the last
  * step; with checkpointing, snapshots of every segment start in [n_begin, n_end) are encoded.
- * On entry levels n_begin-1 and n_begin must be in place. `tune` may be NULL.
+ * On entry ring levels n_begin-1 and n_begin must be in place. `tune` may be NULL.
  * Replaces WaveOperator.simulate / run_timestepping (nefi/physics/wave.py:699-740,
  * nefi/physics/timestep.py:144-149).
  */

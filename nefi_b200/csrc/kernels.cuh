@@ -4,7 +4,7 @@
 //   p^{n+1} = A * ( 2 p^n - B p^{n-1} + C * Lap(p^n) + S w(n) ),   C = c^2 dt^2,
 // with A = B = 1 outside the absorbing layer. Its exact discrete adjoint, with mu^n = A lambda^n:
 //   mu^n = A * ( R^T g_n + 2 mu^{n+1} + Lap(C mu^{n+1}) - B mu^{n+2} ),
-//   dJ/dC += mu^{n+1} * Lap(p^n).
+//   dJ/dC += mu^{n+1} * Lap(p^n), with Lap(p^n) stored by the forward step that computed it.
 // Fields live in the ghost layout (see nw_grid in include/nefi_wave.h): every neighbour read is
 // in bounds and reads zero outside the padded grid, so the stencils carry no boundary branches.
 #pragma once
@@ -48,6 +48,7 @@ struct FwdStep {
   const int64_t* __restrict__ rec_idx;
   const T* __restrict__ rec_w;
   int n_rec, n_t, j;
+  T* __restrict__ lap_out;             // non-null: also store Lap p^n (the gradient factor)
 };
 
 template <typename T>
@@ -59,7 +60,7 @@ struct AdjStep {
   const T* __restrict__ A;
   const T* __restrict__ B;
   int apply_a;
-  const T* __restrict__ p;      // p^n (nullptr: no gradient term)
+  const T* __restrict__ lap;    // Lap p^n as the forward step stored it (nullptr: no gradient term)
   double* __restrict__ grad;    // per-shot float64 dJ/dC accumulators
 };
 
@@ -147,6 +148,7 @@ __global__ void __launch_bounds__(256) fwd3d(KGrid<T> g, FwdStep<T> a) {
         layer = x < g.lo0 || x >= g.hi0 || t.y < g.lo1 || t.y >= g.hi1 || t.z < g.lo2 || t.z >= g.hi2;
         if (layer) { av = a.A[i]; bv = a.b_one ? T(1) : a.B[i]; }
       }
+      if (a.lap_out) a.lap_out[so + i] = lap;
       T rhs = (T(2) * c - bv * pp) + a.C[i] * lap;
       const int dx = x - bx, dy = t.y - by, dz = t.z - bz;
       if (dx >= 0 && dx <= 1 && dy >= 0 && dy <= 1 && dz >= 0 && dz <= 1) rhs += sw[4 * dx + 2 * dy + dz] * wn;
@@ -174,15 +176,7 @@ __global__ void __launch_bounds__(256) adj3d(KGrid<T> g, AdjStep<T> a) {
     q[k] = (xr < g.n0 + R) ? C[i] * mv : T(0);
     if (k >= R && k < R + RX) m[k - R] = mv;
   }
-  const T* __restrict__ pn = a.p ? a.p + so : nullptr;
-  T pw[RX + 2 * R];
-  if (pn) {
-#pragma unroll
-    for (int k = 0; k < RX + 2 * R; ++k) {
-      const int xr = t.x0 - R + k;
-      pw[k] = (xr < g.n0 + R) ? pn[base + (long long)(k - R) * g.s0] : T(0);
-    }
-  }
+  const T* __restrict__ ln = a.lap ? a.lap + so : nullptr;
 #pragma unroll
   for (int k = 0; k < RX; ++k) {
     const int x = t.x0 + k;
@@ -203,14 +197,7 @@ __global__ void __launch_bounds__(256) adj3d(KGrid<T> g, AdjStep<T> a) {
       }
       T lam = (T(2) * m[k] + lq) - bv * a.mu2[so + i];
       a.out[so + i] = (layer && a.apply_a) ? av * lam : lam;
-      if (pn) {
-        T lp = g.wc * pw[k + R] + g.w1a * (pw[k + R - 1] + pw[k + R + 1]) +
-               g.w1b * (pn[i - sy] + pn[i + sy]) + g.w1c * (pn[i - 1] + pn[i + 1]);
-        if (R == 2)
-          lp += g.w2a * (pw[k] + pw[k + 4]) + g.w2b * (pn[i - 2 * sy] + pn[i + 2 * sy]) +
-                g.w2c * (pn[i - 2] + pn[i + 2]);
-        a.grad[so + i] += (double)(m[k] * lp);
-      }
+      if (ln) a.grad[so + i] += (double)(m[k] * ln[i]);
     }
   }
 }

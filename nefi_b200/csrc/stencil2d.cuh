@@ -2,14 +2,19 @@
 //
 // One CTA (8 warps) owns a tile of TX = 8*RX rows by TZ = 32*VZ columns and loops over a group
 // of shots. For every shot the input tiles (p^n or mu^{n+1} with an R-row and 16-byte-column halo,
-// and the core of p^{n-1} or mu^{n+2}) are staged in shared memory by cp.async, double buffered
-// so that the copies of shot s+1 overlap the arithmetic of shot s. Each thread computes the
-// shared/global offsets of the 16-byte chunks it copies once per CTA; per shot it only adds the
-// shot's base address. A thread owns VZ adjacent columns and RX rows: it slides a (2R+1)-row
-// register window down its columns, reading each row once as a VZ-wide vector plus two halo
-// vectors, so every shared-memory access is a conflict-free 8- or 16-byte load. Coefficients
-// (c^2 dt^2 and the absorbing A/B) are read per row from global memory; they are the same for
-// every shot of the CTA and stay in L1.
+// and core tiles: p^{n-1}, or mu^{n+2} and the stored Lap p^n) are staged in shared memory by
+// cp.async through a ring of NS buffers, so that the copies of the next NS-1 shots are in flight
+// while shot s is computed. Each thread computes the shared/global offsets of the 16-byte chunks it
+// copies once per CTA; per shot it only adds the shot's base address. A thread owns VZ adjacent
+// columns and RX rows: it slides a (2R+1)-row register window down its columns, reading each row
+// once as a VZ-wide vector plus two halo vectors, so every shared-memory access is a
+// conflict-free 8- or 16-byte load. c^2 dt^2 is staged once per CTA (it is the same for every
+// shot); the absorbing A/B are read per row from global memory in layer tiles only and stay in L1.
+//
+// The step kernels are launched with programmatic dependent launch: each one waits
+// (griddepcontrol.wait) for the previous kernel in the stream to finish and flush before it reads
+// or writes any field, and lets the next one be scheduled (griddepcontrol.launch_dependents) as
+// soon as its own last wave is resident, which hides the launch gap between time steps.
 //
 // Receivers are gathered and adjoint sources injected inside the same kernels, from per-tile
 // tables built on the host (the receivers whose stencil corner lies in the tile; the cells of the
@@ -30,6 +35,10 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
+// Programmatic dependent launch: block until the preceding grid's memory is visible / allow the
+// following grid to be scheduled. Both are no-ops for a kernel launched without the attribute.
+__device__ __forceinline__ void wait_previous_grid() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void allow_next_grid() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
 
 // Vector of N elements of T loaded/stored as one 8- or 16-byte access.
 template <typename T, int N>
@@ -110,6 +119,7 @@ struct FwdTiled {
   const T* __restrict__ rec_w;
   int n_rec, n_t, j;
   TileTables tt;
+  T* __restrict__ lap_out;  // non-null: also store Lap p^n (the adjoint's gradient factor)
 };
 
 template <typename T>
@@ -121,7 +131,7 @@ struct AdjTiled {
   const T* __restrict__ A;
   const T* __restrict__ B;
   int apply_a;
-  const T* __restrict__ p;      // p^n, nullptr: no gradient term
+  const T* __restrict__ lap;    // Lap p^n as the forward step computed it; nullptr: no gradient term
   double* __restrict__ gacc;    // (n_groups, field) float64 accumulators of dJ/dC
   int n_shots, shots_per_cta;
   const T* __restrict__ gtr;    // trace cotangents (n_shots, n_rec, n_t); non-null on record steps
@@ -142,6 +152,7 @@ struct Tile2Shape {
   static constexpr int QS = TX * TZ;              // elements of a core tile
   static constexpr int NCH = (HR * (SW / EPC) + 255) / 256;  // halo chunks per thread
   static constexpr int NCC = (TX * (TZ / EPC) + 255) / 256;  // core chunks per thread
+  static constexpr int NS = sizeof(T) == 8 ? 2 : 3;          // shot buffers in the copy ring
 };
 
 // The chunks one thread copies for one tile region: shared and global element offsets (the
@@ -215,15 +226,19 @@ __device__ __forceinline__ void store_row(T* dst, const T (&o)[VZ], int zc, int 
   }
 }
 
+
 // ------------------------------------------------------------------------------------------
-// forward step
+// forward step: p^{n+1} = A (2 p^n - B p^{n-1} + C Lap p^n + S w(n)); with lap_out, the same
+// launch also stores Lap p^n, the factor the adjoint multiplies mu^{n+1} by
 // ------------------------------------------------------------------------------------------
 template <typename T, int R, int VZ, int RX, bool AB>
 __global__ void __launch_bounds__(256, 3) fwd2d_tiled(KGrid<T> g, FwdTiled<T> a) {
   using S = Tile2Shape<T, VZ, RX, R>;
+  constexpr int NS = S::NS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* sp = reinterpret_cast<T*>(smem_raw);  // [2][PS] p^n
-  T* sq = sp + 2 * S::PS;                  // [2][QS] p^{n-1}
+  T* scc = reinterpret_cast<T*>(smem_raw);  // [QS] c^2 dt^2
+  T* sp = scc + S::QS;                      // [NS][PS] p^n with halo
+  T* sq = sp + NS * S::PS;                  // [NS][QS] p^{n-1}
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int z0 = blockIdx.x * S::TZ, x0 = blockIdx.y * S::TX;
@@ -237,41 +252,49 @@ __global__ void __launch_bounds__(256, 3) fwd2d_tiled(KGrid<T> g, FwdTiled<T> a)
 
   const CopyPlan<S::NCH> ph = plan_halo<T, VZ, RX, R>(g, x0, z0);
   const CopyPlan<S::NCC> pc = plan_core<T, VZ, RX, R>(g, x0, z0);
-  issue(ph, a.cur + (long long)sb * g.field, sp);
-  issue(pc, a.prev + (long long)sb * g.field, sq);
-  cp_async_commit();
+  wait_previous_grid();
+  allow_next_grid();
+  issue(pc, a.C, scc);
+#pragma unroll
+  for (int i = 0; i < NS - 1; ++i) {  // one commit group per shot, empty groups included, so that
+    if (sb + i < se) {                // wait_group<NS-1> in the loop means "shot s has landed"
+      issue(ph, a.cur + (long long)(sb + i) * g.field, sp + i * S::PS);
+      issue(pc, a.prev + (long long)(sb + i) * g.field, sq + i * S::QS);
+    }
+    cp_async_commit();
+  }
+  const int e0 = a.traces ? a.tt.rec_ptr[tile] : 0, e1 = a.traces ? a.tt.rec_ptr[tile + 1] : 0;
 
   const bool layer_tile = AB && (x0 < g.lo0 || x0 + S::TX > g.hi0 || z0 < g.lo1 || z0 + S::TZ > g.hi1);
   const T wc = g.wc, w1x = g.w1a, w1z = g.w1b, w2x = g.w2a, w2z = g.w2b;
-  const long long cbase = g.origin + (long long)xr * g.s0 + zc;  // owned cells of row k: + k*s0
+  const int ld = (int)g.s0;
+  const long long cbase = g.origin + (long long)xr * ld + zc;  // owned cells of row k: + k*ld
 
   for (int s = sb; s < se; ++s) {
-    const int buf = (s - sb) & 1;
-    if (s + 1 < se) {
-      issue(ph, a.cur + (long long)(s + 1) * g.field, sp + (buf ^ 1) * S::PS);
-      issue(pc, a.prev + (long long)(s + 1) * g.field, sq + (buf ^ 1) * S::QS);
+    const int buf = (s - sb) % NS;
+    {
+      const int sn = s + NS - 1, nb = (sn - sb) % NS;  // nb: the buffer shot s-1 used
+      if (sn < se) {
+        issue(ph, a.cur + (long long)sn * g.field, sp + nb * S::PS);
+        issue(pc, a.prev + (long long)sn * g.field, sq + nb * S::QS);
+      }
       cp_async_commit();
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
+      cp_async_wait<NS - 1>();
     }
     __syncthreads();
     const T* P = sp + buf * S::PS;
     const T* Q = sq + buf * S::QS;
 
-    if (a.traces) {  // receiver samples of p^n from the staged tile
-      const int e0 = a.tt.rec_ptr[tile], e1 = a.tt.rec_ptr[tile + 1];
-      for (int e = e0 + threadIdx.x; e < e1; e += 256) {
-        const int r = a.tt.rec_list[e];
-        const int row = a.tt.rec_corner[2 * r] - x0 + R, col = a.tt.rec_corner[2 * r + 1] - z0 + S::HL;
-        const T* w = a.rec_w + 4 * r;
-        T acc = T(0);
-        acc += w[0] * P[row * S::SW + col];
-        acc += w[1] * P[row * S::SW + col + 1];
-        acc += w[2] * P[(row + 1) * S::SW + col];
-        acc += w[3] * P[(row + 1) * S::SW + col + 1];
-        a.traces[((long long)s * a.n_rec + r) * a.n_t + a.j] = acc;
-      }
+    for (int e = e0 + threadIdx.x; e < e1; e += 256) {  // receiver samples of p^n from the tile
+      const int r = a.tt.rec_list[e];
+      const int row = a.tt.rec_corner[2 * r] - x0 + R, col = a.tt.rec_corner[2 * r + 1] - z0 + S::HL;
+      const T* w = a.rec_w + 4 * r;
+      T acc = T(0);
+      acc += w[0] * P[row * S::SW + col];
+      acc += w[1] * P[row * S::SW + col + 1];
+      acc += w[2] * P[(row + 1) * S::SW + col];
+      acc += w[3] * P[(row + 1) * S::SW + col + 1];
+      a.traces[((long long)s * a.n_rec + r) * a.n_t + a.j] = acc;
     }
     // the shot's source stencil, if it touches this tile (a CTA-uniform test)
     int bx = 0, bz = 0;
@@ -292,7 +315,8 @@ __global__ void __launch_bounds__(256, 3) fwd2d_tiled(KGrid<T> g, FwdTiled<T> a)
     T wv[2 * R + 1][VZ];
 #pragma unroll
     for (int q = 0; q < 2 * R; ++q) vload<T, VZ>(P + (lrow + q) * S::SW + S::HL + lane * VZ, wv[q]);
-    T* nx = a.next + (long long)s * g.field;
+    T* nx = a.next + (long long)s * g.field + cbase;
+    T* lx = a.lap_out ? a.lap_out + (long long)s * g.field + cbase : nullptr;
 #pragma unroll
     for (int k = 0; k < RX; ++k) {
       const int prow = lrow + k + R;  // shared row of the output row
@@ -302,24 +326,25 @@ __global__ void __launch_bounds__(256, 3) fwd2d_tiled(KGrid<T> g, FwdTiled<T> a)
 #pragma unroll
       for (int v = 0; v < VZ; ++v) rw.c[v] = wv[R][v];
       vload<T, VZ>(P + prow * S::SW + S::HL + lane * VZ + VZ, rw.r);
-      T pp[VZ];
+      T pp[VZ], cc[VZ];
       vload<T, VZ>(Q + (lrow + k) * S::TZ + lane * VZ, pp);
+      vload<T, VZ>(scc + (lrow + k) * S::TZ + lane * VZ, cc);
       const int x = xr + k;
       const bool ok = own_cols && x < g.n0;
-      T cc[VZ], ca[VZ], cb[VZ];
+      T ca[VZ], cb[VZ];
 #pragma unroll
-      for (int v = 0; v < VZ; ++v) { cc[v] = T(0); ca[v] = T(1); cb[v] = T(1); }
-      if (ok) vldg<T, VZ>(a.C + cbase + (long long)k * g.s0, cc);
+      for (int v = 0; v < VZ; ++v) { ca[v] = T(1); cb[v] = T(1); }
       if (layer_tile && ok) {
-        vldg<T, VZ>(a.A + cbase + (long long)k * g.s0, ca);
-        if (!a.b_one) vldg<T, VZ>(a.B + cbase + (long long)k * g.s0, cb);
+        vldg<T, VZ>(a.A + cbase + k * ld, ca);
+        if (!a.b_one) vldg<T, VZ>(a.B + cbase + k * ld, cb);
       }
-      T o[VZ];
+      T o[VZ], lp[VZ];
 #pragma unroll
       for (int v = 0; v < VZ; ++v) {
         const T c = wv[R][v];
         T lap = wc * c + w1x * (wv[R - 1][v] + wv[R + 1][v]) + w1z * (zval(rw, v - 1) + zval(rw, v + 1));
         if (R == 2) lap += w2x * (wv[0][v] + wv[4][v]) + w2z * (zval(rw, v - 2) + zval(rw, v + 2));
+        lp[v] = lap;
         o[v] = (T(2) * c - cb[v] * pp[v]) + cc[v] * lap;
       }
       if (src_tile) {
@@ -334,7 +359,8 @@ __global__ void __launch_bounds__(256, 3) fwd2d_tiled(KGrid<T> g, FwdTiled<T> a)
 #pragma unroll
         for (int v = 0; v < VZ; ++v) o[v] = ca[v] * o[v];
       }
-      if (ok) store_row<T, VZ>(nx + cbase + (long long)k * g.s0, o, zc, g.n1);
+      if (ok) store_row<T, VZ>(nx + k * ld, o, zc, g.n1);
+      if (lx && ok) store_row<T, VZ>(lx + k * ld, lp, zc, g.n1);
 #pragma unroll
       for (int q = 0; q < 2 * R; ++q)
 #pragma unroll
@@ -345,17 +371,19 @@ __global__ void __launch_bounds__(256, 3) fwd2d_tiled(KGrid<T> g, FwdTiled<T> a)
 }
 
 // ------------------------------------------------------------------------------------------
-// adjoint step: mu^n = A (R^T g_n + 2 mu1 + Lap(C mu1) - B mu2), grad += mu1 Lap(p^n)
+// adjoint step: mu^n = A (R^T g_n + 2 mu1 + Lap(C mu1) - B mu2), grad += mu1 Lap(p^n), where
+// Lap(p^n) is read back as the forward step stored it (no p halo, no second stencil)
 // ------------------------------------------------------------------------------------------
 template <typename T, int R, int VZ, int RX, bool AB>
 __global__ void __launch_bounds__(256, 2) adj2d_tiled(KGrid<T> g, AdjTiled<T> a) {
   using S = Tile2Shape<T, VZ, RX, R>;
+  constexpr int NS = S::NS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* sc = reinterpret_cast<T*>(smem_raw);  // [PS] C with halo
-  T* sm = sc + S::PS;                      // [2][PS] mu^{n+1} with halo
-  T* sn = sm + 2 * S::PS;                  // [2][PS] p^n with halo
-  T* s2 = sn + 2 * S::PS;                  // [2][QS] mu^{n+2}
-  T* sj = s2 + 2 * S::QS;                  // [QS] adjoint source of the current shot
+  T* sm = sc + S::PS;                      // [NS][PS] mu^{n+1} with halo
+  T* s2 = sm + NS * S::PS;                 // [NS][QS] mu^{n+2}
+  T* sl = s2 + NS * S::QS;                 // [NS][QS] Lap p^n
+  T* sj = sl + NS * S::QS;                 // [QS] adjoint source of the current shot
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int z0 = blockIdx.x * S::TZ, x0 = blockIdx.y * S::TX;
@@ -366,15 +394,22 @@ __global__ void __launch_bounds__(256, 2) adj2d_tiled(KGrid<T> g, AdjTiled<T> a)
   const int xr = x0 + warp * RX;
   const int lrow = warp * RX;
   const bool own_cols = zc < g.n1;
-  const bool grad = a.p != nullptr;
+  const bool grad = a.lap != nullptr;
 
   const CopyPlan<S::NCH> ph = plan_halo<T, VZ, RX, R>(g, x0, z0);
   const CopyPlan<S::NCC> pc = plan_core<T, VZ, RX, R>(g, x0, z0);
+  wait_previous_grid();
+  allow_next_grid();
   issue(ph, a.C, sc);
-  issue(ph, a.mu1 + (long long)sb * g.field, sm);
-  if (grad) issue(ph, a.p + (long long)sb * g.field, sn);
-  issue(pc, a.mu2 + (long long)sb * g.field, s2);
-  cp_async_commit();
+#pragma unroll
+  for (int i = 0; i < NS - 1; ++i) {  // one commit group per shot, empty ones included
+    if (sb + i < se) {
+      issue(ph, a.mu1 + (long long)(sb + i) * g.field, sm + i * S::PS);
+      issue(pc, a.mu2 + (long long)(sb + i) * g.field, s2 + i * S::QS);
+      if (grad) issue(pc, a.lap + (long long)(sb + i) * g.field, sl + i * S::QS);
+    }
+    cp_async_commit();
+  }
 
   const int c0 = a.gtr ? a.tt.cell_ptr[tile] : 0, c1 = a.gtr ? a.tt.cell_ptr[tile + 1] : 0;
   const bool inject = c1 > c0;  // uniform
@@ -386,7 +421,8 @@ __global__ void __launch_bounds__(256, 2) adj2d_tiled(KGrid<T> g, AdjTiled<T> a)
   const bool layer_tile = AB && (x0 < g.lo0 || x0 + S::TX > g.hi0 || z0 < g.lo1 || z0 + S::TZ > g.hi1);
   const bool use_a = layer_tile && a.apply_a;
   const T wc = g.wc, w1x = g.w1a, w1z = g.w1b, w2x = g.w2a, w2z = g.w2b;
-  const long long cbase = g.origin + (long long)xr * g.s0 + zc;
+  const int ld = (int)g.s0;
+  const long long cbase = g.origin + (long long)xr * ld + zc;
   // per-cell sum over this CTA's shots: float for float fields, double for double fields
   using Acc = typename std::conditional<sizeof(T) == 8, double, float>::type;
   Acc gsum[RX][VZ];
@@ -396,15 +432,16 @@ __global__ void __launch_bounds__(256, 2) adj2d_tiled(KGrid<T> g, AdjTiled<T> a)
     for (int v = 0; v < VZ; ++v) gsum[k][v] = Acc(0);
 
   for (int s = sb; s < se; ++s) {
-    const int buf = (s - sb) & 1;
-    if (s + 1 < se) {
-      issue(ph, a.mu1 + (long long)(s + 1) * g.field, sm + (buf ^ 1) * S::PS);
-      if (grad) issue(ph, a.p + (long long)(s + 1) * g.field, sn + (buf ^ 1) * S::PS);
-      issue(pc, a.mu2 + (long long)(s + 1) * g.field, s2 + (buf ^ 1) * S::QS);
+    const int buf = (s - sb) % NS;
+    {
+      const int sn = s + NS - 1, nb = (sn - sb) % NS;  // nb: the buffer shot s-1 used
+      if (sn < se) {
+        issue(ph, a.mu1 + (long long)sn * g.field, sm + nb * S::PS);
+        issue(pc, a.mu2 + (long long)sn * g.field, s2 + nb * S::QS);
+        if (grad) issue(pc, a.lap + (long long)sn * g.field, sl + nb * S::QS);
+      }
       cp_async_commit();
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
+      cp_async_wait<NS - 1>();
     }
     if (inject) {  // adjoint source of shot s: each touched cell summed in table order
       const T* gs = a.gtr + (long long)s * a.n_rec * a.n_t + a.j;
@@ -418,11 +455,10 @@ __global__ void __launch_bounds__(256, 2) adj2d_tiled(KGrid<T> g, AdjTiled<T> a)
     }
     __syncthreads();
     const T* M = sm + buf * S::PS;
-    const T* PN = sn + buf * S::PS;
     const T* M2 = s2 + buf * S::QS;
+    const T* LP = sl + buf * S::QS;
 
     T qv[2 * R + 1][VZ];  // C * mu1, own columns
-    T pv[2 * R + 1][VZ];  // p^n, own columns
 #pragma unroll
     for (int q = 0; q < 2 * R; ++q) {
       T tm[VZ], tc[VZ];
@@ -431,9 +467,8 @@ __global__ void __launch_bounds__(256, 2) adj2d_tiled(KGrid<T> g, AdjTiled<T> a)
       vload<T, VZ>(sc + off, tc);
 #pragma unroll
       for (int v = 0; v < VZ; ++v) qv[q][v] = tc[v] * tm[v];
-      if (grad) vload<T, VZ>(PN + off, pv[q]);
     }
-    T* ob = a.out + (long long)s * g.field;
+    T* ob = a.out + (long long)s * g.field + cbase;
 #pragma unroll
     for (int k = 0; k < RX; ++k) {
       const int prow = lrow + k + R;
@@ -444,7 +479,6 @@ __global__ void __launch_bounds__(256, 2) adj2d_tiled(KGrid<T> g, AdjTiled<T> a)
         vload<T, VZ>(sc + off, tc);
 #pragma unroll
         for (int v = 0; v < VZ; ++v) qv[2 * R][v] = tc[v] * tm[v];
-        if (grad) vload<T, VZ>(PN + off, pv[2 * R]);
       }
       const int coff = prow * S::SW + S::HL + lane * VZ;
       Row3<T, VZ> qw;
@@ -463,13 +497,6 @@ __global__ void __launch_bounds__(256, 2) adj2d_tiled(KGrid<T> g, AdjTiled<T> a)
 #pragma unroll
         for (int v = 0; v < VZ; ++v) qw.c[v] = qv[R][v];
       }
-      Row3<T, VZ> pw;
-      if (grad) {
-        vload<T, VZ>(PN + coff - VZ, pw.l);
-        vload<T, VZ>(PN + coff + VZ, pw.r);
-#pragma unroll
-        for (int v = 0; v < VZ; ++v) pw.c[v] = pv[R][v];
-      }
       T m2[VZ];
       vload<T, VZ>(M2 + (lrow + k) * S::TZ + lane * VZ, m2);
       const int x = xr + k;
@@ -478,8 +505,8 @@ __global__ void __launch_bounds__(256, 2) adj2d_tiled(KGrid<T> g, AdjTiled<T> a)
 #pragma unroll
       for (int v = 0; v < VZ; ++v) { ca[v] = T(1); cb[v] = T(1); }
       if (layer_tile && ok) {
-        vldg<T, VZ>(a.A + cbase + (long long)k * g.s0, ca);
-        vldg<T, VZ>(a.B + cbase + (long long)k * g.s0, cb);
+        vldg<T, VZ>(a.A + cbase + k * ld, ca);
+        vldg<T, VZ>(a.B + cbase + k * ld, cb);
       }
       T o[VZ];
 #pragma unroll
@@ -499,32 +526,27 @@ __global__ void __launch_bounds__(256, 2) adj2d_tiled(KGrid<T> g, AdjTiled<T> a)
         for (int v = 0; v < VZ; ++v) o[v] = ca[v] * o[v];
       }
       if (grad) {
+        T lp[VZ];
+        vload<T, VZ>(LP + (lrow + k) * S::TZ + lane * VZ, lp);
 #pragma unroll
-        for (int v = 0; v < VZ; ++v) {
-          T lp = wc * pv[R][v] + w1x * (pv[R - 1][v] + pv[R + 1][v]) + w1z * (zval(pw, v - 1) + zval(pw, v + 1));
-          if (R == 2) lp += w2x * (pv[0][v] + pv[4][v]) + w2z * (zval(pw, v - 2) + zval(pw, v + 2));
-          gsum[k][v] += (Acc)(mc[v] * lp);
-        }
+        for (int v = 0; v < VZ; ++v) gsum[k][v] += (Acc)(mc[v] * lp[v]);
       }
-      if (ok) store_row<T, VZ>(ob + cbase + (long long)k * g.s0, o, zc, g.n1);
+      if (ok) store_row<T, VZ>(ob + k * ld, o, zc, g.n1);
 #pragma unroll
       for (int q = 0; q < 2 * R; ++q)
 #pragma unroll
-        for (int v = 0; v < VZ; ++v) {
-          qv[q][v] = qv[q + 1][v];
-          if (grad) pv[q][v] = pv[q + 1][v];
-        }
+        for (int v = 0; v < VZ; ++v) qv[q][v] = qv[q + 1][v];
     }
     __syncthreads();
     if (inject)  // the same threads clear the cells they set, before the next shot sets them again
       for (int e = c0 + threadIdx.x; e < c1; e += 256) sj[a.tt.cell_local[e]] = T(0);
   }
   if (grad && own_cols) {
-    double* gp = a.gacc + (long long)blockIdx.z * g.field;
+    double* gp = a.gacc + (long long)blockIdx.z * g.field + cbase;
 #pragma unroll
     for (int k = 0; k < RX; ++k) {
       if (xr + k >= g.n0) continue;
-      double* dst = gp + cbase + (long long)k * g.s0;
+      double* dst = gp + k * ld;
 #pragma unroll
       for (int v = 0; v < VZ; ++v)
         if (zc + v < g.n1) dst[v] += (double)gsum[k][v];

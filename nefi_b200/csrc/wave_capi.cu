@@ -227,12 +227,12 @@ int n_groups(const nw_grid* g, const Tune& t, int n_shots) {
 template <typename T, int R, int VZ, int RX>
 constexpr size_t fwd2_smem() {
   using S = nw::Tile2Shape<T, VZ, RX, R>;
-  return (2 * S::PS + 2 * S::QS) * sizeof(T);
+  return (S::QS + S::NS * (S::PS + S::QS)) * sizeof(T);
 }
 template <typename T, int R, int VZ, int RX>
 constexpr size_t adj2_smem() {
   using S = nw::Tile2Shape<T, VZ, RX, R>;
-  return (5 * S::PS + 3 * S::QS) * sizeof(T);
+  return (S::PS + S::NS * (S::PS + 2 * S::QS) + S::QS) * sizeof(T);
 }
 constexpr size_t kMaxSmem = 227 * 1024;  // opt-in shared memory per CTA on sm_100a
 
@@ -242,6 +242,25 @@ int allow_smem(K kernel, size_t bytes, bool* done) {
   if (*done || bytes <= 48 * 1024) return NW_OK;
   NW_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
   *done = true;
+  return NW_OK;
+}
+
+// Launch a step kernel that may begin while the previous kernel in the stream finishes: the
+// kernel waits (griddepcontrol.wait) for that kernel's writes before it reads any field.
+template <typename K, typename... Args>
+int launch_pdl(K kernel, dim3 grid, size_t smem, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3(256, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  NW_CUDA(cudaLaunchKernelEx(&cfg, kernel, args...));
+  NW_LAUNCHED();
   return NW_OK;
 }
 
@@ -269,9 +288,7 @@ int launch_fwd2_v(const nw_grid* g, const nw::KGrid<T>& kg, const nw::FwdTiled<T
   int rc = allow_smem(nw::fwd2d_tiled<T, R, VZ, RX, AB>, smem, &done);
   if (rc) return rc;
   dim3 grid((g->n[1] + S::TZ - 1) / S::TZ, (g->n[0] + S::TX - 1) / S::TX, (st.n_shots + t.spc - 1) / t.spc);
-  nw::fwd2d_tiled<T, R, VZ, RX, AB><<<grid, 256, smem, s>>>(kg, st);
-  NW_LAUNCHED();
-  return NW_OK;
+  return launch_pdl(nw::fwd2d_tiled<T, R, VZ, RX, AB>, grid, smem, s, kg, st);
 }
 template <typename T, int R, int VZ, int RX, bool AB>
 int launch_adj2_v(const nw_grid* g, const nw::KGrid<T>& kg, const nw::AdjTiled<T>& st, const Tune& t,
@@ -283,9 +300,7 @@ int launch_adj2_v(const nw_grid* g, const nw::KGrid<T>& kg, const nw::AdjTiled<T
   int rc = allow_smem(nw::adj2d_tiled<T, R, VZ, RX, AB>, smem, &done);
   if (rc) return rc;
   dim3 grid((g->n[1] + S::TZ - 1) / S::TZ, (g->n[0] + S::TX - 1) / S::TX, (st.n_shots + t.adj_spc - 1) / t.adj_spc);
-  nw::adj2d_tiled<T, R, VZ, RX, AB><<<grid, 256, smem, s>>>(kg, st);
-  NW_LAUNCHED();
-  return NW_OK;
+  return launch_pdl(nw::adj2d_tiled<T, R, VZ, RX, AB>, grid, smem, s, kg, st);
 }
 
 // Runtime (radius, vz, rx, absorbing) -> template instantiation.
@@ -317,28 +332,25 @@ int launch_adj2_v(const nw_grid* g, const nw::KGrid<T>& kg, const nw::AdjTiled<T
 
 // ---- forward driver ---------------------------------------------------------------------
 template <typename T>
-struct Levels {  // address of time level n (n >= -1) in history, ring or segment buffer
+struct Ring {  // time level n (n >= -1) of the pressure field: three rotating levels
   T* base;
   long long level_elems;
-  int mode;  // 0 history, 1 ring, 2 segment (offset n0)
-  int n0;
-  T* at(int n) const {
-    if (mode == 0) return base + (long long)(n + 1) * level_elems;
-    if (mode == 1) return base + (long long)((n + 1) % 3) * level_elems;
-    return base + (long long)(n - n0 + 1) * level_elems;
-  }
+  T* at(int n) const { return base + (long long)((n + 1) % 3) * level_elems; }
 };
 
-// One forward step n for all shots (traces != NULL: also sample level n if it is a record step).
+// One forward step n for all shots (traces != NULL: also sample level n if it is a record step;
+// lap_out != NULL: also store Lap p^n there, the factor of the step's velocity gradient term).
 template <typename T>
 int forward_step(const nw_grid* g, const nw::KGrid<T>& kg, const nw_medium* m, const nw_acquisition* a,
-                 const nw_time* t, const Tune& tu, const Levels<T>& L, int n, T* traces, cudaStream_t s) {
+                 const nw_time* t, const Tune& tu, const Ring<T>& L, int n, T* traces, T* lap_out,
+                 cudaStream_t s) {
   const bool rec = traces && a->n_rec > 0 && (n % t->substeps) == 0;
   if (g->ndim == 2) {
     nw::FwdTiled<T> st;
     st.prev = L.at(n - 1);
     st.cur = L.at(n);
     st.next = L.at(n + 1);
+    st.lap_out = lap_out;
     st.C = (const T*)m->c2dt2;
     st.A = (const T*)m->coef_a;
     st.B = (const T*)m->coef_b;
@@ -361,6 +373,7 @@ int forward_step(const nw_grid* g, const nw::KGrid<T>& kg, const nw_medium* m, c
   st.prev = L.at(n - 1);
   st.cur = L.at(n);
   st.next = L.at(n + 1);
+  st.lap_out = lap_out;
   st.C = (const T*)m->c2dt2;
   st.A = (const T*)m->coef_a;
   st.B = (const T*)m->coef_b;
@@ -392,12 +405,10 @@ template <typename T>
 int forward_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, const nw_time* t,
                  const nw_storage* st, const Tune& tu, int n_begin, int n_end, T* traces, cudaStream_t s) {
   const long long LE = (long long)a->n_shots * g->field_elems;
-  Levels<T> L;
+  if (!st->ring) return fail(NW_ERR_ARG, "storage needs a ring buffer");
+  Ring<T> L;
+  L.base = (T*)st->ring;
   L.level_elems = LE;
-  L.n0 = 0;
-  if (st->history) { L.base = (T*)st->history; L.mode = 0; }
-  else if (st->ring) { L.base = (T*)st->ring; L.mode = 1; }
-  else return fail(NW_ERR_ARG, "storage needs a history or a ring buffer");
   const bool ckpt = !st->history && st->snap;
   if (ckpt && st->segment < 1) return fail(NW_ERR_ARG, "segment must be >= 1");
   const nw::KGrid<T> kg = kgrid<T>(g);
@@ -406,7 +417,8 @@ int forward_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
       int rc = snap_store<T>(g, st, a->n_shots, L.at(n - 1), L.at(n), n / st->segment, s);
       if (rc) return rc;
     }
-    int rc = forward_step<T>(g, kg, m, a, t, tu, L, n, traces, s);
+    T* lap = st->history ? (T*)st->history + (long long)n * LE : nullptr;
+    int rc = forward_step<T>(g, kg, m, a, t, tu, L, n, traces, lap, s);
     if (rc) return rc;
   }
   if (traces && n_end == t->n_steps && t->n_steps % t->substeps == 0) {
@@ -433,16 +445,12 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
   const bool ckpt = !hist && st->snap != nullptr;
   if (!hist && !ckpt && N > 0) return fail(NW_ERR_ARG, "adjoint needs a history or snapshots");
   const int K = ckpt ? st->segment : 0;
-  Levels<T> H;
-  H.level_elems = LE;
-  H.mode = 0;
-  H.n0 = 0;
-  H.base = hist ? (T*)st->history : nullptr;
-  Levels<T> SEG;
-  SEG.level_elems = LE;
-  SEG.mode = 2;
-  SEG.base = ckpt ? (T*)st->segbuf : nullptr;
-  SEG.n0 = -1;
+  if (ckpt && (K < 1 || !st->ring || !st->segbuf))
+    return fail(NW_ERR_ARG, "snapshots need a ring, a segment buffer and segment >= 1");
+  Ring<T> L;  // the pressure levels of the segment being recomputed
+  L.base = (T*)st->ring;
+  L.level_elems = LE;
+  int seg_n0 = -1;  // first step of the segment whose Lap p levels the segment buffer holds
   const int n_stop = lambda0 ? 0 : 1;
   dim3 ig(((a->n_cells > 0 ? a->n_cells : 1) + 127) / 128, S);
   auto inject3 = [&](int n) -> int {  // 3-D: separate adjoint-source kernel
@@ -453,7 +461,7 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
     NW_LAUNCHED();
     return NW_OK;
   };
-  auto step2 = [&](int n, const T* pn) -> int {  // 2-D: one fused tiled launch
+  auto step2 = [&](int n, const T* lap) -> int {  // 2-D: one fused tiled launch
     nw::AdjTiled<T> as;
     as.mu1 = mu(n + 1);
     as.mu2 = mu(n + 2);
@@ -462,7 +470,7 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
     as.A = (const T*)m->coef_a;
     as.B = (const T*)m->coef_b;
     as.apply_a = n >= 1 ? 1 : 0;
-    as.p = pn;
+    as.lap = lap;
     as.gacc = gacc;
     as.n_shots = S;
     as.shots_per_cta = tu.adj_spc;
@@ -479,25 +487,25 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
     if (rc) return rc;
   }
   for (int n = N - 1; n >= n_stop; --n) {
-    const T* pn;
+    const T* lap;
     if (hist) {
-      pn = H.at(n);
+      lap = (const T*)st->history + (long long)n * LE;
     } else {
       const int n0 = (n / K) * K;
-      if (SEG.n0 != n0) {  // entering a segment from its end: recompute p^{n0..n1-1}
+      if (seg_n0 != n0) {  // entering a segment from its end: recompute Lap p^{n0..n1-1}
         const int n1 = std::min(n0 + K, N);
-        SEG.n0 = n0;
-        int rc = snap_load<T>(g, st, S, n0 / K, SEG.at(n0 - 1), SEG.at(n0), s);
+        seg_n0 = n0;
+        int rc = snap_load<T>(g, st, S, n0 / K, L.at(n0 - 1), L.at(n0), s);
         if (rc) return rc;
-        for (int k = n0; k < n1 - 1; ++k) {
-          rc = forward_step<T>(g, kg, m, a, t, tu, SEG, k, nullptr, s);
+        for (int k = n0; k < n1; ++k) {
+          rc = forward_step<T>(g, kg, m, a, t, tu, L, k, nullptr, (T*)st->segbuf + (long long)(k - n0) * LE, s);
           if (rc) return rc;
         }
       }
-      pn = SEG.at(n);
+      lap = (const T*)st->segbuf + (long long)(n - n0) * LE;
     }
     if (g->ndim == 2) {
-      int rc = step2(n, pn);
+      int rc = step2(n, lap);
       if (rc) return rc;
       continue;
     }
@@ -509,7 +517,7 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
     as.A = (const T*)m->coef_a;
     as.B = (const T*)m->coef_b;
     as.apply_a = n >= 1 ? 1 : 0;
-    as.p = pn;
+    as.lap = lap;
     as.grad = gacc;
     Shape sh = stencil_shape(g, S);
     if (g->radius == 1) {

@@ -177,33 +177,30 @@ class _Run:
         self.kind = mode[0]
         self.storage = _lib.Storage()
         self.history = self.ring = self.snap = self.segbuf = None
+        # the pressure advances through three rotating levels in every mode
+        self.ring = plan.empty_levels(3, n_shots)
+        self.storage.ring = self.ring.data_ptr()
         if self.kind == "history":
-            # every step overwrites the interior of its level: zero only levels -1, 0 and the ghosts
-            self.history = plan.empty_levels(n_steps + 2, n_shots, zero=False)
-            self.history[:2].zero_()
+            # step n stores Lap p^n into the interior of level n; the ghosts are zeroed once
+            self.history = plan.empty_levels(n_steps, n_shots, zero=False)
             if n_steps > 0:
-                _lib.check(_lib.load().nw_zero_ghosts(C.byref(plan.g), self.history[2:].data_ptr(),
+                _lib.check(_lib.load().nw_zero_ghosts(C.byref(plan.g), self.history.data_ptr(),
                                                       n_steps * n_shots, _lib.stream_handle(plan.device)))
             self.storage.history = self.history.data_ptr()
-        else:
-            self.ring = plan.empty_levels(3, n_shots)
-            self.storage.ring = self.ring.data_ptr()
-            if self.kind == "checkpoint":
-                k = int(mode[1])
-                kind = _lib.SNAP_KINDS[snapshot]
-                n_snap = -(-n_steps // k) if n_steps > 0 else 1
-                nbytes = plan.snapshot_bytes(n_shots, n_snap, kind)
-                self.snap = torch.empty(nbytes, dtype=torch.uint8, device=plan.device)
-                self.segbuf = plan.empty_levels(k + 1, n_shots)
-                self.storage.snap = self.snap.data_ptr()
-                self.storage.segbuf = self.segbuf.data_ptr()
-                self.storage.segment = k
-                self.storage.snap_kind = kind
+        elif self.kind == "checkpoint":
+            k = int(mode[1])
+            kind = _lib.SNAP_KINDS[snapshot]
+            n_snap = -(-n_steps // k) if n_steps > 0 else 1
+            nbytes = plan.snapshot_bytes(n_shots, n_snap, kind)
+            self.snap = torch.empty(nbytes, dtype=torch.uint8, device=plan.device)
+            self.segbuf = plan.empty_levels(k, n_shots)
+            self.storage.snap = self.snap.data_ptr()
+            self.storage.segbuf = self.segbuf.data_ptr()
+            self.storage.segment = k
+            self.storage.snap_kind = kind
 
     def level(self, n: int) -> torch.Tensor:
-        """Time level ``n`` (``(n_shots, field)``) while it is resident."""
-        if self.history is not None:
-            return self.history[n + 1]
+        """Pressure level ``n`` (``(n_shots, field)``) while it is in the ring."""
         return self.ring[(n + 1) % 3]
 
     def release(self) -> None:

@@ -238,7 +238,7 @@ def plan_storage(plan: DevicePlan, n_shots: int, n_steps: int, grad_mode: str,
     budget.
     """
     lvl = plan.level_bytes(n_shots)
-    hist = (n_steps + 2) * lvl
+    hist = (n_steps + 3) * lvl  # n_steps Lap p levels and the pressure ring
     if grad_mode == "autograd" and (budget is None or hist <= budget):
         return ("history", None)
     kind = _lib.SNAP_KINDS[snapshot]
@@ -247,7 +247,7 @@ def plan_storage(plan: DevicePlan, n_shots: int, n_steps: int, grad_mode: str,
     k = max(1, int(math.ceil(math.sqrt(max(1, n_steps)))))
     if budget is not None:
         def cost(k_):
-            return plan.snapshot_bytes(n_shots, -(-n_steps // k_), kind) + (k_ + 4) * lvl
+            return plan.snapshot_bytes(n_shots, -(-n_steps // k_), kind) + (k_ + 3) * lvl
         best = min(range(1, n_steps + 1), key=cost) if n_steps < 20000 else k
         if cost(k) > budget:
             k = best
