@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define NW_ABI_VERSION 2
+#define NW_ABI_VERSION 3
 
 /* scalar type of a computation */
 enum { NW_F32 = 0, NW_F64 = 1 };
@@ -206,21 +206,24 @@ int nw_forward(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, co
 /*
  * Adjoint run for all shots: from trace cotangents `grad_traces` (n_shots, n_rec, n_t) computes
  *  - grad_acc: nw_adjoint_groups() float64 fields (zeroed by the call) whose sum is
- *    sum_shots sum_n mu^{n+1} * Lap p^n, the gradient w.r.t. c2dt2, and
+ *    c2dt2 * sum_shots sum_n mu^{n+1} * Lap p^n, i.e. c2dt2 times the gradient w.r.t. c2dt2
+ *    (nw_reduce_grad_c divides the factor out), and
  *  - lambda0 / mu1 (n_shots fields each, may be NULL): the sensitivities of p^0 and A*p^1
  *    needed by the initial-value operator.
- * `work` holds three adjoint levels (3 * n_shots fields). Uses the history or recomputes
- * segments from the snapshots in `st`. This is the discrete adjoint torch.autograd derives from
- * nefi/physics/wave.py:529-552 and nefi/physics/timestep.py:151-169.
+ * The steps advance q = c2dt2 * mu, which obeys the forward recursion with the source replaced
+ * by c2dt2 * R^T g_n; `work` holds three q levels (3 * n_shots fields). Uses the history or
+ * recomputes segments from the snapshots in `st`. This is the discrete adjoint torch.autograd
+ * derives from nefi/physics/wave.py:529-552 and nefi/physics/timestep.py:151-169.
  */
 int nw_adjoint(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, const nw_time* t,
                const nw_storage* st, const nw_tuning* tune, const void* grad_traces, void* work,
                double* grad_acc, void* lambda0, void* mu1, void* stream);
 
 /*
- * Reduce gradient accumulators (n_acc float64 fields) and apply the chain rule of
- * c2dt2 = pad_replicate(c)^2 dt^2: grad_c (physical grid, float64) =
- * pad_replicate^T(2 c_pad dt2 * sum_acc g) (nefi/physics/wave.py:231-240, 718).
+ * Reduce gradient accumulators (n_acc float64 fields holding c2dt2 * dJ/dc2dt2, as nw_adjoint
+ * leaves them) and apply the chain rule of c2dt2 = pad_replicate(c)^2 dt^2: grad_c (physical
+ * grid, float64) = pad_replicate^T(2 c_pad dt2 * sum_acc g / (c_pad^2 dt2))
+ * (nefi/physics/wave.py:231-240, 718).
  * `accumulate` != 0 adds into grad_c instead of overwriting it.
  */
 int nw_reduce_grad_c(const nw_grid* g, const int32_t* n_abs, const void* c, double dt2,
@@ -231,8 +234,8 @@ int nw_reduce_grad_c(const nw_grid* g, const int32_t* n_abs, const void* c, doub
  * Gradient of the initial-value operator w.r.t. p0 (n_shots physical fields, dtype):
  * lambda^0 + lambda^-1 + Lap(1/2 c2dt2 lambda^-1) cropped to the physical grid, with
  * lambda^-1 = -B0 mu^1 (B0 = 1 when time.first_b_one). If grad_acc != NULL also adds
- * 1/2 lambda^-1 * Lap p^0 of shot s to accumulator s / shots_per_acc (the c-dependence of p^-1,
- * nefi/physics/wave.py:850).
+ * c2dt2 * 1/2 lambda^-1 * Lap p^0 of shot s to accumulator s / shots_per_acc (the c-dependence
+ * of p^-1, nefi/physics/wave.py:850, in the accumulators' c2dt2-scaled convention).
  */
 int nw_initial_state_adjoint(const nw_grid* g, const int32_t* n_abs, const nw_medium* m,
                              const nw_time* t, int32_t n_shots, const void* lambda0,

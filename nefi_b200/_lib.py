@@ -13,7 +13,7 @@ from pathlib import Path
 import torch
 
 LIB_PATH = Path(__file__).resolve().parent / "libnefiwave.so"
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 NW_F32, NW_F64 = 0, 1
 NW_ABS_NONE, NW_ABS_SPONGE, NW_ABS_CERJAN = 0, 1, 2

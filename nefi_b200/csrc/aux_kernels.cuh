@@ -108,9 +108,26 @@ __global__ void initial_prev_kernel(KGrid<T> g, int ndim, const T* __restrict__ 
   }
 }
 
+// mu = q / C on the padded grid of shot blockIdx.y (q = C mu is the variable the adjoint steps
+// advance). Ghost cells are left untouched (the caller zeroes them).
+template <typename T>
+__global__ void unscale_kernel(KGrid<T> g, int ndim, const T* __restrict__ C, const T* __restrict__ q,
+                               T* __restrict__ out) {
+  const long long so = (long long)blockIdx.y * g.field;
+  const long long cells = (long long)g.n0 * g.n1 * g.n2;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < cells;
+       t += (long long)gridDim.x * blockDim.x) {
+    int x, y, z;
+    cell_of(t, g.n0, g.n1, g.n2, ndim, x, y, z);
+    const long long i = ghost_index(g, ndim, x, y, z);
+    out[so + i] = q[so + i] / C[i];
+  }
+}
+
 // Adjoint of the initial state: lambda^-1 = -B0 mu^1,
 // grad_p0p = lambda^0 + lambda^-1 + Lap(0.5 C lambda^-1), cropped to the physical grid;
-// optionally acc[s / spa] += 0.5 lambda^-1 Lap p^0. blockIdx.y is an accumulator group whose
+// optionally acc[s / spa] += C * 0.5 lambda^-1 Lap p^0 (the accumulators hold C dJ/dC, as the
+// adjoint steps leave them). blockIdx.y is an accumulator group whose
 // shots a thread visits in order, so no two threads add into the same accumulator cell.
 template <typename T, int R>
 __global__ void initial_adjoint_kernel(KGrid<T> g, PadMap pm, int ndim, const T* __restrict__ C,
@@ -140,7 +157,7 @@ __global__ void initial_adjoint_kernel(KGrid<T> g, PadMap pm, int ndim, const T*
       };
       auto hl = [&](long long k) -> T { return (T(0.5) * C[k]) * lm1(k); };
       const T l = lm1(i);
-      if (ga) ga[i] += (double)((T(0.5) * l) * lap_at<T, R>(g, p0 + so, i, ndim));
+      if (ga) ga[i] += (double)(C[i] * ((T(0.5) * l) * lap_at<T, R>(g, p0 + so, i, ndim)));
       if (!phys) continue;
       T lh;
       if (ndim == 2) {
@@ -159,7 +176,7 @@ __global__ void initial_adjoint_kernel(KGrid<T> g, PadMap pm, int ndim, const T*
   }
 }
 
-// grad_c[phys] (+)= 2 c dt2 * sum_acc sum_{padded cells -> phys} g_acc[cell], in float64.
+// grad_c[phys] (+)= 2 c dt2 * dJ/dC, dJ/dC = sum_acc sum_{padded cells -> phys} g_acc[cell] / C, in float64.
 template <typename T>
 __global__ void reduce_grad_kernel(KGrid<T> g, PadMap pm, int ndim, const T* __restrict__ c,
                                    double dt2, int n_acc, const double* __restrict__ gs,
@@ -183,7 +200,9 @@ __global__ void reduce_grad_kernel(KGrid<T> g, PadMap pm, int ndim, const T* __r
         for (int y = y0; y <= y1; ++y)
           for (int z = z0; z <= z1; ++z) acc += gp[ghost_index(g, ndim, x, y, z)];
     }
-    const double v = 2.0 * (double)c[t] * dt2 * acc;
+    // acc = C dJ/dC summed over the padded cells that replicate c[t], all with C = c^2 dt^2
+    const double cd = (double)c[t];
+    const double v = 2.0 * cd * dt2 * (acc / (cd * cd * dt2));
     out[t] = accumulate ? out[t] + v : v;
   }
 }

@@ -5,6 +5,9 @@
 // with A = B = 1 outside the absorbing layer. Its exact discrete adjoint, with mu^n = A lambda^n:
 //   mu^n = A * ( R^T g_n + 2 mu^{n+1} + Lap(C mu^{n+1}) - B mu^{n+2} ),
 //   dJ/dC += mu^{n+1} * Lap(p^n), with Lap(p^n) stored by the forward step that computed it.
+// The kernels advance q = C mu instead, which obeys the forward's own recursion
+//   q^n = A * ( 2 q^{n+1} - B q^{n+2} + C * Lap(q^{n+1}) + C R^T g_n ),
+// so one stencil serves both directions, and accumulate C dJ/dC = sum_n q^{n+1} Lap(p^n).
 // Fields live in the ghost layout (see nw_grid in include/nefi_wave.h): every neighbour read is
 // in bounds and reads zero outside the padded grid, so the stencils carry no boundary branches.
 #pragma once
@@ -28,40 +31,30 @@ struct KGrid {
   T w2a, w2b, w2c;          // +-2 per axis (order 4)
 };
 
-// Everything one forward step reads and writes.
+// Everything one 3-D step reads and writes: forward (p) or adjoint (q = C mu), as in step2d.
 template <typename T>
-struct FwdStep {
-  const T* __restrict__ prev;   // level n-1 (shot 0); shots follow at +field
-  const T* __restrict__ cur;    // level n
-  T* __restrict__ next;         // level n+1
+struct Step3 {
+  const T* __restrict__ prev;   // forward p^{n-1} | adjoint q^{n+2} (shot 0; shots follow at +field)
+  const T* __restrict__ cur;    // forward p^n     | adjoint q^{n+1}
+  T* __restrict__ next;         // forward p^{n+1} | adjoint q^n
   const T* __restrict__ C;      // c^2 dt^2
   const T* __restrict__ A;      // absorbing coefficients or nullptr
   const T* __restrict__ B;
-  int b_one;                    // use B = 1 on the previous level (first Cerjan step)
-  // source: one multilinear stencil per shot
+  int b_one;                    // forward: use B = 1 on the previous level (first Cerjan step)
+  int apply_a;                  // adjoint: A applies (n >= 1)
+  // forward source: one multilinear stencil per shot
   const int* __restrict__ src_corner;  // (shots, ndim) or nullptr
   const T* __restrict__ src_w;         // (shots, 2^ndim)
   const T* __restrict__ wavelet;       // (n_steps,)
   int n;                               // step index
-  // receivers sampled from level n when `traces` != nullptr
+  // forward receivers sampled from level n when `traces` != nullptr
   T* __restrict__ traces;              // (shots, n_rec, n_t)
   const int64_t* __restrict__ rec_idx;
   const T* __restrict__ rec_w;
   int n_rec, n_t, j;
-  T* __restrict__ lap_out;             // non-null: also store Lap p^n (the gradient factor)
-};
-
-template <typename T>
-struct AdjStep {
-  const T* __restrict__ mu1;    // mu^{n+1}
-  const T* __restrict__ mu2;    // mu^{n+2}
-  T* __restrict__ out;          // mu^n (or lambda^0 when apply_a == 0)
-  const T* __restrict__ C;
-  const T* __restrict__ A;
-  const T* __restrict__ B;
-  int apply_a;
-  const T* __restrict__ lap;    // Lap p^n as the forward step stored it (nullptr: no gradient term)
-  double* __restrict__ grad;    // per-shot float64 dJ/dC accumulators
+  T* __restrict__ lap_out;             // forward, non-null: also store Lap p^n (the gradient factor)
+  const T* __restrict__ lap;           // adjoint: Lap p^n as the forward stored it (nullptr: no gradient)
+  double* __restrict__ grad;           // adjoint: per-shot float64 accumulators of C dJ/dC
 };
 
 __device__ __forceinline__ long long global_thread_in_shot() {
@@ -100,12 +93,12 @@ __device__ __forceinline__ Tile3 tile3(int n2, int RX) {
   return t;
 }
 
-template <typename T, int R, bool AB, int RX>
-__global__ void __launch_bounds__(256) fwd3d(KGrid<T> g, FwdStep<T> a) {
+template <typename T, int R, bool AB, int RX, bool ADJ>
+__global__ void __launch_bounds__(256) step3d(KGrid<T> g, Step3<T> a) {
   const int s = blockIdx.z;
   const long long so = (long long)s * g.field;
   const T* __restrict__ pc = a.cur + so;
-  if (a.traces) gather_receivers<T, 8>(pc, a.traces, a.rec_idx, a.rec_w, a.n_rec, a.n_t, a.j, s);
+  if (!ADJ && a.traces) gather_receivers<T, 8>(pc, a.traces, a.rec_idx, a.rec_w, a.n_rec, a.n_t, a.j, s);
   const Tile3 t = tile3(g.n2, RX);
   if (t.z >= g.n2 || t.y >= g.n1 || t.x0 >= g.n0) return;
   const long long base = g.origin + (long long)t.x0 * g.s0 + (long long)t.y * g.s1 + t.z;
@@ -120,7 +113,7 @@ __global__ void __launch_bounds__(256) fwd3d(KGrid<T> g, FwdStep<T> a) {
   T wn = 0;
 #pragma unroll
   for (int k = 0; k < 8; ++k) sw[k] = 0;
-  if (a.src_corner) {
+  if (!ADJ && a.src_corner) {
     bx = a.src_corner[3 * s]; by = a.src_corner[3 * s + 1]; bz = a.src_corner[3 * s + 2];
     if (bz <= t.z && t.z <= bz + 1 && by <= t.y && t.y <= by + 1 && bx + 1 >= t.x0 && bx <= t.x0 + RX - 1) {
 #pragma unroll
@@ -130,6 +123,7 @@ __global__ void __launch_bounds__(256) fwd3d(KGrid<T> g, FwdStep<T> a) {
       bx = -4;
     }
   }
+  const T* __restrict__ ln = (ADJ && a.lap) ? a.lap + so : nullptr;
 #pragma unroll
   for (int k = 0; k < RX; ++k) {
     const int x = t.x0 + k;
@@ -146,58 +140,16 @@ __global__ void __launch_bounds__(256) fwd3d(KGrid<T> g, FwdStep<T> a) {
       bool layer = false;
       if (AB) {
         layer = x < g.lo0 || x >= g.hi0 || t.y < g.lo1 || t.y >= g.hi1 || t.z < g.lo2 || t.z >= g.hi2;
-        if (layer) { av = a.A[i]; bv = a.b_one ? T(1) : a.B[i]; }
+        if (layer) { av = a.A[i]; bv = (!ADJ && a.b_one) ? T(1) : a.B[i]; }
       }
-      if (a.lap_out) a.lap_out[so + i] = lap;
+      if (!ADJ && a.lap_out) a.lap_out[so + i] = lap;
       T rhs = (T(2) * c - bv * pp) + a.C[i] * lap;
-      const int dx = x - bx, dy = t.y - by, dz = t.z - bz;
-      if (dx >= 0 && dx <= 1 && dy >= 0 && dy <= 1 && dz >= 0 && dz <= 1) rhs += sw[4 * dx + 2 * dy + dz] * wn;
-      a.next[so + i] = layer ? av * rhs : rhs;
-    }
-  }
-}
-
-template <typename T, int R, bool AB, int RX>
-__global__ void __launch_bounds__(256) adj3d(KGrid<T> g, AdjStep<T> a) {
-  const int s = blockIdx.z;
-  const long long so = (long long)s * g.field;
-  const Tile3 t = tile3(g.n2, RX);
-  if (t.z >= g.n2 || t.y >= g.n1 || t.x0 >= g.n0) return;
-  const long long base = g.origin + (long long)t.x0 * g.s0 + (long long)t.y * g.s1 + t.z;
-  const T* __restrict__ m1 = a.mu1 + so;
-  const T* __restrict__ C = a.C;
-  T q[RX + 2 * R];
-  T m[RX];
-#pragma unroll
-  for (int k = 0; k < RX + 2 * R; ++k) {
-    const int xr = t.x0 - R + k;
-    const long long i = base + (long long)(k - R) * g.s0;
-    T mv = (xr < g.n0 + R) ? m1[i] : T(0);
-    q[k] = (xr < g.n0 + R) ? C[i] * mv : T(0);
-    if (k >= R && k < R + RX) m[k - R] = mv;
-  }
-  const T* __restrict__ ln = a.lap ? a.lap + so : nullptr;
-#pragma unroll
-  for (int k = 0; k < RX; ++k) {
-    const int x = t.x0 + k;
-    if (x < g.n0) {
-      const long long i = base + (long long)k * g.s0;
-      const long long sy = g.s1;
-      T lq = g.wc * q[k + R] + g.w1a * (q[k + R - 1] + q[k + R + 1]) +
-             g.w1b * (C[i - sy] * m1[i - sy] + C[i + sy] * m1[i + sy]) +
-             g.w1c * (C[i - 1] * m1[i - 1] + C[i + 1] * m1[i + 1]);
-      if (R == 2)
-        lq += g.w2a * (q[k] + q[k + 4]) + g.w2b * (C[i - 2 * sy] * m1[i - 2 * sy] + C[i + 2 * sy] * m1[i + 2 * sy]) +
-              g.w2c * (C[i - 2] * m1[i - 2] + C[i + 2] * m1[i + 2]);
-      T av = T(1), bv = T(1);
-      bool layer = false;
-      if (AB) {
-        layer = x < g.lo0 || x >= g.hi0 || t.y < g.lo1 || t.y >= g.hi1 || t.z < g.lo2 || t.z >= g.hi2;
-        if (layer) { av = a.A[i]; bv = a.B[i]; }
+      if (!ADJ) {
+        const int dx = x - bx, dy = t.y - by, dz = t.z - bz;
+        if (dx >= 0 && dx <= 1 && dy >= 0 && dy <= 1 && dz >= 0 && dz <= 1) rhs += sw[4 * dx + 2 * dy + dz] * wn;
       }
-      T lam = (T(2) * m[k] + lq) - bv * a.mu2[so + i];
-      a.out[so + i] = (layer && a.apply_a) ? av * lam : lam;
-      if (ln) a.grad[so + i] += (double)(m[k] * ln[i]);
+      a.next[so + i] = (layer && (!ADJ || a.apply_a)) ? av * rhs : rhs;
+      if (ln) a.grad[so + i] += (double)(c * ln[i]);
     }
   }
 }
@@ -220,9 +172,10 @@ __global__ void sample_kernel(const T* __restrict__ lvl, long long field, T* __r
   traces[((long long)s * n_rec + r) * n_t + j] = acc;
 }
 
-// out[s][cell] += (apply_a ? A[cell] : 1) * sum_e w_e g[s, rec_e, j], cells in CSR order.
+// out[s][cell] += (apply_a ? A[cell] : 1) * C[cell] * sum_e w_e g[s, rec_e, j], cells in CSR order
+// (the adjoint source of q = C mu).
 template <typename T>
-__global__ void inject_kernel(T* __restrict__ out, long long field, const T* __restrict__ A,
+__global__ void inject_kernel(T* __restrict__ out, long long field, const T* __restrict__ C, const T* __restrict__ A,
                               int apply_a, const T* __restrict__ g, int n_rec, int n_t, int j,
                               int n_cells, const int64_t* __restrict__ cell,
                               const int* __restrict__ ptr, const int* __restrict__ rec,
@@ -235,7 +188,7 @@ __global__ void inject_kernel(T* __restrict__ out, long long field, const T* __r
   for (int e = ptr[c]; e < ptr[c + 1]; ++e) acc += w[e] * gs[(long long)rec[e] * n_t];
   const long long i = cell[c];
   const T av = (apply_a && A) ? A[i] : T(1);
-  out[(long long)s * field + i] += av * acc;
+  out[(long long)s * field + i] += av * (C[i] * acc);
 }
 
 }  // namespace nw

@@ -101,41 +101,37 @@ struct TileTables {
   const int* __restrict__ gcell_rec;
 };
 
+// Everything one tiled step reads and writes. The forward step advances the pressure,
+//   p^{n+1} = A (2 p^n - B p^{n-1} + C Lap p^n + S w(n)),
+// and the adjoint step advances q = C mu (mu^n = A lambda^n), which obeys the same recursion,
+//   q^n = A (2 q^{n+1} - B q^{n+2} + C Lap q^{n+1} + C R^T g_n),
+// so both directions run the same stencil: multiplying the adjoint of the reference's scheme,
+// mu^n = A (R^T g_n + 2 mu^{n+1} + Lap(C mu^{n+1}) - B mu^{n+2}), by C moves C out of the Laplacian.
+// The velocity gradient sum_n mu^{n+1} Lap p^n is accumulated as sum_n q^{n+1} Lap p^n, i.e. C dJ/dC.
 template <typename T>
-struct FwdTiled {
-  const T* __restrict__ prev;
-  const T* __restrict__ cur;
-  T* __restrict__ next;
+struct Tiled2 {
+  const T* __restrict__ prev;   // forward p^{n-1}   | adjoint q^{n+2}  (core tiles)
+  const T* __restrict__ cur;    // forward p^n       | adjoint q^{n+1}  (halo tiles)
+  T* __restrict__ next;         // forward p^{n+1}   | adjoint q^n
   const T* __restrict__ C;
   const T* __restrict__ A;
   const T* __restrict__ B;
-  int b_one;
+  int b_one;                    // forward: B = 1 on the first step (Cerjan)
+  int apply_a;                  // adjoint: A applies (n >= 1); at n = 0 the output is C lambda^0
+  int n_shots, shots_per_cta;
+  // forward: point sources, receiver samples of p^n
   const int* __restrict__ src_corner;
   const T* __restrict__ src_w;
   const T* __restrict__ wavelet;
   int n;
-  int n_shots, shots_per_cta;
-  T* __restrict__ traces;  // non-null on record steps
+  T* __restrict__ traces;       // non-null on record steps
   const T* __restrict__ rec_w;
-  int n_rec, n_t, j;
-  TileTables tt;
-  T* __restrict__ lap_out;  // non-null: also store Lap p^n (the adjoint's gradient factor)
-};
-
-template <typename T>
-struct AdjTiled {
-  const T* __restrict__ mu1;
-  const T* __restrict__ mu2;
-  T* __restrict__ out;
-  const T* __restrict__ C;
-  const T* __restrict__ A;
-  const T* __restrict__ B;
-  int apply_a;
-  const T* __restrict__ lap;    // Lap p^n as the forward step computed it; nullptr: no gradient term
-  double* __restrict__ gacc;    // (n_groups, field) float64 accumulators of dJ/dC
-  int n_shots, shots_per_cta;
+  T* __restrict__ lap_out;      // non-null: also store Lap p^n (the gradient factor)
+  // adjoint: receiver injection and the gradient
   const T* __restrict__ gtr;    // trace cotangents (n_shots, n_rec, n_t); non-null on record steps
   const T* __restrict__ gcell_w;
+  const T* __restrict__ lap;    // Lap p^n as the forward step stored it; nullptr: no gradient term
+  double* __restrict__ gacc;    // (n_groups, field) float64 accumulators of C dJ/dC
   int n_rec, n_t, j;
   TileTables tt;
 };
@@ -228,17 +224,21 @@ __device__ __forceinline__ void store_row(T* dst, const T (&o)[VZ], int zc, int 
 
 
 // ------------------------------------------------------------------------------------------
-// forward step: p^{n+1} = A (2 p^n - B p^{n-1} + C Lap p^n + S w(n)); with lap_out, the same
-// launch also stores Lap p^n, the factor the adjoint multiplies mu^{n+1} by
+// One leapfrog step of every shot of a group over one tile: forward (ADJ = false) or adjoint
+// (ADJ = true). The forward also samples receivers from the staged p^n tile, adds the shots'
+// point sources and, with lap_out, stores Lap p^n; the adjoint adds C R^T g_n at the
+// receiver-touched cells and accumulates q^{n+1} Lap p^n over the group's shots.
 // ------------------------------------------------------------------------------------------
-template <typename T, int R, int VZ, int RX, bool AB>
-__global__ void __launch_bounds__(256, 3) fwd2d_tiled(KGrid<T> g, FwdTiled<T> a) {
+template <typename T, int R, int VZ, int RX, bool AB, bool ADJ>
+__global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T> a) {
   using S = Tile2Shape<T, VZ, RX, R>;
   constexpr int NS = S::NS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* scc = reinterpret_cast<T*>(smem_raw);  // [QS] c^2 dt^2
-  T* sp = scc + S::QS;                      // [NS][PS] p^n with halo
-  T* sq = sp + NS * S::PS;                  // [NS][QS] p^{n-1}
+  T* scc = reinterpret_cast<T*>(smem_raw);  // [QS] C
+  T* sp = scc + S::QS;                      // [NS][PS] p^n | q^{n+1}, with halo
+  T* sq = sp + NS * S::PS;                  // [NS][QS] p^{n-1} | q^{n+2}
+  T* sl = sq + NS * S::QS;                  // adjoint: [NS][QS] Lap p^n
+  T* sj = sl + NS * S::QS;                  // adjoint: [QS] cotangent injected at this shot's cells
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int z0 = blockIdx.x * S::TZ, x0 = blockIdx.y * S::TX;
@@ -249,6 +249,7 @@ __global__ void __launch_bounds__(256, 3) fwd2d_tiled(KGrid<T> g, FwdTiled<T> a)
   const int xr = x0 + warp * RX;  // first owned row
   const int lrow = warp * RX;     // first owned row inside the tile
   const bool own_cols = zc < g.n1;
+  const bool grad = ADJ && a.lap != nullptr;
 
   const CopyPlan<S::NCH> ph = plan_halo<T, VZ, RX, R>(g, x0, z0);
   const CopyPlan<S::NCC> pc = plan_core<T, VZ, RX, R>(g, x0, z0);
@@ -260,15 +261,32 @@ __global__ void __launch_bounds__(256, 3) fwd2d_tiled(KGrid<T> g, FwdTiled<T> a)
     if (sb + i < se) {                // wait_group<NS-1> in the loop means "shot s has landed"
       issue(ph, a.cur + (long long)(sb + i) * g.field, sp + i * S::PS);
       issue(pc, a.prev + (long long)(sb + i) * g.field, sq + i * S::QS);
+      if (grad) issue(pc, a.lap + (long long)(sb + i) * g.field, sl + i * S::QS);
     }
     cp_async_commit();
   }
-  const int e0 = a.traces ? a.tt.rec_ptr[tile] : 0, e1 = a.traces ? a.tt.rec_ptr[tile + 1] : 0;
+  int e0 = 0, e1 = 0, c0 = 0, c1 = 0;
+  if (!ADJ && a.traces) { e0 = a.tt.rec_ptr[tile]; e1 = a.tt.rec_ptr[tile + 1]; }
+  if (ADJ && a.gtr) { c0 = a.tt.cell_ptr[tile]; c1 = a.tt.cell_ptr[tile + 1]; }
+  const bool inject = ADJ && c1 > c0;  // uniform
+  if (inject) {
+    for (int i = threadIdx.x; i < S::QS; i += 256) sj[i] = T(0);
+    __syncthreads();  // zeroing completes before any thread writes a cotangent value
+  }
 
   const bool layer_tile = AB && (x0 < g.lo0 || x0 + S::TX > g.hi0 || z0 < g.lo1 || z0 + S::TZ > g.hi1);
+  const bool use_a = layer_tile && (!ADJ || a.apply_a);
+  const bool use_b = layer_tile && (ADJ || !a.b_one);
   const T wc = g.wc, w1x = g.w1a, w1z = g.w1b, w2x = g.w2a, w2z = g.w2b;
   const int ld = (int)g.s0;
   const long long cbase = g.origin + (long long)xr * ld + zc;  // owned cells of row k: + k*ld
+  // adjoint: per-cell sum over this CTA's shots, float for float fields, double for double fields
+  using Acc = typename std::conditional<sizeof(T) == 8, double, float>::type;
+  Acc gsum[RX][VZ];
+#pragma unroll
+  for (int k = 0; k < RX; ++k)
+#pragma unroll
+    for (int v = 0; v < VZ; ++v) gsum[k][v] = Acc(0);
 
   for (int s = sb; s < se; ++s) {
     const int buf = (s - sb) % NS;
@@ -277,15 +295,27 @@ __global__ void __launch_bounds__(256, 3) fwd2d_tiled(KGrid<T> g, FwdTiled<T> a)
       if (sn < se) {
         issue(ph, a.cur + (long long)sn * g.field, sp + nb * S::PS);
         issue(pc, a.prev + (long long)sn * g.field, sq + nb * S::QS);
+        if (grad) issue(pc, a.lap + (long long)sn * g.field, sl + nb * S::QS);
       }
       cp_async_commit();
       cp_async_wait<NS - 1>();
     }
+    if (inject) {  // cotangent of shot s at each touched cell, summed in table order
+      const T* gs = a.gtr + (long long)s * a.n_rec * a.n_t + a.j;
+      for (int e = c0 + threadIdx.x; e < c1; e += 256) {
+        const int gid = a.tt.cell_gid[e];
+        T acc = T(0);
+        for (int q = a.tt.gcell_ptr[gid]; q < a.tt.gcell_ptr[gid + 1]; ++q)
+          acc += a.gcell_w[q] * gs[(long long)a.tt.gcell_rec[q] * a.n_t];
+        sj[a.tt.cell_local[e]] = acc;
+      }
+    }
     __syncthreads();
     const T* P = sp + buf * S::PS;
     const T* Q = sq + buf * S::QS;
+    const T* LP = sl + buf * S::QS;
 
-    for (int e = e0 + threadIdx.x; e < e1; e += 256) {  // receiver samples of p^n from the tile
+    for (int e = e0 + threadIdx.x; e < e1; e += 256) {  // forward: receiver samples of p^n
       const int r = a.tt.rec_list[e];
       const int row = a.tt.rec_corner[2 * r] - x0 + R, col = a.tt.rec_corner[2 * r + 1] - z0 + S::HL;
       const T* w = a.rec_w + 4 * r;
@@ -296,11 +326,11 @@ __global__ void __launch_bounds__(256, 3) fwd2d_tiled(KGrid<T> g, FwdTiled<T> a)
       acc += w[3] * P[(row + 1) * S::SW + col + 1];
       a.traces[((long long)s * a.n_rec + r) * a.n_t + a.j] = acc;
     }
-    // the shot's source stencil, if it touches this tile (a CTA-uniform test)
+    // forward: the shot's source stencil, if it touches this tile (a CTA-uniform test)
     int bx = 0, bz = 0;
     bool src_tile = false;
     T sw0 = 0, sw1 = 0, sw2 = 0, sw3 = 0;
-    if (a.src_corner) {
+    if (!ADJ && a.src_corner) {
       bx = a.src_corner[2 * s];
       bz = a.src_corner[2 * s + 1];
       src_tile = bx + 1 >= x0 && bx < x0 + S::TX && bz + 1 >= z0 && bz < z0 + S::TZ;
@@ -316,7 +346,7 @@ __global__ void __launch_bounds__(256, 3) fwd2d_tiled(KGrid<T> g, FwdTiled<T> a)
 #pragma unroll
     for (int q = 0; q < 2 * R; ++q) vload<T, VZ>(P + (lrow + q) * S::SW + S::HL + lane * VZ, wv[q]);
     T* nx = a.next + (long long)s * g.field + cbase;
-    T* lx = a.lap_out ? a.lap_out + (long long)s * g.field + cbase : nullptr;
+    T* lx = (!ADJ && a.lap_out) ? a.lap_out + (long long)s * g.field + cbase : nullptr;
 #pragma unroll
     for (int k = 0; k < RX; ++k) {
       const int prow = lrow + k + R;  // shared row of the output row
@@ -326,18 +356,21 @@ __global__ void __launch_bounds__(256, 3) fwd2d_tiled(KGrid<T> g, FwdTiled<T> a)
 #pragma unroll
       for (int v = 0; v < VZ; ++v) rw.c[v] = wv[R][v];
       vload<T, VZ>(P + prow * S::SW + S::HL + lane * VZ + VZ, rw.r);
+      const int toff = (lrow + k) * S::TZ + lane * VZ;  // the owned cells in a core tile
       T pp[VZ], cc[VZ];
-      vload<T, VZ>(Q + (lrow + k) * S::TZ + lane * VZ, pp);
-      vload<T, VZ>(scc + (lrow + k) * S::TZ + lane * VZ, cc);
+      vload<T, VZ>(Q + toff, pp);
+      vload<T, VZ>(scc + toff, cc);
       const int x = xr + k;
       const bool ok = own_cols && x < g.n0;
       T ca[VZ], cb[VZ];
 #pragma unroll
       for (int v = 0; v < VZ; ++v) { ca[v] = T(1); cb[v] = T(1); }
-      if (layer_tile && ok) {
-        vldg<T, VZ>(a.A + cbase + k * ld, ca);
-        if (!a.b_one) vldg<T, VZ>(a.B + cbase + k * ld, cb);
-      }
+      if (use_a && ok) vldg<T, VZ>(a.A + cbase + k * ld, ca);
+      if (use_b && ok) vldg<T, VZ>(a.B + cbase + k * ld, cb);
+      T inj[VZ];
+#pragma unroll
+      for (int v = 0; v < VZ; ++v) inj[v] = T(0);
+      if (inject) vload<T, VZ>(sj + toff, inj);
       T o[VZ], lp[VZ];
 #pragma unroll
       for (int v = 0; v < VZ; ++v) {
@@ -345,7 +378,7 @@ __global__ void __launch_bounds__(256, 3) fwd2d_tiled(KGrid<T> g, FwdTiled<T> a)
         T lap = wc * c + w1x * (wv[R - 1][v] + wv[R + 1][v]) + w1z * (zval(rw, v - 1) + zval(rw, v + 1));
         if (R == 2) lap += w2x * (wv[0][v] + wv[4][v]) + w2z * (zval(rw, v - 2) + zval(rw, v + 2));
         lp[v] = lap;
-        o[v] = (T(2) * c - cb[v] * pp[v]) + cc[v] * lap;
+        o[v] = (T(2) * c - cb[v] * pp[v]) + cc[v] * (inject ? lap + inj[v] : lap);
       }
       if (src_tile) {
 #pragma unroll
@@ -355,187 +388,22 @@ __global__ void __launch_bounds__(256, 3) fwd2d_tiled(KGrid<T> g, FwdTiled<T> a)
             o[v] += (dx == 0) ? (dz == 0 ? sw0 : sw1) : (dz == 0 ? sw2 : sw3);
         }
       }
-      if (layer_tile) {
+      if (use_a) {
 #pragma unroll
         for (int v = 0; v < VZ; ++v) o[v] = ca[v] * o[v];
       }
       if (ok) store_row<T, VZ>(nx + k * ld, o, zc, g.n1);
       if (lx && ok) store_row<T, VZ>(lx + k * ld, lp, zc, g.n1);
+      if (grad) {
+        T gl[VZ];
+        vload<T, VZ>(LP + toff, gl);
+#pragma unroll
+        for (int v = 0; v < VZ; ++v) gsum[k][v] += (Acc)(wv[R][v] * gl[v]);
+      }
 #pragma unroll
       for (int q = 0; q < 2 * R; ++q)
 #pragma unroll
         for (int v = 0; v < VZ; ++v) wv[q][v] = wv[q + 1][v];
-    }
-    __syncthreads();
-  }
-}
-
-// ------------------------------------------------------------------------------------------
-// adjoint step: mu^n = A (R^T g_n + 2 mu1 + Lap(C mu1) - B mu2), grad += mu1 Lap(p^n), where
-// Lap(p^n) is read back as the forward step stored it (no p halo, no second stencil)
-// ------------------------------------------------------------------------------------------
-template <typename T, int R, int VZ, int RX, bool AB>
-__global__ void __launch_bounds__(256, 2) adj2d_tiled(KGrid<T> g, AdjTiled<T> a) {
-  using S = Tile2Shape<T, VZ, RX, R>;
-  constexpr int NS = S::NS;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* sc = reinterpret_cast<T*>(smem_raw);  // [PS] C with halo
-  T* sm = sc + S::PS;                      // [NS][PS] mu^{n+1} with halo
-  T* s2 = sm + NS * S::PS;                 // [NS][QS] mu^{n+2}
-  T* sl = s2 + NS * S::QS;                 // [NS][QS] Lap p^n
-  T* sj = sl + NS * S::QS;                 // [QS] adjoint source of the current shot
-
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int z0 = blockIdx.x * S::TZ, x0 = blockIdx.y * S::TX;
-  const int tile = blockIdx.y * a.tt.tiles_z + blockIdx.x;
-  const int sb = blockIdx.z * a.shots_per_cta;
-  const int se = min(sb + a.shots_per_cta, a.n_shots);
-  const int zc = z0 + lane * VZ;
-  const int xr = x0 + warp * RX;
-  const int lrow = warp * RX;
-  const bool own_cols = zc < g.n1;
-  const bool grad = a.lap != nullptr;
-
-  const CopyPlan<S::NCH> ph = plan_halo<T, VZ, RX, R>(g, x0, z0);
-  const CopyPlan<S::NCC> pc = plan_core<T, VZ, RX, R>(g, x0, z0);
-  wait_previous_grid();
-  allow_next_grid();
-  issue(ph, a.C, sc);
-#pragma unroll
-  for (int i = 0; i < NS - 1; ++i) {  // one commit group per shot, empty ones included
-    if (sb + i < se) {
-      issue(ph, a.mu1 + (long long)(sb + i) * g.field, sm + i * S::PS);
-      issue(pc, a.mu2 + (long long)(sb + i) * g.field, s2 + i * S::QS);
-      if (grad) issue(pc, a.lap + (long long)(sb + i) * g.field, sl + i * S::QS);
-    }
-    cp_async_commit();
-  }
-
-  const int c0 = a.gtr ? a.tt.cell_ptr[tile] : 0, c1 = a.gtr ? a.tt.cell_ptr[tile + 1] : 0;
-  const bool inject = c1 > c0;  // uniform
-  if (inject) {
-    for (int i = threadIdx.x; i < S::QS; i += 256) sj[i] = T(0);
-    __syncthreads();  // zeroing completes before any thread writes a source value
-  }
-
-  const bool layer_tile = AB && (x0 < g.lo0 || x0 + S::TX > g.hi0 || z0 < g.lo1 || z0 + S::TZ > g.hi1);
-  const bool use_a = layer_tile && a.apply_a;
-  const T wc = g.wc, w1x = g.w1a, w1z = g.w1b, w2x = g.w2a, w2z = g.w2b;
-  const int ld = (int)g.s0;
-  const long long cbase = g.origin + (long long)xr * ld + zc;
-  // per-cell sum over this CTA's shots: float for float fields, double for double fields
-  using Acc = typename std::conditional<sizeof(T) == 8, double, float>::type;
-  Acc gsum[RX][VZ];
-#pragma unroll
-  for (int k = 0; k < RX; ++k)
-#pragma unroll
-    for (int v = 0; v < VZ; ++v) gsum[k][v] = Acc(0);
-
-  for (int s = sb; s < se; ++s) {
-    const int buf = (s - sb) % NS;
-    {
-      const int sn = s + NS - 1, nb = (sn - sb) % NS;  // nb: the buffer shot s-1 used
-      if (sn < se) {
-        issue(ph, a.mu1 + (long long)sn * g.field, sm + nb * S::PS);
-        issue(pc, a.mu2 + (long long)sn * g.field, s2 + nb * S::QS);
-        if (grad) issue(pc, a.lap + (long long)sn * g.field, sl + nb * S::QS);
-      }
-      cp_async_commit();
-      cp_async_wait<NS - 1>();
-    }
-    if (inject) {  // adjoint source of shot s: each touched cell summed in table order
-      const T* gs = a.gtr + (long long)s * a.n_rec * a.n_t + a.j;
-      for (int e = c0 + threadIdx.x; e < c1; e += 256) {
-        const int gid = a.tt.cell_gid[e];
-        T acc = T(0);
-        for (int q = a.tt.gcell_ptr[gid]; q < a.tt.gcell_ptr[gid + 1]; ++q)
-          acc += a.gcell_w[q] * gs[(long long)a.tt.gcell_rec[q] * a.n_t];
-        sj[a.tt.cell_local[e]] = acc;
-      }
-    }
-    __syncthreads();
-    const T* M = sm + buf * S::PS;
-    const T* M2 = s2 + buf * S::QS;
-    const T* LP = sl + buf * S::QS;
-
-    T qv[2 * R + 1][VZ];  // C * mu1, own columns
-#pragma unroll
-    for (int q = 0; q < 2 * R; ++q) {
-      T tm[VZ], tc[VZ];
-      const int off = (lrow + q) * S::SW + S::HL + lane * VZ;
-      vload<T, VZ>(M + off, tm);
-      vload<T, VZ>(sc + off, tc);
-#pragma unroll
-      for (int v = 0; v < VZ; ++v) qv[q][v] = tc[v] * tm[v];
-    }
-    T* ob = a.out + (long long)s * g.field + cbase;
-#pragma unroll
-    for (int k = 0; k < RX; ++k) {
-      const int prow = lrow + k + R;
-      {
-        T tm[VZ], tc[VZ];
-        const int off = (prow + R) * S::SW + S::HL + lane * VZ;
-        vload<T, VZ>(M + off, tm);
-        vload<T, VZ>(sc + off, tc);
-#pragma unroll
-        for (int v = 0; v < VZ; ++v) qv[2 * R][v] = tc[v] * tm[v];
-      }
-      const int coff = prow * S::SW + S::HL + lane * VZ;
-      Row3<T, VZ> qw;
-      T mc[VZ];
-      {
-        T tm[VZ], tc[VZ];
-        vload<T, VZ>(M + coff - VZ, tm);
-        vload<T, VZ>(sc + coff - VZ, tc);
-#pragma unroll
-        for (int v = 0; v < VZ; ++v) qw.l[v] = tc[v] * tm[v];
-        vload<T, VZ>(M + coff + VZ, tm);
-        vload<T, VZ>(sc + coff + VZ, tc);
-#pragma unroll
-        for (int v = 0; v < VZ; ++v) qw.r[v] = tc[v] * tm[v];
-        vload<T, VZ>(M + coff, mc);
-#pragma unroll
-        for (int v = 0; v < VZ; ++v) qw.c[v] = qv[R][v];
-      }
-      T m2[VZ];
-      vload<T, VZ>(M2 + (lrow + k) * S::TZ + lane * VZ, m2);
-      const int x = xr + k;
-      const bool ok = own_cols && x < g.n0;
-      T ca[VZ], cb[VZ];
-#pragma unroll
-      for (int v = 0; v < VZ; ++v) { ca[v] = T(1); cb[v] = T(1); }
-      if (layer_tile && ok) {
-        vldg<T, VZ>(a.A + cbase + k * ld, ca);
-        vldg<T, VZ>(a.B + cbase + k * ld, cb);
-      }
-      T o[VZ];
-#pragma unroll
-      for (int v = 0; v < VZ; ++v) {
-        T lq = wc * qv[R][v] + w1x * (qv[R - 1][v] + qv[R + 1][v]) + w1z * (zval(qw, v - 1) + zval(qw, v + 1));
-        if (R == 2) lq += w2x * (qv[0][v] + qv[4][v]) + w2z * (zval(qw, v - 2) + zval(qw, v + 2));
-        o[v] = (T(2) * mc[v] + lq) - cb[v] * m2[v];
-      }
-      if (inject) {
-        T inj[VZ];
-        vload<T, VZ>(sj + (lrow + k) * S::TZ + lane * VZ, inj);
-#pragma unroll
-        for (int v = 0; v < VZ; ++v) o[v] = inj[v] + o[v];
-      }
-      if (use_a) {
-#pragma unroll
-        for (int v = 0; v < VZ; ++v) o[v] = ca[v] * o[v];
-      }
-      if (grad) {
-        T lp[VZ];
-        vload<T, VZ>(LP + (lrow + k) * S::TZ + lane * VZ, lp);
-#pragma unroll
-        for (int v = 0; v < VZ; ++v) gsum[k][v] += (Acc)(mc[v] * lp[v]);
-      }
-      if (ok) store_row<T, VZ>(ob + k * ld, o, zc, g.n1);
-#pragma unroll
-      for (int q = 0; q < 2 * R; ++q)
-#pragma unroll
-        for (int v = 0; v < VZ; ++v) qv[q][v] = qv[q + 1][v];
     }
     __syncthreads();
     if (inject)  // the same threads clear the cells they set, before the next shot sets them again

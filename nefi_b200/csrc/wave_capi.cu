@@ -224,15 +224,12 @@ int n_groups(const nw_grid* g, const Tune& t, int n_shots) {
   return g->ndim == 3 ? n_shots : (n_shots + t.adj_spc - 1) / t.adj_spc;
 }
 
-template <typename T, int R, int VZ, int RX>
-constexpr size_t fwd2_smem() {
+// Dynamic shared memory of step2d: C, the copy ring (halo tile + core tile, and the Lap p core
+// tile in the adjoint) and, in the adjoint, the injected cotangents.
+template <typename T, int R, int VZ, int RX, bool ADJ>
+constexpr size_t step2_smem() {
   using S = nw::Tile2Shape<T, VZ, RX, R>;
-  return (S::QS + S::NS * (S::PS + S::QS)) * sizeof(T);
-}
-template <typename T, int R, int VZ, int RX>
-constexpr size_t adj2_smem() {
-  using S = nw::Tile2Shape<T, VZ, RX, R>;
-  return (S::PS + S::NS * (S::PS + 2 * S::QS) + S::QS) * sizeof(T);
+  return (ADJ ? 2 * S::QS + S::NS * (S::PS + 2 * S::QS) : S::QS + S::NS * (S::PS + S::QS)) * sizeof(T);
 }
 constexpr size_t kMaxSmem = 227 * 1024;  // opt-in shared memory per CTA on sm_100a
 
@@ -278,29 +275,41 @@ nw::TileTables tile_tables(const nw_acquisition* a) {
   return tt;
 }
 
-template <typename T, int R, int VZ, int RX, bool AB>
-int launch_fwd2_v(const nw_grid* g, const nw::KGrid<T>& kg, const nw::FwdTiled<T>& st, const Tune& t,
-                  cudaStream_t s) {
+template <typename T, int R, int VZ, int RX, bool AB, bool ADJ>
+int launch_step2(const nw_grid* g, const nw::KGrid<T>& kg, const nw::Tiled2<T>& st, cudaStream_t s) {
   using S = nw::Tile2Shape<T, VZ, RX, R>;
-  constexpr size_t smem = fwd2_smem<T, R, VZ, RX>();
-  if (smem > kMaxSmem) return fail(NW_ERR_ARG, "tile too large for shared memory (lower tuning.rx)");
+  constexpr size_t smem = step2_smem<T, R, VZ, RX, ADJ>();
+  if (smem > kMaxSmem) return fail(NW_ERR_ARG, "tile too large for shared memory (lower tuning.rx or vz)");
   static bool done = false;
-  int rc = allow_smem(nw::fwd2d_tiled<T, R, VZ, RX, AB>, smem, &done);
+  int rc = allow_smem(nw::step2d<T, R, VZ, RX, AB, ADJ>, smem, &done);
   if (rc) return rc;
-  dim3 grid((g->n[1] + S::TZ - 1) / S::TZ, (g->n[0] + S::TX - 1) / S::TX, (st.n_shots + t.spc - 1) / t.spc);
-  return launch_pdl(nw::fwd2d_tiled<T, R, VZ, RX, AB>, grid, smem, s, kg, st);
+  dim3 grid((g->n[1] + S::TZ - 1) / S::TZ, (g->n[0] + S::TX - 1) / S::TX,
+            (st.n_shots + st.shots_per_cta - 1) / st.shots_per_cta);
+  return launch_pdl(nw::step2d<T, R, VZ, RX, AB, ADJ>, grid, smem, s, kg, st);
 }
 template <typename T, int R, int VZ, int RX, bool AB>
-int launch_adj2_v(const nw_grid* g, const nw::KGrid<T>& kg, const nw::AdjTiled<T>& st, const Tune& t,
-                  cudaStream_t s) {
-  using S = nw::Tile2Shape<T, VZ, RX, R>;
-  constexpr size_t smem = adj2_smem<T, R, VZ, RX>();
-  if (smem > kMaxSmem) return fail(NW_ERR_ARG, "tile too large for shared memory (lower tuning.rx)");
-  static bool done = false;
-  int rc = allow_smem(nw::adj2d_tiled<T, R, VZ, RX, AB>, smem, &done);
-  if (rc) return rc;
-  dim3 grid((g->n[1] + S::TZ - 1) / S::TZ, (g->n[0] + S::TX - 1) / S::TX, (st.n_shots + t.adj_spc - 1) / t.adj_spc);
-  return launch_pdl(nw::adj2d_tiled<T, R, VZ, RX, AB>, grid, smem, s, kg, st);
+int launch_fwd2_v(const nw_grid* g, const nw::KGrid<T>& kg, const nw::Tiled2<T>& st, cudaStream_t s) {
+  return launch_step2<T, R, VZ, RX, AB, false>(g, kg, st, s);
+}
+template <typename T, int R, int VZ, int RX, bool AB>
+int launch_adj2_v(const nw_grid* g, const nw::KGrid<T>& kg, const nw::Tiled2<T>& st, cudaStream_t s) {
+  return launch_step2<T, R, VZ, RX, AB, true>(g, kg, st, s);
+}
+
+// 3-D step: forward (ADJ = false) or adjoint.
+template <typename T, bool ADJ>
+int launch_step3(const nw_grid* g, const nw::KGrid<T>& kg, const nw::Step3<T>& st, bool ab, int n_shots,
+                 cudaStream_t s) {
+  const Shape sh = stencil_shape(g, n_shots);
+  if (g->radius == 1) {
+    if (ab) nw::step3d<T, 1, true, kRX, ADJ><<<sh.grid, sh.block, 0, s>>>(kg, st);
+    else nw::step3d<T, 1, false, kRX, ADJ><<<sh.grid, sh.block, 0, s>>>(kg, st);
+  } else {
+    if (ab) nw::step3d<T, 2, true, kRX, ADJ><<<sh.grid, sh.block, 0, s>>>(kg, st);
+    else nw::step3d<T, 2, false, kRX, ADJ><<<sh.grid, sh.block, 0, s>>>(kg, st);
+  }
+  NW_LAUNCHED();
+  return NW_OK;
 }
 
 // Runtime (radius, vz, rx, absorbing) -> template instantiation.
@@ -346,7 +355,7 @@ int forward_step(const nw_grid* g, const nw::KGrid<T>& kg, const nw_medium* m, c
                  cudaStream_t s) {
   const bool rec = traces && a->n_rec > 0 && (n % t->substeps) == 0;
   if (g->ndim == 2) {
-    nw::FwdTiled<T> st;
+    nw::Tiled2<T> st = {};
     st.prev = L.at(n - 1);
     st.cur = L.at(n);
     st.next = L.at(n + 1);
@@ -367,9 +376,9 @@ int forward_step(const nw_grid* g, const nw::KGrid<T>& kg, const nw_medium* m, c
     st.n_t = t->n_t;
     st.j = n / t->substeps;
     st.tt = tile_tables(a);
-    return NW_DISPATCH2(launch_fwd2_v, T, tu, g, kg, st, tu, s);
+    return NW_DISPATCH2(launch_fwd2_v, T, tu, g, kg, st, s);
   }
-  nw::FwdStep<T> st;
+  nw::Step3<T> st = {};
   st.prev = L.at(n - 1);
   st.cur = L.at(n);
   st.next = L.at(n + 1);
@@ -388,17 +397,7 @@ int forward_step(const nw_grid* g, const nw::KGrid<T>& kg, const nw_medium* m, c
   st.n_rec = a->n_rec;
   st.n_t = t->n_t;
   st.j = n / t->substeps;
-  Shape sh = stencil_shape(g, a->n_shots);
-  const bool ab = m->coef_a != nullptr;
-  if (g->radius == 1) {
-    if (ab) nw::fwd3d<T, 1, true, kRX><<<sh.grid, sh.block, 0, s>>>(kg, st);
-    else nw::fwd3d<T, 1, false, kRX><<<sh.grid, sh.block, 0, s>>>(kg, st);
-  } else {
-    if (ab) nw::fwd3d<T, 2, true, kRX><<<sh.grid, sh.block, 0, s>>>(kg, st);
-    else nw::fwd3d<T, 2, false, kRX><<<sh.grid, sh.block, 0, s>>>(kg, st);
-  }
-  NW_LAUNCHED();
-  return NW_OK;
+  return launch_step3<T, false>(g, kg, st, m->coef_a != nullptr, a->n_shots, s);
 }
 
 template <typename T>
@@ -429,6 +428,11 @@ int forward_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
 }
 
 // ---- adjoint driver ---------------------------------------------------------------------
+int grid_blocks(long long work, int threads) {
+  long long b = (work + threads - 1) / threads;
+  return (int)std::max(1LL, std::min(b, 148LL * 32));
+}
+
 template <typename T>
 int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, const nw_time* t,
                  const nw_storage* st, const Tune& tu, const T* gtr, T* work, double* gacc, T* lambda0,
@@ -440,7 +444,7 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
   const bool ab = m->coef_a != nullptr;
   NW_CUDA(cudaMemsetAsync(work, 0, 3 * lvl_bytes, s));
   NW_CUDA(cudaMemsetAsync(gacc, 0, (size_t)n_groups(g, tu, S) * g->field_elems * sizeof(double), s));
-  auto mu = [&](int n) { return work + (long long)(n % 3) * LE; };
+  auto q = [&](int n) { return work + (long long)(n % 3) * LE; };  // q^n = C mu^n, three levels
   const bool hist = st->history != nullptr;
   const bool ckpt = !hist && st->snap != nullptr;
   if (!hist && !ckpt && N > 0) return fail(NW_ERR_ARG, "adjoint needs a history or snapshots");
@@ -455,17 +459,17 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
   dim3 ig(((a->n_cells > 0 ? a->n_cells : 1) + 127) / 128, S);
   auto inject3 = [&](int n) -> int {  // 3-D: separate adjoint-source kernel
     if (a->n_cells <= 0 || n % M != 0) return NW_OK;
-    nw::inject_kernel<T><<<ig, 128, 0, s>>>(mu(n), g->field_elems, (const T*)m->coef_a, n >= 1 ? 1 : 0,
+    nw::inject_kernel<T><<<ig, 128, 0, s>>>(q(n), g->field_elems, (const T*)m->c2dt2, (const T*)m->coef_a, n >= 1 ? 1 : 0,
                                             gtr, a->n_rec, t->n_t, n / M, a->n_cells, a->cell_index,
                                             a->cell_ptr, a->cell_rec, (const T*)a->cell_weight);
     NW_LAUNCHED();
     return NW_OK;
   };
   auto step2 = [&](int n, const T* lap) -> int {  // 2-D: one fused tiled launch
-    nw::AdjTiled<T> as;
-    as.mu1 = mu(n + 1);
-    as.mu2 = mu(n + 2);
-    as.out = mu(n);
+    nw::Tiled2<T> as = {};
+    as.cur = q(n + 1);
+    as.prev = q(n + 2);
+    as.next = q(n);
     as.C = (const T*)m->c2dt2;
     as.A = (const T*)m->coef_a;
     as.B = (const T*)m->coef_b;
@@ -480,9 +484,9 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
     as.n_t = t->n_t;
     as.j = n / M;
     as.tt = tile_tables(a);
-    return NW_DISPATCH2(launch_adj2_v, T, tu, g, kg, as, tu, s);
+    return NW_DISPATCH2(launch_adj2_v, T, tu, g, kg, as, s);
   };
-  if (N >= n_stop) {  // level N: mu^N = A R^T g_N (mu^{N+1} = mu^{N+2} = 0)
+  if (N >= n_stop) {  // level N: q^N = A C R^T g_N (q^{N+1} = q^{N+2} = 0)
     int rc = g->ndim == 2 ? step2(N, nullptr) : inject3(N);
     if (rc) return rc;
   }
@@ -509,41 +513,36 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
       if (rc) return rc;
       continue;
     }
-    nw::AdjStep<T> as;
-    as.mu1 = mu(n + 1);
-    as.mu2 = mu(n + 2);
-    as.out = mu(n);
+    nw::Step3<T> as = {};
+    as.cur = q(n + 1);
+    as.prev = q(n + 2);
+    as.next = q(n);
     as.C = (const T*)m->c2dt2;
     as.A = (const T*)m->coef_a;
     as.B = (const T*)m->coef_b;
     as.apply_a = n >= 1 ? 1 : 0;
     as.lap = lap;
     as.grad = gacc;
-    Shape sh = stencil_shape(g, S);
-    if (g->radius == 1) {
-      if (ab) nw::adj3d<T, 1, true, kRX><<<sh.grid, sh.block, 0, s>>>(kg, as);
-      else nw::adj3d<T, 1, false, kRX><<<sh.grid, sh.block, 0, s>>>(kg, as);
-    } else {
-      if (ab) nw::adj3d<T, 2, true, kRX><<<sh.grid, sh.block, 0, s>>>(kg, as);
-      else nw::adj3d<T, 2, false, kRX><<<sh.grid, sh.block, 0, s>>>(kg, as);
-    }
-    NW_LAUNCHED();
-    int rc = inject3(n);
+    int rc = launch_step3<T, true>(g, kg, as, ab, S, s);
+    if (rc) return rc;
+    rc = inject3(n);
     if (rc) return rc;
   }
-  if (lambda0) {
-    NW_CUDA(cudaMemcpyAsync(lambda0, mu(0), lvl_bytes, cudaMemcpyDeviceToDevice, s));
+  if (lambda0) {  // lambda^0 = q^0 / C and mu^1 = q^1 / C on the padded grid, zero ghosts
+    NW_CUDA(cudaMemsetAsync(lambda0, 0, lvl_bytes, s));
+    const long long cells = (long long)g->n[0] * g->n[1] * (g->ndim == 3 ? g->n[2] : 1);
+    dim3 ug(grid_blocks(cells, 256), S);
+    nw::unscale_kernel<T><<<ug, 256, 0, s>>>(kg, g->ndim, (const T*)m->c2dt2, q(0), lambda0);
+    NW_LAUNCHED();
     if (mu1) {
-      if (N == 0) NW_CUDA(cudaMemsetAsync(mu1, 0, lvl_bytes, s));
-      else NW_CUDA(cudaMemcpyAsync(mu1, mu(1), lvl_bytes, cudaMemcpyDeviceToDevice, s));
+      NW_CUDA(cudaMemsetAsync(mu1, 0, lvl_bytes, s));
+      if (N > 0) {
+        nw::unscale_kernel<T><<<ug, 256, 0, s>>>(kg, g->ndim, (const T*)m->c2dt2, q(1), mu1);
+        NW_LAUNCHED();
+      }
     }
   }
   return NW_OK;
-}
-
-int grid_blocks(long long work, int threads) {
-  long long b = (work + threads - 1) / threads;
-  return (int)std::max(1LL, std::min(b, 148LL * 32));
 }
 
 }  // namespace
