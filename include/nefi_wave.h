@@ -78,22 +78,31 @@ typedef struct nw_grid {
 int nw_grid_layout(nw_grid* g);
 
 /*
- * Launch shape of the 2-D tiled kernels. A CTA owns a tile of 8*rx rows by 32*vz columns and
- * loops over shots_per_cta shots. Zero fields take the library's defaults. 3-D grids ignore it.
+ * Launch shape of the 2-D step kernels, forward and adjoint separately. A step is a list of
+ * (tile, shot) units, a tile being 8*rx rows by 32*vz columns; the launch has
+ * min(units, ctas_per_sm * 148) CTAs, each taking a contiguous range of units. Zero fields take
+ * the library's defaults. 3-D grids ignore it.
  */
 typedef struct nw_tuning {
-  int32_t vz;                /* columns per thread: 2 or 4 (float32), 2 (float64) */
-  int32_t rx;                /* rows per thread: 2, 4 or 8 */
-  int32_t shots_per_cta;     /* forward steps: shots per CTA, >= 1 */
-  int32_t adj_shots_per_cta; /* adjoint steps: shots per CTA, >= 1 (one float64 gradient
-                                accumulator per group of this many shots) */
-  int32_t reserved[4];
+  int32_t vz;              /* forward: columns per thread, 2 or 4 (float32), 2 (float64) */
+  int32_t rx;              /* forward: rows per thread, 2, 4 or 8 */
+  int32_t ctas_per_sm;     /* forward: CTAs per SM of the launch, 1..32 */
+  int32_t adj_vz;          /* the same for the adjoint steps */
+  int32_t adj_rx;
+  int32_t adj_ctas_per_sm;
+  int32_t reserved[2];
 } nw_tuning;
 
-/* Resolves the defaults of `t` for grid `g` in place and reports the tile (tx rows, tz columns). */
-int nw_tile_shape(const nw_grid* g, nw_tuning* t, int32_t* tx, int32_t* tz);
+/*
+ * Resolves the defaults of `t` for grid `g` in place and reports the tile shapes:
+ * shape = {forward rows, forward columns, adjoint rows, adjoint columns}.
+ */
+int nw_tile_shape(const nw_grid* g, nw_tuning* t, int32_t* shape);
 
-/* Number of float64 gradient accumulator fields nw_adjoint fills for n_shots shots. */
+/*
+ * Number of gradient accumulator fields (in the grid's dtype) nw_adjoint fills for n_shots
+ * shots: one per shot in 3-D; in 2-D, the largest number of adjoint CTAs sharing one tile.
+ */
 int nw_adjoint_groups(const nw_grid* g, const nw_tuning* t, int32_t n_shots);
 
 /*
@@ -119,14 +128,17 @@ typedef struct nw_acquisition {
   const int32_t* cell_ptr;     /* (n_cells + 1,) CSR row pointers into cell_rec/cell_weight */
   const int32_t* cell_rec;     /* receiver id per entry */
   const void* cell_weight;     /* dtype weight per entry */
-  /* 2-D per-tile tables (tiles in row-major order, tiles_z along the contiguous axis) */
+  /* 2-D per-tile tables (tiles in row-major order, tiles_z along the contiguous axis): receivers
+     by the forward tile shape, receiver-touched cells by the adjoint tile shape */
   int32_t tiles_z;
-  int32_t tile_rows, tile_cols;    /* tile shape the tables were built for */
+  int32_t tile_rows, tile_cols;    /* forward tile shape the receiver tables were built for */
   const int32_t* rec_corner;       /* (n_rec, 2) corner cell of each receiver stencil */
   const int32_t* tile_rec_ptr;     /* (n_tiles + 1): receivers whose corner lies in the tile */
   const int32_t* tile_rec_list;
-  const int32_t* tile_cell_ptr;    /* (n_tiles + 1): touched cells of the tile */
-  const int32_t* tile_cell_local;  /* (x - x0) * tile_cols + (z - z0) */
+  int32_t adj_tiles_z;
+  int32_t adj_tile_rows, adj_tile_cols;  /* adjoint tile shape the cell tables were built for */
+  const int32_t* tile_cell_ptr;    /* (n_adj_tiles + 1): touched cells of the tile */
+  const int32_t* tile_cell_local;  /* (x - x0) * adj_tile_cols + (z - z0) */
   const int32_t* tile_cell_gid;    /* row in cell_index / cell_ptr */
 } nw_acquisition;
 
@@ -205,7 +217,7 @@ int nw_forward(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, co
 
 /*
  * Adjoint run for all shots: from trace cotangents `grad_traces` (n_shots, n_rec, n_t) computes
- *  - grad_acc: nw_adjoint_groups() float64 fields (zeroed by the call) whose sum is
+ *  - grad_acc: nw_adjoint_groups() fields in the grid's dtype (zeroed by the call) whose sum is
  *    c2dt2 * sum_shots sum_n mu^{n+1} * Lap p^n, i.e. c2dt2 times the gradient w.r.t. c2dt2
  *    (nw_reduce_grad_c divides the factor out), and
  *  - lambda0 / mu1 (n_shots fields each, may be NULL): the sensitivities of p^0 and A*p^1
@@ -217,17 +229,17 @@ int nw_forward(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, co
  */
 int nw_adjoint(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, const nw_time* t,
                const nw_storage* st, const nw_tuning* tune, const void* grad_traces, void* work,
-               double* grad_acc, void* lambda0, void* mu1, void* stream);
+               void* grad_acc, void* lambda0, void* mu1, void* stream);
 
 /*
- * Reduce gradient accumulators (n_acc float64 fields holding c2dt2 * dJ/dc2dt2, as nw_adjoint
- * leaves them) and apply the chain rule of c2dt2 = pad_replicate(c)^2 dt^2: grad_c (physical
+ * Reduce gradient accumulators (n_acc fields in the grid's dtype holding c2dt2 * dJ/dc2dt2, as
+ * nw_adjoint leaves them) in float64 and apply the chain rule of c2dt2 = pad_replicate(c)^2 dt^2: grad_c (physical
  * grid, float64) = pad_replicate^T(2 c_pad dt2 * sum_acc g / (c_pad^2 dt2))
  * (nefi/physics/wave.py:231-240, 718).
  * `accumulate` != 0 adds into grad_c instead of overwriting it.
  */
 int nw_reduce_grad_c(const nw_grid* g, const int32_t* n_abs, const void* c, double dt2,
-                     int32_t n_acc, const double* grad_acc, int32_t accumulate, double* grad_c,
+                     int32_t n_acc, const void* grad_acc, int32_t accumulate, double* grad_c,
                      void* stream);
 
 /*
@@ -240,7 +252,7 @@ int nw_reduce_grad_c(const nw_grid* g, const int32_t* n_abs, const void* c, doub
 int nw_initial_state_adjoint(const nw_grid* g, const int32_t* n_abs, const nw_medium* m,
                              const nw_time* t, int32_t n_shots, const void* lambda0,
                              const void* mu1, const void* p0_level, void* grad_p0,
-                             double* grad_acc, int32_t shots_per_acc, void* stream);
+                             void* grad_acc, int32_t shots_per_acc, void* stream);
 
 /*
  * Allocation-free gradient: the work of nw_adjoint followed by nw_reduce_grad_c (overwriting
@@ -253,8 +265,8 @@ int nw_initial_state_adjoint(const nw_grid* g, const int32_t* n_abs, const nw_me
  * that must not call cudaMalloc, which synchronises the device. The caller still passes every
  * input and the output grad_c (physical grid, float64).
  *  - Limit: 3 * n_shots * field_elems * sizeof(dtype), rounded up to 256 bytes, plus
- *    nw_adjoint_groups() * field_elems * 8 bytes must not exceed NW_NOALLOC_SCRATCH_BYTES (64 MiB);
- *    e.g. 8 float32 shots on a 552^2 padded grid fit, 16 do not. Larger requests return
+ *    nw_adjoint_groups() * field_elems * sizeof(dtype) bytes must not exceed NW_NOALLOC_SCRATCH_BYTES (64 MiB);
+ *    e.g. 16 float32 shots on a 552^2 padded grid fit, 20 do not. Larger requests return
  *    NW_ERR_ARG with a message giving the size needed; use nw_adjoint then.
  *  - Every GPU that loads the library holds the 64 MiB array until the process exits.
  *  - The first call on a device looks up the array's device address (with that device current) and

@@ -36,8 +36,9 @@ class Grid(C.Structure):
 
 
 class Tuning(C.Structure):
-    _fields_ = [("vz", C.c_int32), ("rx", C.c_int32), ("shots_per_cta", C.c_int32),
-                ("adj_shots_per_cta", C.c_int32), ("reserved", C.c_int32 * 4)]
+    _fields_ = [("vz", C.c_int32), ("rx", C.c_int32), ("ctas_per_sm", C.c_int32),
+                ("adj_vz", C.c_int32), ("adj_rx", C.c_int32), ("adj_ctas_per_sm", C.c_int32),
+                ("reserved", C.c_int32 * 2)]
 
 
 class Acquisition(C.Structure):
@@ -50,6 +51,7 @@ class Acquisition(C.Structure):
         ("cell_weight", C.c_void_p),
         ("tiles_z", C.c_int32), ("tile_rows", C.c_int32), ("tile_cols", C.c_int32),
         ("rec_corner", C.c_void_p), ("tile_rec_ptr", C.c_void_p), ("tile_rec_list", C.c_void_p),
+        ("adj_tiles_z", C.c_int32), ("adj_tile_rows", C.c_int32), ("adj_tile_cols", C.c_int32),
         ("tile_cell_ptr", C.c_void_p), ("tile_cell_local", C.c_void_p), ("tile_cell_gid", C.c_void_p),
     ]
 
@@ -78,7 +80,7 @@ _SIGNATURES = {
     "nw_snapshot_bytes": (C.c_size_t, [P(Grid), C.c_int32, C.c_int32, C.c_int32]),
     "nw_prepare_medium": (C.c_int, [P(Grid), VP, VP, C.c_double, VP, VP]),
     "nw_initial_state": (C.c_int, [P(Grid), VP, P(Medium), C.c_int32, VP, VP, VP, VP]),
-    "nw_tile_shape": (C.c_int, [P(Grid), P(Tuning), P(C.c_int32), P(C.c_int32)]),
+    "nw_tile_shape": (C.c_int, [P(Grid), P(Tuning), P(C.c_int32)]),
     "nw_adjoint_groups": (C.c_int, [P(Grid), P(Tuning), C.c_int32]),
     "nw_forward": (C.c_int, [P(Grid), P(Medium), P(Acquisition), P(Time), P(Storage), P(Tuning),
                              C.c_int32, C.c_int32, VP, VP]),

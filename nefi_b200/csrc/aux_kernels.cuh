@@ -134,11 +134,11 @@ __global__ void initial_adjoint_kernel(KGrid<T> g, PadMap pm, int ndim, const T*
                                        const T* __restrict__ B, int b_one, int n_shots, int spa,
                                        const T* __restrict__ lam0, const T* __restrict__ mu1,
                                        const T* __restrict__ p0, T* __restrict__ grad_p0,
-                                       double* __restrict__ acc) {
+                                       T* __restrict__ acc) {
   const int grp = blockIdx.y;
   const long long cells = (long long)g.n0 * g.n1 * g.n2;
   const long long pcells = (long long)pm.m0 * pm.m1 * pm.m2;
-  double* ga = acc ? acc + (long long)grp * g.field : nullptr;
+  T* ga = acc ? acc + (long long)grp * g.field : nullptr;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < cells;
        t += (long long)gridDim.x * blockDim.x) {
     int x, y, z;
@@ -157,7 +157,7 @@ __global__ void initial_adjoint_kernel(KGrid<T> g, PadMap pm, int ndim, const T*
       };
       auto hl = [&](long long k) -> T { return (T(0.5) * C[k]) * lm1(k); };
       const T l = lm1(i);
-      if (ga) ga[i] += (double)(C[i] * ((T(0.5) * l) * lap_at<T, R>(g, p0 + so, i, ndim)));
+      if (ga) ga[i] += C[i] * ((T(0.5) * l) * lap_at<T, R>(g, p0 + so, i, ndim));
       if (!phys) continue;
       T lh;
       if (ndim == 2) {
@@ -179,7 +179,7 @@ __global__ void initial_adjoint_kernel(KGrid<T> g, PadMap pm, int ndim, const T*
 // grad_c[phys] (+)= 2 c dt2 * dJ/dC, dJ/dC = sum_acc sum_{padded cells -> phys} g_acc[cell] / C, in float64.
 template <typename T>
 __global__ void reduce_grad_kernel(KGrid<T> g, PadMap pm, int ndim, const T* __restrict__ c,
-                                   double dt2, int n_acc, const double* __restrict__ gs,
+                                   double dt2, int n_acc, const T* __restrict__ gs,
                                    int accumulate, double* __restrict__ out) {
   const long long pcells = (long long)pm.m0 * pm.m1 * pm.m2;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < pcells;
@@ -195,7 +195,7 @@ __global__ void reduce_grad_kernel(KGrid<T> g, PadMap pm, int ndim, const T* __r
     const int z0 = ndim == 3 ? lo(k, pm.a2, pm.m2) : 0, z1 = ndim == 3 ? hi(k, pm.a2, pm.m2) : 0;
     double acc = 0.0;
     for (int s = 0; s < n_acc; ++s) {
-      const double* gp = gs + (long long)s * g.field;
+      const T* gp = gs + (long long)s * g.field;
       for (int x = x0; x <= x1; ++x)
         for (int y = y0; y <= y1; ++y)
           for (int z = z0; z <= z1; ++z) acc += gp[ghost_index(g, ndim, x, y, z)];

@@ -54,7 +54,7 @@ struct Step3 {
   int n_rec, n_t, j;
   T* __restrict__ lap_out;             // forward, non-null: also store Lap p^n (the gradient factor)
   const T* __restrict__ lap;           // adjoint: Lap p^n as the forward stored it (nullptr: no gradient)
-  double* __restrict__ grad;           // adjoint: per-shot float64 accumulators of C dJ/dC
+  T* __restrict__ grad;                // adjoint: per-shot accumulators of C dJ/dC
 };
 
 __device__ __forceinline__ long long global_thread_in_shot() {
@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(256) step3d(KGrid<T> g, Step3<T> a) {
         if (dx >= 0 && dx <= 1 && dy >= 0 && dy <= 1 && dz >= 0 && dz <= 1) rhs += sw[4 * dx + 2 * dy + dz] * wn;
       }
       a.next[so + i] = (layer && (!ADJ || a.apply_a)) ? av * rhs : rhs;
-      if (ln) a.grad[so + i] += (double)(c * ln[i]);
+      if (ln) a.grad[so + i] += c * ln[i];
     }
   }
 }

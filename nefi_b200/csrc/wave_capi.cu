@@ -200,28 +200,61 @@ int snap_load(const nw_grid* g, const nw_storage* st, int n_shots, int j, T* lm1
 }
 
 // ---- launch shapes ------------------------------------------------------------------------
-struct Tune {
-  int vz, rx, spc, adj_spc;
+constexpr int kSMs = 148;  // B200: grids of the 2-D steps are a multiple of its SM count
+
+struct TileCfg {  // one 2-D step kernel's tile: 8*rx rows by 32*vz columns, cps CTAs per SM
+  int vz, rx, cps;
+  int tx() const { return 8 * rx; }
+  int tz() const { return 32 * vz; }
+  int tiles_z(const nw_grid* g) const { return (g->n[1] + tz() - 1) / tz(); }
+  int n_tiles(const nw_grid* g) const { return tiles_z(g) * ((g->n[0] + tx() - 1) / tx()); }
+  // CTAs of one launch over n_shots shots: at most one per (tile, shot) unit
+  int ctas(const nw_grid* g, int n_shots) const {
+    return (int)std::min<long long>((long long)n_tiles(g) * n_shots, (long long)cps * kSMs);
+  }
 };
+struct Tune {
+  TileCfg fwd, adj;
+};
+
+int check_tile(const nw_grid* g, const TileCfg& c, const char* which) {
+  const std::string w(which);
+  if (g->dtype == NW_F32 && c.vz != 2 && c.vz != 4) return fail(NW_ERR_ARG, "tuning." + w + "vz must be 2 or 4 for float32");
+  if (g->dtype == NW_F64 && c.vz != 2) return fail(NW_ERR_ARG, "tuning." + w + "vz must be 2 for float64");
+  if (c.rx != 2 && c.rx != 4 && c.rx != 8) return fail(NW_ERR_ARG, "tuning." + w + "rx must be 2, 4 or 8");
+  if (c.cps < 1 || c.cps > 32) return fail(NW_ERR_ARG, "tuning." + w + "ctas_per_sm must be in [1, 32]");
+  return NW_OK;
+}
 
 int resolve_tune(const nw_grid* g, const nw_tuning* t, Tune* out) {
   Tune r;
-  // defaults: the best combined forward + adjoint time of a sweep on a 552^2 x 16-shot grid
-  r.vz = (t && t->vz) ? t->vz : 2;
-  r.rx = (t && t->rx) ? t->rx : 4;
-  r.spc = (t && t->shots_per_cta) ? t->shots_per_cta : 2;
-  r.adj_spc = (t && t->adj_shots_per_cta) ? t->adj_shots_per_cta : 4;
-  if (g->ndim == 3) r.spc = r.adj_spc = 1;
-  if (g->dtype == NW_F32 && r.vz != 2 && r.vz != 4) return fail(NW_ERR_ARG, "tuning.vz must be 2 or 4 for float32");
-  if (g->dtype == NW_F64 && r.vz != 2) return fail(NW_ERR_ARG, "tuning.vz must be 2 for float64");
-  if (r.rx != 2 && r.rx != 4 && r.rx != 8) return fail(NW_ERR_ARG, "tuning.rx must be 2, 4 or 8");
-  if (r.spc < 1 || r.adj_spc < 1) return fail(NW_ERR_ARG, "tuning shots per CTA must be >= 1");
+  // defaults: the best forward and adjoint times of a sweep on a 552^2 x 16-shot grid
+  r.fwd.vz = (t && t->vz) ? t->vz : 2;
+  r.fwd.rx = (t && t->rx) ? t->rx : 4;
+  r.fwd.cps = (t && t->ctas_per_sm) ? t->ctas_per_sm : 3;
+  r.adj.vz = (t && t->adj_vz) ? t->adj_vz : 2;
+  r.adj.rx = (t && t->adj_rx) ? t->adj_rx : 2;
+  r.adj.cps = (t && t->adj_ctas_per_sm) ? t->adj_ctas_per_sm : 2;
+  int rc = check_tile(g, r.fwd, "");
+  if (rc) return rc;
+  rc = check_tile(g, r.adj, "adj_");
+  if (rc) return rc;
   *out = r;
   return NW_OK;
 }
 
-int n_groups(const nw_grid* g, const Tune& t, int n_shots) {
-  return g->ndim == 3 ? n_shots : (n_shots + t.adj_spc - 1) / t.adj_spc;
+// Accumulator fields the adjoint fills: one per shot in 3-D; in 2-D, for the CTA ranges of
+// step2d, the largest number of CTAs that hold units of one tile.
+int n_acc_fields(const nw_grid* g, const Tune& t, int n_shots) {
+  if (g->ndim == 3) return n_shots;
+  const long long T = t.adj.n_tiles(g), U = T * n_shots, G = t.adj.ctas(g, n_shots);
+  int m = 1;
+  for (long long tile = 0; tile < T; ++tile) {
+    const int c0 = nw::first_cta_of_unit(tile * n_shots, U, G);
+    const int c1 = nw::first_cta_of_unit(tile * n_shots + n_shots - 1, U, G);
+    m = std::max(m, c1 - c0 + 1);
+  }
+  return m;
 }
 
 // Dynamic shared memory of step2d: C, the copy ring (halo tile + core tile, and the Lap p core
@@ -229,7 +262,7 @@ int n_groups(const nw_grid* g, const Tune& t, int n_shots) {
 template <typename T, int R, int VZ, int RX, bool ADJ>
 constexpr size_t step2_smem() {
   using S = nw::Tile2Shape<T, VZ, RX, R>;
-  return (ADJ ? 2 * S::QS + S::NS * (S::PS + 2 * S::QS) : S::QS + S::NS * (S::PS + S::QS)) * sizeof(T);
+  return (ADJ ? S::NS * (S::PS + 3 * S::QS) + S::QS : S::NS * (S::PS + 2 * S::QS)) * sizeof(T);
 }
 constexpr size_t kMaxSmem = 227 * 1024;  // opt-in shared memory per CTA on sm_100a
 
@@ -261,9 +294,10 @@ int launch_pdl(K kernel, dim3 grid, size_t smem, cudaStream_t s, Args... args) {
   return NW_OK;
 }
 
-nw::TileTables tile_tables(const nw_acquisition* a) {
+nw::TileTables tile_tables(const nw_grid* g, const nw_acquisition* a, const TileCfg& c) {
   nw::TileTables tt;
-  tt.tiles_z = a->tiles_z;
+  tt.tiles_z = c.tiles_z(g);
+  tt.n_tiles = c.n_tiles(g);
   tt.rec_ptr = a->tile_rec_ptr;
   tt.rec_list = a->tile_rec_list;
   tt.rec_corner = a->rec_corner;
@@ -276,24 +310,21 @@ nw::TileTables tile_tables(const nw_acquisition* a) {
 }
 
 template <typename T, int R, int VZ, int RX, bool AB, bool ADJ>
-int launch_step2(const nw_grid* g, const nw::KGrid<T>& kg, const nw::Tiled2<T>& st, cudaStream_t s) {
-  using S = nw::Tile2Shape<T, VZ, RX, R>;
+int launch_step2(const nw::KGrid<T>& kg, const nw::Tiled2<T>& st, int n_ctas, cudaStream_t s) {
   constexpr size_t smem = step2_smem<T, R, VZ, RX, ADJ>();
-  if (smem > kMaxSmem) return fail(NW_ERR_ARG, "tile too large for shared memory (lower tuning.rx or vz)");
+  if (smem > kMaxSmem) return fail(NW_ERR_ARG, "tile too large for shared memory (lower tuning rx or vz)");
   static bool done = false;
   int rc = allow_smem(nw::step2d<T, R, VZ, RX, AB, ADJ>, smem, &done);
   if (rc) return rc;
-  dim3 grid((g->n[1] + S::TZ - 1) / S::TZ, (g->n[0] + S::TX - 1) / S::TX,
-            (st.n_shots + st.shots_per_cta - 1) / st.shots_per_cta);
-  return launch_pdl(nw::step2d<T, R, VZ, RX, AB, ADJ>, grid, smem, s, kg, st);
+  return launch_pdl(nw::step2d<T, R, VZ, RX, AB, ADJ>, dim3(n_ctas, 1, 1), smem, s, kg, st);
 }
 template <typename T, int R, int VZ, int RX, bool AB>
-int launch_fwd2_v(const nw_grid* g, const nw::KGrid<T>& kg, const nw::Tiled2<T>& st, cudaStream_t s) {
-  return launch_step2<T, R, VZ, RX, AB, false>(g, kg, st, s);
+int launch_fwd2_v(const nw::KGrid<T>& kg, const nw::Tiled2<T>& st, int n_ctas, cudaStream_t s) {
+  return launch_step2<T, R, VZ, RX, AB, false>(kg, st, n_ctas, s);
 }
 template <typename T, int R, int VZ, int RX, bool AB>
-int launch_adj2_v(const nw_grid* g, const nw::KGrid<T>& kg, const nw::Tiled2<T>& st, cudaStream_t s) {
-  return launch_step2<T, R, VZ, RX, AB, true>(g, kg, st, s);
+int launch_adj2_v(const nw::KGrid<T>& kg, const nw::Tiled2<T>& st, int n_ctas, cudaStream_t s) {
+  return launch_step2<T, R, VZ, RX, AB, true>(kg, st, n_ctas, s);
 }
 
 // 3-D step: forward (ADJ = false) or adjoint.
@@ -369,14 +400,13 @@ int forward_step(const nw_grid* g, const nw::KGrid<T>& kg, const nw_medium* m, c
     st.wavelet = (const T*)a->wavelet;
     st.n = n;
     st.n_shots = a->n_shots;
-    st.shots_per_cta = tu.spc;
     st.traces = rec ? traces : nullptr;
     st.rec_w = (const T*)a->rec_weight;
     st.n_rec = a->n_rec;
     st.n_t = t->n_t;
     st.j = n / t->substeps;
-    st.tt = tile_tables(a);
-    return NW_DISPATCH2(launch_fwd2_v, T, tu, g, kg, st, s);
+    st.tt = tile_tables(g, a, tu.fwd);
+    return NW_DISPATCH2(launch_fwd2_v, T, tu.fwd, kg, st, tu.fwd.ctas(g, a->n_shots), s);
   }
   nw::Step3<T> st = {};
   st.prev = L.at(n - 1);
@@ -435,7 +465,7 @@ int grid_blocks(long long work, int threads) {
 
 template <typename T>
 int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, const nw_time* t,
-                 const nw_storage* st, const Tune& tu, const T* gtr, T* work, double* gacc, T* lambda0,
+                 const nw_storage* st, const Tune& tu, const T* gtr, T* work, T* gacc, T* lambda0,
                  T* mu1, cudaStream_t s) {
   const int N = t->n_steps, M = t->substeps, S = a->n_shots;
   const long long LE = (long long)S * g->field_elems;
@@ -443,7 +473,7 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
   const nw::KGrid<T> kg = kgrid<T>(g);
   const bool ab = m->coef_a != nullptr;
   NW_CUDA(cudaMemsetAsync(work, 0, 3 * lvl_bytes, s));
-  NW_CUDA(cudaMemsetAsync(gacc, 0, (size_t)n_groups(g, tu, S) * g->field_elems * sizeof(double), s));
+  NW_CUDA(cudaMemsetAsync(gacc, 0, (size_t)n_acc_fields(g, tu, S) * g->field_elems * sizeof(T), s));
   auto q = [&](int n) { return work + (long long)(n % 3) * LE; };  // q^n = C mu^n, three levels
   const bool hist = st->history != nullptr;
   const bool ckpt = !hist && st->snap != nullptr;
@@ -477,14 +507,13 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
     as.lap = lap;
     as.gacc = gacc;
     as.n_shots = S;
-    as.shots_per_cta = tu.adj_spc;
     as.gtr = (a->n_cells > 0 && n % M == 0) ? gtr : nullptr;
     as.gcell_w = (const T*)a->cell_weight;
     as.n_rec = a->n_rec;
     as.n_t = t->n_t;
     as.j = n / M;
-    as.tt = tile_tables(a);
-    return NW_DISPATCH2(launch_adj2_v, T, tu, g, kg, as, s);
+    as.tt = tile_tables(g, a, tu.adj);
+    return NW_DISPATCH2(launch_adj2_v, T, tu.adj, kg, as, tu.adj.ctas(g, S), s);
   };
   if (N >= n_stop) {  // level N: q^N = A C R^T g_N (q^{N+1} = q^{N+2} = 0)
     int rc = g->ndim == 2 ? step2(N, nullptr) : inject3(N);
@@ -661,37 +690,43 @@ static int check_run(const nw_grid* g, const nw_medium* m, const nw_acquisition*
   if (t->substeps < 1 || t->n_t < 1 || t->n_steps != (t->n_t - 1) * t->substeps)
     return fail(NW_ERR_ARG, "inconsistent time axis");
   if (g->ndim == 2) {
-    const int tx = 8 * tu.rx, tz = 32 * tu.vz;
-    if (a->tile_rows != tx || a->tile_cols != tz)
+    if (a->tile_rows != tu.fwd.tx() || a->tile_cols != tu.fwd.tz() || a->tiles_z != tu.fwd.tiles_z(g) ||
+        a->adj_tile_rows != tu.adj.tx() || a->adj_tile_cols != tu.adj.tz() || a->adj_tiles_z != tu.adj.tiles_z(g))
       return fail(NW_ERR_ARG, "per-tile tables were built for another tile shape (see nw_tile_shape)");
-    if (a->tiles_z != (g->n[1] + tz - 1) / tz || !a->tile_rec_ptr || !a->tile_cell_ptr || !a->rec_corner ||
+    if (!a->tile_rec_ptr || !a->tile_cell_ptr || !a->rec_corner ||
         (a->n_cells > 0 && (!a->tile_cell_local || !a->tile_cell_gid)) || (a->n_rec > 0 && !a->tile_rec_list))
       return fail(NW_ERR_ARG, "2-D grids need the per-tile receiver tables");
   }
   return NW_OK;
 }
 
-int nw_tile_shape(const nw_grid* g, nw_tuning* t, int32_t* tx, int32_t* tz) {
+int nw_tile_shape(const nw_grid* g, nw_tuning* t, int32_t* shape) {
   int rc = check_grid(g);
   if (rc) return rc;
   Tune tu;
   rc = resolve_tune(g, t, &tu);
   if (rc) return rc;
   if (t) {
-    t->vz = tu.vz;
-    t->rx = tu.rx;
-    t->shots_per_cta = tu.spc;
-    t->adj_shots_per_cta = tu.adj_spc;
+    t->vz = tu.fwd.vz;
+    t->rx = tu.fwd.rx;
+    t->ctas_per_sm = tu.fwd.cps;
+    t->adj_vz = tu.adj.vz;
+    t->adj_rx = tu.adj.rx;
+    t->adj_ctas_per_sm = tu.adj.cps;
   }
-  if (tx) *tx = 8 * tu.rx;
-  if (tz) *tz = 32 * tu.vz;
+  if (shape) {
+    shape[0] = tu.fwd.tx();
+    shape[1] = tu.fwd.tz();
+    shape[2] = tu.adj.tx();
+    shape[3] = tu.adj.tz();
+  }
   return NW_OK;
 }
 
 int nw_adjoint_groups(const nw_grid* g, const nw_tuning* t, int32_t n_shots) {
   Tune tu;
   if (check_grid(g) || resolve_tune(g, t, &tu) || n_shots < 1) return -1;
-  return n_groups(g, tu, n_shots);
+  return n_acc_fields(g, tu, n_shots);
 }
 
 int nw_forward(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, const nw_time* t,
@@ -712,7 +747,7 @@ int nw_forward(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, co
 
 int nw_adjoint(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, const nw_time* t,
                const nw_storage* st, const nw_tuning* tune, const void* grad_traces, void* work,
-               double* grad_acc, void* lambda0, void* mu1, void* stream) {
+               void* grad_acc, void* lambda0, void* mu1, void* stream) {
   int rc = check_grid(g);
   if (rc) return rc;
   Tune tu;
@@ -725,14 +760,14 @@ int nw_adjoint(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, co
     return fail(NW_ERR_ARG, "receiver adjoint table is NULL");
   if (!st->history && st->snap && !st->segbuf) return fail(NW_ERR_ARG, "checkpointing needs segbuf");
   if (g->dtype == NW_F32)
-    return adjoint_impl<float>(g, m, a, t, st, tu, (const float*)grad_traces, (float*)work, grad_acc,
+    return adjoint_impl<float>(g, m, a, t, st, tu, (const float*)grad_traces, (float*)work, (float*)grad_acc,
                                (float*)lambda0, (float*)mu1, (cudaStream_t)stream);
-  return adjoint_impl<double>(g, m, a, t, st, tu, (const double*)grad_traces, (double*)work, grad_acc,
+  return adjoint_impl<double>(g, m, a, t, st, tu, (const double*)grad_traces, (double*)work, (double*)grad_acc,
                               (double*)lambda0, (double*)mu1, (cudaStream_t)stream);
 }
 
 int nw_reduce_grad_c(const nw_grid* g, const int32_t* n_abs, const void* c, double dt2,
-                     int32_t n_acc, const double* grad_acc, int32_t accumulate, double* grad_c,
+                     int32_t n_acc, const void* grad_acc, int32_t accumulate, double* grad_c,
                      void* stream) {
   int rc = check_grid(g);
   if (rc) return rc;
@@ -743,10 +778,10 @@ int nw_reduce_grad_c(const nw_grid* g, const int32_t* n_abs, const void* c, doub
   const int blocks = grid_blocks(pcells, 128);
   if (g->dtype == NW_F32)
     nw::reduce_grad_kernel<float><<<blocks, 128, 0, s>>>(kgrid<float>(g), pm, g->ndim, (const float*)c, dt2,
-                                                         n_acc, grad_acc, accumulate, grad_c);
+                                                         n_acc, (const float*)grad_acc, accumulate, grad_c);
   else
     nw::reduce_grad_kernel<double><<<blocks, 128, 0, s>>>(kgrid<double>(g), pm, g->ndim, (const double*)c,
-                                                          dt2, n_acc, grad_acc, accumulate, grad_c);
+                                                          dt2, n_acc, (const double*)grad_acc, accumulate, grad_c);
   NW_LAUNCHED();
   return NW_OK;
 }
@@ -754,7 +789,7 @@ int nw_reduce_grad_c(const nw_grid* g, const int32_t* n_abs, const void* c, doub
 int nw_initial_state_adjoint(const nw_grid* g, const int32_t* n_abs, const nw_medium* m,
                              const nw_time* t, int32_t n_shots, const void* lambda0,
                              const void* mu1, const void* p0_level, void* grad_p0,
-                             double* grad_acc, int32_t shots_per_acc, void* stream) {
+                             void* grad_acc, int32_t shots_per_acc, void* stream) {
   int rc = check_grid(g);
   if (rc) return rc;
   if (!m || !t || !n_abs || !lambda0 || !mu1 || !p0_level || !grad_p0 || n_shots < 1 || shots_per_acc < 1)
@@ -769,7 +804,7 @@ int nw_initial_state_adjoint(const nw_grid* g, const int32_t* n_abs, const nw_me
   nw::initial_adjoint_kernel<T, R><<<gc, 256, 0, s>>>(kgrid<T>(g), pm, g->ndim, (const T*)m->c2dt2,       \
                                                       (const T*)m->coef_b, b_one, n_shots, shots_per_acc, \
                                                       (const T*)lambda0, (const T*)mu1, (const T*)p0_level, \
-                                                      (T*)grad_p0, grad_acc)
+                                                      (T*)grad_p0, (T*)grad_acc)
   if (g->dtype == NW_F32) { if (g->radius == 1) NW_IA(float, 1); else NW_IA(float, 2); }
   else { if (g->radius == 1) NW_IA(double, 1); else NW_IA(double, 2); }
 #undef NW_IA
@@ -863,8 +898,8 @@ int noalloc_gradient(const nw_grid* g, const int32_t* n_abs, const nw_medium* m,
                      const T* gtr, double* grad_c, cudaStream_t s) {
   const size_t work_bytes = 3 * (size_t)a->n_shots * g->field_elems * sizeof(T);
   const size_t acc_off = (work_bytes + 255) / 256 * 256;
-  const int n_acc = n_groups(g, tu, a->n_shots);
-  const size_t need = acc_off + (size_t)n_acc * g->field_elems * sizeof(double);
+  const int n_acc = n_acc_fields(g, tu, a->n_shots);
+  const size_t need = acc_off + (size_t)n_acc * g->field_elems * sizeof(T);
   if (need > NW_NOALLOC_SCRATCH_BYTES)
     return fail(NW_ERR_ARG, "nw_adjoint_grad_c_noalloc needs " + std::to_string(need) +
                                 " bytes of scratch, above its fixed " + std::to_string(NW_NOALLOC_SCRATCH_BYTES) +
@@ -873,7 +908,7 @@ int noalloc_gradient(const nw_grid* g, const int32_t* n_abs, const nw_medium* m,
   int rc = noalloc_scratch(&base);
   if (rc) return rc;
   T* work = reinterpret_cast<T*>(base);
-  double* acc = reinterpret_cast<double*>(reinterpret_cast<char*>(base) + acc_off);
+  T* acc = reinterpret_cast<T*>(reinterpret_cast<char*>(base) + acc_off);
   // adjoint_impl clears the work levels and the accumulators on `s` before using them, so the
   // previous call's contents never leak into this one.
   rc = adjoint_impl<T>(g, m, a, t, st, tu, gtr, work, acc, nullptr, nullptr, s);

@@ -220,7 +220,7 @@ def _adjoint_sweep(plan: DevicePlan, medium, acq, run: _Run, grad_traces: torch.
     lib = _lib.load()
     S = run.n_shots
     work = plan.empty_levels(3, S, zero=False)
-    gC = torch.empty(plan.n_acc(S), plan.field, device=plan.device, dtype=torch.float64)
+    gC = torch.empty(plan.n_acc(S), plan.field, device=plan.device, dtype=plan.dtype)
     lam0 = mu1 = None
     if want_initial:
         lam0 = plan.empty_levels(1, S, zero=False)[0]
@@ -518,7 +518,7 @@ class _PATFunction(torch.autograd.Function):
         _lib.check(lib.nw_initial_state_adjoint(C.byref(plan.g), plan.n_abs, C.byref(medium),
                                                 C.byref(plan.time), S, lam0.data_ptr(), mu1.data_ptr(),
                                                 p0l.data_ptr(), grad_p0.data_ptr(),
-                                                gC.data_ptr() if need_c else None, plan.shots_per_acc,
+                                                gC.data_ptr() if need_c else None, plan.shots_per_acc(S),
                                                 stream))
         grad_c = None
         if need_c:

@@ -130,28 +130,31 @@ class DevicePlan:
         self._cells = cells
         self.set_tuning(*(getattr(op, "tuning", None) or ()))
 
-    def set_tuning(self, vz: int = 0, rx: int = 0, shots_per_cta: int = 0, adj_shots_per_cta: int = 0) -> None:
-        """Choose the 2-D launch shape (0 = library default) and build the per-tile tables."""
-        t = _lib.Tuning(int(vz), int(rx), int(shots_per_cta), int(adj_shots_per_cta))
-        tx, tz = C.c_int32(), C.c_int32()
-        _lib.check(_lib.load().nw_tile_shape(C.byref(self.g), C.byref(t), C.byref(tx), C.byref(tz)))
+    def set_tuning(self, vz: int = 0, rx: int = 0, ctas_per_sm: int = 0, adj_vz: int = 0, adj_rx: int = 0,
+                   adj_ctas_per_sm: int = 0) -> None:
+        """Choose the 2-D launch shapes (0 = library default) and build the per-tile tables."""
+        t = _lib.Tuning(int(vz), int(rx), int(ctas_per_sm), int(adj_vz), int(adj_rx), int(adj_ctas_per_sm))
+        shape = (C.c_int32 * 4)()
+        _lib.check(_lib.load().nw_tile_shape(C.byref(self.g), C.byref(t), shape))
         self.tuning = t
-        self.tile = (tx.value, tz.value)
-        self.tiles_z = 0
+        self.tile = (shape[0], shape[1])       # forward steps
+        self.adj_tile = (shape[2], shape[3])   # adjoint steps
+        self.tiles_z = self.adj_tiles_z = 0
         self.rec_corner = self.tile_rec_ptr = self.tile_rec_list = None
         self.tile_cell_ptr = self.tile_cell_local = self.tile_cell_gid = None
         if self.g.ndim == 2:
             self._build_tile_tables()
 
     def _build_tile_tables(self) -> None:
-        """Per-tile receiver and adjoint-source tables for the 2-D tiled kernels.
+        """Per-tile receiver tables (forward tile shape) and adjoint-source tables (adjoint tile
+        shape) for the 2-D step kernels.
 
         A receiver belongs to the tile holding its stencil's lower corner (its other corners lie
         in that tile's one-cell halo); a receiver-touched cell belongs to the tile containing it.
         Lists keep ascending receiver / cell order inside each tile.
         """
-        TX, TZ = self.tile
         g = self.g
+        TX, TZ = self.tile
         tiles_z = -(-g.n[1] // TZ)
         n_tiles = tiles_z * -(-g.n[0] // TX)
         corner = self._corner
@@ -159,15 +162,18 @@ class DevicePlan:
         order = torch.argsort(tile_of, stable=True)
         rptr = torch.zeros(n_tiles + 1, dtype=torch.int64)
         rptr[1:] = torch.cumsum(torch.bincount(tile_of, minlength=n_tiles), 0)
+        AX, AZ = self.adj_tile
+        adj_tiles_z = -(-g.n[1] // AZ)
+        n_adj_tiles = adj_tiles_z * -(-g.n[0] // AX)
         rel = self._cells - int(g.origin)
         x, z = rel // int(g.stride[0]), rel % int(g.stride[0])
-        ctile = (x // TX) * tiles_z + z // TZ
+        ctile = (x // AX) * adj_tiles_z + z // AZ
         corder = torch.argsort(ctile, stable=True)
-        cptr = torch.zeros(n_tiles + 1, dtype=torch.int64)
-        cptr[1:] = torch.cumsum(torch.bincount(ctile, minlength=n_tiles), 0)
-        local = (x % TX) * TZ + z % TZ
+        cptr = torch.zeros(n_adj_tiles + 1, dtype=torch.int64)
+        cptr[1:] = torch.cumsum(torch.bincount(ctile, minlength=n_adj_tiles), 0)
+        local = (x % AX) * AZ + z % AZ
         dev, i32 = self.device, torch.int32
-        self.tiles_z = tiles_z
+        self.tiles_z, self.adj_tiles_z = tiles_z, adj_tiles_z
         self.rec_corner = corner.to(i32).contiguous().to(dev)
         self.tile_rec_ptr = rptr.to(i32).to(dev)
         self.tile_rec_list = order.to(i32).to(dev)
@@ -176,15 +182,16 @@ class DevicePlan:
         self.tile_cell_gid = corder.to(i32).to(dev)
 
     def n_acc(self, n_shots: int) -> int:
-        """Float64 gradient accumulators the adjoint sweep fills for ``n_shots`` shots."""
+        """Gradient accumulator fields (plan dtype) the adjoint sweep fills for ``n_shots`` shots."""
         n = _lib.load().nw_adjoint_groups(C.byref(self.g), C.byref(self.tuning), n_shots)
         if n < 1:
             raise _lib.LibraryError(_lib.NW_ERR_ARG, "invalid adjoint group query")
         return n
 
-    @property
-    def shots_per_acc(self) -> int:
-        return int(self.tuning.adj_shots_per_cta) if self.g.ndim == 2 else 1
+    def shots_per_acc(self, n_shots: int) -> int:
+        """Shots whose initial-state gradient term goes to one accumulator field: all of them into
+        field 0 in 2-D, one field per shot in 3-D (the adjoint's own layout there)."""
+        return n_shots if self.g.ndim == 2 else 1
 
     # -- descriptors ------------------------------------------------------------------------
     def medium(self, c2dt2: torch.Tensor) -> _lib.Medium:
@@ -212,6 +219,8 @@ class DevicePlan:
             a.rec_corner = self.rec_corner.data_ptr()
             a.tile_rec_ptr = self.tile_rec_ptr.data_ptr()
             a.tile_rec_list = self.tile_rec_list.data_ptr()
+            a.adj_tiles_z = self.adj_tiles_z
+            a.adj_tile_rows, a.adj_tile_cols = self.adj_tile
             a.tile_cell_ptr = self.tile_cell_ptr.data_ptr()
             a.tile_cell_local = self.tile_cell_local.data_ptr()
             a.tile_cell_gid = self.tile_cell_gid.data_ptr()

@@ -253,3 +253,46 @@ def test_oracle_agrees_with_device_float32_on_cfg1(cuda_device):
     otr, ogc = orc.fwi(case["c"], g, dtype=np.float64)
     assert rel_l2(tr, otr[:, :: case["rec_stride"]]) < 1e-5
     assert rel_l2(gc, ogc) < 1e-4
+
+
+def _layered_op(n=200, shots=6, n_t=81, **kw):
+    """A 200^2 (240^2 padded) sponge problem with several shots: big enough that the 2-D step
+    kernels' CTAs take ranges of several (tile, shot) units that cross tile boundaries."""
+    h = 10.0
+    dom = Domain((n, n), ((0.0, n * h), (0.0, n * h)))
+    src = [[(k + 0.5) * n * h / shots, 1.5 * h] for k in range(shots)]
+    rec = [[(i + 0.5) * h, 2.5 * h] for i in range(0, n, 3)]
+    return WaveOperatorB200(dom, src, rec, n_t=n_t, dt_obs=8e-4, f0=15.0, c_max=3000.0, order=4,
+                            absorbing="sponge", absorb_width=20 * h, courant=1.0, grad_mode="autograd", **kw)
+
+
+def _layered_grad(op, dtype, dev, tuning):
+    op.tuning = tuning
+    op._plans.clear()
+    n = op.grid.shape[0]
+    x = torch.linspace(0, 1, n, dtype=torch.float64)
+    c = (2000.0 + 800.0 * x[None, :] + 150.0 * torch.sin(7 * x)[:, None]).to(dtype).to(dev)
+    c.requires_grad_(True)
+    tr = op({"c": c})
+    g = torch.randn(tr.shape, generator=torch.Generator().manual_seed(5), dtype=torch.float64).to(dtype).to(dev)
+    (gc,) = torch.autograd.grad((tr * g).sum(), c)
+    return tr.detach().cpu().numpy(), gc.double().cpu().numpy()
+
+
+# (vz, rx, ctas_per_sm, adj_vz, adj_rx, adj_ctas_per_sm); ctas_per_sm = 1 gives each CTA several units
+LAUNCH_SHAPES = [(2, 2, 1, 2, 2, 1), (2, 8, 2, 2, 4, 3), (4, 4, 3, 4, 8, 1), (4, 2, 8, 2, 2, 8)]
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_results_do_not_depend_on_the_launch_shape(dtype, cuda_device):
+    """Traces are bitwise the same for every tile shape and CTA count (each cell is computed by the
+    same arithmetic); the gradient only regroups its float sums (float64: 1e-12, float32: 1e-5)."""
+    op = _layered_op()
+    tr0, g0 = _layered_grad(op, dtype, cuda_device, (0, 0, 0, 0, 0, 0))
+    assert np.isfinite(g0).all() and np.abs(g0).max() > 0
+    for shape in LAUNCH_SHAPES:
+        if dtype == torch.float64 and (shape[0] == 4 or shape[3] == 4):
+            continue  # float64 tiles are 2 columns per thread
+        tr, g = _layered_grad(op, dtype, cuda_device, shape)
+        assert np.array_equal(tr, tr0), shape
+        assert rel_l2(g, g0) < (1e-12 if dtype == torch.float64 else 1e-5), shape

@@ -97,16 +97,18 @@ def test_adjoint_table_is_cell_major_and_complete():
     assert pairs == ref
 
 
-@pytest.mark.parametrize("tuning", [(0, 0, 0), (2, 2, 1), (4, 8, 3), (2, 4, 16)])
+@pytest.mark.parametrize("tuning", [(0, 0, 0), (2, 2, 1, 2, 8, 1), (4, 8, 3, 4, 2, 2), (2, 4, 16, 2, 4, 5)])
 @pytest.mark.parametrize("name", ["fwi_o4_sponge", "cfg1_128_o4_sponge", "pat2d_o4_sponge"])
 def test_tile_tables_partition_receivers_and_cells(name, tuning):
-    """Every receiver is owned by exactly the tile holding its stencil corner, and every
-    receiver-touched cell appears once, in its own tile, at the right local index."""
+    """Every receiver is owned by exactly the forward tile holding its stencil corner, and every
+    receiver-touched cell appears once, in its own adjoint tile, at the right local index."""
     case = load_golden(name)
     plan = make_op(case)._plan(CPU, torch.float32)
     plan.set_tuning(*tuning)
     TX, TZ = plan.tile
     assert TX == 8 * plan.tuning.rx and TZ == 32 * plan.tuning.vz
+    AX, AZ = plan.adj_tile
+    assert AX == 8 * plan.tuning.adj_rx and AZ == 32 * plan.tuning.adj_vz
     tz = plan.tiles_z
     rptr, rlist = plan.tile_rec_ptr.numpy(), plan.tile_rec_list.numpy()
     corner = plan.rec_corner.numpy()
@@ -114,18 +116,49 @@ def test_tile_tables_partition_receivers_and_cells(name, tuning):
     for t in range(len(rptr) - 1):
         for r in rlist[rptr[t]:rptr[t + 1]]:
             assert (corner[r, 0] // TX) * tz + corner[r, 1] // TZ == t
+    atz = plan.adj_tiles_z
     cptr = plan.tile_cell_ptr.numpy()
     gid, local = plan.tile_cell_gid.numpy(), plan.tile_cell_local.numpy()
     assert sorted(gid.tolist()) == list(range(plan.n_cells))
     cells = plan.cell_index.numpy() - plan.g.origin
     ld = plan.g.stride[0]
     for t in range(len(cptr) - 1):
-        x0, z0 = (t // tz) * TX, (t % tz) * TZ
+        x0, z0 = (t // atz) * AX, (t % atz) * AZ
         for e in range(cptr[t], cptr[t + 1]):
             x, z = divmod(int(cells[gid[e]]), ld)
-            assert x0 <= x < x0 + TX and z0 <= z < z0 + TZ
-            assert local[e] == (x - x0) * TZ + (z - z0)
-    assert plan.n_acc(16) == (-(-16 // plan.tuning.adj_shots_per_cta))
+            assert x0 <= x < x0 + AX and z0 <= z < z0 + AZ
+            assert local[e] == (x - x0) * AZ + (z - z0)
+
+
+def _unit_ranges(n_tiles, n_shots, ctas_per_sm):
+    """CTA b of a 2-D step takes units [b*U/G, (b+1)*U/G), U = tiles x shots, G = min(U, 148 cps)."""
+    U = n_tiles * n_shots
+    G = min(U, ctas_per_sm * 148)
+    return U, G, [(b * U // G, (b + 1) * U // G) for b in range(G)]
+
+
+@pytest.mark.parametrize("n_shots", [1, 3, 16, 64])
+@pytest.mark.parametrize("tuning", [(0, 0, 0), (2, 4, 3, 2, 2, 2), (4, 2, 1, 4, 8, 1)])
+def test_adjoint_accumulator_slots_cover_every_cta_of_a_tile(n_shots, tuning):
+    """The library's accumulator count is exactly the largest number of adjoint CTAs that hold
+    units of one tile, and the slot each CTA writes for a tile (its index among those CTAs) is
+    below that count: every (tile, slot) pair has one writer."""
+    case = load_golden("fwi_o4_sponge")
+    plan = make_op(case)._plan(CPU, torch.float32)
+    plan.set_tuning(*tuning)
+    AX, AZ = plan.adj_tile
+    n_tiles = -(-plan.g.n[0] // AX) * -(-plan.g.n[1] // AZ)
+    U, G, ranges = _unit_ranges(n_tiles, n_shots, plan.tuning.adj_ctas_per_sm)
+    assert ranges[0][0] == 0 and ranges[-1][1] == U
+    assert all(lo < hi for lo, hi in ranges) and all(ranges[b][1] == ranges[b + 1][0] for b in range(G - 1))
+    writers = {}
+    for b, (lo, hi) in enumerate(ranges):
+        for t in range(lo // n_shots, (hi - 1) // n_shots + 1):
+            writers.setdefault(t, []).append(b)
+    n_acc = plan.n_acc(n_shots)
+    assert n_acc == max(len(v) for v in writers.values())
+    for t, bs in writers.items():
+        assert bs == list(range(bs[0], bs[0] + len(bs)))  # consecutive CTAs: slot = b - first
 
 
 def test_reference_errors_are_raised_on_the_host():
