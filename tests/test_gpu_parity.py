@@ -280,7 +280,7 @@ def _layered_grad(op, dtype, dev, tuning):
 
 
 # (vz, rx, ctas_per_sm, adj_vz, adj_rx, adj_ctas_per_sm); ctas_per_sm = 1 gives each CTA several units
-LAUNCH_SHAPES = [(2, 2, 1, 2, 2, 1), (2, 8, 2, 2, 4, 3), (4, 4, 3, 4, 8, 1), (4, 2, 8, 2, 2, 8)]
+LAUNCH_SHAPES = [(2, 2, 1, 2, 2, 1), (2, 8, 2, 2, 4, 3), (4, 4, 3, 4, 2, 1), (4, 2, 8, 2, 8, 8)]
 
 
 @pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
