@@ -78,18 +78,17 @@ typedef struct nw_grid {
 int nw_grid_layout(nw_grid* g);
 
 /*
- * Launch shape of the 2-D step kernels, forward and adjoint separately. A step is a list of
- * (tile, shot) units, a tile being 8*rx rows by 32*vz columns; the launch has
- * min(units, ctas_per_sm * 148) CTAs, each taking a contiguous range of units. Zero fields take
- * the library's defaults. 3-D grids ignore it.
+ * Launch shape of the 2-D step kernels, forward and adjoint separately: a CTA owns a tile of
+ * 8*rx rows by 32*vz columns and loops over shots_per_cta shots. Zero fields take the library's
+ * defaults. 3-D grids ignore it.
  */
 typedef struct nw_tuning {
-  int32_t vz;              /* forward: columns per thread, 2 or 4 (float32), 2 (float64) */
-  int32_t rx;              /* forward: rows per thread, 2, 4 or 8 */
-  int32_t ctas_per_sm;     /* forward: CTAs per SM of the launch, 1..32 */
-  int32_t adj_vz;          /* the same for the adjoint steps */
-  int32_t adj_rx;
-  int32_t adj_ctas_per_sm;
+  int32_t vz;                /* forward: columns per thread, 2 or 4 (float32), 2 (float64) */
+  int32_t rx;                /* forward: rows per thread, 2, 4 or 8 */
+  int32_t shots_per_cta;     /* forward: shots per CTA, >= 1 */
+  int32_t adj_vz;            /* the same for the adjoint steps; adj_shots_per_cta shots share */
+  int32_t adj_rx;            /*   one gradient accumulator field */
+  int32_t adj_shots_per_cta;
   int32_t reserved[2];
 } nw_tuning;
 
@@ -101,7 +100,7 @@ int nw_tile_shape(const nw_grid* g, nw_tuning* t, int32_t* shape);
 
 /*
  * Number of gradient accumulator fields (in the grid's dtype) nw_adjoint fills for n_shots
- * shots: one per shot in 3-D; in 2-D, the largest number of adjoint CTAs sharing one tile.
+ * shots: one per shot in 3-D, one per group of adj_shots_per_cta shots in 2-D.
  */
 int nw_adjoint_groups(const nw_grid* g, const nw_tuning* t, int32_t n_shots);
 

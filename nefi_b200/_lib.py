@@ -36,8 +36,8 @@ class Grid(C.Structure):
 
 
 class Tuning(C.Structure):
-    _fields_ = [("vz", C.c_int32), ("rx", C.c_int32), ("ctas_per_sm", C.c_int32),
-                ("adj_vz", C.c_int32), ("adj_rx", C.c_int32), ("adj_ctas_per_sm", C.c_int32),
+    _fields_ = [("vz", C.c_int32), ("rx", C.c_int32), ("shots_per_cta", C.c_int32),
+                ("adj_vz", C.c_int32), ("adj_rx", C.c_int32), ("adj_shots_per_cta", C.c_int32),
                 ("reserved", C.c_int32 * 2)]
 
 

@@ -1,18 +1,16 @@
 // stencil2d.cuh — tiled 2-D leapfrog kernels for sm_100a.
 //
-// The work of one step is a list of units, (tile, shot) pairs in tile-major order; a tile is
-// TX = 8*RX rows by TZ = 32*VZ columns. The grid is a fixed number of CTAs (8 warps each, a small
-// multiple of the SM count) and CTA b processes the contiguous unit range
-// [b*U/G, (b+1)*U/G), so the load is balanced to one unit and there is no tail wave. For every unit
-// the input tiles (p^n or mu^{n+1} with an R-row and 16-byte-column halo,
+// One CTA (8 warps) owns a tile of TX = 8*RX rows by TZ = 32*VZ columns and loops over a group
+// of shots; the hardware scheduler balances the (tile, shot group) CTAs over the SMs, which
+// absorbs the extra cost of tiles in the absorbing layer. For every shot the input tiles (p^n or mu^{n+1} with an R-row and 16-byte-column halo,
 // and core tiles: p^{n-1}, or mu^{n+2} and the stored Lap p^n) are staged in shared memory by
-// cp.async through a ring of NS buffers, so that the copies of the next NS-1 units are in flight
-// while a unit is computed, across tile boundaries. Each thread computes the shared/global offsets of the 16-byte chunks it
+// cp.async through a ring of NS buffers, so that the copies of the next NS-1 shots are in flight
+// while shot s is computed. Each thread computes the shared/global offsets of the 16-byte chunks it
 // copies once per CTA; per shot it only adds the shot's base address. A thread owns VZ adjacent
 // columns and RX rows: it slides a (2R+1)-row register window down its columns, reading each row
 // once as a VZ-wide vector plus two halo vectors, so every shared-memory access is a
-// conflict-free 8- or 16-byte load. c^2 dt^2 is staged once per tile a CTA enters (a ring of NS
-// tiles); the absorbing A/B are read per row from global memory in layer tiles only (L1 hits).
+// conflict-free 8- or 16-byte load. c^2 dt^2 is staged once per CTA (it is the same for every
+// shot); the absorbing A/B are read per row from global memory in layer tiles only (L1 hits).
 //
 // The step kernels are launched with programmatic dependent launch: each one waits
 // (griddepcontrol.wait) for the previous kernel in the stream to finish and flush before it reads
@@ -93,8 +91,7 @@ __device__ __forceinline__ void vstore(T* p, const T (&o)[N]) {
 
 // Per-tile tables, built on the host for one tile shape (TX, TZ).
 struct TileTables {
-  int tiles_z;                        // tiles along the contiguous axis
-  int n_tiles;
+  int tiles_z;                        // tiles along the contiguous axis (gridDim.x)
   const int* __restrict__ rec_ptr;    // (n_tiles + 1): receivers whose stencil corner is in the tile
   const int* __restrict__ rec_list;   // receiver ids
   const int* __restrict__ rec_corner; // (n_rec, 2) corner cell (x, z)
@@ -122,7 +119,7 @@ struct Tiled2 {
   const T* __restrict__ B;
   int b_one;                    // forward: B = 1 on the first step (Cerjan)
   int apply_a;                  // adjoint: A applies (n >= 1); at n = 0 the output is C lambda^0
-  int n_shots;
+  int n_shots, shots_per_cta;
   // forward: point sources, receiver samples of p^n
   const int* __restrict__ src_corner;
   const T* __restrict__ src_w;
@@ -135,7 +132,7 @@ struct Tiled2 {
   const T* __restrict__ gtr;    // trace cotangents (n_shots, n_rec, n_t); non-null on record steps
   const T* __restrict__ gcell_w;
   const T* __restrict__ lap;    // Lap p^n as the forward step stored it; nullptr: no gradient term
-  T* __restrict__ gacc;         // (n_slots, field) accumulators of C dJ/dC (see step2d)
+  T* __restrict__ gacc;         // (n_groups, field) accumulators of C dJ/dC, one per shot group
   int n_rec, n_t, j;
   TileTables tt;
 };
@@ -227,124 +224,82 @@ __device__ __forceinline__ void store_row(T* dst, const T (&o)[VZ], int zc, int 
 }
 
 
-// First CTA whose unit range holds unit u, for G CTAs over U units (ranges [b*U/G, (b+1)*U/G)).
-__host__ __device__ __forceinline__ int first_cta_of_unit(long long u, long long U, long long G) {
-  return (int)(((u + 1) * G + U - 1) / U - 1);
-}
-
 // ------------------------------------------------------------------------------------------
-// One leapfrog step of every (tile, shot) unit: forward (ADJ = false) or adjoint (ADJ = true).
-// The forward also samples receivers from the staged p^n tile, adds the shots' point sources
-// and, with lap_out, stores Lap p^n; the adjoint adds C R^T g_n at the receiver-touched cells
-// and accumulates q^{n+1} Lap p^n over the shots of a tile in registers. When the CTA leaves a
-// tile it adds that sum into accumulator slot (b - first CTA holding units of the tile): every
-// (tile, slot) has one writer per launch, so the sums are race-free and reproducible.
+// One leapfrog step of every shot of a group over one tile: forward (ADJ = false) or adjoint
+// (ADJ = true). The forward also samples receivers from the staged p^n tile, adds the shots'
+// point sources and, with lap_out, stores Lap p^n; the adjoint adds C R^T g_n at the
+// receiver-touched cells and accumulates q^{n+1} Lap p^n over the group's shots in registers,
+// then adds the sum into the group's accumulator (one writer per cell and group).
 // ------------------------------------------------------------------------------------------
 template <typename T, int R, int VZ, int RX, bool AB, bool ADJ>
 __global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T> a) {
   using S = Tile2Shape<T, VZ, RX, R>;
   constexpr int NS = S::NS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* scc = reinterpret_cast<T*>(smem_raw);  // [NS][QS] C of the last NS tiles entered
-  T* sp = scc + NS * S::QS;                 // [NS][PS] p^n | q^{n+1}, with halo
+  T* scc = reinterpret_cast<T*>(smem_raw);  // [QS] C
+  T* sp = scc + S::QS;                      // [NS][PS] p^n | q^{n+1}, with halo
   T* sq = sp + NS * S::PS;                  // [NS][QS] p^{n-1} | q^{n+2}
   T* sl = sq + NS * S::QS;                  // adjoint: [NS][QS] Lap p^n
-  T* sj = sl + NS * S::QS;                  // adjoint: [QS] cotangent injected at this unit's cells
+  T* sj = sl + NS * S::QS;                  // adjoint: [QS] cotangent injected at this shot's cells
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int lrow = warp * RX;  // first owned row inside the tile
+  const int z0 = blockIdx.x * S::TZ, x0 = blockIdx.y * S::TX;
+  const int tile = blockIdx.y * a.tt.tiles_z + blockIdx.x;
+  const int sb = blockIdx.z * a.shots_per_cta;
+  const int se = min(sb + a.shots_per_cta, a.n_shots);
+  const int zc = z0 + lane * VZ;  // first owned column
+  const int xr = x0 + warp * RX;  // first owned row
+  const int lrow = warp * RX;     // first owned row inside the tile
+  const bool own_cols = zc < g.n1;
   const bool grad = ADJ && a.lap != nullptr;
-  const int nsh = a.n_shots;
-  const long long U = (long long)a.tt.n_tiles * nsh;
-  const int u_lo = (int)(U * blockIdx.x / gridDim.x), u_hi = (int)(U * (blockIdx.x + 1) / gridDim.x);
-  const int t_lo = u_lo / nsh;  // tile ordinal 0 of this CTA: C slot of tile t is (t - t_lo) % NS
 
+  const CopyPlan<S::NCH> ph = plan_halo<T, VZ, RX, R>(g, x0, z0);
+  const CopyPlan<S::NCC> pc = plan_core<T, VZ, RX, R>(g, x0, z0);
   wait_previous_grid();
   allow_next_grid();
-
-  // copy side: chunk plans of the tile whose units are being issued
-  int ptile = -1;
-  CopyPlan<S::NCH> ph;
-  CopyPlan<S::NCC> pc;
-  auto issue_unit = [&](int u) {
-    const int tile = u / nsh, s = u - tile * nsh;
-    if (tile != ptile) {
-      ptile = tile;
-      const int x0 = (tile / a.tt.tiles_z) * S::TX, z0 = (tile % a.tt.tiles_z) * S::TZ;
-      ph = plan_halo<T, VZ, RX, R>(g, x0, z0);
-      pc = plan_core<T, VZ, RX, R>(g, x0, z0);
-    }
-    const int slot = (u - u_lo) % NS;
-    if (u == u_lo || s == 0) issue(pc, a.C, scc + ((tile - t_lo) % NS) * S::QS);
-    issue(ph, a.cur + (long long)s * g.field, sp + slot * S::PS);
-    issue(pc, a.prev + (long long)s * g.field, sq + slot * S::QS);
-    if (grad) issue(pc, a.lap + (long long)s * g.field, sl + slot * S::QS);
-  };
+  issue(pc, a.C, scc);
 #pragma unroll
-  for (int i = 0; i < NS - 1; ++i) {  // one commit group per unit, empty groups included, so that
-    if (u_lo + i < u_hi) issue_unit(u_lo + i);  // wait_group<NS-1> means "unit v has landed"
+  for (int i = 0; i < NS - 1; ++i) {  // one commit group per shot, empty groups included, so that
+    if (sb + i < se) {                // wait_group<NS-1> in the loop means "shot s has landed"
+      issue(ph, a.cur + (long long)(sb + i) * g.field, sp + i * S::PS);
+      issue(pc, a.prev + (long long)(sb + i) * g.field, sq + i * S::QS);
+      if (grad) issue(pc, a.lap + (long long)(sb + i) * g.field, sl + i * S::QS);
+    }
     cp_async_commit();
   }
-  if (ADJ) {
+  int e0 = 0, e1 = 0, c0 = 0, c1 = 0;
+  if (!ADJ && a.traces) { e0 = a.tt.rec_ptr[tile]; e1 = a.tt.rec_ptr[tile + 1]; }
+  if (ADJ && a.gtr) { c0 = a.tt.cell_ptr[tile]; c1 = a.tt.cell_ptr[tile + 1]; }
+  const bool inject = ADJ && c1 > c0;  // uniform
+  if (inject) {
     for (int i = threadIdx.x; i < S::QS; i += 256) sj[i] = T(0);
     __syncthreads();  // zeroing completes before any thread writes a cotangent value
   }
 
+  const bool layer_tile = AB && (x0 < g.lo0 || x0 + S::TX > g.hi0 || z0 < g.lo1 || z0 + S::TZ > g.hi1);
+  const bool use_a = layer_tile && (!ADJ || a.apply_a);
+  const bool use_b = layer_tile && (ADJ || !a.b_one);
   const T wc = g.wc, w1x = g.w1a, w1z = g.w1b, w2x = g.w2a, w2z = g.w2b;
   const int ld = (int)g.s0;
-  // compute side: the tile of the current unit
-  int ctile = -1, x0 = 0, z0 = 0, zc = 0, xr = 0, e0 = 0, e1 = 0, c0 = 0, c1 = 0;
-  bool own_cols = false, layer_tile = false;
-  long long cbase = 0;
-  T gsum[RX][VZ];
+  const long long cbase = g.origin + (long long)xr * ld + zc;  // owned cells of row k: + k*ld
+  T gsum[RX][VZ];  // adjoint: per-cell sum over this CTA's shots
 #pragma unroll
   for (int k = 0; k < RX; ++k)
 #pragma unroll
     for (int v = 0; v < VZ; ++v) gsum[k][v] = T(0);
-  auto flush = [&]() {  // adjoint: add this CTA's sum over the tile's shots into its slot
-    if (!grad || !own_cols) return;
-    const int slot = (int)blockIdx.x - first_cta_of_unit((long long)ctile * nsh, U, gridDim.x);
-    T* gp = a.gacc + (long long)slot * g.field + cbase;
-#pragma unroll
-    for (int k = 0; k < RX; ++k) {
-      if (xr + k < g.n0) {
-#pragma unroll
-        for (int v = 0; v < VZ; ++v)
-          if (zc + v < g.n1) gp[k * ld + v] += gsum[k][v];
-      }
-#pragma unroll
-      for (int v = 0; v < VZ; ++v) gsum[k][v] = T(0);
-    }
-  };
 
-  for (int u = u_lo; u < u_hi; ++u) {
+  for (int s = sb; s < se; ++s) {
+    const int buf = (s - sb) % NS;
     {
-      const int un = u + NS - 1;
-      if (un < u_hi) issue_unit(un);
+      const int sn = s + NS - 1, nb = (sn - sb) % NS;  // nb: the buffer shot s-1 used
+      if (sn < se) {
+        issue(ph, a.cur + (long long)sn * g.field, sp + nb * S::PS);
+        issue(pc, a.prev + (long long)sn * g.field, sq + nb * S::QS);
+        if (grad) issue(pc, a.lap + (long long)sn * g.field, sl + nb * S::QS);
+      }
       cp_async_commit();
       cp_async_wait<NS - 1>();
     }
-    const int tile = u / nsh, s = u - tile * nsh;
-    if (tile != ctile) {
-      if (ctile >= 0) flush();
-      ctile = tile;
-      x0 = (tile / a.tt.tiles_z) * S::TX;
-      z0 = (tile % a.tt.tiles_z) * S::TZ;
-      zc = z0 + lane * VZ;  // first owned column
-      xr = x0 + warp * RX;  // first owned row
-      own_cols = zc < g.n1;
-      layer_tile = AB && (x0 < g.lo0 || x0 + S::TX > g.hi0 || z0 < g.lo1 || z0 + S::TZ > g.hi1);
-      cbase = g.origin + (long long)xr * ld + zc;  // owned cells of row k: + k*ld
-      if (!ADJ && a.traces) { e0 = a.tt.rec_ptr[tile]; e1 = a.tt.rec_ptr[tile + 1]; }
-      if (ADJ && a.gtr) {
-        c0 = a.tt.cell_ptr[tile];
-        c1 = a.tt.cell_ptr[tile + 1];
-        __syncthreads();  // the previous tile's cells are cleared before this tile's are set
-      }
-    }
-    const bool use_a = layer_tile && (!ADJ || a.apply_a);
-    const bool use_b = layer_tile && (ADJ || !a.b_one);
-    const bool inject = ADJ && c1 > c0;  // uniform
     if (inject) {  // cotangent of shot s at each touched cell, summed in table order
       const T* gs = a.gtr + (long long)s * a.n_rec * a.n_t + a.j;
       for (int e = c0 + threadIdx.x; e < c1; e += 256) {
@@ -356,11 +311,9 @@ __global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T>
       }
     }
     __syncthreads();
-    const int slot = (u - u_lo) % NS;
-    const T* P = sp + slot * S::PS;
-    const T* Q = sq + slot * S::QS;
-    const T* LP = sl + slot * S::QS;
-    const T* CC = scc + ((tile - t_lo) % NS) * S::QS;
+    const T* P = sp + buf * S::PS;
+    const T* Q = sq + buf * S::QS;
+    const T* LP = sl + buf * S::QS;
 
     for (int e = e0 + threadIdx.x; e < e1; e += 256) {  // forward: receiver samples of p^n
       const int r = a.tt.rec_list[e];
@@ -406,7 +359,7 @@ __global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T>
       const int toff = (lrow + k) * S::TZ + lane * VZ;  // the owned cells in a core tile
       T pp[VZ], cc[VZ];
       vload<T, VZ>(Q + toff, pp);
-      vload<T, VZ>(CC + toff, cc);
+      vload<T, VZ>(scc + toff, cc);
       const int x = xr + k;
       const bool ok = own_cols && x < g.n0;
       T ca[VZ], cb[VZ], inj[VZ];
@@ -450,10 +403,19 @@ __global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T>
         for (int v = 0; v < VZ; ++v) wv[q][v] = wv[q + 1][v];
     }
     __syncthreads();
-    if (inject)  // the same threads clear the cells they set, before the next unit sets them again
+    if (inject)  // the same threads clear the cells they set, before the next shot sets them again
       for (int e = c0 + threadIdx.x; e < c1; e += 256) sj[a.tt.cell_local[e]] = T(0);
   }
-  if (ctile >= 0) flush();
+  if (grad && own_cols) {
+    T* gp = a.gacc + (long long)blockIdx.z * g.field + cbase;
+#pragma unroll
+    for (int k = 0; k < RX; ++k) {
+      if (xr + k >= g.n0) continue;
+#pragma unroll
+      for (int v = 0; v < VZ; ++v)
+        if (zc + v < g.n1) gp[k * ld + v] += gsum[k][v];
+    }
+  }
 }
 
 }  // namespace nw

@@ -200,17 +200,14 @@ int snap_load(const nw_grid* g, const nw_storage* st, int n_shots, int j, T* lm1
 }
 
 // ---- launch shapes ------------------------------------------------------------------------
-constexpr int kSMs = 148;  // B200: grids of the 2-D steps are a multiple of its SM count
-
-struct TileCfg {  // one 2-D step kernel's tile: 8*rx rows by 32*vz columns, cps CTAs per SM
-  int vz, rx, cps;
+struct TileCfg {  // one 2-D step kernel's tile: 8*rx rows by 32*vz columns, spc shots per CTA
+  int vz, rx, spc;
   int tx() const { return 8 * rx; }
   int tz() const { return 32 * vz; }
   int tiles_z(const nw_grid* g) const { return (g->n[1] + tz() - 1) / tz(); }
-  int n_tiles(const nw_grid* g) const { return tiles_z(g) * ((g->n[0] + tx() - 1) / tx()); }
-  // CTAs of one launch over n_shots shots: at most one per (tile, shot) unit
-  int ctas(const nw_grid* g, int n_shots) const {
-    return (int)std::min<long long>((long long)n_tiles(g) * n_shots, (long long)cps * kSMs);
+  int groups(int n_shots) const { return (n_shots + spc - 1) / spc; }
+  dim3 grid(const nw_grid* g, int n_shots) const {
+    return dim3(tiles_z(g), (g->n[0] + tx() - 1) / tx(), groups(n_shots));
   }
 };
 struct Tune {
@@ -222,7 +219,7 @@ int check_tile(const nw_grid* g, const TileCfg& c, const char* which) {
   if (g->dtype == NW_F32 && c.vz != 2 && c.vz != 4) return fail(NW_ERR_ARG, "tuning." + w + "vz must be 2 or 4 for float32");
   if (g->dtype == NW_F64 && c.vz != 2) return fail(NW_ERR_ARG, "tuning." + w + "vz must be 2 for float64");
   if (c.rx != 2 && c.rx != 4 && c.rx != 8) return fail(NW_ERR_ARG, "tuning." + w + "rx must be 2, 4 or 8");
-  if (c.cps < 1 || c.cps > 32) return fail(NW_ERR_ARG, "tuning." + w + "ctas_per_sm must be in [1, 32]");
+  if (c.spc < 1) return fail(NW_ERR_ARG, "tuning." + w + "shots_per_cta must be >= 1");
   return NW_OK;
 }
 
@@ -231,30 +228,22 @@ int resolve_tune(const nw_grid* g, const nw_tuning* t, Tune* out) {
   // defaults: the best forward and adjoint times of a sweep on a 552^2 x 16-shot grid
   r.fwd.vz = (t && t->vz) ? t->vz : 2;
   r.fwd.rx = (t && t->rx) ? t->rx : 4;
-  r.fwd.cps = (t && t->ctas_per_sm) ? t->ctas_per_sm : 3;
+  r.fwd.spc = (t && t->shots_per_cta) ? t->shots_per_cta : 2;
   r.adj.vz = (t && t->adj_vz) ? t->adj_vz : 2;
   r.adj.rx = (t && t->adj_rx) ? t->adj_rx : 2;
-  r.adj.cps = (t && t->adj_ctas_per_sm) ? t->adj_ctas_per_sm : 2;
+  r.adj.spc = (t && t->adj_shots_per_cta) ? t->adj_shots_per_cta : 4;
   int rc = check_tile(g, r.fwd, "");
   if (rc) return rc;
   rc = check_tile(g, r.adj, "adj_");
   if (rc) return rc;
+  if (g->ndim == 3) r.fwd.spc = r.adj.spc = 1;
   *out = r;
   return NW_OK;
 }
 
-// Accumulator fields the adjoint fills: one per shot in 3-D; in 2-D, for the CTA ranges of
-// step2d, the largest number of CTAs that hold units of one tile.
+// Accumulator fields the adjoint fills: one per shot in 3-D, one per adjoint shot group in 2-D.
 int n_acc_fields(const nw_grid* g, const Tune& t, int n_shots) {
-  if (g->ndim == 3) return n_shots;
-  const long long T = t.adj.n_tiles(g), U = T * n_shots, G = t.adj.ctas(g, n_shots);
-  int m = 1;
-  for (long long tile = 0; tile < T; ++tile) {
-    const int c0 = nw::first_cta_of_unit(tile * n_shots, U, G);
-    const int c1 = nw::first_cta_of_unit(tile * n_shots + n_shots - 1, U, G);
-    m = std::max(m, c1 - c0 + 1);
-  }
-  return m;
+  return g->ndim == 3 ? n_shots : t.adj.groups(n_shots);
 }
 
 // Dynamic shared memory of step2d: C, the copy ring (halo tile + core tile, and the Lap p core
@@ -262,7 +251,7 @@ int n_acc_fields(const nw_grid* g, const Tune& t, int n_shots) {
 template <typename T, int R, int VZ, int RX, bool ADJ>
 constexpr size_t step2_smem() {
   using S = nw::Tile2Shape<T, VZ, RX, R>;
-  return (ADJ ? S::NS * (S::PS + 3 * S::QS) + S::QS : S::NS * (S::PS + 2 * S::QS)) * sizeof(T);
+  return (ADJ ? 2 * S::QS + S::NS * (S::PS + 2 * S::QS) : S::QS + S::NS * (S::PS + S::QS)) * sizeof(T);
 }
 constexpr size_t kMaxSmem = 227 * 1024;  // opt-in shared memory per CTA on sm_100a
 
@@ -297,7 +286,6 @@ int launch_pdl(K kernel, dim3 grid, size_t smem, cudaStream_t s, Args... args) {
 nw::TileTables tile_tables(const nw_grid* g, const nw_acquisition* a, const TileCfg& c) {
   nw::TileTables tt;
   tt.tiles_z = c.tiles_z(g);
-  tt.n_tiles = c.n_tiles(g);
   tt.rec_ptr = a->tile_rec_ptr;
   tt.rec_list = a->tile_rec_list;
   tt.rec_corner = a->rec_corner;
@@ -310,21 +298,21 @@ nw::TileTables tile_tables(const nw_grid* g, const nw_acquisition* a, const Tile
 }
 
 template <typename T, int R, int VZ, int RX, bool AB, bool ADJ>
-int launch_step2(const nw::KGrid<T>& kg, const nw::Tiled2<T>& st, int n_ctas, cudaStream_t s) {
+int launch_step2(const nw::KGrid<T>& kg, const nw::Tiled2<T>& st, dim3 grid, cudaStream_t s) {
   constexpr size_t smem = step2_smem<T, R, VZ, RX, ADJ>();
   if (smem > kMaxSmem) return fail(NW_ERR_ARG, "tile too large for shared memory (lower tuning rx or vz)");
   static bool done = false;
   int rc = allow_smem(nw::step2d<T, R, VZ, RX, AB, ADJ>, smem, &done);
   if (rc) return rc;
-  return launch_pdl(nw::step2d<T, R, VZ, RX, AB, ADJ>, dim3(n_ctas, 1, 1), smem, s, kg, st);
+  return launch_pdl(nw::step2d<T, R, VZ, RX, AB, ADJ>, grid, smem, s, kg, st);
 }
 template <typename T, int R, int VZ, int RX, bool AB>
-int launch_fwd2_v(const nw::KGrid<T>& kg, const nw::Tiled2<T>& st, int n_ctas, cudaStream_t s) {
-  return launch_step2<T, R, VZ, RX, AB, false>(kg, st, n_ctas, s);
+int launch_fwd2_v(const nw::KGrid<T>& kg, const nw::Tiled2<T>& st, dim3 grid, cudaStream_t s) {
+  return launch_step2<T, R, VZ, RX, AB, false>(kg, st, grid, s);
 }
 template <typename T, int R, int VZ, int RX, bool AB>
-int launch_adj2_v(const nw::KGrid<T>& kg, const nw::Tiled2<T>& st, int n_ctas, cudaStream_t s) {
-  return launch_step2<T, R, VZ, RX, AB, true>(kg, st, n_ctas, s);
+int launch_adj2_v(const nw::KGrid<T>& kg, const nw::Tiled2<T>& st, dim3 grid, cudaStream_t s) {
+  return launch_step2<T, R, VZ, RX, AB, true>(kg, st, grid, s);
 }
 
 // 3-D step: forward (ADJ = false) or adjoint.
@@ -400,13 +388,14 @@ int forward_step(const nw_grid* g, const nw::KGrid<T>& kg, const nw_medium* m, c
     st.wavelet = (const T*)a->wavelet;
     st.n = n;
     st.n_shots = a->n_shots;
+    st.shots_per_cta = tu.fwd.spc;
     st.traces = rec ? traces : nullptr;
     st.rec_w = (const T*)a->rec_weight;
     st.n_rec = a->n_rec;
     st.n_t = t->n_t;
     st.j = n / t->substeps;
     st.tt = tile_tables(g, a, tu.fwd);
-    return NW_DISPATCH2(launch_fwd2_v, T, tu.fwd, kg, st, tu.fwd.ctas(g, a->n_shots), s);
+    return NW_DISPATCH2(launch_fwd2_v, T, tu.fwd, kg, st, tu.fwd.grid(g, a->n_shots), s);
   }
   nw::Step3<T> st = {};
   st.prev = L.at(n - 1);
@@ -507,13 +496,14 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
     as.lap = lap;
     as.gacc = gacc;
     as.n_shots = S;
+    as.shots_per_cta = tu.adj.spc;
     as.gtr = (a->n_cells > 0 && n % M == 0) ? gtr : nullptr;
     as.gcell_w = (const T*)a->cell_weight;
     as.n_rec = a->n_rec;
     as.n_t = t->n_t;
     as.j = n / M;
     as.tt = tile_tables(g, a, tu.adj);
-    return NW_DISPATCH2(launch_adj2_v, T, tu.adj, kg, as, tu.adj.ctas(g, S), s);
+    return NW_DISPATCH2(launch_adj2_v, T, tu.adj, kg, as, tu.adj.grid(g, S), s);
   };
   if (N >= n_stop) {  // level N: q^N = A C R^T g_N (q^{N+1} = q^{N+2} = 0)
     int rc = g->ndim == 2 ? step2(N, nullptr) : inject3(N);
@@ -709,10 +699,10 @@ int nw_tile_shape(const nw_grid* g, nw_tuning* t, int32_t* shape) {
   if (t) {
     t->vz = tu.fwd.vz;
     t->rx = tu.fwd.rx;
-    t->ctas_per_sm = tu.fwd.cps;
+    t->shots_per_cta = tu.fwd.spc;
     t->adj_vz = tu.adj.vz;
     t->adj_rx = tu.adj.rx;
-    t->adj_ctas_per_sm = tu.adj.cps;
+    t->adj_shots_per_cta = tu.adj.spc;
   }
   if (shape) {
     shape[0] = tu.fwd.tx();

@@ -130,10 +130,10 @@ class DevicePlan:
         self._cells = cells
         self.set_tuning(*(getattr(op, "tuning", None) or ()))
 
-    def set_tuning(self, vz: int = 0, rx: int = 0, ctas_per_sm: int = 0, adj_vz: int = 0, adj_rx: int = 0,
-                   adj_ctas_per_sm: int = 0) -> None:
+    def set_tuning(self, vz: int = 0, rx: int = 0, shots_per_cta: int = 0, adj_vz: int = 0, adj_rx: int = 0,
+                   adj_shots_per_cta: int = 0) -> None:
         """Choose the 2-D launch shapes (0 = library default) and build the per-tile tables."""
-        t = _lib.Tuning(int(vz), int(rx), int(ctas_per_sm), int(adj_vz), int(adj_rx), int(adj_ctas_per_sm))
+        t = _lib.Tuning(int(vz), int(rx), int(shots_per_cta), int(adj_vz), int(adj_rx), int(adj_shots_per_cta))
         shape = (C.c_int32 * 4)()
         _lib.check(_lib.load().nw_tile_shape(C.byref(self.g), C.byref(t), shape))
         self.tuning = t
@@ -189,9 +189,9 @@ class DevicePlan:
         return n
 
     def shots_per_acc(self, n_shots: int) -> int:
-        """Shots whose initial-state gradient term goes to one accumulator field: all of them into
-        field 0 in 2-D, one field per shot in 3-D (the adjoint's own layout there)."""
-        return n_shots if self.g.ndim == 2 else 1
+        """Shots whose initial-state gradient term goes to one accumulator field (the adjoint's
+        own grouping: adj_shots_per_cta in 2-D, one shot per field in 3-D)."""
+        return int(self.tuning.adj_shots_per_cta) if self.g.ndim == 2 else 1
 
     # -- descriptors ------------------------------------------------------------------------
     def medium(self, c2dt2: torch.Tensor) -> _lib.Medium:

@@ -256,8 +256,8 @@ def test_oracle_agrees_with_device_float32_on_cfg1(cuda_device):
 
 
 def _layered_op(n=200, shots=6, n_t=81, **kw):
-    """A 200^2 (240^2 padded) sponge problem with several shots: big enough that the 2-D step
-    kernels' CTAs take ranges of several (tile, shot) units that cross tile boundaries."""
+    """A 200^2 (240^2 padded) sponge problem with several shots, so that shot groups, partial
+    groups and many tiles (absorbing-layer and interior ones) all occur."""
     h = 10.0
     dom = Domain((n, n), ((0.0, n * h), (0.0, n * h)))
     src = [[(k + 0.5) * n * h / shots, 1.5 * h] for k in range(shots)]
@@ -279,14 +279,14 @@ def _layered_grad(op, dtype, dev, tuning):
     return tr.detach().cpu().numpy(), gc.double().cpu().numpy()
 
 
-# (vz, rx, ctas_per_sm, adj_vz, adj_rx, adj_ctas_per_sm); ctas_per_sm = 1 gives each CTA several units
+# (vz, rx, shots_per_cta, adj_vz, adj_rx, adj_shots_per_cta)
 LAUNCH_SHAPES = [(2, 2, 1, 2, 2, 1), (2, 8, 2, 2, 4, 3), (4, 4, 3, 4, 2, 1), (4, 2, 8, 2, 8, 8)]
 
 
 @pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
 def test_results_do_not_depend_on_the_launch_shape(dtype, cuda_device):
-    """Traces are bitwise the same for every tile shape and CTA count (each cell is computed by the
-    same arithmetic); the gradient only regroups its float sums (float64: 1e-12, float32: 1e-5)."""
+    """Traces are bitwise the same for every tile shape and shot grouping (each cell is computed by
+    the same arithmetic); the gradient only regroups its float sums (float64: 1e-12, float32: 1e-5)."""
     op = _layered_op()
     tr0, g0 = _layered_grad(op, dtype, cuda_device, (0, 0, 0, 0, 0, 0))
     assert np.isfinite(g0).all() and np.abs(g0).max() > 0

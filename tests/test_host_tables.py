@@ -130,35 +130,15 @@ def test_tile_tables_partition_receivers_and_cells(name, tuning):
             assert local[e] == (x - x0) * AZ + (z - z0)
 
 
-def _unit_ranges(n_tiles, n_shots, ctas_per_sm):
-    """CTA b of a 2-D step takes units [b*U/G, (b+1)*U/G), U = tiles x shots, G = min(U, 148 cps)."""
-    U = n_tiles * n_shots
-    G = min(U, ctas_per_sm * 148)
-    return U, G, [(b * U // G, (b + 1) * U // G) for b in range(G)]
-
-
 @pytest.mark.parametrize("n_shots", [1, 3, 16, 64])
-@pytest.mark.parametrize("tuning", [(0, 0, 0), (2, 4, 3, 2, 2, 2), (4, 2, 1, 4, 8, 1)])
-def test_adjoint_accumulator_slots_cover_every_cta_of_a_tile(n_shots, tuning):
-    """The library's accumulator count is exactly the largest number of adjoint CTAs that hold
-    units of one tile, and the slot each CTA writes for a tile (its index among those CTAs) is
-    below that count: every (tile, slot) pair has one writer."""
+@pytest.mark.parametrize("tuning", [(0, 0, 0), (2, 4, 3, 2, 2, 2), (4, 2, 1, 4, 8, 5)])
+def test_adjoint_accumulators_are_one_per_shot_group(n_shots, tuning):
     case = load_golden("fwi_o4_sponge")
     plan = make_op(case)._plan(CPU, torch.float32)
     plan.set_tuning(*tuning)
-    AX, AZ = plan.adj_tile
-    n_tiles = -(-plan.g.n[0] // AX) * -(-plan.g.n[1] // AZ)
-    U, G, ranges = _unit_ranges(n_tiles, n_shots, plan.tuning.adj_ctas_per_sm)
-    assert ranges[0][0] == 0 and ranges[-1][1] == U
-    assert all(lo < hi for lo, hi in ranges) and all(ranges[b][1] == ranges[b + 1][0] for b in range(G - 1))
-    writers = {}
-    for b, (lo, hi) in enumerate(ranges):
-        for t in range(lo // n_shots, (hi - 1) // n_shots + 1):
-            writers.setdefault(t, []).append(b)
-    n_acc = plan.n_acc(n_shots)
-    assert n_acc == max(len(v) for v in writers.values())
-    for t, bs in writers.items():
-        assert bs == list(range(bs[0], bs[0] + len(bs)))  # consecutive CTAs: slot = b - first
+    spc = plan.tuning.adj_shots_per_cta
+    assert plan.n_acc(n_shots) == -(-n_shots // spc)
+    assert plan.shots_per_acc(n_shots) == spc
 
 
 def test_reference_errors_are_raised_on_the_host():
