@@ -2,10 +2,13 @@
 //
 // One CTA (8 warps) owns a tile of TX = 8*RX rows by TZ = 32*VZ columns and loops over a group
 // of shots; the hardware scheduler balances the (tile, shot group) CTAs over the SMs, which
-// absorbs the extra cost of tiles in the absorbing layer. For every shot the input tiles (p^n or mu^{n+1} with an R-row and 16-byte-column halo,
-// and core tiles: p^{n-1}, or mu^{n+2} and the stored Lap p^n) are staged in shared memory by
-// cp.async through a ring of NS buffers, so that the copies of the next NS-1 shots are in flight
-// while shot s is computed. Each thread computes the shared/global offsets of the 16-byte chunks it
+// absorbs the extra cost of tiles in the absorbing layer. Only the field whose neighbours the
+// stencil reads (p^n, or q^{n+1} in the adjoint) goes through shared memory: its tile with an
+// R-row and 16-byte-column halo is staged by cp.async through a ring of NS buffers, so that the
+// copies of the next NS-1 shots are in flight while shot s is computed. Every other field is read
+// at the thread's own cells only (p^{n-1} or q^{n+2}, the stored Lap p^n, c^2 dt^2, A, B), so a
+// thread loads those straight into registers: C, A and B once per CTA, the per-shot fields one
+// shot ahead of their use. Each thread computes the shared/global offsets of the 16-byte chunks it
 // copies once per CTA; per shot it only adds the shot's base address. A thread owns VZ adjacent
 // columns and RX rows: it slides a (2R+1)-row register window down its columns, reading each row
 // once as a VZ-wide vector plus two halo vectors, so every shared-memory access is a
@@ -146,9 +149,8 @@ struct Tile2Shape {
   static constexpr int EPC = 16 / (int)sizeof(T); // elements per 16-byte chunk
   static constexpr int HR = TX + 2 * R;           // rows of a halo tile
   static constexpr int PS = HR * SW;              // elements of a halo tile
-  static constexpr int QS = TX * TZ;              // elements of a core tile
+  static constexpr int QS = TX * TZ;              // cells of a tile
   static constexpr int NCH = (HR * (SW / EPC) + 255) / 256;  // halo chunks per thread
-  static constexpr int NCC = (TX * (TZ / EPC) + 255) / 256;  // core chunks per thread
   static constexpr int NS = sizeof(T) == 8 ? 2 : 3;          // shot buffers in the copy ring
 };
 
@@ -175,23 +177,6 @@ __device__ __forceinline__ CopyPlan<Tile2Shape<T, VZ, RX, R>::NCH> plan_halo(con
     const int z = z0 - S::HL + ch * S::EPC;
     p.soff[i] = row * S::SW + ch * S::EPC;
     p.goff[i] = (c < S::HR * CPR && x < g.n0 + R && z < (int)g.s0) ? (int)(g.origin + (long long)x * g.s0 + z) : -1;
-  }
-  return p;
-}
-// Core tile: rows [x0, x0 + TX) x columns [z0, z0 + TZ), row pitch TZ.
-template <typename T, int VZ, int RX, int R>
-__device__ __forceinline__ CopyPlan<Tile2Shape<T, VZ, RX, R>::NCC> plan_core(const KGrid<T>& g, int x0, int z0) {
-  using S = Tile2Shape<T, VZ, RX, R>;
-  constexpr int CPR = S::TZ / S::EPC;
-  CopyPlan<S::NCC> p;
-#pragma unroll
-  for (int i = 0; i < S::NCC; ++i) {
-    const int c = threadIdx.x + 256 * i;
-    const int row = c / CPR, ch = c - row * CPR;
-    const int x = x0 + row;
-    const int z = z0 + ch * S::EPC;
-    p.soff[i] = row * S::TZ + ch * S::EPC;
-    p.goff[i] = (c < S::TX * CPR && x < g.n0 && z < (int)g.s0) ? (int)(g.origin + (long long)x * g.s0 + z) : -1;
   }
   return p;
 }
@@ -236,11 +221,8 @@ __global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T>
   using S = Tile2Shape<T, VZ, RX, R>;
   constexpr int NS = S::NS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* scc = reinterpret_cast<T*>(smem_raw);  // [QS] C
-  T* sp = scc + S::QS;                      // [NS][PS] p^n | q^{n+1}, with halo
-  T* sq = sp + NS * S::PS;                  // [NS][QS] p^{n-1} | q^{n+2}
-  T* sl = sq + NS * S::QS;                  // adjoint: [NS][QS] Lap p^n
-  T* sj = sl + NS * S::QS;                  // adjoint: [QS] cotangent injected at this shot's cells
+  T* sp = reinterpret_cast<T*>(smem_raw);  // [NS][PS] p^n | q^{n+1}, with halo
+  T* sj = sp + NS * S::PS;                  // adjoint: [QS] cotangent injected at this shot's cells
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int z0 = blockIdx.x * S::TZ, x0 = blockIdx.y * S::TX;
@@ -252,20 +234,37 @@ __global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T>
   const int lrow = warp * RX;     // first owned row inside the tile
   const bool own_cols = zc < g.n1;
   const bool grad = ADJ && a.lap != nullptr;
+  const int ld = (int)g.s0;
+  const long long cbase = g.origin + (long long)xr * ld + zc;  // owned cells of row k: + k*ld
+  bool ok[RX];  // row k of the owned cells lies in the grid
+#pragma unroll
+  for (int k = 0; k < RX; ++k) ok[k] = own_cols && xr + k < g.n0;
 
   const CopyPlan<S::NCH> ph = plan_halo<T, VZ, RX, R>(g, x0, z0);
-  const CopyPlan<S::NCC> pc = plan_core<T, VZ, RX, R>(g, x0, z0);
   wait_previous_grid();
   allow_next_grid();
-  issue(pc, a.C, scc);
 #pragma unroll
   for (int i = 0; i < NS - 1; ++i) {  // one commit group per shot, empty groups included, so that
-    if (sb + i < se) {                // wait_group<NS-1> in the loop means "shot s has landed"
-      issue(ph, a.cur + (long long)(sb + i) * g.field, sp + i * S::PS);
-      issue(pc, a.prev + (long long)(sb + i) * g.field, sq + i * S::QS);
-      if (grad) issue(pc, a.lap + (long long)(sb + i) * g.field, sl + i * S::QS);
+    if (sb + i < se) issue(ph, a.cur + (long long)(sb + i) * g.field, sp + i * S::PS);
+    cp_async_commit();                // wait_group<NS-1> in the loop means "shot s has landed"
+  }
+  const bool layer_tile = AB && (x0 < g.lo0 || x0 + S::TX > g.hi0 || z0 < g.lo1 || z0 + S::TZ > g.hi1);
+  const bool use_a = layer_tile && (!ADJ || a.apply_a);
+  const bool use_b = layer_tile && (ADJ || !a.b_one);
+  // per-CTA coefficients of the owned cells and the first shot's per-cell fields, in registers
+  T cr[RX][VZ], ar[RX][VZ], br[RX][VZ], pv[RX][VZ], lv[RX][VZ];
+#pragma unroll
+  for (int k = 0; k < RX; ++k) {
+#pragma unroll
+    for (int v = 0; v < VZ; ++v) { cr[k][v] = T(0); ar[k][v] = T(1); br[k][v] = T(1); pv[k][v] = T(0); lv[k][v] = T(0); }
+    if (ok[k]) {
+      const long long o = cbase + (long long)k * ld;
+      vldg<T, VZ>(a.C + o, cr[k]);
+      if (use_a) vldg<T, VZ>(a.A + o, ar[k]);
+      if (use_b) vldg<T, VZ>(a.B + o, br[k]);
+      vldg<T, VZ>(a.prev + (long long)sb * g.field + o, pv[k]);
+      if (grad) vldg<T, VZ>(a.lap + (long long)sb * g.field + o, lv[k]);
     }
-    cp_async_commit();
   }
   int e0 = 0, e1 = 0, c0 = 0, c1 = 0;
   if (!ADJ && a.traces) { e0 = a.tt.rec_ptr[tile]; e1 = a.tt.rec_ptr[tile + 1]; }
@@ -276,12 +275,7 @@ __global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T>
     __syncthreads();  // zeroing completes before any thread writes a cotangent value
   }
 
-  const bool layer_tile = AB && (x0 < g.lo0 || x0 + S::TX > g.hi0 || z0 < g.lo1 || z0 + S::TZ > g.hi1);
-  const bool use_a = layer_tile && (!ADJ || a.apply_a);
-  const bool use_b = layer_tile && (ADJ || !a.b_one);
   const T wc = g.wc, w1x = g.w1a, w1z = g.w1b, w2x = g.w2a, w2z = g.w2b;
-  const int ld = (int)g.s0;
-  const long long cbase = g.origin + (long long)xr * ld + zc;  // owned cells of row k: + k*ld
   T gsum[RX][VZ];  // adjoint: per-cell sum over this CTA's shots
 #pragma unroll
   for (int k = 0; k < RX; ++k)
@@ -292,11 +286,7 @@ __global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T>
     const int buf = (s - sb) % NS;
     {
       const int sn = s + NS - 1, nb = (sn - sb) % NS;  // nb: the buffer shot s-1 used
-      if (sn < se) {
-        issue(ph, a.cur + (long long)sn * g.field, sp + nb * S::PS);
-        issue(pc, a.prev + (long long)sn * g.field, sq + nb * S::QS);
-        if (grad) issue(pc, a.lap + (long long)sn * g.field, sl + nb * S::QS);
-      }
+      if (sn < se) issue(ph, a.cur + (long long)sn * g.field, sp + nb * S::PS);
       cp_async_commit();
       cp_async_wait<NS - 1>();
     }
@@ -312,8 +302,6 @@ __global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T>
     }
     __syncthreads();
     const T* P = sp + buf * S::PS;
-    const T* Q = sq + buf * S::QS;
-    const T* LP = sl + buf * S::QS;
 
     for (int e = e0 + threadIdx.x; e < e1; e += 256) {  // forward: receiver samples of p^n
       const int r = a.tt.rec_list[e];
@@ -340,13 +328,13 @@ __global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T>
         sw2 = a.src_w[4 * s + 2] * wn; sw3 = a.src_w[4 * s + 3] * wn;
       }
     }
+    const bool more = s + 1 < se;
+    const long long so = (long long)s * g.field, sn = so + g.field;
 
     // sliding window: wv[q] holds tile row (lrow + k + q - R) (own columns only)
     T wv[2 * R + 1][VZ];
 #pragma unroll
     for (int q = 0; q < 2 * R; ++q) vload<T, VZ>(P + (lrow + q) * S::SW + S::HL + lane * VZ, wv[q]);
-    T* nx = a.next + (long long)s * g.field + cbase;
-    T* lx = (!ADJ && a.lap_out) ? a.lap_out + (long long)s * g.field + cbase : nullptr;
 #pragma unroll
     for (int k = 0; k < RX; ++k) {
       const int prow = lrow + k + R;  // shared row of the output row
@@ -356,18 +344,11 @@ __global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T>
 #pragma unroll
       for (int v = 0; v < VZ; ++v) rw.c[v] = wv[R][v];
       vload<T, VZ>(P + prow * S::SW + S::HL + lane * VZ + VZ, rw.r);
-      const int toff = (lrow + k) * S::TZ + lane * VZ;  // the owned cells in a core tile
-      T pp[VZ], cc[VZ];
-      vload<T, VZ>(Q + toff, pp);
-      vload<T, VZ>(scc + toff, cc);
       const int x = xr + k;
-      const bool ok = own_cols && x < g.n0;
-      T ca[VZ], cb[VZ], inj[VZ];
+      T inj[VZ];
 #pragma unroll
-      for (int v = 0; v < VZ; ++v) { ca[v] = T(1); cb[v] = T(1); inj[v] = T(0); }
-      if (use_a && ok) vldg<T, VZ>(a.A + cbase + k * ld, ca);
-      if (use_b && ok) vldg<T, VZ>(a.B + cbase + k * ld, cb);
-      if (inject) vload<T, VZ>(sj + toff, inj);
+      for (int v = 0; v < VZ; ++v) inj[v] = T(0);
+      if (inject) vload<T, VZ>(sj + (lrow + k) * S::TZ + lane * VZ, inj);
       T o[VZ], lp[VZ];
 #pragma unroll
       for (int v = 0; v < VZ; ++v) {
@@ -375,7 +356,7 @@ __global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T>
         T lap = wc * c + w1x * (wv[R - 1][v] + wv[R + 1][v]) + w1z * (zval(rw, v - 1) + zval(rw, v + 1));
         if (R == 2) lap += w2x * (wv[0][v] + wv[4][v]) + w2z * (zval(rw, v - 2) + zval(rw, v + 2));
         lp[v] = lap;
-        o[v] = (T(2) * c - cb[v] * pp[v]) + cc[v] * (inject ? lap + inj[v] : lap);
+        o[v] = (T(2) * c - br[k][v] * pv[k][v]) + cr[k][v] * (inject ? lap + inj[v] : lap);
       }
       if (src_tile) {
 #pragma unroll
@@ -387,15 +368,20 @@ __global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T>
       }
       if (use_a) {
 #pragma unroll
-        for (int v = 0; v < VZ; ++v) o[v] = ca[v] * o[v];
+        for (int v = 0; v < VZ; ++v) o[v] = ar[k][v] * o[v];
       }
-      if (ok) store_row<T, VZ>(nx + k * ld, o, zc, g.n1);
-      if (lx && ok) store_row<T, VZ>(lx + k * ld, lp, zc, g.n1);
       if (grad) {
-        T gl[VZ];
-        vload<T, VZ>(LP + toff, gl);
 #pragma unroll
-        for (int v = 0; v < VZ; ++v) gsum[k][v] += wv[R][v] * gl[v];
+        for (int v = 0; v < VZ; ++v) gsum[k][v] += wv[R][v] * lv[k][v];
+      }
+      if (ok[k]) {
+        const long long ro = cbase + (long long)k * ld;
+        store_row<T, VZ>(a.next + so + ro, o, zc, g.n1);
+        if (!ADJ && a.lap_out) store_row<T, VZ>(a.lap_out + so + ro, lp, zc, g.n1);
+        if (more) {  // the next shot's per-cell fields: in flight while the rest of this shot runs
+          vldg<T, VZ>(a.prev + sn + ro, pv[k]);
+          if (grad) vldg<T, VZ>(a.lap + sn + ro, lv[k]);
+        }
       }
 #pragma unroll
       for (int q = 0; q < 2 * R; ++q)
@@ -410,10 +396,10 @@ __global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T>
     T* gp = a.gacc + (long long)blockIdx.z * g.field + cbase;
 #pragma unroll
     for (int k = 0; k < RX; ++k) {
-      if (xr + k >= g.n0) continue;
+      if (!ok[k]) continue;
 #pragma unroll
       for (int v = 0; v < VZ; ++v)
-        if (zc + v < g.n1) gp[k * ld + v] += gsum[k][v];
+        if (zc + v < g.n1) gp[(long long)k * ld + v] += gsum[k][v];
     }
   }
 }

@@ -246,12 +246,12 @@ int n_acc_fields(const nw_grid* g, const Tune& t, int n_shots) {
   return g->ndim == 3 ? n_shots : t.adj.groups(n_shots);
 }
 
-// Dynamic shared memory of step2d: C, the copy ring (halo tile + core tile, and the Lap p core
-// tile in the adjoint) and, in the adjoint, the injected cotangents.
+// Dynamic shared memory of step2d: the ring of halo tiles and, in the adjoint, the injected
+// cotangents of one shot.
 template <typename T, int R, int VZ, int RX, bool ADJ>
 constexpr size_t step2_smem() {
   using S = nw::Tile2Shape<T, VZ, RX, R>;
-  return (ADJ ? 2 * S::QS + S::NS * (S::PS + 2 * S::QS) : S::QS + S::NS * (S::PS + S::QS)) * sizeof(T);
+  return (S::NS * S::PS + (ADJ ? S::QS : 0)) * sizeof(T);
 }
 constexpr size_t kMaxSmem = 227 * 1024;  // opt-in shared memory per CTA on sm_100a
 
