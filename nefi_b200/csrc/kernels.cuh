@@ -18,6 +18,16 @@
 
 namespace nw {
 
+// Arithmetic with a fixed rounding sequence: the compiler may not fuse or reorder these, so a
+// stencil written with them gives bitwise the same result in every kernel instantiation (tile
+// shape, vector width) that evaluates it.
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+
 // Kernel-side copy of the grid geometry, passed by value.
 template <typename T>
 struct KGrid {

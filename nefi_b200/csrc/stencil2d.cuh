@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T>
         const int gid = a.tt.cell_gid[e];
         T acc = T(0);
         for (int q = a.tt.gcell_ptr[gid]; q < a.tt.gcell_ptr[gid + 1]; ++q)
-          acc += a.gcell_w[q] * gs[(long long)a.tt.gcell_rec[q] * a.n_t];
+          acc = fma_rn(a.gcell_w[q], gs[(long long)a.tt.gcell_rec[q] * a.n_t], acc);
         sj[a.tt.cell_local[e]] = acc;
       }
     }
@@ -307,11 +307,10 @@ __global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T>
       const int r = a.tt.rec_list[e];
       const int row = a.tt.rec_corner[2 * r] - x0 + R, col = a.tt.rec_corner[2 * r + 1] - z0 + S::HL;
       const T* w = a.rec_w + 4 * r;
-      T acc = T(0);
-      acc += w[0] * P[row * S::SW + col];
-      acc += w[1] * P[row * S::SW + col + 1];
-      acc += w[2] * P[(row + 1) * S::SW + col];
-      acc += w[3] * P[(row + 1) * S::SW + col + 1];
+      T acc = mul_rn(w[0], P[row * S::SW + col]);
+      acc = fma_rn(w[1], P[row * S::SW + col + 1], acc);
+      acc = fma_rn(w[2], P[(row + 1) * S::SW + col], acc);
+      acc = fma_rn(w[3], P[(row + 1) * S::SW + col + 1], acc);
       a.traces[((long long)s * a.n_rec + r) * a.n_t + a.j] = acc;
     }
     // forward: the shot's source stencil, if it touches this tile (a CTA-uniform test)
@@ -324,8 +323,8 @@ __global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T>
       src_tile = bx + 1 >= x0 && bx < x0 + S::TX && bz + 1 >= z0 && bz < z0 + S::TZ;
       if (src_tile) {
         const T wn = a.wavelet[a.n];
-        sw0 = a.src_w[4 * s] * wn; sw1 = a.src_w[4 * s + 1] * wn;
-        sw2 = a.src_w[4 * s + 2] * wn; sw3 = a.src_w[4 * s + 3] * wn;
+        sw0 = mul_rn(a.src_w[4 * s], wn); sw1 = mul_rn(a.src_w[4 * s + 1], wn);
+        sw2 = mul_rn(a.src_w[4 * s + 2], wn); sw3 = mul_rn(a.src_w[4 * s + 3], wn);
       }
     }
     const bool more = s + 1 < se;
@@ -351,28 +350,31 @@ __global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T>
       if (inject) vload<T, VZ>(sj + (lrow + k) * S::TZ + lane * VZ, inj);
       T o[VZ], lp[VZ];
 #pragma unroll
-      for (int v = 0; v < VZ; ++v) {
+      for (int v = 0; v < VZ; ++v) {  // fixed rounding sequence (see fma_rn)
         const T c = wv[R][v];
-        T lap = wc * c + w1x * (wv[R - 1][v] + wv[R + 1][v]) + w1z * (zval(rw, v - 1) + zval(rw, v + 1));
-        if (R == 2) lap += w2x * (wv[0][v] + wv[4][v]) + w2z * (zval(rw, v - 2) + zval(rw, v + 2));
+        T lap = fma_rn(w1z, add_rn(zval(rw, v - 1), zval(rw, v + 1)),
+                       fma_rn(w1x, add_rn(wv[R - 1][v], wv[R + 1][v]), mul_rn(wc, c)));
+        if (R == 2)
+          lap = fma_rn(w2z, add_rn(zval(rw, v - 2), zval(rw, v + 2)),
+                       fma_rn(w2x, add_rn(wv[0][v], wv[4][v]), lap));
         lp[v] = lap;
-        o[v] = (T(2) * c - br[k][v] * pv[k][v]) + cr[k][v] * (inject ? lap + inj[v] : lap);
+        o[v] = fma_rn(cr[k][v], inject ? add_rn(lap, inj[v]) : lap, fma_rn(-br[k][v], pv[k][v], add_rn(c, c)));
       }
       if (src_tile) {
 #pragma unroll
         for (int v = 0; v < VZ; ++v) {
           const int dx = x - bx, dz = zc + v - bz;
           if (dx >= 0 && dx <= 1 && dz >= 0 && dz <= 1)
-            o[v] += (dx == 0) ? (dz == 0 ? sw0 : sw1) : (dz == 0 ? sw2 : sw3);
+            o[v] = add_rn(o[v], (dx == 0) ? (dz == 0 ? sw0 : sw1) : (dz == 0 ? sw2 : sw3));
         }
       }
       if (use_a) {
 #pragma unroll
-        for (int v = 0; v < VZ; ++v) o[v] = ar[k][v] * o[v];
+        for (int v = 0; v < VZ; ++v) o[v] = mul_rn(ar[k][v], o[v]);
       }
       if (grad) {
 #pragma unroll
-        for (int v = 0; v < VZ; ++v) gsum[k][v] += wv[R][v] * lv[k][v];
+        for (int v = 0; v < VZ; ++v) gsum[k][v] = fma_rn(wv[R][v], lv[k][v], gsum[k][v]);
       }
       if (ok[k]) {
         const long long ro = cbase + (long long)k * ld;
