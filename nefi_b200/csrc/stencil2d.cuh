@@ -7,8 +7,8 @@
 // R-row and 16-byte-column halo is staged by cp.async through a ring of NS buffers, so that the
 // copies of the next NS-1 shots are in flight while shot s is computed. Every other field is read
 // at the thread's own cells only (p^{n-1} or q^{n+2}, the stored Lap p^n, c^2 dt^2, A, B), so a
-// thread loads those straight into registers: C, A and B once per CTA, the per-shot fields one
-// shot ahead of their use. Each thread computes the shared/global offsets of the 16-byte chunks it
+// thread loads those straight into registers: C once per CTA, the per-shot fields one shot ahead
+// of their use, and A/B per row in absorbing-layer tiles only (L1 hits). Each thread computes the shared/global offsets of the 16-byte chunks it
 // copies once per CTA; per shot it only adds the shot's base address. A thread owns VZ adjacent
 // columns and RX rows: it slides a (2R+1)-row register window down its columns, reading each row
 // once as a VZ-wide vector plus two halo vectors, so every shared-memory access is a
@@ -217,7 +217,7 @@ __device__ __forceinline__ void store_row(T* dst, const T (&o)[VZ], int zc, int 
 // then adds the sum into the group's accumulator (one writer per cell and group).
 // ------------------------------------------------------------------------------------------
 template <typename T, int R, int VZ, int RX, bool AB, bool ADJ>
-__global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T> a) {
+__global__ void __launch_bounds__(256, 3) step2d(KGrid<T> g, Tiled2<T> a) {
   using S = Tile2Shape<T, VZ, RX, R>;
   constexpr int NS = S::NS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -251,17 +251,15 @@ __global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T>
   const bool layer_tile = AB && (x0 < g.lo0 || x0 + S::TX > g.hi0 || z0 < g.lo1 || z0 + S::TZ > g.hi1);
   const bool use_a = layer_tile && (!ADJ || a.apply_a);
   const bool use_b = layer_tile && (ADJ || !a.b_one);
-  // per-CTA coefficients of the owned cells and the first shot's per-cell fields, in registers
-  T cr[RX][VZ], ar[RX][VZ], br[RX][VZ], pv[RX][VZ], lv[RX][VZ];
+  // C of the owned cells and the first shot's per-cell fields, in registers
+  T cr[RX][VZ], pv[RX][VZ], lv[RX][VZ];
 #pragma unroll
   for (int k = 0; k < RX; ++k) {
 #pragma unroll
-    for (int v = 0; v < VZ; ++v) { cr[k][v] = T(0); ar[k][v] = T(1); br[k][v] = T(1); pv[k][v] = T(0); lv[k][v] = T(0); }
+    for (int v = 0; v < VZ; ++v) { cr[k][v] = T(0); pv[k][v] = T(0); lv[k][v] = T(0); }
     if (ok[k]) {
       const long long o = cbase + (long long)k * ld;
       vldg<T, VZ>(a.C + o, cr[k]);
-      if (use_a) vldg<T, VZ>(a.A + o, ar[k]);
-      if (use_b) vldg<T, VZ>(a.B + o, br[k]);
       vldg<T, VZ>(a.prev + (long long)sb * g.field + o, pv[k]);
       if (grad) vldg<T, VZ>(a.lap + (long long)sb * g.field + o, lv[k]);
     }
@@ -270,8 +268,27 @@ __global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T>
   if (!ADJ && a.traces) { e0 = a.tt.rec_ptr[tile]; e1 = a.tt.rec_ptr[tile + 1]; }
   if (ADJ && a.gtr) { c0 = a.tt.cell_ptr[tile]; c1 = a.tt.cell_ptr[tile + 1]; }
   const bool inject = ADJ && c1 > c0;  // uniform
+  // adjoint injection: thread t owns touched cell c0 + t of the tile; its table entries (receiver,
+  // weight) are shot-independent and cached here, so a shot only loads the cotangents themselves
+  constexpr int kEnt = 4;
+  int jl = -1, jn = 0, jrec[kEnt];
+  T jw[kEnt];
+  bool jslow = false;  // more entries than cached: read the table every shot
   if (inject) {
     for (int i = threadIdx.x; i < S::QS; i += 256) sj[i] = T(0);
+    const int e = c0 + threadIdx.x;
+    if (e < c1) {
+      jl = a.tt.cell_local[e];
+      const int gid = a.tt.cell_gid[e];
+      const int q0 = a.tt.gcell_ptr[gid];
+      jn = a.tt.gcell_ptr[gid + 1] - q0;
+      jslow = jn > kEnt;
+#pragma unroll
+      for (int m = 0; m < kEnt; ++m) {
+        jrec[m] = (m < jn) ? a.tt.gcell_rec[q0 + m] : 0;
+        jw[m] = (m < jn) ? a.gcell_w[q0 + m] : T(0);
+      }
+    }
     __syncthreads();  // zeroing completes before any thread writes a cotangent value
   }
 
@@ -292,7 +309,14 @@ __global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T>
     }
     if (inject) {  // cotangent of shot s at each touched cell, summed in table order
       const T* gs = a.gtr + (long long)s * a.n_rec * a.n_t + a.j;
-      for (int e = c0 + threadIdx.x; e < c1; e += 256) {
+      if (jl >= 0 && !jslow) {
+        T acc = T(0);
+#pragma unroll
+        for (int m = 0; m < kEnt; ++m)
+          if (m < jn) acc = fma_rn(jw[m], gs[(long long)jrec[m] * a.n_t], acc);
+        sj[jl] = acc;
+      }
+      for (int e = c0 + threadIdx.x + (jslow ? 0 : 256); e < c1; e += 256) {  // the uncached cells
         const int gid = a.tt.cell_gid[e];
         T acc = T(0);
         for (int q = a.tt.gcell_ptr[gid]; q < a.tt.gcell_ptr[gid + 1]; ++q)
@@ -344,6 +368,11 @@ __global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T>
       for (int v = 0; v < VZ; ++v) rw.c[v] = wv[R][v];
       vload<T, VZ>(P + prow * S::SW + S::HL + lane * VZ + VZ, rw.r);
       const int x = xr + k;
+      T ca[VZ], cb[VZ];
+#pragma unroll
+      for (int v = 0; v < VZ; ++v) { ca[v] = T(1); cb[v] = T(1); }
+      if (use_a && ok[k]) vldg<T, VZ>(a.A + cbase + (long long)k * ld, ca);
+      if (use_b && ok[k]) vldg<T, VZ>(a.B + cbase + (long long)k * ld, cb);
       T inj[VZ];
 #pragma unroll
       for (int v = 0; v < VZ; ++v) inj[v] = T(0);
@@ -358,7 +387,7 @@ __global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T>
           lap = fma_rn(w2z, add_rn(zval(rw, v - 2), zval(rw, v + 2)),
                        fma_rn(w2x, add_rn(wv[0][v], wv[4][v]), lap));
         lp[v] = lap;
-        o[v] = fma_rn(cr[k][v], inject ? add_rn(lap, inj[v]) : lap, fma_rn(-br[k][v], pv[k][v], add_rn(c, c)));
+        o[v] = fma_rn(cr[k][v], inject ? add_rn(lap, inj[v]) : lap, fma_rn(-cb[v], pv[k][v], add_rn(c, c)));
       }
       if (src_tile) {
 #pragma unroll
@@ -370,7 +399,7 @@ __global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T>
       }
       if (use_a) {
 #pragma unroll
-        for (int v = 0; v < VZ; ++v) o[v] = mul_rn(ar[k][v], o[v]);
+        for (int v = 0; v < VZ; ++v) o[v] = mul_rn(ca[v], o[v]);
       }
       if (grad) {
 #pragma unroll
@@ -391,8 +420,10 @@ __global__ void __launch_bounds__(256, ADJ ? 2 : 3) step2d(KGrid<T> g, Tiled2<T>
         for (int v = 0; v < VZ; ++v) wv[q][v] = wv[q + 1][v];
     }
     __syncthreads();
-    if (inject)  // the same threads clear the cells they set, before the next shot sets them again
-      for (int e = c0 + threadIdx.x; e < c1; e += 256) sj[a.tt.cell_local[e]] = T(0);
+    if (inject) {  // the same threads clear the cells they set, before the next shot sets them again
+      if (jl >= 0) sj[jl] = T(0);
+      for (int e = c0 + threadIdx.x + 256; e < c1; e += 256) sj[a.tt.cell_local[e]] = T(0);
+    }
   }
   if (grad && own_cols) {
     T* gp = a.gacc + (long long)blockIdx.z * g.field + cbase;
