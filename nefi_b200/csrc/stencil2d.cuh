@@ -2,18 +2,21 @@
 //
 // One CTA (8 warps) owns a tile of TX = 8*RX rows by TZ = 32*VZ columns and loops over a group
 // of shots; the hardware scheduler balances the (tile, shot group) CTAs over the SMs, which
-// absorbs the extra cost of tiles in the absorbing layer. Only the field whose neighbours the
-// stencil reads (p^n, or q^{n+1} in the adjoint) goes through shared memory: its tile with an
-// R-row and 16-byte-column halo is staged by cp.async through a ring of NS buffers, so that the
-// copies of the next NS-1 shots are in flight while shot s is computed. Every other field is read
-// at the thread's own cells only (p^{n-1} or q^{n+2}, the stored Lap p^n, c^2 dt^2, A, B), so a
-// thread loads those straight into registers: C once per CTA, the per-shot fields one shot ahead
-// of their use, and A/B per row in absorbing-layer tiles only (L1 hits). Each thread computes the shared/global offsets of the 16-byte chunks it
-// copies once per CTA; per shot it only adds the shot's base address. A thread owns VZ adjacent
-// columns and RX rows: it slides a (2R+1)-row register window down its columns, reading each row
-// once as a VZ-wide vector plus two halo vectors, so every shared-memory access is a
-// conflict-free 8- or 16-byte load. c^2 dt^2 is staged once per CTA (it is the same for every
-// shot); the absorbing A/B are read per row from global memory in layer tiles only (L1 hits).
+// absorbs the extra cost of tiles in the absorbing layer. A thread owns VZ adjacent columns and
+// RX rows: it slides a (2R+1)-row register window down its columns, reading each row of the
+// stencil field once as a VZ-wide vector plus two halo vectors from shared memory, so every
+// shared-memory access is a conflict-free 8- or 16-byte load. The stencil field (p^n, or q^{n+1}
+// in the adjoint) is staged per shot with an R-row and 16-byte-column halo by cp.async through a
+// ring of NS buffers, so the copies of the next NS-1 shots are in flight while shot s is computed.
+// Each thread computes the shared/global offsets of the 16-byte chunks it copies once per CTA;
+// per shot it only adds the shot's base address.
+//
+// The two directions feed the per-cell fields differently, each the faster way on a 552^2 grid:
+//  - fwd2d loads the fields it reads only at its own cells straight into registers: c^2 dt^2 and
+//    (in absorbing-layer tiles) A and B once per CTA, p^{n-1} one shot ahead of its use;
+//  - adj2d stages q^{n+2}, the stored Lap p^n and c^2 dt^2 as core tiles in the same cp.async
+//    ring and reads A and B per row (layer tiles only, L1 hits), which keeps its register count
+//    at three CTAs per SM next to the gradient sums it holds.
 //
 // The step kernels are launched with programmatic dependent launch: each one waits
 // (griddepcontrol.wait) for the previous kernel in the stream to finish and flush before it reads
@@ -22,7 +25,9 @@
 //
 // Receivers are gathered and adjoint sources injected inside the same kernels, from per-tile
 // tables built on the host (the receivers whose stencil corner lies in the tile; the cells of the
-// tile that receiver stencils touch), in a fixed order, so results are bitwise reproducible.
+// tile that receiver stencils touch), in a fixed order, and the stencil arithmetic has a fixed
+// rounding sequence (fma_rn and friends), so results are bitwise reproducible and independent of
+// the tile shape.
 #pragma once
 #include <type_traits>
 
@@ -149,8 +154,9 @@ struct Tile2Shape {
   static constexpr int EPC = 16 / (int)sizeof(T); // elements per 16-byte chunk
   static constexpr int HR = TX + 2 * R;           // rows of a halo tile
   static constexpr int PS = HR * SW;              // elements of a halo tile
-  static constexpr int QS = TX * TZ;              // cells of a tile
+  static constexpr int QS = TX * TZ;              // elements of a core tile
   static constexpr int NCH = (HR * (SW / EPC) + 255) / 256;  // halo chunks per thread
+  static constexpr int NCC = (TX * (TZ / EPC) + 255) / 256;  // core chunks per thread
   static constexpr int NS = sizeof(T) == 8 ? 2 : 3;          // shot buffers in the copy ring
 };
 
@@ -177,6 +183,23 @@ __device__ __forceinline__ CopyPlan<Tile2Shape<T, VZ, RX, R>::NCH> plan_halo(con
     const int z = z0 - S::HL + ch * S::EPC;
     p.soff[i] = row * S::SW + ch * S::EPC;
     p.goff[i] = (c < S::HR * CPR && x < g.n0 + R && z < (int)g.s0) ? (int)(g.origin + (long long)x * g.s0 + z) : -1;
+  }
+  return p;
+}
+// Core tile: rows [x0, x0 + TX) x columns [z0, z0 + TZ), row pitch TZ.
+template <typename T, int VZ, int RX, int R>
+__device__ __forceinline__ CopyPlan<Tile2Shape<T, VZ, RX, R>::NCC> plan_core(const KGrid<T>& g, int x0, int z0) {
+  using S = Tile2Shape<T, VZ, RX, R>;
+  constexpr int CPR = S::TZ / S::EPC;
+  CopyPlan<S::NCC> p;
+#pragma unroll
+  for (int i = 0; i < S::NCC; ++i) {
+    const int c = threadIdx.x + 256 * i;
+    const int row = c / CPR, ch = c - row * CPR;
+    const int x = x0 + row;
+    const int z = z0 + ch * S::EPC;
+    p.soff[i] = row * S::TZ + ch * S::EPC;
+    p.goff[i] = (c < S::TX * CPR && x < g.n0 && z < (int)g.s0) ? (int)(g.origin + (long long)x * g.s0 + z) : -1;
   }
   return p;
 }
@@ -209,20 +232,29 @@ __device__ __forceinline__ void store_row(T* dst, const T (&o)[VZ], int zc, int 
 }
 
 
+// The Laplacian of the window's centre row at column v, and the leapfrog update, in a fixed
+// rounding sequence.
+template <typename T, int R, int VZ>
+__device__ __forceinline__ T lap_at(const T (&wv)[2 * R + 1][VZ], const Row3<T, VZ>& rw, int v, T wc, T w1x,
+                                    T w1z, T w2x, T w2z) {
+  T lap = fma_rn(w1z, add_rn(zval(rw, v - 1), zval(rw, v + 1)),
+                 fma_rn(w1x, add_rn(wv[R - 1][v], wv[R + 1][v]), mul_rn(wc, wv[R][v])));
+  if (R == 2)
+    lap = fma_rn(w2z, add_rn(zval(rw, v - 2), zval(rw, v + 2)), fma_rn(w2x, add_rn(wv[0][v], wv[4][v]), lap));
+  return lap;
+}
+
 // ------------------------------------------------------------------------------------------
-// One leapfrog step of every shot of a group over one tile: forward (ADJ = false) or adjoint
-// (ADJ = true). The forward also samples receivers from the staged p^n tile, adds the shots'
-// point sources and, with lap_out, stores Lap p^n; the adjoint adds C R^T g_n at the
-// receiver-touched cells and accumulates q^{n+1} Lap p^n over the group's shots in registers,
-// then adds the sum into the group's accumulator (one writer per cell and group).
+// Forward step of every shot of a group over one tile: p^{n+1} = A (2 p^n - B p^{n-1} +
+// C Lap p^n + S w(n)); also samples the tile's receivers from the staged p^n tile, adds the
+// shots' point sources and, with lap_out, stores Lap p^n (the gradient factor).
 // ------------------------------------------------------------------------------------------
-template <typename T, int R, int VZ, int RX, bool AB, bool ADJ>
-__global__ void __launch_bounds__(256, 3) step2d(KGrid<T> g, Tiled2<T> a) {
+template <typename T, int R, int VZ, int RX, bool AB>
+__global__ void __launch_bounds__(256, 3) fwd2d(KGrid<T> g, Tiled2<T> a) {
   using S = Tile2Shape<T, VZ, RX, R>;
   constexpr int NS = S::NS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* sp = reinterpret_cast<T*>(smem_raw);  // [NS][PS] p^n | q^{n+1}, with halo
-  T* sj = sp + NS * S::PS;                  // adjoint: [QS] cotangent injected at this shot's cells
+  T* sp = reinterpret_cast<T*>(smem_raw);  // [NS][PS] p^n with halo
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int z0 = blockIdx.x * S::TZ, x0 = blockIdx.y * S::TX;
@@ -233,7 +265,6 @@ __global__ void __launch_bounds__(256, 3) step2d(KGrid<T> g, Tiled2<T> a) {
   const int xr = x0 + warp * RX;  // first owned row
   const int lrow = warp * RX;     // first owned row inside the tile
   const bool own_cols = zc < g.n1;
-  const bool grad = ADJ && a.lap != nullptr;
   const int ld = (int)g.s0;
   const long long cbase = g.origin + (long long)xr * ld + zc;  // owned cells of row k: + k*ld
   bool ok[RX];  // row k of the owned cells lies in the grid
@@ -249,55 +280,24 @@ __global__ void __launch_bounds__(256, 3) step2d(KGrid<T> g, Tiled2<T> a) {
     cp_async_commit();                // wait_group<NS-1> in the loop means "shot s has landed"
   }
   const bool layer_tile = AB && (x0 < g.lo0 || x0 + S::TX > g.hi0 || z0 < g.lo1 || z0 + S::TZ > g.hi1);
-  const bool use_a = layer_tile && (!ADJ || a.apply_a);
-  const bool use_b = layer_tile && (ADJ || !a.b_one);
-  // C of the owned cells and the first shot's per-cell fields, in registers
-  T cr[RX][VZ], pv[RX][VZ], lv[RX][VZ];
+  const bool use_b = layer_tile && !a.b_one;
+  // coefficients of the owned cells and the first shot's p^{n-1}, in registers
+  T cr[RX][VZ], ar[RX][VZ], br[RX][VZ], pv[RX][VZ];
 #pragma unroll
   for (int k = 0; k < RX; ++k) {
 #pragma unroll
-    for (int v = 0; v < VZ; ++v) { cr[k][v] = T(0); pv[k][v] = T(0); lv[k][v] = T(0); }
+    for (int v = 0; v < VZ; ++v) { cr[k][v] = T(0); ar[k][v] = T(1); br[k][v] = T(1); pv[k][v] = T(0); }
     if (ok[k]) {
       const long long o = cbase + (long long)k * ld;
       vldg<T, VZ>(a.C + o, cr[k]);
+      if (layer_tile) vldg<T, VZ>(a.A + o, ar[k]);
+      if (use_b) vldg<T, VZ>(a.B + o, br[k]);
       vldg<T, VZ>(a.prev + (long long)sb * g.field + o, pv[k]);
-      if (grad) vldg<T, VZ>(a.lap + (long long)sb * g.field + o, lv[k]);
     }
   }
-  int e0 = 0, e1 = 0, c0 = 0, c1 = 0;
-  if (!ADJ && a.traces) { e0 = a.tt.rec_ptr[tile]; e1 = a.tt.rec_ptr[tile + 1]; }
-  if (ADJ && a.gtr) { c0 = a.tt.cell_ptr[tile]; c1 = a.tt.cell_ptr[tile + 1]; }
-  const bool inject = ADJ && c1 > c0;  // uniform
-  // adjoint injection: thread t owns touched cell c0 + t of the tile; its table entries (receiver,
-  // weight) are shot-independent and cached here, so a shot only loads the cotangents themselves
-  constexpr int kEnt = 4;
-  int jl = -1, jn = 0, jrec[kEnt];
-  T jw[kEnt];
-  bool jslow = false;  // more entries than cached: read the table every shot
-  if (inject) {
-    for (int i = threadIdx.x; i < S::QS; i += 256) sj[i] = T(0);
-    const int e = c0 + threadIdx.x;
-    if (e < c1) {
-      jl = a.tt.cell_local[e];
-      const int gid = a.tt.cell_gid[e];
-      const int q0 = a.tt.gcell_ptr[gid];
-      jn = a.tt.gcell_ptr[gid + 1] - q0;
-      jslow = jn > kEnt;
-#pragma unroll
-      for (int m = 0; m < kEnt; ++m) {
-        jrec[m] = (m < jn) ? a.tt.gcell_rec[q0 + m] : 0;
-        jw[m] = (m < jn) ? a.gcell_w[q0 + m] : T(0);
-      }
-    }
-    __syncthreads();  // zeroing completes before any thread writes a cotangent value
-  }
-
+  int e0 = 0, e1 = 0;
+  if (a.traces) { e0 = a.tt.rec_ptr[tile]; e1 = a.tt.rec_ptr[tile + 1]; }
   const T wc = g.wc, w1x = g.w1a, w1z = g.w1b, w2x = g.w2a, w2z = g.w2b;
-  T gsum[RX][VZ];  // adjoint: per-cell sum over this CTA's shots
-#pragma unroll
-  for (int k = 0; k < RX; ++k)
-#pragma unroll
-    for (int v = 0; v < VZ; ++v) gsum[k][v] = T(0);
 
   for (int s = sb; s < se; ++s) {
     const int buf = (s - sb) % NS;
@@ -307,27 +307,10 @@ __global__ void __launch_bounds__(256, 3) step2d(KGrid<T> g, Tiled2<T> a) {
       cp_async_commit();
       cp_async_wait<NS - 1>();
     }
-    if (inject) {  // cotangent of shot s at each touched cell, summed in table order
-      const T* gs = a.gtr + (long long)s * a.n_rec * a.n_t + a.j;
-      if (jl >= 0 && !jslow) {
-        T acc = T(0);
-#pragma unroll
-        for (int m = 0; m < kEnt; ++m)
-          if (m < jn) acc = fma_rn(jw[m], gs[(long long)jrec[m] * a.n_t], acc);
-        sj[jl] = acc;
-      }
-      for (int e = c0 + threadIdx.x + (jslow ? 0 : 256); e < c1; e += 256) {  // the uncached cells
-        const int gid = a.tt.cell_gid[e];
-        T acc = T(0);
-        for (int q = a.tt.gcell_ptr[gid]; q < a.tt.gcell_ptr[gid + 1]; ++q)
-          acc = fma_rn(a.gcell_w[q], gs[(long long)a.tt.gcell_rec[q] * a.n_t], acc);
-        sj[a.tt.cell_local[e]] = acc;
-      }
-    }
     __syncthreads();
     const T* P = sp + buf * S::PS;
 
-    for (int e = e0 + threadIdx.x; e < e1; e += 256) {  // forward: receiver samples of p^n
+    for (int e = e0 + threadIdx.x; e < e1; e += 256) {  // receiver samples of p^n
       const int r = a.tt.rec_list[e];
       const int row = a.tt.rec_corner[2 * r] - x0 + R, col = a.tt.rec_corner[2 * r + 1] - z0 + S::HL;
       const T* w = a.rec_w + 4 * r;
@@ -337,11 +320,11 @@ __global__ void __launch_bounds__(256, 3) step2d(KGrid<T> g, Tiled2<T> a) {
       acc = fma_rn(w[3], P[(row + 1) * S::SW + col + 1], acc);
       a.traces[((long long)s * a.n_rec + r) * a.n_t + a.j] = acc;
     }
-    // forward: the shot's source stencil, if it touches this tile (a CTA-uniform test)
+    // the shot's source stencil, if it touches this tile (a CTA-uniform test)
     int bx = 0, bz = 0;
     bool src_tile = false;
     T sw0 = 0, sw1 = 0, sw2 = 0, sw3 = 0;
-    if (!ADJ && a.src_corner) {
+    if (a.src_corner) {
       bx = a.src_corner[2 * s];
       bz = a.src_corner[2 * s + 1];
       src_tile = bx + 1 >= x0 && bx < x0 + S::TX && bz + 1 >= z0 && bz < z0 + S::TZ;
@@ -368,26 +351,11 @@ __global__ void __launch_bounds__(256, 3) step2d(KGrid<T> g, Tiled2<T> a) {
       for (int v = 0; v < VZ; ++v) rw.c[v] = wv[R][v];
       vload<T, VZ>(P + prow * S::SW + S::HL + lane * VZ + VZ, rw.r);
       const int x = xr + k;
-      T ca[VZ], cb[VZ];
-#pragma unroll
-      for (int v = 0; v < VZ; ++v) { ca[v] = T(1); cb[v] = T(1); }
-      if (use_a && ok[k]) vldg<T, VZ>(a.A + cbase + (long long)k * ld, ca);
-      if (use_b && ok[k]) vldg<T, VZ>(a.B + cbase + (long long)k * ld, cb);
-      T inj[VZ];
-#pragma unroll
-      for (int v = 0; v < VZ; ++v) inj[v] = T(0);
-      if (inject) vload<T, VZ>(sj + (lrow + k) * S::TZ + lane * VZ, inj);
       T o[VZ], lp[VZ];
 #pragma unroll
-      for (int v = 0; v < VZ; ++v) {  // fixed rounding sequence (see fma_rn)
-        const T c = wv[R][v];
-        T lap = fma_rn(w1z, add_rn(zval(rw, v - 1), zval(rw, v + 1)),
-                       fma_rn(w1x, add_rn(wv[R - 1][v], wv[R + 1][v]), mul_rn(wc, c)));
-        if (R == 2)
-          lap = fma_rn(w2z, add_rn(zval(rw, v - 2), zval(rw, v + 2)),
-                       fma_rn(w2x, add_rn(wv[0][v], wv[4][v]), lap));
-        lp[v] = lap;
-        o[v] = fma_rn(cr[k][v], inject ? add_rn(lap, inj[v]) : lap, fma_rn(-cb[v], pv[k][v], add_rn(c, c)));
+      for (int v = 0; v < VZ; ++v) {
+        lp[v] = lap_at<T, R, VZ>(wv, rw, v, wc, w1x, w1z, w2x, w2z);
+        o[v] = fma_rn(cr[k][v], lp[v], fma_rn(-br[k][v], pv[k][v], add_rn(wv[R][v], wv[R][v])));
       }
       if (src_tile) {
 #pragma unroll
@@ -397,23 +365,183 @@ __global__ void __launch_bounds__(256, 3) step2d(KGrid<T> g, Tiled2<T> a) {
             o[v] = add_rn(o[v], (dx == 0) ? (dz == 0 ? sw0 : sw1) : (dz == 0 ? sw2 : sw3));
         }
       }
+      if (layer_tile) {
+#pragma unroll
+        for (int v = 0; v < VZ; ++v) o[v] = mul_rn(ar[k][v], o[v]);
+      }
+      if (ok[k]) {
+        const long long ro = cbase + (long long)k * ld;
+        store_row<T, VZ>(a.next + so + ro, o, zc, g.n1);
+        if (a.lap_out) store_row<T, VZ>(a.lap_out + so + ro, lp, zc, g.n1);
+        if (more) vldg<T, VZ>(a.prev + sn + ro, pv[k]);  // in flight while the rest of this shot runs
+      }
+#pragma unroll
+      for (int q = 0; q < 2 * R; ++q)
+#pragma unroll
+        for (int v = 0; v < VZ; ++v) wv[q][v] = wv[q + 1][v];
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Adjoint step of every shot of a group over one tile: q^n = A (2 q^{n+1} - B q^{n+2} +
+// C (Lap q^{n+1} + R^T g_n)), with the receiver cotangents injected at the touched cells of the
+// tile; accumulates q^{n+1} Lap p^n over the group's shots in registers and adds the sum into
+// the group's accumulator (one writer per cell and group).
+// ------------------------------------------------------------------------------------------
+template <typename T, int R, int VZ, int RX, bool AB>
+__global__ void __launch_bounds__(256, 3) adj2d(KGrid<T> g, Tiled2<T> a) {
+  using S = Tile2Shape<T, VZ, RX, R>;
+  constexpr int NS = S::NS;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* scc = reinterpret_cast<T*>(smem_raw);  // [QS] C
+  T* sp = scc + S::QS;                      // [NS][PS] q^{n+1} with halo
+  T* sq = sp + NS * S::PS;                  // [NS][QS] q^{n+2}
+  T* sl = sq + NS * S::QS;                  // [NS][QS] Lap p^n
+  T* sj = sl + NS * S::QS;                  // [QS] cotangent injected at this shot's cells
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int z0 = blockIdx.x * S::TZ, x0 = blockIdx.y * S::TX;
+  const int tile = blockIdx.y * a.tt.tiles_z + blockIdx.x;
+  const int sb = blockIdx.z * a.shots_per_cta;
+  const int se = min(sb + a.shots_per_cta, a.n_shots);
+  const int zc = z0 + lane * VZ;  // first owned column
+  const int xr = x0 + warp * RX;  // first owned row
+  const int lrow = warp * RX;     // first owned row inside the tile
+  const bool own_cols = zc < g.n1;
+  const bool grad = a.lap != nullptr;
+
+  const CopyPlan<S::NCH> ph = plan_halo<T, VZ, RX, R>(g, x0, z0);
+  const CopyPlan<S::NCC> pc = plan_core<T, VZ, RX, R>(g, x0, z0);
+  wait_previous_grid();
+  allow_next_grid();
+  issue(pc, a.C, scc);
+#pragma unroll
+  for (int i = 0; i < NS - 1; ++i) {  // one commit group per shot, empty groups included, so that
+    if (sb + i < se) {                // wait_group<NS-1> in the loop means "shot s has landed"
+      issue(ph, a.cur + (long long)(sb + i) * g.field, sp + i * S::PS);
+      issue(pc, a.prev + (long long)(sb + i) * g.field, sq + i * S::QS);
+      if (grad) issue(pc, a.lap + (long long)(sb + i) * g.field, sl + i * S::QS);
+    }
+    cp_async_commit();
+  }
+  int c0 = 0, c1 = 0;
+  if (a.gtr) { c0 = a.tt.cell_ptr[tile]; c1 = a.tt.cell_ptr[tile + 1]; }
+  const bool inject = c1 > c0;  // uniform
+  // thread t owns touched cell c0 + t of the tile; its table entries (receiver, weight) are
+  // shot-independent and cached here, so a shot only loads the cotangents themselves
+  constexpr int kEnt = 4;
+  int jl = -1, jn = 0, jrec[kEnt];
+  T jw[kEnt];
+  bool jslow = false;  // more entries than cached: read the table every shot
+  if (inject) {
+    for (int i = threadIdx.x; i < S::QS; i += 256) sj[i] = T(0);
+    const int e = c0 + threadIdx.x;
+    if (e < c1) {
+      jl = a.tt.cell_local[e];
+      const int gid = a.tt.cell_gid[e];
+      const int q0 = a.tt.gcell_ptr[gid];
+      jn = a.tt.gcell_ptr[gid + 1] - q0;
+      jslow = jn > kEnt;
+#pragma unroll
+      for (int m = 0; m < kEnt; ++m) {
+        jrec[m] = (m < jn) ? a.tt.gcell_rec[q0 + m] : 0;
+        jw[m] = (m < jn) ? a.gcell_w[q0 + m] : T(0);
+      }
+    }
+    __syncthreads();  // zeroing completes before any thread writes a cotangent value
+  }
+
+  const bool layer_tile = AB && (x0 < g.lo0 || x0 + S::TX > g.hi0 || z0 < g.lo1 || z0 + S::TZ > g.hi1);
+  const bool use_a = layer_tile && a.apply_a;
+  const T wc = g.wc, w1x = g.w1a, w1z = g.w1b, w2x = g.w2a, w2z = g.w2b;
+  const int ld = (int)g.s0;
+  const long long cbase = g.origin + (long long)xr * ld + zc;  // owned cells of row k: + k*ld
+  T gsum[RX][VZ];  // per-cell sum over this CTA's shots
+#pragma unroll
+  for (int k = 0; k < RX; ++k)
+#pragma unroll
+    for (int v = 0; v < VZ; ++v) gsum[k][v] = T(0);
+
+  for (int s = sb; s < se; ++s) {
+    const int buf = (s - sb) % NS;
+    {
+      const int sn = s + NS - 1, nb = (sn - sb) % NS;  // nb: the buffer shot s-1 used
+      if (sn < se) {
+        issue(ph, a.cur + (long long)sn * g.field, sp + nb * S::PS);
+        issue(pc, a.prev + (long long)sn * g.field, sq + nb * S::QS);
+        if (grad) issue(pc, a.lap + (long long)sn * g.field, sl + nb * S::QS);
+      }
+      cp_async_commit();
+      cp_async_wait<NS - 1>();
+    }
+    if (inject) {  // cotangent of shot s at each touched cell, summed in table order
+      const T* gs = a.gtr + (long long)s * a.n_rec * a.n_t + a.j;
+      if (jl >= 0 && !jslow) {
+        T acc = T(0);
+#pragma unroll
+        for (int m = 0; m < kEnt; ++m)
+          if (m < jn) acc = fma_rn(jw[m], gs[(long long)jrec[m] * a.n_t], acc);
+        sj[jl] = acc;
+      }
+      for (int e = c0 + threadIdx.x + (jslow ? 0 : 256); e < c1; e += 256) {  // the uncached cells
+        const int gid = a.tt.cell_gid[e];
+        T acc = T(0);
+        for (int q = a.tt.gcell_ptr[gid]; q < a.tt.gcell_ptr[gid + 1]; ++q)
+          acc = fma_rn(a.gcell_w[q], gs[(long long)a.tt.gcell_rec[q] * a.n_t], acc);
+        sj[a.tt.cell_local[e]] = acc;
+      }
+    }
+    __syncthreads();
+    const T* P = sp + buf * S::PS;
+    const T* Q = sq + buf * S::QS;
+    const T* LP = sl + buf * S::QS;
+
+    T wv[2 * R + 1][VZ];  // sliding window over q^{n+1}, own columns
+#pragma unroll
+    for (int q = 0; q < 2 * R; ++q) vload<T, VZ>(P + (lrow + q) * S::SW + S::HL + lane * VZ, wv[q]);
+    T* ob = a.next + (long long)s * g.field + cbase;
+#pragma unroll
+    for (int k = 0; k < RX; ++k) {
+      const int prow = lrow + k + R;
+      vload<T, VZ>(P + (prow + R) * S::SW + S::HL + lane * VZ, wv[2 * R]);
+      Row3<T, VZ> rw;
+      vload<T, VZ>(P + prow * S::SW + S::HL + lane * VZ - VZ, rw.l);
+#pragma unroll
+      for (int v = 0; v < VZ; ++v) rw.c[v] = wv[R][v];
+      vload<T, VZ>(P + prow * S::SW + S::HL + lane * VZ + VZ, rw.r);
+      const int toff = (lrow + k) * S::TZ + lane * VZ;  // the owned cells in a core tile
+      T q2[VZ], cc[VZ];
+      vload<T, VZ>(Q + toff, q2);
+      vload<T, VZ>(scc + toff, cc);
+      const int x = xr + k;
+      const bool ok = own_cols && x < g.n0;
+      T ca[VZ], cb[VZ], inj[VZ];
+#pragma unroll
+      for (int v = 0; v < VZ; ++v) { ca[v] = T(1); cb[v] = T(1); inj[v] = T(0); }
+      if (layer_tile && ok) {
+        vldg<T, VZ>(a.A + cbase + (long long)k * ld, ca);
+        vldg<T, VZ>(a.B + cbase + (long long)k * ld, cb);
+      }
+      if (inject) vload<T, VZ>(sj + toff, inj);
+      T o[VZ];
+#pragma unroll
+      for (int v = 0; v < VZ; ++v) {
+        const T lap = lap_at<T, R, VZ>(wv, rw, v, wc, w1x, w1z, w2x, w2z);
+        o[v] = fma_rn(cc[v], inject ? add_rn(lap, inj[v]) : lap, fma_rn(-cb[v], q2[v], add_rn(wv[R][v], wv[R][v])));
+      }
       if (use_a) {
 #pragma unroll
         for (int v = 0; v < VZ; ++v) o[v] = mul_rn(ca[v], o[v]);
       }
       if (grad) {
+        T gl[VZ];
+        vload<T, VZ>(LP + toff, gl);
 #pragma unroll
-        for (int v = 0; v < VZ; ++v) gsum[k][v] = fma_rn(wv[R][v], lv[k][v], gsum[k][v]);
+        for (int v = 0; v < VZ; ++v) gsum[k][v] = fma_rn(wv[R][v], gl[v], gsum[k][v]);
       }
-      if (ok[k]) {
-        const long long ro = cbase + (long long)k * ld;
-        store_row<T, VZ>(a.next + so + ro, o, zc, g.n1);
-        if (!ADJ && a.lap_out) store_row<T, VZ>(a.lap_out + so + ro, lp, zc, g.n1);
-        if (more) {  // the next shot's per-cell fields: in flight while the rest of this shot runs
-          vldg<T, VZ>(a.prev + sn + ro, pv[k]);
-          if (grad) vldg<T, VZ>(a.lap + sn + ro, lv[k]);
-        }
-      }
+      if (ok) store_row<T, VZ>(ob + (long long)k * ld, o, zc, g.n1);
 #pragma unroll
       for (int q = 0; q < 2 * R; ++q)
 #pragma unroll
@@ -429,7 +557,7 @@ __global__ void __launch_bounds__(256, 3) step2d(KGrid<T> g, Tiled2<T> a) {
     T* gp = a.gacc + (long long)blockIdx.z * g.field + cbase;
 #pragma unroll
     for (int k = 0; k < RX; ++k) {
-      if (!ok[k]) continue;
+      if (xr + k >= g.n0) continue;
 #pragma unroll
       for (int v = 0; v < VZ; ++v)
         if (zc + v < g.n1) gp[(long long)k * ld + v] += gsum[k][v];

@@ -246,12 +246,12 @@ int n_acc_fields(const nw_grid* g, const Tune& t, int n_shots) {
   return g->ndim == 3 ? n_shots : t.adj.groups(n_shots);
 }
 
-// Dynamic shared memory of step2d: the ring of halo tiles and, in the adjoint, the injected
-// cotangents of one shot.
+// Dynamic shared memory: fwd2d stages the ring of p^n halo tiles; adj2d stages C, the ring of
+// (q^{n+1} halo, q^{n+2} core, Lap p^n core) tiles and one shot's injected cotangents.
 template <typename T, int R, int VZ, int RX, bool ADJ>
 constexpr size_t step2_smem() {
   using S = nw::Tile2Shape<T, VZ, RX, R>;
-  return (S::NS * S::PS + (ADJ ? S::QS : 0)) * sizeof(T);
+  return (ADJ ? 2 * S::QS + S::NS * (S::PS + 2 * S::QS) : S::NS * S::PS) * sizeof(T);
 }
 constexpr size_t kMaxSmem = 227 * 1024;  // opt-in shared memory per CTA on sm_100a
 
@@ -297,22 +297,23 @@ nw::TileTables tile_tables(const nw_grid* g, const nw_acquisition* a, const Tile
   return tt;
 }
 
-template <typename T, int R, int VZ, int RX, bool AB, bool ADJ>
-int launch_step2(const nw::KGrid<T>& kg, const nw::Tiled2<T>& st, dim3 grid, cudaStream_t s) {
-  constexpr size_t smem = step2_smem<T, R, VZ, RX, ADJ>();
-  if (smem > kMaxSmem) return fail(NW_ERR_ARG, "tile too large for shared memory (lower tuning rx or vz)");
-  static bool done = false;
-  int rc = allow_smem(nw::step2d<T, R, VZ, RX, AB, ADJ>, smem, &done);
-  if (rc) return rc;
-  return launch_pdl(nw::step2d<T, R, VZ, RX, AB, ADJ>, grid, smem, s, kg, st);
-}
 template <typename T, int R, int VZ, int RX, bool AB>
 int launch_fwd2_v(const nw::KGrid<T>& kg, const nw::Tiled2<T>& st, dim3 grid, cudaStream_t s) {
-  return launch_step2<T, R, VZ, RX, AB, false>(kg, st, grid, s);
+  constexpr size_t smem = step2_smem<T, R, VZ, RX, false>();
+  if (smem > kMaxSmem) return fail(NW_ERR_ARG, "tile too large for shared memory (lower tuning rx or vz)");
+  static bool done = false;
+  int rc = allow_smem(nw::fwd2d<T, R, VZ, RX, AB>, smem, &done);
+  if (rc) return rc;
+  return launch_pdl(nw::fwd2d<T, R, VZ, RX, AB>, grid, smem, s, kg, st);
 }
 template <typename T, int R, int VZ, int RX, bool AB>
 int launch_adj2_v(const nw::KGrid<T>& kg, const nw::Tiled2<T>& st, dim3 grid, cudaStream_t s) {
-  return launch_step2<T, R, VZ, RX, AB, true>(kg, st, grid, s);
+  constexpr size_t smem = step2_smem<T, R, VZ, RX, true>();
+  if (smem > kMaxSmem) return fail(NW_ERR_ARG, "tile too large for shared memory (lower tuning adj_rx or adj_vz)");
+  static bool done = false;
+  int rc = allow_smem(nw::adj2d<T, R, VZ, RX, AB>, smem, &done);
+  if (rc) return rc;
+  return launch_pdl(nw::adj2d<T, R, VZ, RX, AB>, grid, smem, s, kg, st);
 }
 
 // 3-D step: forward (ADJ = false) or adjoint.
