@@ -158,6 +158,8 @@ struct Tile2Shape {
   static constexpr int NCH = (HR * (SW / EPC) + 255) / 256;  // halo chunks per thread
   static constexpr int NCC = (TX * (TZ / EPC) + 255) / 256;  // core chunks per thread
   static constexpr int NS = sizeof(T) == 8 ? 2 : 3;          // shot buffers in the copy ring
+  // the adjoint stages three tiles per shot: a two-shot ring keeps larger tiles at 3 CTAs per SM
+  static constexpr int NSA = (sizeof(T) == 8 || RX >= 4) ? 2 : 3;
 };
 
 // The chunks one thread copies for one tile region: shared and global element offsets (the
@@ -393,7 +395,7 @@ __global__ void __launch_bounds__(256, 3) fwd2d(KGrid<T> g, Tiled2<T> a) {
 template <typename T, int R, int VZ, int RX, bool AB>
 __global__ void __launch_bounds__(256, 3) adj2d(KGrid<T> g, Tiled2<T> a) {
   using S = Tile2Shape<T, VZ, RX, R>;
-  constexpr int NS = S::NS;
+  constexpr int NS = S::NSA;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* scc = reinterpret_cast<T*>(smem_raw);  // [QS] C
   T* sp = scc + S::QS;                      // [NS][PS] q^{n+1} with halo

@@ -251,7 +251,7 @@ int n_acc_fields(const nw_grid* g, const Tune& t, int n_shots) {
 template <typename T, int R, int VZ, int RX, bool ADJ>
 constexpr size_t step2_smem() {
   using S = nw::Tile2Shape<T, VZ, RX, R>;
-  return (ADJ ? 2 * S::QS + S::NS * (S::PS + 2 * S::QS) : S::NS * S::PS) * sizeof(T);
+  return (ADJ ? 2 * S::QS + S::NSA * (S::PS + 2 * S::QS) : S::NS * S::PS) * sizeof(T);
 }
 constexpr size_t kMaxSmem = 227 * 1024;  // opt-in shared memory per CTA on sm_100a
 
