@@ -14,9 +14,9 @@
 // The two directions feed the per-cell fields differently, each the faster way on a 552^2 grid:
 //  - fwd2d loads the fields it reads only at its own cells straight into registers: c^2 dt^2 and
 //    (in absorbing-layer tiles) A and B once per CTA, p^{n-1} one shot ahead of its use;
-//  - adj2d stages q^{n+2}, the stored Lap p^n and c^2 dt^2 as core tiles in the same cp.async
-//    ring and reads A and B per row (layer tiles only, L1 hits), which keeps its register count
-//    at three CTAs per SM next to the gradient sums it holds.
+//  - adj2d stages q^{n+2} and the stored Lap p^n as core tiles in the same cp.async ring, and
+//    c^2 dt^2, A, B (layer tiles) and its group's gradient accumulator tile once per CTA, which
+//    keeps its register count at three CTAs per SM next to the gradient sums it holds.
 //
 // The step kernels are launched with programmatic dependent launch: each one waits
 // (griddepcontrol.wait) for the previous kernel in the stream to finish and flush before it reads
@@ -398,7 +398,10 @@ __global__ void __launch_bounds__(256, 3) adj2d(KGrid<T> g, Tiled2<T> a) {
   constexpr int NS = S::NSA;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* scc = reinterpret_cast<T*>(smem_raw);  // [QS] C
-  T* sp = scc + S::QS;                      // [NS][PS] q^{n+1} with halo
+  T* sa = scc + S::QS;                      // [QS] A (layer tiles)
+  T* sbb = sa + S::QS;                      // [QS] B (layer tiles)
+  T* sg = sbb + S::QS;                      // [QS] the group's gradient accumulator
+  T* sp = sg + S::QS;                       // [NS][PS] q^{n+1} with halo
   T* sq = sp + NS * S::PS;                  // [NS][QS] q^{n+2}
   T* sl = sq + NS * S::QS;                  // [NS][QS] Lap p^n
   T* sj = sl + NS * S::QS;                  // [QS] cotangent injected at this shot's cells
@@ -414,11 +417,18 @@ __global__ void __launch_bounds__(256, 3) adj2d(KGrid<T> g, Tiled2<T> a) {
   const bool own_cols = zc < g.n1;
   const bool grad = a.lap != nullptr;
 
+  const bool layer_tile = AB && (x0 < g.lo0 || x0 + S::TX > g.hi0 || z0 < g.lo1 || z0 + S::TZ > g.hi1);
   const CopyPlan<S::NCH> ph = plan_halo<T, VZ, RX, R>(g, x0, z0);
   const CopyPlan<S::NCC> pc = plan_core<T, VZ, RX, R>(g, x0, z0);
   wait_previous_grid();
   allow_next_grid();
+  // once per CTA, in the first commit group: C, A and B (layer tiles) and the accumulator tile
   issue(pc, a.C, scc);
+  if (layer_tile) {
+    issue(pc, a.A, sa);
+    issue(pc, a.B, sbb);
+  }
+  if (grad) issue(pc, a.gacc + (long long)blockIdx.z * g.field, sg);
 #pragma unroll
   for (int i = 0; i < NS - 1; ++i) {  // one commit group per shot, empty groups included, so that
     if (sb + i < se) {                // wait_group<NS-1> in the loop means "shot s has landed"
@@ -455,7 +465,6 @@ __global__ void __launch_bounds__(256, 3) adj2d(KGrid<T> g, Tiled2<T> a) {
     __syncthreads();  // zeroing completes before any thread writes a cotangent value
   }
 
-  const bool layer_tile = AB && (x0 < g.lo0 || x0 + S::TX > g.hi0 || z0 < g.lo1 || z0 + S::TZ > g.hi1);
   const bool use_a = layer_tile && a.apply_a;
   const T wc = g.wc, w1x = g.w1a, w1z = g.w1b, w2x = g.w2a, w2z = g.w2b;
   const int ld = (int)g.s0;
@@ -522,9 +531,9 @@ __global__ void __launch_bounds__(256, 3) adj2d(KGrid<T> g, Tiled2<T> a) {
       T ca[VZ], cb[VZ], inj[VZ];
 #pragma unroll
       for (int v = 0; v < VZ; ++v) { ca[v] = T(1); cb[v] = T(1); inj[v] = T(0); }
-      if (layer_tile && ok) {
-        vldg<T, VZ>(a.A + cbase + (long long)k * ld, ca);
-        vldg<T, VZ>(a.B + cbase + (long long)k * ld, cb);
+      if (layer_tile) {
+        vload<T, VZ>(sa + toff, ca);
+        vload<T, VZ>(sbb + toff, cb);
       }
       if (inject) vload<T, VZ>(sj + toff, inj);
       T o[VZ];
@@ -555,14 +564,16 @@ __global__ void __launch_bounds__(256, 3) adj2d(KGrid<T> g, Tiled2<T> a) {
       for (int e = c0 + threadIdx.x + 256; e < c1; e += 256) sj[a.tt.cell_local[e]] = T(0);
     }
   }
-  if (grad && own_cols) {
+  if (grad && own_cols) {  // the accumulator tile landed with the first commit group
     T* gp = a.gacc + (long long)blockIdx.z * g.field + cbase;
 #pragma unroll
     for (int k = 0; k < RX; ++k) {
       if (xr + k >= g.n0) continue;
+      T old[VZ];
+      vload<T, VZ>(sg + (lrow + k) * S::TZ + lane * VZ, old);
 #pragma unroll
-      for (int v = 0; v < VZ; ++v)
-        if (zc + v < g.n1) gp[(long long)k * ld + v] += gsum[k][v];
+      for (int v = 0; v < VZ; ++v) old[v] = add_rn(old[v], gsum[k][v]);
+      store_row<T, VZ>(gp + (long long)k * ld, old, zc, g.n1);
     }
   }
 }

@@ -246,12 +246,13 @@ int n_acc_fields(const nw_grid* g, const Tune& t, int n_shots) {
   return g->ndim == 3 ? n_shots : t.adj.groups(n_shots);
 }
 
-// Dynamic shared memory: fwd2d stages the ring of p^n halo tiles; adj2d stages C, the ring of
-// (q^{n+1} halo, q^{n+2} core, Lap p^n core) tiles and one shot's injected cotangents.
+// Dynamic shared memory: fwd2d stages the ring of p^n halo tiles; adj2d stages C, A, B, the
+// accumulator tile, the ring of (q^{n+1} halo, q^{n+2} core, Lap p^n core) tiles and one shot's
+// injected cotangents.
 template <typename T, int R, int VZ, int RX, bool ADJ>
 constexpr size_t step2_smem() {
   using S = nw::Tile2Shape<T, VZ, RX, R>;
-  return (ADJ ? 2 * S::QS + S::NSA * (S::PS + 2 * S::QS) : S::NS * S::PS) * sizeof(T);
+  return (ADJ ? 5 * S::QS + S::NSA * (S::PS + 2 * S::QS) : S::NS * S::PS) * sizeof(T);
 }
 constexpr size_t kMaxSmem = 227 * 1024;  // opt-in shared memory per CTA on sm_100a
 

@@ -181,11 +181,9 @@ class _Run:
         self.ring = plan.empty_levels(3, n_shots)
         self.storage.ring = self.ring.data_ptr()
         if self.kind == "history":
-            # step n stores Lap p^n into the interior of level n; the ghosts are zeroed once
+            # step n stores Lap p^n into the interior of level n; nothing reads the ghost cells
+            # (the adjoint multiplies them only into sums of cells outside the grid, never stored)
             self.history = plan.empty_levels(n_steps, n_shots, zero=False)
-            if n_steps > 0:
-                _lib.check(_lib.load().nw_zero_ghosts(C.byref(plan.g), self.history.data_ptr(),
-                                                      n_steps * n_shots, _lib.stream_handle(plan.device)))
             self.storage.history = self.history.data_ptr()
         elif self.kind == "checkpoint":
             k = int(mode[1])
