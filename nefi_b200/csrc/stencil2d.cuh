@@ -12,8 +12,8 @@
 // per shot it only adds the shot's base address.
 //
 // The two directions feed the per-cell fields differently, each the faster way on a 552^2 grid:
-//  - fwd2d loads the fields it reads only at its own cells straight into registers: c^2 dt^2 and
-//    (in absorbing-layer tiles) A and B once per CTA, p^{n-1} one shot ahead of its use;
+//  - fwd2d stages c^2 dt^2 and (in absorbing-layer tiles) A and B once per CTA and loads p^{n-1},
+//    which it reads only at its own cells, straight into registers one shot ahead of its use;
 //  - adj2d stages q^{n+2} and the stored Lap p^n as core tiles in the same cp.async ring, and
 //    c^2 dt^2, A, B (layer tiles) and its group's gradient accumulator tile once per CTA, which
 //    keeps its register count at three CTAs per SM next to the gradient sums it holds.
@@ -252,11 +252,14 @@ __device__ __forceinline__ T lap_at(const T (&wv)[2 * R + 1][VZ], const Row3<T, 
 // shots' point sources and, with lap_out, stores Lap p^n (the gradient factor).
 // ------------------------------------------------------------------------------------------
 template <typename T, int R, int VZ, int RX, bool AB>
-__global__ void __launch_bounds__(256, 3) fwd2d(KGrid<T> g, Tiled2<T> a) {
+__global__ void __launch_bounds__(256, 4) fwd2d(KGrid<T> g, Tiled2<T> a) {
   using S = Tile2Shape<T, VZ, RX, R>;
   constexpr int NS = S::NS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* sp = reinterpret_cast<T*>(smem_raw);  // [NS][PS] p^n with halo
+  T* scc = reinterpret_cast<T*>(smem_raw);  // [QS] C
+  T* sa = scc + S::QS;                      // [QS] A (layer tiles)
+  T* sbb = sa + S::QS;                      // [QS] B (layer tiles)
+  T* sp = sbb + S::QS;                      // [NS][PS] p^n with halo
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int z0 = blockIdx.x * S::TZ, x0 = blockIdx.y * S::TX;
@@ -273,29 +276,28 @@ __global__ void __launch_bounds__(256, 3) fwd2d(KGrid<T> g, Tiled2<T> a) {
 #pragma unroll
   for (int k = 0; k < RX; ++k) ok[k] = own_cols && xr + k < g.n0;
 
+  const bool layer_tile = AB && (x0 < g.lo0 || x0 + S::TX > g.hi0 || z0 < g.lo1 || z0 + S::TZ > g.hi1);
+  const bool use_b = layer_tile && !a.b_one;
   const CopyPlan<S::NCH> ph = plan_halo<T, VZ, RX, R>(g, x0, z0);
+  const CopyPlan<S::NCC> pc = plan_core<T, VZ, RX, R>(g, x0, z0);
   wait_previous_grid();
   allow_next_grid();
+  issue(pc, a.C, scc);  // once per CTA, in the first commit group
+  if (layer_tile) {
+    issue(pc, a.A, sa);
+    issue(pc, a.B, sbb);
+  }
 #pragma unroll
   for (int i = 0; i < NS - 1; ++i) {  // one commit group per shot, empty groups included, so that
     if (sb + i < se) issue(ph, a.cur + (long long)(sb + i) * g.field, sp + i * S::PS);
     cp_async_commit();                // wait_group<NS-1> in the loop means "shot s has landed"
   }
-  const bool layer_tile = AB && (x0 < g.lo0 || x0 + S::TX > g.hi0 || z0 < g.lo1 || z0 + S::TZ > g.hi1);
-  const bool use_b = layer_tile && !a.b_one;
-  // coefficients of the owned cells and the first shot's p^{n-1}, in registers
-  T cr[RX][VZ], ar[RX][VZ], br[RX][VZ], pv[RX][VZ];
+  T pv[RX][VZ];  // p^{n-1} of the owned cells, one shot ahead
 #pragma unroll
   for (int k = 0; k < RX; ++k) {
 #pragma unroll
-    for (int v = 0; v < VZ; ++v) { cr[k][v] = T(0); ar[k][v] = T(1); br[k][v] = T(1); pv[k][v] = T(0); }
-    if (ok[k]) {
-      const long long o = cbase + (long long)k * ld;
-      vldg<T, VZ>(a.C + o, cr[k]);
-      if (layer_tile) vldg<T, VZ>(a.A + o, ar[k]);
-      if (use_b) vldg<T, VZ>(a.B + o, br[k]);
-      vldg<T, VZ>(a.prev + (long long)sb * g.field + o, pv[k]);
-    }
+    for (int v = 0; v < VZ; ++v) pv[k][v] = T(0);
+    if (ok[k]) vldg<T, VZ>(a.prev + (long long)sb * g.field + cbase + (long long)k * ld, pv[k]);
   }
   int e0 = 0, e1 = 0;
   if (a.traces) { e0 = a.tt.rec_ptr[tile]; e1 = a.tt.rec_ptr[tile + 1]; }
@@ -353,11 +355,18 @@ __global__ void __launch_bounds__(256, 3) fwd2d(KGrid<T> g, Tiled2<T> a) {
       for (int v = 0; v < VZ; ++v) rw.c[v] = wv[R][v];
       vload<T, VZ>(P + prow * S::SW + S::HL + lane * VZ + VZ, rw.r);
       const int x = xr + k;
+      const int toff = (lrow + k) * S::TZ + lane * VZ;  // the owned cells in a core tile
+      T cc[VZ], ca[VZ], cb[VZ];
+      vload<T, VZ>(scc + toff, cc);
+#pragma unroll
+      for (int v = 0; v < VZ; ++v) { ca[v] = T(1); cb[v] = T(1); }
+      if (layer_tile) vload<T, VZ>(sa + toff, ca);
+      if (use_b) vload<T, VZ>(sbb + toff, cb);
       T o[VZ], lp[VZ];
 #pragma unroll
       for (int v = 0; v < VZ; ++v) {
         lp[v] = lap_at<T, R, VZ>(wv, rw, v, wc, w1x, w1z, w2x, w2z);
-        o[v] = fma_rn(cr[k][v], lp[v], fma_rn(-br[k][v], pv[k][v], add_rn(wv[R][v], wv[R][v])));
+        o[v] = fma_rn(cc[v], lp[v], fma_rn(-cb[v], pv[k][v], add_rn(wv[R][v], wv[R][v])));
       }
       if (src_tile) {
 #pragma unroll
@@ -369,7 +378,7 @@ __global__ void __launch_bounds__(256, 3) fwd2d(KGrid<T> g, Tiled2<T> a) {
       }
       if (layer_tile) {
 #pragma unroll
-        for (int v = 0; v < VZ; ++v) o[v] = mul_rn(ar[k][v], o[v]);
+        for (int v = 0; v < VZ; ++v) o[v] = mul_rn(ca[v], o[v]);
       }
       if (ok[k]) {
         const long long ro = cbase + (long long)k * ld;

@@ -226,8 +226,8 @@ int check_tile(const nw_grid* g, const TileCfg& c, const char* which) {
 int resolve_tune(const nw_grid* g, const nw_tuning* t, Tune* out) {
   Tune r;
   // defaults: the best forward and adjoint times of a sweep on a 552^2 x 16-shot grid
-  r.fwd.vz = (t && t->vz) ? t->vz : 2;
-  r.fwd.rx = (t && t->rx) ? t->rx : 4;
+  r.fwd.vz = (t && t->vz) ? t->vz : (g->dtype == NW_F32 ? 4 : 2);
+  r.fwd.rx = (t && t->rx) ? t->rx : 2;
   r.fwd.spc = (t && t->shots_per_cta) ? t->shots_per_cta : 2;
   r.adj.vz = (t && t->adj_vz) ? t->adj_vz : 2;
   r.adj.rx = (t && t->adj_rx) ? t->adj_rx : 2;
@@ -246,13 +246,13 @@ int n_acc_fields(const nw_grid* g, const Tune& t, int n_shots) {
   return g->ndim == 3 ? n_shots : t.adj.groups(n_shots);
 }
 
-// Dynamic shared memory: fwd2d stages the ring of p^n halo tiles; adj2d stages C, A, B, the
+// Dynamic shared memory: fwd2d stages C, A, B and the ring of p^n halo tiles; adj2d stages C, A, B, the
 // accumulator tile, the ring of (q^{n+1} halo, q^{n+2} core, Lap p^n core) tiles and one shot's
 // injected cotangents.
 template <typename T, int R, int VZ, int RX, bool ADJ>
 constexpr size_t step2_smem() {
   using S = nw::Tile2Shape<T, VZ, RX, R>;
-  return (ADJ ? 5 * S::QS + S::NSA * (S::PS + 2 * S::QS) : S::NS * S::PS) * sizeof(T);
+  return (ADJ ? 5 * S::QS + S::NSA * (S::PS + 2 * S::QS) : 3 * S::QS + S::NS * S::PS) * sizeof(T);
 }
 constexpr size_t kMaxSmem = 227 * 1024;  // opt-in shared memory per CTA on sm_100a
 
