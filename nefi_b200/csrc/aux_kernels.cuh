@@ -176,34 +176,66 @@ __global__ void initial_adjoint_kernel(KGrid<T> g, PadMap pm, int ndim, const T*
   }
 }
 
-// grad_c[phys] (+)= 2 c dt2 * dJ/dC, dJ/dC = sum_acc sum_{padded cells -> phys} g_acc[cell] / C, in float64.
+// grad_c[phys] (+)= 2 c dt2 * dJ/dC, dJ/dC = sum_acc sum_{padded cells -> phys} g_acc[cell] / C, in
+// float64. A warp takes 32 consecutive physical cells: each lane sums its cell when a single
+// padded cell maps to it (the interior); cells on the border of the physical grid, onto which a
+// whole strip or block of the absorbing layer folds (up to (a+1)^ndim padded cells), are then
+// summed by the whole warp, lanes striding the block in a fixed order and combining by a fixed
+// shuffle tree, so the result is reproducible and no thread walks a corner block alone.
 template <typename T>
 __global__ void reduce_grad_kernel(KGrid<T> g, PadMap pm, int ndim, const T* __restrict__ c,
                                    double dt2, int n_acc, const T* __restrict__ gs,
                                    int accumulate, double* __restrict__ out) {
   const long long pcells = (long long)pm.m0 * pm.m1 * pm.m2;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < pcells;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int k = (int)(t % pm.m2);
-    const int j = (int)((t / pm.m2) % pm.m1);
-    const int i = (int)(t / ((long long)pm.m2 * pm.m1));
-    // padded range mapping onto physical index i along an axis of width m with layer a
-    auto lo = [](int i, int a, int m) { return i == 0 ? 0 : i + a; };
-    auto hi = [](int i, int a, int m) { return i == m - 1 ? m + 2 * a - 1 : i + a; };
-    const int x0 = lo(i, pm.a0, pm.m0), x1 = hi(i, pm.a0, pm.m0);
-    const int y0 = lo(j, pm.a1, pm.m1), y1 = hi(j, pm.a1, pm.m1);
-    const int z0 = ndim == 3 ? lo(k, pm.a2, pm.m2) : 0, z1 = ndim == 3 ? hi(k, pm.a2, pm.m2) : 0;
-    double acc = 0.0;
-    for (int s = 0; s < n_acc; ++s) {
-      const T* gp = gs + (long long)s * g.field;
-      for (int x = x0; x <= x1; ++x)
-        for (int y = y0; y <= y1; ++y)
-          for (int z = z0; z <= z1; ++z) acc += gp[ghost_index(g, ndim, x, y, z)];
-    }
+  const int lane = threadIdx.x & 31;
+  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long n_warps = ((long long)gridDim.x * blockDim.x) >> 5;
+  // padded range mapping onto physical index i along an axis of width m with layer a
+  auto lo = [](int i, int a, int m) { return i == 0 ? 0 : i + a; };
+  auto hi = [](int i, int a, int m) { return i == m - 1 ? m + 2 * a - 1 : i + a; };
+  auto finish = [&](long long t, double acc) {
     // acc = C dJ/dC summed over the padded cells that replicate c[t], all with C = c^2 dt^2
     const double cd = (double)c[t];
     const double v = 2.0 * cd * dt2 * (acc / (cd * cd * dt2));
     out[t] = accumulate ? out[t] + v : v;
+  };
+  for (long long base = warp * 32; base < pcells; base += n_warps * 32) {
+    const long long t = base + lane;
+    int x0 = 0, x1 = -1, y0 = 0, y1 = 0, z0 = 0, z1 = 0;
+    if (t < pcells) {
+      const int k = (int)(t % pm.m2);
+      const int j = (int)((t / pm.m2) % pm.m1);
+      const int i = (int)(t / ((long long)pm.m2 * pm.m1));
+      x0 = lo(i, pm.a0, pm.m0); x1 = hi(i, pm.a0, pm.m0);
+      y0 = lo(j, pm.a1, pm.m1); y1 = hi(j, pm.a1, pm.m1);
+      z0 = ndim == 3 ? lo(k, pm.a2, pm.m2) : 0; z1 = ndim == 3 ? hi(k, pm.a2, pm.m2) : 0;
+    }
+    const bool single = t < pcells && x0 == x1 && y0 == y1 && z0 == z1;
+    if (single) {
+      const long long idx = ghost_index(g, ndim, x0, y0, z0);
+      double acc = 0.0;
+      for (int s = 0; s < n_acc; ++s) acc += (double)gs[(long long)s * g.field + idx];
+      finish(t, acc);
+    }
+    unsigned todo = __ballot_sync(0xffffffffu, t < pcells && !single);
+    while (todo) {
+      const int src = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const int bx0 = __shfl_sync(0xffffffffu, x0, src), bx1 = __shfl_sync(0xffffffffu, x1, src);
+      const int by0 = __shfl_sync(0xffffffffu, y0, src), by1 = __shfl_sync(0xffffffffu, y1, src);
+      const int bz0 = __shfl_sync(0xffffffffu, z0, src), bz1 = __shfl_sync(0xffffffffu, z1, src);
+      const int ny = by1 - by0 + 1, nz = bz1 - bz0 + 1;
+      const long long nb = (long long)(bx1 - bx0 + 1) * ny * nz;
+      double part = 0.0;
+      for (long long q = lane; q < nb; q += 32) {
+        const int z = bz0 + (int)(q % nz), y = by0 + (int)((q / nz) % ny), x = bx0 + (int)(q / ((long long)nz * ny));
+        const long long idx = ghost_index(g, ndim, x, y, z);
+        for (int s = 0; s < n_acc; ++s) part += (double)gs[(long long)s * g.field + idx];
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(0xffffffffu, part, off);
+      if (lane == src) finish(t, part);
+    }
   }
 }
 
