@@ -291,6 +291,60 @@ int nw_zero_ghosts(const nw_grid* g, void* fields, int64_t n_fields, void* strea
 /* Number of kernels this library has enqueued since it was loaded (all threads). Host only. */
 uint64_t nw_launch_count(void);
 
+/*
+ * Batched FWI gradients: many independent 2-D problems (grids of different size, shot counts and
+ * step counts, one dtype and stencil order) advanced together, one launch per time step for the
+ * whole batch. This has no single counterpart in the reference, whose operators cannot be batched
+ * (nefi/solve/batched.py:68-77); each problem's traces and gradient are those nw_forward /
+ * nw_adjoint give it alone with the same tuning and snapshots (bitwise).
+ *
+ * Every problem is an FWI problem (has_source) with checkpointed storage: a ring, a snapshot pool
+ * for ceil(n_steps / segment) snapshots, a `segment`-level buffer; `segment` and snap_kind are the
+ * same for all problems. Problems must be ordered by non-increasing time.n_steps. The buffers are
+ * bound by nw_batch_prepare: later calls use the pointers given there.
+ */
+typedef struct nw_batch_problem {
+  nw_grid grid;
+  nw_medium medium;
+  nw_acquisition acq;
+  nw_time time;
+  nw_storage storage;
+  void* work;               /* 3 * n_shots fields: the adjoint's levels */
+  void* grad_acc;           /* nw_adjoint_groups() fields: c2dt2 * dJ/dc2dt2, as nw_adjoint */
+  void* traces;             /* (n_shots, n_rec, n_t): forward output */
+  const void* grad_traces;  /* (n_shots, n_rec, n_t): adjoint input */
+} nw_batch_problem;
+
+/* Bytes of the device table nw_batch_prepare writes for n_problems problems. */
+size_t nw_batch_table_bytes(int32_t n_problems);
+
+/*
+ * Validates the batch, builds the per-problem step descriptors and the CTA offsets of the batched
+ * launches, and copies them into `table` (nw_batch_table_bytes() bytes of device memory) on
+ * `stream`, waiting for the copy. Call once per batch, before any capture of the sweeps.
+ */
+int nw_batch_prepare(const nw_batch_problem* problems, int32_t n_problems, const nw_tuning* tune,
+                     void* table, void* stream);
+
+/*
+ * Forward sweep of the whole batch from p^-1 = p^0 = 0: traces of every problem, and the
+ * snapshots of every segment start. One kernel per global step over the problems still running,
+ * plus the snapshot encodes and each problem's final receiver sample. Asynchronous; no host
+ * synchronisation, so a caller may capture it in a CUDA graph.
+ */
+int nw_batch_forward(const nw_batch_problem* problems, int32_t n_problems, const nw_tuning* tune,
+                     const void* table, void* stream);
+
+/*
+ * Adjoint sweep of the whole batch from each problem's grad_traces: per segment (latest first) the
+ * snapshots are decoded and Lap p recomputed for all problems in one kernel per step, then the
+ * adjoint steps run for all problems in one kernel per step; grad_acc of every problem is zeroed
+ * first and holds the accumulated sums at the end (reduce each with nw_reduce_grad_c).
+ * Asynchronous, no host synchronisation.
+ */
+int nw_batch_adjoint(const nw_batch_problem* problems, int32_t n_problems, const nw_tuning* tune,
+                     const void* table, void* stream);
+
 /* Receiver samples of one level (n_shots fields) into traces[:, :, j]. */
 int nw_sample(const nw_grid* g, const nw_acquisition* a, int32_t n_t, const void* level,
               int32_t j, void* traces, void* stream);

@@ -70,6 +70,12 @@ class Storage(C.Structure):
                 ("segbuf", C.c_void_p), ("segment", C.c_int32), ("snap_kind", C.c_int32)]
 
 
+class BatchProblem(C.Structure):
+    _fields_ = [("grid", Grid), ("medium", Medium), ("acq", Acquisition), ("time", Time),
+                ("storage", Storage), ("work", C.c_void_p), ("grad_acc", C.c_void_p),
+                ("traces", C.c_void_p), ("grad_traces", C.c_void_p)]
+
+
 P = C.POINTER
 VP = C.c_void_p
 _SIGNATURES = {
@@ -95,6 +101,10 @@ _SIGNATURES = {
     "nw_adjoint_grad_c_noalloc": (C.c_int, [P(Grid), VP, P(Medium), P(Acquisition), P(Time), P(Storage),
                                             P(Tuning), VP, C.c_double, VP, VP, VP]),
     "nw_launch_count": (C.c_uint64, []),
+    "nw_batch_table_bytes": (C.c_size_t, [C.c_int32]),
+    "nw_batch_prepare": (C.c_int, [P(BatchProblem), C.c_int32, P(Tuning), VP, VP]),
+    "nw_batch_forward": (C.c_int, [P(BatchProblem), C.c_int32, P(Tuning), VP, VP]),
+    "nw_batch_adjoint": (C.c_int, [P(BatchProblem), C.c_int32, P(Tuning), VP, VP]),
 }
 EXPORTED = tuple(_SIGNATURES)
 

@@ -252,19 +252,19 @@ __device__ __forceinline__ T lap_at(const T (&wv)[2 * R + 1][VZ], const Row3<T, 
 // shots' point sources and, with lap_out, stores Lap p^n (the gradient factor).
 // ------------------------------------------------------------------------------------------
 template <typename T, int R, int VZ, int RX, bool AB>
-__global__ void __launch_bounds__(256, 4) fwd2d(KGrid<T> g, Tiled2<T> a) {
+__device__ __forceinline__ void fwd2d_body(const KGrid<T>& g, const Tiled2<T>& a, int bx, int by, int bz,
+                                           unsigned char* smem_raw) {
   using S = Tile2Shape<T, VZ, RX, R>;
   constexpr int NS = S::NS;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   T* scc = reinterpret_cast<T*>(smem_raw);  // [QS] C
   T* sa = scc + S::QS;                      // [QS] A (layer tiles)
   T* sbb = sa + S::QS;                      // [QS] B (layer tiles)
   T* sp = sbb + S::QS;                      // [NS][PS] p^n with halo
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int z0 = blockIdx.x * S::TZ, x0 = blockIdx.y * S::TX;
-  const int tile = blockIdx.y * a.tt.tiles_z + blockIdx.x;
-  const int sb = blockIdx.z * a.shots_per_cta;
+  const int z0 = bx * S::TZ, x0 = by * S::TX;
+  const int tile = by * a.tt.tiles_z + bx;
+  const int sb = bz * a.shots_per_cta;
   const int se = min(sb + a.shots_per_cta, a.n_shots);
   const int zc = z0 + lane * VZ;  // first owned column
   const int xr = x0 + warp * RX;  // first owned row
@@ -402,10 +402,10 @@ __global__ void __launch_bounds__(256, 4) fwd2d(KGrid<T> g, Tiled2<T> a) {
 // the group's accumulator (one writer per cell and group).
 // ------------------------------------------------------------------------------------------
 template <typename T, int R, int VZ, int RX, bool AB>
-__global__ void __launch_bounds__(256, 3) adj2d(KGrid<T> g, Tiled2<T> a) {
+__device__ __forceinline__ void adj2d_body(const KGrid<T>& g, const Tiled2<T>& a, int bx, int by, int bz,
+                                           unsigned char* smem_raw) {
   using S = Tile2Shape<T, VZ, RX, R>;
   constexpr int NS = S::NSA;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   T* scc = reinterpret_cast<T*>(smem_raw);  // [QS] C
   T* sa = scc + S::QS;                      // [QS] A (layer tiles)
   T* sbb = sa + S::QS;                      // [QS] B (layer tiles)
@@ -416,9 +416,9 @@ __global__ void __launch_bounds__(256, 3) adj2d(KGrid<T> g, Tiled2<T> a) {
   T* sj = sl + NS * S::QS;                  // [QS] cotangent injected at this shot's cells
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int z0 = blockIdx.x * S::TZ, x0 = blockIdx.y * S::TX;
-  const int tile = blockIdx.y * a.tt.tiles_z + blockIdx.x;
-  const int sb = blockIdx.z * a.shots_per_cta;
+  const int z0 = bx * S::TZ, x0 = by * S::TX;
+  const int tile = by * a.tt.tiles_z + bx;
+  const int sb = bz * a.shots_per_cta;
   const int se = min(sb + a.shots_per_cta, a.n_shots);
   const int zc = z0 + lane * VZ;  // first owned column
   const int xr = x0 + warp * RX;  // first owned row
@@ -437,7 +437,7 @@ __global__ void __launch_bounds__(256, 3) adj2d(KGrid<T> g, Tiled2<T> a) {
     issue(pc, a.A, sa);
     issue(pc, a.B, sbb);
   }
-  if (grad) issue(pc, a.gacc + (long long)blockIdx.z * g.field, sg);
+  if (grad) issue(pc, a.gacc + (long long)bz * g.field, sg);
 #pragma unroll
   for (int i = 0; i < NS - 1; ++i) {  // one commit group per shot, empty groups included, so that
     if (sb + i < se) {                // wait_group<NS-1> in the loop means "shot s has landed"
@@ -574,7 +574,7 @@ __global__ void __launch_bounds__(256, 3) adj2d(KGrid<T> g, Tiled2<T> a) {
     }
   }
   if (grad && own_cols) {  // the accumulator tile landed with the first commit group
-    T* gp = a.gacc + (long long)blockIdx.z * g.field + cbase;
+    T* gp = a.gacc + (long long)bz * g.field + cbase;
 #pragma unroll
     for (int k = 0; k < RX; ++k) {
       if (xr + k >= g.n0) continue;
@@ -585,6 +585,117 @@ __global__ void __launch_bounds__(256, 3) adj2d(KGrid<T> g, Tiled2<T> a) {
       store_row<T, VZ>(gp + (long long)k * ld, old, zc, g.n1);
     }
   }
+}
+
+// The per-CTA launches of one problem: blockIdx = (tile along z, tile along x, shot group).
+template <typename T, int R, int VZ, int RX, bool AB>
+__global__ void __launch_bounds__(256, 4) fwd2d(KGrid<T> g, Tiled2<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  fwd2d_body<T, R, VZ, RX, AB>(g, a, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
+}
+template <typename T, int R, int VZ, int RX, bool AB>
+__global__ void __launch_bounds__(256, 3) adj2d(KGrid<T> g, Tiled2<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  adj2d_body<T, R, VZ, RX, AB>(g, a, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
+}
+
+// ------------------------------------------------------------------------------------------
+// Batched steps: one launch advances every active problem of a batch (grids of different size,
+// shot counts and step counts) by one step. All problems share the global step index n (the
+// forward runs n upwards from 0, the adjoint downwards from the largest step count, so a problem
+// with N steps takes part in forward steps n < N and adjoint steps n <= N); the host sorts the
+// problems by step count, so the active ones are a prefix of the table and the launch covers
+// cta_start[n_active] CTAs. CTA b finds its problem by binary search over cta_start, builds that
+// problem's step descriptor in shared memory and runs the same body as the one-problem kernels.
+// ------------------------------------------------------------------------------------------
+template <typename T>
+struct BatchProb {
+  KGrid<T> g;
+  Tiled2<T> fwd, adj;  // the step-independent fields of the forward and adjoint descriptors
+  T* ring;             // 3 levels of p
+  T* work;             // 3 levels of q
+  T* segbuf;           // `segment` levels of Lap p, level n % segment
+  T* traces;
+  long long level;     // elements of one level: n_shots * field
+  int n_steps, substeps, first_b_one;
+  int ftx, atx;        // tiles along x of the forward and adjoint tile shapes
+};
+
+__device__ __forceinline__ int batch_problem(const int* __restrict__ cta_start, int n_active, int b) {
+  int lo = 0, hi = n_active - 1;  // last problem whose first CTA is <= b
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (cta_start[mid] <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// store_lap != 0: a recompute step that stores Lap p^n into the segment buffer and records no
+// traces; otherwise a forward-sweep step that records traces on the problem's record steps.
+template <typename T, int R, int VZ, int RX>
+__global__ void __launch_bounds__(256, 4) fwd2d_batch(const BatchProb<T>* __restrict__ probs,
+                                                      const int* __restrict__ cta_start, int n_active, int n,
+                                                      int store_lap, int segment) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ KGrid<T> sg;
+  __shared__ Tiled2<T> st;
+  __shared__ int sidx[3];
+  if (threadIdx.x == 0) {  // the tables are written once, before any step: read before the wait
+    const int p = batch_problem(cta_start, n_active, blockIdx.x);
+    const BatchProb<T>& P = probs[p];
+    int local = blockIdx.x - cta_start[p];
+    const int tz = P.fwd.tt.tiles_z;
+    sidx[0] = local % tz;
+    local /= tz;
+    sidx[1] = local % P.ftx;
+    sidx[2] = local / P.ftx;
+    sg = P.g;
+    Tiled2<T> t = P.fwd;
+    t.prev = P.ring + (long long)(n % 3) * P.level;
+    t.cur = P.ring + (long long)((n + 1) % 3) * P.level;
+    t.next = P.ring + (long long)((n + 2) % 3) * P.level;
+    t.b_one = (n == 0 && P.first_b_one) ? 1 : 0;
+    t.n = n;
+    t.traces = (!store_lap && P.traces && t.n_rec > 0 && n % P.substeps == 0) ? P.traces : nullptr;
+    t.j = n / P.substeps;
+    t.lap_out = store_lap ? P.segbuf + (long long)(n % segment) * P.level : nullptr;
+    st = t;
+  }
+  __syncthreads();
+  fwd2d_body<T, R, VZ, RX, true>(sg, st, sidx[0], sidx[1], sidx[2], smem_raw);
+}
+
+template <typename T, int R, int VZ, int RX>
+__global__ void __launch_bounds__(256, 3) adj2d_batch(const BatchProb<T>* __restrict__ probs,
+                                                      const int* __restrict__ cta_start, int n_active, int n,
+                                                      int segment) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ KGrid<T> sg;
+  __shared__ Tiled2<T> st;
+  __shared__ int sidx[3];
+  if (threadIdx.x == 0) {
+    const int p = batch_problem(cta_start, n_active, blockIdx.x);
+    const BatchProb<T>& P = probs[p];
+    int local = blockIdx.x - cta_start[p];
+    const int tz = P.adj.tt.tiles_z;
+    sidx[0] = local % tz;
+    local /= tz;
+    sidx[1] = local % P.atx;
+    sidx[2] = local / P.atx;
+    sg = P.g;
+    Tiled2<T> t = P.adj;
+    t.cur = P.work + (long long)((n + 1) % 3) * P.level;
+    t.prev = P.work + (long long)((n + 2) % 3) * P.level;
+    t.next = P.work + (long long)(n % 3) * P.level;
+    t.apply_a = n >= 1 ? 1 : 0;
+    t.lap = n < P.n_steps ? P.segbuf + (long long)(n % segment) * P.level : nullptr;
+    if (n % P.substeps != 0) t.gtr = nullptr;  // the descriptor holds the cotangents
+    t.j = n / P.substeps;
+    st = t;
+  }
+  __syncthreads();
+  adj2d_body<T, R, VZ, RX, true>(sg, st, sidx[0], sidx[1], sidx[2], smem_raw);
 }
 
 }  // namespace nw

@@ -6,6 +6,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
+#include <vector>
 #include <atomic>
 #include <cstdio>
 #include <cstring>
@@ -856,7 +858,7 @@ int nw_status(void* stream) {
 
 // =============================================================================================
 // Allocation-free adjoint gradient: nw_adjoint + nw_reduce_grad_c with their scratch (the three
-// adjoint levels and the float64 accumulators) carved out of a fixed array in device memory
+// adjoint levels and the gradient accumulators) carved out of a fixed array in device memory
 // instead of caller buffers. The array is module-scope device storage, so every GPU that loads
 // this library holds NW_NOALLOC_SCRATCH_BYTES of it until the process exits.
 // =============================================================================================
@@ -936,3 +938,286 @@ extern "C" int nw_adjoint_grad_c_noalloc(const nw_grid* g, const int32_t* n_abs,
   return noalloc_gradient<double>(g, n_abs, m, a, t, st, tu, c, dt2, (const double*)grad_traces, grad_c,
                                   (cudaStream_t)stream);
 }
+
+// =============================================================================================
+// Batched problems (nw_batch_*): the device table is [BatchProb x n][fwd CTA offsets x (n+1)]
+// [adj CTA offsets x (n+1)]; the CTA offsets are prefix sums over the problems in table order,
+// which is non-increasing step count, so the problems taking part in step n are a prefix.
+// =============================================================================================
+namespace {
+
+struct BatchLayout {
+  size_t fcta, acta, bytes;
+};
+BatchLayout batch_layout(int n) {
+  BatchLayout L;
+  const size_t probs = ((sizeof(nw::BatchProb<double>) * (size_t)n + 255) / 256) * 256;
+  L.fcta = probs;
+  L.acta = L.fcta + ((sizeof(int) * (size_t)(n + 1) + 255) / 256) * 256;
+  L.bytes = L.acta + ((sizeof(int) * (size_t)(n + 1) + 255) / 256) * 256;
+  return L;
+}
+
+int check_batch(const nw_batch_problem* P, int n, const Tune& tu) {
+  if (!P || n < 1) return fail(NW_ERR_ARG, "empty batch");
+  for (int p = 0; p < n; ++p) {
+    const nw_batch_problem& q = P[p];
+    int rc = check_run(&q.grid, &q.medium, &q.acq, &q.time, &q.storage, tu);
+    if (rc) return fail(rc, "batch problem " + std::to_string(p) + ": " + g_err);
+    if (q.grid.ndim != 2) return fail(NW_ERR_UNSUPPORTED, "batched problems are 2-D");
+    if (q.grid.dtype != P[0].grid.dtype || q.grid.order != P[0].grid.order)
+      return fail(NW_ERR_ARG, "batched problems share one dtype and stencil order");
+    if (!q.acq.has_source) return fail(NW_ERR_UNSUPPORTED, "batched problems are FWI problems (with sources)");
+    if (!q.storage.ring || !q.storage.snap || !q.storage.segbuf || q.storage.history)
+      return fail(NW_ERR_ARG, "batched problems use checkpointed storage (ring, snapshots, segment buffer)");
+    if (q.storage.segment != P[0].storage.segment || q.storage.snap_kind != P[0].storage.snap_kind ||
+        q.storage.segment < 1)
+      return fail(NW_ERR_ARG, "batched problems share one segment length >= 1 and snapshot kind");
+    if (p > 0 && q.time.n_steps > P[p - 1].time.n_steps)
+      return fail(NW_ERR_ARG, "batched problems must be ordered by non-increasing n_steps");
+    if (!q.work || !q.grad_acc || !q.traces || (q.acq.n_cells > 0 && !q.grad_traces))
+      return fail(NW_ERR_ARG, "batch problem " + std::to_string(p) + " lacks a work, accumulator or trace buffer");
+  }
+  return NW_OK;
+}
+
+template <typename T>
+int batch_prepare_impl(const nw_batch_problem* P, int n, const Tune& tu, void* table, cudaStream_t s) {
+  const BatchLayout L = batch_layout(n);
+  std::vector<char> host(L.bytes, 0);
+  auto* probs = reinterpret_cast<nw::BatchProb<T>*>(host.data());
+  int* fcta = reinterpret_cast<int*>(host.data() + L.fcta);
+  int* acta = reinterpret_cast<int*>(host.data() + L.acta);
+  long long fsum = 0, asum = 0;
+  for (int p = 0; p < n; ++p) {
+    const nw_batch_problem& q = P[p];
+    const nw_grid* g = &q.grid;
+    const nw_acquisition* a = &q.acq;
+    nw::BatchProb<T>& B = probs[p];
+    B.g = kgrid<T>(g);
+    nw::Tiled2<T> f = {};
+    f.C = (const T*)q.medium.c2dt2;
+    f.A = (const T*)q.medium.coef_a;
+    f.B = (const T*)q.medium.coef_b;
+    f.n_shots = a->n_shots;
+    f.src_corner = a->src_corner;
+    f.src_w = (const T*)a->src_weight;
+    f.wavelet = (const T*)a->wavelet;
+    f.rec_w = (const T*)a->rec_weight;
+    f.gcell_w = (const T*)a->cell_weight;
+    f.n_rec = a->n_rec;
+    f.n_t = q.time.n_t;
+    nw::Tiled2<T> b = f;
+    f.shots_per_cta = tu.fwd.spc;
+    f.tt = tile_tables(g, a, tu.fwd);
+    b.shots_per_cta = tu.adj.spc;
+    b.tt = tile_tables(g, a, tu.adj);
+    b.gtr = a->n_cells > 0 ? (const T*)q.grad_traces : nullptr;
+    b.gacc = (T*)q.grad_acc;
+    B.fwd = f;
+    B.adj = b;
+    B.ring = (T*)q.storage.ring;
+    B.work = (T*)q.work;
+    B.segbuf = (T*)q.storage.segbuf;
+    B.traces = (T*)q.traces;
+    B.level = (long long)a->n_shots * g->field_elems;
+    B.n_steps = q.time.n_steps;
+    B.substeps = q.time.substeps;
+    B.first_b_one = q.time.first_b_one;
+    const dim3 fg = tu.fwd.grid(g, a->n_shots), ag = tu.adj.grid(g, a->n_shots);
+    B.ftx = (int)fg.y;
+    B.atx = (int)ag.y;
+    fcta[p] = (int)fsum;
+    acta[p] = (int)asum;
+    fsum += (long long)fg.x * fg.y * fg.z;
+    asum += (long long)ag.x * ag.y * ag.z;
+    if (fsum > INT32_MAX || asum > INT32_MAX) return fail(NW_ERR_ARG, "batch too large for one launch");
+  }
+  fcta[n] = (int)fsum;
+  acta[n] = (int)asum;
+  NW_CUDA(cudaMemcpyAsync(table, host.data(), L.bytes, cudaMemcpyHostToDevice, s));
+  NW_CUDA(cudaStreamSynchronize(s));  // the host staging copy dies with this call
+  return NW_OK;
+}
+
+// Problems taking part in step n: forward (n_steps > n) or adjoint (n_steps >= n).
+int batch_active(const nw_batch_problem* P, int n, int step, bool adjoint) {
+  int k = 0;
+  while (k < n && (adjoint ? P[k].time.n_steps >= step : P[k].time.n_steps > step)) ++k;
+  return k;
+}
+
+template <typename T, int R, int VZ, int RX>
+int launch_fwd_batch(const void* table, int n, int n_active, int n_ctas, int step, int store_lap, int segment,
+                     cudaStream_t s) {
+  const BatchLayout L = batch_layout(n);
+  const char* base = (const char*)table;
+  constexpr size_t smem = step2_smem<T, R, VZ, RX, false>();
+  if (smem > kMaxSmem) return fail(NW_ERR_ARG, "tile too large for shared memory (lower tuning rx or vz)");
+  static bool done = false;
+  int rc = allow_smem(nw::fwd2d_batch<T, R, VZ, RX>, smem, &done);
+  if (rc) return rc;
+  return launch_pdl(nw::fwd2d_batch<T, R, VZ, RX>, dim3(n_ctas, 1, 1), smem, s, (const nw::BatchProb<T>*)base,
+                    (const int*)(base + L.fcta), n_active, step, store_lap, segment);
+}
+template <typename T, int R, int VZ, int RX>
+int launch_adj_batch(const void* table, int n, int n_active, int n_ctas, int step, int store_lap, int segment,
+                     cudaStream_t s) {
+  const BatchLayout L = batch_layout(n);
+  const char* base = (const char*)table;
+  (void)store_lap;
+  constexpr size_t smem = step2_smem<T, R, VZ, RX, true>();
+  if (smem > kMaxSmem) return fail(NW_ERR_ARG, "tile too large for shared memory (lower tuning adj_rx or adj_vz)");
+  static bool done = false;
+  int rc = allow_smem(nw::adj2d_batch<T, R, VZ, RX>, smem, &done);
+  if (rc) return rc;
+  return launch_pdl(nw::adj2d_batch<T, R, VZ, RX>, dim3(n_ctas, 1, 1), smem, s, (const nw::BatchProb<T>*)base,
+                    (const int*)(base + L.acta), n_active, step, segment);
+}
+
+// (radius, vz, rx) -> batched kernel instantiation; batches take rx 2 or 4.
+#define NW_DISPATCH_BATCH(FN, T, TU, R_, ...)                                                      \
+  [&]() -> int {                                                                                  \
+    if (TU.rx != 2 && TU.rx != 4) return fail(NW_ERR_UNSUPPORTED, "batched steps take rx 2 or 4"); \
+    if constexpr (sizeof(T) == 4) {                                                               \
+      if (TU.vz == 4) {                                                                           \
+        if (R_ == 2) return TU.rx == 2 ? FN<T, 2, 4, 2>(__VA_ARGS__) : FN<T, 2, 4, 4>(__VA_ARGS__); \
+        return TU.rx == 2 ? FN<T, 1, 4, 2>(__VA_ARGS__) : FN<T, 1, 4, 4>(__VA_ARGS__);            \
+      }                                                                                           \
+    }                                                                                             \
+    if (R_ == 2) return TU.rx == 2 ? FN<T, 2, 2, 2>(__VA_ARGS__) : FN<T, 2, 2, 4>(__VA_ARGS__);   \
+    return TU.rx == 2 ? FN<T, 1, 2, 2>(__VA_ARGS__) : FN<T, 1, 2, 4>(__VA_ARGS__);                \
+  }()
+
+// Host copy of the CTA offsets: cta[p] = CTAs of the problems before p.
+std::vector<int> batch_ctas(const nw_batch_problem* P, int n, const TileCfg& c) {
+  std::vector<int> cta(n + 1, 0);
+  for (int p = 0; p < n; ++p) {
+    const dim3 gr = c.grid(&P[p].grid, P[p].acq.n_shots);
+    cta[p + 1] = cta[p] + (int)(gr.x * gr.y * gr.z);
+  }
+  return cta;
+}
+
+template <typename T>
+T* ring_level(const nw_batch_problem& q, int level) {  // pressure level `level` (>= -1) in the ring
+  return (T*)q.storage.ring + (long long)((level + 1) % 3) * q.acq.n_shots * q.grid.field_elems;
+}
+
+template <typename T>
+int batch_forward_impl(const nw_batch_problem* P, int n, const Tune& tu, const void* table, cudaStream_t s) {
+  const int K = P[0].storage.segment, Nmax = P[0].time.n_steps, R = P[0].grid.radius;
+  const std::vector<int> cta = batch_ctas(P, n, tu.fwd);
+  for (int p = 0; p < n; ++p)  // p^-1 = p^0 = 0 (FWI)
+    NW_CUDA(cudaMemsetAsync(P[p].storage.ring, 0, 3 * (size_t)P[p].acq.n_shots * P[p].grid.field_elems * sizeof(T), s));
+  for (int k = 0; k < Nmax; ++k) {
+    const int na = batch_active(P, n, k, false);
+    if (k % K == 0)
+      for (int p = 0; p < na; ++p) {
+        int rc = snap_store<T>(&P[p].grid, &P[p].storage, P[p].acq.n_shots, ring_level<T>(P[p], k - 1),
+                               ring_level<T>(P[p], k), k / K, s);
+        if (rc) return rc;
+      }
+    int rc = NW_DISPATCH_BATCH(launch_fwd_batch, T, tu.fwd, R, table, n, na, cta[na], k, 0, K, s);
+    if (rc) return rc;
+    for (int p = 0; p < na; ++p) {  // the final receiver sample of problems ending after step k
+      const nw_batch_problem& q = P[p];
+      if (q.time.n_steps == k + 1 && q.time.n_steps % q.time.substeps == 0) {
+        rc = launch_sample<T>(&q.grid, &q.acq, q.time.n_t, ring_level<T>(q, k + 1), (k + 1) / q.time.substeps,
+                              (T*)q.traces, s);
+        if (rc) return rc;
+      }
+    }
+  }
+  return NW_OK;
+}
+
+template <typename T>
+int batch_adjoint_impl(const nw_batch_problem* P, int n, const Tune& tu, const void* table, cudaStream_t s) {
+  const int K = P[0].storage.segment, Nmax = P[0].time.n_steps, R = P[0].grid.radius;
+  const std::vector<int> fcta = batch_ctas(P, n, tu.fwd), acta = batch_ctas(P, n, tu.adj);
+  for (int p = 0; p < n; ++p) {
+    const nw_batch_problem& q = P[p];
+    const size_t lvl = (size_t)q.acq.n_shots * q.grid.field_elems * sizeof(T);
+    NW_CUDA(cudaMemsetAsync(q.work, 0, 3 * lvl, s));
+    NW_CUDA(cudaMemsetAsync(q.grad_acc, 0, (size_t)n_acc_fields(&q.grid, tu, q.acq.n_shots) * q.grid.field_elems * sizeof(T), s));
+  }
+  auto adj_step = [&](int step) -> int {
+    const int na = batch_active(P, n, step, true);
+    return NW_DISPATCH_BATCH(launch_adj_batch, T, tu.adj, R, table, n, na, acta[na], step, 0, K, s);
+  };
+  int rc = adj_step(Nmax);  // problems with the largest step count start: q^N = A C R^T g_N
+  if (rc) return rc;
+  for (int seg = Nmax > 0 ? (Nmax - 1) / K : -1; seg >= 0; --seg) {
+    const int n0 = seg * K, n1 = std::min(n0 + K, Nmax);
+    const int na0 = batch_active(P, n, n0, false);
+    for (int p = 0; p < na0; ++p) {  // decode the segment's snapshots into the rings
+      rc = snap_load<T>(&P[p].grid, &P[p].storage, P[p].acq.n_shots, seg, ring_level<T>(P[p], n0 - 1),
+                        ring_level<T>(P[p], n0), s);
+      if (rc) return rc;
+    }
+    for (int k = n0; k < n1; ++k) {  // recompute Lap p^k into the segment buffers
+      const int na = batch_active(P, n, k, false);
+      rc = NW_DISPATCH_BATCH(launch_fwd_batch, T, tu.fwd, R, table, n, na, fcta[na], k, 1, K, s);
+      if (rc) return rc;
+    }
+    for (int step = n1 - 1; step >= n0; --step) {
+      rc = adj_step(step);
+      if (rc) return rc;
+    }
+  }
+  return NW_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t nw_batch_table_bytes(int32_t n_problems) { return n_problems < 1 ? 0 : batch_layout(n_problems).bytes; }
+
+int nw_batch_prepare(const nw_batch_problem* problems, int32_t n_problems, const nw_tuning* tune, void* table,
+                     void* stream) {
+  if (!problems || n_problems < 1 || !table) return fail(NW_ERR_ARG, "invalid batch arguments");
+  Tune tu;
+  int rc = check_grid(&problems[0].grid);
+  if (rc) return rc;
+  rc = resolve_tune(&problems[0].grid, tune, &tu);
+  if (rc) return rc;
+  rc = check_batch(problems, n_problems, tu);
+  if (rc) return rc;
+  if (problems[0].grid.dtype == NW_F32)
+    return batch_prepare_impl<float>(problems, n_problems, tu, table, (cudaStream_t)stream);
+  return batch_prepare_impl<double>(problems, n_problems, tu, table, (cudaStream_t)stream);
+}
+
+int nw_batch_forward(const nw_batch_problem* problems, int32_t n_problems, const nw_tuning* tune,
+                     const void* table, void* stream) {
+  if (!problems || n_problems < 1 || !table) return fail(NW_ERR_ARG, "invalid batch arguments");
+  Tune tu;
+  int rc = check_grid(&problems[0].grid);
+  if (rc) return rc;
+  rc = resolve_tune(&problems[0].grid, tune, &tu);
+  if (rc) return rc;
+  rc = check_batch(problems, n_problems, tu);
+  if (rc) return rc;
+  if (problems[0].grid.dtype == NW_F32)
+    return batch_forward_impl<float>(problems, n_problems, tu, table, (cudaStream_t)stream);
+  return batch_forward_impl<double>(problems, n_problems, tu, table, (cudaStream_t)stream);
+}
+
+int nw_batch_adjoint(const nw_batch_problem* problems, int32_t n_problems, const nw_tuning* tune,
+                     const void* table, void* stream) {
+  if (!problems || n_problems < 1 || !table) return fail(NW_ERR_ARG, "invalid batch arguments");
+  Tune tu;
+  int rc = check_grid(&problems[0].grid);
+  if (rc) return rc;
+  rc = resolve_tune(&problems[0].grid, tune, &tu);
+  if (rc) return rc;
+  rc = check_batch(problems, n_problems, tu);
+  if (rc) return rc;
+  if (problems[0].grid.dtype == NW_F32)
+    return batch_adjoint_impl<float>(problems, n_problems, tu, table, (cudaStream_t)stream);
+  return batch_adjoint_impl<double>(problems, n_problems, tu, table, (cudaStream_t)stream);
+}
+
+}  // extern "C"
