@@ -6,7 +6,8 @@ together, one kernel launch per time step for all problems still running (the pr
 by step count, so those are a prefix of the batch table). Storage is checkpointed with one segment
 length for the batch (16-bit snapshots by default); the adjoint recomputes each segment for all
 problems at once. ``BatchedFWI.capture()`` records the whole gradient (forward sweep, misfit,
-adjoint sweep, float64 reductions) as one CUDA graph that ``run()`` replays; ``autotune()`` picks
+adjoint sweep, float64 reductions) as one CUDA graph that ``misfit_gradients`` then replays;
+``autotune()`` picks
 the tile shapes of the forward and adjoint steps by timing candidates on a shortened batch.
 
 Each problem's traces and gradient equal what ``WaveOperatorB200.misfit_gradient`` gives it alone
@@ -63,8 +64,8 @@ class BatchedFWI:
         for slot, i in enumerate(self.order):
             op = self.ops[i]
             op.tuning = self.tuning
-            op._plans.pop((str(dev), self.dtype), None)
             plan = op._plan(dev, self.dtype)
+            plan.set_tuning(*self.tuning)
             S = op.n_sources
             b = {"plan": plan, "S": S}
             b["ring"] = plan.empty_levels(3, S)
@@ -167,8 +168,11 @@ class BatchedFWI:
         self._step()
         torch.cuda.synchronize(self.device)
         g = torch.cuda.CUDAGraph()
+        lib = _lib.load()
+        n0 = lib.nw_launch_count()
         with torch.cuda.graph(g):
             self._step()
+        self.graph_launches = int(lib.nw_launch_count() - n0)  # this library's kernels per replay
         self._graph = g
         torch.cuda.synchronize(self.device)
 
