@@ -42,12 +42,13 @@ def peaks() -> tuple[float, str]:
     return 6650.0, "fallback"
 
 
-def workload_desc(w) -> dict:
+def workload_desc(w, storage: str = "full history in HBM") -> dict:
     P = w.n + 2 * w.absorb_cells
-    return {"workload": f"{w.name}: {w.n}x{w.n} FP32 grid h={w.h:g} m, seeded layered model "
-                        f"(6-10 layers 1500-4500 m/s + 4 anomalies), {len(w.sources)} Ricker shots "
+    model = ("seeded layered model (6-10 layers 1500-4500 m/s + 4 anomalies) + salt body (4500 m/s)"
+             if w.name == "fwi_2048" else "seeded layered model (6-10 layers 1500-4500 m/s + 4 anomalies)")
+    return {"workload": f"{w.name}: {w.n}x{w.n} FP32 grid h={w.h:g} m, {model}, {len(w.sources)} Ricker shots "
                         f"{w.f0:g} Hz, {len(w.receivers)} receivers, {w.n_steps} steps, Courant "
-                        f"{w.courant_number}, order {w.order}, {w.absorb_cells}-cell sponge, full history in HBM",
+                        f"{w.courant_number}, order {w.order}, {w.absorb_cells}-cell sponge, {storage}",
             "grid_padded": [P, P], "shots_per_gpu": len(w.sources), "n_steps": w.n_steps,
             "l2": "256 MiB buffer written between timed steps; working set (history) far above L2"}
 
@@ -102,6 +103,7 @@ def cpu_sample(w, n_shots=CPU_SAMPLE_SHOTS, n_steps=CPU_SAMPLE_STEPS) -> tuple[f
 
     threads = os.cpu_count() or 1
     oracle.set_threads(threads)
+    n_steps = max(20, min(n_steps, int(n_steps * 552**2 / (w.n + 2 * w.absorb_cells) ** 2)))  # ~10-30 s of CPU
     kw = w.operator_kwargs()
     kw["n_t"] = n_steps + 1
     L = w.n * w.h
@@ -272,6 +274,12 @@ def main() -> None:
     ap.add_argument("--n-steps", type=int, default=None, help="override the leapfrog steps (profiling cases)")
     ap.add_argument("--shots", type=int, default=None, help="override the shots per GPU (profiling cases)")
     ap.add_argument("--problems", type=int, default=64, help="fwi_batch: problems in the batch")
+    ap.add_argument("--grad-mode", default="autograd", choices=("autograd", "checkpoint"),
+                    help="autograd keeps the full history when it fits, else checkpoints")
+    ap.add_argument("--snapshot", default="exact", choices=("exact", "fixed16", "fp16", "bf16"))
+    ap.add_argument("--checkpoint-every", type=int, default=None)
+    ap.add_argument("--accuracy-shots", type=int, default=None,
+                    help="shots of the float64 accuracy check (all by default)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -293,7 +301,8 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
 
     w = make_workload(args)
-    op = WaveOperatorB200(w.domain, w.sources, w.receivers, grad_mode="autograd", **w.operator_kwargs())
+    op = WaveOperatorB200(w.domain, w.sources, w.receivers, grad_mode=args.grad_mode, snapshot=args.snapshot,
+                          checkpoint_every=args.checkpoint_every, **w.operator_kwargs())
     c = torch.tensor(w.c, dtype=torch.float32, device=dev)
     # observed data: traces of a smoothed model (the misfit of a typical early FWI iteration)
     with torch.no_grad():
@@ -396,13 +405,26 @@ def main() -> None:
     h2d = c_h.numel() * c_h.element_size() + d_h.numel() * d_h.element_size()
     d2h = g_h.numel() * 8 + 8
 
+    from nefi_b200.plan import plan_storage
+
+    mode = plan_storage(op._plan(dev, torch.float32), len(w.sources), op.n_steps, op.grad_mode,
+                        op.checkpoint_every, op.snapshot, op._budget(dev))
+    storage = ("full history in HBM" if mode[0] == "history" else
+               f"checkpointed every {mode[1]} steps with {args.snapshot} snapshots")
     accuracy = None
     if not args.no_accuracy and rank == 0:
-        # float32 gradient against a float64 device run of the same step (checkpointed, exact snapshots)
-        _, g32 = op.misfit_gradient(c, d)
-        op64 = WaveOperatorB200(w.domain, w.sources, w.receivers, grad_mode="checkpoint", **w.operator_kwargs())
-        _, g64 = op64.misfit_gradient(c.double(), d.double())
-        accuracy = {"grad_rel_l2_fp32_vs_fp64": float((g32 - g64).norm() / g64.norm())}
+        # float32 gradient against a float64 device run of the same step (checkpointed, exact
+        # snapshots), over the first --accuracy-shots shots (all by default)
+        na = args.accuracy_shots or len(w.sources)
+        kw = w.operator_kwargs()
+        op32 = WaveOperatorB200(w.domain, w.sources[:na], w.receivers, grad_mode=args.grad_mode,
+                                snapshot=args.snapshot, checkpoint_every=args.checkpoint_every, **kw)
+        _, g32 = op32.misfit_gradient(c, d[:na])
+        del op32
+        op64 = WaveOperatorB200(w.domain, w.sources[:na], w.receivers, grad_mode="checkpoint", **kw)
+        _, g64 = op64.misfit_gradient(c.double(), d[:na].double())
+        accuracy = {"grad_rel_l2_fp32_vs_fp64": float((g32 - g64).norm() / g64.norm()), "shots": na,
+                    "fp32_storage": f"{args.grad_mode}, {args.snapshot} snapshots"}
         del op64
 
     cpu = None
@@ -416,7 +438,7 @@ def main() -> None:
                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "f32",
                "data": "synthetic (seeded layered model; observed data from a smoothed model)",
-               "config": {**workload_desc(w), "method": "plain (per-step launches, full history)",
+               "config": {**workload_desc(w, storage), "method": f"plain (per-step launches, {storage})",
                           "parallelism": f"shots sharded over {world} GPU(s), fp64 gradient all-reduce"},
                "gcell_updates_per_s": gcells, "roofline": roofline, "cpu_baseline": cpu,
                "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
