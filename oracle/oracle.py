@@ -8,7 +8,9 @@ padded grid and layer depth (nefi/physics/wave.py:204-270), sponge and Cerjan co
 (nefi/physics/wave.py:431-475), CFL time axis (nefi/physics/timestep.py:177-207,
 nefi/physics/wave.py:394-397), multilinear stencils and the source density
 (nefi/physics/wave.py:272-318), the Ricker wavelet (nefi/physics/wave.py:101-111), replicate / zero
-padding and its adjoint (nefi/physics/wave.py:222-246), the photoacoustic start
+padding and its adjoint (nefi/physics/wave.py:222-246), the 2-D PML of ``_static`` and ``_step_fn``
+(nefi/physics/wave.py:449-456, 476-501, 529-552; restated in numpy, with its adjoint derived by
+hand: see ``_run_pml``), the photoacoustic start
 ``p^-1 = p0 + 1/2 c^2 dt^2 Lap p0`` (nefi/physics/wave.py:849-850) and the chain rule of
 ``c2dt2 = pad(c)^2 dt^2`` (nefi/physics/wave.py:718).
 """
@@ -93,8 +95,8 @@ class OracleWave:
     def __init__(self, shape, extent, receivers, *, n_t, dt_obs, c_max, order=4, absorbing="sponge",
                  absorb_width=None, absorb_R=1e-3, cerjan_gamma=0.3, courant=0.9, sources=None,
                  f0=None, t0=None, amplitude=1.0):
-        if absorbing == "pml":
-            raise ValueError("the oracle restates sponge, cerjan and none layers")
+        if absorbing == "pml" and len(shape) != 2:
+            raise ValueError("the PML is 1-D/2-D only (nefi/physics/wave.py:371-372)")
         self.shape = tuple(int(s) for s in shape)
         self.d = len(self.shape)
         self.extent = tuple((float(a), float(b)) for a, b in extent)
@@ -148,10 +150,39 @@ class OracleWave:
         s[ax] = -1
         return v.reshape(s)
 
+    def _face_depth(self, ax):
+        a, n = self.a[ax], self.shape[ax]
+        pos = np.arange(n + 2 * a + 1, dtype=np.float64)
+        if a == 0:
+            return np.zeros_like(pos)
+        return np.clip(np.maximum(a - pos, pos - (a + n)), 0.0, None) / a
+
     def _coefs(self):
         self.A = self.B = None
         self.first_b_one = 0
+        self.pml = None
         if not any(self.a) or self.absorbing == "none":
+            return
+        if self.absorbing == "pml":
+            # zeta = 1.5 c_max ln(1/R) / (a h) xi^2 at cell centres and faces (wave.py:449-456, 476-501)
+            zc, zf = [], []
+            for ax, a in enumerate(self.a):
+                zmax = 1.5 * self.c_max * math.log(1.0 / self.R) / (a * self.h[ax]) if a else 0.0
+                zc.append(self._bcast(zmax * self._depth(ax) ** 2, ax))
+                zf.append(self._bcast(zmax * self._face_depth(ax) ** 2, ax))
+            zsum = np.broadcast_to(zc[0] + zc[1], self.P)
+            dt = self.dt
+            self.A = 1.0 / (1.0 + 0.5 * dt * zsum)
+            self.B = 1.0 - 0.5 * dt * zsum
+            pml = {"zz": np.broadcast_to(dt**2 * zc[0] * zc[1], self.P).copy(), "alpha": [], "beta": []}
+            for ax in range(2):
+                fshape = list(self.P)
+                fshape[ax] += 1
+                other = zc[1 - ax]
+                den = 1.0 + 0.5 * dt * zf[ax]
+                pml["alpha"].append(np.broadcast_to((1.0 - 0.5 * dt * zf[ax]) / den, fshape).copy())
+                pml["beta"].append(np.broadcast_to(dt * (other - zf[ax]) / (den * self.h[ax]), fshape).copy())
+            self.pml = pml
             return
         if self.absorbing == "sponge":
             sig = np.zeros(self.P)
@@ -226,6 +257,8 @@ class OracleWave:
 
     # -- runs --------------------------------------------------------------------------------
     def _run(self, C2, n_shots, init_prev, init_cur, gtr, dtype, want_initial=False):
+        if self.pml is not None:
+            return self._run_pml(C2, n_shots, init_prev, init_cur, gtr, dtype)
         L = lib()
         sfx = "_f64" if dtype == np.float64 else "_f32"
         cast = lambda a: None if a is None else np.ascontiguousarray(a, dtype=dtype)  # noqa: E731
@@ -253,6 +286,97 @@ class OracleWave:
             C.byref(self.geom), _p(C2), _p(A), _p(B), n_shots, self.rec_idx.shape[0],
             self.rec_idx.shape[1], _p(self.rec_idx), _p(rec_w), _p(hist), self.N, self.m, self.n_t,
             _p(g), _p(gC), _p(lam0), _p(mu1))
+        return traces, gC, lam0, mu1
+
+    def _run_pml(self, C2, S, init_prev, init_cur, gtr, dtype):
+        """2-D PML run in numpy (all shots at once) and, given cotangents, its exact adjoint.
+
+        Forward, step k (nefi/physics/wave.py:529-552), with face differences D+ (zero outside
+        the grid, ``_face_diff``) and cell differences D- of face arrays:
+            psi_k = alpha psi_{k-1} + beta D+ p^k                      (per axis, on faces)
+            L_k   = Lap p^k + sum_ax (0.5/h) D-(psi_k + psi_{k-1})
+            p^{k+1} = A (2 p^k - B p^{k-1} + C L_k - ZZ p^k + S w(k))
+        Adjoint (derived by hand; D+^T = -D-, D-^T = -D+), with mu^k = A lambda^k:
+            Psi_k  = alpha Psi_{k+1} - (0.5/h) D+(C mu^{k+1} + C mu^{k+2})
+            lambda^k = R^T g_k + 2 mu^{k+1} - ZZ mu^{k+1} + Lap(C mu^{k+1})
+                       - sum_ax D-(beta Psi_k) - B mu^{k+2}
+            dJ/dC = sum_k mu^{k+1} L_k
+        Returns (traces, per-shot dJ/dC, lambda^0, mu^1) like ``_run``.
+        """
+        P0, P1 = self.P
+        cast = lambda a: np.asarray(a, dtype=dtype)  # noqa: E731
+        Cf, A, B, ZZ = cast(C2).reshape(P0, P1), cast(self.A), cast(self.B), cast(self.pml["zz"])
+        al = [cast(x) for x in self.pml["alpha"]]
+        be = [cast(x) for x in self.pml["beta"]]
+        half = [dtype(0.5 / h) for h in self.h]
+        rec_idx, rec_w = self.rec_idx, cast(self.rec_w)
+        src = self.sources is not None
+
+        def lap(u):
+            return self.laplacian(u.reshape(S, -1), dtype).reshape(S, P0, P1)
+
+        def dplus(u, ax):  # cells -> faces, zero outside
+            pw = [(0, 0), (0, 0), (0, 0)]
+            pw[1 + ax] = (1, 1)
+            return np.diff(np.pad(u, pw), axis=1 + ax)
+
+        def dminus(f, ax):  # faces -> cells
+            return np.diff(f, axis=1 + ax)
+
+        pp = np.zeros((S, P0, P1), dtype) if init_prev is None else cast(init_prev).reshape(S, P0, P1).copy()
+        pc = np.zeros((S, P0, P1), dtype) if init_cur is None else cast(init_cur).reshape(S, P0, P1).copy()
+        psi = [np.zeros((S, P0 + 1, P1), dtype), np.zeros((S, P0, P1 + 1), dtype)]
+        n_rec = rec_idx.shape[0]
+        traces = np.zeros((S, n_rec, self.n_t), dtype)
+        Ls = [] if gtr is not None else None
+        for n in range(self.N + 1):
+            if n % self.m == 0:
+                flat = pc.reshape(S, -1)
+                traces[:, :, n // self.m] = (flat[:, rec_idx] * rec_w).sum(-1)
+            if n == self.N:
+                break
+            L = lap(pc)
+            new = []
+            for ax in range(2):
+                ps = al[ax] * psi[ax] + be[ax] * dplus(pc, ax)
+                L = L + dminus(ps + psi[ax], ax) * half[ax]
+                new.append(ps)
+            if Ls is not None:
+                Ls.append(L)
+            rhs = (dtype(2) * pc - B * pp) + Cf * L - ZZ * pc
+            if src:
+                flat = rhs.reshape(S, -1)
+                for s in range(S):
+                    np.add.at(flat[s], self.src_idx[s], cast(self.src_w[s]) * dtype(self.wavelet[n]))
+            pp, pc, psi = pc, A * rhs, new
+        if gtr is None:
+            return traces, None, None, None
+        g = cast(gtr)
+        z = lambda: np.zeros((S, P0, P1), dtype)  # noqa: E731
+        m1, m2 = z(), z()                          # mu^{k+1}, mu^{k+2}
+        Psi = [np.zeros((S, P0 + 1, P1), dtype), np.zeros((S, P0, P1 + 1), dtype)]  # Psi_{k+1}
+        gC = np.zeros((S, P0 * P1), dtype)
+        lam0 = mu1 = None
+        for k in range(self.N, -1, -1):
+            lam = z()
+            if k <= self.N - 1:
+                q = Cf * m1
+                s2 = q + Cf * m2
+                Psi = [al[ax] * Psi[ax] - half[ax] * dplus(s2, ax) for ax in range(2)]
+                lam = (dtype(2) * m1 - ZZ * m1) + lap(q)
+                for ax in range(2):
+                    lam = lam - dminus(be[ax] * Psi[ax], ax)
+                lam = lam - B * m2
+                gC += (m1 * Ls[k]).reshape(S, -1)
+            if k % self.m == 0:
+                flat = lam.reshape(S, -1)
+                gv = g[:, :, k // self.m]
+                for s in range(S):
+                    np.add.at(flat[s], rec_idx.reshape(-1), (rec_w * gv[s][:, None]).reshape(-1))
+            if k == 0:
+                lam0, mu1 = lam.reshape(S, -1), m1.reshape(S, -1)
+                break
+            m2, m1 = m1, A * lam
         return traces, gC, lam0, mu1
 
     def c2dt2(self, c, dtype):

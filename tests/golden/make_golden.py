@@ -2,7 +2,10 @@
 
 Run where the reference checkout is available (it is not needed anywhere else):
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py [/path/to/reference] [case-name-prefix ...]
+
+With name prefixes only the matching cases are written (every case is seeded on its own, so a
+subset reproduces the same fixtures as a full run).
 
 Every case stores its inputs, the operator arguments (JSON) and the reference's outputs in float64
 and float32: traces of ``op(fields)`` and the gradient of ``sum(traces * g)`` for a seeded
@@ -24,6 +27,7 @@ import torch
 
 HERE = Path(__file__).resolve().parent
 REF = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+ONLY = tuple(sys.argv[2:])
 sys.path.insert(0, str(REF))
 
 from nefi.domain import Domain  # noqa: E402
@@ -39,6 +43,8 @@ def cotangent(shape, seed):
 
 
 def fwi_case(name, shape, extent, sources, receivers, c, kw, seed, rec_stride=1):
+    if not wanted(name):
+        return
     dom = Domain(shape, extent)
     out = {"kind": "fwi", "shape": list(shape), "extent": [list(e) for e in extent],
            "sources": np.asarray(sources, dtype=np.float64), "receivers": np.asarray(receivers, dtype=np.float64),
@@ -57,6 +63,8 @@ def fwi_case(name, shape, extent, sources, receivers, c, kw, seed, rec_stride=1)
 
 
 def pat_case(name, shape, extent, receivers, p0, c, kw, seed):
+    if not wanted(name):
+        return
     dom = Domain(shape, extent)
     out = {"kind": "pat", "shape": list(shape), "extent": [list(e) for e in extent],
            "receivers": np.asarray(receivers, dtype=np.float64), "p0": p0.numpy(), "c": c.numpy(), "kw": kw,
@@ -91,6 +99,10 @@ def pat_case(name, shape, extent, receivers, p0, c, kw, seed):
         out["meta"] = {"substeps": op.substeps, "n_steps": op.n_steps, "dt": op.dt,
                        "padded": list(op.grid.padded_shape), "n_abs": list(op.grid.n_abs)}
     save(name, out)
+
+
+def wanted(name):
+    return not ONLY or name.startswith(ONLY)
 
 
 def save(name, out):
@@ -159,6 +171,14 @@ def main():
     sens_in[:, 2] = 0.125  # first cell centre: without a layer the sensors must sit inside the grid
     pat_case("pat3d_o4_none", (10, 9, 8), ((0.0, 2.5), (0.0, 2.25), (0.0, 2.0)), sens_in, p03[:10, :9],
              c3[:10, :9], dict(n_t=20, dt_obs=0.08, order=4, absorbing="none"), 9)
+    # 2-D PML (the reference's default layer), FWI and photoacoustic, same geometries as above
+    fwi_case("fwi_o4_pml", (20, 24), ext, src, rec, c, {**base, "order": 4, "absorbing": "pml",
+                                                         "absorb_width": 0.2}, 10)
+    fwi_case("fwi_o2_pml_aniso", (18, 30), ((0.0, 0.9), (0.0, 1.2)), [[0.45, 0.1]],
+             [[0.1 + 0.1 * i, 1.0] for i in range(7)], c2,
+             {**base, "n_t": 25, "order": 2, "absorbing": "pml", "absorb_width": 0.16, "courant": 0.8}, 11)
+    pat_case("pat2d_o4_pml", (n2, n2), ((-1.0, 1.0), (-1.0, 1.0)), ring, p0, cpat,
+             dict(n_t=50, dt_obs=0.03, order=4, absorbing="pml", absorb_width=0.25), 12)
 
 
 if __name__ == "__main__":
