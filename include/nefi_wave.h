@@ -35,8 +35,8 @@ extern "C" {
 
 /* scalar type of a computation */
 enum { NW_F32 = 0, NW_F64 = 1 };
-/* absorbing layer kind (nefi/physics/wave.py:80, 469-501) */
-enum { NW_ABS_NONE = 0, NW_ABS_SPONGE = 1, NW_ABS_CERJAN = 2 };
+/* absorbing layer kind (nefi/physics/wave.py:80, 469-501); NW_ABS_PML is 2-D only */
+enum { NW_ABS_NONE = 0, NW_ABS_SPONGE = 1, NW_ABS_CERJAN = 2, NW_ABS_PML = 3 };
 /* snapshot encodings for checkpointed gradients */
 enum { NW_SNAP_EXACT = 0, NW_SNAP_F16 = 1, NW_SNAP_BF16 = 2, NW_SNAP_I16 = 3 };
 /* status codes */
@@ -100,7 +100,7 @@ int nw_tile_shape(const nw_grid* g, nw_tuning* t, int32_t* shape);
 
 /*
  * Number of gradient accumulator fields (in the grid's dtype) nw_adjoint fills for n_shots
- * shots: one per shot in 3-D, one per group of adj_shots_per_cta shots in 2-D.
+ * shots: one per shot in 3-D and with a PML, one per group of adj_shots_per_cta shots otherwise.
  */
 int nw_adjoint_groups(const nw_grid* g, const nw_tuning* t, int32_t n_shots);
 
@@ -144,8 +144,18 @@ typedef struct nw_acquisition {
 /* The medium: c^2 dt^2 on the padded grid and the absorbing coefficients. */
 typedef struct nw_medium {
   const void* c2dt2;  /* field (ghost layout) */
-  const void* coef_a; /* field: A = 1/(1 + sigma dt/2) (sponge) or the Cerjan taper; NULL if none */
-  const void* coef_b; /* field: B = 1 - sigma dt/2 (sponge) or the Cerjan taper; NULL if none */
+  const void* coef_a; /* field: A = 1/(1 + sigma dt/2) (sponge), 1/(1 + dt/2 sum zeta) (PML) or the
+                         Cerjan taper; NULL if none */
+  const void* coef_b; /* field: B = 1 - sigma dt/2 (sponge), 1 - dt/2 sum zeta (PML) or the Cerjan
+                         taper; NULL if none */
+  /* PML only (nefi/physics/wave.py:476-501), NULL otherwise: ZZ = dt^2 zeta_x zeta_z on cells, and
+     per axis the face coefficients alpha = (1 - dt/2 zeta_f)/(1 + dt/2 zeta_f) and
+     beta = dt (zeta_other - zeta_f)/((1 + dt/2 zeta_f) h), face f of an axis stored at the cell
+     index f (face P_ax in the first ghost row / column) */
+  const void* pml_zz;
+  const void* pml_alpha[2];
+  const void* pml_beta[2];
+  double pml_half_inv_h[2];  /* 0.5 / h per axis: the factor of the psi divergence */
 } nw_medium;
 
 /* Time axis: n_steps = (n_t - 1) * substeps; trace sample j is the state after j*substeps steps. */
@@ -180,6 +190,9 @@ typedef struct nw_storage {
   void* segbuf;        /* `segment` levels of Lap p^n, used when snap != NULL */
   int32_t segment;     /* steps per checkpoint segment */
   int32_t snap_kind;   /* NW_SNAP_* */
+  void* pml_psi;       /* PML only: 4 levels (axis x {even, odd step}), each n_shots fields, zero
+                          before step 0: the auxiliary face fields psi. PML runs keep a history
+                          (checkpointed PML storage is not built) */
 } nw_storage;
 
 /* Bytes of one snapshot pool for `n_snap` snapshots of n_shots shots (both levels). */
@@ -222,7 +235,8 @@ int nw_forward(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, co
  *  - lambda0 / mu1 (n_shots fields each, may be NULL): the sensitivities of p^0 and A*p^1
  *    needed by the initial-value operator.
  * The steps advance q = c2dt2 * mu, which obeys the forward recursion with the source replaced
- * by c2dt2 * R^T g_n; `work` holds three q levels (3 * n_shots fields). Uses the history or
+ * by c2dt2 * R^T g_n; `work` holds three q levels (3 * n_shots fields; 7 * n_shots with a PML, whose
+ * adjoint also carries the face cotangents of psi, 2 axes x 2 levels). Uses the history or
  * recomputes segments from the snapshots in `st`. This is the discrete adjoint torch.autograd
  * derives from nefi/physics/wave.py:529-552 and nefi/physics/timestep.py:151-169.
  */

@@ -16,7 +16,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libnefiwave.so"
 ABI_VERSION = 3
 
 NW_F32, NW_F64 = 0, 1
-NW_ABS_NONE, NW_ABS_SPONGE, NW_ABS_CERJAN = 0, 1, 2
+NW_ABS_NONE, NW_ABS_SPONGE, NW_ABS_CERJAN, NW_ABS_PML = 0, 1, 2, 3
 NW_SNAP_EXACT, NW_SNAP_F16, NW_SNAP_BF16 = 0, 1, 2
 NW_OK, NW_ERR_ARG, NW_ERR_CUDA, NW_ERR_UNSUPPORTED, NW_ERR_NONFINITE, NW_ERR_TIMEOUT = range(6)
 NW_SNAP_BLOCK = 32
@@ -57,7 +57,9 @@ class Acquisition(C.Structure):
 
 
 class Medium(C.Structure):
-    _fields_ = [("c2dt2", C.c_void_p), ("coef_a", C.c_void_p), ("coef_b", C.c_void_p)]
+    _fields_ = [("c2dt2", C.c_void_p), ("coef_a", C.c_void_p), ("coef_b", C.c_void_p),
+                ("pml_zz", C.c_void_p), ("pml_alpha", C.c_void_p * 2), ("pml_beta", C.c_void_p * 2),
+                ("pml_half_inv_h", C.c_double * 2)]
 
 
 class Time(C.Structure):
@@ -67,7 +69,8 @@ class Time(C.Structure):
 
 class Storage(C.Structure):
     _fields_ = [("history", C.c_void_p), ("ring", C.c_void_p), ("snap", C.c_void_p),
-                ("segbuf", C.c_void_p), ("segment", C.c_int32), ("snap_kind", C.c_int32)]
+                ("segbuf", C.c_void_p), ("segment", C.c_int32), ("snap_kind", C.c_int32),
+                ("pml_psi", C.c_void_p)]
 
 
 class BatchProblem(C.Structure):

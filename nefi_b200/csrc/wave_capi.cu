@@ -17,6 +17,7 @@
 #include "../../include/nefi_wave.h"
 #include "aux_kernels.cuh"
 #include "kernels.cuh"
+#include "pml2d.cuh"
 #include "stencil2d.cuh"
 
 namespace {
@@ -51,8 +52,9 @@ int check_grid(const nw_grid* g) {
   if (g->ndim != 2 && g->ndim != 3) return fail(NW_ERR_UNSUPPORTED, "ndim must be 2 or 3");
   if (g->order != 2 && g->order != 4) return fail(NW_ERR_ARG, "order must be 2 or 4");
   if (g->dtype != NW_F32 && g->dtype != NW_F64) return fail(NW_ERR_ARG, "dtype must be NW_F32 or NW_F64");
-  if (g->absorbing < NW_ABS_NONE || g->absorbing > NW_ABS_CERJAN)
+  if (g->absorbing < NW_ABS_NONE || g->absorbing > NW_ABS_PML)
     return fail(NW_ERR_UNSUPPORTED, "absorbing kind not built");
+  if (g->absorbing == NW_ABS_PML && g->ndim != 2) return fail(NW_ERR_UNSUPPORTED, "the PML is 2-D only");
   for (int a = 0; a < g->ndim; ++a)
     if (g->n[a] < 2) return fail(NW_ERR_ARG, "every padded extent must be >= 2");
   if (g->field_elems >= (1LL << 31)) return fail(NW_ERR_ARG, "a field must hold fewer than 2^31 elements");
@@ -243,10 +245,13 @@ int resolve_tune(const nw_grid* g, const nw_tuning* t, Tune* out) {
   return NW_OK;
 }
 
-// Accumulator fields the adjoint fills: one per shot in 3-D, one per adjoint shot group in 2-D.
+// Accumulator fields the adjoint fills: one per shot in 3-D and with a PML, one per adjoint shot
+// group for the tiled 2-D steps.
 int n_acc_fields(const nw_grid* g, const Tune& t, int n_shots) {
-  return g->ndim == 3 ? n_shots : t.adj.groups(n_shots);
+  return (g->ndim == 3 || g->absorbing == NW_ABS_PML) ? n_shots : t.adj.groups(n_shots);
 }
+// Levels of nw_adjoint's work buffer: q^{n..n+2}, and with a PML the face cotangents.
+int work_levels(const nw_grid* g) { return g->absorbing == NW_ABS_PML ? 7 : 3; }
 
 // Dynamic shared memory: fwd2d stages C, A, B and the ring of p^n halo tiles; adj2d stages C, A, B, the
 // accumulator tile, the ring of (q^{n+1} halo, q^{n+2} core, Lap p^n core) tiles and one shot's
@@ -363,6 +368,31 @@ int launch_step3(const nw_grid* g, const nw::KGrid<T>& kg, const nw::Step3<T>& s
   }()
 
 // ---- forward driver ---------------------------------------------------------------------
+// The PML coefficients of a medium into a step descriptor.
+template <typename T>
+void pml_medium(const nw_medium* m, nw::PmlStep<T>& st) {
+  st.C = (const T*)m->c2dt2;
+  st.A = (const T*)m->coef_a;
+  st.B = (const T*)m->coef_b;
+  st.ZZ = (const T*)m->pml_zz;
+  for (int ax = 0; ax < 2; ++ax) {
+    st.alpha[ax] = (const T*)m->pml_alpha[ax];
+    st.beta[ax] = (const T*)m->pml_beta[ax];
+  }
+  st.hx2 = (T)m->pml_half_inv_h[0];
+  st.hz2 = (T)m->pml_half_inv_h[1];
+}
+
+template <typename T, bool ADJ>
+int launch_pml(const nw_grid* g, const nw::KGrid<T>& kg, const nw::PmlStep<T>& st, int n_shots, cudaStream_t s) {
+  const long long cells = (long long)g->n[0] * g->n[1];
+  const dim3 grid((unsigned)((cells + 255) / 256), n_shots);
+  if (g->radius == 1) nw::pml2d_step<T, 1, ADJ><<<grid, 256, 0, s>>>(kg, st);
+  else nw::pml2d_step<T, 2, ADJ><<<grid, 256, 0, s>>>(kg, st);
+  NW_LAUNCHED();
+  return NW_OK;
+}
+
 template <typename T>
 struct Ring {  // time level n (n >= -1) of the pressure field: three rotating levels
   T* base;
@@ -375,8 +405,30 @@ struct Ring {  // time level n (n >= -1) of the pressure field: three rotating l
 template <typename T>
 int forward_step(const nw_grid* g, const nw::KGrid<T>& kg, const nw_medium* m, const nw_acquisition* a,
                  const nw_time* t, const Tune& tu, const Ring<T>& L, int n, T* traces, T* lap_out,
-                 cudaStream_t s) {
+                 cudaStream_t s, T* psi = nullptr) {
   const bool rec = traces && a->n_rec > 0 && (n % t->substeps) == 0;
+  if (g->absorbing == NW_ABS_PML) {  // 2-D with the reference's PML: psi levels 2*axis + parity
+    if (rec) {
+      int rc = launch_sample<T>(g, a, t->n_t, L.at(n), n / t->substeps, traces, s);
+      if (rc) return rc;
+    }
+    const long long LE = (long long)a->n_shots * g->field_elems;
+    nw::PmlStep<T> st = {};
+    st.prev = L.at(n - 1);
+    st.cur = L.at(n);
+    st.next = L.at(n + 1);
+    pml_medium(m, st);
+    for (int ax = 0; ax < 2; ++ax) {
+      st.f_old[ax] = psi + (long long)(2 * ax + n % 2) * LE;
+      st.f_new[ax] = psi + (long long)(2 * ax + (n + 1) % 2) * LE;
+    }
+    st.src_corner = a->has_source ? a->src_corner : nullptr;
+    st.src_w = (const T*)a->src_weight;
+    st.wavelet = (const T*)a->wavelet;
+    st.n = n;
+    st.lap_out = lap_out;
+    return launch_pml<T, false>(g, kg, st, a->n_shots, s);
+  }
   if (g->ndim == 2) {
     nw::Tiled2<T> st = {};
     st.prev = L.at(n - 1);
@@ -433,6 +485,9 @@ int forward_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
   L.level_elems = LE;
   const bool ckpt = !st->history && st->snap;
   if (ckpt && st->segment < 1) return fail(NW_ERR_ARG, "segment must be >= 1");
+  const bool pml = g->absorbing == NW_ABS_PML;
+  if (pml && ckpt) return fail(NW_ERR_UNSUPPORTED, "checkpointed storage with a PML is not built; keep a history");
+  if (pml && !st->pml_psi) return fail(NW_ERR_ARG, "a PML run needs storage.pml_psi");
   const nw::KGrid<T> kg = kgrid<T>(g);
   for (int n = n_begin; n < n_end; ++n) {
     if (ckpt && n % st->segment == 0) {
@@ -440,7 +495,7 @@ int forward_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
       if (rc) return rc;
     }
     T* lap = st->history ? (T*)st->history + (long long)n * LE : nullptr;
-    int rc = forward_step<T>(g, kg, m, a, t, tu, L, n, traces, lap, s);
+    int rc = forward_step<T>(g, kg, m, a, t, tu, L, n, traces, lap, s, (T*)st->pml_psi);
     if (rc) return rc;
   }
   if (traces && n_end == t->n_steps && t->n_steps % t->substeps == 0) {
@@ -465,7 +520,7 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
   const size_t lvl_bytes = (size_t)LE * sizeof(T);
   const nw::KGrid<T> kg = kgrid<T>(g);
   const bool ab = m->coef_a != nullptr;
-  NW_CUDA(cudaMemsetAsync(work, 0, 3 * lvl_bytes, s));
+  NW_CUDA(cudaMemsetAsync(work, 0, work_levels(g) * lvl_bytes, s));
   NW_CUDA(cudaMemsetAsync(gacc, 0, (size_t)n_acc_fields(g, tu, S) * g->field_elems * sizeof(T), s));
   auto q = [&](int n) { return work + (long long)(n % 3) * LE; };  // q^n = C mu^n, three levels
   const bool hist = st->history != nullptr;
@@ -509,8 +564,27 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
     as.tt = tile_tables(g, a, tu.adj);
     return NW_DISPATCH2(launch_adj2_v, T, tu.adj, kg, as, tu.adj.grid(g, S), s);
   };
+  const bool pml = g->absorbing == NW_ABS_PML;
+  if (pml && ckpt) return fail(NW_ERR_UNSUPPORTED, "checkpointed storage with a PML is not built; keep a history");
+  auto step_pml = [&](int n, const T* lap) -> int {  // PML step (face cotangents in work levels 3..6)
+    nw::PmlStep<T> ps = {};
+    ps.prev = q(n + 2);
+    ps.cur = q(n + 1);
+    ps.next = q(n);
+    pml_medium(m, ps);
+    for (int ax = 0; ax < 2; ++ax) {
+      ps.f_old[ax] = work + (long long)(3 + 2 * ax + (n + 1) % 2) * LE;
+      ps.f_new[ax] = work + (long long)(3 + 2 * ax + n % 2) * LE;
+    }
+    ps.apply_a = n >= 1 ? 1 : 0;
+    ps.lap = lap;
+    ps.grad = gacc;
+    int rc = launch_pml<T, true>(g, kg, ps, S, s);
+    if (rc) return rc;
+    return inject3(n);
+  };
   if (N >= n_stop) {  // level N: q^N = A C R^T g_N (q^{N+1} = q^{N+2} = 0)
-    int rc = g->ndim == 2 ? step2(N, nullptr) : inject3(N);
+    int rc = pml ? step_pml(N, nullptr) : (g->ndim == 2 ? step2(N, nullptr) : inject3(N));
     if (rc) return rc;
   }
   for (int n = N - 1; n >= n_stop; --n) {
@@ -530,6 +604,11 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
         }
       }
       lap = (const T*)st->segbuf + (long long)(n - n0) * LE;
+    }
+    if (pml) {
+      int rc = step_pml(n, lap);
+      if (rc) return rc;
+      continue;
     }
     if (g->ndim == 2) {
       int rc = step2(n, lap);
@@ -890,7 +969,7 @@ template <typename T>
 int noalloc_gradient(const nw_grid* g, const int32_t* n_abs, const nw_medium* m, const nw_acquisition* a,
                      const nw_time* t, const nw_storage* st, const Tune& tu, const void* c, double dt2,
                      const T* gtr, double* grad_c, cudaStream_t s) {
-  const size_t work_bytes = 3 * (size_t)a->n_shots * g->field_elems * sizeof(T);
+  const size_t work_bytes = (size_t)work_levels(g) * a->n_shots * g->field_elems * sizeof(T);
   const size_t acc_off = (work_bytes + 255) / 256 * 256;
   const int n_acc = n_acc_fields(g, tu, a->n_shots);
   const size_t need = acc_off + (size_t)n_acc * g->field_elems * sizeof(T);

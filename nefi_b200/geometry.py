@@ -251,3 +251,23 @@ def pml_profile(grid: PaddedGrid, ax: int, c_max: float, absorb_R: float, faces:
         return grid.layer_depth(ax, faces) * 0.0
     zmax = 1.5 * c_max * math.log(1.0 / absorb_R) / (grid.n_abs[ax] * grid.spacing[ax])
     return zmax * grid.layer_depth(ax, faces) ** 2
+
+
+def pml_coefficients(grid: PaddedGrid, c_max: float, absorb_R: float, dt: float) -> dict:
+    """float64 coefficients of the 2-D PML step (nefi/physics/wave.py:476-501): on cells
+    ``A = 1/(1 + dt/2 sum zeta)``, ``B = 1 - dt/2 sum zeta``, ``ZZ = dt^2 zeta_x zeta_z``; per axis on
+    its ``P+1`` faces ``alpha = (1 - dt/2 zeta_f)/(1 + dt/2 zeta_f)`` and
+    ``beta = dt (zeta_other - zeta_f) / ((1 + dt/2 zeta_f) h)`` (``zeta_other`` at the cell
+    centres of the other axis)."""
+    zc = [grid._broadcast(pml_profile(grid, ax, c_max, absorb_R), ax) for ax in range(2)]
+    zsum = (zc[0] + zc[1]).expand(grid.padded_shape)
+    out = {"A": 1.0 / (1.0 + 0.5 * dt * zsum), "B": 1.0 - 0.5 * dt * zsum,
+           "ZZ": (dt**2 * zc[0] * zc[1]).expand(grid.padded_shape), "alpha": [], "beta": []}
+    for ax in range(2):
+        zf = grid._broadcast(pml_profile(grid, ax, c_max, absorb_R, faces=True), ax)
+        fshape = list(grid.padded_shape)
+        fshape[ax] += 1
+        den = 1.0 + 0.5 * dt * zf
+        out["alpha"].append(((1.0 - 0.5 * dt * zf) / den).expand(fshape))
+        out["beta"].append((dt * (zc[1 - ax] - zf) / (den * grid.spacing[ax])).expand(fshape))
+    return out

@@ -100,9 +100,6 @@ class _LeapfrogB200(Operator):
         self.grid = PaddedGrid(domain, self.absorb_width)
         ta = TimeAxis(self.n_t, self.dt_obs, self.c_max, self.grid.spacing, self.order, self.courant)
         self.substeps, self.dt, self.n_steps = ta.substeps, ta.dt, ta.n_steps
-        if self.use_pml:
-            raise ConfigError("absorbing='pml' is not available in the B200 propagator yet; "
-                              "use 'sponge', 'cerjan' or 'none'")
         self._plans: dict = {}
         self._res: dict = {}
 
@@ -180,6 +177,10 @@ class _Run:
         # the pressure advances through three rotating levels in every mode
         self.ring = plan.empty_levels(3, n_shots)
         self.storage.ring = self.ring.data_ptr()
+        self.psi = None
+        if plan.pml is not None:  # the PML's face fields, two axes x two step parities, zero at start
+            self.psi = plan.empty_levels(4, n_shots)
+            self.storage.pml_psi = self.psi.data_ptr()
         if self.kind == "history":
             # step n stores Lap p^n into the interior of level n; nothing reads the ghost cells
             # (the adjoint multiplies them only into sums of cells outside the grid, never stored)
@@ -202,7 +203,7 @@ class _Run:
         return self.ring[(n + 1) % 3]
 
     def release(self) -> None:
-        self.history = self.ring = self.snap = self.segbuf = None
+        self.history = self.ring = self.snap = self.segbuf = self.psi = None
 
 
 def _forward_sweep(plan: DevicePlan, medium, acq, run: _Run, n_begin: int, n_end: int,
@@ -217,7 +218,7 @@ def _adjoint_sweep(plan: DevicePlan, medium, acq, run: _Run, grad_traces: torch.
                    want_initial: bool, stream: int):
     lib = _lib.load()
     S = run.n_shots
-    work = plan.empty_levels(3, S, zero=False)
+    work = plan.empty_levels(7 if plan.pml is not None else 3, S, zero=False)
     gC = torch.empty(plan.n_acc(S), plan.field, device=plan.device, dtype=plan.dtype)
     lam0 = mu1 = None
     if want_initial:

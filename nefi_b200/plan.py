@@ -15,7 +15,7 @@ import torch
 
 from . import _lib
 from ._compat import ConfigError
-from .geometry import PaddedGrid, cerjan_taper, sponge_coefficients, stencil_weights
+from .geometry import PaddedGrid, cerjan_taper, pml_coefficients, sponge_coefficients, stencil_weights
 
 
 def ghost_layout(grid_struct: _lib.Grid) -> _lib.Grid:
@@ -28,8 +28,8 @@ def make_grid(grid: PaddedGrid, order: int, dtype: torch.dtype, absorbing: str) 
     g.ndim = grid.d
     g.order = order
     g.dtype = _lib.dtype_code(dtype)
-    g.absorbing = {"none": _lib.NW_ABS_NONE, "sponge": _lib.NW_ABS_SPONGE,
-                   "cerjan": _lib.NW_ABS_CERJAN}[absorbing if any(grid.n_abs) else "none"]
+    g.absorbing = {"none": _lib.NW_ABS_NONE, "sponge": _lib.NW_ABS_SPONGE, "cerjan": _lib.NW_ABS_CERJAN,
+                   "pml": _lib.NW_ABS_PML}[absorbing if any(grid.n_abs) else "none"]
     for ax in range(3):
         if ax < grid.d:
             g.n[ax] = grid.padded_shape[ax]
@@ -67,6 +67,16 @@ def ghost_view(g: _lib.Grid, flat: torch.Tensor) -> torch.Tensor:
     return v[..., r:r + g.n[0], : g.n[1], : g.n[2]]
 
 
+def to_ghost_faces(g: _lib.Grid, faces: torch.Tensor, ax: int) -> torch.Tensor:
+    """Place a 2-D face array (padded shape with ``P_ax + 1`` along ``ax``) into a ghost-layout field:
+    face ``f`` at the cell index ``f``, so face ``P_ax`` lands in the first ghost row / column."""
+    out = torch.zeros((g.field_elems,), dtype=faces.dtype)
+    body = out[g.guard:].view(-1, g.stride[0])
+    r = g.radius
+    body[r:r + faces.shape[0], : faces.shape[1]].copy_(faces)
+    return out
+
+
 def ghost_offsets(g: _lib.Grid, corner: torch.Tensor) -> torch.Tensor:
     """Ghost-layout offsets ``(n, 2^d)`` of the stencil corners (same ordering as the weights)."""
     d = g.ndim
@@ -99,6 +109,15 @@ class DevicePlan:
             tp = cerjan_taper(grid, op.cerjan_gamma)
             self.A = to_ghost(self.g, tp.to(dtype)).to(device)
             self.B = self.A
+        self.pml = None
+        if self.g.absorbing == _lib.NW_ABS_PML:
+            co = pml_coefficients(grid, op.c_max, op.absorb_R, op.dt)
+            self.A = to_ghost(self.g, co["A"].to(dtype)).to(device)
+            self.B = to_ghost(self.g, co["B"].to(dtype)).to(device)
+            self.pml = {"ZZ": to_ghost(self.g, co["ZZ"].to(dtype)).to(device),
+                        "alpha": [to_ghost_faces(self.g, co["alpha"][ax].to(dtype), ax).to(device) for ax in range(2)],
+                        "beta": [to_ghost_faces(self.g, co["beta"][ax].to(dtype), ax).to(device) for ax in range(2)],
+                        "half_inv_h": [0.5 / h for h in grid.spacing]}
         self.first_b_one = 1 if self.g.absorbing == _lib.NW_ABS_CERJAN else 0
         # receivers
         corner, w = grid.point_stencils(op.receivers)
@@ -195,7 +214,14 @@ class DevicePlan:
 
     # -- descriptors ------------------------------------------------------------------------
     def medium(self, c2dt2: torch.Tensor) -> _lib.Medium:
-        return _lib.Medium(c2dt2.data_ptr(), _lib.ptr(self.A), _lib.ptr(self.B))
+        m = _lib.Medium(c2dt2.data_ptr(), _lib.ptr(self.A), _lib.ptr(self.B))
+        if self.pml is not None:
+            m.pml_zz = self.pml["ZZ"].data_ptr()
+            for ax in range(2):
+                m.pml_alpha[ax] = self.pml["alpha"][ax].data_ptr()
+                m.pml_beta[ax] = self.pml["beta"][ax].data_ptr()
+                m.pml_half_inv_h[ax] = self.pml["half_inv_h"][ax]
+        return m
 
     def acquisition(self, n_shots: int, shot0: int = 0) -> _lib.Acquisition:
         a = _lib.Acquisition()
@@ -249,6 +275,11 @@ def plan_storage(plan: DevicePlan, n_shots: int, n_steps: int, grad_mode: str,
     lvl = plan.level_bytes(n_shots)
     hist = (n_steps + 3) * lvl  # n_steps Lap p levels and the pressure ring
     if grad_mode == "autograd" and (budget is None or hist <= budget):
+        return ("history", None)
+    if plan.pml is not None:  # PML runs keep a history (checkpointed PML storage is not built)
+        if budget is not None and hist + 4 * lvl > budget:
+            raise ConfigError(f"a PML gradient keeps the full history: {hist / 2**30:.1f} GiB, above the "
+                              f"budget {budget / 2**30:.1f} GiB; lower source_batch or n_t, or use 'sponge'")
         return ("history", None)
     kind = _lib.SNAP_KINDS[snapshot]
     if checkpoint_every:

@@ -37,6 +37,12 @@ class GhostModel:
         self.w2 = [g.w2[ax] for ax in range(self.d)]
         self.wc = g.w_center
         self.F = int(g.field_elems)
+        self.pml = None
+        if plan.pml is not None:
+            self.pml = {"ZZ": plan.pml["ZZ"].numpy().astype(np.float64),
+                        "alpha": [a.numpy().astype(np.float64) for a in plan.pml["alpha"]],
+                        "beta": [b.numpy().astype(np.float64) for b in plan.pml["beta"]],
+                        "h2": list(plan.pml["half_inv_h"])}
 
     def lap(self, p):
         I = self.I
@@ -90,8 +96,97 @@ class GhostModel:
             a = self.A[cells[c]] if (apply_a and self.A is not None) else 1.0
             mu[cells[c]] += a * acc
 
+    def _pml_faces(self, u, fo, ax, adjoint, other=None):
+        """The kernel's face pair (f = x, x+1) of axis ``ax`` for every interior cell."""
+        I, s, pm = self.I, self.s[ax], self.pml
+        al, be = pm["alpha"][ax], pm["beta"][ax]
+        if not adjoint:
+            f0 = be[I] * (u[I] - u[I - s]) + al[I] * fo[I]
+            f1 = be[I + s] * (u[I + s] - u[I]) + al[I + s] * fo[I + s]
+        else:
+            sm, s0, sp = u[I - s] + other[I - s], u[I] + other[I], u[I + s] + other[I + s]
+            f0 = al[I] * fo[I] - pm["h2"][ax] * (s0 - sm)
+            f1 = al[I + s] * fo[I + s] - pm["h2"][ax] * (sp - s0)
+        last = self.coords[ax] == self.P[ax] - 1
+        new = np.zeros(self.F)
+        new[I] = f0
+        new[I[last] + s] = f1[last]
+        return f0, f1, new
+
+    def run_pml(self, C, n_steps, m, n_t, shots, init=None, grad_traces=None):
+        """``run`` for the 2-D PML (pml2d_step): face fields stored at the cell index of the face."""
+        I, pm = self.I, self.pml
+        S = len(shots)
+        traces = np.zeros((S, self.plan.n_rec, n_t))
+        Ls = []
+        for si, shot in enumerate(shots):
+            prev = np.zeros(self.F) if init is None else init[0][si].copy()
+            cur = np.zeros(self.F) if init is None else init[1][si].copy()
+            psi = [np.zeros(self.F), np.zeros(self.F)]
+            L_s = []
+            for n in range(n_steps):
+                if n % m == 0:
+                    traces[si, :, n // m] = self.sample(cur)
+                L = self.lap(cur)
+                new = []
+                for ax in range(2):
+                    f0, f1, nf = self._pml_faces(cur, psi[ax], ax, False)
+                    L = L + pm["h2"][ax] * ((f1 + psi[ax][I + self.s[ax]]) - (f0 + psi[ax][I]))
+                    new.append(nf)
+                L_s.append(L)
+                rhs = (2.0 * cur[I] - self.B[I] * prev[I]) + C[I] * L - pm["ZZ"][I] * cur[I]
+                nxt = np.zeros(self.F)
+                nxt[I] = rhs
+                if self.plan.has_source:
+                    corner = self.plan.src_corner[shot].numpy()
+                    w = self.plan.src_weight[shot].numpy().astype(np.float64)
+                    for k, bits in enumerate(itertools.product((0, 1), repeat=2)):
+                        off = self.g.origin + sum((corner[ax] + bits[ax]) * self.s[ax] for ax in range(2))
+                        nxt[off] += w[k] * float(self.plan.wavelet[n])
+                nxt[I] = self.A[I] * nxt[I]
+                prev, cur, psi = cur, nxt, new
+            traces[si, :, n_steps // m] = self.sample(cur)
+            Ls.append(L_s)
+        if grad_traces is None:
+            return traces, None, None, None
+        gC = np.zeros((S, self.F))
+        lam0 = np.zeros((S, self.F))
+        mu1_out = np.zeros((S, self.F))
+        for si in range(S):
+            q1, q2 = np.zeros(self.F), np.zeros(self.F)  # C mu^{n+1}, C mu^{n+2}
+            Psi = [np.zeros(self.F), np.zeros(self.F)]
+            qs = {}
+            for n in range(n_steps, -1, -1):
+                lapq = self.lap(q1)
+                term = np.zeros(I.shape)
+                new = []
+                for ax in range(2):
+                    f0, f1, nf = self._pml_faces(q1, Psi[ax], ax, True, other=q2)
+                    be = pm["beta"][ax]
+                    term = term + (be[I + self.s[ax]] * f1 - be[I] * f0)
+                    new.append(nf)
+                Psi = new
+                o = (2.0 * q1[I] - pm["ZZ"][I] * q1[I]) + C[I] * (lapq - term) - self.B[I] * q2[I]
+                out = np.zeros(self.F)
+                out[I] = self.A[I] * o if n >= 1 else o
+                if n % m == 0:  # C R^T g_n, scaled by A like the rest of the step
+                    inj = np.zeros(self.F)
+                    self.inject(inj, grad_traces[si, :, n // m], False)
+                    out[I] += (self.A[I] if n >= 1 else 1.0) * C[I] * inj[I]
+                if n <= n_steps - 1:
+                    gC[si, I] += q1[I] * Ls[si][n]
+                qs[n] = out
+                q1, q2 = out, q1
+            with np.errstate(divide="ignore", invalid="ignore"):
+                lam0[si, I] = qs[0][I] / C[I]
+                mu1_out[si, I] = (qs[1][I] / C[I]) if n_steps >= 1 else 0.0
+            gC[si, I] = gC[si, I] / C[I]  # C dJ/dC -> dJ/dC
+        return traces, gC, lam0, mu1_out
+
     def run(self, C, n_steps, m, n_t, shots, init=None, grad_traces=None):
         """Forward (and adjoint) for every shot; returns traces, per-shot dJ/dC, lambda0, mu1."""
+        if self.pml is not None:
+            return self.run_pml(C, n_steps, m, n_t, shots, init, grad_traces)
         S = len(shots)
         n_rec = self.plan.n_rec
         traces = np.zeros((S, n_rec, n_t))
