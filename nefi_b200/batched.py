@@ -41,6 +41,8 @@ class BatchedFWI:
                 raise ConfigError("BatchedFWI takes 2-D WaveOperatorB200 problems")
             if op.order != ops[0].order:
                 raise ConfigError("the problems of a batch share one stencil order")
+            if op.use_pml:
+                raise ConfigError("batched problems use absorbing='sponge', 'cerjan' or 'none'")
         self.device = torch.device(device)
         self.dtype = dtype
         self.ops = list(ops)
@@ -67,7 +69,11 @@ class BatchedFWI:
             plan = op._plan(dev, self.dtype)
             plan.set_tuning(*self.tuning)
             S = op.n_sources
-            b = {"plan": plan, "S": S}
+            # the device table and the descriptors point at the plan's per-tile tables: keep these
+            # tensors (and the tuning) alive even if the operator's plan is re-tuned later
+            b = {"plan": plan, "S": S, "tune": plan.tuning,
+                 "tables": [plan.rec_corner, plan.tile_rec_ptr, plan.tile_rec_list, plan.tile_cell_ptr,
+                            plan.tile_cell_local, plan.tile_cell_gid]}
             b["ring"] = plan.empty_levels(3, S)
             n_snap = -(-op.n_steps // K) if op.n_steps > 0 else 1
             b["snap"] = torch.empty(plan.snapshot_bytes(S, n_snap, kind), dtype=torch.uint8, device=dev)
@@ -91,7 +97,7 @@ class BatchedFWI:
             q.work, q.grad_acc = b["work"].data_ptr(), b["acc"].data_ptr()
             q.traces, q.grad_traces = b["traces"].data_ptr(), b["gtr"].data_ptr()
             self.bufs.append(b)
-        self.tune = self.bufs[0]["plan"].tuning
+        self.tune = self.bufs[0]["tune"]
         self.table = torch.empty(int(lib.nw_batch_table_bytes(n)), dtype=torch.uint8, device=dev)
         _lib.check(lib.nw_batch_prepare(self.problems, n, C.byref(self.tune), self.table.data_ptr(),
                                         _lib.stream_handle(dev)))

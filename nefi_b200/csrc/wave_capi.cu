@@ -1044,6 +1044,8 @@ int check_batch(const nw_batch_problem* P, int n, const Tune& tu) {
     int rc = check_run(&q.grid, &q.medium, &q.acq, &q.time, &q.storage, tu);
     if (rc) return fail(rc, "batch problem " + std::to_string(p) + ": " + g_err);
     if (q.grid.ndim != 2) return fail(NW_ERR_UNSUPPORTED, "batched problems are 2-D");
+    if (q.grid.absorbing == NW_ABS_PML)
+      return fail(NW_ERR_UNSUPPORTED, "batched problems use a sponge, Cerjan or no absorbing layer");
     if (q.grid.dtype != P[0].grid.dtype || q.grid.order != P[0].grid.order)
       return fail(NW_ERR_ARG, "batched problems share one dtype and stencil order");
     if (!q.acq.has_source) return fail(NW_ERR_UNSUPPORTED, "batched problems are FWI problems (with sources)");
