@@ -277,7 +277,7 @@ int nw_initial_state_adjoint(const nw_grid* g, const int32_t* n_abs, const nw_me
  * reserves its device memory at start-up and may not allocate afterwards, or a latency-bound loop
  * that must not call cudaMalloc, which synchronises the device. The caller still passes every
  * input and the output grad_c (physical grid, float64).
- *  - Limit: 3 * n_shots * field_elems * sizeof(dtype), rounded up to 256 bytes, plus
+ *  - Limit: 3 * n_shots * field_elems * sizeof(dtype) (7 * ... with a PML), rounded up to 256 bytes, plus
  *    nw_adjoint_groups() * field_elems * sizeof(dtype) bytes must not exceed NW_NOALLOC_SCRATCH_BYTES (64 MiB);
  *    e.g. 16 float32 shots on a 552^2 padded grid fit, 20 do not. Larger requests return
  *    NW_ERR_ARG with a message giving the size needed; use nw_adjoint then.
