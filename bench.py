@@ -42,13 +42,13 @@ def peaks() -> tuple[float, str]:
     return 6650.0, "fallback"
 
 
-def workload_desc(w, storage: str = "full history in HBM") -> dict:
+def workload_desc(w, storage: str = "full history in HBM", layer: str = "sponge") -> dict:
     P = w.n + 2 * w.absorb_cells
     model = ("seeded layered model (6-10 layers 1500-4500 m/s + 4 anomalies) + salt body (4500 m/s)"
              if w.name == "fwi_2048" else "seeded layered model (6-10 layers 1500-4500 m/s + 4 anomalies)")
     return {"workload": f"{w.name}: {w.n}x{w.n} FP32 grid h={w.h:g} m, {model}, {len(w.sources)} Ricker shots "
                         f"{w.f0:g} Hz, {len(w.receivers)} receivers, {w.n_steps} steps, Courant "
-                        f"{w.courant_number}, order {w.order}, {w.absorb_cells}-cell sponge, {storage}",
+                        f"{w.courant_number}, order {w.order}, {w.absorb_cells}-cell {layer}, {storage}",
             "grid_padded": [P, P], "shots_per_gpu": len(w.sources), "n_steps": w.n_steps,
             "l2": "256 MiB buffer written between timed steps; working set (history) far above L2"}
 
@@ -235,6 +235,71 @@ def run_batch(args) -> None:
     print(json.dumps(out), flush=True)
 
 
+def run_pat(args) -> None:
+    """3-D photoacoustic gradient (configuration 5): 256^3 grid + 20-cell sponge, c = 1500 m/s
+    +-5 % smooth seeded perturbation, 4 instances of 20 random ellipsoids, a 256 x 256 sensor plane,
+    2000 steps; the gradient w.r.t. p0 and c of 1/2 ||F(p0) - d||^2, checkpointed storage."""
+    from nefi_b200 import WaveInitialConditionOperatorB200, workloads
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    n_steps = args.n_steps or 2000
+    n = args.pat_n
+    w = workloads.pat_volume(n=n, batch=4, n_steps=n_steps)
+    op = WaveInitialConditionOperatorB200(w.domain, w.sensors, grad_mode="checkpoint", snapshot=args.snapshot,
+                                          checkpoint_every=args.checkpoint_every, **w.operator_kwargs())
+    p0 = torch.tensor(w.p0, device=dev)
+    c = torch.tensor(w.c, dtype=torch.float32, device=dev)
+    with torch.no_grad():
+        d = op({"p0": p0 * 0.9})
+
+    def step():
+        x = p0.clone().requires_grad_(True)
+        cc = c.clone().requires_grad_(True)
+        tr = op.with_speed(x, cc)
+        loss = 0.5 * (tr - d).double().square().sum()
+        gp, gc = torch.autograd.grad(loss, (x, cc))
+        return loss, gp, gc
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    lib = __import__("nefi_b200")._lib.load()
+    l0 = lib.nw_launch_count()
+    sampler = ClockSampler(dev.index)
+    times = []
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        step()
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    clocks = sampler.stop()
+    launches = lib.nw_launch_count() - l0
+    ms = sum(times) / len(times)
+    P = op.grid.padded_shape
+    cells = P[0] * P[1] * P[2]
+    useful = 2 * cells * op.n_steps * 4
+    peak, peak_kind = peaks()
+    achieved = 16.0 * useful / (ms * 1e-3) / 1e9
+    out = {"metric": METRIC, "value": 4 / (ms * 1e-3), "unit": "instance-gradients/s", "n_gpus": 1,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic (seeded smooth speed, 20 random ellipsoids per instance)",
+           "config": {"workload": f"pat_{n}: {n}^3 grid + 20-cell sponge ({P[0]}^3 padded), order 2, 4 instances, "
+                                  f"{len(w.sensors)} sensors on one face, {op.n_steps} steps; gradient w.r.t. p0 and c; "
+                                  f"checkpointed with {args.snapshot} snapshots",
+                      "method": "plain (per-step launches)",
+                      "l2": "working set (4 x {0:.0f} MB per level) far above L2".format(cells * 16 / 1e6)},
+           "gcell_updates_per_s": useful / (ms * 1e-3) / 1e9,
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "traffic": None, "peak_source": peak_kind,
+                        "note": "16 B per useful cell-update (forward + adjoint); the segment recompute is not counted"},
+           "clocks": clocks, "gpu_launches": int(launches)}
+    print(json.dumps(out), flush=True)
+
+
 def run_reference(args) -> None:
     from nefi_b200 import workloads
 
@@ -278,6 +343,9 @@ def main() -> None:
                     help="autograd keeps the full history when it fits, else checkpoints")
     ap.add_argument("--snapshot", default="exact", choices=("exact", "fixed16", "fp16", "bf16"))
     ap.add_argument("--checkpoint-every", type=int, default=None)
+    ap.add_argument("--absorbing", default=None, choices=("sponge", "pml", "cerjan", "none"),
+                    help="override the workload's absorbing layer (fwi workloads)")
+    ap.add_argument("--pat-n", type=int, default=256, help="pat_256: grid edge (profiling cases)")
     ap.add_argument("--accuracy-shots", type=int, default=None,
                     help="shots of the float64 accuracy check (all by default)")
     args = ap.parse_args()
@@ -286,6 +354,9 @@ def main() -> None:
         return
     if args.workload == "fwi_batch":
         run_batch(args)
+        return
+    if args.workload == "pat_256":
+        run_pat(args)
         return
 
     import torch.distributed as dist
@@ -301,8 +372,11 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
 
     w = make_workload(args)
+    okw = w.operator_kwargs()
+    if args.absorbing:
+        okw["absorbing"] = args.absorbing
     op = WaveOperatorB200(w.domain, w.sources, w.receivers, grad_mode=args.grad_mode, snapshot=args.snapshot,
-                          checkpoint_every=args.checkpoint_every, **w.operator_kwargs())
+                          checkpoint_every=args.checkpoint_every, **okw)
     c = torch.tensor(w.c, dtype=torch.float32, device=dev)
     # observed data: traces of a smoothed model (the misfit of a typical early FWI iteration)
     with torch.no_grad():
@@ -416,7 +490,7 @@ def main() -> None:
         # float32 gradient against a float64 device run of the same step (checkpointed, exact
         # snapshots), over the first --accuracy-shots shots (all by default)
         na = args.accuracy_shots or len(w.sources)
-        kw = w.operator_kwargs()
+        kw = okw
         op32 = WaveOperatorB200(w.domain, w.sources[:na], w.receivers, grad_mode=args.grad_mode,
                                 snapshot=args.snapshot, checkpoint_every=args.checkpoint_every, **kw)
         _, g32 = op32.misfit_gradient(c, d[:na])
@@ -438,7 +512,7 @@ def main() -> None:
                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "f32",
                "data": "synthetic (seeded layered model; observed data from a smoothed model)",
-               "config": {**workload_desc(w, storage), "method": f"plain (per-step launches, {storage})",
+               "config": {**workload_desc(w, storage, op.absorbing), "method": f"plain (per-step launches, {storage})",
                           "parallelism": f"shots sharded over {world} GPU(s), fp64 gradient all-reduce"},
                "gcell_updates_per_s": gcells, "roofline": roofline, "cpu_baseline": cpu,
                "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
