@@ -1,0 +1,175 @@
+// stencil3d.cuh — plane-marching 3-D leapfrog step for sm_100a (forward and q-form adjoint).
+//
+// A CTA (8 warps) owns a (y, z) tile of 8 rows by TZ = 32*VZ columns and marches along x over a
+// chunk of XC planes. Warp w owns row y0 + w, lane l the VZ columns z0 + l*VZ. Every plane the
+// march touches passes once through a ring of NSP shared-memory tiles, (8 + 2R) rows by
+// TZ + 2*HL columns (the y/z halo), staged by cp.async two planes ahead of its first use; the
+// x-neighbours of a thread's cells stay in a (2R+1)-plane register window, fed from the ring when a
+// plane arrives. The y/z neighbours of the centre plane come from its shared tile. Planes outside
+// the grid are never copied: their window values are zero, like the ghost planes they stand for.
+// C, p^{n-1} (q^{n+2}), A/B (layer cells) and the stored Lap p are read at the thread's own cells
+// straight from global memory with vector loads.
+#pragma once
+#include "kernels.cuh"
+#include "stencil2d.cuh"
+
+namespace nw {
+
+template <typename T, int VZ, int R>
+struct Tile3Shape {
+  static constexpr int TY = 8;
+  static constexpr int TZ = 32 * VZ;
+  static constexpr int HL = 16 / (int)sizeof(T);
+  static constexpr int SW = TZ + 2 * HL;
+  static constexpr int EPC = 16 / (int)sizeof(T);
+  static constexpr int HR = TY + 2 * R;
+  static constexpr int PS = HR * SW;                        // elements of a plane tile
+  static constexpr int NCH = (HR * (SW / EPC) + 255) / 256;  // chunks per thread and plane
+  static constexpr int NSP = R + 3;                          // planes in the ring
+};
+
+// The chunks of one plane tile: offsets relative to the plane's cell (x, 0, 0); rows and columns
+// that no output cell reads (beyond the ghost rows / past the row pitch) are not copied.
+template <typename T, int VZ, int R>
+__device__ __forceinline__ CopyPlan<Tile3Shape<T, VZ, R>::NCH> plan_plane(const KGrid<T>& g, int y0, int z0) {
+  using S = Tile3Shape<T, VZ, R>;
+  constexpr int CPR = S::SW / S::EPC;
+  CopyPlan<S::NCH> p;
+#pragma unroll
+  for (int i = 0; i < S::NCH; ++i) {
+    const int c = threadIdx.x + 256 * i;
+    const int row = c / CPR, ch = c - row * CPR;
+    const int y = y0 - R + row;
+    const int z = z0 - S::HL + ch * S::EPC;
+    p.soff[i] = row * S::SW + ch * S::EPC;
+    p.goff[i] = (c < S::HR * CPR && y < g.n1 + R && z < (int)g.s1) ? (int)((long long)y * g.s1 + z) : -1;
+  }
+  return p;
+}
+
+template <typename T, int R, int VZ, bool ADJ>
+__global__ void __launch_bounds__(256, 4) step3t(KGrid<T> g, Step3<T> a, int xc) {
+  using S = Tile3Shape<T, VZ, R>;
+  constexpr int NSP = S::NSP;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* ring = reinterpret_cast<T*>(smem_raw);  // [NSP][PS]
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int tiles_z = (g.n2 + S::TZ - 1) / S::TZ;
+  const int z0 = (blockIdx.x % tiles_z) * S::TZ, y0 = (blockIdx.x / tiles_z) * S::TY;
+  const int x0 = blockIdx.y * xc, x1 = min(x0 + xc, g.n0);
+  const int s = blockIdx.z;
+  const long long so = (long long)s * g.field;
+  const int y = y0 + warp, zc = z0 + lane * VZ;
+  const bool own = y < g.n1 && zc < g.n2;
+  const long long ld = g.s1;
+  const T* __restrict__ cur = a.cur + so;
+  const CopyPlan<S::NCH> pp = plan_plane<T, VZ, R>(g, y0, z0);
+  // the planes of the march: xa = x0 - R .. xb - 1 = x1 + R - 1; plane p sits in ring slot
+  // (p - xa) % NSP. When plane p is consumed (its own cells enter the window front) the centre is
+  // p - R: planes p - R .. p must be resident, and the copy of plane p + 2 goes into the slot of
+  // plane p - R - 1 (NSP = R + 3), the centre of the previous iteration.
+  const int xa = x0 - R, xb = x1 + R;
+  auto issue_plane = [&](int p) {
+    if (p >= 0 && p < g.n0 && p < xb) issue(pp, cur + g.origin + (long long)p * g.s0, ring + ((p - xa) % NSP) * S::PS);
+  };
+  wait_previous_grid();
+  allow_next_grid();
+  if (!ADJ && a.traces) gather_receivers<T, 8>(cur, a.traces, a.rec_idx, a.rec_w, a.n_rec, a.n_t, a.j, s);
+  issue_plane(xa);  // one commit group per plane, empty groups included
+  cp_async_commit();
+  issue_plane(xa + 1);
+  cp_async_commit();
+  const bool yz_layer = y0 < g.lo1 || y0 + S::TY > g.hi1 || z0 < g.lo2 || z0 + S::TZ > g.hi2;
+  const T wc = g.wc, w1x = g.w1a, w1y = g.w1b, w1z = g.w1c, w2x = g.w2a, w2y = g.w2b, w2z = g.w2c;
+  // source corners of this shot (forward)
+  int bx = -4, by = -4, bz = -4;
+  if (!ADJ && a.src_corner) { bx = a.src_corner[3 * s]; by = a.src_corner[3 * s + 1]; bz = a.src_corner[3 * s + 2]; }
+
+  T wv[2 * R + 1][VZ];  // own cells of planes p - 2R .. p
+#pragma unroll
+  for (int q = 0; q < 2 * R + 1; ++q)
+#pragma unroll
+    for (int v = 0; v < VZ; ++v) wv[q][v] = T(0);
+  const int own_off = (warp + R) * S::SW + S::HL + lane * VZ;
+  for (int p = xa; p < xb; ++p) {
+    issue_plane(p + 2);
+    cp_async_commit();
+    cp_async_wait<2>();
+    __syncthreads();  // plane p has landed (its centre p - R landed R planes ago)
+    if (p >= 0 && p < g.n0) vload<T, VZ>(ring + ((p - xa) % NSP) * S::PS + own_off, wv[2 * R]);
+    else {
+#pragma unroll
+      for (int v = 0; v < VZ; ++v) wv[2 * R][v] = T(0);
+    }
+    const int x = p - R;
+    if (x >= x0 && own) {
+      const T* P = ring + ((x - xa) % NSP) * S::PS;  // the centre plane's tile
+      const long long i = g.origin + (long long)x * g.s0 + (long long)y * ld + zc;
+      Row3<T, VZ> rw;
+      vload<T, VZ>(P + own_off - VZ, rw.l);
+#pragma unroll
+      for (int v = 0; v < VZ; ++v) rw.c[v] = wv[R][v];
+      vload<T, VZ>(P + own_off + VZ, rw.r);
+      T ym[VZ], yp[VZ], ym2[VZ], yp2[VZ];
+      vload<T, VZ>(P + own_off - S::SW, ym);
+      vload<T, VZ>(P + own_off + S::SW, yp);
+      if (R == 2) {
+        vload<T, VZ>(P + own_off - 2 * S::SW, ym2);
+        vload<T, VZ>(P + own_off + 2 * S::SW, yp2);
+      }
+      T pv[VZ], cc[VZ], ca[VZ], cb[VZ];
+      vldg<T, VZ>(a.prev + so + i, pv);
+      vldg<T, VZ>(a.C + i, cc);
+      const bool layer = yz_layer || x < g.lo0 || x >= g.hi0;
+#pragma unroll
+      for (int v = 0; v < VZ; ++v) { ca[v] = T(1); cb[v] = T(1); }
+      if (a.A && layer) {
+        vldg<T, VZ>(a.A + i, ca);
+        if (ADJ || !a.b_one) vldg<T, VZ>(a.B + i, cb);
+      }
+      T o[VZ], lp[VZ];
+#pragma unroll
+      for (int v = 0; v < VZ; ++v) {
+        const T c = wv[R][v];
+        T lap = fma_rn(w1z, add_rn(zval(rw, v - 1), zval(rw, v + 1)),
+                       fma_rn(w1y, add_rn(ym[v], yp[v]),
+                              fma_rn(w1x, add_rn(wv[R - 1][v], wv[R + 1][v]), mul_rn(wc, c))));
+        if (R == 2)
+          lap = fma_rn(w2z, add_rn(zval(rw, v - 2), zval(rw, v + 2)),
+                       fma_rn(w2y, add_rn(ym2[v], yp2[v]), fma_rn(w2x, add_rn(wv[0][v], wv[4][v]), lap)));
+        lp[v] = lap;
+        o[v] = fma_rn(cc[v], lap, fma_rn(-cb[v], pv[v], add_rn(c, c)));
+      }
+      if (!ADJ && bx >= x - 1 && bx <= x && by >= y - 1 && by <= y) {  // the source stencil touches this row
+        const T wn = a.wavelet[a.n];
+#pragma unroll
+        for (int v = 0; v < VZ; ++v) {
+          const int dx = x - bx, dy = y - by, dz = zc + v - bz;
+          if (dz >= 0 && dz <= 1) o[v] = add_rn(o[v], mul_rn(a.src_w[8 * s + 4 * dx + 2 * dy + dz], wn));
+        }
+      }
+      if (layer && a.A && (!ADJ || a.apply_a)) {
+#pragma unroll
+        for (int v = 0; v < VZ; ++v) o[v] = mul_rn(ca[v], o[v]);
+      }
+      store_row<T, VZ>(a.next + so + i, o, zc, g.n2);
+      if (!ADJ && a.lap_out) store_row<T, VZ>(a.lap_out + so + i, lp, zc, g.n2);
+      if (ADJ && a.lap) {
+        T gl[VZ], gg[VZ];
+        vldg<T, VZ>(a.lap + so + i, gl);
+        vload<T, VZ>(a.grad + so + i, gg);
+#pragma unroll
+        for (int v = 0; v < VZ; ++v) gg[v] = fma_rn(wv[R][v], gl[v], gg[v]);
+        store_row<T, VZ>(a.grad + so + i, gg, zc, g.n2);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 2 * R; ++q)
+#pragma unroll
+      for (int v = 0; v < VZ; ++v) wv[q][v] = wv[q + 1][v];
+    __syncthreads();  // every thread is done with the centre's slot, which the next copy refills
+  }
+}
+
+}  // namespace nw

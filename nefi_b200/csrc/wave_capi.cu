@@ -19,6 +19,7 @@
 #include "kernels.cuh"
 #include "pml2d.cuh"
 #include "stencil2d.cuh"
+#include "stencil3d.cuh"
 
 namespace {
 
@@ -324,20 +325,23 @@ int launch_adj2_v(const nw::KGrid<T>& kg, const nw::Tiled2<T>& st, dim3 grid, cu
   return launch_pdl(nw::adj2d<T, R, VZ, RX, AB>, grid, smem, s, kg, st);
 }
 
-// 3-D step: forward (ADJ = false) or adjoint.
+// 3-D step: forward (ADJ = false) or adjoint, plane-marching tiles of 8 x 64 (y, z) cells over
+// chunks of kXChunk planes.
+constexpr int kXChunk = 32;
+template <typename T, int R, bool ADJ>
+int launch_step3_r(const nw_grid* g, const nw::KGrid<T>& kg, const nw::Step3<T>& st, int n_shots, cudaStream_t s) {
+  using S = nw::Tile3Shape<T, 2, R>;
+  const int tz = (g->n[2] + S::TZ - 1) / S::TZ, ty = (g->n[1] + S::TY - 1) / S::TY;
+  const dim3 grid(tz * ty, (g->n[0] + kXChunk - 1) / kXChunk, n_shots);
+  constexpr size_t smem = (size_t)S::NSP * S::PS * sizeof(T);
+  static_assert(smem <= 48 * 1024, "plane ring above the default shared-memory limit");
+  return launch_pdl(nw::step3t<T, R, 2, ADJ>, grid, smem, s, kg, st, kXChunk);
+}
 template <typename T, bool ADJ>
 int launch_step3(const nw_grid* g, const nw::KGrid<T>& kg, const nw::Step3<T>& st, bool ab, int n_shots,
                  cudaStream_t s) {
-  const Shape sh = stencil_shape(g, n_shots);
-  if (g->radius == 1) {
-    if (ab) nw::step3d<T, 1, true, kRX, ADJ><<<sh.grid, sh.block, 0, s>>>(kg, st);
-    else nw::step3d<T, 1, false, kRX, ADJ><<<sh.grid, sh.block, 0, s>>>(kg, st);
-  } else {
-    if (ab) nw::step3d<T, 2, true, kRX, ADJ><<<sh.grid, sh.block, 0, s>>>(kg, st);
-    else nw::step3d<T, 2, false, kRX, ADJ><<<sh.grid, sh.block, 0, s>>>(kg, st);
-  }
-  NW_LAUNCHED();
-  return NW_OK;
+  (void)ab;  // the kernel reads A/B in layer cells when the medium has them
+  return g->radius == 1 ? launch_step3_r<T, 1, ADJ>(g, kg, st, n_shots, s) : launch_step3_r<T, 2, ADJ>(g, kg, st, n_shots, s);
 }
 
 // Runtime (radius, vz, rx, absorbing) -> template instantiation.
