@@ -28,8 +28,10 @@ struct Tile3Shape {
   static constexpr int NSP = R + 3;                          // planes in the ring
 };
 
-// The chunks of one plane tile: offsets relative to the plane's cell (x, 0, 0); rows and columns
-// that no output cell reads (beyond the ghost rows / past the row pitch) are not copied.
+// The chunks of one plane tile: element offsets from the field base for plane 0 (add x * s0 for
+// plane x; they are >= 0 for x >= 0 thanks to the ghost planes and the guard, and -1 marks a chunk
+// that is not copied); rows and columns that no output cell reads (beyond the ghost rows, past the
+// row pitch) are not copied.
 template <typename T, int VZ, int R>
 __device__ __forceinline__ CopyPlan<Tile3Shape<T, VZ, R>::NCH> plan_plane(const KGrid<T>& g, int y0, int z0) {
   using S = Tile3Shape<T, VZ, R>;
@@ -42,7 +44,7 @@ __device__ __forceinline__ CopyPlan<Tile3Shape<T, VZ, R>::NCH> plan_plane(const 
     const int y = y0 - R + row;
     const int z = z0 - S::HL + ch * S::EPC;
     p.soff[i] = row * S::SW + ch * S::EPC;
-    p.goff[i] = (c < S::HR * CPR && y < g.n1 + R && z < (int)g.s1) ? (int)((long long)y * g.s1 + z) : -1;
+    p.goff[i] = (c < S::HR * CPR && y < g.n1 + R && z < (int)g.s1) ? (int)(g.origin + (long long)y * g.s1 + z) : -1;
   }
   return p;
 }
@@ -71,7 +73,7 @@ __global__ void __launch_bounds__(256, 4) step3t(KGrid<T> g, Step3<T> a, int xc)
   // plane p - R - 1 (NSP = R + 3), the centre of the previous iteration.
   const int xa = x0 - R, xb = x1 + R;
   auto issue_plane = [&](int p) {
-    if (p >= 0 && p < g.n0 && p < xb) issue(pp, cur + g.origin + (long long)p * g.s0, ring + ((p - xa) % NSP) * S::PS);
+    if (p >= 0 && p < g.n0 && p < xb) issue(pp, cur + (long long)p * g.s0, ring + ((p - xa) % NSP) * S::PS);
   };
   wait_previous_grid();
   allow_next_grid();
