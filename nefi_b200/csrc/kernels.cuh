@@ -88,83 +88,6 @@ __device__ __forceinline__ void gather_receivers(const T* __restrict__ lvl, T* _
 }
 
 // ------------------------------------------------------------------------------------------
-// 3-D kernels: thread (tx, ty) owns (y, z) = (by*blockDim.y + ty, bz*32 + tx) and RX planes
-// along x starting at x0 = blockIdx.y*RX; blockIdx.x enumerates (y-tile, z-tile).
-// ------------------------------------------------------------------------------------------
-struct Tile3 {
-  int y, z, x0;
-};
-__device__ __forceinline__ Tile3 tile3(int n2, int RX) {
-  const int zt = (n2 + blockDim.x - 1) / blockDim.x;
-  Tile3 t;
-  t.z = (blockIdx.x % zt) * blockDim.x + threadIdx.x;
-  t.y = (blockIdx.x / zt) * blockDim.y + threadIdx.y;
-  t.x0 = blockIdx.y * RX;
-  return t;
-}
-
-template <typename T, int R, bool AB, int RX, bool ADJ>
-__global__ void __launch_bounds__(256) step3d(KGrid<T> g, Step3<T> a) {
-  const int s = blockIdx.z;
-  const long long so = (long long)s * g.field;
-  const T* __restrict__ pc = a.cur + so;
-  if (!ADJ && a.traces) gather_receivers<T, 8>(pc, a.traces, a.rec_idx, a.rec_w, a.n_rec, a.n_t, a.j, s);
-  const Tile3 t = tile3(g.n2, RX);
-  if (t.z >= g.n2 || t.y >= g.n1 || t.x0 >= g.n0) return;
-  const long long base = g.origin + (long long)t.x0 * g.s0 + (long long)t.y * g.s1 + t.z;
-  T col[RX + 2 * R];
-#pragma unroll
-  for (int k = 0; k < RX + 2 * R; ++k) {
-    const int xr = t.x0 - R + k;
-    col[k] = (xr < g.n0 + R) ? pc[base + (long long)(k - R) * g.s0] : T(0);
-  }
-  int bx = -4, by = -4, bz = -4;
-  T sw[8];
-  T wn = 0;
-#pragma unroll
-  for (int k = 0; k < 8; ++k) sw[k] = 0;
-  if (!ADJ && a.src_corner) {
-    bx = a.src_corner[3 * s]; by = a.src_corner[3 * s + 1]; bz = a.src_corner[3 * s + 2];
-    if (bz <= t.z && t.z <= bz + 1 && by <= t.y && t.y <= by + 1 && bx + 1 >= t.x0 && bx <= t.x0 + RX - 1) {
-#pragma unroll
-      for (int k = 0; k < 8; ++k) sw[k] = a.src_w[8 * s + k];
-      wn = a.wavelet[a.n];
-    } else {
-      bx = -4;
-    }
-  }
-  const T* __restrict__ ln = (ADJ && a.lap) ? a.lap + so : nullptr;
-#pragma unroll
-  for (int k = 0; k < RX; ++k) {
-    const int x = t.x0 + k;
-    if (x < g.n0) {
-      const long long i = base + (long long)k * g.s0;
-      const T c = col[k + R];
-      T lap = g.wc * c + g.w1a * (col[k + R - 1] + col[k + R + 1]) +
-              g.w1b * (pc[i - g.s1] + pc[i + g.s1]) + g.w1c * (pc[i - 1] + pc[i + 1]);
-      if (R == 2)
-        lap += g.w2a * (col[k] + col[k + 4]) + g.w2b * (pc[i - 2 * g.s1] + pc[i + 2 * g.s1]) +
-               g.w2c * (pc[i - 2] + pc[i + 2]);
-      const T pp = a.prev[so + i];
-      T av = T(1), bv = T(1);
-      bool layer = false;
-      if (AB) {
-        layer = x < g.lo0 || x >= g.hi0 || t.y < g.lo1 || t.y >= g.hi1 || t.z < g.lo2 || t.z >= g.hi2;
-        if (layer) { av = a.A[i]; bv = (!ADJ && a.b_one) ? T(1) : a.B[i]; }
-      }
-      if (!ADJ && a.lap_out) a.lap_out[so + i] = lap;
-      T rhs = (T(2) * c - bv * pp) + a.C[i] * lap;
-      if (!ADJ) {
-        const int dx = x - bx, dy = t.y - by, dz = t.z - bz;
-        if (dx >= 0 && dx <= 1 && dy >= 0 && dy <= 1 && dz >= 0 && dz <= 1) rhs += sw[4 * dx + 2 * dy + dz] * wn;
-      }
-      a.next[so + i] = (layer && (!ADJ || a.apply_a)) ? av * rhs : rhs;
-      if (ln) a.grad[so + i] += c * ln[i];
-    }
-  }
-}
-
-// ------------------------------------------------------------------------------------------
 // Small kernels: receiver gather, adjoint injection, medium/initial-state preparation,
 // gradient reduction and the snapshot codec.
 // ------------------------------------------------------------------------------------------

@@ -90,24 +90,7 @@ nw::PadMap padmap(const nw_grid* g, const int32_t* n_abs) {
   return p;
 }
 
-constexpr int kRX = 4;     // rows (2-D) or planes (3-D) per thread
 constexpr int kGuard = 32; // zero elements in front of every field (see nw_grid.guard)
-
-// Launch shape of the stencil kernels: 32 x 8 threads, each owning kRX cells along axis 0.
-struct Shape {
-  dim3 grid, block;
-};
-Shape stencil_shape(const nw_grid* g, int n_shots) {
-  Shape s;
-  s.block = dim3(32, 8, 1);
-  if (g->ndim == 2) {
-    s.grid = dim3((g->n[1] + 31) / 32, (g->n[0] + 8 * kRX - 1) / (8 * kRX), n_shots);
-  } else {
-    const unsigned zt = (g->n[2] + 31) / 32, yt = (g->n[1] + 7) / 8;
-    s.grid = dim3(zt * yt, (g->n[0] + kRX - 1) / kRX, n_shots);
-  }
-  return s;
-}
 
 template <typename T>
 int launch_sample(const nw_grid* g, const nw_acquisition* a, int n_t, const T* lvl, int j, T* traces,
