@@ -379,6 +379,66 @@ class OracleWave:
             m2, m1 = m1, A * lam
         return traces, gC, lam0, mu1
 
+    def nearest_cells(self, pts):
+        """Flattened padded-grid index of the cell containing each point (nefi/physics/wave.py:302-310)."""
+        pts = np.asarray(pts, dtype=np.float64)
+        flat = np.zeros(pts.shape[0], dtype=np.int64)
+        for ax in range(self.d):
+            i = np.clip(np.floor((pts[:, ax] - self.lo[ax]) / self.h[ax]).astype(np.int64), 0, self.P[ax] - 1)
+            flat = flat * self.P[ax] + i
+        return flat
+
+    def time_reversal(self, traces, c, receivers, dtype=np.float64):
+        """Dirichlet time reversal (nefi/physics/wave.py:878-968): from rest, the receivers' cells are
+        set to the traces at reversed time (linear in time between samples) after every step; the
+        cropped field after the last step estimates p0. numpy, all in ``dtype``."""
+        tr = np.asarray(traces, dtype=dtype)
+        n_t = tr.shape[-1]
+        m, N = self.m, self.N
+        C2 = self.c2dt2_f64(c).astype(dtype).reshape(self.P)
+        cells = self.nearest_cells(receivers)
+
+        def rev(n):
+            u = (n_t - 1) - n / m
+            j0 = min(max(int(math.floor(u)), 0), n_t - 1)
+            j1 = min(j0 + 1, n_t - 1)
+            t = u - j0
+            return dtype(1.0 - t) * tr[:, j0] + dtype(t) * tr[:, j1]
+
+        pp = np.zeros(self.P, dtype)
+        pc = np.zeros(self.P, dtype)
+        pc.reshape(-1)[cells] = rev(0)
+        A = None if self.A is None else np.asarray(self.A, dtype)
+        B = None if self.B is None else np.asarray(self.B, dtype)
+        psi = None
+        if self.pml is not None:
+            psi = [np.zeros((self.P[0] + 1, self.P[1]), dtype), np.zeros((self.P[0], self.P[1] + 1), dtype)]
+        for n in range(N):
+            L = self.laplacian(pc.reshape(1, -1), dtype).reshape(self.P)
+            if psi is not None:
+                new = []
+                for ax in range(2):
+                    pw = [(0, 0), (0, 0)]
+                    pw[ax] = (1, 1)
+                    ps = np.asarray(self.pml["alpha"][ax], dtype) * psi[ax] + \
+                        np.asarray(self.pml["beta"][ax], dtype) * np.diff(np.pad(pc, pw), axis=ax)
+                    L = L + np.diff(ps + psi[ax], axis=ax) * dtype(0.5 / self.h[ax])
+                    new.append(ps)
+                psi = new
+                rhs = (dtype(2) * pc - B * pp) + C2 * L - np.asarray(self.pml["zz"], dtype) * pc
+            else:
+                b = 1 if B is None or (self.first_b_one and n == 0) else B
+                rhs = (dtype(2) * pc - b * pp) + C2 * L
+            nxt = rhs if A is None else A * rhs
+            nxt.reshape(-1)[cells] = rev(n + 1)
+            pp, pc = pc, nxt
+        return self.crop(pc)
+
+    def c2dt2_f64(self, c):
+        """c^2 dt^2 of a fixed speed map, formed in float64 (nefi/physics/wave.py:814-820)."""
+        cp = self.pad(np.broadcast_to(np.asarray(c, dtype=np.float64), self.shape), "replicate")
+        return cp * cp * self.dt**2
+
     def c2dt2(self, c, dtype):
         cp = self.pad(np.asarray(c, dtype=dtype), "replicate")
         return (cp * cp) * dtype(self.dt**2)

@@ -32,7 +32,7 @@ sys.path.insert(0, str(REF))
 
 from nefi.domain import Domain  # noqa: E402
 from nefi.physics.timestep import run_timestepping  # noqa: E402
-from nefi.physics.wave import WaveInitialConditionOperator, WaveOperator, laplacian  # noqa: E402
+from nefi.physics.wave import WaveInitialConditionOperator, WaveOperator, laplacian, time_reversal  # noqa: E402
 
 F64, F32 = torch.float64, torch.float32
 
@@ -98,6 +98,23 @@ def pat_case(name, shape, extent, receivers, p0, c, kw, seed):
         out[f"grad_c_{tag}"] = gc.numpy()
         out["meta"] = {"substeps": op.substeps, "n_steps": op.n_steps, "dt": op.dt,
                        "padded": list(op.grid.padded_shape), "n_abs": list(op.grid.n_abs)}
+    save(name, out)
+
+
+def tr_case(name, shape, extent, receivers, traces, kw, seed):
+    """time_reversal(mode="dirichlet") of given traces (nefi/physics/wave.py:878-968)."""
+    if not wanted(name):
+        return
+    dom = Domain(shape, extent)
+    kw = dict(kw)
+    c = kw.pop("c")
+    c = c if isinstance(c, torch.Tensor) else torch.full(tuple(shape), float(c), dtype=F64)
+    out = {"kind": "tr", "shape": list(shape), "extent": [list(e) for e in extent],
+           "receivers": np.asarray(receivers, dtype=np.float64), "traces": traces.numpy(), "c": c.numpy(),
+           "kw": kw, "seed": seed, "rec_stride": 1}
+    for dt, tag in ((F64, "f64"), (F32, "f32")):
+        p0 = time_reversal(traces.to(dt), dom, receivers, mode="dirichlet", c=c, **kw)
+        out[f"p0_{tag}"] = p0.numpy()
     save(name, out)
 
 
@@ -179,6 +196,18 @@ def main():
              {**base, "n_t": 25, "order": 2, "absorbing": "pml", "absorb_width": 0.16, "courant": 0.8}, 11)
     pat_case("pat2d_o4_pml", (n2, n2), ((-1.0, 1.0), (-1.0, 1.0)), ring, p0, cpat,
              dict(n_t=50, dt_obs=0.03, order=4, absorbing="pml", absorb_width=0.25), 12)
+    # classical PAT baseline: Dirichlet time reversal of smooth seeded traces (2 substeps per sample)
+    gtr = torch.Generator().manual_seed(13)
+    tt = torch.linspace(0.0, 1.0, 40, dtype=F64)
+    trc = torch.stack([torch.sin(6.0 * tt + 2 * math.pi * torch.rand(1, generator=gtr, dtype=F64))
+                       * torch.exp(-3.0 * tt) for _ in range(32)])
+    tr_case("tr2d_o4_pml", (n2, n2), ((-1.0, 1.0), (-1.0, 1.0)), ring, trc,
+            dict(dt_obs=0.03, c=cpat, order=4, absorbing="pml", absorb_width=0.25), 13)
+    tr_case("tr2d_o2_sponge", (n2, n2), ((-1.0, 1.0), (-1.0, 1.0)), ring, trc,
+            dict(dt_obs=0.03, c=1.0, order=2, absorbing="sponge", absorb_width=0.25, courant=0.8), 14)
+    tr3 = torch.stack([torch.sin(5.0 * tt[:24] + 0.3 * k) * torch.exp(-2.0 * tt[:24]) for k in range(16)])
+    tr_case("tr3d_o2_sponge", (12, 12, 8), ((0.0, 3.0), (0.0, 3.0), (0.0, 2.0)), sens, tr3,
+            dict(dt_obs=0.1, c=c3, order=2, absorbing="sponge", absorb_width=0.75), 15)
 
 
 if __name__ == "__main__":

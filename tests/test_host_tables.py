@@ -25,7 +25,7 @@ def make_op(case):
                                             grad_mode="autograd", **case["kw"])
 
 
-@pytest.mark.parametrize("name", golden_names())
+@pytest.mark.parametrize("name", golden_names("fwi") + golden_names("pat"))
 def test_time_axis_and_padding_match_reference(name):
     case = load_golden(name)
     op = make_op(case)

@@ -68,3 +68,17 @@ def test_oracle_detects_a_planted_error():
     g = cotangent(full_trace_shape(case), case["seed"])
     tr, gc = orc.fwi(case["c"], g)
     assert rel_l2(gc, case["grad_c_f64"]) > 1e-9
+
+
+@pytest.mark.parametrize("name", golden_names("tr"))
+@pytest.mark.parametrize("dtype,tol", [(np.float64, 1e-12), (np.float32, 1e-5)])
+def test_oracle_time_reversal_matches_reference(name, dtype, tol):
+    import oracle
+
+    case = load_golden(name)
+    kw = dict(case["kw"])
+    orc = oracle.OracleWave(case["shape"], case["extent"], case["receivers"], n_t=case["traces"].shape[-1],
+                            c_max=float(np.max(case["c"])), **kw)
+    p0 = orc.time_reversal(case["traces"], case["c"], case["receivers"], dtype=dtype)
+    ref = case["p0_f64"] if dtype == np.float64 else case["p0_f32"]
+    assert rel_l2(p0, ref) < tol
