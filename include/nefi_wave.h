@@ -359,6 +359,20 @@ int nw_batch_forward(const nw_batch_problem* problems, int32_t n_problems, const
 int nw_batch_adjoint(const nw_batch_problem* problems, int32_t n_problems, const nw_tuning* tune,
                      const void* table, void* stream);
 
+/*
+ * Dirichlet time reversal of one trace set (time_reversal(mode="dirichlet"),
+ * nefi/physics/wave.py:878-968): starting from rest, the cells `cells` (n_cells distinct ghost-layout
+ * offsets, the receivers' nearest cells) hold the traces at reversed time T - n dt, linear in time
+ * between samples, at level 0 and after every step n; `traces` is (n_cells, time->n_t) in dtype.
+ * The acquisition describes one shot without sources (its receiver tables are not used). The call
+ * zeroes st->ring (and st->pml_psi with a PML) and leaves the estimate of p0 in ring level
+ * time->n_steps. This has no counterpart in the reference's operators; it replaces the time loop of
+ * its `time_reversal`.
+ */
+int nw_time_reversal(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, const nw_time* t,
+                     const nw_storage* st, const nw_tuning* tune, const int64_t* cells, int32_t n_cells,
+                     const void* traces, void* stream);
+
 /* Receiver samples of one level (n_shots fields) into traces[:, :, j]. */
 int nw_sample(const nw_grid* g, const nw_acquisition* a, int32_t n_t, const void* level,
               int32_t j, void* traces, void* stream);

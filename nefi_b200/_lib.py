@@ -104,6 +104,8 @@ _SIGNATURES = {
     "nw_adjoint_grad_c_noalloc": (C.c_int, [P(Grid), VP, P(Medium), P(Acquisition), P(Time), P(Storage),
                                             P(Tuning), VP, C.c_double, VP, VP, VP]),
     "nw_launch_count": (C.c_uint64, []),
+    "nw_time_reversal": (C.c_int, [P(Grid), P(Medium), P(Acquisition), P(Time), P(Storage), P(Tuning), VP,
+                                   C.c_int32, VP, VP]),
     "nw_batch_table_bytes": (C.c_size_t, [C.c_int32]),
     "nw_batch_prepare": (C.c_int, [P(BatchProblem), C.c_int32, P(Tuning), VP, VP]),
     "nw_batch_forward": (C.c_int, [P(BatchProblem), C.c_int32, P(Tuning), VP, VP]),

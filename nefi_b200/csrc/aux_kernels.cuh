@@ -108,6 +108,18 @@ __global__ void initial_prev_kernel(KGrid<T> g, int ndim, const T* __restrict__ 
   }
 }
 
+// Dirichlet condition of time reversal: lvl[cells[c]] = w0 traces[c, j0] + w1 traces[c, j1] (the
+// traces at a reversed time, linear between samples; products and sum rounded separately, as the
+// reference's scalar-times-tensor expression is).
+template <typename T>
+__global__ void dirichlet_kernel(T* __restrict__ lvl, const int64_t* __restrict__ cells, int n_cells,
+                                 const T* __restrict__ traces, int n_t, int j0, int j1, T w0, T w1) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n_cells) return;
+  const T* tr = traces + (long long)c * n_t;
+  lvl[cells[c]] = add_rn(mul_rn(w0, tr[j0]), mul_rn(w1, tr[j1]));
+}
+
 // mu = q / C on the padded grid of shot blockIdx.y (q = C mu is the variable the adjoint steps
 // advance). Ghost cells are left untouched (the caller zeroes them).
 template <typename T>

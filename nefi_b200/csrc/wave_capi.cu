@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cmath>
 #include <vector>
 #include <atomic>
 #include <cstdio>
@@ -1289,3 +1290,62 @@ int nw_batch_adjoint(const nw_batch_problem* problems, int32_t n_problems, const
 }
 
 }  // extern "C"
+
+// =============================================================================================
+// Dirichlet time reversal: the forward step loop with the receivers' cells overwritten after
+// every step.
+// =============================================================================================
+namespace {
+
+template <typename T>
+int time_reversal_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, const nw_time* t,
+                       const nw_storage* st, const Tune& tu, const int64_t* cells, int n_cells, const T* traces,
+                       cudaStream_t s) {
+  const long long LE = g->field_elems;
+  const int N = t->n_steps, M = t->substeps, n_t = t->n_t;
+  NW_CUDA(cudaMemsetAsync(st->ring, 0, 3 * (size_t)LE * sizeof(T), s));
+  if (g->absorbing == NW_ABS_PML) NW_CUDA(cudaMemsetAsync(st->pml_psi, 0, 4 * (size_t)LE * sizeof(T), s));
+  Ring<T> L;
+  L.base = (T*)st->ring;
+  L.level_elems = LE;
+  const nw::KGrid<T> kg = kgrid<T>(g);
+  auto impose = [&](int n) -> int {  // the traces at reversed time T - n dt on level n
+    const double u = (n_t - 1) - (double)n / M;
+    const int j0 = std::min(std::max((int)std::floor(u), 0), n_t - 1);
+    const int j1 = std::min(j0 + 1, n_t - 1);
+    const double w = u - j0;
+    nw::dirichlet_kernel<T><<<(n_cells + 127) / 128, 128, 0, s>>>(L.at(n), cells, n_cells, traces, n_t, j0, j1,
+                                                                 (T)(1.0 - w), (T)w);
+    NW_LAUNCHED();
+    return NW_OK;
+  };
+  int rc = impose(0);
+  if (rc) return rc;
+  for (int n = 0; n < N; ++n) {
+    rc = forward_step<T>(g, kg, m, a, t, tu, L, n, nullptr, nullptr, s, (T*)st->pml_psi);
+    if (rc) return rc;
+    rc = impose(n + 1);
+    if (rc) return rc;
+  }
+  return NW_OK;
+}
+
+}  // namespace
+
+extern "C" int nw_time_reversal(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, const nw_time* t,
+                                const nw_storage* st, const nw_tuning* tune, const int64_t* cells, int32_t n_cells,
+                                const void* traces, void* stream) {
+  int rc = check_grid(g);
+  if (rc) return rc;
+  Tune tu;
+  rc = resolve_tune(g, tune, &tu);
+  if (rc) return rc;
+  rc = check_run(g, m, a, t, st, tu);
+  if (rc) return rc;
+  if (a->n_shots != 1 || a->has_source) return fail(NW_ERR_ARG, "time reversal runs one shot without sources");
+  if (!st->ring || (g->absorbing == NW_ABS_PML && !st->pml_psi)) return fail(NW_ERR_ARG, "time reversal needs the ring (and pml_psi with a PML)");
+  if (n_cells < 1 || !cells || !traces) return fail(NW_ERR_ARG, "time reversal needs receiver cells and traces");
+  if (g->dtype == NW_F32)
+    return time_reversal_impl<float>(g, m, a, t, st, tu, cells, n_cells, (const float*)traces, (cudaStream_t)stream);
+  return time_reversal_impl<double>(g, m, a, t, st, tu, cells, n_cells, (const double*)traces, (cudaStream_t)stream);
+}

@@ -181,3 +181,14 @@ def test_attributes_mirror_reference_operator():
     pat = WaveInitialConditionOperatorB200(dom, rec, n_t=20, dt_obs=0.01, absorbing="sponge")
     assert pat.homogeneity == 1.0 and pat.fidelity_tag == "wave-leapfrog-ic-o4-sponge"
     assert pat.output_shape((32, 32)) == (6, 20)
+
+
+def test_time_reversal_refuses_host_traces():
+    """The baseline runs on the device only: host traces are an error, never a CPU fallback."""
+    from nefi_b200 import time_reversal
+
+    case = load_golden("tr2d_o4_pml")
+    dom = Domain(tuple(case["shape"]), tuple(tuple(e) for e in case["extent"]))
+    for mode in ("dirichlet", "adjoint"):
+        with pytest.raises(ConfigError):
+            time_reversal(torch.tensor(case["traces"]), dom, case["receivers"], dt_obs=0.03, mode=mode)
