@@ -47,8 +47,8 @@ def time_reversal(traces, domain, receivers, *, dt_obs: float, c=1.0, mode: str 
             (grad,) = torch.autograd.grad((op({"p0": p0}) * tr).sum(), p0)
         return grad
     op._check_device(tr, "traces")
-    if tr.shape[0] != op.n_receivers:
-        raise ShapeError(f"traces have {tr.shape[0]} rows for {op.n_receivers} receivers")
+    if tr.shape[0] != op.receivers.shape[0]:
+        raise ShapeError(f"traces have {tr.shape[0]} rows for {op.receivers.shape[0]} receivers")
     plan = op._plan(device, dtype)
     _, c2dt2 = op._known_speed(device, dtype)
     medium = plan.medium(c2dt2)
