@@ -300,6 +300,105 @@ def run_pat(args) -> None:
     print(json.dumps(out), flush=True)
 
 
+def run_datagen(args) -> None:
+    """FP64 data generation on the device (the DataGenerator path, nefi/bench/base.py:74-90): the
+    512^2 workload's operator moved to float64 and called through ``at_resolution`` with the ground
+    truth on the 2x-refined 1024^2 grid (2 substeps per sample), all shots, no gradient. One step =
+    the traces of every shot. The CPU baseline is the float64 oracle on a bounded sample."""
+    from nefi_b200 import WaveOperatorB200, _lib
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    args.workload = "fwi_512"
+    w = make_workload(args)
+    op = WaveOperatorB200(w.domain, w.sources, w.receivers, **w.operator_kwargs()).to(device=dev, dtype=torch.float64)
+    fine_n = 2 * w.n
+    c_fine = torch.nn.functional.interpolate(torch.tensor(w.c, dtype=torch.float64)[None, None], size=(fine_n, fine_n),
+                                             mode="bilinear", align_corners=False)[0, 0]
+    gen = op.at_resolution((fine_n, fine_n))
+    c_dev = c_fine.to(dev)
+    flush = torch.empty(64 * 2**20, dtype=torch.float32, device=dev)
+
+    def step(cc):
+        with torch.no_grad():
+            return gen({"c": cc})
+
+    for _ in range(args.warmup):
+        step(c_dev)
+    torch.cuda.synchronize()
+    lib = _lib.load()
+    l0 = lib.nw_launch_count()
+    sampler = ClockSampler(dev.index)
+    times = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        tr = step(c_dev)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    clocks = sampler.stop()
+    launches = lib.nw_launch_count() - l0
+    ms = statistics.median(times)
+    S = len(w.sources)
+    P = gen.grid.padded_shape
+    cells = P[0] * P[1]
+    N = gen.n_steps
+    peak, peak_kind = peaks()
+    alg = 32.0 * cells * S  # float64: read p^n, p^n-1, c^2 dt^2, write p^n+1
+    achieved = alg / (ms / N * 1e-3) / 1e9
+    # end to end: ground truth in from pinned host memory, every trace back to pinned host memory
+    c_h = c_fine.pin_memory()
+    tr_h = torch.empty(tr.shape, dtype=torch.float64).pin_memory()
+    e2e = []
+    for i in range(1 + args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = step(c_h.to(dev, non_blocking=True))
+        tr_h.copy_(out, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        if i:
+            e2e.append(e0.elapsed_time(e1))
+    cpu = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle  # noqa: E402  (the checker, used here only as the timed CPU baseline)
+
+        oracle.set_threads(os.cpu_count() or 1)
+        ns, nst = 2, 400
+        kw = dict(w.operator_kwargs())
+        kw["n_t"] = nst // 2 + 1
+        L = w.n * w.h
+        orc = oracle.OracleWave((fine_n, fine_n), ((0.0, L), (0.0, L)), w.receivers, sources=w.sources[:ns], **kw)
+        t0 = time.perf_counter()
+        orc.fwi(c_fine.numpy(), None, dtype=np.float64)
+        t = time.perf_counter() - t0
+        steps_done = (kw["n_t"] - 1) * gen.substeps
+        v = 1.0 / (t / ns * N / steps_done)
+        cpu = {"value": v, "unit": "shot-generations/s", "cores": min(os.cpu_count() or 1, ns), "kind": "port",
+               "sample": f"{ns} shots x {steps_done} of {N} steps, float64 forward on the {P[0]}^2 padded grid; "
+                         "extrapolated linearly in steps",
+               "gcell_updates_per_s": cells * steps_done * ns / t / 1e9}
+    out = {"metric": METRIC, "value": S / (ms * 1e-3), "unit": "shot-generations/s", "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded layered model, bilinear 2x ground truth)",
+           "config": {"workload": f"datagen_512x2: fwi_512 operator (16 shots, 512 receivers, Ricker 10 Hz) generating "
+                                  f"float64 traces from a {fine_n}^2 ground truth ({P[0]}^2 padded, {N} steps, "
+                                  f"{gen.substeps} substeps per sample), forward only",
+                      "l2": "256 MiB buffer written between timed steps; working set far above L2"},
+           "gcell_updates_per_s": cells * N * S / (ms * 1e-3) / 1e9,
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "traffic": None, "kernel": "fwd2d<double>", "peak_source": peak_kind,
+                        "note": "32 B per float64 cell-update; launch time = step time / steps (injection included)"},
+           "cpu_baseline": cpu,
+           "e2e": {"value": S / (statistics.median(e2e) * 1e-3), "unit": "shot-generations/s",
+                   "h2d_bytes_per_step": c_h.numel() * 8, "d2h_bytes_per_step": tr_h.numel() * 8},
+           "clocks": clocks, "gpu_launches": int(launches)}
+    print(json.dumps(out), flush=True)
+
+
 def run_reference(args) -> None:
     from nefi_b200 import workloads
 
@@ -357,6 +456,9 @@ def main() -> None:
         return
     if args.workload == "pat_256":
         run_pat(args)
+        return
+    if args.workload == "datagen_512x2":
+        run_datagen(args)
         return
 
     import torch.distributed as dist

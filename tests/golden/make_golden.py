@@ -118,6 +118,24 @@ def tr_case(name, shape, extent, receivers, traces, kw, seed):
     save(name, out)
 
 
+def gen_case(name, shape, extent, sources, receivers, c_fine, kw, factor):
+    """FP64 data generation as ``DataGenerator.clean`` does it (nefi/bench/base.py:74-90): an operator
+    built on the native grid, moved to float64, called through ``at_resolution`` with the ground truth
+    on the ``factor``-times refined grid (the 2x-supersampled wave_fwi generator,
+    nefi/instances/wave_fwi/__init__.py:248-260)."""
+    if not wanted(name):
+        return
+    dom = Domain(shape, extent)
+    op = WaveOperator(dom, sources, receivers, **kw).to(dtype=F64)
+    fine = tuple(int(s) * factor for s in shape)
+    with torch.no_grad():
+        tr = op.at_resolution(fine)({"c": c_fine.to(F64)})
+    out = {"kind": "gen", "shape": list(shape), "fine": list(fine), "extent": [list(e) for e in extent],
+           "sources": np.asarray(sources, dtype=np.float64), "receivers": np.asarray(receivers, dtype=np.float64),
+           "c": c_fine.numpy(), "kw": kw, "seed": 0, "rec_stride": 1, "traces_f64": tr.numpy()}
+    save(name, out)
+
+
 def wanted(name):
     return not ONLY or name.startswith(ONLY)
 
@@ -208,6 +226,13 @@ def main():
     tr3 = torch.stack([torch.sin(5.0 * tt[:24] + 0.3 * k) * torch.exp(-2.0 * tt[:24]) for k in range(16)])
     tr_case("tr3d_o2_sponge", (12, 12, 8), ((0.0, 3.0), (0.0, 3.0), (0.0, 2.0)), sens, tr3,
             dict(dt_obs=0.1, c=c3, order=2, absorbing="sponge", absorb_width=0.75), 15)
+    # FP64 data generation at 2x supersampling through at_resolution (order-4 generator, both layers)
+    cf = (2.0 + 0.2 * torch.randn(40, 48, generator=torch.Generator().manual_seed(16), dtype=F64)).clamp(1.6, 2.4)
+    cf = torch.nn.functional.avg_pool2d(cf[None, None], 3, 1, 1, count_include_pad=False)[0, 0]
+    gen_case("gen2x_o4_pml", (20, 24), ext, src, rec, cf, {**base, "order": 4, "absorbing": "pml",
+                                                            "absorb_width": 0.2}, 2)
+    gen_case("gen2x_o4_sponge", (20, 24), ext, src, rec, cf, {**base, "order": 4, "absorbing": "sponge",
+                                                               "absorb_width": 0.2}, 2)
 
 
 if __name__ == "__main__":

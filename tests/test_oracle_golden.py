@@ -82,3 +82,15 @@ def test_oracle_time_reversal_matches_reference(name, dtype, tol):
     p0 = orc.time_reversal(case["traces"], case["c"], case["receivers"], dtype=dtype)
     ref = case["p0_f64"] if dtype == np.float64 else case["p0_f32"]
     assert rel_l2(p0, ref) < tol
+
+
+@pytest.mark.parametrize("name", golden_names("gen"))
+def test_oracle_supersampled_generation_matches_reference(name):
+    """FP64 data generation on the refined grid (the operator's ``at_resolution``)."""
+    import oracle
+
+    case = load_golden(name)
+    orc = oracle.OracleWave(case["fine"], case["extent"], case["receivers"], sources=case["sources"], **case["kw"])
+    g = np.zeros(case["traces_f64"].shape)
+    tr, _ = orc.fwi(case["c"], g, dtype=np.float64)
+    assert rel_l2(tr, case["traces_f64"]) < 1e-12
