@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define NW_ABI_VERSION 3
+#define NW_ABI_VERSION 4
 
 /* scalar type of a computation */
 enum { NW_F32 = 0, NW_F64 = 1 };
@@ -376,6 +376,71 @@ int nw_time_reversal(const nw_grid* g, const nw_medium* m, const nw_acquisition*
 /* Receiver samples of one level (n_shots fields) into traces[:, :, j]. */
 int nw_sample(const nw_grid* g, const nw_acquisition* a, int32_t n_t, const void* level,
               int32_t j, void* traces, void* stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * Trace misfit: the band-limited relative MSE of FWI (BandLimitedMSE with `lowpass`,
+ * nefi/instances/wave_fwi/losses.py:28-86), the sensors' Gaussian response of photoacoustics
+ * (gaussian_lowpass, nefi/instances/photoacoustic3d/sensor.py:24-66) and the masked mean of a
+ * measurement (nefi/measurement.py:86-91), fused with the adjoint source they feed.
+ *
+ * Traces are (n_traces, n_t) arrays of dtype, row-major, on the device. A filter is passed as its
+ * response: nw_filter_response() writes it on the host (2^log2_len values of dtype, from the
+ * reference's own window in float64); copy it to the device once. Every call is asynchronous on
+ * `stream`; a state array is one caller-owned device buffer of NW_MISFIT_STATE doubles, and calls
+ * that share one state must not overlap on the device.
+ * ------------------------------------------------------------------------------------------- */
+enum { NW_FILTER_LOWPASS = 0, NW_FILTER_GAUSSIAN = 1 };
+#define NW_MISFIT_STATE 2056 /* doubles of a misfit state array */
+#define NW_MISFIT_COUNT 2048 /* state slot: the number of observed samples (mask sum) */
+#define NW_MISFIT_DEN 2049   /* state slot: masked_mean((W obs)^2) clamped to 1e-30 (1 if not relative) */
+#define NW_MISFIT_SCALE 2050 /* state slot: 2 / (count * den), the factor of the adjoint source */
+#define NW_MISFIT_SUM 2051   /* state slot: accumulated sum of mask * (W r)^2 */
+#define NW_MISFIT_LOSS 2052  /* state slot: the loss, sum / count / den */
+
+typedef struct nw_traces {
+  int32_t dtype;           /* NW_F32 or NW_F64 */
+  int32_t n_t;             /* samples per trace */
+  int64_t n_traces;        /* rows */
+  const void* mask;        /* NULL, or observation weights of dtype: one per trace or one per sample */
+  int32_t mask_per_sample; /* 0: mask[n_traces]; 1: mask[n_traces * n_t] */
+  int32_t log2_len;        /* nw_filter_log2_len(n_t) when a filter is passed (else ignored) */
+} nw_traces;
+
+/* Filter length exponent for traces of n_t samples: the smallest k >= 6 with 2^k >= 2 n_t. Filtered
+ * traces are limited to 8192 samples in float32 and 4096 in float64 (the FFT stays in shared memory). */
+int nw_filter_log2_len(int32_t n_t);
+
+/*
+ * Host: the response of a zero-phase filter on traces of n_t samples at interval dt, written to
+ * `out` (host memory, 2^nw_filter_log2_len(n_t) values of dtype). NW_FILTER_LOWPASS: flat to
+ * (1 - taper) f, cosine roll-off to 0 at f (`_window`/`lowpass`, losses.py:28-48, FFT length
+ * next_fast_len(2 n_t)); NW_FILTER_GAUSSIAN: exp(-(freq / f)^2 / 2) (`gaussian_lowpass`,
+ * sensor.py:24-38, FFT length 2 n_t; taper unused).
+ */
+int nw_filter_response(int32_t kind, int32_t n_t, double dt, double f, double taper, int32_t dtype, void* out);
+
+/* y = the filter `response` applied to every trace of x (lowpass(x) / gaussian_lowpass(x)); the
+ * filter is its own adjoint, so the same call maps an output cotangent to the input's. */
+int nw_trace_filter(const nw_traces* t, const void* x, const void* response, void* y, void* stream);
+
+/*
+ * Once per observed data set: the sample count (mask sum) and, when `relative`, the normaliser
+ * masked_mean((W obs)^2) (W = loss_response, or the identity when NULL) go into `state`, with the
+ * adjoint-source scale and a zero misfit sum. `t` describes the whole observed set.
+ */
+int nw_misfit_prepare(const nw_traces* t, const void* obs, const void* loss_response, int32_t relative,
+                      double* state, void* stream);
+
+/*
+ * One pass over predicted traces (a whole set or a slice of rows of the prepared one):
+ *   r = G pred - obs (G = sensor_response, identity when NULL), r_f = W r (W = loss_response),
+ *   state[NW_MISFIT_SUM] += sum(mask * r_f^2), state[NW_MISFIT_LOSS] = SUM / COUNT / DEN,
+ *   grad = SCALE * G W (mask * r_f)  (= dLoss/dpred; skipped when grad is NULL).
+ * One launch plus a one-warp reduction; the partial sums are reduced in a fixed order, so results are
+ * bitwise reproducible. Replaces BandLimitedMSE.forward (losses.py:78-86) and its autograd backward.
+ */
+int nw_misfit(const nw_traces* t, const void* pred, const void* obs, const void* sensor_response,
+              const void* loss_response, double* state, void* grad, void* stream);
 
 /*
  * Synchronises `stream`, then returns and clears the device status word that kernels set on a

@@ -26,6 +26,7 @@ try:  # the reference package is present: bind to it
         ShapeError,
         SolverError,
     )
+    from nefi.losses.data import DataLoss  # type: ignore
     from nefi.operators.base import Operator  # type: ignore
     from nefi.registry import register  # type: ignore
 
@@ -127,6 +128,25 @@ except Exception:  # pragma: no cover - exercised where nefi is absent
                 axes.append(lo + (i + 0.5) * (hi - lo) / n)
             return torch.stack(torch.meshgrid(*axes, indexing="ij"), dim=-1)
 
+    class Loss(nn.Module):
+        """A scalar loss term (mirror of ``nefi.losses.base.Loss``, nefi/losses/base.py:53-69)."""
+
+        is_data: bool = False
+        step_dependent: bool = False
+
+        def __init__(self, name: str | None = None) -> None:
+            super().__init__()
+            self.name = name or type(self).__name__.lower()
+
+    class DataLoss(Loss):
+        """A data-fidelity term (mirror of ``nefi.losses.data.DataLoss``, nefi/losses/data.py:32-45)."""
+
+        is_data = True
+
+        def __init__(self, name: str | None = None, noise_aware: bool = False) -> None:
+            super().__init__(name)
+            self.noise_aware = noise_aware
+
     def register(kind: str, name: str | None = None):
         """No registry without NEFI: the decorator returns the class unchanged."""
 
@@ -173,6 +193,7 @@ def resample(x: torch.Tensor, shape: Sequence[int]) -> torch.Tensor:
 __all__ = [
     "HAVE_NEFI",
     "ConfigError",
+    "DataLoss",
     "Domain",
     "NefiError",
     "Operator",

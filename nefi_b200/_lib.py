@@ -13,7 +13,7 @@ from pathlib import Path
 import torch
 
 LIB_PATH = Path(__file__).resolve().parent / "libnefiwave.so"
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 NW_F32, NW_F64 = 0, 1
 NW_ABS_NONE, NW_ABS_SPONGE, NW_ABS_CERJAN, NW_ABS_PML = 0, 1, 2, 3
@@ -79,6 +79,15 @@ class BatchProblem(C.Structure):
                 ("traces", C.c_void_p), ("grad_traces", C.c_void_p)]
 
 
+class Traces(C.Structure):
+    _fields_ = [("dtype", C.c_int32), ("n_t", C.c_int32), ("n_traces", C.c_int64), ("mask", C.c_void_p),
+                ("mask_per_sample", C.c_int32), ("log2_len", C.c_int32)]
+
+
+NW_FILTER_LOWPASS, NW_FILTER_GAUSSIAN = 0, 1
+NW_MISFIT_STATE, NW_MISFIT_COUNT, NW_MISFIT_DEN, NW_MISFIT_SCALE, NW_MISFIT_SUM, NW_MISFIT_LOSS = (
+    2056, 2048, 2049, 2050, 2051, 2052)
+
 P = C.POINTER
 VP = C.c_void_p
 _SIGNATURES = {
@@ -106,6 +115,11 @@ _SIGNATURES = {
     "nw_launch_count": (C.c_uint64, []),
     "nw_time_reversal": (C.c_int, [P(Grid), P(Medium), P(Acquisition), P(Time), P(Storage), P(Tuning), VP,
                                    C.c_int32, VP, VP]),
+    "nw_filter_log2_len": (C.c_int, [C.c_int32]),
+    "nw_filter_response": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_int32, VP]),
+    "nw_trace_filter": (C.c_int, [P(Traces), VP, VP, VP, VP]),
+    "nw_misfit_prepare": (C.c_int, [P(Traces), VP, VP, C.c_int32, VP, VP]),
+    "nw_misfit": (C.c_int, [P(Traces), VP, VP, VP, VP, VP, VP, VP]),
     "nw_batch_table_bytes": (C.c_size_t, [C.c_int32]),
     "nw_batch_prepare": (C.c_int, [P(BatchProblem), C.c_int32, P(Tuning), VP, VP]),
     "nw_batch_forward": (C.c_int, [P(BatchProblem), C.c_int32, P(Tuning), VP, VP]),

@@ -18,6 +18,7 @@
 #include "../../include/nefi_wave.h"
 #include "aux_kernels.cuh"
 #include "kernels.cuh"
+#include "misfit.cuh"
 #include "pml2d.cuh"
 #include "stencil2d.cuh"
 #include "stencil3d.cuh"
@@ -1348,4 +1349,300 @@ extern "C" int nw_time_reversal(const nw_grid* g, const nw_medium* m, const nw_a
   if (g->dtype == NW_F32)
     return time_reversal_impl<float>(g, m, a, t, st, tu, cells, n_cells, (const float*)traces, (cudaStream_t)stream);
   return time_reversal_impl<double>(g, m, a, t, st, tu, cells, n_cells, (const double*)traces, (cudaStream_t)stream);
+}
+
+// ------------------------------------------------------------------------------------------------
+// trace misfit: band-limited residual, masked mean square, adjoint source
+// ------------------------------------------------------------------------------------------------
+namespace {
+
+int smallest_5smooth(int n) {  // scipy.fft.next_fast_len(n, real=True): the next 2^a 3^b 5^c >= n
+  for (int m = std::max(n, 1);; ++m) {
+    int r = m;
+    for (int p : {2, 3, 5})
+      while (r % p == 0) r /= p;
+    if (r == 1) return m;
+  }
+}
+
+int filter_log2_len(int n_t) {
+  int k = 6;
+  while ((1LL << k) < 2LL * n_t) ++k;
+  return k;
+}
+
+// In-place radix-2 complex FFT (forward, float64) of length 2^k: iterative, bit-reversed input order.
+void host_fft(std::vector<double>& re, std::vector<double>& im) {
+  const size_t L = re.size();
+  for (size_t i = 1, j = 0; i < L; ++i) {
+    size_t bit = L >> 1;
+    for (; j & bit; bit >>= 1) j ^= bit;
+    j ^= bit;
+    if (i < j) {
+      std::swap(re[i], re[j]);
+      std::swap(im[i], im[j]);
+    }
+  }
+  for (size_t len = 2; len <= L; len <<= 1) {
+    const size_t half = len >> 1;
+    for (size_t k = 0; k < half; ++k) {
+      const double a = -2.0 * M_PI * (double)k / (double)len;
+      const double wr = std::cos(a), wi = std::sin(a);
+      for (size_t b = 0; b < L; b += len) {
+        const size_t i = b + k, j = i + half;
+        const double xr = re[j] * wr - im[j] * wi, xi = re[j] * wi + im[j] * wr;
+        re[j] = re[i] - xr;
+        im[j] = im[i] - xi;
+        re[i] += xr;
+        im[i] += xi;
+      }
+    }
+  }
+}
+
+// Hp[p] = H_L[bitrev(p)] / L for the reference's filter of `kind` on traces of n_t samples, float64.
+int filter_response(int kind, int n_t, double dt, double f, double taper, std::vector<double>* out) {
+  if (n_t < 1 || !(dt > 0.0) || !(f > 0.0)) return fail(NW_ERR_ARG, "filter response needs n_t >= 1, dt > 0, f > 0");
+  if (kind != NW_FILTER_LOWPASS && kind != NW_FILTER_GAUSSIAN) return fail(NW_ERR_ARG, "unknown filter kind");
+  if (kind == NW_FILTER_LOWPASS && !(taper >= 0.0 && taper <= 1.0)) return fail(NW_ERR_ARG, "taper must be in [0, 1]");
+  // the reference's FFT length and half spectrum (losses.py:28-48; sensor.py:33-38)
+  const int N = kind == NW_FILTER_LOWPASS ? smallest_5smooth(2 * n_t) : 2 * n_t;
+  const int J = N / 2;
+  std::vector<double> w(J + 1);
+  const double f1 = (1.0 - taper) * f;
+  for (int j = 0; j <= J; ++j) {
+    const double fj = (double)j / ((double)N * dt);
+    if (kind == NW_FILTER_GAUSSIAN) {
+      w[j] = std::exp(-0.5 * (fj / f) * (fj / f));
+    } else {
+      double v = 1.0;
+      if (fj > f1 && fj < f) v = 0.5 * (1.0 + std::cos(M_PI * (fj - f1) / std::max(f - f1, 1e-30)));
+      if (fj >= f) v = 0.0;
+      w[j] = v;
+    }
+  }
+  // impulse response h = irfft(w, N) at lags 0..n_t-1 (it is even: h[N - k] = h[k])
+  std::vector<double> ct(N);
+  for (int m = 0; m < N; ++m) ct[m] = std::cos(2.0 * M_PI * (double)m / (double)N);
+  const int M = (N % 2 == 0) ? J - 1 : J;
+  std::vector<double> h(n_t);
+  for (int k = 0; k < n_t; ++k) {
+    double acc = 0.0;
+    long long idx = 0;
+    for (int j = 1; j <= M; ++j) {
+      idx += k;
+      if (idx >= N) idx %= N;
+      acc += w[j] * ct[idx];
+    }
+    double v = w[0] + 2.0 * acc;
+    if (N % 2 == 0) v += w[J] * ((k & 1) ? -1.0 : 1.0);
+    h[k] = v / (double)N;
+  }
+  // the same lags on a power-of-two circle, its spectrum (real: the response is even), bit-reversed
+  const int k2 = filter_log2_len(n_t);
+  const size_t L = (size_t)1 << k2;
+  std::vector<double> re(L, 0.0), im(L, 0.0);
+  re[0] = h[0];
+  for (int k = 1; k < n_t; ++k) re[k] = re[L - k] = h[k];
+  host_fft(re, im);
+  out->assign(L, 0.0);
+  for (size_t p = 0; p < L; ++p) {
+    size_t r = 0;
+    for (int b = 0; b < k2; ++b)
+      if (p & ((size_t)1 << b)) r |= (size_t)1 << (k2 - 1 - b);
+    (*out)[p] = re[r] / (double)L;
+  }
+  return NW_OK;
+}
+
+int check_traces(const nw_traces* t) {
+  if (!t) return fail(NW_ERR_ARG, "traces descriptor is NULL");
+  if (t->dtype != NW_F32 && t->dtype != NW_F64) return fail(NW_ERR_ARG, "dtype must be NW_F32 or NW_F64");
+  if (t->n_t < 1 || t->n_traces < 0) return fail(NW_ERR_ARG, "traces need n_t >= 1 and n_traces >= 0");
+  if (t->mask_per_sample != 0 && t->mask_per_sample != 1) return fail(NW_ERR_ARG, "mask_per_sample must be 0 or 1");
+  return NW_OK;
+}
+
+int check_filter_len(const nw_traces* t) {
+  const int want = filter_log2_len(t->n_t);
+  if (t->log2_len != want) return fail(NW_ERR_ARG, "log2_len must be nw_filter_log2_len(n_t)");
+  const int cap = t->dtype == NW_F32 ? 14 : 13;
+  if (t->log2_len > cap)
+    return fail(NW_ERR_UNSUPPORTED, t->dtype == NW_F32 ? "filtered traces are limited to 8192 samples in float32"
+                                                       : "filtered traces are limited to 4096 samples in float64");
+  return NW_OK;
+}
+
+template <typename T>
+int run_misfit_program(const nw_traces* t, nw::MisfitArgs<T> a, cudaStream_t s, int* ctas) {
+  a.n_traces = t->n_traces;
+  a.n_t = t->n_t;
+  a.mask = (const T*)t->mask;
+  a.mask_per_sample = t->mask_per_sample;
+  int n_ctas = 1;
+  if (a.n_filters == 0) {
+    const long long N = t->n_traces * (long long)t->n_t;
+    n_ctas = (int)std::max(1LL, std::min<long long>(nw::kMisfitCtas, (N + 255) / 256));
+    if (N > 0) {
+      nw::misfit_plain_kernel<T><<<n_ctas, 256, 0, s>>>(a);
+      NW_LAUNCHED();
+    } else if (a.partials) {
+      NW_CUDA(cudaMemsetAsync(a.partials, 0, 2 * sizeof(double), s));
+    }
+    *ctas = n_ctas;
+    return NW_OK;
+  }
+  const nw::fft::Groups G = nw::fft::make_groups(t->log2_len);
+  const int L = 1 << t->log2_len;
+  const size_t smem = (size_t)(G.tab_len + nw::fft::slot(L - 1) + 1) * sizeof(typename nw::fft::Cx<T>::t);
+  const int threads = std::min(512, std::max(32, L >> 4));
+  auto kern = nw::misfit_fft_kernel<T>;
+  NW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int dev = 0, sms = 0, per_sm = 0;
+  NW_CUDA(cudaGetDevice(&dev));
+  NW_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  NW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
+  const long long pairs = (t->n_traces + 1) / 2;
+  n_ctas = (int)std::max(1LL, std::min<long long>({(long long)nw::kMisfitCtas, pairs,
+                                                   (long long)std::max(1, per_sm) * sms}));
+  if (pairs > 0) {
+    kern<<<n_ctas, threads, smem, s>>>(a, G);
+    NW_LAUNCHED();
+  } else if (a.partials) {
+    NW_CUDA(cudaMemsetAsync(a.partials, 0, 2 * sizeof(double), s));
+  }
+  *ctas = n_ctas;
+  return NW_OK;
+}
+
+template <typename T>
+int misfit_prepare_impl(const nw_traces* t, const void* obs, const void* loss_response, int relative, double* state,
+                        cudaStream_t s) {
+  nw::MisfitArgs<T> a{};
+  a.obs = (const T*)obs;
+  a.partials = state;
+  a.state = nullptr;
+  const bool filtered = relative && loss_response;
+  a.n_filters = filtered ? 1 : 0;
+  if (filtered) {
+    a.spec[0] = (const T*)loss_response;
+    a.op[0] = nw::MF_LOAD_OBS;
+    a.op[1] = nw::MF_LOSS | nw::MF_END;
+  } else {
+    a.op[0] = nw::MF_LOAD_OBS | nw::MF_LOSS;
+  }
+  int n_ctas = 0;
+  const int rc = run_misfit_program<T>(t, a, s, &n_ctas);
+  if (rc) return rc;
+  const double count = t->mask ? 0.0 : (double)t->n_traces * (double)t->n_t;
+  nw::misfit_finalize_kernel<<<1, 32, 0, s>>>(state, n_ctas, 1, relative ? 1 : 0, count);
+  NW_LAUNCHED();
+  return NW_OK;
+}
+
+template <typename T>
+int misfit_impl(const nw_traces* t, const void* pred, const void* obs, const void* sensor, const void* loss,
+                double* state, void* grad, cudaStream_t s) {
+  nw::MisfitArgs<T> a{};
+  a.pred = (const T*)pred;
+  a.obs = (const T*)obs;
+  a.grad = (T*)grad;
+  a.state = state;
+  a.partials = state;
+  const unsigned store = grad ? nw::MF_STORE : nw::MF_END;
+  int f = 0;
+  if (sensor) {  // r = G pred - obs
+    a.spec[f++] = (const T*)sensor;
+    a.op[0] = nw::MF_LOAD_PRED;
+    a.op[1] = nw::MF_SUB_OBS;
+  } else {
+    a.op[0] = nw::MF_LOAD_PRED | nw::MF_SUB_OBS;
+  }
+  if (loss) {
+    a.spec[f++] = (const T*)loss;  // r_f = W r; sum m r_f^2; x = m r_f
+    a.op[f] |= nw::MF_LOSS;
+    if (grad) {
+      a.spec[f++] = (const T*)loss;  // W^T = W
+    }
+  } else {
+    a.op[f] |= nw::MF_LOSS;
+  }
+  if (sensor && grad) a.spec[f++] = (const T*)sensor;  // G^T = G
+  a.n_filters = f;
+  a.op[f] |= store;
+  int n_ctas = 0;
+  const int rc = run_misfit_program<T>(t, a, s, &n_ctas);
+  if (rc) return rc;
+  nw::misfit_finalize_kernel<<<1, 32, 0, s>>>(state, n_ctas, 0, 0, 0.0);
+  NW_LAUNCHED();
+  return NW_OK;
+}
+
+template <typename T>
+int filter_impl(const nw_traces* t, const void* x, const void* response, void* y, cudaStream_t s) {
+  nw::MisfitArgs<T> a{};
+  a.pred = (const T*)x;
+  a.grad = (T*)y;
+  a.spec[0] = (const T*)response;
+  a.n_filters = 1;
+  a.op[0] = nw::MF_LOAD_PRED;
+  a.op[1] = nw::MF_STORE;
+  int n_ctas = 0;
+  return run_misfit_program<T>(t, a, s, &n_ctas);
+}
+
+}  // namespace
+
+extern "C" int nw_filter_log2_len(int32_t n_t) { return n_t < 1 ? fail(NW_ERR_ARG, "n_t must be >= 1") : filter_log2_len(n_t); }
+
+extern "C" int nw_filter_response(int32_t kind, int32_t n_t, double dt, double f, double taper, int32_t dtype,
+                                  void* out) {
+  if (!out) return fail(NW_ERR_ARG, "out is NULL");
+  if (dtype != NW_F32 && dtype != NW_F64) return fail(NW_ERR_ARG, "dtype must be NW_F32 or NW_F64");
+  std::vector<double> hp;
+  const int rc = filter_response(kind, n_t, dt, f, taper, &hp);
+  if (rc) return rc;
+  for (size_t i = 0; i < hp.size(); ++i) {
+    if (dtype == NW_F32) ((float*)out)[i] = (float)hp[i];
+    else ((double*)out)[i] = hp[i];
+  }
+  return NW_OK;
+}
+
+extern "C" int nw_trace_filter(const nw_traces* t, const void* x, const void* response, void* y, void* stream) {
+  int rc = check_traces(t);
+  if (rc) return rc;
+  if (!x || !response || !y) return fail(NW_ERR_ARG, "trace filter needs x, response and y");
+  rc = check_filter_len(t);
+  if (rc) return rc;
+  if (t->dtype == NW_F32) return filter_impl<float>(t, x, response, y, (cudaStream_t)stream);
+  return filter_impl<double>(t, x, response, y, (cudaStream_t)stream);
+}
+
+extern "C" int nw_misfit_prepare(const nw_traces* t, const void* obs, const void* loss_response, int32_t relative,
+                                 double* state, void* stream) {
+  int rc = check_traces(t);
+  if (rc) return rc;
+  if (!obs || !state) return fail(NW_ERR_ARG, "misfit prepare needs obs and state");
+  if (relative && loss_response) {
+    rc = check_filter_len(t);
+    if (rc) return rc;
+  }
+  if (t->dtype == NW_F32)
+    return misfit_prepare_impl<float>(t, obs, loss_response, relative, state, (cudaStream_t)stream);
+  return misfit_prepare_impl<double>(t, obs, loss_response, relative, state, (cudaStream_t)stream);
+}
+
+extern "C" int nw_misfit(const nw_traces* t, const void* pred, const void* obs, const void* sensor_response,
+                         const void* loss_response, double* state, void* grad, void* stream) {
+  int rc = check_traces(t);
+  if (rc) return rc;
+  if (!pred || !obs || !state) return fail(NW_ERR_ARG, "misfit needs pred, obs and state");
+  if (sensor_response || loss_response) {
+    rc = check_filter_len(t);
+    if (rc) return rc;
+  }
+  if (t->dtype == NW_F32)
+    return misfit_impl<float>(t, pred, obs, sensor_response, loss_response, state, grad, (cudaStream_t)stream);
+  return misfit_impl<double>(t, pred, obs, sensor_response, loss_response, state, grad, (cudaStream_t)stream);
 }

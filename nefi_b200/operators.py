@@ -362,8 +362,12 @@ class WaveOperatorB200(_LeapfrogB200):
         outs = [_FWIFunction.apply(c, self, s0, min(n, s0 + chunk) - s0) for s0 in range(0, n, chunk)]
         return outs[0] if len(outs) == 1 else torch.cat(outs, dim=0)
 
-    def misfit_gradient(self, c: torch.Tensor, observed: torch.Tensor, events: dict | None = None):
-        """One FWI gradient without autograd: ``(J, dJ/dc)`` for ``J = 1/2 ||F(c) - observed||^2``.
+    def misfit_gradient(self, c: torch.Tensor, observed: torch.Tensor, events: dict | None = None,
+                        misfit=None, mask: torch.Tensor | None = None):
+        """One FWI gradient without autograd: ``(J, dJ/dc)`` for ``J = 1/2 ||F(c) - observed||^2``, or,
+        given a :class:`nefi_b200.misfit.TraceMisfit` ``misfit``, for its band-limited (relative) MSE
+        with observation weights ``mask``; that loss and its adjoint source come from one fused pass
+        over each chunk's traces.
 
         ``dJ/dc`` is returned in float64 (the cross-shot reduction is float64), ready for a
         cross-device sum. All shots run in one sweep (``source_batch`` chunks them when set).
@@ -384,6 +388,8 @@ class WaveOperatorB200(_LeapfrogB200):
         medium = plan.medium(c2dt2)
         grad = torch.zeros(c.shape, device=c.device, dtype=torch.float64)
         loss = torch.zeros((), device=c.device, dtype=torch.float64)
+        if misfit is not None:
+            misfit.prepare(observed.to(c.dtype), mask)
         n = self.n_sources
         chunk = self.source_batch or n
         for s0 in range(0, n, chunk):
@@ -401,8 +407,11 @@ class WaveOperatorB200(_LeapfrogB200):
             if tm is not None:
                 tm["fwd1"] = torch.cuda.Event(enable_timing=True)
                 tm["fwd1"].record()
-            resid = traces - observed[s0:s0 + S].to(c.dtype)
-            loss += 0.5 * resid.double().square().sum()
+            if misfit is None:
+                resid = traces - observed[s0:s0 + S].to(c.dtype)
+                loss += 0.5 * resid.double().square().sum()
+            else:
+                j, resid = misfit.value_and_grad(traces, rows=slice(s0, s0 + S))
             if tm is not None:
                 tm["adj0"] = torch.cuda.Event(enable_timing=True)
                 tm["adj0"].record()
@@ -413,6 +422,8 @@ class WaveOperatorB200(_LeapfrogB200):
                 tm["adj1"] = torch.cuda.Event(enable_timing=True)
                 tm["adj1"].record()
             run.release()
+        if misfit is not None:
+            loss = j.clone()
         return loss, grad
 
     def simulate(self, c: torch.Tensor, observe: Callable | None = None,

@@ -136,6 +136,56 @@ def gen_case(name, shape, extent, sources, receivers, c_fine, kw, factor):
     save(name, out)
 
 
+def misfit_case(name, n_rows, n_t, dt, kw, seed, mask_rows=None, sensor=None):
+    """The reference's trace misfit: ``BandLimitedMSE(**kw).forward(ctx)`` (wave_fwi/losses.py:51-86)
+    and its gradient w.r.t. the prediction by autograd, ``lowpass`` of the prediction, and -- with
+    ``sensor`` -- ``gaussian_lowpass`` (photoacoustic3d/sensor.py:24-38) of the prediction and the
+    gradient of the MSE of the sensor-filtered prediction (nefi/losses/data.py:46-52)."""
+    if not wanted(name):
+        return
+    from nefi.instances.photoacoustic3d.sensor import gaussian_lowpass
+    from nefi.instances.wave_fwi.losses import BandLimitedMSE, lowpass
+    from nefi.losses.data import MSE
+    from nefi.measurement import Measurement
+
+    g = torch.Generator().manual_seed(seed)
+    t = torch.arange(n_t, dtype=F64) * dt
+    f = 1.0 / (8 * dt) * (0.5 + torch.rand(n_rows, 1, generator=g, dtype=F64))
+    obs = torch.sin(2 * math.pi * f * t) * torch.exp(-t / (n_t * dt)) + 0.3 * torch.randn(n_rows, n_t, generator=g, dtype=F64)
+    pred = obs + 0.5 * torch.randn(n_rows, n_t, generator=g, dtype=F64)
+    mask = None
+    if mask_rows is not None:
+        mask = torch.ones(n_rows, 1, dtype=F64)
+        mask[mask_rows] = 0.0
+    out = {"kind": "misfit", "pred": pred.numpy(), "obs": obs.numpy(), "dt": dt, "kw": kw, "seed": seed,
+           "sensor": sensor}
+    if mask is not None:
+        out["mask"] = mask.numpy()
+
+    class Ctx:  # the two attributes a data loss reads (nefi/losses/base.py:26-38)
+        def __init__(self, p, m):
+            self.pred, self.obs = p, m
+
+    for dt_, tag in ((F64, "f64"), (F32, "f32")):
+        x = pred.to(dt_).clone().requires_grad_(True)
+        meas = Measurement(obs.to(dt_), None if mask is None else mask.to(dt_))
+        loss = BandLimitedMSE(**kw).forward(Ctx(x, meas))
+        (gx,) = torch.autograd.grad(loss, x)
+        out[f"loss_{tag}"] = np.array(float(loss))
+        out[f"grad_{tag}"] = gx.numpy()
+        if kw.get("f_max") is not None:
+            out[f"lowpass_{tag}"] = lowpass(pred.to(dt_), dt, kw["f_max"], kw.get("taper", 0.3)).numpy()
+        if sensor is not None:
+            x = pred.to(dt_).clone().requires_grad_(True)
+            y = gaussian_lowpass(x, dt, sensor)
+            loss = MSE().forward(Ctx(y, meas))
+            (gx,) = torch.autograd.grad(loss, x)
+            out[f"sensor_{tag}"] = y.detach().numpy()
+            out[f"sensor_loss_{tag}"] = np.array(float(loss))
+            out[f"sensor_grad_{tag}"] = gx.numpy()
+    save(name, out)
+
+
 def wanted(name):
     return not ONLY or name.startswith(ONLY)
 
@@ -233,6 +283,13 @@ def main():
                                                             "absorb_width": 0.2}, 2)
     gen_case("gen2x_o4_sponge", (20, 24), ext, src, rec, cf, {**base, "order": 4, "absorbing": "sponge",
                                                                "absorb_width": 0.2}, 2)
+    # trace misfit: band-limited relative MSE (with a muted-trace mask), absolute, unfiltered; sensor response
+    misfit_case("misfit_bl_rel", 6, 120, 0.004, {"f_max": 30.0, "dt": 0.004, "taper": 0.3, "relative": True}, 17)
+    misfit_case("misfit_bl_mask", 7, 333, 0.002, {"f_max": 45.0, "dt": 0.002, "taper": 0.5, "relative": True}, 18,
+                mask_rows=[1, 4], sensor=60.0)
+    misfit_case("misfit_bl_abs", 5, 1001, 0.001, {"f_max": 25.0, "dt": 0.001, "taper": 0.2, "relative": False}, 19,
+                sensor=80.0)
+    misfit_case("misfit_plain_rel", 4, 64, 0.01, {"f_max": None, "dt": 0.01, "relative": True}, 20, mask_rows=[2])
 
 
 if __name__ == "__main__":

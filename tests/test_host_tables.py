@@ -192,3 +192,46 @@ def test_time_reversal_refuses_host_traces():
     for mode in ("dirichlet", "adjoint"):
         with pytest.raises(ConfigError):
             time_reversal(torch.tensor(case["traces"]), dom, case["receivers"], dt_obs=0.03, mode=mode)
+
+
+def test_filter_response_is_the_reference_window_on_a_power_of_two_circle():
+    """nw_filter_response (host code) against numpy: the reference's window -> impulse response at lags
+    (-n, n) -> spectrum on 2^k points, bit-reversed and divided by 2^k."""
+    import ctypes as C
+
+    import misfit_oracle as mo
+    from nefi_b200 import _lib
+
+    lib = _lib.load()
+    for kind, n_t, dt, f, taper in [(0, 120, 0.004, 30.0, 0.3), (0, 333, 0.002, 45.0, 0.5), (1, 1001, 0.001, 80.0, 0.0),
+                                    (0, 44, 0.01, 12.0, 0.0)]:
+        k = lib.nw_filter_log2_len(n_t)
+        L = 1 << k
+        assert L >= 2 * n_t and k >= 6
+        hp = np.zeros(L)
+        assert lib.nw_filter_response(kind, n_t, C.c_double(dt), C.c_double(f), C.c_double(taper), 1, hp.ctypes.data) == 0
+        if kind == 0:
+            n_fft = mo.next_fast_len(2 * n_t)
+            w = mo.window(n_fft, dt, f, taper)
+        else:
+            n_fft = 2 * n_t
+            w = np.exp(-0.5 * (np.fft.rfftfreq(n_fft, d=dt) / f) ** 2)
+        h = np.fft.irfft(w, n=n_fft)
+        hl = np.zeros(L)
+        hl[:n_t] = h[:n_t]
+        hl[L - n_t + 1:] = h[n_fft - n_t + 1:]
+        H = np.fft.fft(hl).real / L
+        rev = np.array([int(format(p, f"0{k}b")[::-1], 2) for p in range(L)])
+        assert np.abs(hp - H[rev]).max() <= 1e-13 * np.abs(H).max()
+    with pytest.raises(_lib.LibraryError):
+        _lib.check(lib.nw_filter_response(0, 100, C.c_double(0.0), C.c_double(10.0), C.c_double(0.3), 1,
+                                          np.zeros(256).ctypes.data))
+
+
+def test_misfit_refuses_host_tensors():
+    from nefi_b200.misfit import TraceMisfit, lowpass
+
+    with pytest.raises(ConfigError):
+        TraceMisfit(0.01, 5.0).prepare(torch.zeros(3, 40))
+    with pytest.raises(ConfigError):
+        lowpass(torch.zeros(3, 40), 0.01, 5.0)

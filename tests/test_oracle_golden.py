@@ -94,3 +94,24 @@ def test_oracle_supersampled_generation_matches_reference(name):
     g = np.zeros(case["traces_f64"].shape)
     tr, _ = orc.fwi(case["c"], g, dtype=np.float64)
     assert rel_l2(tr, case["traces_f64"]) < 1e-12
+
+
+@pytest.mark.parametrize("name", golden_names("misfit"))
+def test_misfit_oracle_matches_reference(name):
+    """The numpy misfit oracle against the reference's loss, gradient and filters (float64)."""
+    import misfit_oracle as mo
+
+    case = load_golden(name)
+    kw = case["kw"]
+    mask = case.get("mask")
+    loss, grad = mo.band_limited_mse(case["pred"], case["obs"], kw["dt"], kw["f_max"], kw.get("taper", 0.3),
+                                     kw["relative"], mask)
+    assert abs(loss - float(case["loss_f64"])) <= 1e-12 * abs(float(case["loss_f64"]))
+    assert rel_l2(grad, case["grad_f64"]) < 1e-12
+    if kw["f_max"] is not None:
+        assert rel_l2(mo.lowpass(case["pred"], kw["dt"], kw["f_max"], kw.get("taper", 0.3)), case["lowpass_f64"]) < 1e-13
+    if case["sensor"] is not None:
+        y, sl, sg = mo.sensor_mse(case["pred"], case["obs"], case["dt"], case["sensor"], mask)
+        assert rel_l2(y, case["sensor_f64"]) < 1e-13
+        assert abs(sl - float(case["sensor_loss_f64"])) <= 1e-12 * abs(float(case["sensor_loss_f64"]))
+        assert rel_l2(sg, case["sensor_grad_f64"]) < 1e-12
