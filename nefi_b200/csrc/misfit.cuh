@@ -237,6 +237,23 @@ __device__ __forceinline__ void inner_pass(typename Cx<T>::t* s, const fft::Grou
   }
 }
 
+// The 2^NB response values of one lowest group: contiguous and aligned to their size, so they are read
+// as 16-byte vectors where they fill one (the response stays in L2; every CTA re-reads it per pair).
+template <typename T, int NB>
+__device__ __forceinline__ void load_response(const T* __restrict__ src, T* h) {
+  constexpr int kBytes = (1 << NB) * (int)sizeof(T);
+  if constexpr (kBytes >= 16) {
+#pragma unroll
+    for (int c = 0; c < kBytes / 16; ++c) {
+      const float4 q = __ldg(reinterpret_cast<const float4*>(src) + c);
+      memcpy(reinterpret_cast<char*>(h) + 16 * c, &q, 16);
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < (1 << NB); ++k) h[k] = __ldg(src + k);
+  }
+}
+
 // The lowest group (bits [0, NB)): forward stages, the response, inverse stages.
 template <typename T, int NB>
 __device__ __forceinline__ void middle_pass(typename Cx<T>::t* s, const fft::Groups& G, const T* __restrict__ spec,
@@ -247,11 +264,10 @@ __device__ __forceinline__ void middle_pass(typename Cx<T>::t* s, const fft::Gro
     typename Cx<T>::t v[1 << NB];
     load_group<T, NB>(s, v, base, 0);
     fft::dif_group<T, NB>(v, 0, 0, G, tab);
+    T h[1 << NB];
+    load_response<T, NB>(spec + base, h);
 #pragma unroll
-    for (int k = 0; k < (1 << NB); ++k) {
-      const T h = __ldg(spec + base + k);
-      v[k] = {v[k].x * h, v[k].y * h};
-    }
+    for (int k = 0; k < (1 << NB); ++k) v[k] = {v[k].x * h[k], v[k].y * h[k]};
     fft::dit_group<T, NB>(v, 0, 0, G, tab);
     store_group<T, NB>(s, v, base, 0);
   }
@@ -321,7 +337,10 @@ __device__ __forceinline__ void middle_dispatch_(typename Cx<T>::t* s, const fft
 
 // Persistent CTAs over trace pairs; dynamic shared memory = twiddle tables + L padded complex slots.
 template <typename T>
-__global__ void __launch_bounds__(512) misfit_fft_kernel(MisfitArgs<T> a, fft::Groups Gp) {
+constexpr int misfit_threads() { return sizeof(T) == 8 ? 256 : 512; }  // float64 needs twice the registers
+
+template <typename T>
+__global__ void __launch_bounds__(misfit_threads<T>()) misfit_fft_kernel(MisfitArgs<T> a, fft::Groups Gp) {
   using C = typename Cx<T>::t;
   extern __shared__ __align__(16) unsigned char misfit_smem[];
   __shared__ fft::Groups G;

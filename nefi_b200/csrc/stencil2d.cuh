@@ -305,13 +305,13 @@ __device__ __forceinline__ void fwd2d_body(const KGrid<T>& g, const Tiled2<T>& a
 
   for (int s = sb; s < se; ++s) {
     const int buf = (s - sb) % NS;
+    cp_async_wait<NS - 2>();  // this thread's copies of shot s have landed
+    __syncthreads();          // everyone's have, and every thread is done with shot s-1
     {
       const int sn = s + NS - 1, nb = (sn - sb) % NS;  // nb: the buffer shot s-1 used
       if (sn < se) issue(ph, a.cur + (long long)sn * g.field, sp + nb * S::PS);
       cp_async_commit();
-      cp_async_wait<NS - 1>();
     }
-    __syncthreads();
     const T* P = sp + buf * S::PS;
 
     for (int e = e0 + threadIdx.x; e < e1; e += 256) {  // receiver samples of p^n
@@ -391,7 +391,6 @@ __device__ __forceinline__ void fwd2d_body(const KGrid<T>& g, const Tiled2<T>& a
 #pragma unroll
         for (int v = 0; v < VZ; ++v) wv[q][v] = wv[q + 1][v];
     }
-    __syncthreads();
   }
 }
 
@@ -413,7 +412,7 @@ __device__ __forceinline__ void adj2d_body(const KGrid<T>& g, const Tiled2<T>& a
   T* sp = sg + S::QS;                       // [NS][PS] q^{n+1} with halo
   T* sq = sp + NS * S::PS;                  // [NS][QS] q^{n+2}
   T* sl = sq + NS * S::QS;                  // [NS][QS] Lap p^n
-  T* sj = sl + NS * S::QS;                  // [QS] cotangent injected at this shot's cells
+  T* sj = sl + NS * S::QS;                  // [2][QS] cotangents injected at a shot's cells, by shot parity
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int z0 = bx * S::TZ, x0 = by * S::TX;
@@ -457,7 +456,7 @@ __device__ __forceinline__ void adj2d_body(const KGrid<T>& g, const Tiled2<T>& a
   T jw[kEnt];
   bool jslow = false;  // more entries than cached: read the table every shot
   if (inject) {
-    for (int i = threadIdx.x; i < S::QS; i += 256) sj[i] = T(0);
+    for (int i = threadIdx.x; i < 2 * S::QS; i += 256) sj[i] = T(0);
     const int e = c0 + threadIdx.x;
     if (e < c1) {
       jl = a.tt.cell_local[e];
@@ -486,6 +485,28 @@ __device__ __forceinline__ void adj2d_body(const KGrid<T>& g, const Tiled2<T>& a
 
   for (int s = sb; s < se; ++s) {
     const int buf = (s - sb) % NS;
+    // this shot's cotangent half; shot s-2 read it last, and every thread finished shot s-2 before
+    // the previous barrier, so it is free; the same thread sets the same cells every shot
+    T* sjs = sj + ((s - sb) & 1) * S::QS;
+    cp_async_wait<NS - 2>();  // this thread's copies of shot s have landed
+    if (inject) {  // cotangent of shot s at each touched cell, summed in table order
+      const T* gs = a.gtr + (long long)s * a.n_rec * a.n_t + a.j;
+      if (jl >= 0 && !jslow) {
+        T acc = T(0);
+#pragma unroll
+        for (int m = 0; m < kEnt; ++m)
+          if (m < jn) acc = fma_rn(jw[m], gs[(long long)jrec[m] * a.n_t], acc);
+        sjs[jl] = acc;
+      }
+      for (int e = c0 + threadIdx.x + (jslow ? 0 : 256); e < c1; e += 256) {  // the uncached cells
+        const int gid = a.tt.cell_gid[e];
+        T acc = T(0);
+        for (int q = a.tt.gcell_ptr[gid]; q < a.tt.gcell_ptr[gid + 1]; ++q)
+          acc = fma_rn(a.gcell_w[q], gs[(long long)a.tt.gcell_rec[q] * a.n_t], acc);
+        sjs[a.tt.cell_local[e]] = acc;
+      }
+    }
+    __syncthreads();  // every thread's copies and cotangents of shot s are in place; shot s-1 is done
     {
       const int sn = s + NS - 1, nb = (sn - sb) % NS;  // nb: the buffer shot s-1 used
       if (sn < se) {
@@ -494,26 +515,7 @@ __device__ __forceinline__ void adj2d_body(const KGrid<T>& g, const Tiled2<T>& a
         if (grad) issue(pc, a.lap + (long long)sn * g.field, sl + nb * S::QS);
       }
       cp_async_commit();
-      cp_async_wait<NS - 1>();
     }
-    if (inject) {  // cotangent of shot s at each touched cell, summed in table order
-      const T* gs = a.gtr + (long long)s * a.n_rec * a.n_t + a.j;
-      if (jl >= 0 && !jslow) {
-        T acc = T(0);
-#pragma unroll
-        for (int m = 0; m < kEnt; ++m)
-          if (m < jn) acc = fma_rn(jw[m], gs[(long long)jrec[m] * a.n_t], acc);
-        sj[jl] = acc;
-      }
-      for (int e = c0 + threadIdx.x + (jslow ? 0 : 256); e < c1; e += 256) {  // the uncached cells
-        const int gid = a.tt.cell_gid[e];
-        T acc = T(0);
-        for (int q = a.tt.gcell_ptr[gid]; q < a.tt.gcell_ptr[gid + 1]; ++q)
-          acc = fma_rn(a.gcell_w[q], gs[(long long)a.tt.gcell_rec[q] * a.n_t], acc);
-        sj[a.tt.cell_local[e]] = acc;
-      }
-    }
-    __syncthreads();
     const T* P = sp + buf * S::PS;
     const T* Q = sq + buf * S::QS;
     const T* LP = sl + buf * S::QS;
@@ -544,7 +546,7 @@ __device__ __forceinline__ void adj2d_body(const KGrid<T>& g, const Tiled2<T>& a
         vload<T, VZ>(sa + toff, ca);
         vload<T, VZ>(sbb + toff, cb);
       }
-      if (inject) vload<T, VZ>(sj + toff, inj);
+      if (inject) vload<T, VZ>(sjs + toff, inj);
       T o[VZ];
 #pragma unroll
       for (int v = 0; v < VZ; ++v) {
@@ -566,11 +568,6 @@ __device__ __forceinline__ void adj2d_body(const KGrid<T>& g, const Tiled2<T>& a
       for (int q = 0; q < 2 * R; ++q)
 #pragma unroll
         for (int v = 0; v < VZ; ++v) wv[q][v] = wv[q + 1][v];
-    }
-    __syncthreads();
-    if (inject) {  // the same threads clear the cells they set, before the next shot sets them again
-      if (jl >= 0) sj[jl] = T(0);
-      for (int e = c0 + threadIdx.x + 256; e < c1; e += 256) sj[a.tt.cell_local[e]] = T(0);
     }
   }
   if (grad && own_cols) {  // the accumulator tile landed with the first commit group

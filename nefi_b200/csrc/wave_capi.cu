@@ -245,7 +245,7 @@ int work_levels(const nw_grid* g) { return g->absorbing == NW_ABS_PML ? 7 : 3; }
 template <typename T, int R, int VZ, int RX, bool ADJ>
 constexpr size_t step2_smem() {
   using S = nw::Tile2Shape<T, VZ, RX, R>;
-  return (ADJ ? 5 * S::QS + S::NSA * (S::PS + 2 * S::QS) : 3 * S::QS + S::NS * S::PS) * sizeof(T);
+  return (ADJ ? 6 * S::QS + S::NSA * (S::PS + 2 * S::QS) : 3 * S::QS + S::NS * S::PS) * sizeof(T);
 }
 constexpr size_t kMaxSmem = 227 * 1024;  // opt-in shared memory per CTA on sm_100a
 
@@ -1495,7 +1495,7 @@ int run_misfit_program(const nw_traces* t, nw::MisfitArgs<T> a, cudaStream_t s, 
   const nw::fft::Groups G = nw::fft::make_groups(t->log2_len);
   const int L = 1 << t->log2_len;
   const size_t smem = (size_t)(G.tab_len + nw::fft::slot(L - 1) + 1) * sizeof(typename nw::fft::Cx<T>::t);
-  const int threads = std::min(512, std::max(32, L >> 4));
+  const int threads = std::min(nw::misfit_threads<T>(), std::max(32, L >> 4));
   auto kern = nw::misfit_fft_kernel<T>;
   NW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int dev = 0, sms = 0, per_sm = 0;

@@ -146,13 +146,18 @@ class TraceMisfit:
         obs = obs.detach().contiguous()
         m = None
         if mask is not None:
-            m = torch.as_tensor(mask).to(device=obs.device, dtype=obs.dtype).expand_as(obs).contiguous()
+            m = torch.as_tensor(mask).to(device=obs.device, dtype=obs.dtype)
+            if m.ndim >= 1 and m.shape[-1] == 1:  # one weight per trace (a trace mute): no per-sample array
+                m = m.expand(*obs.shape[:-1], 1)[..., 0].contiguous()
+            else:
+                m = m.expand_as(obs).contiguous()
         w, _ = self._responses(obs.shape[-1], obs.dtype, obs.device)
         state = torch.empty(_lib.NW_MISFIT_STATE, dtype=torch.float64, device=obs.device)
         if obs.numel() == 0:
             raise ShapeError("observed traces are empty")
         _lib.check(_lib.load().nw_misfit_prepare(
-            C.byref(_traces(obs, m)), obs.data_ptr(), None if w is None else w.data_ptr(),
+            C.byref(_traces(obs, m, m is not None and m.shape == obs.shape)), obs.data_ptr(),
+            None if w is None else w.data_ptr(),
             1 if self.relative else 0, state.data_ptr(), _lib.stream_handle(obs.device)))
         self._obs, self._mask, self._state, self._key = obs, m, state, key
 
@@ -175,7 +180,7 @@ class TraceMisfit:
         grad = torch.empty_like(pred) if want_grad else None
         w, g = self._responses(pred.shape[-1], pred.dtype, pred.device)
         _lib.check(_lib.load().nw_misfit(
-            C.byref(_traces(pred, m)), pred.data_ptr(), obs.data_ptr(), None if g is None else g.data_ptr(),
+            C.byref(_traces(pred, m, m is not None and m.shape == pred.shape)), pred.data_ptr(), obs.data_ptr(), None if g is None else g.data_ptr(),
             None if w is None else w.data_ptr(), self._state.data_ptr(), None if grad is None else grad.data_ptr(),
             _lib.stream_handle(pred.device)))
         return self._state[_lib.NW_MISFIT_LOSS], grad
