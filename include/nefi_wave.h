@@ -191,11 +191,13 @@ typedef struct nw_storage {
   int32_t segment;     /* steps per checkpoint segment */
   int32_t snap_kind;   /* NW_SNAP_* */
   void* pml_psi;       /* PML only: 4 levels (axis x {even, odd step}), each n_shots fields, zero
-                          before step 0: the auxiliary face fields psi. PML runs keep a history
-                          (checkpointed PML storage is not built) */
+                          before step 0: the auxiliary face fields psi. With snapshots the
+                          snapshots also hold the two face fields each segment starts from, and
+                          nw_adjoint re-runs segments in these levels */
 } nw_storage;
 
-/* Bytes of one snapshot pool for `n_snap` snapshots of n_shots shots (both levels). */
+/* Bytes of one snapshot pool for `n_snap` snapshots of n_shots shots (both levels, and with a PML
+ * the two face fields). */
 size_t nw_snapshot_bytes(const nw_grid* g, int32_t n_shots, int32_t n_snap, int32_t snap_kind);
 
 /*

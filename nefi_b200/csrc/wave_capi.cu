@@ -109,7 +109,8 @@ int launch_sample(const nw_grid* g, const nw_acquisition* a, int n_t, const T* l
   return NW_OK;
 }
 
-// ---- snapshot pool layout: per snapshot, 2 levels x n_shots fields ------------------------
+// ---- snapshot pool layout: per snapshot, 2 levels x n_shots fields (with a PML, also the two
+// face fields the next step reads: 4 x n_shots) ----------------------------------------------
 struct SnapLayout {
   int nblk;             // blocks per field
   size_t vals_bytes;    // 16-bit payload of one snapshot
@@ -123,7 +124,7 @@ SnapLayout snap_layout(const nw_grid* g, int n_shots) {
   SnapLayout L;
   const size_t esz = g->dtype == NW_F64 ? 8 : 4;
   L.nblk = (int)((g->field_elems + nw::SNAP_BLOCK - 1) / nw::SNAP_BLOCK);
-  const size_t fields = 2 * (size_t)n_shots;
+  const size_t fields = (g->absorbing == NW_ABS_PML ? 4 : 2) * (size_t)n_shots;
   L.vals_bytes = fields * L.nblk * nw::SNAP_BLOCK * 2;
   L.scale_bytes = fields * L.nblk * sizeof(float);
   L.exact_bytes = fields * g->field_elems * esz;
@@ -132,48 +133,68 @@ SnapLayout snap_layout(const nw_grid* g, int n_shots) {
 
 // Encodes levels (lm1, l0) (each n_shots fields, contiguous) into snapshot j. The 16-bit kinds
 // store p^{n0} and the difference p^{n0} - p^{n0-1}, each block-scaled, so the small level
-// difference (the discrete time derivative) keeps 16-bit relative precision.
+// difference (the discrete time derivative) keeps 16-bit relative precision. With a PML, slots 2
+// and 3 hold the two face fields f0, f1 (block-scaled as they are).
 template <typename T, int K>
 int snap_codec(const nw_grid* g, const SnapLayout& L, int n_shots, char* base, const T* lm1, T* lm1_out,
-               const T* l0, T* l0_out, bool encode, cudaStream_t s) {
+               const T* l0, T* l0_out, bool encode, cudaStream_t s, const T* const* faces = nullptr,
+               T* const* faces_out = nullptr) {
   using H = typename nw::Codec<K>::H;
   float* scales = (float*)(base + L.vals_bytes);
   const size_t half_fields = (size_t)n_shots * L.nblk * nw::SNAP_BLOCK;
   dim3 grid((L.nblk + 7) / 8, n_shots);
-  for (int lv = 0; lv < 2; ++lv) {  // slot 0: p^{n0}; slot 1: p^{n0} - p^{n0-1}
+  const int slots = g->absorbing == NW_ABS_PML ? 4 : 2;
+  for (int lv = 0; lv < slots; ++lv) {  // slot 0: p^{n0}; slot 1: p^{n0} - p^{n0-1}; 2, 3: faces
     H* v = (H*)base + lv * half_fields;
     float* sc = scales + (size_t)lv * n_shots * L.nblk;
-    if (encode)
+    if (lv >= 2) {
+      if (encode)
+        nw::snap_encode<T, K><<<grid, 256, 0, s>>>(faces[lv - 2], nullptr, g->field_elems, L.nblk, v, sc);
+      else
+        nw::snap_decode<T, K><<<grid, 256, 0, s>>>(v, sc, L.nblk, g->field_elems, nullptr, faces_out[lv - 2]);
+    } else if (encode) {
       nw::snap_encode<T, K><<<grid, 256, 0, s>>>(l0, lv == 0 ? nullptr : lm1, g->field_elems, L.nblk, v, sc);
-    else  // p^{n0} first, then p^{n0-1} = p^{n0} - difference
+    } else {  // p^{n0} first, then p^{n0-1} = p^{n0} - difference
       nw::snap_decode<T, K><<<grid, 256, 0, s>>>(v, sc, L.nblk, g->field_elems, lv == 0 ? nullptr : l0_out,
                                                  lv == 0 ? l0_out : lm1_out);
+    }
     NW_LAUNCHED();
   }
   return NW_OK;
 }
 
+// The two PML face fields that step n reads (parity n % 2 of the double-buffered levels).
+template <typename T>
+void pml_faces(T* psi, long long level_elems, int n, T* out[2]) {
+  for (int ax = 0; ax < 2; ++ax) out[ax] = psi + (long long)(2 * ax + n % 2) * level_elems;
+}
+
+// Snapshot j of the levels (lm1, l0) and, with a PML, of the face fields `faces` (NULL otherwise).
 template <typename T>
 int snap_store(const nw_grid* g, const nw_storage* st, int n_shots, const T* lm1, const T* l0, int j,
-               cudaStream_t s) {
+               cudaStream_t s, T* const* faces = nullptr) {
   SnapLayout L = snap_layout(g, n_shots);
   char* base = (char*)st->snap + (size_t)j * L.per_snap(st->snap_kind);
   const size_t lvl_bytes = (size_t)n_shots * g->field_elems * sizeof(T);
+  const T* const* fc = (const T* const*)faces;
   switch (st->snap_kind) {
     case NW_SNAP_EXACT:
       NW_CUDA(cudaMemcpyAsync(base, lm1, lvl_bytes, cudaMemcpyDeviceToDevice, s));
       NW_CUDA(cudaMemcpyAsync(base + lvl_bytes, l0, lvl_bytes, cudaMemcpyDeviceToDevice, s));
+      if (faces)
+        for (int f = 0; f < 2; ++f)
+          NW_CUDA(cudaMemcpyAsync(base + (2 + f) * lvl_bytes, faces[f], lvl_bytes, cudaMemcpyDeviceToDevice, s));
       return NW_OK;
-    case NW_SNAP_F16: return snap_codec<T, nw::CODEC_F16>(g, L, n_shots, base, lm1, nullptr, l0, nullptr, true, s);
-    case NW_SNAP_BF16: return snap_codec<T, nw::CODEC_BF16>(g, L, n_shots, base, lm1, nullptr, l0, nullptr, true, s);
-    case NW_SNAP_I16: return snap_codec<T, nw::CODEC_I16>(g, L, n_shots, base, lm1, nullptr, l0, nullptr, true, s);
+    case NW_SNAP_F16: return snap_codec<T, nw::CODEC_F16>(g, L, n_shots, base, lm1, nullptr, l0, nullptr, true, s, fc);
+    case NW_SNAP_BF16: return snap_codec<T, nw::CODEC_BF16>(g, L, n_shots, base, lm1, nullptr, l0, nullptr, true, s, fc);
+    case NW_SNAP_I16: return snap_codec<T, nw::CODEC_I16>(g, L, n_shots, base, lm1, nullptr, l0, nullptr, true, s, fc);
   }
   return fail(NW_ERR_ARG, "unknown snapshot kind");
 }
 
 template <typename T>
 int snap_load(const nw_grid* g, const nw_storage* st, int n_shots, int j, T* lm1, T* l0,
-              cudaStream_t s) {
+              cudaStream_t s, T* const* faces = nullptr) {
   SnapLayout L = snap_layout(g, n_shots);
   char* base = (char*)st->snap + (size_t)j * L.per_snap(st->snap_kind);
   const size_t lvl_bytes = (size_t)n_shots * g->field_elems * sizeof(T);
@@ -181,10 +202,16 @@ int snap_load(const nw_grid* g, const nw_storage* st, int n_shots, int j, T* lm1
     case NW_SNAP_EXACT:
       NW_CUDA(cudaMemcpyAsync(lm1, base, lvl_bytes, cudaMemcpyDeviceToDevice, s));
       NW_CUDA(cudaMemcpyAsync(l0, base + lvl_bytes, lvl_bytes, cudaMemcpyDeviceToDevice, s));
+      if (faces)
+        for (int f = 0; f < 2; ++f)
+          NW_CUDA(cudaMemcpyAsync(faces[f], base + (2 + f) * lvl_bytes, lvl_bytes, cudaMemcpyDeviceToDevice, s));
       return NW_OK;
-    case NW_SNAP_F16: return snap_codec<T, nw::CODEC_F16>(g, L, n_shots, base, nullptr, lm1, nullptr, l0, false, s);
-    case NW_SNAP_BF16: return snap_codec<T, nw::CODEC_BF16>(g, L, n_shots, base, nullptr, lm1, nullptr, l0, false, s);
-    case NW_SNAP_I16: return snap_codec<T, nw::CODEC_I16>(g, L, n_shots, base, nullptr, lm1, nullptr, l0, false, s);
+    case NW_SNAP_F16:
+      return snap_codec<T, nw::CODEC_F16>(g, L, n_shots, base, nullptr, lm1, nullptr, l0, false, s, nullptr, faces);
+    case NW_SNAP_BF16:
+      return snap_codec<T, nw::CODEC_BF16>(g, L, n_shots, base, nullptr, lm1, nullptr, l0, false, s, nullptr, faces);
+    case NW_SNAP_I16:
+      return snap_codec<T, nw::CODEC_I16>(g, L, n_shots, base, nullptr, lm1, nullptr, l0, false, s, nullptr, faces);
   }
   return fail(NW_ERR_ARG, "unknown snapshot kind");
 }
@@ -475,12 +502,13 @@ int forward_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
   const bool ckpt = !st->history && st->snap;
   if (ckpt && st->segment < 1) return fail(NW_ERR_ARG, "segment must be >= 1");
   const bool pml = g->absorbing == NW_ABS_PML;
-  if (pml && ckpt) return fail(NW_ERR_UNSUPPORTED, "checkpointed storage with a PML is not built; keep a history");
   if (pml && !st->pml_psi) return fail(NW_ERR_ARG, "a PML run needs storage.pml_psi");
   const nw::KGrid<T> kg = kgrid<T>(g);
   for (int n = n_begin; n < n_end; ++n) {
     if (ckpt && n % st->segment == 0) {
-      int rc = snap_store<T>(g, st, a->n_shots, L.at(n - 1), L.at(n), n / st->segment, s);
+      T* faces[2];
+      if (pml) pml_faces<T>((T*)st->pml_psi, LE, n, faces);
+      int rc = snap_store<T>(g, st, a->n_shots, L.at(n - 1), L.at(n), n / st->segment, s, pml ? faces : nullptr);
       if (rc) return rc;
     }
     T* lap = st->history ? (T*)st->history + (long long)n * LE : nullptr;
@@ -554,7 +582,7 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
     return NW_DISPATCH2(launch_adj2_v, T, tu.adj, kg, as, tu.adj.grid(g, S), s);
   };
   const bool pml = g->absorbing == NW_ABS_PML;
-  if (pml && ckpt) return fail(NW_ERR_UNSUPPORTED, "checkpointed storage with a PML is not built; keep a history");
+  if (pml && ckpt && !st->pml_psi) return fail(NW_ERR_ARG, "a checkpointed PML adjoint needs storage.pml_psi");
   auto step_pml = [&](int n, const T* lap) -> int {  // PML step (face cotangents in work levels 3..6)
     nw::PmlStep<T> ps = {};
     ps.prev = q(n + 2);
@@ -585,10 +613,13 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
       if (seg_n0 != n0) {  // entering a segment from its end: recompute Lap p^{n0..n1-1}
         const int n1 = std::min(n0 + K, N);
         seg_n0 = n0;
-        int rc = snap_load<T>(g, st, S, n0 / K, L.at(n0 - 1), L.at(n0), s);
+        T* faces[2];  // with a PML the recompute runs its face fields in storage.pml_psi
+        if (pml) pml_faces<T>((T*)st->pml_psi, LE, n0, faces);
+        int rc = snap_load<T>(g, st, S, n0 / K, L.at(n0 - 1), L.at(n0), s, pml ? faces : nullptr);
         if (rc) return rc;
         for (int k = n0; k < n1; ++k) {
-          rc = forward_step<T>(g, kg, m, a, t, tu, L, k, nullptr, (T*)st->segbuf + (long long)(k - n0) * LE, s);
+          rc = forward_step<T>(g, kg, m, a, t, tu, L, k, nullptr, (T*)st->segbuf + (long long)(k - n0) * LE, s,
+                               (T*)st->pml_psi);
           if (rc) return rc;
         }
       }

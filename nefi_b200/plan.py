@@ -276,18 +276,14 @@ def plan_storage(plan: DevicePlan, n_shots: int, n_steps: int, grad_mode: str,
     hist = (n_steps + 3) * lvl  # n_steps Lap p levels and the pressure ring
     if grad_mode == "autograd" and (budget is None or hist <= budget):
         return ("history", None)
-    if plan.pml is not None:  # PML runs keep a history (checkpointed PML storage is not built)
-        if budget is not None and hist + 4 * lvl > budget:
-            raise ConfigError(f"a PML gradient keeps the full history: {hist / 2**30:.1f} GiB, above the "
-                              f"budget {budget / 2**30:.1f} GiB; lower source_batch or n_t, or use 'sponge'")
-        return ("history", None)
     kind = _lib.SNAP_KINDS[snapshot]
+    extra = 4 * lvl if plan.pml is not None else 0  # the PML's face fields
     if checkpoint_every:
         return ("checkpoint", max(1, int(checkpoint_every)))
     k = max(1, int(math.ceil(math.sqrt(max(1, n_steps)))))
     if budget is not None:
         def cost(k_):
-            return plan.snapshot_bytes(n_shots, -(-n_steps // k_), kind) + (k_ + 3) * lvl
+            return plan.snapshot_bytes(n_shots, -(-n_steps // k_), kind) + (k_ + 3) * lvl + extra
         best = min(range(1, n_steps + 1), key=cost) if n_steps < 20000 else k
         if cost(k) > budget:
             k = best

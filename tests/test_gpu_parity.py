@@ -98,7 +98,8 @@ def test_pat_float32_matches_reference_float32(name, cuda_device):
 
 
 @pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
-@pytest.mark.parametrize("name", ["fwi_o4_sponge", "fwi_o4_cerjan", "pat3d_o2_sponge"])
+@pytest.mark.parametrize("name", ["fwi_o4_sponge", "fwi_o4_cerjan", "pat3d_o2_sponge", "fwi_o4_pml",
+                                  "fwi_o2_pml_aniso", "pat2d_o4_pml"])
 def test_checkpointed_gradient_is_identical_to_full_history(name, dtype, cuda_device):
     case = load_golden(name)
     if case["kind"] == "fwi":
@@ -122,6 +123,17 @@ def test_reduced_precision_snapshots_error_is_bounded(snapshot, tol, cuda_device
                      snapshot=snapshot)
     assert rel_l2(tr, case["traces_f64"]) < 1e-5  # the forward never reads a snapshot
     assert rel_l2(gc, case["grad_c_f64"]) < tol
+
+
+@pytest.mark.parametrize("snapshot", ["fixed16", "bf16"])
+def test_pml_checkpoints_with_16_bit_snapshots(snapshot, cuda_device):
+    """The PML's face fields travel through the 16-bit codec with the pressure; the traces stay exact
+    and the gradient stays close to the reference's float64 one."""
+    case = load_golden("fwi_o4_pml")
+    tr, gc = run_fwi(case, torch.float32, cuda_device, grad_mode="checkpoint", checkpoint_every=6,
+                     snapshot=snapshot)
+    assert rel_l2(tr, case["traces_f64"]) < 1e-5
+    assert rel_l2(gc, case["grad_c_f64"]) < (1e-3 if snapshot == "fixed16" else 3e-2)
 
 
 def test_runs_are_bitwise_deterministic(cuda_device):
