@@ -156,6 +156,9 @@ typedef struct nw_medium {
   const void* pml_alpha[2];
   const void* pml_beta[2];
   double pml_half_inv_h[2];  /* 0.5 / h per axis: the factor of the psi divergence */
+  int32_t pml_core[4];       /* x0, x1, z0, z1: a box of padded cells where every PML term vanishes
+                                exactly (A = B = 1, ZZ = 0, and alpha = 1, beta = 0 on both faces of
+                                both axes); the step skips the face fields there. All 0: no box */
 } nw_medium;
 
 /* Time axis: n_steps = (n_t - 1) * substeps; trace sample j is the state after j*substeps steps. */

@@ -59,7 +59,7 @@ class Acquisition(C.Structure):
 class Medium(C.Structure):
     _fields_ = [("c2dt2", C.c_void_p), ("coef_a", C.c_void_p), ("coef_b", C.c_void_p),
                 ("pml_zz", C.c_void_p), ("pml_alpha", C.c_void_p * 2), ("pml_beta", C.c_void_p * 2),
-                ("pml_half_inv_h", C.c_double * 2)]
+                ("pml_half_inv_h", C.c_double * 2), ("pml_core", C.c_int32 * 4)]
 
 
 class Time(C.Structure):

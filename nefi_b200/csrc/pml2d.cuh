@@ -35,6 +35,9 @@ struct PmlStep {
   const T* __restrict__ f_old[2];  // psi_{k-1} | Psi_{k+1} (per shot at +field)
   T* __restrict__ f_new[2];        // psi_k     | Psi_k
   T hx2, hz2;                      // 0.5 / h per axis
+  int cx0, cx1, cz0, cz1;          // core box: every PML term vanishes exactly, the faces are skipped
+  int kx0, kx1, kz0, kz1;          // a box inside the core box that a tiled kernel steps instead:
+                                   // this kernel enumerates only the cells outside it (all 0: none)
   int apply_a;                     // adjoint: A applies (k >= 1)
   // forward: point sources and the stored Laplacian
   const int* __restrict__ src_corner;
@@ -52,8 +55,26 @@ __global__ void __launch_bounds__(256) pml2d_step(KGrid<T> g, PmlStep<T> a) {
   const int s = blockIdx.y;
   const long long so = (long long)s * g.field;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long)g.n0 * g.n1) return;
-  const int x = (int)(t / g.n1), z = (int)(t % g.n1);
+  // thread t -> the t-th cell outside the tiled box, row by row: the rows above it, the left and right
+  // strips beside it, the rows below it
+  const long long top = (long long)a.kx0 * g.n1;
+  const int bw = a.kz0 + (g.n1 - a.kz1);
+  const long long mid = (long long)(a.kx1 - a.kx0) * bw;
+  if (t >= top + mid + (long long)(g.n0 - a.kx1) * g.n1) return;
+  int x, z;
+  if (t < top) {
+    x = (int)(t / g.n1);
+    z = (int)(t % g.n1);
+  } else if (t < top + mid) {
+    const long long u = t - top;
+    x = a.kx0 + (int)(u / bw);
+    const int r = (int)(u % bw);
+    z = r < a.kz0 ? r : a.kz1 + (r - a.kz0);
+  } else {
+    const long long u = t - top - mid;
+    x = a.kx1 + (int)(u / g.n1);
+    z = (int)(u % g.n1);
+  }
   const long long ld = g.s0;
   const long long i = g.origin + x * ld + z;
   const T* __restrict__ pc = a.cur + so;
@@ -65,8 +86,13 @@ __global__ void __launch_bounds__(256) pml2d_step(KGrid<T> g, PmlStep<T> a) {
     lap = fma_rn(g.w2b, add_rn(pc[i - 2], pc[i + 2]), fma_rn(g.w2a, add_rn(pc[i - 2 * ld], pc[i + 2 * ld]), lap));
   // the faces f = x, x+1 (axis 0, stride ld) and f = z, z+1 (axis 1, stride 1)
   T pml = T(0);    // forward: sum_ax (0.5/h) D-(psi_k + psi_{k-1});  adjoint: sum_ax D-(beta Psi_k)
+  // Inside the core box the faces contribute exact zeros (forward: psi stays zero there, alpha = 1,
+  // beta = 0; adjoint: beta = 0 multiplies the face cotangents) and A = B = 1, ZZ = 0, so the cell
+  // takes the same rounding sequence with those constants and neither reads nor writes a face.
+  const bool core = x >= a.cx0 && x < a.cx1 && z >= a.cz0 && z < a.cz1;
 #pragma unroll
   for (int ax = 0; ax < 2; ++ax) {
+    if (core) break;
     const long long st = ax == 0 ? ld : 1;
     const long long j = i + st;  // index of face f+1
     const T* __restrict__ al = a.alpha[ax];
@@ -89,7 +115,7 @@ __global__ void __launch_bounds__(256) pml2d_step(KGrid<T> g, PmlStep<T> a) {
     fn[i] = f0;
     if ((ax == 0 ? x : z) == (ax == 0 ? g.n0 : g.n1) - 1) fn[j] = f1;  // the last face of the axis
   }
-  const T av = a.A[i], bv = a.B[i], zz = a.ZZ[i], cc = a.C[i];
+  const T av = core ? T(1) : a.A[i], bv = core ? T(1) : a.B[i], zz = core ? T(0) : a.ZZ[i], cc = a.C[i];
   T o;
   if (!ADJ) {
     const T L = add_rn(lap, pml);

@@ -397,16 +397,52 @@ void pml_medium(const nw_medium* m, nw::PmlStep<T>& st) {
   }
   st.hx2 = (T)m->pml_half_inv_h[0];
   st.hz2 = (T)m->pml_half_inv_h[1];
+  st.cx0 = m->pml_core[0];
+  st.cx1 = m->pml_core[1];
+  st.cz0 = m->pml_core[2];
+  st.cz1 = m->pml_core[3];
 }
 
 template <typename T, bool ADJ>
 int launch_pml(const nw_grid* g, const nw::KGrid<T>& kg, const nw::PmlStep<T>& st, int n_shots, cudaStream_t s) {
-  const long long cells = (long long)g->n[0] * g->n[1];
+  const long long cells = (long long)g->n[0] * g->n[1] - (long long)(st.kx1 - st.kx0) * (st.kz1 - st.kz0);
+  if (cells <= 0) return NW_OK;
   const dim3 grid((unsigned)((cells + 255) / 256), n_shots);
   if (g->radius == 1) nw::pml2d_step<T, 1, ADJ><<<grid, 256, 0, s>>>(kg, st);
   else nw::pml2d_step<T, 2, ADJ><<<grid, 256, 0, s>>>(kg, st);
   NW_LAUNCHED();
   return NW_OK;
+}
+
+// The PML's interior box that the tiled kernels step (nw_medium.pml_core with its first column rounded
+// up to a 16-byte chunk), recorded in st.k*; left empty when the core box is missing or smaller than
+// one tile of `c`. Returns an error for a core box outside the grid.
+template <typename T>
+int pml_tiled_box(const nw_grid* g, const nw_medium* m, const TileCfg& c, nw::PmlStep<T>& st) {
+  constexpr int epc = 16 / (int)sizeof(T);
+  int x0 = m->pml_core[0], x1 = m->pml_core[1], z0 = m->pml_core[2], z1 = m->pml_core[3];
+  if (x0 < 0 || z0 < 0 || x1 < x0 || z1 < z0 || x1 > g->n[0] || z1 > g->n[1])
+    return fail(NW_ERR_ARG, "medium.pml_core lies outside the grid");
+  z0 = (z0 + epc - 1) / epc * epc;
+  if (x1 - x0 < c.tx() || z1 - z0 < c.tz()) x0 = x1 = z0 = z1 = 0;
+  st.kx0 = x0;
+  st.kx1 = x1;
+  st.kz0 = z0;
+  st.kz1 = z1;
+  return NW_OK;
+}
+
+// Tiled-kernel descriptor of that box: tiles from its corner, stores below its end.
+template <typename T>
+dim3 box_tiles(const nw::PmlStep<T>& st, const TileCfg& c, int n_shots, nw::Tiled2<T>& tb) {
+  tb.tx_off = st.kx0;
+  tb.tz_off = st.kz0;
+  tb.x_end = st.kx1;
+  tb.z_end = st.kz1;
+  tb.n_shots = n_shots;
+  tb.shots_per_cta = c.spc;
+  tb.tt.tiles_z = (st.kz1 - st.kz0 + c.tz() - 1) / c.tz();
+  return dim3(tb.tt.tiles_z, (st.kx1 - st.kx0 + c.tx() - 1) / c.tx(), c.groups(n_shots));
 }
 
 template <typename T>
@@ -443,7 +479,24 @@ int forward_step(const nw_grid* g, const nw::KGrid<T>& kg, const nw_medium* m, c
     st.wavelet = (const T*)a->wavelet;
     st.n = n;
     st.lap_out = lap_out;
-    return launch_pml<T, false>(g, kg, st, a->n_shots, s);
+    int rc = pml_tiled_box<T>(g, m, tu.fwd, st);
+    if (rc) return rc;
+    rc = launch_pml<T, false>(g, kg, st, a->n_shots, s);  // the layer (every cell outside the box)
+    if (rc || st.kx1 == st.kx0) return rc;
+    nw::Tiled2<T> tb = {};  // the interior box: the plain step (A = B = 1 and no PML term there)
+    tb.prev = st.prev;
+    tb.cur = st.cur;
+    tb.next = st.next;
+    tb.lap_out = lap_out;
+    tb.C = (const T*)m->c2dt2;
+    tb.A = (const T*)m->coef_a;
+    tb.B = (const T*)m->coef_b;
+    tb.src_corner = st.src_corner;
+    tb.src_w = st.src_w;
+    tb.wavelet = st.wavelet;
+    tb.n = n;
+    const dim3 grid = box_tiles<T>(st, tu.fwd, a->n_shots, tb);
+    return NW_DISPATCH2(launch_fwd2_v, T, tu.fwd, kg, tb, grid, s);
   }
   if (g->ndim == 2) {
     nw::Tiled2<T> st = {};
@@ -596,8 +649,25 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
     ps.apply_a = n >= 1 ? 1 : 0;
     ps.lap = lap;
     ps.grad = gacc;
-    int rc = launch_pml<T, true>(g, kg, ps, S, s);
+    int rc = pml_tiled_box<T>(g, m, tu.adj, ps);
     if (rc) return rc;
+    rc = launch_pml<T, true>(g, kg, ps, S, s);  // the layer: per-shot accumulators
+    if (rc) return rc;
+    if (ps.kx1 > ps.kx0) {  // the interior box: the plain adjoint step, accumulators per shot group
+      nw::Tiled2<T> tb = {};  // (disjoint cells, so the reduction over all accumulators stays exact)
+      tb.cur = ps.cur;
+      tb.prev = ps.prev;
+      tb.next = ps.next;
+      tb.C = (const T*)m->c2dt2;
+      tb.A = (const T*)m->coef_a;
+      tb.B = (const T*)m->coef_b;
+      tb.apply_a = ps.apply_a;
+      tb.lap = lap;
+      tb.gacc = gacc;
+      const dim3 grid = box_tiles<T>(ps, tu.adj, S, tb);
+      rc = NW_DISPATCH2(launch_adj2_v, T, tu.adj, kg, tb, grid, s);
+      if (rc) return rc;
+    }
     return inject3(n);
   };
   if (N >= n_stop) {  // level N: q^N = A C R^T g_N (q^{N+1} = q^{N+2} = 0)

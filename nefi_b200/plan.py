@@ -88,6 +88,29 @@ def ghost_offsets(g: _lib.Grid, corner: torch.Tensor) -> torch.Tensor:
     return out
 
 
+def pml_core_box(co: dict) -> tuple[int, int, int, int]:
+    """The box ``(x0, x1, z0, z1)`` of padded cells where the PML step reduces exactly to the plain
+    leapfrog update (``A = B = 1``, ``ZZ = 0``, and on both faces of both axes ``alpha = 1``,
+    ``beta = 0``, in the computation's dtype), so the step may skip the face fields there; the
+    faces of such cells never leave zero in the forward, and their cotangents meet a zero ``beta``.
+    ``(0, 0, 0, 0)`` when no such box exists."""
+    A, B, ZZ = co["A"], co["B"], co["ZZ"]
+    ok = (A == 1) & (B == 1) & (ZZ == 0)
+    for ax in range(2):
+        face = (co["alpha"][ax] == 1) & (co["beta"][ax] == 0)  # P_ax + 1 faces along ax
+        lo = face.narrow(ax, 0, face.shape[ax] - 1)
+        hi = face.narrow(ax, 1, face.shape[ax] - 1)
+        ok &= (lo & hi).expand(ok.shape)
+    if not bool(ok.any()):
+        return (0, 0, 0, 0)
+    rows = torch.nonzero(ok.any(dim=1)).flatten()
+    cols = torch.nonzero(ok.any(dim=0)).flatten()
+    x0, x1, z0, z1 = int(rows[0]), int(rows[-1]) + 1, int(cols[0]), int(cols[-1]) + 1
+    if not bool(ok[x0:x1, z0:z1].all()):
+        return (0, 0, 0, 0)
+    return (x0, x1, z0, z1)
+
+
 class DevicePlan:
     """Constant device tables of one operator (``op``) for ``device`` and ``dtype``."""
 
@@ -117,7 +140,9 @@ class DevicePlan:
             self.pml = {"ZZ": to_ghost(self.g, co["ZZ"].to(dtype)).to(device),
                         "alpha": [to_ghost_faces(self.g, co["alpha"][ax].to(dtype), ax).to(device) for ax in range(2)],
                         "beta": [to_ghost_faces(self.g, co["beta"][ax].to(dtype), ax).to(device) for ax in range(2)],
-                        "half_inv_h": [0.5 / h for h in grid.spacing]}
+                        "half_inv_h": [0.5 / h for h in grid.spacing],
+                        "core": pml_core_box({k: (v.to(dtype) if torch.is_tensor(v) else [t.to(dtype) for t in v])
+                                              for k, v in co.items()})}
         self.first_b_one = 1 if self.g.absorbing == _lib.NW_ABS_CERJAN else 0
         # receivers
         corner, w = grid.point_stencils(op.receivers)
@@ -221,6 +246,8 @@ class DevicePlan:
                 m.pml_alpha[ax] = self.pml["alpha"][ax].data_ptr()
                 m.pml_beta[ax] = self.pml["beta"][ax].data_ptr()
                 m.pml_half_inv_h[ax] = self.pml["half_inv_h"][ax]
+            for k in range(4):
+                m.pml_core[k] = self.pml["core"][k]
         return m
 
     def acquisition(self, n_shots: int, shot0: int = 0) -> _lib.Acquisition:

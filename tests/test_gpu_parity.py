@@ -308,3 +308,40 @@ def test_results_do_not_depend_on_the_launch_shape(dtype, cuda_device):
         tr, g = _layered_grad(op, dtype, cuda_device, shape)
         assert np.array_equal(tr, tr0), shape
         assert rel_l2(g, g0) < (1e-12 if dtype == torch.float64 else 1e-5), shape
+
+
+def _pml_interior_case():
+    """A PML grid whose interior holds several tiles, so the interior runs through the tiled kernels
+    and only the layer through the PML kernel (the golden PML grids are smaller than a tile)."""
+    g = torch.Generator().manual_seed(21)
+    shape, extent = (56, 200), ((0.0, 0.56), (0.0, 2.0))
+    c = (2.0 + 0.15 * torch.randn(shape, generator=g, dtype=torch.float64)).clamp(1.7, 2.3)
+    c = torch.nn.functional.avg_pool2d(c[None, None], 5, 1, 2, count_include_pad=False)[0, 0]
+    src = [[0.05, 0.4], [0.3, 1.5]]
+    rec = [[0.02, 0.1 + 0.09 * i] for i in range(20)] + [[0.5, 1.0]]
+    kw = dict(n_t=50, dt_obs=0.004, f0=25.0, c_max=2.5, order=4, absorbing="pml", absorb_width=0.08)
+    return shape, extent, c, src, rec, kw
+
+
+@pytest.mark.parametrize("dtype,tt,tg", [(torch.float64, 1e-11, 1e-10), (torch.float32, 1e-5, 1e-4)])
+def test_pml_interior_through_tiled_kernels_matches_the_oracle(dtype, tt, tg, cuda_device):
+    import oracle
+
+    shape, extent, c, src, rec, kw = _pml_interior_case()
+    dom = Domain(shape, extent)
+    op = WaveOperatorB200(dom, src, rec, grad_mode="autograd", **kw)
+    x0, x1, z0, z1 = op._plan(cuda_device, dtype).pml["core"]
+    assert x1 - x0 >= 32 and z1 - z0 >= 128  # larger than the default forward and adjoint tiles
+    cd = c.to(dtype).to(cuda_device).requires_grad_(True)
+    tr = op({"c": cd})
+    gt = torch.tensor(cotangent(tr.shape, 22), dtype=dtype, device=cuda_device)
+    (gc,) = torch.autograd.grad((tr * gt).sum(), cd)
+    orc = oracle.OracleWave(shape, extent, np.asarray(rec), sources=np.asarray(src), **kw)
+    tr_o, gc_o = orc.fwi(c.numpy(), cotangent(tr.shape, 22), dtype=np.float64)
+    assert rel_l2(tr.detach().cpu().numpy(), tr_o) < tt
+    assert rel_l2(gc.cpu().numpy(), gc_o) < tg
+    # checkpointed (exact snapshots): bitwise the same gradient
+    opk = WaveOperatorB200(dom, src, rec, grad_mode="checkpoint", checkpoint_every=9, **kw)
+    cd2 = c.to(dtype).to(cuda_device).requires_grad_(True)
+    (gk,) = torch.autograd.grad((opk({"c": cd2}) * gt).sum(), cd2)
+    assert torch.equal(gk, gc)
