@@ -143,8 +143,9 @@ struct Tiled2 {
   T* __restrict__ gacc;         // (n_groups, field) accumulators of C dJ/dC, one per shot group
   int n_rec, n_t, j;
   TileTables tt;
-  // a sub-box of the grid (the PML's interior): tiles start at (tx_off, tz_off), tz_off a multiple of
-  // the 16-byte chunk, and only cells below (x_end, z_end) are stored; all 0: the whole grid
+  // the cells a launch steps: tiles start at (tx_off, tz_off) (tz_off a multiple of the 16-byte chunk)
+  // and only cells below (x_end, z_end) are stored; the whole grid is (0, 0, n0, n1), a sub-box is the
+  // PML's interior
   int tx_off, tz_off, x_end, z_end;
 };
 
@@ -266,19 +267,18 @@ __device__ __forceinline__ void fwd2d_body(const KGrid<T>& g, const Tiled2<T>& a
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int z0 = bx * S::TZ + a.tz_off, x0 = by * S::TX + a.tx_off;
-  const int x_end = a.x_end ? a.x_end : g.n0, z_end = a.z_end ? a.z_end : g.n1;
   const int tile = by * a.tt.tiles_z + bx;
   const int sb = bz * a.shots_per_cta;
   const int se = min(sb + a.shots_per_cta, a.n_shots);
   const int zc = z0 + lane * VZ;  // first owned column
   const int xr = x0 + warp * RX;  // first owned row
   const int lrow = warp * RX;     // first owned row inside the tile
-  const bool own_cols = zc < z_end;
+  const bool own_cols = zc < a.z_end;
   const int ld = (int)g.s0;
   const long long cbase = g.origin + (long long)xr * ld + zc;  // owned cells of row k: + k*ld
   bool ok[RX];  // row k of the owned cells lies in the grid
 #pragma unroll
-  for (int k = 0; k < RX; ++k) ok[k] = own_cols && xr + k < x_end;
+  for (int k = 0; k < RX; ++k) ok[k] = own_cols && xr + k < a.x_end;
 
   const bool layer_tile = AB && (x0 < g.lo0 || x0 + S::TX > g.hi0 || z0 < g.lo1 || z0 + S::TZ > g.hi1);
   const bool use_b = layer_tile && !a.b_one;
@@ -386,8 +386,8 @@ __device__ __forceinline__ void fwd2d_body(const KGrid<T>& g, const Tiled2<T>& a
       }
       if (ok[k]) {
         const long long ro = cbase + (long long)k * ld;
-        store_row<T, VZ>(a.next + so + ro, o, zc, z_end);
-        if (a.lap_out) store_row<T, VZ>(a.lap_out + so + ro, lp, zc, z_end);
+        store_row<T, VZ>(a.next + so + ro, o, zc, a.z_end);
+        if (a.lap_out) store_row<T, VZ>(a.lap_out + so + ro, lp, zc, a.z_end);
         if (more) vldg<T, VZ>(a.prev + sn + ro, pv[k]);  // in flight while the rest of this shot runs
       }
 #pragma unroll
@@ -420,14 +420,13 @@ __device__ __forceinline__ void adj2d_body(const KGrid<T>& g, const Tiled2<T>& a
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int z0 = bx * S::TZ + a.tz_off, x0 = by * S::TX + a.tx_off;
-  const int x_end = a.x_end ? a.x_end : g.n0, z_end = a.z_end ? a.z_end : g.n1;
   const int tile = by * a.tt.tiles_z + bx;
   const int sb = bz * a.shots_per_cta;
   const int se = min(sb + a.shots_per_cta, a.n_shots);
   const int zc = z0 + lane * VZ;  // first owned column
   const int xr = x0 + warp * RX;  // first owned row
   const int lrow = warp * RX;     // first owned row inside the tile
-  const bool own_cols = zc < z_end;
+  const bool own_cols = zc < a.z_end;
   const bool grad = a.lap != nullptr;
 
   const bool layer_tile = AB && (x0 < g.lo0 || x0 + S::TX > g.hi0 || z0 < g.lo1 || z0 + S::TZ > g.hi1);
@@ -543,7 +542,7 @@ __device__ __forceinline__ void adj2d_body(const KGrid<T>& g, const Tiled2<T>& a
       vload<T, VZ>(Q + toff, q2);
       vload<T, VZ>(scc + toff, cc);
       const int x = xr + k;
-      const bool ok = own_cols && x < x_end;
+      const bool ok = own_cols && x < a.x_end;
       T ca[VZ], cb[VZ], inj[VZ];
 #pragma unroll
       for (int v = 0; v < VZ; ++v) { ca[v] = T(1); cb[v] = T(1); inj[v] = T(0); }
@@ -568,7 +567,7 @@ __device__ __forceinline__ void adj2d_body(const KGrid<T>& g, const Tiled2<T>& a
 #pragma unroll
         for (int v = 0; v < VZ; ++v) gsum[k][v] = fma_rn(wv[R][v], gl[v], gsum[k][v]);
       }
-      if (ok) store_row<T, VZ>(ob + (long long)k * ld, o, zc, z_end);
+      if (ok) store_row<T, VZ>(ob + (long long)k * ld, o, zc, a.z_end);
 #pragma unroll
       for (int q = 0; q < 2 * R; ++q)
 #pragma unroll
@@ -579,12 +578,12 @@ __device__ __forceinline__ void adj2d_body(const KGrid<T>& g, const Tiled2<T>& a
     T* gp = a.gacc + (long long)bz * g.field + cbase;
 #pragma unroll
     for (int k = 0; k < RX; ++k) {
-      if (xr + k >= x_end) continue;
+      if (xr + k >= a.x_end) continue;
       T old[VZ];
       vload<T, VZ>(sg + (lrow + k) * S::TZ + lane * VZ, old);
 #pragma unroll
       for (int v = 0; v < VZ; ++v) old[v] = add_rn(old[v], gsum[k][v]);
-      store_row<T, VZ>(gp + (long long)k * ld, old, zc, z_end);
+      store_row<T, VZ>(gp + (long long)k * ld, old, zc, a.z_end);
     }
   }
 }

@@ -318,6 +318,17 @@ nw::TileTables tile_tables(const nw_grid* g, const nw_acquisition* a, const Tile
   return tt;
 }
 
+// A descriptor without a sub-box (x_end = 0) covers the whole grid.
+template <typename T>
+nw::Tiled2<T> whole_grid(const nw::KGrid<T>& kg, nw::Tiled2<T> st) {
+  if (st.x_end == 0) {
+    st.tx_off = st.tz_off = 0;
+    st.x_end = kg.n0;
+    st.z_end = kg.n1;
+  }
+  return st;
+}
+
 template <typename T, int R, int VZ, int RX, bool AB>
 int launch_fwd2_v(const nw::KGrid<T>& kg, const nw::Tiled2<T>& st, dim3 grid, cudaStream_t s) {
   constexpr size_t smem = step2_smem<T, R, VZ, RX, false>();
@@ -325,7 +336,7 @@ int launch_fwd2_v(const nw::KGrid<T>& kg, const nw::Tiled2<T>& st, dim3 grid, cu
   static bool done = false;
   int rc = allow_smem(nw::fwd2d<T, R, VZ, RX, AB>, smem, &done);
   if (rc) return rc;
-  return launch_pdl(nw::fwd2d<T, R, VZ, RX, AB>, grid, smem, s, kg, st);
+  return launch_pdl(nw::fwd2d<T, R, VZ, RX, AB>, grid, smem, s, kg, whole_grid(kg, st));
 }
 template <typename T, int R, int VZ, int RX, bool AB>
 int launch_adj2_v(const nw::KGrid<T>& kg, const nw::Tiled2<T>& st, dim3 grid, cudaStream_t s) {
@@ -334,7 +345,7 @@ int launch_adj2_v(const nw::KGrid<T>& kg, const nw::Tiled2<T>& st, dim3 grid, cu
   static bool done = false;
   int rc = allow_smem(nw::adj2d<T, R, VZ, RX, AB>, smem, &done);
   if (rc) return rc;
-  return launch_pdl(nw::adj2d<T, R, VZ, RX, AB>, grid, smem, s, kg, st);
+  return launch_pdl(nw::adj2d<T, R, VZ, RX, AB>, grid, smem, s, kg, whole_grid(kg, st));
 }
 
 // 3-D step: forward (ADJ = false) or adjoint, plane-marching tiles of 8 x 64 (y, z) cells over
@@ -1178,6 +1189,8 @@ int batch_prepare_impl(const nw_batch_problem* P, int n, const Tune& tu, void* t
     f.gcell_w = (const T*)a->cell_weight;
     f.n_rec = a->n_rec;
     f.n_t = q.time.n_t;
+    f.x_end = g->n[0];
+    f.z_end = g->n[1];
     nw::Tiled2<T> b = f;
     f.shots_per_cta = tu.fwd.spc;
     f.tt = tile_tables(g, a, tu.fwd);
