@@ -18,6 +18,11 @@
 
 namespace nw {
 
+// Programmatic dependent launch: block until the preceding grid's memory is visible / allow the
+// following grid to be scheduled. Both are no-ops for a kernel launched without the attribute.
+__device__ __forceinline__ void wait_previous_grid() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void allow_next_grid() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
 // Arithmetic with a fixed rounding sequence: the compiler may not fuse or reorder these, so a
 // stencil written with them gives bitwise the same result in every kernel instantiation (tile
 // shape, vector width) that evaluates it.
@@ -95,6 +100,8 @@ template <typename T, int NPTS>
 __global__ void sample_kernel(const T* __restrict__ lvl, long long field, T* __restrict__ traces,
                               const int64_t* __restrict__ idx, const T* __restrict__ w, int n_rec,
                               int n_t, int j) {
+  wait_previous_grid();
+  allow_next_grid();
   const int s = blockIdx.y;
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n_rec) return;
@@ -113,6 +120,8 @@ __global__ void inject_kernel(T* __restrict__ out, long long field, const T* __r
                               int n_cells, const int64_t* __restrict__ cell,
                               const int* __restrict__ ptr, const int* __restrict__ rec,
                               const T* __restrict__ w) {
+  wait_previous_grid();
+  allow_next_grid();
   const int s = blockIdx.y;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n_cells) return;

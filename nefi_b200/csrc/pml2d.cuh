@@ -52,6 +52,8 @@ struct PmlStep {
 
 template <typename T, int R, bool ADJ>
 __global__ void __launch_bounds__(256) pml2d_step(KGrid<T> g, PmlStep<T> a) {
+  wait_previous_grid();
+  allow_next_grid();
   const int s = blockIdx.y;
   const long long so = (long long)s * g.field;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;

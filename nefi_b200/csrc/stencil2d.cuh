@@ -44,10 +44,6 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
-// Programmatic dependent launch: block until the preceding grid's memory is visible / allow the
-// following grid to be scheduled. Both are no-ops for a kernel launched without the attribute.
-__device__ __forceinline__ void wait_previous_grid() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
-__device__ __forceinline__ void allow_next_grid() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
 
 // Vector of N elements of T loaded/stored as one 8- or 16-byte access.
 template <typename T, int N>

@@ -94,19 +94,37 @@ nw::PadMap padmap(const nw_grid* g, const int32_t* n_abs) {
 
 constexpr int kGuard = 32; // zero elements in front of every field (see nw_grid.guard)
 
+// Launch a kernel that may begin while the previous kernel in the stream finishes: the kernel waits
+// (griddepcontrol.wait) for that kernel's writes before it touches memory.
+template <typename K, typename... Args>
+int launch_pdl_b(K kernel, dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  NW_CUDA(cudaLaunchKernelEx(&cfg, kernel, args...));
+  NW_LAUNCHED();
+  return NW_OK;
+}
+
 template <typename T>
 int launch_sample(const nw_grid* g, const nw_acquisition* a, int n_t, const T* lvl, int j, T* traces,
                   cudaStream_t s) {
   if (a->n_rec <= 0) return NW_OK;
   dim3 grid((a->n_rec + 127) / 128, a->n_shots);
+  const T* w = (const T*)a->rec_weight;
+  const int64_t* idx = a->rec_index;
   if (g->ndim == 2)
-    nw::sample_kernel<T, 4><<<grid, 128, 0, s>>>(lvl, g->field_elems, traces, a->rec_index,
-                                                 (const T*)a->rec_weight, a->n_rec, n_t, j);
-  else
-    nw::sample_kernel<T, 8><<<grid, 128, 0, s>>>(lvl, g->field_elems, traces, a->rec_index,
-                                                 (const T*)a->rec_weight, a->n_rec, n_t, j);
-  NW_LAUNCHED();
-  return NW_OK;
+    return launch_pdl_b(nw::sample_kernel<T, 4>, grid, dim3(128), 0, s, lvl, (long long)g->field_elems, traces, idx, w,
+                        (int)a->n_rec, n_t, j);
+  return launch_pdl_b(nw::sample_kernel<T, 8>, grid, dim3(128), 0, s, lvl, (long long)g->field_elems, traces, idx, w,
+                      (int)a->n_rec, n_t, j);
 }
 
 // ---- snapshot pool layout: per snapshot, 2 levels x n_shots fields (with a PML, also the two
@@ -289,19 +307,7 @@ int allow_smem(K kernel, size_t bytes, bool* done) {
 // kernel waits (griddepcontrol.wait) for that kernel's writes before it reads any field.
 template <typename K, typename... Args>
 int launch_pdl(K kernel, dim3 grid, size_t smem, cudaStream_t s, Args... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = grid;
-  cfg.blockDim = dim3(256, 1, 1);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = s;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  NW_CUDA(cudaLaunchKernelEx(&cfg, kernel, args...));
-  NW_LAUNCHED();
-  return NW_OK;
+  return launch_pdl_b(kernel, grid, dim3(256, 1, 1), smem, s, args...);
 }
 
 nw::TileTables tile_tables(const nw_grid* g, const nw_acquisition* a, const TileCfg& c) {
@@ -419,10 +425,8 @@ int launch_pml(const nw_grid* g, const nw::KGrid<T>& kg, const nw::PmlStep<T>& s
   const long long cells = (long long)g->n[0] * g->n[1] - (long long)(st.kx1 - st.kx0) * (st.kz1 - st.kz0);
   if (cells <= 0) return NW_OK;
   const dim3 grid((unsigned)((cells + 255) / 256), n_shots);
-  if (g->radius == 1) nw::pml2d_step<T, 1, ADJ><<<grid, 256, 0, s>>>(kg, st);
-  else nw::pml2d_step<T, 2, ADJ><<<grid, 256, 0, s>>>(kg, st);
-  NW_LAUNCHED();
-  return NW_OK;
+  if (g->radius == 1) return launch_pdl(nw::pml2d_step<T, 1, ADJ>, grid, 0, s, kg, st);
+  return launch_pdl(nw::pml2d_step<T, 2, ADJ>, grid, 0, s, kg, st);
 }
 
 // The PML's interior box that the tiled kernels step (nw_medium.pml_core with its first column rounded
@@ -618,11 +622,10 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
   dim3 ig(((a->n_cells > 0 ? a->n_cells : 1) + 127) / 128, S);
   auto inject3 = [&](int n) -> int {  // 3-D: separate adjoint-source kernel
     if (a->n_cells <= 0 || n % M != 0) return NW_OK;
-    nw::inject_kernel<T><<<ig, 128, 0, s>>>(q(n), g->field_elems, (const T*)m->c2dt2, (const T*)m->coef_a, n >= 1 ? 1 : 0,
-                                            gtr, a->n_rec, t->n_t, n / M, a->n_cells, a->cell_index,
-                                            a->cell_ptr, a->cell_rec, (const T*)a->cell_weight);
-    NW_LAUNCHED();
-    return NW_OK;
+    return launch_pdl_b(nw::inject_kernel<T>, ig, dim3(128), 0, s, q(n), (long long)g->field_elems,
+                        (const T*)m->c2dt2, (const T*)m->coef_a, n >= 1 ? 1 : 0, gtr, (int)a->n_rec, (int)t->n_t,
+                        n / M, (int)a->n_cells, a->cell_index, (const int*)a->cell_ptr, (const int*)a->cell_rec,
+                        (const T*)a->cell_weight);
   };
   auto step2 = [&](int n, const T* lap) -> int {  // 2-D: one fused tiled launch
     nw::Tiled2<T> as = {};
