@@ -3,12 +3,14 @@
 // A CTA (8 warps) owns a (y, z) tile of 8 rows by TZ = 32*VZ columns and marches along x over a
 // chunk of XC planes. Warp w owns row y0 + w, lane l the VZ columns z0 + l*VZ. Every plane the
 // march touches passes once through a ring of NSP shared-memory tiles, (8 + 2R) rows by
-// TZ + 2*HL columns (the y/z halo), staged by cp.async two planes ahead of its first use; the
+// TZ + 2*HL columns (the y/z halo), staged by cp.async two planes ahead of its first use (one
+// barrier per plane: a plane's copy is issued right after the barrier that frees its slot); the
 // x-neighbours of a thread's cells stay in a (2R+1)-plane register window, fed from the ring when a
 // plane arrives. The y/z neighbours of the centre plane come from its shared tile. Planes outside
 // the grid are never copied: their window values are zero, like the ghost planes they stand for.
-// C, p^{n-1} (q^{n+2}), A/B (layer cells) and the stored Lap p are read at the thread's own cells
-// straight from global memory with vector loads.
+// C, p^{n-1} (q^{n+2}), the stored Lap p and the gradient accumulator are read at the thread's own
+// cells straight from global memory with vector loads issued one plane ahead; A/B (layer cells) when
+// needed.
 #pragma once
 #include "kernels.cuh"
 #include "stencil2d.cuh"
@@ -50,7 +52,7 @@ __device__ __forceinline__ CopyPlan<Tile3Shape<T, VZ, R>::NCH> plan_plane(const 
 }
 
 template <typename T, int R, int VZ, bool ADJ>
-__global__ void __launch_bounds__(256, 4) step3t(KGrid<T> g, Step3<T> a, int xc) {
+__global__ void __launch_bounds__(256, sizeof(T) == 8 ? 3 : 4) step3t(KGrid<T> g, Step3<T> a, int xc) {
   using S = Tile3Shape<T, VZ, R>;
   constexpr int NSP = S::NSP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -94,11 +96,26 @@ __global__ void __launch_bounds__(256, 4) step3t(KGrid<T> g, Step3<T> a, int xc)
 #pragma unroll
     for (int v = 0; v < VZ; ++v) wv[q][v] = T(0);
   const int own_off = (warp + R) * S::SW + S::HL + lane * VZ;
+  // the per-cell fields of the next plane's own cells, loaded one plane ahead into registers
+  const long long row_off = g.origin + (long long)y * ld + zc;  // + x * s0
+  T pvn[VZ], ccn[VZ], gln[VZ], ggn[VZ];
+  auto prefetch = [&](int x) {
+    if (x < x1 && own) {
+      const long long i = row_off + (long long)x * g.s0;
+      vldg<T, VZ>(a.prev + so + i, pvn);
+      vldg<T, VZ>(a.C + i, ccn);
+      if (ADJ && a.lap) {
+        vldg<T, VZ>(a.lap + so + i, gln);
+        vload<T, VZ>(a.grad + so + i, ggn);
+      }
+    }
+  };
+  prefetch(x0);
   for (int p = xa; p < xb; ++p) {
-    issue_plane(p + 2);
+    cp_async_wait<1>();  // this thread's copies of plane p have landed
+    __syncthreads();     // everyone's have, and every thread is done with the previous centre's slot
+    issue_plane(p + 2);  // into that slot
     cp_async_commit();
-    cp_async_wait<2>();
-    __syncthreads();  // plane p has landed (its centre p - R landed R planes ago)
     if (p >= 0 && p < g.n0) vload<T, VZ>(ring + ((p - xa) % NSP) * S::PS + own_off, wv[2 * R]);
     else {
 #pragma unroll
@@ -120,9 +137,15 @@ __global__ void __launch_bounds__(256, 4) step3t(KGrid<T> g, Step3<T> a, int xc)
         vload<T, VZ>(P + own_off - 2 * S::SW, ym2);
         vload<T, VZ>(P + own_off + 2 * S::SW, yp2);
       }
-      T pv[VZ], cc[VZ], ca[VZ], cb[VZ];
-      vldg<T, VZ>(a.prev + so + i, pv);
-      vldg<T, VZ>(a.C + i, cc);
+      T pv[VZ], cc[VZ], ca[VZ], cb[VZ], gl[VZ], gg[VZ];
+#pragma unroll
+      for (int v = 0; v < VZ; ++v) {
+        pv[v] = pvn[v];
+        cc[v] = ccn[v];
+        gl[v] = gln[v];
+        gg[v] = ggn[v];
+      }
+      prefetch(x + 1);  // in flight while this plane is computed
       const bool layer = yz_layer || x < g.lo0 || x >= g.hi0;
 #pragma unroll
       for (int v = 0; v < VZ; ++v) { ca[v] = T(1); cb[v] = T(1); }
@@ -158,9 +181,6 @@ __global__ void __launch_bounds__(256, 4) step3t(KGrid<T> g, Step3<T> a, int xc)
       store_row<T, VZ>(a.next + so + i, o, zc, g.n2);
       if (!ADJ && a.lap_out) store_row<T, VZ>(a.lap_out + so + i, lp, zc, g.n2);
       if (ADJ && a.lap) {
-        T gl[VZ], gg[VZ];
-        vldg<T, VZ>(a.lap + so + i, gl);
-        vload<T, VZ>(a.grad + so + i, gg);
 #pragma unroll
         for (int v = 0; v < VZ; ++v) gg[v] = fma_rn(wv[R][v], gl[v], gg[v]);
         store_row<T, VZ>(a.grad + so + i, gg, zc, g.n2);
@@ -170,7 +190,6 @@ __global__ void __launch_bounds__(256, 4) step3t(KGrid<T> g, Step3<T> a, int xc)
     for (int q = 0; q < 2 * R; ++q)
 #pragma unroll
       for (int v = 0; v < VZ; ++v) wv[q][v] = wv[q + 1][v];
-    __syncthreads();  // every thread is done with the centre's slot, which the next copy refills
   }
 }
 
