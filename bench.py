@@ -236,7 +236,7 @@ def run_batch(args) -> None:
 
 
 def run_pat(args) -> None:
-    """3-D photoacoustic gradient (configuration 5): 256^3 grid + 20-cell sponge, c = 1500 m/s
+    """3-D photoacoustic gradient: 256^3 grid + 20-cell sponge, c = 1500 m/s
     +-5 % smooth seeded perturbation, 4 instances of 20 random ellipsoids, a 256 x 256 sensor plane,
     2000 steps; the gradient w.r.t. p0 and c of 1/2 ||F(p0) - d||^2, checkpointed storage."""
     from nefi_b200 import WaveInitialConditionOperatorB200, workloads

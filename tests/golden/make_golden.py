@@ -217,7 +217,7 @@ def main():
     fwi_case("fwi_o2_sponge_aniso", (18, 30), ((0.0, 0.9), (0.0, 1.2)), [[0.45, 0.1]],
              [[0.1 + 0.1 * i, 1.0] for i in range(7)], c2,
              {**base, "n_t": 25, "order": 2, "absorbing": "sponge", "absorb_width": 0.16, "courant": 0.8}, 4)
-    # 128^2, h = 10 m, 2000 m/s + two +-300 m/s Gaussian anomalies (sigma 8 cells),
+    # the plain 128^2 FWI workload: h = 10 m, 2000 m/s + two +-300 m/s Gaussian anomalies (sigma 8 cells),
     # 20-cell sponge, one 15 Hz Ricker at top centre, 128 receivers on row 2, 1000 steps at CFL 0.4.
     n, h = 128, 10.0
     rng = torch.Generator().manual_seed(0)
