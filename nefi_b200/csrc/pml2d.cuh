@@ -56,26 +56,27 @@ __global__ void __launch_bounds__(256) pml2d_step(KGrid<T> g, PmlStep<T> a) {
   allow_next_grid();
   const int s = blockIdx.y;
   const long long so = (long long)s * g.field;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   // thread t -> the t-th cell outside the tiled box, row by row: the rows above it, the left and right
-  // strips beside it, the rows below it
-  const long long top = (long long)a.kx0 * g.n1;
+  // strips beside it, the rows below it (32-bit arithmetic: a field holds fewer than 2^31 cells)
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int top = a.kx0 * g.n1;
   const int bw = a.kz0 + (g.n1 - a.kz1);
-  const long long mid = (long long)(a.kx1 - a.kx0) * bw;
-  if (t >= top + mid + (long long)(g.n0 - a.kx1) * g.n1) return;
+  const int mid = (a.kx1 - a.kx0) * bw;
+  if (t >= top + mid + (g.n0 - a.kx1) * g.n1) return;
   int x, z;
   if (t < top) {
-    x = (int)(t / g.n1);
-    z = (int)(t % g.n1);
+    x = t / g.n1;
+    z = t - x * g.n1;
   } else if (t < top + mid) {
-    const long long u = t - top;
-    x = a.kx0 + (int)(u / bw);
-    const int r = (int)(u % bw);
+    const int u = t - top;
+    const int q = u / bw;
+    const int r = u - q * bw;
+    x = a.kx0 + q;
     z = r < a.kz0 ? r : a.kz1 + (r - a.kz0);
   } else {
-    const long long u = t - top - mid;
-    x = a.kx1 + (int)(u / g.n1);
-    z = (int)(u % g.n1);
+    const int u = t - top - mid;
+    x = a.kx1 + u / g.n1;
+    z = u - (x - a.kx1) * g.n1;
   }
   const long long ld = g.s0;
   const long long i = g.origin + x * ld + z;
