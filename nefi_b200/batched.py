@@ -41,8 +41,6 @@ class BatchedFWI:
                 raise ConfigError("BatchedFWI takes 2-D WaveOperatorB200 problems")
             if op.order != ops[0].order:
                 raise ConfigError("the problems of a batch share one stencil order")
-            if op.use_pml:
-                raise ConfigError("batched problems use absorbing='sponge', 'cerjan' or 'none'")
         self.device = torch.device(device)
         self.dtype = dtype
         self.ops = list(ops)
@@ -78,7 +76,10 @@ class BatchedFWI:
             n_snap = -(-op.n_steps // K) if op.n_steps > 0 else 1
             b["snap"] = torch.empty(plan.snapshot_bytes(S, n_snap, kind), dtype=torch.uint8, device=dev)
             b["segbuf"] = plan.empty_levels(K, S)
-            b["work"] = plan.empty_levels(3, S, zero=False)
+            # the adjoint's q levels, and with a PML its four face-cotangent levels
+            b["work"] = plan.empty_levels(7 if plan.pml is not None else 3, S, zero=False)
+            if plan.pml is not None:  # the forward's face fields (the forward zeroes them)
+                b["psi"] = plan.empty_levels(4, S, zero=False)
             b["acc"] = torch.empty(plan.n_acc(S), plan.field, device=dev, dtype=self.dtype)
             b["traces"] = torch.empty(S, plan.n_rec, op.n_t, device=dev, dtype=self.dtype)
             b["gtr"] = torch.zeros_like(b["traces"])
@@ -92,6 +93,8 @@ class BatchedFWI:
             st = _lib.Storage()
             st.ring, st.snap, st.segbuf = b["ring"].data_ptr(), b["snap"].data_ptr(), b["segbuf"].data_ptr()
             st.segment, st.snap_kind = K, kind
+            if plan.pml is not None:
+                st.pml_psi = b["psi"].data_ptr()
             q = self.problems[slot]
             q.grid, q.medium, q.acq, q.time, q.storage = plan.g, b["medium"], b["acq"], plan.time, st
             q.work, q.grad_acc = b["work"].data_ptr(), b["acc"].data_ptr()

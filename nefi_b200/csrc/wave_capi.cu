@@ -1148,8 +1148,8 @@ int check_batch(const nw_batch_problem* P, int n, const Tune& tu) {
     int rc = check_run(&q.grid, &q.medium, &q.acq, &q.time, &q.storage, tu);
     if (rc) return fail(rc, "batch problem " + std::to_string(p) + ": " + g_err);
     if (q.grid.ndim != 2) return fail(NW_ERR_UNSUPPORTED, "batched problems are 2-D");
-    if (q.grid.absorbing == NW_ABS_PML)
-      return fail(NW_ERR_UNSUPPORTED, "batched problems use a sponge, Cerjan or no absorbing layer");
+    if (q.grid.absorbing == NW_ABS_PML && !q.storage.pml_psi)
+      return fail(NW_ERR_ARG, "batch problem " + std::to_string(p) + " has a PML but no storage.pml_psi");
     if (q.grid.dtype != P[0].grid.dtype || q.grid.order != P[0].grid.order)
       return fail(NW_ERR_ARG, "batched problems share one dtype and stencil order");
     if (!q.acq.has_source) return fail(NW_ERR_UNSUPPORTED, "batched problems are FWI problems (with sources)");
@@ -1164,6 +1164,18 @@ int check_batch(const nw_batch_problem* P, int n, const Tune& tu) {
       return fail(NW_ERR_ARG, "batch problem " + std::to_string(p) + " lacks a work, accumulator or trace buffer");
   }
   return NW_OK;
+}
+
+// The tiles a batched launch steps for problem q: the whole grid, or with a PML the interior box
+// (the layer goes through the PML kernel in launches of its own). The box depends on T only through
+// its 16-byte column alignment, which the batch's dtype fixes.
+template <typename T>
+dim3 batch_grid(const nw_batch_problem& q, const TileCfg& c) {
+  if (q.grid.absorbing != NW_ABS_PML) return c.grid(&q.grid, q.acq.n_shots);
+  nw::PmlStep<T> st = {};
+  if (pml_tiled_box<T>(&q.grid, &q.medium, c, st) || st.kx1 == st.kx0) return dim3(0, 0, 0);
+  nw::Tiled2<T> tb = {};
+  return box_tiles<T>(st, c, q.acq.n_shots, tb);
 }
 
 template <typename T>
@@ -1211,7 +1223,23 @@ int batch_prepare_impl(const nw_batch_problem* P, int n, const Tune& tu, void* t
     B.n_steps = q.time.n_steps;
     B.substeps = q.time.substeps;
     B.first_b_one = q.time.first_b_one;
-    const dim3 fg = tu.fwd.grid(g, a->n_shots), ag = tu.adj.grid(g, a->n_shots);
+    if (g->absorbing == NW_ABS_PML) {  // the interior box only: no receivers or cotangents in it
+      nw::PmlStep<T> sf = {}, sa = {};
+      int rc = pml_tiled_box<T>(g, &q.medium, tu.fwd, sf);
+      if (rc) return rc;
+      rc = pml_tiled_box<T>(g, &q.medium, tu.adj, sa);
+      if (rc) return rc;
+      nw::Tiled2<T> tf = {}, ta = {};
+      box_tiles<T>(sf, tu.fwd, a->n_shots, tf);
+      box_tiles<T>(sa, tu.adj, a->n_shots, ta);
+      for (auto* d : {&B.fwd, &B.adj}) d->n_rec = 0;
+      B.adj.gtr = nullptr;
+      B.fwd.tx_off = tf.tx_off; B.fwd.tz_off = tf.tz_off; B.fwd.x_end = tf.x_end; B.fwd.z_end = tf.z_end;
+      B.fwd.tt.tiles_z = tf.tt.tiles_z;
+      B.adj.tx_off = ta.tx_off; B.adj.tz_off = ta.tz_off; B.adj.x_end = ta.x_end; B.adj.z_end = ta.z_end;
+      B.adj.tt.tiles_z = ta.tt.tiles_z;
+    }
+    const dim3 fg = batch_grid<T>(q, tu.fwd), ag = batch_grid<T>(q, tu.adj);
     B.ftx = (int)fg.y;
     B.atx = (int)ag.y;
     fcta[p] = (int)fsum;
@@ -1244,6 +1272,7 @@ int launch_fwd_batch(const void* table, int n, int n_active, int n_ctas, int ste
   static bool done = false;
   int rc = allow_smem(nw::fwd2d_batch<T, R, VZ, RX>, smem, &done);
   if (rc) return rc;
+  if (n_ctas == 0) return NW_OK;  // only PML problems whose interior is smaller than a tile
   return launch_pdl(nw::fwd2d_batch<T, R, VZ, RX>, dim3(n_ctas, 1, 1), smem, s, (const nw::BatchProb<T>*)base,
                     (const int*)(base + L.fcta), n_active, step, store_lap, segment);
 }
@@ -1258,6 +1287,7 @@ int launch_adj_batch(const void* table, int n, int n_active, int n_ctas, int ste
   static bool done = false;
   int rc = allow_smem(nw::adj2d_batch<T, R, VZ, RX>, smem, &done);
   if (rc) return rc;
+  if (n_ctas == 0) return NW_OK;  // only PML problems whose interior is smaller than a tile
   return launch_pdl(nw::adj2d_batch<T, R, VZ, RX>, dim3(n_ctas, 1, 1), smem, s, (const nw::BatchProb<T>*)base,
                     (const int*)(base + L.acta), n_active, step, segment);
 }
@@ -1277,10 +1307,11 @@ int launch_adj_batch(const void* table, int n, int n_active, int n_ctas, int ste
   }()
 
 // Host copy of the CTA offsets: cta[p] = CTAs of the problems before p.
+template <typename T>
 std::vector<int> batch_ctas(const nw_batch_problem* P, int n, const TileCfg& c) {
   std::vector<int> cta(n + 1, 0);
   for (int p = 0; p < n; ++p) {
-    const dim3 gr = c.grid(&P[p].grid, P[p].acq.n_shots);
+    const dim3 gr = batch_grid<T>(P[p], c);
     cta[p + 1] = cta[p] + (int)(gr.x * gr.y * gr.z);
   }
   return cta;
@@ -1291,20 +1322,100 @@ T* ring_level(const nw_batch_problem& q, int level) {  // pressure level `level`
   return (T*)q.storage.ring + (long long)((level + 1) % 3) * q.acq.n_shots * q.grid.field_elems;
 }
 
+// The PML layer of batch problem q at forward step k (its interior box is in the batched launch);
+// store_lap: a recompute step that stores the step's Lap p into the segment buffer.
+template <typename T>
+int batch_pml_forward(const nw_batch_problem& q, const Tune& tu, int k, bool store_lap, cudaStream_t s) {
+  const nw_grid* g = &q.grid;
+  const long long LE = (long long)q.acq.n_shots * g->field_elems;
+  nw::PmlStep<T> st = {};
+  st.prev = ring_level<T>(q, k - 1);
+  st.cur = ring_level<T>(q, k);
+  st.next = ring_level<T>(q, k + 1);
+  pml_medium(&q.medium, st);
+  T* psi = (T*)q.storage.pml_psi;
+  for (int ax = 0; ax < 2; ++ax) {
+    st.f_old[ax] = psi + (long long)(2 * ax + k % 2) * LE;
+    st.f_new[ax] = psi + (long long)(2 * ax + (k + 1) % 2) * LE;
+  }
+  st.src_corner = q.acq.src_corner;
+  st.src_w = (const T*)q.acq.src_weight;
+  st.wavelet = (const T*)q.acq.wavelet;
+  st.n = k;
+  st.lap_out = store_lap ? (T*)q.storage.segbuf + (long long)(k % q.storage.segment) * LE : nullptr;
+  int rc = pml_tiled_box<T>(g, &q.medium, tu.fwd, st);
+  if (rc) return rc;
+  return launch_pml<T, false>(g, kgrid<T>(g), st, q.acq.n_shots, s);
+}
+
+// The PML layer of batch problem q at adjoint step n, then its receiver cotangents at every cell.
+template <typename T>
+int batch_pml_adjoint(const nw_batch_problem& q, const Tune& tu, int n, cudaStream_t s) {
+  const nw_grid* g = &q.grid;
+  const long long LE = (long long)q.acq.n_shots * g->field_elems;
+  T* work = (T*)q.work;
+  auto lv = [&](int m) { return work + (long long)(m % 3) * LE; };
+  nw::PmlStep<T> ps = {};
+  ps.prev = lv(n + 2);
+  ps.cur = lv(n + 1);
+  ps.next = lv(n);
+  pml_medium(&q.medium, ps);
+  for (int ax = 0; ax < 2; ++ax) {
+    ps.f_old[ax] = work + (long long)(3 + 2 * ax + (n + 1) % 2) * LE;
+    ps.f_new[ax] = work + (long long)(3 + 2 * ax + n % 2) * LE;
+  }
+  ps.apply_a = n >= 1 ? 1 : 0;
+  ps.lap = n < q.time.n_steps ? (const T*)q.storage.segbuf + (long long)(n % q.storage.segment) * LE : nullptr;
+  ps.grad = (T*)q.grad_acc;
+  int rc = pml_tiled_box<T>(g, &q.medium, tu.adj, ps);
+  if (rc) return rc;
+  rc = launch_pml<T, true>(g, kgrid<T>(g), ps, q.acq.n_shots, s);
+  if (rc) return rc;
+  const nw_acquisition* a = &q.acq;
+  const int M = q.time.substeps;
+  if (a->n_cells <= 0 || n % M != 0) return NW_OK;
+  const dim3 ig((a->n_cells + 127) / 128, a->n_shots);
+  return launch_pdl_b(nw::inject_kernel<T>, ig, dim3(128), 0, s, lv(n), (long long)g->field_elems,
+                      (const T*)q.medium.c2dt2, (const T*)q.medium.coef_a, n >= 1 ? 1 : 0, (const T*)q.grad_traces,
+                      (int)a->n_rec, (int)q.time.n_t, n / M, (int)a->n_cells, a->cell_index, (const int*)a->cell_ptr,
+                      (const int*)a->cell_rec, (const T*)a->cell_weight);
+}
+
+// Face fields of batch problem q that step k reads (PML only).
+template <typename T>
+void batch_pml_faces(const nw_batch_problem& q, int k, T* out[2]) {
+  pml_faces<T>((T*)q.storage.pml_psi, (long long)q.acq.n_shots * q.grid.field_elems, k, out);
+}
+
 template <typename T>
 int batch_forward_impl(const nw_batch_problem* P, int n, const Tune& tu, const void* table, cudaStream_t s) {
   const int K = P[0].storage.segment, Nmax = P[0].time.n_steps, R = P[0].grid.radius;
-  const std::vector<int> cta = batch_ctas(P, n, tu.fwd);
-  for (int p = 0; p < n; ++p)  // p^-1 = p^0 = 0 (FWI)
-    NW_CUDA(cudaMemsetAsync(P[p].storage.ring, 0, 3 * (size_t)P[p].acq.n_shots * P[p].grid.field_elems * sizeof(T), s));
+  const std::vector<int> cta = batch_ctas<T>(P, n, tu.fwd);
+  for (int p = 0; p < n; ++p) {  // p^-1 = p^0 = 0 (FWI), and the PML's face fields
+    const size_t lvl = (size_t)P[p].acq.n_shots * P[p].grid.field_elems * sizeof(T);
+    NW_CUDA(cudaMemsetAsync(P[p].storage.ring, 0, 3 * lvl, s));
+    if (P[p].grid.absorbing == NW_ABS_PML) NW_CUDA(cudaMemsetAsync(P[p].storage.pml_psi, 0, 4 * lvl, s));
+  }
   for (int k = 0; k < Nmax; ++k) {
     const int na = batch_active(P, n, k, false);
     if (k % K == 0)
       for (int p = 0; p < na; ++p) {
+        const bool pml = P[p].grid.absorbing == NW_ABS_PML;
+        T* faces[2];
+        if (pml) batch_pml_faces<T>(P[p], k, faces);
         int rc = snap_store<T>(&P[p].grid, &P[p].storage, P[p].acq.n_shots, ring_level<T>(P[p], k - 1),
-                               ring_level<T>(P[p], k), k / K, s);
+                               ring_level<T>(P[p], k), k / K, s, pml ? faces : nullptr);
         if (rc) return rc;
       }
+    for (int p = 0; p < na; ++p) {  // PML problems: receivers of level k and the layer cells
+      const nw_batch_problem& q = P[p];
+      if (q.grid.absorbing != NW_ABS_PML) continue;
+      int rc = NW_OK;
+      if (k % q.time.substeps == 0)
+        rc = launch_sample<T>(&q.grid, &q.acq, q.time.n_t, ring_level<T>(q, k), k / q.time.substeps, (T*)q.traces, s);
+      if (!rc) rc = batch_pml_forward<T>(q, tu, k, false, s);
+      if (rc) return rc;
+    }
     int rc = NW_DISPATCH_BATCH(launch_fwd_batch, T, tu.fwd, R, table, n, na, cta[na], k, 0, K, s);
     if (rc) return rc;
     for (int p = 0; p < na; ++p) {  // the final receiver sample of problems ending after step k
@@ -1322,29 +1433,37 @@ int batch_forward_impl(const nw_batch_problem* P, int n, const Tune& tu, const v
 template <typename T>
 int batch_adjoint_impl(const nw_batch_problem* P, int n, const Tune& tu, const void* table, cudaStream_t s) {
   const int K = P[0].storage.segment, Nmax = P[0].time.n_steps, R = P[0].grid.radius;
-  const std::vector<int> fcta = batch_ctas(P, n, tu.fwd), acta = batch_ctas(P, n, tu.adj);
+  const std::vector<int> fcta = batch_ctas<T>(P, n, tu.fwd), acta = batch_ctas<T>(P, n, tu.adj);
   for (int p = 0; p < n; ++p) {
     const nw_batch_problem& q = P[p];
     const size_t lvl = (size_t)q.acq.n_shots * q.grid.field_elems * sizeof(T);
-    NW_CUDA(cudaMemsetAsync(q.work, 0, 3 * lvl, s));
+    NW_CUDA(cudaMemsetAsync(q.work, 0, work_levels(&q.grid) * lvl, s));
     NW_CUDA(cudaMemsetAsync(q.grad_acc, 0, (size_t)n_acc_fields(&q.grid, tu, q.acq.n_shots) * q.grid.field_elems * sizeof(T), s));
   }
   auto adj_step = [&](int step) -> int {
     const int na = batch_active(P, n, step, true);
-    return NW_DISPATCH_BATCH(launch_adj_batch, T, tu.adj, R, table, n, na, acta[na], step, 0, K, s);
+    int rc = NW_DISPATCH_BATCH(launch_adj_batch, T, tu.adj, R, table, n, na, acta[na], step, 0, K, s);
+    for (int p = 0; p < na && !rc; ++p)  // PML problems: the layer cells and the cotangents
+      if (P[p].grid.absorbing == NW_ABS_PML) rc = batch_pml_adjoint<T>(P[p], tu, step, s);
+    return rc;
   };
   int rc = adj_step(Nmax);  // problems with the largest step count start: q^N = A C R^T g_N
   if (rc) return rc;
   for (int seg = Nmax > 0 ? (Nmax - 1) / K : -1; seg >= 0; --seg) {
     const int n0 = seg * K, n1 = std::min(n0 + K, Nmax);
     const int na0 = batch_active(P, n, n0, false);
-    for (int p = 0; p < na0; ++p) {  // decode the segment's snapshots into the rings
+    for (int p = 0; p < na0; ++p) {  // decode the segment's snapshots into the rings (and faces)
+      const bool pml = P[p].grid.absorbing == NW_ABS_PML;
+      T* faces[2];
+      if (pml) batch_pml_faces<T>(P[p], n0, faces);
       rc = snap_load<T>(&P[p].grid, &P[p].storage, P[p].acq.n_shots, seg, ring_level<T>(P[p], n0 - 1),
-                        ring_level<T>(P[p], n0), s);
+                        ring_level<T>(P[p], n0), s, pml ? faces : nullptr);
       if (rc) return rc;
     }
     for (int k = n0; k < n1; ++k) {  // recompute Lap p^k into the segment buffers
       const int na = batch_active(P, n, k, false);
+      for (int p = 0; p < na; ++p)
+        if (P[p].grid.absorbing == NW_ABS_PML && (rc = batch_pml_forward<T>(P[p], tu, k, true, s))) return rc;
       rc = NW_DISPATCH_BATCH(launch_fwd_batch, T, tu.fwd, R, table, n, na, fcta[na], k, 1, K, s);
       if (rc) return rc;
     }

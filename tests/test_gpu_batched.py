@@ -22,13 +22,13 @@ pytestmark = pytest.mark.gpu
 K = 16
 
 
-def _problem(n, shots, n_t, seed, h=10.0):
+def _problem(n, shots, n_t, seed, h=10.0, absorbing="sponge"):
     rng = np.random.default_rng(seed)
     dom = Domain((n, n + 8), ((0.0, n * h), (0.0, (n + 8) * h)))
     src = [[(k + 0.5) * n * h / shots, 1.5 * h] for k in range(shots)]
     rec = [[(i + 0.5) * h, 2.5 * h] for i in range(0, n, 2)]
     op = WaveOperatorB200(dom, src, rec, n_t=n_t, dt_obs=1e-3, f0=12.0, c_max=3200.0, order=4,
-                          absorbing="sponge", absorb_width=8 * h, courant=1.0, grad_mode="checkpoint",
+                          absorbing=absorbing, absorb_width=8 * h, courant=1.0, grad_mode="checkpoint",
                           checkpoint_every=K)
     x = np.linspace(0, 1, n)[:, None] + np.linspace(0, 1, n + 8)[None, :]
     c = 2000.0 + 600.0 * x / 2 + 80.0 * rng.standard_normal((n, n + 8)) * 0.2
@@ -96,3 +96,32 @@ def test_autotune_returns_a_valid_tuning(cuda_device):
     bt = BatchedFWI(ops, device=cuda_device, segment=K, tuning=tuning)
     _, g = bt.misfit_gradients(cs, obs)
     assert all(torch.isfinite(x).all() for x in g)
+
+
+@pytest.mark.parametrize("snapshot", ["fixed16", "exact"])
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_pml_problems_in_a_batch_equal_each_problem_alone(dtype, snapshot, cuda_device):
+    """PML problems (the reference's default layer) in a batch: the interior box goes through the
+    batched launch, the layer through the PML kernel; one interior smaller than a tile (all cells
+    through the PML kernel) and a sponge problem share the batch."""
+    specs = [(96, 3, 95, 5, "pml"), (40, 2, 61, 6, "pml"), (64, 3, 95, 1, "sponge")]
+    ops, cs, obs = [], [], []
+    for n, shots, n_t, seed, layer in specs:
+        op, c = _problem(n, shots, n_t, seed, absorbing=layer)
+        with torch.no_grad():
+            obs.append(op({"c": (c * 0.97).to(dtype).to(cuda_device)}))
+        ops.append(op)
+        cs.append(c.to(dtype).to(cuda_device))
+    tuning = (2, 2, 2, 2, 2, 2)
+    bt = BatchedFWI(ops, device=cuda_device, dtype=dtype, segment=K, snapshot=snapshot, tuning=tuning)
+    losses, grads = bt.misfit_gradients(cs, obs)
+    losses = [float(x) for x in losses]
+    grads = [g.clone() for g in grads]
+    for i, op in enumerate(ops):
+        op.snapshot = snapshot
+        op.tuning = tuning
+        op._plans.clear()
+        loss1, g1 = op.misfit_gradient(cs[i], obs[i])
+        assert losses[i] == float(loss1), i
+        assert torch.equal(grads[i], g1), i
+        assert torch.isfinite(g1).all() and g1.abs().max() > 0
