@@ -328,7 +328,8 @@ typedef struct nw_batch_problem {
   nw_acquisition acq;
   nw_time time;
   nw_storage storage;
-  void* work;               /* 3 * n_shots fields: the adjoint's levels */
+  void* work;               /* 3 * n_shots fields: the adjoint's levels (PML: 7 * n_shots, with the
+                               face cotangents; the PML also needs storage.pml_psi) */
   void* grad_acc;           /* nw_adjoint_groups() fields: c2dt2 * dJ/dc2dt2, as nw_adjoint */
   void* traces;             /* (n_shots, n_rec, n_t): forward output */
   const void* grad_traces;  /* (n_shots, n_rec, n_t): adjoint input */
@@ -347,8 +348,9 @@ int nw_batch_prepare(const nw_batch_problem* problems, int32_t n_problems, const
 
 /*
  * Forward sweep of the whole batch from p^-1 = p^0 = 0: traces of every problem, and the
- * snapshots of every segment start. One kernel per global step over the problems still running,
- * plus the snapshot encodes and each problem's final receiver sample. Asynchronous; no host
+ * snapshots of every segment start. One kernel per global step over the problems still running
+ * (a PML problem's interior box; its layer cells and receivers take launches of their own), plus
+ * the snapshot encodes and each problem's final receiver sample. Asynchronous; no host
  * synchronisation, so a caller may capture it in a CUDA graph.
  */
 int nw_batch_forward(const nw_batch_problem* problems, int32_t n_problems, const nw_tuning* tune,
