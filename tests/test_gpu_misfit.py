@@ -207,3 +207,20 @@ def test_fused_misfit_gradient_with_source_chunks_and_a_trace_mute():
     # the mute: a muted trace carries no adjoint source, so masking it changes the gradient
     l3, g3 = whole.misfit_gradient(c, obs, misfit=TraceMisfit(dt_obs, 20.0))
     assert rel_l2(g3.cpu().numpy(), g1.cpu().numpy()) > 1e-6
+
+
+@pytest.mark.parametrize("n_t,n_tr", [(1, 1), (2, 3), (33, 1), (64, 2), (65, 5)])
+def test_short_and_single_traces_against_the_oracle(n_t, n_tr):
+    """Edge sizes: one-sample traces, a single trace (no partner in its pair), lengths at the 64-point
+    minimum filter and just above it."""
+    import misfit_oracle as mo
+
+    rng = np.random.default_rng(n_t * 10 + n_tr)
+    obs = rng.standard_normal((n_tr, n_t))
+    pred = obs + 0.5 * rng.standard_normal((n_tr, n_t))
+    lo, go = mo.band_limited_mse(pred, obs, 0.01, 12.0, 0.3, True, None, sensor=20.0)
+    mf = TraceMisfit(0.01, 12.0, 0.3, True, sensor_cutoff=20.0)
+    mf.prepare(_t(obs, torch.float64))
+    loss, g = mf.value_and_grad(_t(pred, torch.float64))
+    assert _rel(loss, lo) < 1e-11
+    assert rel_l2(g.cpu().numpy(), go) < 1e-10
