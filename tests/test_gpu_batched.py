@@ -125,3 +125,22 @@ def test_pml_problems_in_a_batch_equal_each_problem_alone(dtype, snapshot, cuda_
         assert losses[i] == float(loss1), i
         assert torch.equal(grads[i], g1), i
         assert torch.isfinite(g1).all() and g1.abs().max() > 0
+
+
+def test_pml_batch_graph_replay_equals_eager(cuda_device):
+    """The per-problem PML launches are captured with the batched ones: replay equals eager."""
+    ops, cs, obs = [], [], []
+    for n, shots, n_t, seed, layer in [(96, 2, 61, 7, "pml"), (48, 2, 40, 8, "sponge")]:
+        op, c = _problem(n, shots, n_t, seed, absorbing=layer)
+        with torch.no_grad():
+            obs.append(op({"c": (c * 0.97).float().to(cuda_device)}))
+        ops.append(op)
+        cs.append(c.float().to(cuda_device))
+    bt = BatchedFWI(ops, device=cuda_device, segment=K)
+    l0, g0 = bt.misfit_gradients(cs, obs)
+    l0 = [float(x) for x in l0]
+    g0 = [g.clone() for g in g0]
+    bt.capture()
+    l1, g1 = bt.misfit_gradients(cs, obs)
+    for i in range(len(ops)):
+        assert float(l1[i]) == l0[i] and torch.equal(g1[i], g0[i])
