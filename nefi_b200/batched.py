@@ -29,11 +29,14 @@ from .operators import WaveOperatorB200
 
 
 class BatchedFWI:
-    """Misfit gradients ``J_i = 1/2 ||F_i(c_i) - d_i||^2`` of a batch of FWI operators."""
+    """Misfit gradients ``J_i = 1/2 ||F_i(c_i) - d_i||^2`` of a batch of FWI operators, or with
+    ``misfits`` (one :class:`nefi_b200.misfit.TraceMisfit` per operator, optional ``masks``) their
+    band-limited (relative) MSE, loss and adjoint source from the fused misfit pass."""
 
     def __init__(self, ops: Sequence[WaveOperatorB200], *, device: torch.device | str = "cuda",
                  dtype: torch.dtype = torch.float32, segment: int | None = None, snapshot: str = "fixed16",
-                 tuning: Sequence[int] | None = None) -> None:
+                 tuning: Sequence[int] | None = None, misfits: Sequence | None = None,
+                 masks: Sequence | None = None) -> None:
         if not ops:
             raise ConfigError("an empty batch")
         for op in ops:
@@ -50,6 +53,12 @@ class BatchedFWI:
         self.segment = int(segment) if segment else max(1, int(math.ceil(math.sqrt(max(1, n_max)))))
         self.snapshot = snapshot
         self.tuning = tuple(tuning) if tuning else (0, 0, 0, 0, 0, 0)
+        if misfits is not None and len(misfits) != len(ops):
+            raise ConfigError("misfits: one per operator")
+        if masks is not None and (misfits is None or len(masks) != len(ops)):
+            raise ConfigError("masks: one per operator, with misfits")
+        self.misfits = list(misfits) if misfits is not None else None
+        self.masks = list(masks) if masks is not None else [None] * len(ops)
         self._graph = None
         self._build()
 
@@ -87,6 +96,8 @@ class BatchedFWI:
             b["obs"] = torch.empty_like(b["traces"])
             b["c2dt2"] = torch.zeros(plan.field, device=dev, dtype=self.dtype)
             b["grad"] = torch.empty(op.domain.shape, device=dev, dtype=torch.float64)
+            mask = self.masks[i]
+            b["mask"] = None if mask is None else torch.as_tensor(mask).to(dev, self.dtype)
             b["loss"] = torch.empty((), device=dev, dtype=torch.float64)
             b["medium"] = plan.medium(b["c2dt2"])
             b["acq"] = plan.acquisition(S)
@@ -121,9 +132,16 @@ class BatchedFWI:
             _lib.check(lib.nw_prepare_medium(C.byref(b["plan"].g), b["plan"].n_abs, b["c"].data_ptr(),
                                              op.dt**2, b["c2dt2"].data_ptr(), s))
         _lib.check(lib.nw_batch_forward(self.problems, n, C.byref(self.tune), self.table.data_ptr(), s))
-        for b in self.bufs:
-            torch.sub(b["traces"], b["obs"], out=b["gtr"])
-            b["loss"].copy_(0.5 * b["gtr"].double().square().sum())
+        if self.misfits is None:
+            for b in self.bufs:
+                torch.sub(b["traces"], b["obs"], out=b["gtr"])
+                b["loss"].copy_(0.5 * b["gtr"].double().square().sum())
+        else:  # the fused pass: observation terms, then loss and adjoint source straight into gtr
+            for slot, i in enumerate(self.order):
+                b, mf = self.bufs[slot], self.misfits[i]
+                mf.prepare(b["obs"], b["mask"], always=True)
+                loss, _ = mf.value_and_grad(b["traces"], out=b["gtr"])
+                b["loss"].copy_(loss)
         _lib.check(lib.nw_batch_adjoint(self.problems, n, C.byref(self.tune), self.table.data_ptr(), s))
         for slot, i in enumerate(self.order):
             b, op = self.bufs[slot], self.ops[i]

@@ -135,12 +135,15 @@ class TraceMisfit:
              if self.sensor_cutoff is not None else None)
         return w, g
 
-    def prepare(self, obs: torch.Tensor, mask: torch.Tensor | None = None) -> None:
-        """Fix the observed traces ``obs`` (``(..., n_t)``, CUDA) and their weights."""
+    def prepare(self, obs: torch.Tensor, mask: torch.Tensor | None = None, always: bool = False) -> None:
+        """Fix the observed traces ``obs`` (``(..., n_t)``, CUDA) and their weights. The observation's
+        terms are recomputed only when ``obs`` or ``mask`` changed, or with ``always`` (a caller that
+        records the launches in a CUDA graph and refills ``obs`` in place between replays). The state
+        array is kept across calls, so its device address does not change."""
         _check(obs, "observed")
         key = (obs.data_ptr(), obs._version, tuple(obs.shape), obs.dtype,
                None if mask is None else (mask.data_ptr(), mask._version, tuple(mask.shape)))
-        if key == self._key:
+        if key == self._key and not always:
             self._state[_lib.NW_MISFIT_SUM:_lib.NW_MISFIT_LOSS + 1].zero_()
             return
         obs = obs.detach().contiguous()
@@ -152,7 +155,9 @@ class TraceMisfit:
             else:
                 m = m.expand_as(obs).contiguous()
         w, _ = self._responses(obs.shape[-1], obs.dtype, obs.device)
-        state = torch.empty(_lib.NW_MISFIT_STATE, dtype=torch.float64, device=obs.device)
+        state = self._state
+        if state is None or state.device != obs.device:
+            state = torch.empty(_lib.NW_MISFIT_STATE, dtype=torch.float64, device=obs.device)
         if obs.numel() == 0:
             raise ShapeError("observed traces are empty")
         _lib.check(_lib.load().nw_misfit_prepare(
@@ -161,10 +166,12 @@ class TraceMisfit:
             1 if self.relative else 0, state.data_ptr(), _lib.stream_handle(obs.device)))
         self._obs, self._mask, self._state, self._key = obs, m, state, key
 
-    def value_and_grad(self, pred: torch.Tensor, rows: slice | None = None, want_grad: bool = True):
+    def value_and_grad(self, pred: torch.Tensor, rows: slice | None = None, want_grad: bool = True,
+                       out: torch.Tensor | None = None):
         """Add ``pred`` (the rows ``rows`` of the prepared observation along its first axis, all rows by
         default) to the misfit; returns ``(loss so far, dLoss/dpred)``, the loss a 0-dim float64 view of
-        the device state and the gradient in ``pred``'s dtype (None without ``want_grad``)."""
+        the device state and the gradient in ``pred``'s dtype (None without ``want_grad``), written
+        into ``out`` when given (contiguous, ``pred``'s shape and dtype)."""
         if self._state is None:
             raise ConfigError("TraceMisfit.prepare(observed) must come first")
         _check(pred, "pred")
@@ -177,7 +184,14 @@ class TraceMisfit:
         if pred.dtype != obs.dtype:
             raise ConfigError(f"pred dtype {pred.dtype} differs from the observed {obs.dtype}")
         pred = pred.detach().contiguous()
-        grad = torch.empty_like(pred) if want_grad else None
+        grad = None
+        if want_grad:
+            if out is not None:
+                if tuple(out.shape) != tuple(pred.shape) or out.dtype != pred.dtype or not out.is_contiguous():
+                    raise ShapeError("out must be a contiguous tensor of pred's shape and dtype")
+                grad = out
+            else:
+                grad = torch.empty_like(pred)
         w, g = self._responses(pred.shape[-1], pred.dtype, pred.device)
         _lib.check(_lib.load().nw_misfit(
             C.byref(_traces(pred, m, m is not None and m.shape == pred.shape)), pred.data_ptr(), obs.data_ptr(), None if g is None else g.data_ptr(),

@@ -144,3 +144,41 @@ def test_pml_batch_graph_replay_equals_eager(cuda_device):
     l1, g1 = bt.misfit_gradients(cs, obs)
     for i in range(len(ops)):
         assert float(l1[i]) == l0[i] and torch.equal(g1[i], g0[i])
+
+
+def test_fused_misfit_batch_equals_each_problem_alone_and_replays(cuda_device):
+    """Band-limited relative misfits (with a trace mute) inside the batch: each problem's loss and
+    gradient are bitwise those of misfit_gradient(..., misfit=...) alone, and the captured graph
+    replays them, also after the observed data change in place."""
+    from nefi_b200.misfit import TraceMisfit
+
+    ops, cs, obs = _batch(torch.float32, cuda_device)
+    tuning = (2, 2, 2, 2, 2, 2)
+    masks = []
+    for d in obs:
+        m = torch.ones(d.shape[0], d.shape[1], 1, device=cuda_device)
+        m[0, 0] = 0.0
+        masks.append(m)
+    mfs = [TraceMisfit(1e-3, 40.0, 0.3, True) for _ in ops]
+    bt = BatchedFWI(ops, device=cuda_device, segment=K, tuning=tuning, misfits=mfs, masks=masks)
+    l0, g0 = bt.misfit_gradients(cs, obs)
+    l0 = [float(x) for x in l0]
+    g0 = [g.clone() for g in g0]
+    for i, op in enumerate(ops):
+        op.snapshot = "fixed16"
+        op.tuning = tuning
+        op._plans.clear()
+        l1, g1 = op.misfit_gradient(cs[i], obs[i], misfit=TraceMisfit(1e-3, 40.0, 0.3, True), mask=masks[i])
+        assert l0[i] == float(l1), i
+        assert torch.equal(g0[i], g1), i
+    bt.capture()
+    obs2 = [d * 1.1 for d in obs]  # new observations through the same graph
+    l2, g2 = bt.misfit_gradients(cs, obs2)
+    l2 = [float(x) for x in l2]
+    g2 = [g.clone() for g in g2]
+    bt2 = BatchedFWI(ops, device=cuda_device, segment=K, tuning=tuning,
+                     misfits=[TraceMisfit(1e-3, 40.0, 0.3, True) for _ in ops], masks=masks)
+    l3, g3 = bt2.misfit_gradients(cs, obs2)
+    for i in range(len(ops)):
+        assert l2[i] == float(l3[i]) and torch.equal(g2[i], g3[i]), i
+        assert l2[i] != l0[i]
