@@ -43,7 +43,6 @@ from .geometry import (
     damping_rate,
     pml_profile,
     ricker,
-    sponge_coefficients,
 )
 from .plan import DevicePlan, ghost_view, plan_storage, to_ghost
 
