@@ -601,6 +601,8 @@ def main() -> None:
     ap.add_argument("--absorbing", default=None, choices=("sponge", "pml", "cerjan", "none"),
                     help="override the workload's absorbing layer (fwi workloads)")
     ap.add_argument("--pat-n", type=int, default=256, help="pat_256: grid edge (profiling cases)")
+    ap.add_argument("--fd-directions", type=int, default=8,
+                    help="central finite-difference checks of the float64 gradient (0: none)")
     ap.add_argument("--accuracy-shots", type=int, default=None,
                     help="shots of the float64 accuracy check (all by default)")
     args = ap.parse_args()
@@ -760,6 +762,24 @@ def main() -> None:
         _, g64 = op64.misfit_gradient(c.double(), d[:na].double())
         accuracy = {"grad_rel_l2_fp32_vs_fp64": float((g32 - g64).norm() / g64.norm()), "shots": na,
                     "fp32_storage": f"{args.grad_mode}, {args.snapshot} snapshots"}
+        if args.fd_directions > 0:
+            # central differences of the float64 misfit along seeded unit directions, step scaled to
+            # ||c||, against the float64 gradient's directional derivative
+            c64, d64 = c.double(), d[:na].double()
+            gen = torch.Generator(device=dev).manual_seed(2)
+            eps = 1e-7 * float(c64.norm())
+            errs = []
+            with torch.no_grad():
+                def misfit(cc):
+                    return 0.5 * float((op64({"c": cc}) - d64).square().sum())
+                for _ in range(args.fd_directions):
+                    u = torch.randn(c64.shape, generator=gen, device=dev, dtype=torch.float64)
+                    u /= u.norm()
+                    fd = (misfit(c64 + eps * u) - misfit(c64 - eps * u)) / (2 * eps)
+                    ad = float((g64 * u).sum())
+                    errs.append(abs(fd - ad) / max(abs(ad), 1e-300))
+            accuracy["fd_check"] = {"directions": args.fd_directions, "eps": eps, "max_rel_err": max(errs),
+                                    "median_rel_err": statistics.median(errs), "dtype": "f64"}
         del op64
 
     cpu = None
