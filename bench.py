@@ -136,15 +136,32 @@ def run_batch(args) -> None:
     """The uneven batch (64 seeded 2-D problems, 256-768^2, 4-16 shots, 1500-6000 steps) in one
     batched, checkpointed (fixed16 snapshots), graph-replayed sweep per step, with the plain
     one-problem-at-a-time path timed on the same problems beside it."""
+    import torch.distributed as dist
+
     from nefi_b200 import WaveOperatorB200, workloads
     from nefi_b200.batched import BatchedFWI, autotune
+    from nefi_b200.distributed import problem_shards
 
-    dev = torch.device("cuda", 0)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
     torch.cuda.set_device(dev)
-    ws = workloads.fwi_batch_problems(seed=0, n_problems=args.problems)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+    ws_all = workloads.fwi_batch_problems(seed=0, n_problems=args.problems)
     if args.n_steps:  # shortened case for profiling: steps scaled to at most n_steps
-        for w in ws:
+        for w in ws_all:
             w.n_steps = max(2, round(w.n_steps * args.n_steps / 6000))
+    # whole problems over the ranks, balanced by shots x cells x steps (no collective on the data path)
+    mine = problem_shards([len(w.sources) * w.padded_cells() * w.n_steps for w in ws_all], world)[rank]
+    ws = [ws_all[i] for i in mine]
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t)
     ops = [WaveOperatorB200(w.domain, w.sources, w.receivers, grad_mode="checkpoint", snapshot="fixed16",
                             **w.operator_kwargs()) for w in ws]
     cs = [torch.tensor(w.c, dtype=torch.float32, device=dev) for w in ws]
@@ -163,6 +180,8 @@ def run_batch(args) -> None:
     for _ in range(args.warmup):
         bt.misfit_gradients(cs, obs)
     torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
     sampler = ClockSampler(dev.index)
     times = []
     for _ in range(args.steps):
@@ -174,10 +193,10 @@ def run_batch(args) -> None:
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1))
     clocks = sampler.stop()
-    ms = sum(times) / len(times)
-    shots = sum(len(w.sources) for w in ws)
-    useful = sum(2 * w.padded_cells() * w.n_steps * len(w.sources) for w in ws)
-    recompute = sum(w.padded_cells() * w.n_steps * len(w.sources) for w in ws)
+    ms = max_over_ranks(sum(times) / len(times))
+    shots = sum(len(w.sources) for w in ws_all)
+    useful = sum(2 * w.padded_cells() * w.n_steps * len(w.sources) for w in ws_all)
+    recompute = sum(w.padded_cells() * w.n_steps * len(w.sources) for w in ws_all)
     peak, peak_kind = peaks()
     achieved = 16.0 * useful / (ms * 1e-3) / 1e9
     # the plain path on the same problems, one problem at a time (checkpointed, fixed16, default tuning)
@@ -192,7 +211,7 @@ def run_batch(args) -> None:
         op.misfit_gradient(c, d)
     e1.record()
     torch.cuda.synchronize()
-    plain_ms = e0.elapsed_time(e1)
+    plain_ms = max_over_ranks(e0.elapsed_time(e1))
     # end to end: models and observed data from pinned host memory in, gradients and losses out
     c_h = [c.cpu().pin_memory() for c in cs]
     d_h = [d.cpu().pin_memory() for d in obs]
@@ -206,18 +225,23 @@ def run_batch(args) -> None:
     loss_h = torch.stack(losses).cpu()
     e1.record()
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
     h2d = sum(t.numel() * t.element_size() for t in c_h + d_h)
     d2h = sum(t.numel() * 8 for t in g_h) + loss_h.numel() * 8
-    out = {"metric": METRIC, "value": shots / (ms * 1e-3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+    if world > 1:  # whole-job bytes per step, and the device bytes of the rank with the most problems
+        t = torch.tensor([float(h2d), float(d2h)], dtype=torch.float64, device=dev)
+        dist.all_reduce(t)
+        h2d, d2h = int(t[0]), int(t[1])
+    out = {"metric": METRIC, "value": shots / (ms * 1e-3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32",
            "data": "synthetic (64 seeded layered models; observed data from smoothed models)",
-           "config": {"workload": f"fwi_batch: {len(ws)} problems, grids {{256,384,512,768}}^2 + 20-cell sponge, "
+           "config": {"workload": f"fwi_batch: {len(ws_all)} problems, grids {{256,384,512,768}}^2 + 20-cell sponge, "
                                   f"4-16 Ricker shots, 1500-6000 steps (seed 0), order 4; checkpointed with "
                                   f"fixed16 snapshots, segment {bt.segment}; one launch per step over all running "
                                   f"problems, whole gradient replayed from one CUDA graph",
                       "method": "batched", "shots_total": shots, "tuning": list(tuning),
+                      "parallelism": f"whole problems balanced by cost over {world} GPU(s); no collective",
                       "autotune_s": t_tune, "graph_capture_s": t_capture,
                       "device_bytes": bt.memory_bytes(),
                       "l2": "256 MiB buffer written between timed steps; working set far above L2"},
@@ -232,7 +256,12 @@ def run_batch(args) -> None:
            "e2e": {"value": shots / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
            "clocks": clocks,
            "gpu_launches": bt.graph_launches * args.steps}
-    print(json.dumps(out), flush=True)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        bt._graph = None  # no NCCL calls in the graph, but release it before the group goes
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def run_pat(args) -> None:

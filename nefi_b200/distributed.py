@@ -53,3 +53,27 @@ def misfit_gradient_sharded(op, c: torch.Tensor, observed: torch.Tensor, group=N
         dist.all_reduce(grad, group=group)
         dist.all_reduce(loss, group=group)
     return loss, grad
+
+
+def problem_shards(costs, world: int) -> list[list[int]]:
+    """Whole problems of a batch over ``world`` ranks, balanced by cost (for FWI: shots x padded cells
+    x steps): largest first, each to the rank with the least cost so far (ties to the lower rank).
+    Deterministic, so every rank computes the same assignment; returns each rank's problem indices
+    in ascending order."""
+    if world < 1:
+        raise ValueError(f"invalid world size {world}")
+    load = [0.0] * world
+    out: list[list[int]] = [[] for _ in range(world)]
+    for i in sorted(range(len(costs)), key=lambda k: (-float(costs[k]), k)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        out[r].append(i)
+        load[r] += float(costs[i])
+    return [sorted(x) for x in out]
+
+
+def fwi_cost(op) -> float:
+    """Work of one FWI gradient of ``op``: shots x padded cells x steps (forward + adjoint alike)."""
+    cells = 1
+    for p in op.grid.padded_shape:
+        cells *= int(p)
+    return float(op.n_sources) * cells * int(op.n_steps)

@@ -105,3 +105,55 @@ def test_sharded_gradient_equals_one_process_gradient(n_src, world):
     for _, loss, grad in results:  # every rank holds the total
         assert abs(loss - ref_loss) <= 1e-12 * abs(ref_loss)
         assert rel_l2(grad, ref_grad) < 1e-12
+
+
+def test_problem_shards_cover_every_problem_once_and_balance():
+    from nefi_b200.distributed import problem_shards
+
+    rng = np.random.default_rng(3)
+    costs = rng.integers(1, 100, size=37).astype(float)
+    for world in (1, 2, 3, 8, 40):
+        shards = problem_shards(costs, world)
+        flat = sorted(i for s in shards for i in s)
+        assert flat == list(range(len(costs)))
+        loads = [sum(costs[i] for i in s) for s in shards]
+        # largest-first greedy: the spread never exceeds the largest single cost
+        assert max(loads) - min(loads) <= costs.max() + 1e-9
+        assert shards == problem_shards(list(costs), world)  # deterministic
+
+
+def _shard_worker(rank, world, port, q):
+    import torch.distributed as dist
+
+    from nefi_b200.distributed import problem_shards
+
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    try:
+        costs = [5.0, 1.0, 7.0, 3.0, 3.0, 2.0]
+        mine = problem_shards(costs, world)[rank]
+        t = torch.tensor([float(len(mine)), sum(costs[i] for i in mine)], dtype=torch.float64)
+        dist.all_reduce(t)
+        q.put((rank, mine, t.tolist()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_problem_shards_agree_across_gloo_ranks():
+    import multiprocessing as mp
+    import socket
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_shard_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    got = dict((r, (m, t)) for r, m, t in res)
+    assert sorted(got[0][0] + got[1][0]) == list(range(6))
+    assert got[0][1] == [6.0, 21.0] and got[1][1] == [6.0, 21.0]
