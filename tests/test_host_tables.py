@@ -235,3 +235,33 @@ def test_misfit_refuses_host_tensors():
         TraceMisfit(0.01, 5.0).prepare(torch.zeros(3, 40))
     with pytest.raises(ConfigError):
         lowpass(torch.zeros(3, 40), 0.01, 5.0)
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_pml_core_box_is_exactly_trivial(dtype):
+    """The interior box the PML step hands to the tiled kernels: every PML term vanishes exactly on it
+    (so the plain step is bitwise the PML step there), and it is the largest such box."""
+    from nefi_b200.geometry import pml_coefficients
+    from nefi_b200.plan import pml_core_box
+
+    for shape, width in [((40, 56), 0.08), ((24, 24), 0.25), ((64, 33), 0.05)]:
+        dom = Domain(shape, ((0.0, shape[0] * 0.01), (0.0, shape[1] * 0.01)))
+        op = WaveOperatorB200(dom, [[0.05, 0.05]], [[0.02, 0.1]], n_t=10, dt_obs=0.002, f0=20.0, c_max=2.5,
+                              absorbing="pml", absorb_width=width)
+        co = pml_coefficients(op.grid, op.c_max, op.absorb_R, op.dt)
+        cd = {k: (v.to(dtype) if torch.is_tensor(v) else [t.to(dtype) for t in v]) for k, v in co.items()}
+        x0, x1, z0, z1 = pml_core_box(cd)
+        P = op.grid.padded_shape
+        assert 0 <= x0 <= x1 <= P[0] and 0 <= z0 <= z1 <= P[1]
+        if x1 > x0:
+            sl = (slice(x0, x1), slice(z0, z1))
+            assert bool((cd["A"][sl] == 1).all() and (cd["B"][sl] == 1).all() and (cd["ZZ"][sl] == 0).all())
+            for ax in range(2):
+                lo = [slice(x0, x1), slice(z0, z1)]
+                hi = list(lo)
+                hi[ax] = slice(lo[ax].start + 1, lo[ax].stop + 1)
+                for fs in (tuple(lo), tuple(hi)):
+                    assert bool((cd["alpha"][ax][fs] == 1).all() and (cd["beta"][ax][fs] == 0).all())
+            # one more row or column on any side would leave the trivial set
+            a = op.grid.n_abs
+            assert (x0, x1, z0, z1) == (a[0], P[0] - a[0], a[1], P[1] - a[1])
