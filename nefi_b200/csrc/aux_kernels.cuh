@@ -323,57 +323,86 @@ struct Codec<CODEC_I16> {
 __device__ int g_status;  // sticky device status word (NW_ERR_* or 0)
 
 // Encodes src (or src - sub when sub != nullptr: the level difference, whose small magnitude
-// would be lost if both levels were rounded to 16 bits separately). One warp per block;
-// grid.x covers the blocks of one field, grid.y the fields.
+// would be lost if both levels were rounded to 16 bits separately). One warp per SNAP_WARP_BLOCKS
+// consecutive blocks, their loads issued together; grid.x covers the blocks of one field, grid.y the
+// fields. Each block is coded exactly as on its own.
+constexpr int SNAP_WARP_BLOCKS = 4;
 template <typename T, int K>
 __global__ void __launch_bounds__(256) snap_encode(const T* __restrict__ src, const T* __restrict__ sub,
                                                    long long field, int nblk,
                                                    typename Codec<K>::H* __restrict__ vals,
                                                    float* __restrict__ scales) {
   const int f = blockIdx.y;
-  const long long b = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
-  if (b >= nblk) return;
+  const long long b0 = ((long long)blockIdx.x * 8 + (threadIdx.x >> 5)) * SNAP_WARP_BLOCKS;
+  if (b0 >= nblk) return;
   const int lane = threadIdx.x & 31;
-  const long long e = b * SNAP_BLOCK + lane;
-  float v = 0.f;
-  if (e < field) {
-    const long long i = (long long)f * field + e;
-    v = (float)(sub ? src[i] - sub[i] : src[i]);
+  float v[SNAP_WARP_BLOCKS];
+#pragma unroll
+  for (int u = 0; u < SNAP_WARP_BLOCKS; ++u) {
+    const long long e = (b0 + u) * SNAP_BLOCK + lane;
+    v[u] = 0.f;
+    if (b0 + u < nblk && e < field) {
+      const long long i = (long long)f * field + e;
+      v[u] = (float)(sub ? src[i] - sub[i] : src[i]);
+    }
   }
-  const bool bad = !(fabsf(v) <= 3.0e38f);  // NaN or Inf
-  float mx = fabsf(v);
-  for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-  const bool any_bad = __any_sync(0xffffffffu, bad);
-  float s = 1.f;
-  if (any_bad) {
-    s = __int_as_float(0x7fc00000);
-    if (lane == 0) atomicExch(&g_status, 4);
-  } else if (mx > 0.f) {
-    s = Codec<K>::scale(mx);
+#pragma unroll
+  for (int u = 0; u < SNAP_WARP_BLOCKS; ++u) {
+    const long long b = b0 + u;
+    if (b >= nblk) break;  // warp-uniform
+    const bool bad = !(fabsf(v[u]) <= 3.0e38f);  // NaN or Inf
+    float mx = fabsf(v[u]);
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    const bool any_bad = __any_sync(0xffffffffu, bad);
+    float s = 1.f;
+    if (any_bad) {
+      s = __int_as_float(0x7fc00000);
+      if (lane == 0) atomicExch(&g_status, 4);
+    } else if (mx > 0.f) {
+      s = Codec<K>::scale(mx);
+    }
+    const float inv = any_bad ? 0.f : 1.f / s;
+    vals[(long long)f * nblk * SNAP_BLOCK + b * SNAP_BLOCK + lane] = Codec<K>::enc(v[u], inv);
+    if (lane == 0) scales[(long long)f * nblk + b] = s;
   }
-  const float inv = any_bad ? 0.f : 1.f / s;
-  vals[(long long)f * nblk * SNAP_BLOCK + b * SNAP_BLOCK + lane] = Codec<K>::enc(v, inv);
-  if (lane == 0) scales[(long long)f * nblk + b] = s;
 }
 
 // Decodes into dst (or dst = minuend - decoded when minuend != nullptr, undoing the difference
-// encoding of snap_encode).
+// encoding of snap_encode); SNAP_WARP_BLOCKS blocks per warp like the encoder.
 template <typename T, int K>
 __global__ void __launch_bounds__(256) snap_decode(const typename Codec<K>::H* __restrict__ vals,
                                                    const float* __restrict__ scales, int nblk,
                                                    long long field, const T* __restrict__ minuend,
                                                    T* __restrict__ dst) {
   const int f = blockIdx.y;
-  const long long b = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
-  if (b >= nblk) return;
+  const long long b0 = ((long long)blockIdx.x * 8 + (threadIdx.x >> 5)) * SNAP_WARP_BLOCKS;
+  if (b0 >= nblk) return;
   const int lane = threadIdx.x & 31;
-  const float s = scales[(long long)f * nblk + b];
-  if (!(s > 0.f && s <= 3.0e38f) && lane == 0) atomicExch(&g_status, 4);
-  const long long e = b * SNAP_BLOCK + lane;
-  if (e >= field) return;
-  const long long i = (long long)f * field + e;
-  const T v = (T)Codec<K>::dec(vals[(long long)f * nblk * SNAP_BLOCK + b * SNAP_BLOCK + lane], s);
-  dst[i] = minuend ? minuend[i] - v : v;
+  float sc[SNAP_WARP_BLOCKS];
+  typename Codec<K>::H q[SNAP_WARP_BLOCKS];
+  T mn[SNAP_WARP_BLOCKS];
+#pragma unroll
+  for (int u = 0; u < SNAP_WARP_BLOCKS; ++u) {
+    const long long b = b0 + u;
+    const long long e = b * SNAP_BLOCK + lane;
+    sc[u] = 1.f;
+    mn[u] = T(0);
+    if (b < nblk) {
+      sc[u] = scales[(long long)f * nblk + b];
+      q[u] = vals[(long long)f * nblk * SNAP_BLOCK + b * SNAP_BLOCK + lane];
+      if (minuend && e < field) mn[u] = minuend[(long long)f * field + e];
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < SNAP_WARP_BLOCKS; ++u) {
+    const long long b = b0 + u;
+    if (b >= nblk) break;
+    if (!(sc[u] > 0.f && sc[u] <= 3.0e38f) && lane == 0) atomicExch(&g_status, 4);
+    const long long e = b * SNAP_BLOCK + lane;
+    if (e >= field) continue;
+    const T v = (T)Codec<K>::dec(q[u], sc[u]);
+    dst[(long long)f * field + e] = minuend ? mn[u] - v : v;
+  }
 }
 
 }  // namespace nw

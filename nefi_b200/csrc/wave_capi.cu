@@ -160,7 +160,7 @@ int snap_codec(const nw_grid* g, const SnapLayout& L, int n_shots, char* base, c
   using H = typename nw::Codec<K>::H;
   float* scales = (float*)(base + L.vals_bytes);
   const size_t half_fields = (size_t)n_shots * L.nblk * nw::SNAP_BLOCK;
-  dim3 grid((L.nblk + 7) / 8, n_shots);
+  dim3 grid((L.nblk + 8 * nw::SNAP_WARP_BLOCKS - 1) / (8 * nw::SNAP_WARP_BLOCKS), n_shots);
   const int slots = g->absorbing == NW_ABS_PML ? 4 : 2;
   for (int lv = 0; lv < slots; ++lv) {  // slot 0: p^{n0}; slot 1: p^{n0} - p^{n0-1}; 2, 3: faces
     H* v = (H*)base + lv * half_fields;
