@@ -309,6 +309,59 @@ def run_pat(args) -> None:
     ms = sum(times) / len(times)
     P = op.grid.padded_shape
     cells = P[0] * P[1] * P[2]
+    # end to end: p0, c and the observed traces from pinned host memory, both gradients and the loss back
+    p0_h, c_h, d_h = p0.cpu().pin_memory(), c.cpu().pin_memory(), d.cpu().pin_memory()
+    gp_h = torch.empty(p0.shape, dtype=p0.dtype).pin_memory()
+    gc_h = torch.empty(c.shape, dtype=c.dtype).pin_memory()
+    e2e = []
+    for i in range(1 + args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        x = p0_h.to(dev, non_blocking=True).requires_grad_(True)
+        cc = c_h.to(dev, non_blocking=True).requires_grad_(True)
+        dd = d_h.to(dev, non_blocking=True)
+        loss = 0.5 * (op.with_speed(x, cc) - dd).double().square().sum()
+        gp, gc = torch.autograd.grad(loss, (x, cc))
+        gp_h.copy_(gp, non_blocking=True)
+        gc_h.copy_(gc, non_blocking=True)
+        loss.detach().cpu()
+        e1.record()
+        torch.cuda.synchronize()
+        if i:
+            e2e.append(e0.elapsed_time(e1))
+        del x, cc, dd, gp, gc, loss
+    e2e_ms = statistics.median(e2e)
+    h2d = sum(t.numel() * t.element_size() for t in (p0_h, c_h, d_h))
+    d2h = gp_h.numel() * gp_h.element_size() + gc_h.numel() * gc_h.element_size() + 8
+    cpu = None
+    if not args.no_cpu_baseline:
+        # the float32 C oracle (all host threads) on one instance and a few steps of the same grid,
+        # forward and adjoint with the p0 and c gradients, extrapolated to the workload
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle  # noqa: E402  (the checker, used here only as the timed CPU baseline)
+
+        oracle.set_threads(os.cpu_count() or 1)
+        kw = dict(w.operator_kwargs())
+        cs_ = kw.pop("c").numpy()
+
+        def oracle_seconds(n_t):
+            orc = oracle.OracleWave(w.domain.shape, w.domain.extent, w.sensors, c_max=float(cs_.max()),
+                                    **{**kw, "n_t": n_t})
+            g_s = np.random.default_rng(1).standard_normal((1, len(w.sensors), n_t)).astype(np.float32)
+            t0 = time.perf_counter()
+            orc.pat(w.p0[:1], cs_, g_s, dtype=np.float32)
+            return time.perf_counter() - t0
+
+        # the per-step cost from two sample lengths (the setup each run repeats cancels out)
+        t_a, t_b = oracle_seconds(3), oracle_seconds(9)
+        steps_done = 6 * op.substeps
+        per_step = max(t_b - t_a, 1e-9) / steps_done
+        cpu = {"value": 1.0 / (per_step * op.n_steps), "unit": "instance-gradients/s",
+               "cores": os.cpu_count() or 1, "kind": "port",
+               "sample": f"1 instance, runs of {2 * op.substeps} and {8 * op.substeps} of {op.n_steps} steps "
+                         f"(forward + adjoint, p0 and c gradients) on the {P[0]}^3 padded grid, float32; the "
+                         "difference of the two times per step, times the workload's steps",
+               "gcell_updates_per_s": 2 * cells / per_step / 1e9}
     useful = 2 * cells * op.n_steps * 4
     peak, peak_kind = peaks()
     achieved = 16.0 * useful / (ms * 1e-3) / 1e9
@@ -325,6 +378,9 @@ def run_pat(args) -> None:
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                         "traffic": None, "peak_source": peak_kind,
                         "note": "16 B per useful cell-update (forward + adjoint); the segment recompute is not counted"},
+           "cpu_baseline": cpu,
+           "e2e": {"value": 4 / (e2e_ms * 1e-3), "unit": "instance-gradients/s", "h2d_bytes_per_step": h2d,
+                   "d2h_bytes_per_step": d2h},
            "clocks": clocks, "gpu_launches": int(launches)}
     print(json.dumps(out), flush=True)
 
