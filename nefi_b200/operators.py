@@ -142,12 +142,13 @@ class _LeapfrogB200(Operator):
             raise ConfigError(f"{name} must be float32 or float64, got {x.dtype}")
 
     def _check_speed(self, c: torch.Tensor) -> None:
-        cmax = float(c.detach().max())
+        lo, hi = torch.aminmax(c.detach())  # one reduction, one host round trip
+        cmin, cmax = (float(v) for v in torch.stack([lo, hi]).tolist())
         if cmax > self.c_max * (1.0 + 1e-6):
             raise OperatorError(
                 f"wave speed max {cmax:.4g} exceeds the c_max={self.c_max:.4g} used for the CFL "
                 "time step; raise c_max or bound the field (e.g. a Bounded head)")
-        if float(c.detach().min()) <= 0:
+        if cmin <= 0:
             raise OperatorError("wave speed must be positive everywhere")
 
     def _budget(self, device: torch.device) -> int:
