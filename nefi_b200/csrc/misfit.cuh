@@ -273,7 +273,7 @@ __device__ __forceinline__ void middle_pass(typename Cx<T>::t* s, const fft::Gro
   }
 }
 
-// The top group (bits [L-4, L)): optional inverse stages (the end of filter f), the pointwise op at the
+// The top group (bits [log2 L - 4, log2 L)): optional inverse stages (the end of filter f), the pointwise op at the
 // natural-order samples, optional forward stages (the start of filter f + 1).
 template <typename T>
 __device__ __forceinline__ void top_pass(typename Cx<T>::t* s, const fft::Groups& G, const MisfitArgs<T>& a,
