@@ -429,6 +429,30 @@ int launch_pml(const nw_grid* g, const nw::KGrid<T>& kg, const nw::PmlStep<T>& s
   return launch_pdl(nw::pml2d_step<T, 2, ADJ>, grid, 0, s, kg, st);
 }
 
+// A second stream of the calling thread on the current device, with a fork and a join event: a PML
+// step runs its layer kernel there beside the interior box's tiled kernel (the two write disjoint
+// cells and read the same levels), forked from and joined back into the caller's stream, so stream
+// order (and a CUDA-graph capture of the caller's stream) is kept. Created at first use, kept until
+// the process exits.
+struct SideStream {
+  cudaStream_t s = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
+int side_stream(SideStream** out) {
+  thread_local SideStream per_device[64];
+  int dev = 0;
+  NW_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(NW_ERR_UNSUPPORTED, "device index above 63");
+  SideStream& r = per_device[dev];
+  if (!r.s) {
+    NW_CUDA(cudaStreamCreateWithFlags(&r.s, cudaStreamNonBlocking));
+    NW_CUDA(cudaEventCreateWithFlags(&r.fork, cudaEventDisableTiming));
+    NW_CUDA(cudaEventCreateWithFlags(&r.join, cudaEventDisableTiming));
+  }
+  *out = &r;
+  return NW_OK;
+}
+
 // The PML's interior box that the tiled kernels step (nw_medium.pml_core with its first column rounded
 // up to a 16-byte chunk), recorded in st.k*; left empty when the core box is missing or smaller than
 // one tile of `c`. Returns an error for a core box outside the grid.
@@ -496,8 +520,15 @@ int forward_step(const nw_grid* g, const nw::KGrid<T>& kg, const nw_medium* m, c
     st.lap_out = lap_out;
     int rc = pml_tiled_box<T>(g, m, tu.fwd, st);
     if (rc) return rc;
-    rc = launch_pml<T, false>(g, kg, st, a->n_shots, s);  // the layer (every cell outside the box)
-    if (rc || st.kx1 == st.kx0) return rc;
+    if (st.kx1 == st.kx0) return launch_pml<T, false>(g, kg, st, a->n_shots, s);  // no interior box
+    SideStream* side = nullptr;
+    rc = side_stream(&side);
+    if (rc) return rc;
+    NW_CUDA(cudaEventRecord(side->fork, s));
+    NW_CUDA(cudaStreamWaitEvent(side->s, side->fork, 0));
+    rc = launch_pml<T, false>(g, kg, st, a->n_shots, side->s);  // the layer, beside the box
+    if (rc) return rc;
+    NW_CUDA(cudaEventRecord(side->join, side->s));
     nw::Tiled2<T> tb = {};  // the interior box: the plain step (A = B = 1 and no PML term there)
     tb.prev = st.prev;
     tb.cur = st.cur;
@@ -511,7 +542,10 @@ int forward_step(const nw_grid* g, const nw::KGrid<T>& kg, const nw_medium* m, c
     tb.wavelet = st.wavelet;
     tb.n = n;
     const dim3 grid = box_tiles<T>(st, tu.fwd, a->n_shots, tb);
-    return NW_DISPATCH2(launch_fwd2_v, T, tu.fwd, kg, tb, grid, s);
+    rc = NW_DISPATCH2(launch_fwd2_v, T, tu.fwd, kg, tb, grid, s);
+    if (rc) return rc;
+    NW_CUDA(cudaStreamWaitEvent(s, side->join, 0));  // the step ends when both halves have
+    return NW_OK;
   }
   if (g->ndim == 2) {
     nw::Tiled2<T> st = {};
@@ -665,9 +699,19 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
     ps.grad = gacc;
     int rc = pml_tiled_box<T>(g, m, tu.adj, ps);
     if (rc) return rc;
-    rc = launch_pml<T, true>(g, kg, ps, S, s);  // the layer: per-shot accumulators
-    if (rc) return rc;
-    if (ps.kx1 > ps.kx0) {  // the interior box: the plain adjoint step, accumulators per shot group
+    if (ps.kx1 == ps.kx0) {  // no interior box: the layer kernel over every cell
+      rc = launch_pml<T, true>(g, kg, ps, S, s);
+      if (rc) return rc;
+    } else {  // the layer (per-shot accumulators) on the side stream, beside the interior box
+      SideStream* side = nullptr;
+      rc = side_stream(&side);
+      if (rc) return rc;
+      NW_CUDA(cudaEventRecord(side->fork, s));
+      NW_CUDA(cudaStreamWaitEvent(side->s, side->fork, 0));
+      rc = launch_pml<T, true>(g, kg, ps, S, side->s);
+      if (rc) return rc;
+      NW_CUDA(cudaEventRecord(side->join, side->s));
+      // the interior box: the plain adjoint step, accumulators per shot group
       nw::Tiled2<T> tb = {};  // (disjoint cells, so the reduction over all accumulators stays exact)
       tb.cur = ps.cur;
       tb.prev = ps.prev;
@@ -681,6 +725,7 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
       const dim3 grid = box_tiles<T>(ps, tu.adj, S, tb);
       rc = NW_DISPATCH2(launch_adj2_v, T, tu.adj, kg, tb, grid, s);
       if (rc) return rc;
+      NW_CUDA(cudaStreamWaitEvent(s, side->join, 0));
     }
     return inject3(n);
   };
