@@ -10,6 +10,18 @@ misfit 1/2 ||F(c) - d||^2 with its gradient w.r.t. c reduced over shots in float
 Rank 0 prints one JSON line. Under torchrun every rank runs its own 16 shots (weak scaling) and the
 float64 gradient is summed with one NCCL all-reduce per step. ``--impl reference`` times the CPU
 restatement of the reference algorithm (the oracle, float32, all host threads) on a bounded sample.
+
+Other workloads (``--workload``), each printing one line of the same form:
+
+* ``fwi_batch``: 64 uneven 2-D problems in one batched, checkpointed, graph-replayed gradient, with
+  the one-problem-at-a-time path timed beside it (whole problems over the ranks under torchrun);
+* ``fwi_2048``: the 2048^2 workload (32 shots, 8000 steps), with ``--grad-mode checkpoint
+  --snapshot fixed16`` for its 16-bit checkpointed gradient;
+* ``pat_256``: the 3-D photoacoustic gradient (256^3, 4 instances, 2000 steps, p0 and c);
+* ``datagen_512x2``: float64 data generation from a 2x-refined ground truth;
+* ``misfit_2048``: the fused band-limited misfit and adjoint source at the 2048^2 trace shape.
+
+``--absorbing pml`` switches the 2-D workloads to the reference's default layer.
 """
 
 from __future__ import annotations
