@@ -453,6 +453,25 @@ int side_stream(SideStream** out) {
   return NW_OK;
 }
 
+// side(t) on the calling thread's second stream beside main(s), both ordered after the work already
+// in s and joined back into it (with no side work, main(s) alone).
+template <typename FS, typename FM>
+int fork_join(cudaStream_t s, bool with_side, FS side, FM main) {
+  if (!with_side) return main(s);
+  SideStream* ss = nullptr;
+  int rc = side_stream(&ss);
+  if (rc) return rc;
+  NW_CUDA(cudaEventRecord(ss->fork, s));
+  NW_CUDA(cudaStreamWaitEvent(ss->s, ss->fork, 0));
+  rc = side(ss->s);
+  if (rc) return rc;
+  NW_CUDA(cudaEventRecord(ss->join, ss->s));
+  rc = main(s);
+  if (rc) return rc;
+  NW_CUDA(cudaStreamWaitEvent(s, ss->join, 0));
+  return NW_OK;
+}
+
 // The PML's interior box that the tiled kernels step (nw_medium.pml_core with its first column rounded
 // up to a 16-byte chunk), recorded in st.k*; left empty when the core box is missing or smaller than
 // one tile of `c`. Returns an error for a core box outside the grid.
@@ -1393,7 +1412,7 @@ int batch_pml_forward(const nw_batch_problem& q, const Tune& tu, int k, bool sto
   return launch_pml<T, false>(g, kgrid<T>(g), st, q.acq.n_shots, s);
 }
 
-// The PML layer of batch problem q at adjoint step n, then its receiver cotangents at every cell.
+// The PML layer of batch problem q at adjoint step n.
 template <typename T>
 int batch_pml_adjoint(const nw_batch_problem& q, const Tune& tu, int n, cudaStream_t s) {
   const nw_grid* g = &q.grid;
@@ -1414,8 +1433,17 @@ int batch_pml_adjoint(const nw_batch_problem& q, const Tune& tu, int n, cudaStre
   ps.grad = (T*)q.grad_acc;
   int rc = pml_tiled_box<T>(g, &q.medium, tu.adj, ps);
   if (rc) return rc;
-  rc = launch_pml<T, true>(g, kgrid<T>(g), ps, q.acq.n_shots, s);
-  if (rc) return rc;
+  return launch_pml<T, true>(g, kgrid<T>(g), ps, q.acq.n_shots, s);
+}
+
+// The receiver cotangents of batch problem q at adjoint step n at every cell (a PML problem's
+// batched launch skips them), after its interior box and layer cells.
+template <typename T>
+int batch_pml_inject(const nw_batch_problem& q, int n, cudaStream_t s) {
+  const nw_grid* g = &q.grid;
+  const long long LE = (long long)q.acq.n_shots * g->field_elems;
+  T* work = (T*)q.work;
+  auto lv = [&](int m) { return work + (long long)(m % 3) * LE; };
   const nw_acquisition* a = &q.acq;
   const int M = q.time.substeps;
   if (a->n_cells <= 0 || n % M != 0) return NW_OK;
@@ -1452,16 +1480,24 @@ int batch_forward_impl(const nw_batch_problem* P, int n, const Tune& tu, const v
                                ring_level<T>(P[p], k), k / K, s, pml ? faces : nullptr);
         if (rc) return rc;
       }
-    for (int p = 0; p < na; ++p) {  // PML problems: receivers of level k and the layer cells
-      const nw_batch_problem& q = P[p];
-      if (q.grid.absorbing != NW_ABS_PML) continue;
-      int rc = NW_OK;
-      if (k % q.time.substeps == 0)
-        rc = launch_sample<T>(&q.grid, &q.acq, q.time.n_t, ring_level<T>(q, k), k / q.time.substeps, (T*)q.traces, s);
-      if (!rc) rc = batch_pml_forward<T>(q, tu, k, false, s);
-      if (rc) return rc;
-    }
-    int rc = NW_DISPATCH_BATCH(launch_fwd_batch, T, tu.fwd, R, table, n, na, cta[na], k, 0, K, s);
+    bool any_pml = false;
+    for (int p = 0; p < na; ++p) any_pml |= P[p].grid.absorbing == NW_ABS_PML;
+    int rc = fork_join(
+        s, any_pml,
+        [&](cudaStream_t t) -> int {  // PML problems: receivers of level k and the layer cells
+          for (int p = 0; p < na; ++p) {
+            const nw_batch_problem& q = P[p];
+            if (q.grid.absorbing != NW_ABS_PML) continue;
+            int r = NW_OK;
+            if (k % q.time.substeps == 0)
+              r = launch_sample<T>(&q.grid, &q.acq, q.time.n_t, ring_level<T>(q, k), k / q.time.substeps,
+                                   (T*)q.traces, t);
+            if (!r) r = batch_pml_forward<T>(q, tu, k, false, t);
+            if (r) return r;
+          }
+          return NW_OK;
+        },
+        [&](cudaStream_t t) -> int { return NW_DISPATCH_BATCH(launch_fwd_batch, T, tu.fwd, R, table, n, na, cta[na], k, 0, K, t); });
     if (rc) return rc;
     for (int p = 0; p < na; ++p) {  // the final receiver sample of problems ending after step k
       const nw_batch_problem& q = P[p];
@@ -1487,9 +1523,21 @@ int batch_adjoint_impl(const nw_batch_problem* P, int n, const Tune& tu, const v
   }
   auto adj_step = [&](int step) -> int {
     const int na = batch_active(P, n, step, true);
-    int rc = NW_DISPATCH_BATCH(launch_adj_batch, T, tu.adj, R, table, n, na, acta[na], step, 0, K, s);
-    for (int p = 0; p < na && !rc; ++p)  // PML problems: the layer cells and the cotangents
-      if (P[p].grid.absorbing == NW_ABS_PML) rc = batch_pml_adjoint<T>(P[p], tu, step, s);
+    bool any_pml = false;
+    for (int p = 0; p < na; ++p) any_pml |= P[p].grid.absorbing == NW_ABS_PML;
+    int rc = fork_join(
+        s, any_pml,
+        [&](cudaStream_t t) -> int {  // PML problems: the layer cells
+          for (int p = 0; p < na; ++p)
+            if (P[p].grid.absorbing == NW_ABS_PML) {
+              const int r = batch_pml_adjoint<T>(P[p], tu, step, t);
+              if (r) return r;
+            }
+          return NW_OK;
+        },
+        [&](cudaStream_t t) -> int { return NW_DISPATCH_BATCH(launch_adj_batch, T, tu.adj, R, table, n, na, acta[na], step, 0, K, t); });
+    for (int p = 0; p < na && !rc; ++p)  // and their cotangents, once both halves are done
+      if (P[p].grid.absorbing == NW_ABS_PML) rc = batch_pml_inject<T>(P[p], step, s);
     return rc;
   };
   int rc = adj_step(Nmax);  // problems with the largest step count start: q^N = A C R^T g_N
@@ -1507,9 +1555,19 @@ int batch_adjoint_impl(const nw_batch_problem* P, int n, const Tune& tu, const v
     }
     for (int k = n0; k < n1; ++k) {  // recompute Lap p^k into the segment buffers
       const int na = batch_active(P, n, k, false);
-      for (int p = 0; p < na; ++p)
-        if (P[p].grid.absorbing == NW_ABS_PML && (rc = batch_pml_forward<T>(P[p], tu, k, true, s))) return rc;
-      rc = NW_DISPATCH_BATCH(launch_fwd_batch, T, tu.fwd, R, table, n, na, fcta[na], k, 1, K, s);
+      bool any_pml = false;
+      for (int p = 0; p < na; ++p) any_pml |= P[p].grid.absorbing == NW_ABS_PML;
+      rc = fork_join(
+          s, any_pml,
+          [&](cudaStream_t t) -> int {
+            for (int p = 0; p < na; ++p)
+              if (P[p].grid.absorbing == NW_ABS_PML) {
+                const int r = batch_pml_forward<T>(P[p], tu, k, true, t);
+                if (r) return r;
+              }
+            return NW_OK;
+          },
+          [&](cudaStream_t t) -> int { return NW_DISPATCH_BATCH(launch_fwd_batch, T, tu.fwd, R, table, n, na, fcta[na], k, 1, K, t); });
       if (rc) return rc;
     }
     for (int step = n1 - 1; step >= n0; --step) {
