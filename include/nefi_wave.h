@@ -226,9 +226,9 @@ int nw_initial_state(const nw_grid* g, const int32_t* n_abs, const nw_medium* m,
  * step; with checkpointing, snapshots of every segment start in [n_begin, n_end) are encoded.
  * On entry ring levels n_begin-1 and n_begin must be in place. `tune` may be NULL.
  * With the PML and an interior box of at least one tile, each step forks its layer kernel onto a
- * second stream of the calling thread and joins it back into `stream`; the first such call on a
- * thread and device creates that stream and two events, so make it before any stream capture (the
- * same holds for nw_adjoint and the batched sweeps).
+ * second stream of the calling thread and joins it back into `stream` (also in nw_adjoint and the
+ * batched sweeps); the first such call on a thread and device creates that stream and two events,
+ * in relaxed capture mode, and keeps them until the process exits.
  * Replaces WaveOperator.simulate / run_timestepping (nefi/physics/wave.py:699-740,
  * nefi/physics/timestep.py:144-149).
  */

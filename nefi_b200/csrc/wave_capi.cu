@@ -444,10 +444,17 @@ int side_stream(SideStream** out) {
   NW_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return fail(NW_ERR_UNSUPPORTED, "device index above 63");
   SideStream& r = per_device[dev];
-  if (!r.s) {
-    NW_CUDA(cudaStreamCreateWithFlags(&r.s, cudaStreamNonBlocking));
-    NW_CUDA(cudaEventCreateWithFlags(&r.fork, cudaEventDisableTiming));
-    NW_CUDA(cudaEventCreateWithFlags(&r.join, cudaEventDisableTiming));
+  if (!r.s) {  // created in relaxed capture mode, so a first call inside a stream capture is safe too
+    cudaStreamCaptureMode mode = cudaStreamCaptureModeRelaxed;
+    NW_CUDA(cudaThreadExchangeStreamCaptureMode(&mode));
+    const cudaError_t e0 = cudaStreamCreateWithFlags(&r.s, cudaStreamNonBlocking);
+    const cudaError_t e1 = e0 ? e0 : cudaEventCreateWithFlags(&r.fork, cudaEventDisableTiming);
+    const cudaError_t e2 = e1 ? e1 : cudaEventCreateWithFlags(&r.join, cudaEventDisableTiming);
+    NW_CUDA(cudaThreadExchangeStreamCaptureMode(&mode));
+    if (e2 != cudaSuccess) {
+      r.s = nullptr;
+      return fail(NW_ERR_CUDA, std::string("side stream: ") + cudaGetErrorString(e2));
+    }
   }
   *out = &r;
   return NW_OK;
