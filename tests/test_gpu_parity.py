@@ -345,3 +345,57 @@ def test_pml_interior_through_tiled_kernels_matches_the_oracle(dtype, tt, tg, cu
     cd2 = c.to(dtype).to(cuda_device).requires_grad_(True)
     (gk,) = torch.autograd.grad((opk({"c": cd2}) * gt).sum(), cd2)
     assert torch.equal(gk, gc)
+
+
+def test_pml_forward_captured_in_a_fresh_thread(cuda_device):
+    """A PML forward sweep (its layer kernel on the calling thread's second stream) captured into a
+    CUDA graph by a thread that never ran one: the second stream is created inside the capture, and
+    the replay equals the eager sweep."""
+    import ctypes as C
+    import threading
+
+    from nefi_b200 import _lib
+    from nefi_b200.operators import _forward_sweep, _Run
+
+    shape, extent, c, src, rec, kw = _pml_interior_case()
+    op = WaveOperatorB200(Domain(shape, extent), src, rec, grad_mode="autograd", **kw)
+    plan = op._plan(cuda_device, torch.float32)
+    S = op.n_sources
+    cd = c.float().to(cuda_device).contiguous()
+    c2dt2 = torch.empty(plan.field, device=cuda_device, dtype=torch.float32)
+    _lib.check(_lib.load().nw_prepare_medium(C.byref(plan.g), plan.n_abs, cd.data_ptr(), op.dt**2,
+                                             c2dt2.data_ptr(), _lib.stream_handle(cuda_device)))
+    medium, acq = plan.medium(c2dt2), plan.acquisition(S)
+    run = _Run(plan, S, op.n_steps, ("ring", None), "exact")
+    traces = torch.zeros(S, plan.n_rec, op.n_t, device=cuda_device)
+
+    def sweep(stream_handle):
+        run.ring.zero_()
+        run.psi.zero_()
+        _forward_sweep(plan, medium, acq, run, 0, op.n_steps, traces, stream_handle)
+
+    sweep(_lib.stream_handle(cuda_device))  # this thread: kernels loaded, shared-memory opt-ins done
+    torch.cuda.synchronize(cuda_device)
+    eager = traces.clone()
+    traces.zero_()
+    out = {}
+
+    def worker():
+        try:
+            torch.cuda.set_device(cuda_device)
+            st = torch.cuda.Stream(cuda_device)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.stream(st):
+                with torch.cuda.graph(g, stream=st):
+                    sweep(st.cuda_stream)
+            g.replay()
+            torch.cuda.synchronize(cuda_device)
+            out["y"] = traces.clone()
+        except Exception as e:  # reported by the main thread
+            out["err"] = e
+
+    t = threading.Thread(target=worker)
+    t.start()
+    t.join(timeout=300)
+    assert "err" not in out, out.get("err")
+    assert torch.equal(out["y"], eager)
