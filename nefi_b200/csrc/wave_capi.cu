@@ -1757,7 +1757,7 @@ int filter_response(int kind, int n_t, double dt, double f, double taper, std::v
   std::vector<double> w(J + 1);
   const double f1 = (1.0 - taper) * f;
   for (int j = 0; j <= J; ++j) {
-    const double fj = (double)j / ((double)N * dt);
+    const double fj = (double)j * (1.0 / ((double)N * dt));  // rfftfreq's own rounding: j * (1 / (N dt))
     if (kind == NW_FILTER_GAUSSIAN) {
       w[j] = std::exp(-0.5 * (fj / f) * (fj / f));
     } else {

@@ -290,6 +290,8 @@ def main():
     misfit_case("misfit_bl_abs", 5, 1001, 0.001, {"f_max": 25.0, "dt": 0.001, "taper": 0.2, "relative": False}, 19,
                 sensor=80.0)
     misfit_case("misfit_plain_rel", 4, 64, 0.01, {"f_max": None, "dt": 0.01, "relative": True}, 20, mask_rows=[2])
+    # a brick-wall window (taper 0) whose cutoff falls on an rfft bin up to rounding (f_108 of 540 bins)
+    misfit_case("misfit_brick", 3, 257, 0.002, {"f_max": 100.0, "dt": 0.002, "taper": 0.0, "relative": True}, 21)
 
 
 if __name__ == "__main__":
