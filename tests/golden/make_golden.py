@@ -186,6 +186,23 @@ def misfit_case(name, n_rows, n_t, dt, kw, seed, mask_rows=None, sensor=None):
     save(name, out)
 
 
+def gen_pat_case(name, shape, extent, receivers, c_coarse, p0_fine, kw, factor):
+    """Photoacoustic traces through ``at_resolution`` (nefi/physics/wave.py:822-835): the operator built
+    on the native grid with a known speed map, called with ``p0`` on the refined grid, so the speed is
+    resampled (nefi/utils/tensor.py:35-69) before the run; float64."""
+    if not wanted(name):
+        return
+    dom = Domain(shape, extent)
+    op = WaveInitialConditionOperator(dom, receivers, c=c_coarse, **kw).to(dtype=F64)
+    fine = tuple(int(s) * factor for s in shape)
+    with torch.no_grad():
+        tr = op.at_resolution(fine)({"p0": p0_fine.to(F64)})
+    out = {"kind": "genpat", "shape": list(shape), "fine": list(fine), "extent": [list(e) for e in extent],
+           "receivers": np.asarray(receivers, dtype=np.float64), "c": c_coarse.numpy(), "p0": p0_fine.numpy(),
+           "kw": kw, "seed": 0, "rec_stride": 1, "traces_f64": tr.numpy()}
+    save(name, out)
+
+
 def wanted(name):
     return not ONLY or name.startswith(ONLY)
 
@@ -292,6 +309,13 @@ def main():
     misfit_case("misfit_plain_rel", 4, 64, 0.01, {"f_max": None, "dt": 0.01, "relative": True}, 20, mask_rows=[2])
     # a brick-wall window (taper 0) whose cutoff falls on an rfft bin up to rounding (f_108 of 540 bins)
     misfit_case("misfit_brick", 3, 257, 0.002, {"f_max": 100.0, "dt": 0.002, "taper": 0.0, "relative": True}, 21)
+
+    # photoacoustic traces through at_resolution: a 2-D speed map resampled to the refined grid
+    gp = torch.Generator().manual_seed(22)
+    cpc = 1.0 + 0.05 * torch.rand(n2, n2, generator=gp, dtype=F64)
+    p0f = torch.rand(2 * n2, 2 * n2, generator=gp, dtype=F64)
+    gen_pat_case("genpat2x_o4_sponge", (n2, n2), ((-1.0, 1.0), (-1.0, 1.0)), ring, cpc, p0f,
+                 dict(n_t=40, dt_obs=0.03, order=4, absorbing="sponge", absorb_width=0.25), 2)
 
 
 if __name__ == "__main__":

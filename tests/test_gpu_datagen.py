@@ -29,3 +29,17 @@ def test_fp64_supersampled_generation_matches_reference(name, cuda_device):
     assert fine is op.at_resolution(tuple(case["fine"])) and fine.grid.shape == tuple(case["fine"])
     assert tr.dtype == torch.float64 and tr.device.type == "cuda"
     assert rel_l2(tr.cpu().numpy(), case["traces_f64"]) < 1e-11
+
+
+def test_photoacoustic_at_resolution_resamples_the_speed_like_the_reference(cuda_device):
+    """The photoacoustic operator at a finer resolution resamples its known speed map before the run
+    (nefi/physics/wave.py:822-835): float64 traces equal the reference's to rounding."""
+    from nefi_b200 import WaveInitialConditionOperatorB200
+
+    case = load_golden("genpat2x_o4_sponge")
+    dom = Domain(tuple(case["shape"]), tuple(tuple(e) for e in case["extent"]))
+    op = WaveInitialConditionOperatorB200(dom, case["receivers"], c=torch.tensor(case["c"]), **case["kw"])
+    fine = op.to(device=cuda_device, dtype=torch.float64).at_resolution(tuple(case["fine"]))
+    with torch.no_grad():
+        tr = fine({"p0": torch.tensor(case["p0"], dtype=torch.float64, device=cuda_device)})
+    assert rel_l2(tr.cpu().numpy(), case["traces_f64"]) < 1e-11
