@@ -184,17 +184,26 @@ def test_pat_adjoint_identity_and_linearity_float64(cuda_device):
     assert float((ya * y).sum()) == pytest.approx(float((a * adj).sum()), rel=1e-9)
 
 
-def test_source_batching_and_speed_check(cuda_device):
-    """tests/test_physics_wave.py:168-189 on the device."""
+@pytest.mark.parametrize("absorbing", ["pml", "sponge"])
+def test_multiresolution_source_batching_and_speed_check(absorbing, cuda_device):
+    """tests/test_physics_wave.py:168-189 on the device: a 2x coarser grid gives the same physics
+    within 20 %, shot chunks give the same traces, a speed above c_max is refused."""
     dom = Domain((32, 32), ((0.0, 1.0), (0.0, 1.0)))
     src = [[0.1, 0.3], [0.1, 0.5], [0.1, 0.7]]
     rec = [[0.9, y] for y in torch.linspace(0.1, 0.9, 6).tolist()]
-    kw = dict(n_t=60, dt_obs=0.016, f0=3.0, c_max=2.5, absorb_width=0.25, absorbing="sponge")
+    kw = dict(n_t=60, dt_obs=0.016, f0=3.0, c_max=2.5, absorb_width=0.25, absorbing=absorbing)
     op = WaveOperatorB200(dom, src, rec, **kw)
     x = dom.physical_coords(dtype=torch.float64)
     c = (2.0 + 0.2 * torch.exp(-((x - 0.5) ** 2).sum(-1) / 0.02)).to(cuda_device)
     y = op({"c": c})
-    assert y.shape == (3, 6, 60)
+    assert y.shape == (3, 6, 60) == op.output_shape((32, 32))
+    coarse = op.at_resolution((16, 16))
+    assert coarse is op.at_resolution((16, 16)) and coarse.grid.shape == (16, 16)
+    assert coarse.fidelity_tag == op.fidelity_tag
+    xc = dom.at((16, 16)).physical_coords(dtype=torch.float64)
+    yc = coarse({"c": (2.0 + 0.2 * torch.exp(-((xc - 0.5) ** 2).sum(-1) / 0.02)).to(cuda_device)})
+    assert yc.shape == y.shape
+    assert float((yc - y).norm() / y.norm()) < 0.2
     batched = WaveOperatorB200(dom, src, rec, source_batch=2, **kw)
     assert torch.allclose(batched({"c": c}), y, atol=1e-12)
     with pytest.raises(OperatorError, match="exceeds"):

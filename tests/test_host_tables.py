@@ -265,3 +265,30 @@ def test_pml_core_box_is_exactly_trivial(dtype):
             # one more row or column on any side would leave the trivial set
             a = op.grid.n_abs
             assert (x0, x1, z0, z1) == (a[0], P[0] - a[0], a[1], P[1] - a[1])
+
+
+def test_cfl_limit_and_ricker_wavelet():
+    """tests/test_physics_wave.py:60-64 and :217-221: the leapfrog step limits of the order-2 and
+    order-4 Laplacians, the refused safety factors, and the Ricker wavelet's peak, start and mean."""
+    import math
+
+    from nefi_b200.geometry import TimeAxis, ricker, stable_dt
+
+    h = (0.1, 0.1)
+    assert math.isclose(stable_dt(1.0, h, order=2, courant=1.0), 0.1 / math.sqrt(2))
+    assert math.isclose(stable_dt(1.0, h, order=4, courant=1.0), 0.1 * math.sqrt(3 / 8))
+    for bad in (0.0, 1.05):
+        with pytest.raises(ConfigError):
+            stable_dt(1.0, h, courant=bad)
+    with pytest.raises(ConfigError):
+        stable_dt(0.0, h)
+    with pytest.raises(ConfigError):
+        stable_dt(1.0, h, order=6)
+    # the simulation step divides the observation step evenly and stays inside the limit
+    ta = TimeAxis(100, 0.01, 2.5, h, 4, 0.9)
+    assert ta.dt * ta.substeps == pytest.approx(0.01) and ta.dt <= stable_dt(2.5, h, 4, 0.9)
+    assert ta.n_steps == 99 * ta.substeps
+    t = torch.linspace(0, 1, 2001, dtype=torch.float64)
+    w = ricker(t, 5.0)
+    assert abs(float(w.max()) - 1.0) < 1e-6 and abs(float(t[w.argmax()]) - 1.2 / 5.0) < 1e-3
+    assert abs(float(w[0])) < 1e-4 and abs(float(w.sum() * (t[1] - t[0]))) < 1e-4
