@@ -224,3 +224,24 @@ def test_short_and_single_traces_against_the_oracle(n_t, n_tr):
     loss, g = mf.value_and_grad(_t(pred, torch.float64))
     assert _rel(loss, lo) < 1e-11
     assert rel_l2(g.cpu().numpy(), go) < 1e-10
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_filters_are_zero_phase_and_attenuate(dtype):
+    """tests/test_photoacoustic3d.py:40-46 and tests/test_instances_wave_family.py:49-55 on the device:
+    the pass band comes through without a phase shift, the stop band is removed, a single 1-D trace
+    is filtered like a row, and no sensor cutoff returns the input itself."""
+    t = torch.arange(200, dtype=torch.float64, device="cuda") * 0.05
+    slow, fast = torch.sin(2 * torch.pi * 0.2 * t).to(dtype), torch.sin(2 * torch.pi * 4.0 * t).to(dtype)
+    out = gaussian_lowpass(torch.stack([slow, fast]), 0.05, 1.0)
+    assert float((out[0] - slow)[20:-20].abs().max()) < 0.05
+    assert float(out[1][20:-20].abs().max()) < 1e-3
+    single = gaussian_lowpass(slow, 0.05, 1.0)  # no partner trace in its complex pair
+    assert single.shape == slow.shape
+    assert rel_l2(single.cpu().numpy(), out[0].cpu().numpy()) < TOL[dtype][0]
+    assert gaussian_lowpass(slow, 0.05, None) is slow
+    dt = 0.004
+    t = torch.arange(500, dtype=torch.float64, device="cuda") * dt
+    low, high = torch.sin(2 * torch.pi * 2.0 * t), torch.sin(2 * torch.pi * 20.0 * t)
+    y = lowpass((low + high).to(dtype), dt, f_max=6.0)
+    assert float((y[100:400].double() - low[100:400]).abs().max()) < 0.05
