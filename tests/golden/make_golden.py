@@ -317,6 +317,16 @@ def main():
     gen_pat_case("genpat2x_o4_sponge", (n2, n2), ((-1.0, 1.0), (-1.0, 1.0)), ring, cpc, p0f,
                  dict(n_t=40, dt_obs=0.03, order=4, absorbing="sponge", absorb_width=0.25), 2)
 
+    # 2-D PML on a grid whose interior holds whole step tiles, so that a propagator which sends the
+    # trivial interior box through its plain step and only the layer through the PML update is
+    # checked against the reference on both parts
+    gb = torch.Generator().manual_seed(21)
+    cb = (2.0 + 0.15 * torch.randn(56, 200, generator=gb, dtype=F64)).clamp(1.7, 2.3)
+    cb = torch.nn.functional.avg_pool2d(cb[None, None], 5, 1, 2, count_include_pad=False)[0, 0]
+    fwi_case("fwi_o4_pml_box", (56, 200), ((0.0, 0.56), (0.0, 2.0)), [[0.05, 0.4], [0.3, 1.5]],
+             [[0.02, 0.1 + 0.09 * i] for i in range(20)] + [[0.5, 1.0]], cb,
+             dict(n_t=50, dt_obs=0.004, f0=25.0, c_max=2.5, order=4, absorbing="pml", absorb_width=0.08), 23)
+
 
 if __name__ == "__main__":
     main()

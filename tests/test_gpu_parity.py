@@ -321,7 +321,7 @@ def test_results_do_not_depend_on_the_launch_shape(dtype, cuda_device):
 
 def _pml_interior_case():
     """A PML grid whose interior holds several tiles, so the interior runs through the tiled kernels
-    and only the layer through the PML kernel (the golden PML grids are smaller than a tile)."""
+    and only the layer through the PML kernel (the geometry of the ``fwi_o4_pml_box`` fixture)."""
     g = torch.Generator().manual_seed(21)
     shape, extent = (56, 200), ((0.0, 0.56), (0.0, 2.0))
     c = (2.0 + 0.15 * torch.randn(shape, generator=g, dtype=torch.float64)).clamp(1.7, 2.3)
@@ -330,6 +330,20 @@ def _pml_interior_case():
     rec = [[0.02, 0.1 + 0.09 * i] for i in range(20)] + [[0.5, 1.0]]
     kw = dict(n_t=50, dt_obs=0.004, f0=25.0, c_max=2.5, order=4, absorbing="pml", absorb_width=0.08)
     return shape, extent, c, src, rec, kw
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_pml_box_fixture_sends_its_interior_through_the_tiled_kernels(dtype, cuda_device):
+    """The reference fixture ``fwi_o4_pml_box`` (checked by the float64/float32 parity tests above)
+    has a trivial interior box larger than the forward and the adjoint tiles, after the box's first
+    column is rounded up to a 16-byte boundary."""
+    case = load_golden("fwi_o4_pml_box")
+    plan = make_op(case)._plan(cuda_device, dtype)
+    x0, x1, z0, z1 = plan.pml["core"]
+    epc = 16 // torch.tensor([], dtype=dtype).element_size()
+    z0 = -(-z0 // epc) * epc
+    for tx, tz in (plan.tile, plan.adj_tile):
+        assert x1 - x0 >= tx and z1 - z0 >= tz
 
 
 @pytest.mark.parametrize("dtype,tt,tg", [(torch.float64, 1e-11, 1e-10), (torch.float32, 1e-5, 1e-4)])
