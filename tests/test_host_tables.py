@@ -292,3 +292,24 @@ def test_cfl_limit_and_ricker_wavelet():
     w = ricker(t, 5.0)
     assert abs(float(w.max()) - 1.0) < 1e-6 and abs(float(t[w.argmax()]) - 1.2 / 5.0) < 1e-3
     assert abs(float(w[0])) < 1e-4 and abs(float(w.sum() * (t[1] - t[0]))) < 1e-4
+
+
+def test_sensor_wrapped_3d_operator_shapes_and_resolution_cache():
+    """tests/test_photoacoustic3d.py:27-37 with the drop-ins: a planar 8x8 sensor array on the top
+    face, the trace shape independent of the grid, one cached operator per resolution, and the
+    fidelity tag carried to the coarse operator."""
+    from nefi_b200.misfit import SensorBandwidthB200
+
+    dom = Domain((20, 20, 14), ((0.0, 3.0), (0.0, 3.0), (0.0, 2.1)))
+    xs = (torch.arange(8, dtype=torch.float64) + 0.5) * 3.0 / 8
+    X, Y = torch.meshgrid(xs, xs, indexing="ij")
+    sensors = torch.stack([X.ravel(), Y.ravel(), torch.zeros(64, dtype=torch.float64)], -1)
+    inner = WaveInitialConditionOperatorB200(dom, sensors, n_t=40, dt_obs=0.05, c=1.5, order=2,
+                                             absorbing="sponge", absorb_width=0.45)
+    op = SensorBandwidthB200(inner, 0.05, 2.0)
+    assert op.homogeneity == 1.0 and op.primary == "p0" and op.required_fields() == ("p0",)
+    assert op.output_shape((20, 20, 14)) == (64, 40) == op.output_shape((10, 10, 7))
+    coarse = op.at_resolution((10, 10, 7))
+    assert coarse is op.at_resolution((10, 10, 7)) and coarse.inner.domain.shape == (10, 10, 7)
+    assert coarse.fidelity_tag == op.fidelity_tag and op.at_resolution((20, 20, 14)) is op
+    assert SensorBandwidthB200(inner, 0.05, None).fidelity_tag == inner.fidelity_tag
