@@ -543,8 +543,6 @@ def run_misfit(args) -> None:
 
     # the unfused chain with torch.fft (cuFFT), for comparison: G pred - obs, low-pass, masked mean, and
     # the backward through autograd
-    import math as _m
-
     def fast_len(n):
         m = n
         while True:
@@ -561,7 +559,7 @@ def run_misfit(args) -> None:
     f1 = 0.7 * 20.0
     w = torch.ones_like(f)
     roll = (f > f1) & (f < 20.0)
-    w[roll] = 0.5 * (1.0 + torch.cos(_m.pi * (f[roll] - f1) / (20.0 - f1)))
+    w[roll] = 0.5 * (1.0 + torch.cos(math.pi * (f[roll] - f1) / (20.0 - f1)))
     w[f >= 20.0] = 0.0
     w = w.float().to(dev)
     fs = torch.fft.rfftfreq(2 * n_t, d=dt, dtype=torch.float64)
