@@ -42,10 +42,9 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         return LIB
     cus = [str(p) for p in sorted(CSRC.glob("*.cu"))]
     tmp = LIB.with_suffix(".so.tmp")
-    cmd = [nvcc(), *ARCH_FLAGS, "-lineinfo", "-O3", "-std=c++17", "--use_fast_math=false",
+    cmd = [nvcc(), *ARCH_FLAGS, "-lineinfo", "-O3", "-std=c++17",
            "-Xcompiler", "-fPIC,-O2", "-shared", "-o", str(tmp), *cus,
            f"-I{ROOT / 'include'}", "-lcudart"]
-    cmd = [c for c in cmd if c != "--use_fast_math=false"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
