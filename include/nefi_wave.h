@@ -417,8 +417,9 @@ typedef struct nw_traces {
   int32_t log2_len;        /* nw_filter_log2_len(n_t) when a filter is passed (else ignored) */
 } nw_traces;
 
-/* Filter length exponent for traces of n_t samples: the smallest k >= 6 with 2^k >= 2 n_t. Filtered
- * traces are limited to 8192 samples in float32 and 4096 in float64 (the FFT stays in shared memory). */
+/* Filter length exponent for traces of n_t samples: the smallest k >= 6 with 2^k >= 2 n_t (n_t < 1
+ * returns NW_ERR_ARG, a value below 6). Filtered traces are limited to 8192 samples in float32 and
+ * 4096 in float64 (the FFT stays in shared memory); nw_filter_response refuses n_t > 8192. */
 int nw_filter_log2_len(int32_t n_t);
 
 /*

@@ -1749,6 +1749,7 @@ void host_fft(std::vector<double>& re, std::vector<double>& im) {
 // Hp[p] = H_L[bitrev(p)] / L for the reference's filter of `kind` on traces of n_t samples, float64.
 int filter_response(int kind, int n_t, double dt, double f, double taper, std::vector<double>* out) {
   if (n_t < 1 || !(dt > 0.0) || !(f > 0.0)) return fail(NW_ERR_ARG, "filter response needs n_t >= 1, dt > 0, f > 0");
+  if (n_t > 8192) return fail(NW_ERR_UNSUPPORTED, "filtered traces are limited to 8192 samples");
   if (kind != NW_FILTER_LOWPASS && kind != NW_FILTER_GAUSSIAN) return fail(NW_ERR_ARG, "unknown filter kind");
   if (kind == NW_FILTER_LOWPASS && !(taper >= 0.0 && taper <= 1.0)) return fail(NW_ERR_ARG, "taper must be in [0, 1]");
   // the reference's FFT length and half spectrum (losses.py:28-48; sensor.py:33-38)

@@ -7,6 +7,7 @@ import ctypes as C
 import re
 from pathlib import Path
 
+import numpy as np
 import pytest
 
 from nefi_b200 import _lib
@@ -100,3 +101,46 @@ def test_snapshot_pool_sizes(lib):
 def test_missing_library_fails_loudly(tmp_path):
     with pytest.raises(_lib.LibraryError, match="missing"):
         _lib.load(tmp_path / "libnefiwave.so")
+
+
+def test_filter_length_and_response_limits(lib):
+    assert lib.nw_filter_log2_len(0) == _lib.NW_ERR_ARG
+    assert [lib.nw_filter_log2_len(n) for n in (1, 32, 33, 4096, 4097, 8192)] == [6, 6, 7, 13, 14, 14]
+    out = np.empty(1 << 15, dtype=np.float64)
+    for kind in (_lib.NW_FILTER_LOWPASS, _lib.NW_FILTER_GAUSSIAN):
+        assert lib.nw_filter_response(kind, 8193, 1e-3, 50.0, 0.3, _lib.NW_F64, out.ctypes.data) == \
+            _lib.NW_ERR_UNSUPPORTED
+        assert lib.nw_filter_response(kind, 8192, 1e-3, 50.0, 0.3, _lib.NW_F64, out.ctypes.data) == _lib.NW_OK
+        assert lib.nw_filter_response(kind, 100, 0.0, 50.0, 0.3, _lib.NW_F64, out.ctypes.data) == _lib.NW_ERR_ARG
+    assert lib.nw_filter_response(7, 100, 1e-3, 50.0, 0.3, _lib.NW_F64, out.ctypes.data) == _lib.NW_ERR_ARG
+    assert lib.nw_filter_response(_lib.NW_FILTER_LOWPASS, 100, 1e-3, 50.0, 1.5, _lib.NW_F64,
+                                  out.ctypes.data) == _lib.NW_ERR_ARG
+
+
+def test_grid_validation_runs_before_any_device_call(lib):
+    """Entry points refuse a bad grid on the host: NULL, a 3-D PML, an unknown dtype, a padded extent
+    below 2, a field of 2^31 elements or more."""
+    shape = (C.c_int32 * 4)()
+    assert lib.nw_forward(None, None, None, None, None, None, 0, 0, None, None) == _lib.NW_ERR_ARG
+    assert b"NULL" in lib.nw_last_error()
+
+    def grid(**kw):
+        g = _lib.Grid()
+        g.ndim, g.order, g.dtype, g.absorbing = 2, 4, _lib.NW_F32, _lib.NW_ABS_SPONGE
+        g.n[0], g.n[1], g.n[2] = 64, 64, 1
+        for k, v in kw.items():
+            if k == "n":
+                g.n[0], g.n[1], g.n[2] = v
+            else:
+                setattr(g, k, v)
+        assert lib.nw_grid_layout(C.byref(g)) == _lib.NW_OK
+        return g
+
+    t = _lib.Tuning()
+    assert lib.nw_tile_shape(C.byref(grid()), C.byref(t), shape) == _lib.NW_OK
+    cases = [(dict(ndim=3, n=(16, 16, 16), absorbing=_lib.NW_ABS_PML), _lib.NW_ERR_UNSUPPORTED),
+             (dict(dtype=9), _lib.NW_ERR_ARG),
+             (dict(n=(1, 64, 1)), _lib.NW_ERR_ARG),
+             (dict(n=(50000, 50000, 1)), _lib.NW_ERR_ARG)]
+    for kw, rc in cases:
+        assert lib.nw_tile_shape(C.byref(grid(**kw)), C.byref(t), shape) == rc, kw
