@@ -8,6 +8,7 @@ Loading fails loudly when the library is missing: there is no CPU or eager fallb
 from __future__ import annotations
 
 import ctypes as C
+import functools
 from pathlib import Path
 
 import torch
@@ -170,6 +171,37 @@ def ptr(t: torch.Tensor | None) -> int | None:
 
 def stream_handle(device: torch.device) -> int:
     return torch.cuda.current_stream(device).cuda_stream
+
+
+def _cuda_device(v) -> torch.device | None:
+    if isinstance(v, torch.Tensor):
+        return v.device if v.is_cuda else None
+    if isinstance(v, str) and v.startswith("cuda"):
+        return torch.device(v)
+    if isinstance(v, torch.device):
+        return v if v.type == "cuda" else None
+    d = getattr(v, "device", None)
+    return d if isinstance(d, torch.device) and d.type == "cuda" else None
+
+
+def on_device(fn):
+    """Run ``fn`` with the current CUDA device set to the device of its first CUDA tensor argument
+    (else of its first argument naming a CUDA device, or holding one as ``.device``). The library
+    launches on the current device and the side streams it keeps are per device, so a call whose
+    tensors live on another GPU than the current one runs there instead of failing or mixing devices."""
+
+    @functools.wraps(fn)
+    def wrapper(*args, **kwargs):
+        vals = (*args, *kwargs.values())
+        dev = next((v.device for v in vals if isinstance(v, torch.Tensor) and v.is_cuda), None)
+        if dev is None:
+            dev = next((d for d in map(_cuda_device, vals) if d is not None), None)
+        if dev is None:
+            return fn(*args, **kwargs)
+        with torch.cuda.device(dev):
+            return fn(*args, **kwargs)
+
+    return wrapper
 
 
 def dtype_code(dtype: torch.dtype) -> int:

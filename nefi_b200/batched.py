@@ -63,6 +63,7 @@ class BatchedFWI:
         self._build()
 
     # -- buffers and the device table ----------------------------------------------------------
+    @_lib.on_device
     def _build(self) -> None:
         lib = _lib.load()
         dev, K = self.device, self.segment
@@ -122,6 +123,7 @@ class BatchedFWI:
                    if isinstance(t, torch.Tensor)) + self.table.numel()
 
     # -- one gradient ---------------------------------------------------------------------------
+    @_lib.on_device
     def _step(self) -> None:
         """The whole batched gradient from the static inputs (``c``, ``obs``) to the outputs."""
         lib = _lib.load()
@@ -166,6 +168,7 @@ class BatchedFWI:
             grads[i] = self.bufs[slot]["grad"]
         return losses, grads
 
+    @_lib.on_device
     def misfit_gradients(self, cs: Sequence[torch.Tensor], observed: Sequence[torch.Tensor]):
         """``(losses, grads)``: per problem, in the order the operators were given; the gradients are
         float64 (the tensors are reused by the next call: clone to keep them)."""
@@ -177,6 +180,7 @@ class BatchedFWI:
             self.check_snapshots()
         return self._outputs()
 
+    @_lib.on_device
     def check_snapshots(self) -> None:
         """Synchronise and raise if a 16-bit snapshot block held a non-finite value."""
         if self.snapshot == "exact":
@@ -187,6 +191,7 @@ class BatchedFWI:
             raise SolverError("a wavefield snapshot held a non-finite value: a forward run diverged")
         _lib.check(rc)
 
+    @_lib.on_device
     def capture(self) -> None:
         """Record the whole gradient as one CUDA graph; later ``misfit_gradients`` calls replay it.
         Runs the gradient once first (on the current inputs) so that every kernel's shared-memory
@@ -204,6 +209,7 @@ class BatchedFWI:
         torch.cuda.synchronize(self.device)
 
 
+@_lib.on_device
 def autotune(ops: Sequence[WaveOperatorB200], *, steps: int = 120, device="cuda", dtype=torch.float32,
              snapshot: str = "fixed16", fwd_candidates=((4, 2, 2), (2, 4, 2), (4, 2, 1), (2, 2, 2), (4, 4, 1)),
              adj_candidates=((2, 2, 4), (2, 2, 2), (4, 2, 4), (2, 4, 4), (2, 2, 8)), repeats: int = 2):

@@ -68,6 +68,7 @@ def _traces(x: torch.Tensor, mask: torch.Tensor | None = None, per_sample: bool 
     return t
 
 
+@_lib.on_device
 def _apply_filter(x: torch.Tensor, kind: int, dt: float, f: float, taper: float) -> torch.Tensor:
     _check(x, "traces")
     x = x.contiguous()
@@ -135,6 +136,7 @@ class TraceMisfit:
              if self.sensor_cutoff is not None else None)
         return w, g
 
+    @_lib.on_device
     def prepare(self, obs: torch.Tensor, mask: torch.Tensor | None = None, always: bool = False) -> None:
         """Fix the observed traces ``obs`` (``(..., n_t)``, CUDA) and their weights. The observation's
         terms are recomputed only when ``obs`` or ``mask`` changed, or with ``always`` (a caller that
@@ -166,6 +168,7 @@ class TraceMisfit:
             1 if self.relative else 0, state.data_ptr(), _lib.stream_handle(obs.device)))
         self._obs, self._mask, self._state, self._key = obs, m, state, key
 
+    @_lib.on_device
     def value_and_grad(self, pred: torch.Tensor, rows: slice | None = None, want_grad: bool = True,
                        out: torch.Tensor | None = None):
         """Add ``pred`` (the rows ``rows`` of the prepared observation along its first axis, all rows by
@@ -176,19 +179,22 @@ class TraceMisfit:
             raise ConfigError("TraceMisfit.prepare(observed) must come first")
         _check(pred, "pred")
         obs, m = self._obs, self._mask
-        if rows is not None:
-            obs = obs[rows]
-            m = None if m is None else m[rows]
+        if rows is not None:  # the kernels read dense rows: a strided selection is gathered first
+            obs = obs[rows].contiguous()
+            m = None if m is None else m[rows].contiguous()
         if tuple(pred.shape) != tuple(obs.shape):
             raise ShapeError(f"pred has shape {tuple(pred.shape)}, observed rows {tuple(obs.shape)}")
         if pred.dtype != obs.dtype:
             raise ConfigError(f"pred dtype {pred.dtype} differs from the observed {obs.dtype}")
+        if pred.device != obs.device:
+            raise ConfigError(f"pred is on {pred.device}, the observed traces on {obs.device}")
         pred = pred.detach().contiguous()
         grad = None
         if want_grad:
             if out is not None:
-                if tuple(out.shape) != tuple(pred.shape) or out.dtype != pred.dtype or not out.is_contiguous():
-                    raise ShapeError("out must be a contiguous tensor of pred's shape and dtype")
+                if (tuple(out.shape) != tuple(pred.shape) or out.dtype != pred.dtype or not out.is_contiguous()
+                        or out.device != pred.device):
+                    raise ShapeError("out must be a contiguous tensor of pred's shape, dtype and device")
                 grad = out
             else:
                 grad = torch.empty_like(pred)

@@ -242,6 +242,7 @@ def _adjoint_sweep(plan: DevicePlan, medium, acq, run: _Run, grad_traces: torch.
 # ------------------------------------------------------------------------------------------------
 class _FWIFunction(torch.autograd.Function):
     @staticmethod
+    @_lib.on_device
     def forward(ctx, c: torch.Tensor, op: "WaveOperatorB200", shot0: int, n_shots: int):
         plan = op._plan(c.device, c.dtype)
         stream = _lib.stream_handle(c.device)
@@ -268,6 +269,7 @@ class _FWIFunction(torch.autograd.Function):
 
     @staticmethod
     @once_differentiable
+    @_lib.on_device
     def backward(ctx, grad_traces: torch.Tensor):
         (c,) = ctx.saved_tensors
         op, run = ctx.op, ctx.run
@@ -362,6 +364,7 @@ class WaveOperatorB200(_LeapfrogB200):
         outs = [_FWIFunction.apply(c, self, s0, min(n, s0 + chunk) - s0) for s0 in range(0, n, chunk)]
         return outs[0] if len(outs) == 1 else torch.cat(outs, dim=0)
 
+    @_lib.on_device
     def misfit_gradient(self, c: torch.Tensor, observed: torch.Tensor, events: dict | None = None,
                         misfit=None, mask: torch.Tensor | None = None):
         """One FWI gradient without autograd: ``(J, dJ/dc)`` for ``J = 1/2 ||F(c) - observed||^2``, or,
@@ -426,6 +429,7 @@ class WaveOperatorB200(_LeapfrogB200):
             loss = j.clone()
         return loss, grad
 
+    @_lib.on_device
     def simulate(self, c: torch.Tensor, observe: Callable | None = None,
                  record: Sequence[int] | None = None, sources: slice | None = None):
         """Leapfrog run returning ``(state, obs)`` like the reference's ``simulate``
@@ -475,6 +479,7 @@ class WaveOperatorB200(_LeapfrogB200):
 # ------------------------------------------------------------------------------------------------
 class _PATFunction(torch.autograd.Function):
     @staticmethod
+    @_lib.on_device
     def forward(ctx, p0: torch.Tensor, c: torch.Tensor, op: "WaveInitialConditionOperatorB200",
                 c2dt2_known: torch.Tensor | None):
         plan = op._plan(p0.device, p0.dtype)
@@ -511,6 +516,7 @@ class _PATFunction(torch.autograd.Function):
 
     @staticmethod
     @once_differentiable
+    @_lib.on_device
     def backward(ctx, grad_traces: torch.Tensor):
         (c,) = ctx.saved_tensors
         op, run, S = ctx.op, ctx.run, ctx.S

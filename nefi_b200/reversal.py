@@ -22,6 +22,7 @@ from .plan import ghost_view
 
 
 @torch.no_grad()
+@_lib.on_device
 def time_reversal(traces, domain, receivers, *, dt_obs: float, c=1.0, mode: str = "dirichlet", order: int = 4,
                   absorbing: str = "pml", absorb_width: float | None = None, absorb_R: float = 1e-3,
                   courant: float = 0.9) -> torch.Tensor:

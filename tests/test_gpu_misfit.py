@@ -149,6 +149,13 @@ def test_row_slices_accumulate_to_the_whole():
         grads.append(g)
     assert _rel(loss, whole) < 1e-13
     assert rel_l2(torch.cat(grads).cpu().numpy(), case["grad_f64"]) < 1e-10
+    # strided selections (every other row) are gathered, then accumulate the same way
+    mf.prepare(obs, mask, always=True)
+    g = torch.empty_like(pred)
+    for rows in (slice(0, None, 2), slice(1, None, 2)):
+        loss, g[rows] = mf.value_and_grad(pred[rows], rows=rows)
+    assert _rel(loss, whole) < 1e-13
+    assert rel_l2(g.cpu().numpy(), case["grad_f64"]) < 1e-10
 
 
 def test_filtered_length_limit_is_reported():

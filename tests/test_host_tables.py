@@ -313,3 +313,32 @@ def test_sensor_wrapped_3d_operator_shapes_and_resolution_cache():
     assert coarse is op.at_resolution((10, 10, 7)) and coarse.inner.domain.shape == (10, 10, 7)
     assert coarse.fidelity_tag == op.fidelity_tag and op.at_resolution((20, 20, 14)) is op
     assert SensorBandwidthB200(inner, 0.05, None).fidelity_tag == inner.fidelity_tag
+
+
+def test_device_guard_follows_the_arguments(monkeypatch):
+    """``_lib.on_device`` makes the arguments' GPU current for the library call: a CUDA tensor first,
+    else a device name or an object's ``.device``; with no CUDA device in sight it only calls."""
+    from nefi_b200 import _lib
+
+    seen = []
+
+    class Guard:
+        def __init__(self, d):
+            seen.append(torch.device(d))
+
+        def __enter__(self):
+            return self
+
+        def __exit__(self, *exc):
+            return False
+
+    monkeypatch.setattr(torch.cuda, "device", Guard)
+
+    class Holder:
+        device = torch.device("cuda", 3)
+
+    f = _lib.on_device(lambda *a, **k: "ran")
+    assert f(1, torch.zeros(2), device="cpu") == "ran" and seen == []
+    assert f(Holder()) == "ran" and seen == [torch.device("cuda", 3)]
+    assert f([torch.zeros(1)], device="cuda:2") == "ran" and seen[-1] == torch.device("cuda", 2)
+    assert f(torch.zeros(1), Holder(), device="cuda:1") == "ran" and seen[-1] == torch.device("cuda", 3)
