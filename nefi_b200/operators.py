@@ -154,8 +154,11 @@ class _LeapfrogB200(Operator):
     def _budget(self, device: torch.device) -> int:
         if self.memory_budget is not None:
             return int(self.memory_budget)
+        # memory the driver has free plus blocks PyTorch's caching allocator holds unused (the last
+        # gradient's history, say): the allocator hands those out again, or frees them on a miss
         free, _ = torch.cuda.mem_get_info(device)
-        return int(0.85 * free)
+        idle = torch.cuda.memory_reserved(device) - torch.cuda.memory_allocated(device)
+        return int(0.85 * (free + max(idle, 0)))
 
     def extra_repr(self) -> str:
         g = self.grid
@@ -293,8 +296,9 @@ class WaveOperatorB200(_LeapfrogB200):
     """Acoustic FWI forward model on the B200: sound speed ``c(x)`` -> traces of every source.
 
     Same arguments as ``nefi.physics.wave.WaveOperator`` (nefi/physics/wave.py:610-632), plus
-    ``snapshot`` (``"exact"`` | ``"fp16"`` | ``"bf16"``: encoding of checkpoint snapshots) and
-    ``memory_budget`` (bytes available for wavefield storage; default 85 % of free device memory).
+    ``snapshot`` (``"exact"`` | ``"fixed16"`` | ``"fp16"`` | ``"bf16"``: encoding of checkpoint snapshots) and
+    ``memory_budget`` (bytes available for wavefield storage; default 85 % of the device memory that
+    is free or held unused by PyTorch's allocator).
     Output ``(n_sources, n_receivers, n_t)`` at ``t_j = j dt_obs``; the gradient w.r.t. ``c`` is
     the exact discrete adjoint, reduced over shots in float64.
     """
