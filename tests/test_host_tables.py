@@ -342,3 +342,15 @@ def test_device_guard_follows_the_arguments(monkeypatch):
     assert f(Holder()) == "ran" and seen == [torch.device("cuda", 3)]
     assert f([torch.zeros(1)], device="cuda:2") == "ran" and seen[-1] == torch.device("cuda", 2)
     assert f(torch.zeros(1), Holder(), device="cuda:1") == "ran" and seen[-1] == torch.device("cuda", 3)
+
+
+def test_default_memory_budget_counts_the_allocators_idle_blocks(monkeypatch):
+    dom = Domain((16, 16), ((0.0, 1.0), (0.0, 1.0)))
+    op = WaveOperatorB200(dom, [[0.5, 0.5]], [[0.2, 0.2]], n_t=10, dt_obs=0.01, f0=5.0, c_max=2.5)
+    monkeypatch.setattr(torch.cuda, "mem_get_info", lambda d=None: (10 * 2**30, 180 * 2**30))
+    monkeypatch.setattr(torch.cuda, "memory_reserved", lambda d=None: 50 * 2**30)
+    monkeypatch.setattr(torch.cuda, "memory_allocated", lambda d=None: 20 * 2**30)
+    assert op._budget(torch.device("cuda", 0)) == int(0.85 * 40 * 2**30)
+    op2 = WaveOperatorB200(dom, [[0.5, 0.5]], [[0.2, 0.2]], n_t=10, dt_obs=0.01, f0=5.0, c_max=2.5,
+                           memory_budget=123)
+    assert op2._budget(torch.device("cuda", 0)) == 123
