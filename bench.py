@@ -8,7 +8,7 @@ misfit 1/2 ||F(c) - d||^2 with its gradient w.r.t. c reduced over shots in float
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
 Rank 0 prints one JSON line. Under torchrun every rank runs its own 16 shots (weak scaling) and the
-float64 gradient is summed with one NCCL all-reduce per step. ``--impl reference`` times the CPU
+float64 gradient and the scalar misfit are summed with NCCL all-reduces each step. ``--impl reference`` times the CPU
 restatement of the reference algorithm (the oracle, float32, all host threads) on a bounded sample.
 
 Other workloads (``--workload``), each printing one line of the same form:
@@ -746,8 +746,9 @@ def main() -> None:
 
     def step(cc, dd, events=None):
         loss, g = op.misfit_gradient(cc, dd, events=events)
-        if world > 1:
+        if world > 1:  # the float64 gradient and the scalar misfit summed over the ranks' shots
             dist.all_reduce(g)
+            dist.all_reduce(loss)
         return loss, g
 
     for _ in range(args.warmup):
@@ -889,7 +890,7 @@ def main() -> None:
                "vs_baseline": None, "dtype": "f32",
                "data": "synthetic (seeded layered model; observed data from a smoothed model)",
                "config": {**workload_desc(w, storage, op.absorbing), "method": f"plain (per-step launches, {storage})",
-                          "parallelism": f"shots sharded over {world} GPU(s), fp64 gradient all-reduce"},
+                          "parallelism": f"shots sharded over {world} GPU(s), fp64 gradient and loss all-reduce"},
                "gcell_updates_per_s": gcells, "roofline": roofline, "cpu_baseline": cpu,
                "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                        "ms_each": e2e_ms},
