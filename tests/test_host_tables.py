@@ -105,6 +105,10 @@ def test_tile_tables_partition_receivers_and_cells(name, tuning):
     case = load_golden(name)
     plan = make_op(case)._plan(CPU, torch.float32)
     plan.set_tuning(*tuning)
+    _check_tile_tables(plan)
+
+
+def _check_tile_tables(plan):
     TX, TZ = plan.tile
     assert TX == 8 * plan.tuning.rx and TZ == 32 * plan.tuning.vz
     AX, AZ = plan.adj_tile
@@ -128,6 +132,37 @@ def test_tile_tables_partition_receivers_and_cells(name, tuning):
             x, z = divmod(int(cells[gid[e]]), ld)
             assert x0 <= x < x0 + AX and z0 <= z < z0 + AZ
             assert local[e] == (x - x0) * AZ + (z - z0)
+
+
+def test_tile_tables_partition_random_geometries():
+    """The same invariants over seeded random grids, layers, tile shapes and receivers, including
+    receivers on the outermost admissible positions (the domain's corners with a layer, the corner
+    cell centres without), on cell centres and sharing cells."""
+    import random
+
+    rnd = random.Random(1234)
+    for _ in range(25):
+        n0, n1 = rnd.randint(8, 300), rnd.randint(8, 300)
+        h = rnd.choice([0.01, 0.02, 0.005])
+        ext = ((0.0, n0 * h), (0.0, n1 * h))
+        width = rnd.choice([0.0, 3 * h, 20 * h])
+        # without a layer a point must lie between the outermost cell centres (the reference's rule)
+        a0, a1 = (0.0, 0.0) if width else (0.5 * h, 0.5 * h)
+        b0, b1 = (n0 * h - a0, n1 * h - a1)
+        rec = [[rnd.uniform(a0, b0), rnd.uniform(a1, b1)] for _ in range(rnd.randint(1, 40))]
+        rec += [[a0, a1], [b0, b1], [a0, b1], [(0.5 + rnd.randrange(n0)) * h, 0.5 * h]]
+        rec += rec[:2]  # coincident receivers
+        order = rnd.choice([2, 4])
+        absorbing = "none" if width == 0.0 else rnd.choice(["sponge", "pml", "cerjan"])
+        op = WaveOperatorB200(Domain((n0, n1), ext), [[0.5 * n0 * h, 0.5 * n1 * h]], rec, n_t=5,
+                              dt_obs=0.001, f0=10.0, c_max=2.0, order=order, absorbing=absorbing,
+                              absorb_width=width)
+        for dtype in (torch.float32, torch.float64):
+            plan = op._plan(CPU, dtype)
+            vz = [2, 4] if dtype == torch.float32 else [2]
+            plan.set_tuning(rnd.choice(vz), rnd.choice([2, 4, 8]), rnd.randint(1, 5),
+                            rnd.choice(vz), rnd.choice([2, 4, 8]), rnd.randint(1, 5))
+            _check_tile_tables(plan)
 
 
 @pytest.mark.parametrize("n_shots", [1, 3, 16, 64])
