@@ -422,3 +422,49 @@ def test_pml_forward_captured_in_a_fresh_thread(cuda_device):
     t.join(timeout=300)
     assert "err" not in out, out.get("err")
     assert torch.equal(out["y"], eager)
+
+
+@pytest.mark.parametrize("seed", range(8))
+@pytest.mark.parametrize("dtype,tt,tg", [(torch.float64, 1e-11, 1e-10), (torch.float32, 1e-5, 1e-4)])
+def test_random_geometries_match_the_oracle(seed, dtype, tt, tg, cuda_device):
+    """Seeded random 2-D geometries (grid shape and spacing, every layer kind, order, substeps,
+    several shots, receivers anywhere in the domain, long enough for the wave to cross the domain)
+    through the device path against the float64 oracle: traces and the gradient of
+    ``sum(traces * g)``."""
+    import random
+
+    import oracle
+
+    rnd = random.Random(seed)
+    n0, n1 = rnd.randint(10, 90), rnd.randint(10, 170)
+    h0, h1 = rnd.choice([0.04, 0.05]), rnd.choice([0.04, 0.05])
+    ext = ((0.0, n0 * h0), (0.0, n1 * h1))
+    absorbing = ["none", "sponge", "cerjan", "pml"][seed % 4]
+    width = 0.0 if absorbing == "none" else rnd.choice([0.1, 0.2])
+    lo = 0.5 * max(h0, h1) if absorbing == "none" else 0.0
+
+    def point():
+        return [rnd.uniform(lo, n0 * h0 - lo), rnd.uniform(lo, n1 * h1 - lo)]
+
+    src = [point() for _ in range(rnd.randint(1, 5))]
+    rec = [point() for _ in range(rnd.randint(1, 12))]
+    dt_obs = rnd.choice([0.01, 0.02])  # long enough for the wave to cross the domain once
+    n_t = int((n0 * h0 + n1 * h1) / 1.6 / dt_obs) + 10
+    kw = dict(n_t=n_t, dt_obs=dt_obs, f0=rnd.choice([4.0, 6.0]), c_max=2.5,
+              order=rnd.choice([2, 4]), absorbing=absorbing, absorb_width=width)
+    g = np.random.default_rng(seed)
+    c = np.clip(2.0 + 0.2 * g.standard_normal((n0, n1)), 1.6, 2.4)
+    gt = g.standard_normal((len(src), len(rec), kw["n_t"]))
+    op = WaveOperatorB200(Domain((n0, n1), ext), src, rec, grad_mode="autograd", **kw)
+    cd = torch.tensor(c, dtype=dtype, device=cuda_device).requires_grad_(True)
+    tr = op({"c": cd})
+    (gc,) = torch.autograd.grad((tr * torch.tensor(gt, dtype=dtype, device=cuda_device)).sum(), cd)
+    orc = oracle.OracleWave((n0, n1), ext, np.asarray(rec), sources=np.asarray(src), **kw)
+    tr_o, gc_o = orc.fwi(c, gt, dtype=np.float64)
+    if dtype == torch.float32:
+        # float32 rounding grows with the step count (up to 1200 steps here): the bound is twice the
+        # error of the same arithmetic in float32 on the host, the reference's own float32 path
+        tr32, gc32 = orc.fwi(c, gt, dtype=np.float32)
+        tt, tg = max(tt, 2.0 * rel_l2(tr32, tr_o)), max(tg, 2.0 * rel_l2(gc32, gc_o))
+    assert rel_l2(tr.detach().cpu().numpy(), tr_o) < tt, (absorbing, kw)
+    assert rel_l2(gc.cpu().numpy(), gc_o) < tg, (absorbing, kw)

@@ -413,7 +413,9 @@ def test_kernel_semantics_match_the_oracle_on_random_geometries(seed):
 
     src = [point() for _ in range(rnd.randint(1, 3))]
     rec = [point() for _ in range(rnd.randint(1, 6))]
-    kw = dict(n_t=rnd.randint(8, 16), dt_obs=rnd.choice([0.01, 0.02]), f0=rnd.choice([4.0, 6.0]), c_max=2.5,
+    dt_obs = rnd.choice([0.01, 0.02])  # long enough for the wave to cross the domain once
+    n_t = int((n0 * h0 + n1 * h1) / 1.6 / dt_obs) + 10
+    kw = dict(n_t=n_t, dt_obs=dt_obs, f0=rnd.choice([4.0, 6.0]), c_max=2.5,
               order=rnd.choice([2, 4]), absorbing=absorbing, absorb_width=width)
     g = np.random.default_rng(seed)
     c = np.clip(2.0 + 0.2 * g.standard_normal((n0, n1)), 1.6, 2.4)
