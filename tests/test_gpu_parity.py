@@ -461,6 +461,7 @@ def test_random_geometries_match_the_oracle(seed, dtype, tt, tg, cuda_device):
     (gc,) = torch.autograd.grad((tr * torch.tensor(gt, dtype=dtype, device=cuda_device)).sum(), cd)
     orc = oracle.OracleWave((n0, n1), ext, np.asarray(rec), sources=np.asarray(src), **kw)
     tr_o, gc_o = orc.fwi(c, gt, dtype=np.float64)
+    assert np.linalg.norm(tr_o) > 0 and np.linalg.norm(gc_o) > 0  # the wave reaches the receivers
     if dtype == torch.float32:
         # float32 rounding grows with the step count (up to 1200 steps here): the bound is twice the
         # error of the same arithmetic in float32 on the host, the reference's own float32 path
