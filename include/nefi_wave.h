@@ -38,7 +38,7 @@ enum { NW_F32 = 0, NW_F64 = 1 };
 /* absorbing layer kind (nefi/physics/wave.py:80, 469-501); NW_ABS_PML is 2-D only */
 enum { NW_ABS_NONE = 0, NW_ABS_SPONGE = 1, NW_ABS_CERJAN = 2, NW_ABS_PML = 3 };
 /* snapshot encodings for checkpointed gradients */
-enum { NW_SNAP_EXACT = 0, NW_SNAP_F16 = 1, NW_SNAP_BF16 = 2, NW_SNAP_I16 = 3 };
+enum { NW_SNAP_EXACT = 0, NW_SNAP_F16 = 1, NW_SNAP_BF16 = 2, NW_SNAP_I16 = 3, NW_SNAP_D16 = 4 };
 /* status codes */
 enum {
   NW_OK = 0,
@@ -182,7 +182,11 @@ typedef struct nw_time {
  *    recomputes Lap p^{n0..n0+segment-1} into `segbuf` (segment levels). snap_kind selects exact
  *    copies or 16-bit values with one float scale per block of NW_SNAP_BLOCK elements: fp16 /
  *    bf16 with a power-of-two scale, or int16 mantissas scaled by the block maximum (NW_SNAP_I16,
- *    block floating point). The 16-bit kinds store p^{n0} and p^{n0} - p^{n0-1}.
+ *    block floating point), or (NW_SNAP_D16) int16 codes of the second differences along the
+ *    contiguous axis of integer values relative to a float anchor, with a float step per block
+ *    (element z = anchor + step * Q[z]; the step is 1/32000 of the block's largest second
+ *    difference, so the error of a smooth field is several times below NW_SNAP_I16's). The 16-bit
+ *    kinds store p^{n0} and p^{n0} - p^{n0-1}.
  *  both NULL: forward only.
  */
 #define NW_SNAP_BLOCK 32
@@ -278,7 +282,8 @@ int nw_initial_state_adjoint(const nw_grid* g, const int32_t* n_abs, const nw_me
 
 /*
  * Allocation-free gradient: the work of nw_adjoint followed by nw_reduce_grad_c (overwriting
- * grad_c), with the adjoint's scratch -- three adjoint levels and the float64 accumulators -- taken
+ * grad_c), with the adjoint's scratch -- the adjoint levels and the gradient accumulators (in the
+ * computation's dtype) -- taken
  * from one fixed array that the library holds in device memory instead of from caller buffers.
  * This entry point has no counterpart in the reference; it exists for callers that cannot allocate
  * device memory themselves: a host runtime that reaches this library only through the C ABI and
@@ -292,7 +297,9 @@ int nw_initial_state_adjoint(const nw_grid* g, const int32_t* n_abs, const nw_me
  *    NW_ERR_ARG with a message giving the size needed; use nw_adjoint then.
  *  - Every GPU that loads the library holds the 64 MiB array until the process exits.
  *  - The first call on a device looks up the array's device address (with that device current) and
- *    caches it; make that first call before any stream capture begins.
+ *    caches it; make that first call before any stream capture begins. The cached address belongs to
+ *    the device's current context: after cudaDeviceReset (or any teardown of the primary context)
+ *    the library must be unloaded and loaded again before this entry point is called.
  *  - All calls share the one array and it keeps the last call's contents; each call clears what it
  *    uses before use, but two calls whose GPU work overlaps (different streams or host threads)
  *    race on it, so serialise them.

@@ -23,7 +23,9 @@ NW_OK, NW_ERR_ARG, NW_ERR_CUDA, NW_ERR_UNSUPPORTED, NW_ERR_NONFINITE, NW_ERR_TIM
 NW_SNAP_BLOCK = 32
 
 NW_SNAP_I16 = 3
-SNAP_KINDS = {"exact": NW_SNAP_EXACT, "fp16": NW_SNAP_F16, "bf16": NW_SNAP_BF16, "fixed16": NW_SNAP_I16}
+NW_SNAP_D16 = 4
+SNAP_KINDS = {"exact": NW_SNAP_EXACT, "fp16": NW_SNAP_F16, "bf16": NW_SNAP_BF16, "fixed16": NW_SNAP_I16,
+              "delta16": NW_SNAP_D16}
 
 
 class Grid(C.Structure):

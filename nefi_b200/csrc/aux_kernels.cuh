@@ -405,4 +405,168 @@ __global__ void __launch_bounds__(256) snap_decode(const typename Codec<K>::H* _
   }
 }
 
+// ------------------------------------------------------------------------------------------
+// delta16 snapshot codec: a block of SNAP_BLOCK values x[0..31] (one warp, lane = element) is
+// stored as a float anchor a = x[0], a float step s and 32 int16 codes. Element z decodes to
+//   fmaf(s, Q[z], a),  Q[z] integer, Q[0] = 0,
+// and the int16 code of element z is the second difference Q[z] - 2 Q[z-1] + Q[z-2] (Q[-1] = 0),
+// so decoding is two warp prefix sums. The encoder takes Q[z] = rint((x[z] - a) / s) with
+//   s = max( max(|x[1] - x[0]|, max_z |x[z] - 2 x[z-1] + x[z-2]|) / 32000, max_z |x[z] - a| / 2^22 ):
+// the rounding error |x - decoded| is s/2 (plus one rounding of the fma), i.e. 2^-16 of the
+// block's largest second difference instead of its largest value. Smooth fields (wavefields
+// sampled at many cells per wavelength) have second differences several times smaller than their
+// values, and the error the Laplacian of the recomputed field sees is smaller by that factor.
+// Bounds: |x - a| / s <= 2^22, so |Q| and its differences are exact in float and int; each
+// computed ratio (x - a) / s carries at most 0.5 of rounding error, so a code is at most
+// 32000 (1 + 2^-22) + 2 (rint) + 2 (ratio rounding) < 32767 in magnitude.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ float warp_max_f(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ int warp_scan_i(int v, int lane) {  // inclusive prefix sum over the warp
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += t;
+  }
+  return v;
+}
+
+struct D16Block {  // one encoded block: this lane's code, and the block's step and anchor
+  short code;
+  float step, anchor;
+};
+
+// All 32 lanes call this with their element x (0 past the end of the field). Sets the device status
+// word if the block holds a non-finite value (the block then decodes to NaN).
+__device__ __forceinline__ D16Block d16_encode(float x, int lane) {
+  const unsigned full = 0xffffffffu;
+  D16Block b;
+  if (__any_sync(full, !(fabsf(x) <= 3.0e38f))) {
+    if (lane == 0) atomicExch(&g_status, 4);
+    b.code = 0;
+    b.step = __int_as_float(0x7fc00000);
+    b.anchor = b.step;
+    return b;
+  }
+  const float a = __shfl_sync(full, x, 0);
+  const float xm1 = __shfl_up_sync(full, x, 1);
+  const float dx = lane >= 1 ? x - xm1 : 0.f;
+  const float dxm1 = __shfl_up_sync(full, dx, 1);
+  const float d2 = lane >= 2 ? dx - dxm1 : dx;
+  const float m = warp_max_f(fabsf(d2));
+  const float r = warp_max_f(fabsf(x - a));
+  const float s = fmaxf(fmaxf(m * (1.f / 32000.f), r * 0x1p-22f), 1.17549435e-38f);
+  const float inv = 1.f / s;
+  const int q = (int)rintf((x - a) * inv);
+  const int qm1 = __shfl_up_sync(full, q, 1);
+  const int qm2 = __shfl_up_sync(full, q, 2);
+  int d = lane >= 2 ? q - 2 * qm1 + qm2 : (lane == 1 ? q : 0);
+  d = max(-32767, min(32767, d));
+  b.code = (short)d;
+  b.step = s;
+  b.anchor = a;
+  return b;
+}
+
+__device__ __forceinline__ float d16_decode(short code, float s, float a, int lane) {
+  const int d1 = warp_scan_i((int)code, lane);
+  const int q = warp_scan_i(d1, lane);
+  return fmaf(s, (float)q, a);
+}
+
+// Encodes snapshot slots with one launch: grid.z = slot (0: l0 = p^{n0}; 1: l0 - lm1; 2, 3: the
+// PML face fields f0, f1), grid.y = shot, SNAP_WARP_BLOCKS blocks per warp with their loads issued
+// together. Slot k of shot f occupies blocks (k * n_shots + f) * nblk of vals / steps / anchors.
+template <typename T>
+__global__ void __launch_bounds__(256) snap_encode_d16(const T* __restrict__ lm1, const T* __restrict__ l0,
+                                                       const T* __restrict__ f0, const T* __restrict__ f1,
+                                                       long long field, int nblk, short* __restrict__ vals,
+                                                       float* __restrict__ steps, float* __restrict__ anchors) {
+  const int f = blockIdx.y, slot = blockIdx.z, n_shots = gridDim.y;
+  const long long b0 = ((long long)blockIdx.x * 8 + (threadIdx.x >> 5)) * SNAP_WARP_BLOCKS;
+  if (b0 >= nblk) return;
+  const int lane = threadIdx.x & 31;
+  const T* src = slot == 0 ? l0 : (slot == 1 ? l0 : (slot == 2 ? f0 : f1));
+  const T* sub = slot == 1 ? lm1 : nullptr;
+  float v[SNAP_WARP_BLOCKS];
+#pragma unroll
+  for (int u = 0; u < SNAP_WARP_BLOCKS; ++u) {
+    const long long e = (b0 + u) * SNAP_BLOCK + lane;
+    v[u] = 0.f;
+    if (b0 + u < nblk && e < field) {
+      const long long i = (long long)f * field + e;
+      v[u] = (float)(sub ? src[i] - sub[i] : src[i]);
+    }
+  }
+  const long long blk0 = ((long long)slot * n_shots + f) * nblk;
+#pragma unroll
+  for (int u = 0; u < SNAP_WARP_BLOCKS; ++u) {
+    const long long b = b0 + u;
+    if (b >= nblk) break;  // warp-uniform
+    const D16Block e = d16_encode(v[u], lane);
+    vals[(blk0 + b) * SNAP_BLOCK + lane] = e.code;
+    if (lane == 0) {
+      steps[blk0 + b] = e.step;
+      anchors[blk0 + b] = e.anchor;
+    }
+  }
+}
+
+// Decodes with one launch: grid.z = 0 decodes slots 0 and 1 of each block together (l0_out = p^{n0},
+// lm1_out = p^{n0} - difference, in T like the separate-slot codecs), grid.z = 1 (PML) the face
+// slots 2 and 3 into f0_out, f1_out.
+template <typename T>
+__global__ void __launch_bounds__(256) snap_decode_d16(const short* __restrict__ vals, const float* __restrict__ steps,
+                                                       const float* __restrict__ anchors, int nblk, long long field,
+                                                       T* __restrict__ lm1_out, T* __restrict__ l0_out,
+                                                       T* __restrict__ f0_out, T* __restrict__ f1_out) {
+  const int f = blockIdx.y, pair = blockIdx.z, n_shots = gridDim.y;
+  const long long b0 = ((long long)blockIdx.x * 8 + (threadIdx.x >> 5)) * SNAP_WARP_BLOCKS;
+  if (b0 >= nblk) return;
+  const int lane = threadIdx.x & 31;
+  const long long blkA = ((long long)(2 * pair) * n_shots + f) * nblk;
+  const long long blkB = ((long long)(2 * pair + 1) * n_shots + f) * nblk;
+  short qa[SNAP_WARP_BLOCKS], qb[SNAP_WARP_BLOCKS];
+  float sa[SNAP_WARP_BLOCKS], aa[SNAP_WARP_BLOCKS], sb[SNAP_WARP_BLOCKS], ab[SNAP_WARP_BLOCKS];
+#pragma unroll
+  for (int u = 0; u < SNAP_WARP_BLOCKS; ++u) {
+    const long long b = b0 + u;
+    qa[u] = qb[u] = 0;
+    sa[u] = sb[u] = 1.f;
+    aa[u] = ab[u] = 0.f;
+    if (b < nblk) {
+      qa[u] = vals[(blkA + b) * SNAP_BLOCK + lane];
+      qb[u] = vals[(blkB + b) * SNAP_BLOCK + lane];
+      sa[u] = steps[blkA + b];
+      aa[u] = anchors[blkA + b];
+      sb[u] = steps[blkB + b];
+      ab[u] = anchors[blkB + b];
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < SNAP_WARP_BLOCKS; ++u) {
+    const long long b = b0 + u;
+    if (b >= nblk) break;  // warp-uniform
+    if (lane == 0 && !(sa[u] > 0.f && sa[u] <= 3.0e38f && sb[u] > 0.f && sb[u] <= 3.0e38f &&
+                       fabsf(aa[u]) <= 3.0e38f && fabsf(ab[u]) <= 3.0e38f))
+      atomicExch(&g_status, 4);
+    const float va = d16_decode(qa[u], sa[u], aa[u], lane);
+    const float vb = d16_decode(qb[u], sb[u], ab[u], lane);
+    const long long e = b * SNAP_BLOCK + lane;
+    if (e >= field) continue;
+    const long long i = (long long)f * field + e;
+    if (pair == 0) {
+      const T p0 = (T)va;
+      l0_out[i] = p0;
+      lm1_out[i] = p0 - (T)vb;
+    } else {
+      f0_out[i] = (T)va;
+      f1_out[i] = (T)vb;
+    }
+  }
+}
+
 }  // namespace nw

@@ -132,10 +132,12 @@ int launch_sample(const nw_grid* g, const nw_acquisition* a, int n_t, const T* l
 struct SnapLayout {
   int nblk;             // blocks per field
   size_t vals_bytes;    // 16-bit payload of one snapshot
-  size_t scale_bytes;   // scales of one snapshot
+  size_t scale_bytes;   // scales of one snapshot (delta16: the steps, followed by as many anchors)
   size_t exact_bytes;   // exact copy of one snapshot
   size_t per_snap(int kind) const {
-    return kind == NW_SNAP_EXACT ? exact_bytes : ((vals_bytes + scale_bytes + 255) / 256) * 256;
+    if (kind == NW_SNAP_EXACT) return exact_bytes;
+    const size_t b = vals_bytes + scale_bytes * (kind == NW_SNAP_D16 ? 2 : 1);
+    return ((b + 255) / 256) * 256;
   }
 };
 SnapLayout snap_layout(const nw_grid* g, int n_shots) {
@@ -181,6 +183,30 @@ int snap_codec(const nw_grid* g, const SnapLayout& L, int n_shots, char* base, c
   return NW_OK;
 }
 
+// delta16 snapshots (nw::snap_encode_d16): both pressure slots in one launch, and the face slots
+// in the same launch with a PML; decoding writes p^{n0} and p^{n0-1} from one pass over the slots.
+template <typename T>
+int snap_codec_d16(const nw_grid* g, const SnapLayout& L, int n_shots, char* base, const T* lm1, T* lm1_out,
+                   const T* l0, T* l0_out, bool encode, cudaStream_t s, const T* const* faces = nullptr,
+                   T* const* faces_out = nullptr) {
+  short* vals = (short*)base;
+  float* steps = (float*)(base + L.vals_bytes);
+  float* anchors = (float*)(base + L.vals_bytes + L.scale_bytes);
+  const int slots = g->absorbing == NW_ABS_PML ? 4 : 2;
+  const unsigned gx = (unsigned)((L.nblk + 8 * nw::SNAP_WARP_BLOCKS - 1) / (8 * nw::SNAP_WARP_BLOCKS));
+  if (encode) {
+    nw::snap_encode_d16<T><<<dim3(gx, n_shots, slots), 256, 0, s>>>(
+        lm1, l0, slots == 4 ? faces[0] : nullptr, slots == 4 ? faces[1] : nullptr, g->field_elems, L.nblk, vals,
+        steps, anchors);
+  } else {
+    nw::snap_decode_d16<T><<<dim3(gx, n_shots, slots / 2), 256, 0, s>>>(
+        vals, steps, anchors, L.nblk, g->field_elems, lm1_out, l0_out, slots == 4 ? faces_out[0] : nullptr,
+        slots == 4 ? faces_out[1] : nullptr);
+  }
+  NW_LAUNCHED();
+  return NW_OK;
+}
+
 // The two PML face fields that step n reads (parity n % 2 of the double-buffered levels).
 template <typename T>
 void pml_faces(T* psi, long long level_elems, int n, T* out[2]) {
@@ -206,6 +232,7 @@ int snap_store(const nw_grid* g, const nw_storage* st, int n_shots, const T* lm1
     case NW_SNAP_F16: return snap_codec<T, nw::CODEC_F16>(g, L, n_shots, base, lm1, nullptr, l0, nullptr, true, s, fc);
     case NW_SNAP_BF16: return snap_codec<T, nw::CODEC_BF16>(g, L, n_shots, base, lm1, nullptr, l0, nullptr, true, s, fc);
     case NW_SNAP_I16: return snap_codec<T, nw::CODEC_I16>(g, L, n_shots, base, lm1, nullptr, l0, nullptr, true, s, fc);
+    case NW_SNAP_D16: return snap_codec_d16<T>(g, L, n_shots, base, lm1, nullptr, l0, nullptr, true, s, fc);
   }
   return fail(NW_ERR_ARG, "unknown snapshot kind");
 }
@@ -230,6 +257,8 @@ int snap_load(const nw_grid* g, const nw_storage* st, int n_shots, int j, T* lm1
       return snap_codec<T, nw::CODEC_BF16>(g, L, n_shots, base, nullptr, lm1, nullptr, l0, false, s, nullptr, faces);
     case NW_SNAP_I16:
       return snap_codec<T, nw::CODEC_I16>(g, L, n_shots, base, nullptr, lm1, nullptr, l0, false, s, nullptr, faces);
+    case NW_SNAP_D16:
+      return snap_codec_d16<T>(g, L, n_shots, base, nullptr, lm1, nullptr, l0, false, s, nullptr, faces);
   }
   return fail(NW_ERR_ARG, "unknown snapshot kind");
 }
@@ -461,7 +490,9 @@ int side_stream(SideStream** out) {
 }
 
 // side(t) on the calling thread's second stream beside main(s), both ordered after the work already
-// in s and joined back into it (with no side work, main(s) alone).
+// in s and joined back into it (with no side work, main(s) alone). Once the side stream is forked it
+// is joined back on every path, errors included, so a capture of s never ends with it still forked;
+// the first error is the one returned.
 template <typename FS, typename FM>
 int fork_join(cudaStream_t s, bool with_side, FS side, FM main) {
   if (!with_side) return main(s);
@@ -471,11 +502,11 @@ int fork_join(cudaStream_t s, bool with_side, FS side, FM main) {
   NW_CUDA(cudaEventRecord(ss->fork, s));
   NW_CUDA(cudaStreamWaitEvent(ss->s, ss->fork, 0));
   rc = side(ss->s);
+  const cudaError_t ej = cudaEventRecord(ss->join, ss->s);
+  if (rc == NW_OK && ej == cudaSuccess) rc = main(s);
+  const cudaError_t ew = ej == cudaSuccess ? cudaStreamWaitEvent(s, ss->join, 0) : ej;
   if (rc) return rc;
-  NW_CUDA(cudaEventRecord(ss->join, ss->s));
-  rc = main(s);
-  if (rc) return rc;
-  NW_CUDA(cudaStreamWaitEvent(s, ss->join, 0));
+  if (ew != cudaSuccess) return fail(NW_ERR_CUDA, std::string("side stream join: ") + cudaGetErrorString(ew));
   return NW_OK;
 }
 
@@ -547,14 +578,6 @@ int forward_step(const nw_grid* g, const nw::KGrid<T>& kg, const nw_medium* m, c
     int rc = pml_tiled_box<T>(g, m, tu.fwd, st);
     if (rc) return rc;
     if (st.kx1 == st.kx0) return launch_pml<T, false>(g, kg, st, a->n_shots, s);  // no interior box
-    SideStream* side = nullptr;
-    rc = side_stream(&side);
-    if (rc) return rc;
-    NW_CUDA(cudaEventRecord(side->fork, s));
-    NW_CUDA(cudaStreamWaitEvent(side->s, side->fork, 0));
-    rc = launch_pml<T, false>(g, kg, st, a->n_shots, side->s);  // the layer, beside the box
-    if (rc) return rc;
-    NW_CUDA(cudaEventRecord(side->join, side->s));
     nw::Tiled2<T> tb = {};  // the interior box: the plain step (A = B = 1 and no PML term there)
     tb.prev = st.prev;
     tb.cur = st.cur;
@@ -568,10 +591,10 @@ int forward_step(const nw_grid* g, const nw::KGrid<T>& kg, const nw_medium* m, c
     tb.wavelet = st.wavelet;
     tb.n = n;
     const dim3 grid = box_tiles<T>(st, tu.fwd, a->n_shots, tb);
-    rc = NW_DISPATCH2(launch_fwd2_v, T, tu.fwd, kg, tb, grid, s);
-    if (rc) return rc;
-    NW_CUDA(cudaStreamWaitEvent(s, side->join, 0));  // the step ends when both halves have
-    return NW_OK;
+    // the layer on the side stream beside the box; the step ends when both halves have
+    return fork_join(
+        s, true, [&](cudaStream_t t) { return launch_pml<T, false>(g, kg, st, a->n_shots, t); },
+        [&](cudaStream_t t) { return NW_DISPATCH2(launch_fwd2_v, T, tu.fwd, kg, tb, grid, t); });
   }
   if (g->ndim == 2) {
     nw::Tiled2<T> st = {};
@@ -729,14 +752,6 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
       rc = launch_pml<T, true>(g, kg, ps, S, s);
       if (rc) return rc;
     } else {  // the layer (per-shot accumulators) on the side stream, beside the interior box
-      SideStream* side = nullptr;
-      rc = side_stream(&side);
-      if (rc) return rc;
-      NW_CUDA(cudaEventRecord(side->fork, s));
-      NW_CUDA(cudaStreamWaitEvent(side->s, side->fork, 0));
-      rc = launch_pml<T, true>(g, kg, ps, S, side->s);
-      if (rc) return rc;
-      NW_CUDA(cudaEventRecord(side->join, side->s));
       // the interior box: the plain adjoint step, accumulators per shot group
       nw::Tiled2<T> tb = {};  // (disjoint cells, so the reduction over all accumulators stays exact)
       tb.cur = ps.cur;
@@ -749,9 +764,10 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
       tb.lap = lap;
       tb.gacc = gacc;
       const dim3 grid = box_tiles<T>(ps, tu.adj, S, tb);
-      rc = NW_DISPATCH2(launch_adj2_v, T, tu.adj, kg, tb, grid, s);
+      rc = fork_join(
+          s, true, [&](cudaStream_t t) { return launch_pml<T, true>(g, kg, ps, S, t); },
+          [&](cudaStream_t t) { return NW_DISPATCH2(launch_adj2_v, T, tu.adj, kg, tb, grid, t); });
       if (rc) return rc;
-      NW_CUDA(cudaStreamWaitEvent(s, side->join, 0));
     }
     return inject3(n);
   };

@@ -131,21 +131,26 @@ class PaddedGrid:
         return x[tuple(idx)]
 
     def pad(self, x: torch.Tensor, mode: str = "replicate") -> torch.Tensor:
-        """Host-side padding (replicate for material maps, zeros otherwise); used for checks."""
+        """Host-side padding (replicate for material maps, zeros otherwise); used for checks.
+
+        Padded cell ``i`` of an axis with layer width ``a`` and ``n`` physical cells holds physical
+        cell ``i - a`` (zeros), or the nearest physical cell ``clamp(i - a, 0, n - 1)`` (replicate)."""
         if not any(self.n_abs):
             return x
-        if mode == "zeros":
-            pads: list[int] = []
-            for a in reversed(self.n_abs):
-                pads += [a, a]
-            return torch.nn.functional.pad(x, pads)
         for ax, a in enumerate(self.n_abs):
             if a == 0:
                 continue
             dim = x.ndim - self.d + ax
             n = x.shape[dim]
-            size = [a if i == dim else -1 for i in range(x.ndim)]
-            x = torch.cat([x.narrow(dim, 0, 1).expand(*size), x, x.narrow(dim, n - 1, 1).expand(*size)], dim)
+            src = torch.arange(-a, n + a, device=x.device)
+            if mode == "zeros":
+                shape = list(x.shape)
+                shape[dim] = n + 2 * a
+                out = x.new_zeros(shape)
+                out.narrow(dim, a, n).copy_(x)
+                x = out
+            else:
+                x = x.index_select(dim, src.clamp(0, n - 1))
         return x
 
     def point_stencils(self, points: torch.Tensor) -> tuple[torch.Tensor, torch.Tensor]:
@@ -188,14 +193,18 @@ class PaddedGrid:
         return out
 
     def nearest_index(self, points: torch.Tensor) -> torch.Tensor:
-        """Flat padded-grid index of the cell containing each point."""
+        """Flat padded-grid index of the cell containing each point: per axis the cell whose
+        faces ``lo + [i, i + 1) h`` enclose the coordinate, clamped to the padded grid, combined
+        with the row-major strides of the padded shape."""
         pts = torch.as_tensor(points, dtype=torch.float64)
-        flat = torch.zeros(pts.shape[0], dtype=torch.long)
-        for ax in range(self.d):
-            h, lo, m = self.spacing[ax], self.lo_pad[ax], self.padded_shape[ax]
-            i = torch.floor((pts[:, ax] - lo) / h).long().clamp(0, m - 1)
-            flat = flat * m + i
-        return flat
+        lo = torch.tensor(self.lo_pad[: self.d], dtype=torch.float64)
+        h = torch.tensor(self.spacing[: self.d], dtype=torch.float64)
+        hi = torch.tensor(self.padded_shape[: self.d], dtype=torch.long) - 1
+        cell = torch.minimum(torch.floor((pts - lo) / h).long().clamp(min=0), hi)
+        strides = [1] * self.d
+        for ax in range(self.d - 2, -1, -1):
+            strides[ax] = strides[ax + 1] * self.padded_shape[ax + 1]
+        return (cell * torch.tensor(strides, dtype=torch.long)).sum(1)
 
 
 def as_points(x, d: int, name: str) -> torch.Tensor:

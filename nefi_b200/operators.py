@@ -48,7 +48,7 @@ from .plan import DevicePlan, ghost_view, plan_storage, to_ghost
 
 log = logging.getLogger("nefi_b200")
 
-SNAPSHOTS = ("exact", "fixed16", "fp16", "bf16")
+SNAPSHOTS = ("exact", "delta16", "fixed16", "fp16", "bf16")
 
 
 class _LeapfrogB200(Operator):

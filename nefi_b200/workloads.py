@@ -143,6 +143,16 @@ def fwi_2048(seed: int = 0, n_shots: int = 32, n_steps: int = 8000) -> FWIWorklo
     return FWIWorkload("fwi_2048", n, h, c, src, rec, 12.0, n_steps)
 
 
+def fwi_salt(n: int = 192, n_shots: int = 32, n_steps: int = 1000, seed: int = 3) -> FWIWorkload:
+    """``fwi_2048``'s model family (layers + salt body, 12 Hz, receivers every other cell) on a
+    smaller grid: the size at which a float64 CPU run checks the checkpointed 16-bit gradient."""
+    h = 10.0
+    rng = np.random.default_rng(seed)
+    c = salt_body(layered_model(n, h, rng), h, rng)
+    src, rec = _surface(n, h, n_shots, n // 2)
+    return FWIWorkload(f"fwi_salt_{n}", n, h, c, src, rec, 12.0, n_steps)
+
+
 def fwi_batch_problems(seed: int = 0, n_problems: int = 64):
     """The uneven batch: grid sizes from {256, 384, 512, 768}^2, 4-16 shots, 1500-6000 steps."""
     rng = np.random.default_rng(seed)
@@ -223,4 +233,4 @@ def cell_updates(w: FWIWorkload, n_shots: int | None = None) -> int:
 
 
 __all__ = ["FWIWorkload", "PATWorkload", "WORKLOADS", "cell_updates", "fwi_2048", "fwi_512",
-           "fwi_batch_problems", "fwi_plain_128", "layered_model", "pat_volume", "salt_body"]
+           "fwi_batch_problems", "fwi_salt", "fwi_plain_128", "layered_model", "pat_volume", "salt_body"]

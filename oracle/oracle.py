@@ -64,6 +64,13 @@ def lib():
             getattr(_lib, "oracle_adjoint" + sfx).argtypes = [
                 C.POINTER(Geom), dp, dp, dp, C.c_int, C.c_int, C.c_int, lp, dp, dp, C.c_int, C.c_int,
                 C.c_int, dp, dp, dp, dp]
+            real = C.c_double if sfx == "_f64" else C.c_float
+            getattr(_lib, "oracle_pml_forward" + sfx).argtypes = [
+                C.POINTER(Geom), dp, dp, dp, dp, dp, dp, dp, dp, real, real, C.c_int, lp, dp, C.c_int, dp,
+                C.c_int, C.c_int, lp, dp, dp, dp, C.c_int, C.c_int, C.c_int, dp, dp]
+            getattr(_lib, "oracle_pml_adjoint" + sfx).argtypes = [
+                C.POINTER(Geom), dp, dp, dp, dp, dp, dp, dp, dp, real, real, C.c_int, C.c_int, C.c_int, lp,
+                dp, dp, C.c_int, C.c_int, C.c_int, dp, dp, dp, dp]
     return _lib
 
 
@@ -256,17 +263,35 @@ class OracleWave:
         return out
 
     # -- runs --------------------------------------------------------------------------------
+    # history bytes one call may hold; runs with more shots go through in chunks of shots (the shots
+    # are independent, so the results are those of one call)
+    HISTORY_BYTES = 2 << 30
+
     def _run(self, C2, n_shots, init_prev, init_cur, gtr, dtype, want_initial=False):
+        per_shot = (self.N + 2) * math.prod(self.P) * np.dtype(dtype).itemsize
+        chunk = max(1, int(self.HISTORY_BYTES // max(per_shot, 1)))
+        if gtr is not None and n_shots > chunk:
+            parts = []
+            for s0 in range(0, n_shots, chunk):
+                s1 = min(n_shots, s0 + chunk)
+                sel = lambda a: None if a is None else np.asarray(a).reshape(n_shots, -1)[s0:s1]  # noqa: E731
+                g = np.asarray(gtr).reshape(n_shots, -1, self.n_t)[s0:s1]
+                parts.append(self._run_shots(C2, s1 - s0, sel(init_prev), sel(init_cur), g, dtype, want_initial, s0))
+            cat = lambda i: None if parts[0][i] is None else np.concatenate([p[i] for p in parts], 0)  # noqa: E731
+            return cat(0), cat(1), cat(2), cat(3)
+        return self._run_shots(C2, n_shots, init_prev, init_cur, gtr, dtype, want_initial, 0)
+
+    def _run_shots(self, C2, n_shots, init_prev, init_cur, gtr, dtype, want_initial, shot0):
         if self.pml is not None:
-            return self._run_pml(C2, n_shots, init_prev, init_cur, gtr, dtype)
+            return self._run_pml(C2, n_shots, init_prev, init_cur, gtr, dtype, shot0)
         L = lib()
         sfx = "_f64" if dtype == np.float64 else "_f32"
         cast = lambda a: None if a is None else np.ascontiguousarray(a, dtype=dtype)  # noqa: E731
         C2, A, B = cast(C2), cast(self.A), cast(self.B)
         rec_w = cast(self.rec_w)
         src = self.sources is not None
-        src_idx = np.ascontiguousarray(self.src_idx) if src else None
-        src_w = cast(self.src_w) if src else None
+        src_idx = np.ascontiguousarray(self.src_idx[shot0:shot0 + n_shots]) if src else None
+        src_w = cast(self.src_w[shot0:shot0 + n_shots]) if src else None
         wav = cast(self.wavelet) if src else None
         cells = math.prod(self.P)
         traces = np.zeros((n_shots, self.rec_idx.shape[0], self.n_t), dtype=dtype)
@@ -288,7 +313,42 @@ class OracleWave:
             _p(g), _p(gC), _p(lam0), _p(mu1))
         return traces, gC, lam0, mu1
 
-    def _run_pml(self, C2, S, init_prev, init_cur, gtr, dtype):
+    def _run_pml(self, C2, S, init_prev, init_cur, gtr, dtype, shot0=0):
+        """2-D PML run and, given cotangents, its exact adjoint, in C (``oracle_pml_forward`` /
+        ``oracle_pml_adjoint``: the loops of ``_run_pml_numpy`` below, same operation order)."""
+        L = lib()
+        sfx = "_f64" if dtype == np.float64 else "_f32"
+        cast = lambda a: None if a is None else np.ascontiguousarray(a, dtype=dtype)  # noqa: E731
+        C2, A, B, ZZ = cast(C2), cast(self.A), cast(self.B), cast(self.pml["zz"])
+        al = [cast(x) for x in self.pml["alpha"]]
+        be = [cast(x) for x in self.pml["beta"]]
+        hx, hz = (0.5 / h for h in self.h)
+        rec_w = cast(self.rec_w)
+        src = self.sources is not None
+        src_idx = np.ascontiguousarray(self.src_idx[shot0:shot0 + S]) if src else None
+        src_w = cast(self.src_w[shot0:shot0 + S]) if src else None
+        wav = cast(self.wavelet) if src else None
+        cells = math.prod(self.P)
+        n_rec, rec_pts = self.rec_idx.shape
+        traces = np.zeros((S, n_rec, self.n_t), dtype=dtype)
+        Lh = np.zeros((self.N, S, cells), dtype=dtype) if gtr is not None else None
+        getattr(L, "oracle_pml_forward" + sfx)(
+            C.byref(self.geom), _p(C2), _p(A), _p(B), _p(ZZ), _p(al[0]), _p(be[0]), _p(al[1]), _p(be[1]), hx, hz,
+            S, _p(src_idx), _p(src_w), src_idx.shape[1] if src else 0, _p(wav), n_rec, rec_pts, _p(self.rec_idx),
+            _p(rec_w), _p(cast(init_prev)), _p(cast(init_cur)), self.N, self.m, self.n_t, _p(traces), _p(Lh))
+        if gtr is None:
+            return traces, None, None, None
+        g = cast(gtr)
+        gC = np.zeros((S, cells), dtype=dtype)
+        lam0 = np.zeros((S, cells), dtype=dtype)
+        mu1 = np.zeros((S, cells), dtype=dtype)
+        getattr(L, "oracle_pml_adjoint" + sfx)(
+            C.byref(self.geom), _p(C2), _p(A), _p(B), _p(ZZ), _p(al[0]), _p(be[0]), _p(al[1]), _p(be[1]), hx, hz,
+            S, n_rec, rec_pts, _p(self.rec_idx), _p(rec_w), _p(Lh), self.N, self.m, self.n_t, _p(g), _p(gC),
+            _p(lam0), _p(mu1))
+        return traces, gC, lam0, mu1
+
+    def _run_pml_numpy(self, C2, S, init_prev, init_cur, gtr, dtype, shot0=0):
         """2-D PML run in numpy (all shots at once) and, given cotangents, its exact adjoint.
 
         Forward, step k (nefi/physics/wave.py:529-552), with face differences D+ (zero outside
@@ -347,7 +407,7 @@ class OracleWave:
             if src:
                 flat = rhs.reshape(S, -1)
                 for s in range(S):
-                    np.add.at(flat[s], self.src_idx[s], cast(self.src_w[s]) * dtype(self.wavelet[n]))
+                    np.add.at(flat[s], self.src_idx[shot0 + s], cast(self.src_w[shot0 + s]) * dtype(self.wavelet[n]))
             pp, pc, psi = pc, A * rhs, new
         if gtr is None:
             return traces, None, None, None

@@ -1,8 +1,10 @@
 """Generate golden vectors for the wave propagator by running the reference NEFI package itself.
 
-Run where the reference checkout is available (it is not needed anywhere else):
+Run where the reference checkout is available (it is not needed anywhere else), naming it by
+argument or by the NEFI_REFERENCE environment variable:
 
-    python tests/golden/make_golden.py [/path/to/reference] [case-name-prefix ...]
+    python tests/golden/make_golden.py /path/to/reference [case-name-prefix ...]
+    NEFI_REFERENCE=/path/to/reference python tests/golden/make_golden.py - [case-name-prefix ...]
 
 With name prefixes only the matching cases are written (every case is seeded on its own, so a
 subset reproduces the same fixtures as a full run).
@@ -19,6 +21,7 @@ from __future__ import annotations
 
 import json
 import math
+import os
 import sys
 from pathlib import Path
 
@@ -26,7 +29,11 @@ import numpy as np
 import torch
 
 HERE = Path(__file__).resolve().parent
-REF = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+_arg = sys.argv[1] if len(sys.argv) > 1 else "-"
+if _arg == "-" and not os.environ.get("NEFI_REFERENCE"):
+    sys.exit("usage: make_golden.py /path/to/reference [case-name-prefix ...] "
+             "(or '-' with NEFI_REFERENCE set to the reference checkout)")
+REF = Path(os.environ["NEFI_REFERENCE"] if _arg == "-" else _arg)
 ONLY = tuple(sys.argv[2:])
 sys.path.insert(0, str(REF))
 

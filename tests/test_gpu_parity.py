@@ -113,11 +113,13 @@ def test_checkpointed_gradient_is_identical_to_full_history(name, dtype, cuda_de
         assert np.array_equal(got[0], ref[0]) and np.array_equal(got[1], ref[1])
 
 
-@pytest.mark.parametrize("snapshot,tol", [("fixed16", 3e-4), ("fp16", 3e-3), ("bf16", 2.5e-2)])
+@pytest.mark.parametrize("snapshot,tol", [("delta16", 1e-4), ("fixed16", 3e-4), ("fp16", 3e-3), ("bf16", 2.5e-2)])
 def test_reduced_precision_snapshots_error_is_bounded(snapshot, tol, cuda_device):
     """16-bit snapshots perturb only the recomputed forward field, so the traces stay exact and the
-    gradient error is set by the rounding noise of the codec (measured on this case with the float64
-    oracle: fixed16 1.8e-4, fp16 2.0e-3, bf16 1.7e-2 at 40-step segments)."""
+    gradient error is set by the rounding noise of the codec. The seeded white-noise cotangent of
+    this fixture excites the grid's shortest wavelengths, where the Laplacian amplifies that noise
+    most: delta16 meets the 1e-4 gradient budget (4.4e-5 in a CPU model of the codec), fixed16, fp16
+    and bf16 do not (1.8e-4, 2.0e-3, 1.7e-2; 40-step segments, float64 oracle)."""
     case = load_golden("cfg1_128_o4_sponge")
     tr, gc = run_fwi(case, torch.float32, cuda_device, grad_mode="checkpoint", checkpoint_every=40,
                      snapshot=snapshot)
@@ -125,7 +127,38 @@ def test_reduced_precision_snapshots_error_is_bounded(snapshot, tol, cuda_device
     assert rel_l2(gc, case["grad_c_f64"]) < tol
 
 
-@pytest.mark.parametrize("snapshot", ["fixed16", "bf16"])
+@pytest.mark.parametrize("absorbing,n", [("sponge", 192), ("pml", 160)])
+@pytest.mark.parametrize("snapshot", ["delta16", "fixed16"])
+def test_checkpointed_16_bit_gradient_of_a_salt_model_meets_the_budget(absorbing, n, snapshot, cuda_device):
+    """The north-star method on the large configuration's model family (layers + a 4500 m/s salt body,
+    12 Hz), reduced to a grid a float64 CPU run finishes in seconds: 32 shots, 1000 steps, the default
+    ceil(sqrt(N)) = 32-step segments, 16-bit snapshots. The cotangent is the residual of
+    1/2 ||d(c0) - d(c_true)||^2 at a smoothed model c0, as an FWI iteration takes it. The float32
+    gradient must be within 1e-4 (relative L2) of the float64 oracle's, with the sponge and the PML."""
+    import oracle
+    from scipy.ndimage import gaussian_filter
+    from nefi_b200.workloads import fwi_salt
+
+    w = fwi_salt(n=n, n_shots=32, n_steps=1000)
+    kw = {**w.operator_kwargs(), "absorbing": absorbing}
+    orc = oracle.OracleWave((n, n), ((0.0, n * w.h), (0.0, n * w.h)), w.receivers, sources=w.sources, **kw)
+    oracle.set_threads(max(1, __import__("os").cpu_count() or 1))
+    c0 = gaussian_filter(w.c, 6.0)
+    obs, _ = orc.fwi(w.c)
+    pred, _ = orc.fwi(c0)
+    resid = pred - obs
+    _, g64 = orc.fwi(c0, resid)
+    op = WaveOperatorB200(w.domain, w.sources, w.receivers, grad_mode="checkpoint", snapshot=snapshot, **kw)
+    c = torch.tensor(c0, dtype=torch.float32, device=cuda_device, requires_grad=True)
+    tr = op({"c": c})
+    (gc,) = torch.autograd.grad((tr * torch.tensor(resid, dtype=torch.float32, device=cuda_device)).sum(), c)
+    assert rel_l2(tr.detach().cpu().numpy(), pred) < 1e-5
+    err = rel_l2(gc.cpu().numpy(), g64)
+    print(f"{absorbing} {snapshot}: float32 checkpointed gradient vs float64 oracle {err:.2e}")
+    assert err < 1e-4
+
+
+@pytest.mark.parametrize("snapshot", ["delta16", "fixed16", "bf16"])
 def test_pml_checkpoints_with_16_bit_snapshots(snapshot, cuda_device):
     """The PML's face fields travel through the 16-bit codec with the pressure; the traces stay exact
     and the gradient stays close to the reference's float64 one."""
@@ -133,7 +166,7 @@ def test_pml_checkpoints_with_16_bit_snapshots(snapshot, cuda_device):
     tr, gc = run_fwi(case, torch.float32, cuda_device, grad_mode="checkpoint", checkpoint_every=6,
                      snapshot=snapshot)
     assert rel_l2(tr, case["traces_f64"]) < 1e-5
-    assert rel_l2(gc, case["grad_c_f64"]) < (1e-3 if snapshot == "fixed16" else 3e-2)
+    assert rel_l2(gc, case["grad_c_f64"]) < {"delta16": 1e-3, "fixed16": 1e-3, "bf16": 3e-2}[snapshot]
 
 
 def test_runs_are_bitwise_deterministic(cuda_device):
@@ -250,11 +283,12 @@ def _shift(p, o, dim):
     return out
 
 
-def test_corrupted_snapshot_raises(cuda_device):
+@pytest.mark.parametrize("snapshot", ["fp16", "delta16"])
+def test_corrupted_snapshot_raises(snapshot, cuda_device):
     """Host-side fault injection: a NaN written into the snapshot pool between the forward and the
     backward sweep must surface as SolverError, not as a silent gradient."""
     case = load_golden("fwi_o4_sponge")
-    op = make_op(case, grad_mode="checkpoint", checkpoint_every=10, snapshot="fp16")
+    op = make_op(case, grad_mode="checkpoint", checkpoint_every=10, snapshot=snapshot)
     c = torch.tensor(case["c"], dtype=torch.float32, device=cuda_device, requires_grad=True)
     tr = op({"c": c})
     ctx_run = tr.grad_fn.run  # the _Run object saved on the autograd context
@@ -467,5 +501,9 @@ def test_random_geometries_match_the_oracle(seed, dtype, tt, tg, cuda_device):
         # error of the same arithmetic in float32 on the host, the reference's own float32 path
         tr32, gc32 = orc.fwi(c, gt, dtype=np.float32)
         tt, tg = max(tt, 2.0 * rel_l2(tr32, tr_o)), max(tg, 2.0 * rel_l2(gc32, gc_o))
-    assert rel_l2(tr.detach().cpu().numpy(), tr_o) < tt, (absorbing, kw)
-    assert rel_l2(gc.cpu().numpy(), gc_o) < tg, (absorbing, kw)
+        # a fixed ceiling, so that a drifting host error cannot hide a device regression
+        assert tt <= 1e-4 and tg <= 1e-3, (tt, tg)
+    e_tr, e_gc = rel_l2(tr.detach().cpu().numpy(), tr_o), rel_l2(gc.cpu().numpy(), gc_o)
+    print(f"seed {seed} {absorbing} {dtype}: traces {e_tr:.2e} (bound {tt:.1e}), gradient {e_gc:.2e} (bound {tg:.1e})")
+    assert e_tr < tt, (absorbing, kw)
+    assert e_gc < tg, (absorbing, kw)

@@ -466,3 +466,27 @@ def test_kernel_semantics_match_the_oracle_on_random_3d_geometries(seed):
     assert np.linalg.norm(tr_o) > 0
     assert rel_l2(tr, tr_o) < 1e-12, (absorbing, kw)
     assert rel_l2(model.fold_grad(c, op.dt**2, gC), gc_o) < 1e-11, (absorbing, kw)
+
+
+@pytest.mark.parametrize("shape,extent", [((20, 31), ((0.0, 2.0), (-1.0, 2.1))),
+                                          ((9, 12, 7), ((0.0, 0.9), (0.0, 1.2), (0.5, 1.2)))])
+def test_padding_and_nearest_cells_match_the_oracle(shape, extent):
+    """Replicate / zero padding and the cell containing a point (the receivers of time reversal)
+    against the oracle's independent numpy versions, on points anywhere in the padded grid."""
+    import oracle
+
+    d = len(shape)
+    rng = np.random.default_rng(2)
+    op = WaveOperatorB200(Domain(shape, extent), [[e[0] + 0.3 * (e[1] - e[0]) for e in extent]],
+                          [[e[0] + 0.6 * (e[1] - e[0]) for e in extent]], n_t=5, dt_obs=0.01, f0=5.0,
+                          c_max=2.0, absorbing="sponge", absorb_width=0.25)
+    orc = oracle.OracleWave(shape, extent, [[e[0] + 0.6 * (e[1] - e[0]) for e in extent]], n_t=5,
+                            dt_obs=0.01, c_max=2.0, absorbing="sponge", absorb_width=0.25)
+    x = rng.standard_normal((2, *shape))
+    for mode in ("replicate", "zeros"):
+        got = op.grid.pad(torch.tensor(x), mode).numpy()
+        assert np.array_equal(got, orc.pad(x, mode))
+    lo = [op.grid.lo_pad[ax] for ax in range(d)]
+    span = [op.grid.padded_shape[ax] * op.grid.spacing[ax] for ax in range(d)]
+    pts = np.stack([rng.uniform(lo[ax] - 0.1, lo[ax] + span[ax] + 0.1, 500) for ax in range(d)], 1)
+    assert np.array_equal(op.grid.nearest_index(torch.tensor(pts)).numpy(), orc.nearest_cells(pts))

@@ -115,3 +115,34 @@ def test_misfit_oracle_matches_reference(name):
         assert rel_l2(y, case["sensor_f64"]) < 1e-13
         assert abs(sl - float(case["sensor_loss_f64"])) <= 1e-12 * abs(float(case["sensor_loss_f64"]))
         assert rel_l2(sg, case["sensor_grad_f64"]) < 1e-12
+
+
+@pytest.mark.parametrize("dtype,tol", [(np.float64, 1e-13), (np.float32, 1e-6)])
+def test_oracle_pml_loops_match_the_array_restatement(dtype, tol):
+    """The C loops of the PML run and its adjoint against the numpy array description of the same
+    step, on a small seeded anisotropic grid with two shots."""
+    import oracle
+
+    rng = np.random.default_rng(5)
+    shape, extent = (22, 30), ((0.0, 1.1), (0.0, 1.2))
+    c = 2.0 + 0.3 * rng.random(shape)
+    src, rec = [[0.3, 0.2], [0.7, 0.9]], [[0.9, y] for y in (0.1, 0.4, 0.8, 1.1)]
+    orc = oracle.OracleWave(shape, extent, rec, sources=src, n_t=40, dt_obs=0.01, f0=5.0, c_max=2.4,
+                            absorbing="pml", absorb_width=0.2)
+    C2 = orc.c2dt2(c, dtype).reshape(-1)
+    g = rng.standard_normal((2, len(rec), 40))
+    a = orc._run_pml(C2, 2, None, None, g, dtype)
+    b = orc._run_pml_numpy(C2, 2, None, None, g, dtype)
+    for x, y in zip(a, b):
+        assert rel_l2(x, y) < tol
+
+
+def test_oracle_runs_in_shot_chunks_like_one_call():
+    """Shot chunks (a history budget below one run's) give the results of one call."""
+    case = load_golden("fwi_o4_pml")
+    g = cotangent(full_trace_shape(case), case["seed"])
+    one = oracle_for(case).fwi(case["c"], g)
+    orc = oracle_for(case)
+    orc.HISTORY_BYTES = 1
+    chunked = orc.fwi(case["c"], g)
+    assert np.array_equal(one[0], chunked[0]) and np.array_equal(one[1], chunked[1])

@@ -30,7 +30,28 @@ pytestmark = pytest.mark.gpu
 TOL = {torch.float64: 1e-10, torch.float32: 1e-4}
 
 
-def _setup(case, dtype, dev):
+def _fwi3d_case() -> dict:
+    """A small 3-D FWI geometry (sponge, order 2): the 3-D adjoint keeps one accumulator per shot."""
+    return {"shape": (14, 12, 10), "extent": ((0.0, 1.4), (0.0, 1.2), (0.0, 1.0)),
+            "sources": np.array([[0.5, 0.4, 0.25], [0.9, 0.7, 0.35]]),
+            "receivers": np.array([[0.3 + 0.2 * i, 0.6, 0.15] for i in range(4)]),
+            "c": 2.0 + 0.2 * np.random.default_rng(4).random((14, 12, 10)), "seed": 11,
+            "kw": dict(n_t=30, dt_obs=0.012, f0=5.0, c_max=2.4, order=2, absorbing="sponge",
+                       absorb_width=0.2)}
+
+
+# (case, storage mode, snapshot kind): each lays out the shared array differently -- the sponge's three
+# adjoint levels and one accumulator per shot group, the PML's seven levels (face cotangents) and one
+# accumulator per shot, the 3-D adjoint's accumulator per shot, and checkpointed runs that decode
+# snapshots and recompute each segment into the caller's segment buffer
+CASES = [("fwi_o4_sponge", ("history", None), "exact"),
+         ("fwi_o4_pml", ("history", None), "exact"),
+         ("fwi3d", ("history", None), "exact"),
+         ("fwi_o4_sponge", ("checkpoint", 7), "delta16"),
+         ("fwi_o4_pml", ("checkpoint", 6), "exact")]
+
+
+def _setup(case, dtype, dev, mode=("history", None), snapshot="exact"):
     dom = Domain(tuple(case["shape"]), tuple(tuple(e) for e in case["extent"]))
     op = WaveOperatorB200(dom, case["sources"], case["receivers"], grad_mode="autograd", **case["kw"])
     plan = op._plan(dev, dtype)
@@ -43,7 +64,7 @@ def _setup(case, dtype, dev):
     medium = plan.medium(c2dt2)
     S = op.n_sources
     acq = plan.acquisition(S)
-    run = _Run(plan, S, op.n_steps, ("history", None), "exact")
+    run = _Run(plan, S, op.n_steps, mode, snapshot)
     traces = torch.empty(S, plan.n_rec, op.n_t, dtype=dtype, device=dev)
     _forward_sweep(plan, medium, acq, run, 0, op.n_steps, traces, stream)
     g = torch.tensor(cotangent(traces.shape, case["seed"]), dtype=dtype, device=dev)
@@ -51,10 +72,11 @@ def _setup(case, dtype, dev):
     return op, plan, lib, stream, c, medium, acq, run, g, c2dt2
 
 
+@pytest.mark.parametrize("name,mode,snapshot", CASES)
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
-def test_noalloc_gradient_matches_allocating_path_twice(dtype, cuda_device):
-    case = load_golden("fwi_o4_sponge")
-    op, plan, lib, stream, c, medium, acq, run, g, _c2dt2 = _setup(case, dtype, cuda_device)
+def test_noalloc_gradient_matches_allocating_path_twice(name, mode, snapshot, dtype, cuda_device):
+    case = _fwi3d_case() if name == "fwi3d" else load_golden(name)
+    op, plan, lib, stream, c, medium, acq, run, g, _c2dt2 = _setup(case, dtype, cuda_device, mode, snapshot)
     # the allocating path
     gC, _, _ = _adjoint_sweep(plan, medium, acq, run, g, False, stream)
     ref = torch.empty(c.shape, dtype=torch.float64, device=cuda_device)
@@ -70,9 +92,10 @@ def test_noalloc_gradient_matches_allocating_path_twice(dtype, cuda_device):
         got = out.cpu().numpy()
         assert np.isfinite(got).all()
         assert rel_l2(got, ref_h) < TOL[dtype]
-        # and it is the reference's gradient, to the parity tolerance of this dtype
-        golden = case["grad_c_f64"] if dtype == torch.float64 else case["grad_c_f32"]
-        assert rel_l2(got, golden) < TOL[dtype]
+        if "grad_c_f64" in case and snapshot == "exact":
+            # and it is the reference's gradient, to the parity tolerance of this dtype
+            golden = case["grad_c_f64"] if dtype == torch.float64 else case["grad_c_f32"]
+            assert rel_l2(got, golden) < TOL[dtype]
 
 
 def test_noalloc_refuses_requests_above_its_array(cuda_device):
