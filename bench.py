@@ -691,7 +691,7 @@ def main() -> None:
     ap.add_argument("--problems", type=int, default=64, help="fwi_batch: problems in the batch")
     ap.add_argument("--grad-mode", default="autograd", choices=("autograd", "checkpoint"),
                     help="autograd keeps the full history when it fits, else checkpoints")
-    ap.add_argument("--snapshot", default="exact", choices=("exact", "fixed16", "fp16", "bf16"))
+    ap.add_argument("--snapshot", default="exact", choices=("exact", "delta16", "fixed16", "fp16", "bf16"))
     ap.add_argument("--checkpoint-every", type=int, default=None)
     ap.add_argument("--absorbing", default=None, choices=("sponge", "pml", "cerjan", "none"),
                     help="override the workload's absorbing layer (fwi workloads)")

@@ -3,6 +3,7 @@
 from __future__ import annotations
 
 import json
+import os
 import sys
 from pathlib import Path
 
@@ -15,6 +16,14 @@ GOLDEN = Path(__file__).resolve().parent / "golden"
 for p in (str(ROOT), str(ROOT / "oracle")):
     if p not in sys.path:
         sys.path.insert(0, p)
+# The NEFI package, when an installed copy is at hand (NEFI_REFERENCE, or the offline install under
+# baseline/_ref): the B200 operators then subclass its Operator and raise its error types, and
+# tests/test_gpu_dropin.py runs NEFI's own instances on them. Without it the package's mirror of
+# the same API is used and those tests skip.
+for p in (os.environ.get("NEFI_REFERENCE"), str(ROOT / "baseline" / "_ref")):
+    if p and (Path(p) / "nefi" / "__init__.py").exists() and p not in sys.path:
+        sys.path.append(p)
+        break
 
 
 def pytest_configure(config):
