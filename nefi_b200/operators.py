@@ -385,9 +385,25 @@ class WaveOperatorB200(_LeapfrogB200):
         if tuple(observed.shape) != (self.n_sources, self.n_receivers, self.n_t):
             raise ShapeError(f"observed has shape {tuple(observed.shape)}, expected "
                              f"{(self.n_sources, self.n_receivers, self.n_t)}")
+        return self._gradient(c, observed, events, misfit, mask, self._storage_modes(c))
+
+    def _storage_modes(self, c: torch.Tensor) -> list:
+        """Wavefield storage of each source chunk of a gradient (host decision, no device work)."""
+        plan = self._plan(c.device, c.dtype)
+        n = self.n_sources
+        chunk = self.source_batch or n
+        budget = self._budget(c.device)
+        return [plan_storage(plan, min(n, s0 + chunk) - s0, self.n_steps, self.grad_mode, self.checkpoint_every,
+                             self.snapshot, budget) for s0 in range(0, n, chunk)]
+
+    def _gradient(self, c, observed, events, misfit, mask, modes):
+        """The device work of ``misfit_gradient`` (validated inputs, storage decided): enqueues only,
+        with no host synchronisation, so that it can be recorded in a CUDA graph."""
         plan = self._plan(c.device, c.dtype)
         stream = _lib.stream_handle(c.device)
         lib = _lib.load()
+        # timing events recorded inside a graph capture must become event-record nodes of the graph
+        ext = torch.cuda.is_current_stream_capturing()
         c = c.detach().contiguous()
         c2dt2 = torch.empty(plan.field, device=c.device, dtype=c.dtype)
         _lib.check(lib.nw_prepare_medium(C.byref(plan.g), plan.n_abs, c.data_ptr(), self.dt**2,
@@ -399,20 +415,19 @@ class WaveOperatorB200(_LeapfrogB200):
             misfit.prepare(observed.to(c.dtype), mask)
         n = self.n_sources
         chunk = self.source_batch or n
-        for s0 in range(0, n, chunk):
+        for k, s0 in enumerate(range(0, n, chunk)):
             S = min(n, s0 + chunk) - s0
             acq = plan.acquisition(S, s0)
-            mode = plan_storage(plan, S, self.n_steps, self.grad_mode, self.checkpoint_every,
-                                self.snapshot, self._budget(c.device))
+            mode = modes[k]
             tm = events if (events is not None and s0 == 0) else None
             run = _Run(plan, S, self.n_steps, mode, self.snapshot)
             traces = torch.empty(S, plan.n_rec, self.n_t, device=c.device, dtype=c.dtype)
             if tm is not None:
-                tm["fwd0"] = torch.cuda.Event(enable_timing=True)
+                tm["fwd0"] = torch.cuda.Event(enable_timing=True, external=ext)
                 tm["fwd0"].record()
             _forward_sweep(plan, medium, acq, run, 0, self.n_steps, traces, stream)
             if tm is not None:
-                tm["fwd1"] = torch.cuda.Event(enable_timing=True)
+                tm["fwd1"] = torch.cuda.Event(enable_timing=True, external=ext)
                 tm["fwd1"].record()
             if misfit is None:
                 resid = traces - observed[s0:s0 + S].to(c.dtype)
@@ -420,18 +435,32 @@ class WaveOperatorB200(_LeapfrogB200):
             else:
                 j, resid = misfit.value_and_grad(traces, rows=slice(s0, s0 + S))
             if tm is not None:
-                tm["adj0"] = torch.cuda.Event(enable_timing=True)
+                tm["adj0"] = torch.cuda.Event(enable_timing=True, external=ext)
                 tm["adj0"].record()
             gC, _, _ = _adjoint_sweep(plan, medium, acq, run, resid.contiguous(), False, stream)
             _lib.check(lib.nw_reduce_grad_c(C.byref(plan.g), plan.n_abs, c.data_ptr(), self.dt**2,
                                             gC.shape[0], gC.data_ptr(), 1, grad.data_ptr(), stream))
             if tm is not None:
-                tm["adj1"] = torch.cuda.Event(enable_timing=True)
+                tm["adj1"] = torch.cuda.Event(enable_timing=True, external=ext)
                 tm["adj1"].record()
             run.release()
         if misfit is not None:
             loss = j.clone()
         return loss, grad
+
+    @_lib.on_device
+    def gradient_graph(self, c: torch.Tensor, observed: torch.Tensor, events: bool = False) -> "GradientGraph":
+        """``misfit_gradient(c, observed)`` recorded once as a CUDA graph: a :class:`GradientGraph` whose
+        ``replay()`` recomputes ``loss`` and ``grad`` from its static inputs ``c`` and ``observed``
+        (copies of the arguments; write new values into them with ``run``). The speed check of
+        ``c`` and the storage decision are made when the graph is recorded and by ``run``, not by
+        ``replay``. ``events=True`` also records timing events around the first chunk's forward and
+        adjoint sweeps (``GradientGraph.events``)."""
+        self._validate(c)
+        if tuple(observed.shape) != (self.n_sources, self.n_receivers, self.n_t):
+            raise ShapeError(f"observed has shape {tuple(observed.shape)}, expected "
+                             f"{(self.n_sources, self.n_receivers, self.n_t)}")
+        return GradientGraph(self, c, observed, events)
 
     @_lib.on_device
     def simulate(self, c: torch.Tensor, observe: Callable | None = None,
@@ -551,6 +580,45 @@ class _PATFunction(torch.autograd.Function):
         ctx.p0_level = None
         gp0 = grad_p0.reshape(*ctx.batch, *plan.pgrid.shape) if ctx.needs_input_grad[0] else None
         return gp0, grad_c, None, None
+
+
+class GradientGraph:
+    """One FWI gradient of a :class:`WaveOperatorB200` recorded as a CUDA graph (see
+    ``WaveOperatorB200.gradient_graph``). The graph owns its wavefield storage for its lifetime."""
+
+    def __init__(self, op: "WaveOperatorB200", c: torch.Tensor, observed: torch.Tensor, events: bool):
+        self.op = op
+        self.device = c.device
+        self.c = c.detach().contiguous().clone()
+        self.observed = observed.to(c.dtype).contiguous().clone()
+        self._modes = op._storage_modes(self.c)
+        lib = _lib.load()
+        op._gradient(self.c, self.observed, None, None, None, self._modes)  # kernels loaded, opt-ins done
+        torch.cuda.synchronize(self.device)
+        self.events = {} if events else None
+        graph = torch.cuda.CUDAGraph()
+        n0 = lib.nw_launch_count()
+        with torch.cuda.graph(graph):
+            self.loss, self.grad = op._gradient(self.c, self.observed, self.events, None, None, self._modes)
+        self.launches = int(lib.nw_launch_count() - n0)  # this library's kernels per replay
+        self._graph = graph
+        torch.cuda.synchronize(self.device)
+
+    def replay(self) -> None:
+        """Recompute ``loss`` and ``grad`` from the current ``c`` and ``observed`` (asynchronous)."""
+        self._graph.replay()
+
+    def run(self, c: torch.Tensor, observed: torch.Tensor):
+        """Check ``c`` like the operator does, copy both inputs in, replay; returns ``(loss, grad)``."""
+        self.op._validate(c)
+        self.c.copy_(c)
+        self.observed.copy_(observed)
+        self.replay()
+        return self.loss, self.grad
+
+    def release(self) -> None:
+        self._graph = None
+        self.loss = self.grad = None
 
 
 @register("operator", "wave_initial_condition_b200")

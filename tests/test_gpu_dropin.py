@@ -8,8 +8,10 @@ and on ``cuda``, the reference's checks:
 
 * ``tests/test_instances_wave_family.py:58-62`` (``test_wave_fwi_smoke``): ``WaveFWI(steps=(20, 30))``
   runs its whole curriculum through ``Solver._run_stage`` (nefi/solve/solver.py:349,427), which calls
-  the operator as ``op(fields)`` and back-propagates through it; the data loss must fall below half its
-  start and the recovered speed must beat the initial guess (``_check_common``, :22-36);
+  the operator as ``op(fields)`` and back-propagates through it, after generating its data in
+  float64 on a 2x finer grid (``DataGenerator.clean``, nefi/bench/base.py:86-90, pointed at the GPU);
+  the data loss must fall below half its start and the recovered speed must beat the initial guess
+  (``_check_common``, :22-36);
 * ``tests/test_physics_wave.py:145-165``: checkpointed and full-history gradients agree, and agree
   with central finite differences, in float64;
 * ``tests/test_photoacoustic3d.py:49-59``: linearity and the exact adjoint identity of the
@@ -47,6 +49,15 @@ def test_wave_fwi_instance_runs_on_the_b200_operator(cuda_device, monkeypatch):
     from nefi.metrics import evaluate
 
     monkeypatch.setattr(wf, "WaveOperator", WaveOperatorB200)
+    # NEFI's data generator simulates on the CPU unless told otherwise (nefi/bench/base.py:68-80); the
+    # B200 operator has no CPU path, so the instance's float64 data generation is pointed at the GPU
+    gen_init = wf.TraceDataGenerator.__init__
+
+    def gen_on_device(self, operator, trace_mask=None, **kw):
+        kw.setdefault("device", cuda_device)
+        gen_init(self, operator, trace_mask=trace_mask, **kw)
+
+    monkeypatch.setattr(wf.TraceDataGenerator, "__init__", gen_on_device)
     inst = WaveFWI(steps=(20, 30))
     assert isinstance(inst.operator(), WaveOperatorB200)
     out = inst.run(seed=0, device=str(cuda_device))
