@@ -42,9 +42,15 @@ import numpy as np
 import torch
 
 ROOT = Path(__file__).resolve().parent
+# an installed copy of the NEFI package (the offline install under baseline/_ref), when present: the
+# B200 operators then subclass its Operator, and the reference arm also times its own torch operator
+_REF = ROOT / "baseline" / "_ref"
+if (_REF / "nefi" / "__init__.py").exists() and str(_REF) not in sys.path:
+    sys.path.append(str(_REF))
 METRIC = "FWI shot-gradients/s & Gcell-updates/s at 1e-4 grad err vs FP64; plain vs batched"
 UNIT = "shot-gradients/s"
 CPU_SAMPLE_SHOTS, CPU_SAMPLE_STEPS = 8, 300
+REF_SAMPLE_STEPS = 100  # per reference-arm step: every shot of the workload for this many steps
 
 
 def peaks() -> tuple[float, str]:
@@ -127,8 +133,8 @@ def cpu_sample(w, n_shots=CPU_SAMPLE_SHOTS, n_steps=CPU_SAMPLE_STEPS) -> tuple[f
     t = time.perf_counter() - t0
     per_shot_full = t / n_shots * (w.n_steps / n_steps)
     info = {"cores": min(threads, n_shots), "sample": f"{n_shots} shots x {n_steps} of {w.n_steps} steps "
-            f"(forward + adjoint, full {w.n + 2 * w.absorb_cells}^2 padded grid), float32; "
-            f"extrapolated linearly in steps", "seconds": t,
+            f"(forward + adjoint, full {w.n + 2 * w.absorb_cells}^2 padded grid), float32; measured {t:.2f} s, "
+            f"extrapolated linearly in steps", "seconds": t, "steps": n_steps,
             "gcell_updates_per_s": 2 * w.padded_cells() * n_steps * n_shots / t / 1e9}
     return 1.0 / per_shot_full, info
 
@@ -144,26 +150,23 @@ def make_workload(args):
     return workloads.WORKLOADS[args.workload](**kw)
 
 
-def run_batch(args) -> None:
-    """The uneven batch (64 seeded 2-D problems, 256-768^2, 4-16 shots, 1500-6000 steps) in one
-    batched, checkpointed (fixed16 snapshots), graph-replayed sweep per step, with the plain
-    one-problem-at-a-time path timed on the same problems beside it."""
+def measure_batch(dev, world: int, rank: int, n_problems: int = 64, steps: int = 3, warmup: int = 3,
+                  snapshot: str = "delta16", n_steps: int | None = None, with_plain: bool = True,
+                  with_e2e: bool = True, accuracy_problems: int = 0) -> dict:
+    """The uneven batch (seeded 2-D problems, 256-768^2, 4-16 shots, 1500-6000 steps) in one batched,
+    checkpointed (16-bit snapshots), graph-replayed gradient; with the plain one-problem-at-a-time
+    path timed beside it, the end-to-end figure, and the float32 gradient error against float64 runs
+    of ``accuracy_problems`` of the problems. Returns the bench line's fields."""
     import torch.distributed as dist
 
     from nefi_b200 import WaveOperatorB200, workloads
     from nefi_b200.batched import BatchedFWI, autotune
     from nefi_b200.distributed import problem_shards
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
-    torch.cuda.set_device(dev)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
-    ws_all = workloads.fwi_batch_problems(seed=0, n_problems=args.problems)
-    if args.n_steps:  # shortened case for profiling: steps scaled to at most n_steps
+    ws_all = workloads.fwi_batch_problems(seed=0, n_problems=n_problems)
+    if n_steps:  # shortened case for profiling: steps scaled to at most n_steps
         for w in ws_all:
-            w.n_steps = max(2, round(w.n_steps * args.n_steps / 6000))
+            w.n_steps = max(2, round(w.n_steps * n_steps / 6000))
     # whole problems over the ranks, balanced by shots x cells x steps (no collective on the data path)
     mine = problem_shards([len(w.sources) * w.padded_cells() * w.n_steps for w in ws_all], world)[rank]
     ws = [ws_all[i] for i in mine]
@@ -174,29 +177,29 @@ def run_batch(args) -> None:
         t = torch.tensor([x], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t)
-    ops = [WaveOperatorB200(w.domain, w.sources, w.receivers, grad_mode="checkpoint", snapshot="fixed16",
+    ops = [WaveOperatorB200(w.domain, w.sources, w.receivers, grad_mode="checkpoint", snapshot=snapshot,
                             **w.operator_kwargs()) for w in ws]
     cs = [torch.tensor(w.c, dtype=torch.float32, device=dev) for w in ws]
     with torch.no_grad():
         obs = [op({"c": torch.nn.functional.avg_pool2d(c[None, None], 9, 1, 4, count_include_pad=False)[0, 0]
                          .contiguous()}) for op, c in zip(ops, cs)]
     t0 = time.perf_counter()
-    tuning, _ = autotune(ops, steps=40, device=dev, repeats=1)
+    tuning, _ = autotune(ops, steps=40, device=dev, repeats=1, snapshot=snapshot)
     t_tune = time.perf_counter() - t0
-    bt = BatchedFWI(ops, device=dev, snapshot="fixed16", tuning=tuning)
+    bt = BatchedFWI(ops, device=dev, snapshot=snapshot, tuning=tuning)
     bt.misfit_gradients(cs, obs)
     t0 = time.perf_counter()
     bt.capture()
     t_capture = time.perf_counter() - t0
     flush = torch.empty(64 * 2**20, dtype=torch.float32, device=dev)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         bt.misfit_gradients(cs, obs)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     sampler = ClockSampler(dev.index)
     times = []
-    for _ in range(args.steps):
+    for _ in range(steps):
         flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -205,52 +208,35 @@ def run_batch(args) -> None:
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1))
     clocks = sampler.stop()
+    bt.check_snapshots()
     ms = max_over_ranks(sum(times) / len(times))
     shots = sum(len(w.sources) for w in ws_all)
     useful = sum(2 * w.padded_cells() * w.n_steps * len(w.sources) for w in ws_all)
     recompute = sum(w.padded_cells() * w.n_steps * len(w.sources) for w in ws_all)
     peak, peak_kind = peaks()
     achieved = 16.0 * useful / (ms * 1e-3) / 1e9
-    # the plain path on the same problems, one problem at a time (checkpointed, fixed16, default tuning)
-    for op in ops:
-        op.tuning = None
-        op._plans.clear()
-    ops[0].misfit_gradient(cs[0], obs[0])
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for op, c, d in zip(ops, cs, obs):
-        op.misfit_gradient(c, d)
-    e1.record()
-    torch.cuda.synchronize()
-    plain_ms = max_over_ranks(e0.elapsed_time(e1))
-    # end to end: models and observed data from pinned host memory in, gradients and losses out
-    c_h = [c.cpu().pin_memory() for c in cs]
-    d_h = [d.cpu().pin_memory() for d in obs]
-    g_h = [torch.empty(c.shape, dtype=torch.float64).pin_memory() for c in cs]
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    losses, grads = bt.misfit_gradients([c.to(dev, non_blocking=True) for c in c_h],
-                                        [d.to(dev, non_blocking=True) for d in d_h])
-    for g, gh in zip(grads, g_h):
-        gh.copy_(g, non_blocking=True)
-    loss_h = torch.stack(losses).cpu()
-    e1.record()
-    torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
-    h2d = sum(t.numel() * t.element_size() for t in c_h + d_h)
-    d2h = sum(t.numel() * 8 for t in g_h) + loss_h.numel() * 8
-    if world > 1:  # whole-job bytes per step, and the device bytes of the rank with the most problems
-        t = torch.tensor([float(h2d), float(d2h)], dtype=torch.float64, device=dev)
-        dist.all_reduce(t)
-        h2d, d2h = int(t[0]), int(t[1])
-    out = {"metric": METRIC, "value": shots / (ms * 1e-3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f32",
-           "data": "synthetic (64 seeded layered models; observed data from smoothed models)",
+    accuracy = None
+    if accuracy_problems > 0:
+        # the batch's float32 gradients (16-bit snapshots) against float64 runs of the same problems
+        # alone (exact checkpoints), for the problems with the least work
+        _, grads = bt._outputs()
+        pick = sorted(range(len(ws)), key=lambda i: len(ws[i].sources) * ws[i].padded_cells() * ws[i].n_steps)
+        errs = {}
+        for i in pick[:accuracy_problems]:
+            g32 = grads[i].clone()
+            w = ws[i]
+            op64 = WaveOperatorB200(w.domain, w.sources, w.receivers, grad_mode="checkpoint", **w.operator_kwargs())
+            _, g64 = op64.misfit_gradient(cs[i].double(), obs[i].double())
+            errs[f"problem{mine[i]} ({w.n}^2, {len(w.sources)} shots, {w.n_steps} steps)"] = float(
+                (g32 - g64).norm() / g64.norm())
+            del op64, g64
+        accuracy = {"grad_rel_l2_fp32_vs_fp64": max(errs.values()), "per_problem": errs,
+                    "fp32_storage": f"checkpointed, {snapshot} snapshots, segment {bt.segment}",
+                    "fp64_storage": "checkpointed, exact snapshots"}
+    out = {"value": shots / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "steps": steps, "warmup": warmup,
            "config": {"workload": f"fwi_batch: {len(ws_all)} problems, grids {{256,384,512,768}}^2 + 20-cell sponge, "
                                   f"4-16 Ricker shots, 1500-6000 steps (seed 0), order 4; checkpointed with "
-                                  f"fixed16 snapshots, segment {bt.segment}; one launch per step over all running "
+                                  f"{snapshot} snapshots, segment {bt.segment}; one launch per step over all running "
                                   f"problems, whole gradient replayed from one CUDA graph",
                       "method": "batched", "shots_total": shots, "tuning": list(tuning),
                       "parallelism": f"whole problems balanced by cost over {world} GPU(s); no collective",
@@ -260,18 +246,139 @@ def run_batch(args) -> None:
            "gcell_updates_per_s": useful / (ms * 1e-3) / 1e9,
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                         "traffic": None, "peak_source": peak_kind,
-                        "note": "16 B per useful cell-update (forward + adjoint); the segment recompute "
-                                f"({recompute / 1e9:.0f} G extra cell-updates per gradient) is not counted",
+                        "note": "16 B per useful cell-update (forward + adjoint) over the CUDA-event time of the "
+                                f"replays; the segment recompute ({recompute / 1e9:.0f} G extra cell-updates per "
+                                "gradient) is not counted",
                         "kernel_rate_GBps_incl_recompute": 16.0 * (useful + recompute) / (ms * 1e-3) / 1e9},
-           "plain": {"value": shots / (plain_ms * 1e-3), "unit": UNIT, "ms_per_gradient_of_all_problems": plain_ms,
-                     "method": "each problem alone through WaveOperatorB200.misfit_gradient (same storage)"},
-           "e2e": {"value": shots / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-           "clocks": clocks,
-           "gpu_launches": bt.graph_launches * args.steps}
+           "accuracy": accuracy, "clocks": clocks, "gpu_launches": bt.graph_launches * steps}
+    if with_plain:
+        # the plain path on the same problems, one problem at a time (same storage, default tuning)
+        for op in ops:
+            op.tuning = None
+            op._plans.clear()
+        ops[0].misfit_gradient(cs[0], obs[0])
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for op, c, d in zip(ops, cs, obs):
+            op.misfit_gradient(c, d)
+        e1.record()
+        torch.cuda.synchronize()
+        plain_ms = max_over_ranks(e0.elapsed_time(e1))
+        out["plain"] = {"value": shots / (plain_ms * 1e-3), "unit": UNIT, "ms_per_gradient_of_all_problems": plain_ms,
+                        "method": "each problem alone through WaveOperatorB200.misfit_gradient (same storage)"}
+    if with_e2e:
+        # end to end: models and observed data from pinned host memory in, gradients and losses out
+        c_h = [c.cpu().pin_memory() for c in cs]
+        d_h = [d.cpu().pin_memory() for d in obs]
+        g_h = [torch.empty(c.shape, dtype=torch.float64).pin_memory() for c in cs]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        losses, grads = bt.misfit_gradients([c.to(dev, non_blocking=True) for c in c_h],
+                                            [d.to(dev, non_blocking=True) for d in d_h])
+        for g, gh in zip(grads, g_h):
+            gh.copy_(g, non_blocking=True)
+        loss_h = torch.stack(losses).cpu()
+        e1.record()
+        torch.cuda.synchronize()
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+        h2d = sum(t.numel() * t.element_size() for t in c_h + d_h)
+        d2h = sum(t.numel() * 8 for t in g_h) + loss_h.numel() * 8
+        if world > 1:  # whole-job bytes per step
+            t = torch.tensor([float(h2d), float(d2h)], dtype=torch.float64, device=dev)
+            dist.all_reduce(t)
+            h2d, d2h = int(t[0]), int(t[1])
+        out["e2e"] = {"value": shots / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                      "d2h_bytes_per_step": d2h}
+    bt._graph = None
+    del bt
+    torch.cuda.empty_cache()
+    return out
+
+
+def measure_checkpointed(dev, w, snapshot: str = "delta16", steps: int = 1, warmup: int = 1,
+                         accuracy_shots: int = 4) -> dict:
+    """One FWI gradient of workload ``w`` with checkpointed storage and 16-bit snapshots (the large
+    configuration's method), CUDA-event timed; with the float32 gradient error against a float64 run
+    (exact snapshots) over the first ``accuracy_shots`` shots. Returns the bench line's fields."""
+    from nefi_b200 import WaveOperatorB200
+    from nefi_b200.plan import plan_storage
+
+    op = WaveOperatorB200(w.domain, w.sources, w.receivers, grad_mode="checkpoint", snapshot=snapshot,
+                          **w.operator_kwargs())
+    c = torch.tensor(w.c, dtype=torch.float32, device=dev)
+    with torch.no_grad():
+        d = op({"c": torch.nn.functional.avg_pool2d(c[None, None], 9, 1, 4, count_include_pad=False)[0, 0]
+                .contiguous()})
+    mode = plan_storage(op._plan(dev, torch.float32), len(w.sources), op.n_steps, op.grad_mode,
+                        op.checkpoint_every, op.snapshot, op._budget(dev))
+    flush = torch.empty(64 * 2**20, dtype=torch.float32, device=dev)
+    for _ in range(warmup):
+        op.misfit_gradient(c, d)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(dev.index)
+    times = []
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        op.misfit_gradient(c, d)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    clocks = sampler.stop()
+    ms = sum(times) / len(times)
+    S = len(w.sources)
+    useful = 2 * w.padded_cells() * w.n_steps * S
+    peak, peak_kind = peaks()
+    achieved = 16.0 * useful / (ms * 1e-3) / 1e9
+    accuracy = None
+    if accuracy_shots > 0:
+        na = accuracy_shots
+        op32 = WaveOperatorB200(w.domain, w.sources[:na], w.receivers, grad_mode="checkpoint", snapshot=snapshot,
+                                **w.operator_kwargs())
+        _, g32 = op32.misfit_gradient(c, d[:na])
+        del op32
+        op64 = WaveOperatorB200(w.domain, w.sources[:na], w.receivers, grad_mode="checkpoint", **w.operator_kwargs())
+        _, g64 = op64.misfit_gradient(c.double(), d[:na].double())
+        accuracy = {"grad_rel_l2_fp32_vs_fp64": float((g32 - g64).norm() / g64.norm()), "shots": na,
+                    "fp32_storage": f"checkpointed every {mode[1]} steps, {snapshot} snapshots",
+                    "fp64_storage": "checkpointed, exact snapshots"}
+        del op64, g32, g64
+    del op, c, d
+    torch.cuda.empty_cache()
+    return {"value": S / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "steps": steps, "warmup": warmup,
+            "config": workload_desc(w, f"checkpointed every {mode[1]} steps with {snapshot} snapshots"),
+            "gcell_updates_per_s": useful / (ms * 1e-3) / 1e9,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                         "note": "16 B per useful cell-update (forward + adjoint) over the CUDA-event time of "
+                                 "the whole gradient; the segment recompute is not counted"},
+            "accuracy": accuracy, "clocks": clocks}
+
+
+def run_batch(args) -> None:
+    """``--workload fwi_batch``: the batch's own bench line (whole problems over the ranks under
+    torchrun, no collective on the data path)."""
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+    snapshot = args.snapshot if args.snapshot != "exact" else "delta16"
+    m = measure_batch(dev, world, rank, args.problems, args.steps, args.warmup, snapshot, args.n_steps,
+                      accuracy_problems=0 if args.no_accuracy else 4)
+    out = {"metric": METRIC, "value": m["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic (64 seeded layered models; observed data from smoothed models)",
+           **{k: v for k, v in m.items() if k not in ("value", "unit", "ms_per_step", "steps", "warmup")}}
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:
-        bt._graph = None  # no NCCL calls in the graph, but release it before the group goes
         dist.barrier()
         dist.destroy_process_group()
 
@@ -650,27 +757,66 @@ def run_misfit(args) -> None:
     print(json.dumps(out), flush=True)
 
 
-def run_reference(args) -> None:
-    from nefi_b200 import workloads
+def reference_torch_sample(w, n_shots: int = 4, n_steps: int = 50) -> dict | None:
+    """The reference's own operator (nefi.physics.wave.WaveOperator, torch on the host cores) on a
+    bounded sample of workload ``w``: forward + autograd gradient of 1/2 ||traces||^2 w.r.t. c for
+    ``n_shots`` shots x ``n_steps`` steps, extrapolated linearly in shots and steps. None when the
+    nefi package is not importable (an installed copy under baseline/_ref is used when present)."""
+    try:
+        from nefi.domain import Domain
+        from nefi.physics.wave import WaveOperator
+    except Exception:
+        return None
+    torch.set_num_threads(os.cpu_count() or 1)
+    kw = dict(w.operator_kwargs())
+    kw["n_t"] = n_steps + 1
+    L = w.n * w.h
+    op = WaveOperator(Domain((w.n, w.n), ((0.0, L), (0.0, L)), axes=("x", "z")), torch.tensor(w.sources[:n_shots]),
+                      torch.tensor(w.receivers), grad_mode="autograd", **kw)
+    c = torch.tensor(w.c, dtype=torch.float32, requires_grad=True)
+    t0 = time.perf_counter()
+    (0.5 * op({"c": c}).square().sum()).backward()
+    t = time.perf_counter() - t0
+    per_shot_full = t / n_shots * (w.n_steps / n_steps)
+    return {"value": 1.0 / per_shot_full, "unit": UNIT, "cores": torch.get_num_threads(), "kind": "reference",
+            "sample": f"nefi.physics.wave.WaveOperator (torch {torch.__version__}, CPU) forward + autograd gradient, "
+                      f"{n_shots} shots x {n_steps} of {w.n_steps} steps, float32; measured {t:.2f} s, "
+                      f"extrapolated linearly in shots and steps",
+            "sample_s": t, "gcell_updates_per_s": 2 * w.padded_cells() * n_steps * n_shots / t / 1e9}
 
+
+def run_reference(args) -> None:
+    """The reference arm: the CPU restatement of the reference's algorithm (the float32 C oracle, OpenMP
+    over shots on every host thread) timed on a bounded sample of the same workload per step: all of
+    the workload's shots for the first REF_SAMPLE_STEPS leapfrog steps, forward and adjoint. Each step
+    costs the same (fixed grid, fixed stencil), so ``value`` extrapolates the sample linearly in steps
+    to the full gradient; ``ms_per_step`` is the measured time of one sample."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     w = make_workload(args)
-    vals, info = [], {}
+    S = len(w.sources)
+    vals, secs, info = [], [], {}
     for i in range(args.warmup + args.steps):
-        v, info = cpu_sample(w)
+        v, info = cpu_sample(w, n_shots=S, n_steps=REF_SAMPLE_STEPS)
         if i >= args.warmup:
             vals.append(v)
+            secs.append(info["seconds"])
     v = statistics.median(vals)
+    sample_ms = 1000.0 * statistics.median(secs)
     out = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * len(w.sources) / v,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": sample_ms,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
            "data": "synthetic (seeded)", "config": {**workload_desc(w), "parallelism": "cpu threads"},
+           "sample": {"what": info["sample"], "measured_ms_per_sample": sample_ms,
+                      "extrapolation": f"value = {S} shots / (sample time x {w.n_steps} / {info['steps']} steps)"},
            "cpu_baseline": {"value": v, "unit": UNIT, "cores": info["cores"], "kind": "port",
                             "sample": info["sample"]},
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
            "gcell_updates_per_s": info["gcell_updates_per_s"]}
+    ref = reference_torch_sample(w)
+    if ref is not None:
+        out["cpu_baseline"]["reference_torch"] = ref
     print(json.dumps(out), flush=True)
 
 
@@ -686,6 +832,8 @@ def main() -> None:
     ap.add_argument("--workload", default="fwi_512")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="fwi_512: skip the batched and 2048^2 checkpointed measurements of the same line")
     ap.add_argument("--n-steps", type=int, default=None, help="override the leapfrog steps (profiling cases)")
     ap.add_argument("--shots", type=int, default=None, help="override the shots per GPU (profiling cases)")
     ap.add_argument("--problems", type=int, default=64, help="fwi_batch: problems in the batch")
@@ -744,40 +892,43 @@ def main() -> None:
     flush = torch.empty(64 * 2**20, dtype=torch.float32, device=dev)
     lib = _lib.load()
 
-    def step(cc, dd, events=None):
-        loss, g = op.misfit_gradient(cc, dd, events=events)
+    # the timed step: the whole gradient (media, forward sweep, misfit, adjoint sweep, float64
+    # reduction) recorded once as a CUDA graph and replayed, so no host work sits inside the timed
+    # region; under torchrun the gradient and the misfit are then summed over the ranks
+    graph = op.gradient_graph(c, d, events=True)
+
+    def step():
+        graph.replay()
         if world > 1:  # the float64 gradient and the scalar misfit summed over the ranks' shots
-            dist.all_reduce(g)
-            dist.all_reduce(loss)
-        return loss, g
+            dist.all_reduce(graph.grad)
+            dist.all_reduce(graph.loss)
 
     for _ in range(args.warmup):
-        step(c, d)
+        step()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
 
     sampler = ClockSampler(dev.index if "CUDA_VISIBLE_DEVICES" not in os.environ else local)
     times, fwd_ms, adj_ms = [], [], []
-    launches0 = lib.nw_launch_count()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     for _ in range(args.steps):
         flush.zero_()
-        ev = {}
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        step(c, d, ev)
+        step()
         e1.record()
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1))
+        ev = graph.events
         fwd_ms.append(ev["fwd0"].elapsed_time(ev["fwd1"]))
         adj_ms.append(ev["adj0"].elapsed_time(ev["adj1"]))
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    launches = lib.nw_launch_count() - launches0
+    launches = graph.launches * args.steps
     clocks = sampler.stop()
     total_ms = sum(times)
     if world > 1:
@@ -789,8 +940,12 @@ def main() -> None:
     value = S * world / (ms_per_step / 1000.0)
     cells = w.padded_cells()
     gcells = 2 * cells * w.n_steps * S * world / (ms_per_step / 1000.0) / 1e9
+    graph.release()
+    del graph
+    torch.cuda.empty_cache()
 
-    # roofline of the dominant stencil kernel: 16 B per cell-update, per launch = cells * shots
+    # roofline of the dominant stencil kernel: 16 B per cell-update, per launch = cells * shots; the
+    # kernels' time is the CUDA-event time of their sweeps inside the timed replays, per step
     peak, peak_kind = peaks()
     alg_bytes = 16.0 * cells * S
     fwd_launch_ms = statistics.median(fwd_ms) / w.n_steps
@@ -806,29 +961,40 @@ def main() -> None:
             traffic = tj[kern]["bytes_per_launch_full"]
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "kernel": kern, "peak_source": peak_kind,
+                "traffic_source": "profiles/traffic.json: one cold-cache ncu capture of a 100-step case, "
+                                  "bytes per launch scaled to this workload; not this run's traffic",
                 "algorithmic_bytes_per_launch": alg_bytes,
                 "per_kernel_GBps": {"fwd2d": alg_bytes / (fwd_launch_ms * 1e-3) / 1e9,
                                     "adj2d_with_injection": alg_bytes / (adj_launch_ms * 1e-3) / 1e9}}
 
-    # end to end through the public API: H2D of c and d from pinned memory, D2H of loss and gradient
+    # end to end through the drop-in call a NEFI solver makes (nefi/physics/wave.py:742-750): c and
+    # the observed traces from pinned host memory, traces = op({"c": c}), the misfit
+    # 1/2 ||traces - d||^2 in torch, loss.backward() through the autograd function, then the
+    # gradient and the loss back to the host
     c_h = c.cpu().pin_memory()
     d_h = d.cpu().pin_memory()
-    g_h = torch.empty(c.shape, dtype=torch.float64).pin_memory()
+    g_h = torch.empty(c.shape, dtype=torch.float32).pin_memory()
     l_h = torch.empty((), dtype=torch.float64).pin_memory()
     e2e_ms = []
     for i in range(2 + args.steps):  # two untimed passes: the pinned copies' first use, allocator growth
         flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        cd = c_h.to(dev, non_blocking=True)
+        cd = c_h.to(dev, non_blocking=True).requires_grad_(True)
         dd = d_h.to(dev, non_blocking=True)
-        loss, g = step(cd, dd)
+        loss = 0.5 * (op({"c": cd}) - dd).double().square().sum()
+        loss.backward()
+        g = cd.grad
+        if world > 1:
+            dist.all_reduce(g)
+            dist.all_reduce(loss)
         g_h.copy_(g, non_blocking=True)
-        l_h.copy_(loss, non_blocking=True)
+        l_h.copy_(loss.detach(), non_blocking=True)
         e1.record()
         torch.cuda.synchronize()
         if i > 1:
             e2e_ms.append(e0.elapsed_time(e1))
+        del cd, dd, loss, g
     e2e_total = sum(e2e_ms)
     if world > 1:
         t = torch.tensor([e2e_total], device=dev, dtype=torch.float64)
@@ -836,7 +1002,33 @@ def main() -> None:
         e2e_total = float(t)
     e2e_val = S * world / (e2e_total / len(e2e_ms) / 1000.0)
     h2d = c_h.numel() * c_h.element_size() + d_h.numel() * d_h.element_size()
-    d2h = g_h.numel() * 8 + 8
+    d2h = g_h.numel() * g_h.element_size() + 8
+
+    # the same end to end through this package's own gradient call (misfit_gradient: no traces
+    # materialised for torch, float64 gradient)
+    g64_h = torch.empty(c.shape, dtype=torch.float64).pin_memory()
+    mg_ms = []
+    for i in range(2 + args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        loss, g = op.misfit_gradient(c_h.to(dev, non_blocking=True), d_h.to(dev, non_blocking=True))
+        if world > 1:
+            dist.all_reduce(g)
+            dist.all_reduce(loss)
+        g64_h.copy_(g, non_blocking=True)
+        l_h.copy_(loss, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        if i > 1:
+            mg_ms.append(e0.elapsed_time(e1))
+        del loss, g
+    mg_total = sum(mg_ms)
+    if world > 1:
+        t = torch.tensor([mg_total], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        mg_total = float(t)
+    mg_val = S * world / (mg_total / len(mg_ms) / 1000.0)
 
     from nefi_b200.plan import plan_storage
 
@@ -884,17 +1076,35 @@ def main() -> None:
         cpu = {"value": v, "unit": UNIT, "cores": info["cores"], "kind": "port", "sample": info["sample"],
                "gcell_updates_per_s": info["gcell_updates_per_s"]}
 
+    # the north-star method under the same clock: the uneven batch (batched, checkpointed, 16-bit
+    # snapshots, graph-replayed) and the large configuration (checkpointed, 16-bit snapshots), each
+    # with its own roofline, accuracy against float64 and clocks; one GPU, default workload only
+    extras = {}
+    if world == 1 and args.workload == "fwi_512" and not args.no_extras and not args.n_steps:
+        from nefi_b200 import workloads as _wl
+
+        torch.cuda.empty_cache()
+        extras["batched"] = measure_batch(dev, 1, 0, 64, steps=2, warmup=0, snapshot="delta16",
+                                          with_plain=True, with_e2e=False, accuracy_problems=0 if args.no_accuracy else 4)
+        extras["checkpointed_2048"] = measure_checkpointed(dev, _wl.fwi_2048(), snapshot="delta16", steps=1, warmup=1,
+                                                           accuracy_shots=0 if args.no_accuracy else 4)
+
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "f32",
                "data": "synthetic (seeded layered model; observed data from a smoothed model)",
-               "config": {**workload_desc(w, storage, op.absorbing), "method": f"plain (per-step launches, {storage})",
+               "config": {**workload_desc(w, storage, op.absorbing),
+                          "method": f"plain (per-step launches replayed from one CUDA graph, {storage})",
                           "parallelism": f"shots sharded over {world} GPU(s), fp64 gradient and loss all-reduce"},
                "gcell_updates_per_s": gcells, "roofline": roofline, "cpu_baseline": cpu,
                "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                       "call": "traces = op({'c': c}); loss = 1/2 ||traces - d||^2 (torch); loss.backward()",
                        "ms_each": e2e_ms},
-               "clocks": clocks, "gpu_launches": int(launches), "accuracy": accuracy}
+               "e2e_misfit_gradient": {"value": mg_val, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                                       "d2h_bytes_per_step": g64_h.numel() * 8 + 8,
+                                       "call": "op.misfit_gradient(c, d)", "ms_each": mg_ms},
+               "clocks": clocks, "gpu_launches": int(launches), "accuracy": accuracy, **extras}
         print(json.dumps(out), flush=True)
     if world > 1:
         dist.barrier()

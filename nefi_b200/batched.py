@@ -34,7 +34,7 @@ class BatchedFWI:
     band-limited (relative) MSE, loss and adjoint source from the fused misfit pass."""
 
     def __init__(self, ops: Sequence[WaveOperatorB200], *, device: torch.device | str = "cuda",
-                 dtype: torch.dtype = torch.float32, segment: int | None = None, snapshot: str = "fixed16",
+                 dtype: torch.dtype = torch.float32, segment: int | None = None, snapshot: str = "delta16",
                  tuning: Sequence[int] | None = None, misfits: Sequence | None = None,
                  masks: Sequence | None = None) -> None:
         if not ops:
@@ -211,7 +211,7 @@ class BatchedFWI:
 
 @_lib.on_device
 def autotune(ops: Sequence[WaveOperatorB200], *, steps: int = 120, device="cuda", dtype=torch.float32,
-             snapshot: str = "fixed16", fwd_candidates=((4, 2, 2), (2, 4, 2), (4, 2, 1), (2, 2, 2), (4, 4, 1)),
+             snapshot: str = "delta16", fwd_candidates=((4, 2, 2), (2, 4, 2), (4, 2, 1), (2, 2, 2), (4, 4, 1)),
              adj_candidates=((2, 2, 4), (2, 2, 2), (4, 2, 4), (2, 4, 4), (2, 2, 8)), repeats: int = 2):
     """Choose the forward and adjoint tile shapes ``(vz, rx, shots_per_cta)`` for a batch by timing
     each candidate's sweep on a copy of the batch shortened to ``steps`` time steps (the per-step
