@@ -76,6 +76,22 @@ __device__ __forceinline__ void vldg(const T* p, T (&o)[N]) {
     for (int i = 0; i < N; ++i) o[i] = q[i];
   }
 }
+// Global load through L2 only (ld.global.cg): used for levels an earlier kernel wrote, read before
+// griddepcontrol.wait, where a line left in this SM's L1 by an older kernel must not be returned.
+template <typename T, int N>
+__device__ __forceinline__ void vldcg(const T* p, T (&o)[N]) {
+  if constexpr (sizeof(T) * N == 16) {
+    const float4 t = __ldcg(reinterpret_cast<const float4*>(p));
+    const T* q = reinterpret_cast<const T*>(&t);
+#pragma unroll
+    for (int i = 0; i < N; ++i) o[i] = q[i];
+  } else {
+    const float2 t = __ldcg(reinterpret_cast<const float2*>(p));
+    const T* q = reinterpret_cast<const T*>(&t);
+#pragma unroll
+    for (int i = 0; i < N; ++i) o[i] = q[i];
+  }
+}
 template <typename T, int N>
 __device__ __forceinline__ void vstore(T* p, const T (&o)[N]) {
   if constexpr (sizeof(T) * N == 16) {
@@ -122,6 +138,8 @@ struct Tiled2 {
   const T* __restrict__ A;
   const T* __restrict__ B;
   int b_one;                    // forward: B = 1 on the first step (Cerjan)
+  int prev_ready;               // forward: p^{n-1} was written two or more launches back, so it may be
+                                // read before griddepcontrol.wait (0: after it)
   int apply_a;                  // adjoint: A applies (n >= 1); at n = 0 the output is C lambda^0
   int n_shots, shots_per_cta;
   // forward: point sources, receiver samples of p^n
@@ -280,27 +298,39 @@ __device__ __forceinline__ void fwd2d_body(const KGrid<T>& g, const Tiled2<T>& a
   const bool use_b = layer_tile && !a.b_one;
   const CopyPlan<S::NCH> ph = plan_halo<T, VZ, RX, R>(g, x0, z0);
   const CopyPlan<S::NCC> pc = plan_core<T, VZ, RX, R>(g, x0, z0);
-  wait_previous_grid();
-  allow_next_grid();
+  // Before the wait, while the previous step finishes: everything this launch reads that no kernel
+  // still running writes -- the coefficients (constant over the sweep), the per-tile tables, the
+  // first shot's source corner, and p^{n-1}, which the step two launches back wrote (that launch
+  // completed before the previous one passed its own wait, which had to happen before this one
+  // could start) and which nothing writes until this step has finished reading it.
   issue(pc, a.C, scc);  // once per CTA, in the first commit group
   if (layer_tile) {
     issue(pc, a.A, sa);
     issue(pc, a.B, sbb);
-  }
-#pragma unroll
-  for (int i = 0; i < NS - 1; ++i) {  // one commit group per shot, empty groups included, so that
-    if (sb + i < se) issue(ph, a.cur + (long long)(sb + i) * g.field, sp + i * S::PS);
-    cp_async_commit();                // wait_group<NS-1> in the loop means "shot s has landed"
   }
   T pv[RX][VZ];  // p^{n-1} of the owned cells, one shot ahead
 #pragma unroll
   for (int k = 0; k < RX; ++k) {
 #pragma unroll
     for (int v = 0; v < VZ; ++v) pv[k][v] = T(0);
-    if (ok[k]) vldg<T, VZ>(a.prev + (long long)sb * g.field + cbase + (long long)k * ld, pv[k]);
+    if (a.prev_ready && ok[k]) vldcg<T, VZ>(a.prev + (long long)sb * g.field + cbase + (long long)k * ld, pv[k]);
   }
   int e0 = 0, e1 = 0;
   if (a.traces) { e0 = a.tt.rec_ptr[tile]; e1 = a.tt.rec_ptr[tile + 1]; }
+  int2 scor = make_int2(-1 << 20, -1 << 20);  // the next shot's source corner (x, z), one shot ahead
+  if (a.src_corner) scor = make_int2(a.src_corner[2 * sb], a.src_corner[2 * sb + 1]);
+  wait_previous_grid();
+  allow_next_grid();
+  if (!a.prev_ready) {  // p^{n-1} came from the launch just before (a snapshot decode, an initial state)
+#pragma unroll
+    for (int k = 0; k < RX; ++k)
+      if (ok[k]) vldg<T, VZ>(a.prev + (long long)sb * g.field + cbase + (long long)k * ld, pv[k]);
+  }
+#pragma unroll
+  for (int i = 0; i < NS - 1; ++i) {  // one commit group per shot, empty groups included, so that
+    if (sb + i < se) issue(ph, a.cur + (long long)(sb + i) * g.field, sp + i * S::PS);
+    cp_async_commit();                // wait_group<NS-1> in the loop means "shot s has landed"
+  }
   const T wc = g.wc, w1x = g.w1a, w1z = g.w1b, w2x = g.w2a, w2z = g.w2b;
 
   for (int s = sb; s < se; ++s) {
@@ -325,12 +355,11 @@ __device__ __forceinline__ void fwd2d_body(const KGrid<T>& g, const Tiled2<T>& a
       a.traces[((long long)s * a.n_rec + r) * a.n_t + a.j] = acc;
     }
     // the shot's source stencil, if it touches this tile (a CTA-uniform test)
-    int bx = 0, bz = 0;
     bool src_tile = false;
     T sw0 = 0, sw1 = 0, sw2 = 0, sw3 = 0;
+    const int bx = scor.x, bz = scor.y;
     if (a.src_corner) {
-      bx = a.src_corner[2 * s];
-      bz = a.src_corner[2 * s + 1];
+      if (s + 1 < se) scor = make_int2(a.src_corner[2 * (s + 1)], a.src_corner[2 * (s + 1) + 1]);
       src_tile = bx + 1 >= x0 && bx < x0 + S::TX && bz + 1 >= z0 && bz < z0 + S::TZ;
       if (src_tile) {
         const T wn = a.wavelet[a.n];
@@ -428,23 +457,12 @@ __device__ __forceinline__ void adj2d_body(const KGrid<T>& g, const Tiled2<T>& a
   const bool layer_tile = AB && (x0 < g.lo0 || x0 + S::TX > g.hi0 || z0 < g.lo1 || z0 + S::TZ > g.hi1);
   const CopyPlan<S::NCH> ph = plan_halo<T, VZ, RX, R>(g, x0, z0);
   const CopyPlan<S::NCC> pc = plan_core<T, VZ, RX, R>(g, x0, z0);
-  wait_previous_grid();
-  allow_next_grid();
-  // once per CTA, in the first commit group: C, A and B (layer tiles) and the accumulator tile
+  // once per CTA, in the first commit group: C, A and B (layer tiles), constant over the sweep, so
+  // issued before the wait while the previous step finishes
   issue(pc, a.C, scc);
   if (layer_tile) {
     issue(pc, a.A, sa);
     issue(pc, a.B, sbb);
-  }
-  if (grad) issue(pc, a.gacc + (long long)bz * g.field, sg);
-#pragma unroll
-  for (int i = 0; i < NS - 1; ++i) {  // one commit group per shot, empty groups included, so that
-    if (sb + i < se) {                // wait_group<NS-1> in the loop means "shot s has landed"
-      issue(ph, a.cur + (long long)(sb + i) * g.field, sp + i * S::PS);
-      issue(pc, a.prev + (long long)(sb + i) * g.field, sq + i * S::QS);
-      if (grad) issue(pc, a.lap + (long long)(sb + i) * g.field, sl + i * S::QS);
-    }
-    cp_async_commit();
   }
   int c0 = 0, c1 = 0;
   if (a.gtr) { c0 = a.tt.cell_ptr[tile]; c1 = a.tt.cell_ptr[tile + 1]; }
@@ -471,6 +489,18 @@ __device__ __forceinline__ void adj2d_body(const KGrid<T>& g, const Tiled2<T>& a
       }
     }
     __syncthreads();  // zeroing completes before any thread writes a cotangent value
+  }
+  wait_previous_grid();
+  allow_next_grid();
+  if (grad) issue(pc, a.gacc + (long long)bz * g.field, sg);  // the previous step updated it
+#pragma unroll
+  for (int i = 0; i < NS - 1; ++i) {  // one commit group per shot, empty groups included, so that
+    if (sb + i < se) {                // wait_group<NS-1> in the loop means "shot s has landed"
+      issue(ph, a.cur + (long long)(sb + i) * g.field, sp + i * S::PS);
+      issue(pc, a.prev + (long long)(sb + i) * g.field, sq + i * S::QS);
+      if (grad) issue(pc, a.lap + (long long)(sb + i) * g.field, sl + i * S::QS);
+    }
+    cp_async_commit();
   }
 
   const bool use_a = layer_tile && a.apply_a;
@@ -653,6 +683,9 @@ __global__ void __launch_bounds__(256, 4) fwd2d_batch(const BatchProb<T>* __rest
     t.cur = P.ring + (long long)((n + 1) % 3) * P.level;
     t.next = P.ring + (long long)((n + 2) % 3) * P.level;
     t.b_one = (n == 0 && P.first_b_one) ? 1 : 0;
+    // a recompute segment starts from decoded snapshots, the sweep from the initial state: the
+    // launch just before wrote p^{n-1}
+    t.prev_ready = store_lap ? (n % segment != 0) : (n > 0);
     t.n = n;
     t.traces = (!store_lap && P.traces && t.n_rec > 0 && n % P.substeps == 0) ? P.traces : nullptr;
     t.j = n / P.substeps;

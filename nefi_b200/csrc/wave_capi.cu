@@ -449,13 +449,22 @@ void pml_medium(const nw_medium* m, nw::PmlStep<T>& st) {
   st.cz1 = m->pml_core[3];
 }
 
+// The PML cells outside the tiled box (all cells when there is none): 16-byte chunks of a row, a
+// thread per chunk, a CTA of 128 threads per 128 chunks and group of shots; the shot groups are as
+// small as keeps about four CTAs per SM busy, since a CTA reuses its cells' coefficients over its
+// group.
 template <typename T, bool ADJ>
 int launch_pml(const nw_grid* g, const nw::KGrid<T>& kg, const nw::PmlStep<T>& st, int n_shots, cudaStream_t s) {
   const long long cells = (long long)g->n[0] * g->n[1] - (long long)(st.kx1 - st.kx0) * (st.kz1 - st.kz0);
   if (cells <= 0) return NW_OK;
-  const dim3 grid((unsigned)((cells + 255) / 256), n_shots);
-  if (g->radius == 1) return launch_pdl(nw::pml2d_step<T, 1, ADJ>, grid, 0, s, kg, st);
-  return launch_pdl(nw::pml2d_step<T, 2, ADJ>, grid, 0, s, kg, st);
+  nw::PmlChunks<T> ck = nw::pml_chunks<T>(g->n[0], g->n[1], st.kx0, st.kx1, st.kz0, st.kz1, 1);
+  const int per_group = (ck.n_all + 127) / 128;
+  const int groups = std::max(1, std::min(n_shots, (4 * 148 + per_group - 1) / per_group));
+  ck.spc = (n_shots + groups - 1) / groups;
+  const dim3 grid((unsigned)per_group, (unsigned)((n_shots + ck.spc - 1) / ck.spc));
+  if (g->radius == 1)
+    return launch_pdl_b(nw::pml2d_chunk_step<T, 1, ADJ>, grid, dim3(128), 0, s, kg, st, ck, n_shots);
+  return launch_pdl_b(nw::pml2d_chunk_step<T, 2, ADJ>, grid, dim3(128), 0, s, kg, st, ck, n_shots);
 }
 
 // A second stream of the calling thread on the current device, with a fork and a join event: a PML
@@ -553,7 +562,7 @@ struct Ring {  // time level n (n >= -1) of the pressure field: three rotating l
 template <typename T>
 int forward_step(const nw_grid* g, const nw::KGrid<T>& kg, const nw_medium* m, const nw_acquisition* a,
                  const nw_time* t, const Tune& tu, const Ring<T>& L, int n, T* traces, T* lap_out,
-                 cudaStream_t s, T* psi = nullptr) {
+                 cudaStream_t s, T* psi = nullptr, bool prev_ready = false) {
   const bool rec = traces && a->n_rec > 0 && (n % t->substeps) == 0;
   if (g->absorbing == NW_ABS_PML) {  // 2-D with the reference's PML: psi levels 2*axis + parity
     if (rec) {
@@ -606,6 +615,7 @@ int forward_step(const nw_grid* g, const nw::KGrid<T>& kg, const nw_medium* m, c
     st.A = (const T*)m->coef_a;
     st.B = (const T*)m->coef_b;
     st.b_one = (n == 0 && t->first_b_one) ? 1 : 0;
+    st.prev_ready = prev_ready ? 1 : 0;
     st.src_corner = a->has_source ? a->src_corner : nullptr;
     st.src_w = (const T*)a->src_weight;
     st.wavelet = (const T*)a->wavelet;
@@ -663,7 +673,8 @@ int forward_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
       if (rc) return rc;
     }
     T* lap = st->history ? (T*)st->history + (long long)n * LE : nullptr;
-    int rc = forward_step<T>(g, kg, m, a, t, tu, L, n, traces, lap, s, (T*)st->pml_psi);
+    // from the second step of the call on, p^{n-1} is the output of a step two launches back
+    int rc = forward_step<T>(g, kg, m, a, t, tu, L, n, traces, lap, s, (T*)st->pml_psi, n > n_begin);
     if (rc) return rc;
   }
   if (traces && n_end == t->n_steps && t->n_steps % t->substeps == 0) {
@@ -790,7 +801,7 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
         if (rc) return rc;
         for (int k = n0; k < n1; ++k) {
           rc = forward_step<T>(g, kg, m, a, t, tu, L, k, nullptr, (T*)st->segbuf + (long long)(k - n0) * LE, s,
-                               (T*)st->pml_psi);
+                               (T*)st->pml_psi, k > n0);
           if (rc) return rc;
         }
       }
