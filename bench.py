@@ -221,18 +221,27 @@ def measure_batch(dev, world: int, rank: int, n_problems: int = 64, steps: int =
         # alone (exact checkpoints), for the problems with the least work
         _, grads = bt._outputs()
         pick = sorted(range(len(ws)), key=lambda i: len(ws[i].sources) * ws[i].padded_cells() * ws[i].n_steps)
-        errs = {}
+        errs, fixed = {}, {}
         for i in pick[:accuracy_problems]:
             g32 = grads[i].clone()
             w = ws[i]
+            name = f"problem{mine[i]} ({w.n}^2, {len(w.sources)} shots, {w.n_steps} steps)"
             op64 = WaveOperatorB200(w.domain, w.sources, w.receivers, grad_mode="checkpoint", **w.operator_kwargs())
             _, g64 = op64.misfit_gradient(cs[i].double(), obs[i].double())
-            errs[f"problem{mine[i]} ({w.n}^2, {len(w.sources)} shots, {w.n_steps} steps)"] = float(
-                (g32 - g64).norm() / g64.norm())
+            errs[name] = float((g32 - g64).norm() / g64.norm())
+            fixed[name] = fixed_cotangent_error(op64, WaveOperatorB200(
+                w.domain, w.sources, w.receivers, grad_mode="checkpoint", snapshot=snapshot, checkpoint_every=bt.segment,
+                **w.operator_kwargs()), cs[i], obs[i])
             del op64, g64
         accuracy = {"grad_rel_l2_fp32_vs_fp64": max(errs.values()), "per_problem": errs,
+                    "fixed_cotangent": {"grad_rel_l2_fp32_vs_fp64": max(v["grad"] for v in fixed.values()),
+                                        "per_problem": fixed},
                     "fp32_storage": f"checkpointed, {snapshot} snapshots, segment {bt.segment}",
-                    "fp64_storage": "checkpointed, exact snapshots"}
+                    "fp64_storage": "checkpointed, exact snapshots",
+                    "note": "grad_rel_l2_fp32_vs_fp64: each precision's own misfit gradient (its own residual); "
+                            "fixed_cotangent: the float32 adjoint given the float64 residual, which isolates the "
+                            "adjoint and the snapshots from the float32 rounding of the traces that the residual "
+                            "magnifies by ||traces|| / ||residual|| (resid_ratio)"}
     out = {"value": shots / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "steps": steps, "warmup": warmup,
            "config": {"workload": f"fwi_batch: {len(ws_all)} problems, grids {{256,384,512,768}}^2 + 20-cell sponge, "
                                   f"4-16 Ricker shots, 1500-6000 steps (seed 0), order 4; checkpointed with "
@@ -296,6 +305,25 @@ def measure_batch(dev, world: int, rank: int, n_problems: int = 64, steps: int =
     return out
 
 
+def fixed_cotangent_error(op64, op32, c, obs) -> dict:
+    """The float32 gradient of ``op32`` given the float64 residual of ``op64`` as the trace cotangent,
+    against the float64 gradient: the error of the adjoint sweep and its storage alone. Also the
+    float32 traces' error and the residual's size relative to the traces."""
+    c64 = c.double().clone().requires_grad_(True)
+    tr64 = op64({"c": c64})
+    r64 = (tr64 - obs.double()).detach()
+    (g64,) = torch.autograd.grad((tr64 * r64).sum(), c64)
+    c32 = c.float().clone().requires_grad_(True)
+    tr32 = op32({"c": c32})
+    (g32,) = torch.autograd.grad((tr32 * r64.float()).sum(), c32)
+    out = {"grad": float((g32.double() - g64).norm() / g64.norm()),
+           "traces": float((tr32.detach().double() - tr64.detach()).norm() / tr64.detach().norm()),
+           "resid_ratio": float(tr64.detach().norm() / r64.norm())}
+    del c64, tr64, r64, g64, c32, tr32, g32
+    torch.cuda.empty_cache()
+    return out
+
+
 def measure_checkpointed(dev, w, snapshot: str = "delta16", steps: int = 1, warmup: int = 1,
                          accuracy_shots: int = 4) -> dict:
     """One FWI gradient of workload ``w`` with checkpointed storage and 16-bit snapshots (the large
@@ -341,7 +369,11 @@ def measure_checkpointed(dev, w, snapshot: str = "delta16", steps: int = 1, warm
         del op32
         op64 = WaveOperatorB200(w.domain, w.sources[:na], w.receivers, grad_mode="checkpoint", **w.operator_kwargs())
         _, g64 = op64.misfit_gradient(c.double(), d[:na].double())
+        fixed = fixed_cotangent_error(op64, WaveOperatorB200(
+            w.domain, w.sources[:na], w.receivers, grad_mode="checkpoint", snapshot=snapshot,
+            checkpoint_every=mode[1], **w.operator_kwargs()), c, d[:na])
         accuracy = {"grad_rel_l2_fp32_vs_fp64": float((g32 - g64).norm() / g64.norm()), "shots": na,
+                    "fixed_cotangent": fixed,
                     "fp32_storage": f"checkpointed every {mode[1]} steps, {snapshot} snapshots",
                     "fp64_storage": "checkpointed, exact snapshots"}
         del op64, g32, g64
@@ -452,6 +484,27 @@ def run_pat(args) -> None:
     e2e_ms = statistics.median(e2e)
     h2d = sum(t.numel() * t.element_size() for t in (p0_h, c_h, d_h))
     d2h = gp_h.numel() * gp_h.element_size() + gc_h.numel() * gc_h.element_size() + 8
+    accuracy = None
+    if not args.no_accuracy:
+        # the float32 gradients of instance 0 (this run's storage and snapshots) against a float64 device
+        # run of the same instance (exact checkpoints); tests/test_gpu_parity.py checks that float64
+        # path against the float64 oracle on a 96^3 grid
+        def grads(dtype, snapshot):
+            o = WaveInitialConditionOperatorB200(w.domain, w.sensors, grad_mode="checkpoint", snapshot=snapshot,
+                                                 checkpoint_every=args.checkpoint_every, **w.operator_kwargs())
+            x = p0[:1].to(dtype).clone().requires_grad_(True)
+            cc = c.to(dtype).clone().requires_grad_(True)
+            lo = 0.5 * (o.with_speed(x, cc) - d[:1].to(dtype)).double().square().sum()
+            return torch.autograd.grad(lo, (x, cc))
+        gp32, gc32 = grads(torch.float32, args.snapshot)
+        torch.cuda.empty_cache()
+        gp64, gc64 = grads(torch.float64, "exact")
+        accuracy = {"grad_p0_rel_l2_fp32_vs_fp64": float((gp32.double() - gp64).norm() / gp64.norm()),
+                    "grad_c_rel_l2_fp32_vs_fp64": float((gc32.double() - gc64).norm() / gc64.norm()),
+                    "instances": 1, "fp32_storage": f"checkpointed, {args.snapshot} snapshots",
+                    "fp64_storage": "checkpointed, exact snapshots"}
+        del gp32, gc32, gp64, gc64
+        torch.cuda.empty_cache()
     cpu = None
     if not args.no_cpu_baseline:
         # the float32 C oracle (all host threads) on one instance and a few steps of the same grid,
@@ -500,7 +553,7 @@ def run_pat(args) -> None:
            "cpu_baseline": cpu,
            "e2e": {"value": 4 / (e2e_ms * 1e-3), "unit": "instance-gradients/s", "h2d_bytes_per_step": h2d,
                    "d2h_bytes_per_step": d2h},
-           "clocks": clocks, "gpu_launches": int(launches)}
+           "accuracy": accuracy, "clocks": clocks, "gpu_launches": int(launches)}
     print(json.dumps(out), flush=True)
 
 

@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define NW_ABI_VERSION 4
+#define NW_ABI_VERSION 5
 
 /* scalar type of a computation */
 enum { NW_F32 = 0, NW_F64 = 1 };
@@ -201,7 +201,21 @@ typedef struct nw_storage {
                           before step 0: the auxiliary face fields psi. With snapshots the
                           snapshots also hold the two face fields each segment starts from, and
                           nw_adjoint re-runs segments in these levels */
+  /* Binomial checkpointing (optional; both NULL: segment j's start goes into snapshot slot j and the
+     adjoint decodes slot j for segment j). HOST memory, read during the calls: */
+  const int32_t* snap_slot; /* per segment j: the slot nw_forward encodes its start state into, or -1 */
+  const int32_t* schedule;  /* the adjoint's program: n_schedule triples (op, x, y), executed in order;
+                               NW_SCHED_RESTORE (slot, j): decode slot `slot`, the state at segment j's
+                               start; NW_SCHED_ADVANCE (j0, j1): forward steps from segment j0's start
+                               to j1's, storing nothing; NW_SCHED_TAKE (slot, j): encode the state at
+                               segment j's start (the ring's) into `slot`; NW_SCHED_YOUTURN (j, 0):
+                               recompute segment j's Lap p levels from the state the ring holds at its
+                               start, then run its adjoint steps. The segments are reversed last to
+                               first, each by one YOUTURN. The batched calls ignore both fields */
+  int32_t n_schedule;
+  int32_t reserved;
 } nw_storage;
+enum { NW_SCHED_RESTORE = 1, NW_SCHED_ADVANCE = 2, NW_SCHED_TAKE = 3, NW_SCHED_YOUTURN = 4 };
 
 /* Bytes of one snapshot pool for `n_snap` snapshots of n_shots shots (both levels, and with a PML
  * the two face fields). */

@@ -14,7 +14,7 @@ from pathlib import Path
 import torch
 
 LIB_PATH = Path(__file__).resolve().parent / "libnefiwave.so"
-ABI_VERSION = 4
+ABI_VERSION = 5
 
 NW_F32, NW_F64 = 0, 1
 NW_ABS_NONE, NW_ABS_SPONGE, NW_ABS_CERJAN, NW_ABS_PML = 0, 1, 2, 3
@@ -73,7 +73,8 @@ class Time(C.Structure):
 class Storage(C.Structure):
     _fields_ = [("history", C.c_void_p), ("ring", C.c_void_p), ("snap", C.c_void_p),
                 ("segbuf", C.c_void_p), ("segment", C.c_int32), ("snap_kind", C.c_int32),
-                ("pml_psi", C.c_void_p)]
+                ("pml_psi", C.c_void_p), ("snap_slot", C.c_void_p), ("schedule", C.c_void_p),
+                ("n_schedule", C.c_int32), ("reserved", C.c_int32)]
 
 
 class BatchProblem(C.Structure):

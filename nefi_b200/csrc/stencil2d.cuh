@@ -141,6 +141,9 @@ struct Tiled2 {
   int prev_ready;               // forward: p^{n-1} was written two or more launches back, so it may be
                                 // read before griddepcontrol.wait (0: after it)
   int apply_a;                  // adjoint: A applies (n >= 1); at n = 0 the output is C lambda^0
+  int lap_ready;                // adjoint: Lap p^n was written two or more launches back, so its tiles
+                                // may be copied before griddepcontrol.wait (q^{n+2} always may: the
+                                // adjoint step two launches back wrote it)
   int n_shots, shots_per_cta;
   // forward: point sources, receiver samples of p^n
   const int* __restrict__ src_corner;
@@ -490,6 +493,14 @@ __device__ __forceinline__ void adj2d_body(const KGrid<T>& g, const Tiled2<T>& a
     }
     __syncthreads();  // zeroing completes before any thread writes a cotangent value
   }
+  // the first shots' q^{n+2} core tiles (and Lap p^n, when it was not written by the launch just
+  // before) join the copies issued before the wait; they land in the first commit group
+#pragma unroll
+  for (int i = 0; i < NS - 1; ++i)
+    if (sb + i < se) {
+      issue(pc, a.prev + (long long)(sb + i) * g.field, sq + i * S::QS);
+      if (grad && a.lap_ready) issue(pc, a.lap + (long long)(sb + i) * g.field, sl + i * S::QS);
+    }
   wait_previous_grid();
   allow_next_grid();
   if (grad) issue(pc, a.gacc + (long long)bz * g.field, sg);  // the previous step updated it
@@ -497,8 +508,7 @@ __device__ __forceinline__ void adj2d_body(const KGrid<T>& g, const Tiled2<T>& a
   for (int i = 0; i < NS - 1; ++i) {  // one commit group per shot, empty groups included, so that
     if (sb + i < se) {                // wait_group<NS-1> in the loop means "shot s has landed"
       issue(ph, a.cur + (long long)(sb + i) * g.field, sp + i * S::PS);
-      issue(pc, a.prev + (long long)(sb + i) * g.field, sq + i * S::QS);
-      if (grad) issue(pc, a.lap + (long long)(sb + i) * g.field, sl + i * S::QS);
+      if (grad && !a.lap_ready) issue(pc, a.lap + (long long)(sb + i) * g.field, sl + i * S::QS);
     }
     cp_async_commit();
   }
@@ -720,6 +730,9 @@ __global__ void __launch_bounds__(256, 3) adj2d_batch(const BatchProb<T>* __rest
     t.next = P.work + (long long)(n % 3) * P.level;
     t.apply_a = n >= 1 ? 1 : 0;
     t.lap = n < P.n_steps ? P.segbuf + (long long)(n % segment) * P.level : nullptr;
+    // the first adjoint step of a segment directly follows the recompute step that wrote its Lap p
+    // (a segment ends at a multiple of `segment` or at the batch's last step, problem 0's step count)
+    t.lap_ready = (n + 1) % segment != 0 && n + 1 != probs[0].n_steps;
     if (n % P.substeps != 0) t.gtr = nullptr;  // the descriptor holds the cotangents
     t.j = n / P.substeps;
     st = t;

@@ -666,10 +666,13 @@ int forward_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
   if (pml && !st->pml_psi) return fail(NW_ERR_ARG, "a PML run needs storage.pml_psi");
   const nw::KGrid<T> kg = kgrid<T>(g);
   for (int n = n_begin; n < n_end; ++n) {
-    if (ckpt && n % st->segment == 0) {
+    // a segment start: its snapshot slot (segment j -> slot j, or the binomial schedule's slot, -1: none)
+    const int slot = !(ckpt && n % st->segment == 0) ? -1
+                     : st->snap_slot ? st->snap_slot[n / st->segment] : n / st->segment;
+    if (slot >= 0) {
       T* faces[2];
       if (pml) pml_faces<T>((T*)st->pml_psi, LE, n, faces);
-      int rc = snap_store<T>(g, st, a->n_shots, L.at(n - 1), L.at(n), n / st->segment, s, pml ? faces : nullptr);
+      int rc = snap_store<T>(g, st, a->n_shots, L.at(n - 1), L.at(n), slot, s, pml ? faces : nullptr);
       if (rc) return rc;
     }
     T* lap = st->history ? (T*)st->history + (long long)n * LE : nullptr;
@@ -731,6 +734,9 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
     as.B = (const T*)m->coef_b;
     as.apply_a = n >= 1 ? 1 : 0;
     as.lap = lap;
+    // the history was written by the forward sweep; a segment buffer level by the recompute, whose
+    // last step the segment's first adjoint step (n = segment end - 1) directly follows
+    as.lap_ready = hist || (K > 0 && (n + 1) % K != 0 && n + 1 != N);
     as.gacc = gacc;
     as.n_shots = S;
     as.shots_per_cta = tu.adj.spc;
@@ -786,6 +792,42 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
     int rc = pml ? step_pml(N, nullptr) : (g->ndim == 2 ? step2(N, nullptr) : inject3(N));
     if (rc) return rc;
   }
+  // the binomial schedule's program (host memory), run up to the YOUTURN of each segment as the
+  // adjoint reaches the segment's end
+  const int32_t* prog = ckpt ? st->schedule : nullptr;
+  int pc = 0;
+  auto run_program = [&](int seg) -> int {
+    while (pc < st->n_schedule) {
+      const int op = prog[3 * pc], x = prog[3 * pc + 1], y = prog[3 * pc + 2];
+      ++pc;
+      T* faces[2];
+      switch (op) {
+        case NW_SCHED_RESTORE:
+        case NW_SCHED_TAKE: {
+          if (y < 0 || (long long)y * K >= N || x < 0) return fail(NW_ERR_ARG, "schedule: bad slot or segment");
+          if (pml) pml_faces<T>((T*)st->pml_psi, LE, y * K, faces);
+          const int rc = op == NW_SCHED_RESTORE
+                             ? snap_load<T>(g, st, S, x, L.at(y * K - 1), L.at(y * K), s, pml ? faces : nullptr)
+                             : snap_store<T>(g, st, S, L.at(y * K - 1), L.at(y * K), x, s, pml ? faces : nullptr);
+          if (rc) return rc;
+          break;
+        }
+        case NW_SCHED_ADVANCE:
+          if (x < 0 || y <= x || (long long)y * K >= N) return fail(NW_ERR_ARG, "schedule: bad advance");
+          for (int k = x * K; k < y * K; ++k) {
+            const int rc = forward_step<T>(g, kg, m, a, t, tu, L, k, nullptr, nullptr, s, (T*)st->pml_psi, k > x * K);
+            if (rc) return rc;
+          }
+          break;
+        case NW_SCHED_YOUTURN:
+          if (x != seg) return fail(NW_ERR_ARG, "schedule: segments must be reversed last to first, one YOUTURN each");
+          return NW_OK;
+        default:
+          return fail(NW_ERR_ARG, "schedule: unknown operation");
+      }
+    }
+    return fail(NW_ERR_ARG, "schedule: ended before the YOUTURN of segment " + std::to_string(seg));
+  };
   for (int n = N - 1; n >= n_stop; --n) {
     const T* lap;
     if (hist) {
@@ -797,7 +839,9 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
         seg_n0 = n0;
         T* faces[2];  // with a PML the recompute runs its face fields in storage.pml_psi
         if (pml) pml_faces<T>((T*)st->pml_psi, LE, n0, faces);
-        int rc = snap_load<T>(g, st, S, n0 / K, L.at(n0 - 1), L.at(n0), s, pml ? faces : nullptr);
+        // the ring to the segment's start: the schedule's program, or the segment's own snapshot
+        int rc = prog ? run_program(n0 / K)
+                      : snap_load<T>(g, st, S, n0 / K, L.at(n0 - 1), L.at(n0), s, pml ? faces : nullptr);
         if (rc) return rc;
         for (int k = n0; k < n1; ++k) {
           rc = forward_step<T>(g, kg, m, a, t, tu, L, k, nullptr, (T*)st->segbuf + (long long)(k - n0) * LE, s,

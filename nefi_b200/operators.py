@@ -44,7 +44,7 @@ from .geometry import (
     pml_profile,
     ricker,
 )
-from .plan import DevicePlan, ghost_view, plan_storage, to_ghost
+from .plan import DevicePlan, cached_schedule, ghost_view, plan_storage, to_ghost
 
 log = logging.getLogger("nefi_b200")
 
@@ -62,7 +62,7 @@ class _LeapfrogB200(Operator):
                  absorbing: str = "pml", absorb_width: float | None = None, absorb_R: float = 1e-3,
                  cerjan_gamma: float = 0.3, courant: float = 0.9, grad_mode: str = "checkpoint",
                  checkpoint_every: int | None = None, snapshot: str = "exact",
-                 memory_budget: int | None = None) -> None:
+                 memory_budget: int | None = None, checkpoint_slots: int | None = None) -> None:
         super().__init__()
         if absorbing not in ABSORBING:
             raise ConfigError(f"absorbing must be one of {ABSORBING}, got {absorbing!r}")
@@ -96,6 +96,9 @@ class _LeapfrogB200(Operator):
         self.checkpoint_every = checkpoint_every
         self.snapshot = snapshot
         self.memory_budget = memory_budget
+        # snapshot slots of a checkpointed gradient (None: as the memory budget allows); fewer than the
+        # segments selects binomial checkpointing
+        self.checkpoint_slots = checkpoint_slots
         self.grid = PaddedGrid(domain, self.absorb_width)
         ta = TimeAxis(self.n_t, self.dt_obs, self.c_max, self.grid.spacing, self.order, self.courant)
         self.substeps, self.dt, self.n_steps = ta.substeps, ta.dt, ta.n_steps
@@ -112,7 +115,7 @@ class _LeapfrogB200(Operator):
                 "absorb_R": self.absorb_R, "cerjan_gamma": self.cerjan_gamma,
                 "courant": self.courant, "grad_mode": self.grad_mode,
                 "checkpoint_every": self.checkpoint_every, "snapshot": self.snapshot,
-                "memory_budget": self.memory_budget}
+                "memory_budget": self.memory_budget, "checkpoint_slots": self.checkpoint_slots}
 
     @property
     def times(self) -> torch.Tensor:
@@ -193,6 +196,14 @@ class _Run:
             k = int(mode[1])
             kind = _lib.SNAP_KINDS[snapshot]
             n_snap = -(-n_steps // k) if n_steps > 0 else 1
+            self.schedule = None
+            if len(mode) > 2 and mode[2] < n_snap:  # binomial checkpointing over mode[2] slots
+                sweep_slot, program = cached_schedule(n_snap, int(mode[2]))
+                self.schedule = (sweep_slot, program)  # host arrays the library reads during the calls
+                self.storage.snap_slot = sweep_slot.data_ptr()
+                self.storage.schedule = program.data_ptr()
+                self.storage.n_schedule = program.numel() // 3
+                n_snap = int(mode[2])
             nbytes = plan.snapshot_bytes(n_shots, n_snap, kind)
             self.snap = torch.empty(nbytes, dtype=torch.uint8, device=plan.device)
             self.segbuf = plan.empty_levels(k, n_shots)
@@ -258,7 +269,7 @@ class _FWIFunction(torch.autograd.Function):
         acq = plan.acquisition(n_shots, shot0)
         needs_grad = ctx.needs_input_grad[0]
         mode = (plan_storage(plan, n_shots, op.n_steps, op.grad_mode, op.checkpoint_every,
-                             op.snapshot, op._budget(c.device)) if needs_grad else ("ring", None))
+                             op.snapshot, op._budget(c.device), op.checkpoint_slots) if needs_grad else ("ring", None))
         run = _Run(plan, n_shots, op.n_steps, mode, op.snapshot)
         traces = torch.empty(n_shots, plan.n_rec, op.n_t, device=c.device, dtype=c.dtype)
         _forward_sweep(plan, medium, acq, run, 0, op.n_steps, traces, stream)
@@ -309,12 +320,12 @@ class WaveOperatorB200(_LeapfrogB200):
                  absorb_R: float = 1e-3, cerjan_gamma: float = 0.3, courant: float = 0.9,
                  grad_mode: str = "checkpoint", checkpoint_every: int | None = None,
                  source_batch: int | None = None, snapshot: str = "exact",
-                 memory_budget: int | None = None) -> None:
+                 memory_budget: int | None = None, checkpoint_slots: int | None = None) -> None:
         super().__init__(domain, receivers, n_t=n_t, dt_obs=dt_obs, c_max=c_max, order=order,
                          absorbing=absorbing, absorb_width=absorb_width, absorb_R=absorb_R,
                          cerjan_gamma=cerjan_gamma, courant=courant, grad_mode=grad_mode,
                          checkpoint_every=checkpoint_every, snapshot=snapshot,
-                         memory_budget=memory_budget)
+                         memory_budget=memory_budget, checkpoint_slots=checkpoint_slots)
         self.primary = field
         self.homogeneity = None
         self.sources = as_points(sources, len(domain.shape), "sources")
@@ -394,7 +405,7 @@ class WaveOperatorB200(_LeapfrogB200):
         chunk = self.source_batch or n
         budget = self._budget(c.device)
         return [plan_storage(plan, min(n, s0 + chunk) - s0, self.n_steps, self.grad_mode, self.checkpoint_every,
-                             self.snapshot, budget) for s0 in range(0, n, chunk)]
+                             self.snapshot, budget, self.checkpoint_slots) for s0 in range(0, n, chunk)]
 
     def _gradient(self, c, observed, events, misfit, mask, modes):
         """The device work of ``misfit_gradient`` (validated inputs, storage decided): enqueues only,
@@ -533,7 +544,7 @@ class _PATFunction(torch.autograd.Function):
         need_p0, need_c = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
         needs_grad = need_p0 or need_c
         mode = (plan_storage(plan, S, op.n_steps, op.grad_mode, op.checkpoint_every, op.snapshot,
-                             op._budget(p0.device)) if needs_grad else ("ring", None))
+                             op._budget(p0.device), op.checkpoint_slots) if needs_grad else ("ring", None))
         run = _Run(plan, S, op.n_steps, mode, op.snapshot)
         _lib.check(lib.nw_initial_state(C.byref(plan.g), plan.n_abs, C.byref(medium), S, p0f.data_ptr(),
                                         run.level(-1).data_ptr(), run.level(0).data_ptr(), stream))
@@ -636,7 +647,8 @@ class WaveInitialConditionOperatorB200(_LeapfrogB200):
                  field: str = "p0", order: int = 4, absorbing: str = "pml",
                  absorb_width: float | None = None, absorb_R: float = 1e-3, cerjan_gamma: float = 0.3,
                  courant: float = 0.9, grad_mode: str = "checkpoint", checkpoint_every: int | None = None,
-                 snapshot: str = "exact", memory_budget: int | None = None) -> None:
+                 snapshot: str = "exact", memory_budget: int | None = None,
+                 checkpoint_slots: int | None = None) -> None:
         c_t = torch.as_tensor(c, dtype=torch.float64)
         if c_t.ndim not in (0, len(domain.shape)):
             raise ShapeError("c must be a scalar or a map on the domain grid")
@@ -647,7 +659,7 @@ class WaveInitialConditionOperatorB200(_LeapfrogB200):
                          absorbing=absorbing, absorb_width=absorb_width, absorb_R=absorb_R,
                          cerjan_gamma=cerjan_gamma, courant=courant, grad_mode=grad_mode,
                          checkpoint_every=checkpoint_every, snapshot=snapshot,
-                         memory_budget=memory_budget)
+                         memory_budget=memory_budget, checkpoint_slots=checkpoint_slots)
         self.primary = field
         self.homogeneity = 1.0
         self.c_known = c_t

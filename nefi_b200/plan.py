@@ -9,6 +9,7 @@ forward or adjoint sweep does no host-side geometry work.
 from __future__ import annotations
 
 import ctypes as C
+import functools
 import math
 
 import torch
@@ -290,32 +291,217 @@ class DevicePlan:
         return int(_lib.load().nw_snapshot_bytes(C.byref(self.g), n_shots, n_snap, kind))
 
 
-def plan_storage(plan: DevicePlan, n_shots: int, n_steps: int, grad_mode: str,
-                 checkpoint_every: int | None, snapshot: str, budget: int | None):
-    """Choose the wavefield storage of a gradient run: ``("history",)`` or ``("checkpoint", K)``.
+# ------------------------------------------------------------------------------------------------
+# Binomial checkpointing over segments (the revolve strategy of Griewank and Walther, ACM TOMS 26
+# (2000), "Algorithm 799: revolve", restated here for segments of K leapfrog steps). Reversing a
+# segment is the recompute of its K Laplacian levels from its start state followed by its K adjoint
+# steps; the start states live in snapshot slots. With fewer slots than segments, the adjoint re-runs
+# parts of the forward sweep ("advances") to regenerate start states, taking new snapshots on the way.
+# ------------------------------------------------------------------------------------------------
+RESTORE, ADVANCE, TAKE, YOUTURN = 1, 2, 3, 4
 
-    ``grad_mode="autograd"`` keeps every level when it fits ``budget`` bytes and otherwise falls
-    back to checkpointing; ``"checkpoint"`` uses segments of ``checkpoint_every`` steps (default
-    ``ceil(sqrt(n_steps))``, the reference's choice) or the shortest segment whose pool fits the
-    budget.
+
+def _beta(c: int, r: int) -> int:
+    """Number of segments c slots can reverse with r advances per segment at most: C(c + r, c)."""
+    return math.comb(c + r, c) if c >= 0 and r >= 0 else 0
+
+
+def _repetitions(l: int, c: int) -> int:
+    r = 0
+    while _beta(c, r) < l:
+        r += 1
+    return r
+
+
+def binomial_advances(l: int, c: int) -> int:
+    """Fewest segment advances that reverse ``l`` segments with ``c`` slots, the first segment's start
+    state in one of them: ``r l - C(c + r, c + 1)`` with ``r`` the least integer with
+    ``C(c + r, c) >= l``. The first forward sweep is part of the count (it advances ``l - 1``)."""
+    if l <= 1:
+        return 0
+    r = _repetitions(l, c)
+    return r * l - _beta(c + 1, r - 1)
+
+
+def binomial_schedule(n_seg: int, n_slots: int):
+    """The binomial schedule of ``n_seg`` segments over ``n_slots`` snapshot slots.
+
+    Returns ``(sweep_slot, actions)``: ``sweep_slot[j]`` is the slot the forward sweep encodes segment
+    ``j``'s start state into (``-1``: none), and ``actions`` the adjoint's program, triples
+    ``(RESTORE, slot, j)`` (decode a slot: the state at segment ``j``'s start), ``(ADVANCE, j0, j1)``
+    (forward steps from segment ``j0``'s start to ``j1``'s), ``(TAKE, slot, j)`` (encode the state at
+    segment ``j``'s start), ``(YOUTURN, j, 0)`` (recompute segment ``j``'s Laplacian levels from the
+    state at its start, then its adjoint steps). Segments are reversed last to first.
+
+    The recursion is revolve's: a subproblem of ``l`` segments whose first start state is in a slot,
+    with ``c`` slots in all, puts its next snapshot ``m`` segments ahead, ``m`` the largest value of
+    ``[max(l - C(c-1+r, c-1), C(c-2+r, c)), min(l - C(c-2+r, c-1), C(c-1+r, c))]`` (``r`` its
+    repetition number), a range of optimal splits; with one slot it re-advances from its start for
+    every segment. The first descent's snapshots are taken by the forward sweep, which then runs on to
+    the last step for the traces; the first reversal therefore starts from a decoded snapshot, and if
+    the descent ended inside a one-slot subproblem, the segments it advanced there are advanced again
+    (``sweep_readvance``)."""
+    if n_slots < 1 or n_seg < 1:
+        raise ConfigError("binomial checkpointing needs at least one segment and one snapshot slot")
+    sweep_slot = [-1] * n_seg
+    actions: list[tuple[int, int, int]] = []
+    free = list(range(n_slots - 1, 0, -1))  # slot 0 holds segment 0's start
+    slot_of = {0: 0}
+    st = {"cur": 0, "sweep": True}  # the segment start the ring holds (-1: none), and the sweep phase
+
+    def reach(j):  # the ring to segment j's start: decode the nearest snapshot at or before j, advance
+        if st["cur"] == j:
+            return
+        a = max(k for k in slot_of if k <= j)
+        if st["cur"] < a or st["cur"] > j:
+            actions.append((RESTORE, slot_of[a], a))
+            st["cur"] = a
+        if j > st["cur"]:
+            actions.append((ADVANCE, st["cur"], j))
+            st["cur"] = j
+
+    def advance(a, b):
+        if st["sweep"]:
+            st["cur"] = b
+        else:
+            reach(a)
+            reach(b)
+
+    def take(j):
+        k = free.pop()
+        slot_of[j] = k
+        if st["sweep"]:
+            sweep_slot[j] = k
+        else:
+            reach(j)
+            actions.append((TAKE, k, j))
+
+    def youturn(j):
+        if st["sweep"]:  # the sweep ran on to the end: the ring no longer holds any segment start
+            st["sweep"] = False
+            st["cur"] = -1
+        reach(j)
+        actions.append((YOUTURN, j, 0))
+        st["cur"] = -1  # the recompute leaves the ring at the segment's end, which no one reverses next
+
+    def reverse(a, b, c):
+        l = b - a
+        if l == 1:
+            youturn(a)
+            return
+        if c == 1:
+            for j in range(b - 1, a - 1, -1):
+                advance(a, j)
+                youturn(j)
+            return
+        r = _repetitions(l, c)
+        lo = max(l - _beta(c - 1, r), _beta(c, r - 2), 1)
+        hi = min(l - _beta(c - 1, r - 1), _beta(c, r - 1), l - 1)
+        m = a + max(lo, hi)
+        advance(a, m)
+        take(m)
+        reverse(m, b, c - 1)
+        free.append(slot_of.pop(m))
+        reverse(a, m, c)
+
+    sweep_slot[0] = 0
+    reverse(0, n_seg, n_slots)
+    return sweep_slot, actions
+
+
+def sweep_readvance(n_seg: int, n_slots: int) -> int:
+    """Segments the first reversal re-advances because the forward sweep ran past its start: the length
+    minus one of the one-slot subproblem the first descent ends in (0 when it ends on a snapshot)."""
+    a, l, c = 0, n_seg, n_slots
+    while l > 1 and c > 1:
+        r = _repetitions(l, c)
+        lo = max(l - _beta(c - 1, r), _beta(c, r - 2), 1)
+        hi = min(l - _beta(c - 1, r - 1), _beta(c, r - 1), l - 1)
+        m = max(lo, hi)
+        a, l, c = a + m, l - m, c - 1
+    return l - 1 if l > 1 else 0
+
+
+def schedule_advances(n_seg: int, sweep_slot, actions) -> int:
+    """Segment advances of a schedule: the forward sweep's ``n_seg - 1`` plus the adjoint's."""
+    return n_seg - 1 + sum(b - a for op, a, b in actions if op == ADVANCE)
+
+
+@functools.lru_cache(maxsize=64)
+def cached_schedule(n_seg: int, n_slots: int):
+    """``binomial_schedule`` as int32 triples for the library: ``(sweep_slot, program)``."""
+    sweep_slot, actions = binomial_schedule(n_seg, n_slots)
+    return (torch.tensor(sweep_slot, dtype=torch.int32),
+            torch.tensor([v for a in actions for v in a] or [0], dtype=torch.int32))
+
+
+def binomial_steps(n_steps: int, k: int, n_slots: int) -> int:
+    """Forward steps of a binomial-checkpointed gradient: the sweep, each segment's recompute, and the
+    adjoint's advances (``k`` steps each; the last segment may be shorter, which this ignores)."""
+    n_seg = -(-n_steps // k)
+    if n_slots >= n_seg:
+        return 2 * n_steps
+    extra = binomial_advances(n_seg, n_slots) - (n_seg - 1) + sweep_readvance(n_seg, n_slots)
+    return 2 * n_steps + k * extra
+
+
+def plan_storage(plan: DevicePlan, n_shots: int, n_steps: int, grad_mode: str,
+                 checkpoint_every: int | None, snapshot: str, budget: int | None,
+                 checkpoint_slots: int | None = None):
+    """Choose the wavefield storage of a gradient run: ``("history",)``, ``("checkpoint", K)``
+    (segments of ``K`` steps, a snapshot per segment start) or ``("checkpoint", K, slots)`` (binomial
+    checkpointing of the segments over ``slots`` snapshot slots, fewer than the segments).
+
+    ``grad_mode="autograd"`` keeps every level when it fits ``budget`` bytes and otherwise
+    checkpoints; ``"checkpoint"`` uses segments of ``checkpoint_every`` steps (default
+    ``ceil(sqrt(n_steps))``, the reference's choice) or the shortest segment whose storage fits the
+    budget. When no segment length lets a snapshot per segment fit, the segment length and slot count
+    that fit and need the fewest forward steps are chosen (binomial checkpointing, whose extra forward
+    steps grow as the slots shrink). ``checkpoint_slots`` fixes the slot count.
     """
     lvl = plan.level_bytes(n_shots)
     hist = (n_steps + 3) * lvl  # n_steps Lap p levels and the pressure ring
-    if grad_mode == "autograd" and (budget is None or hist <= budget):
+    if grad_mode == "autograd" and (budget is None or hist <= budget) and not checkpoint_slots:
         return ("history", None)
     kind = _lib.SNAP_KINDS[snapshot]
     extra = 4 * lvl if plan.pml is not None else 0  # the PML's face fields
+    snap1 = plan.snapshot_bytes(n_shots, 1, kind)
+
+    def n_seg(k_):
+        return -(-n_steps // k_)
+
+    def cost(k_, slots=None):
+        return snap1 * (n_seg(k_) if slots is None else slots) + (k_ + 3) * lvl + extra
+
+    if checkpoint_slots:
+        k = max(1, int(checkpoint_every)) if checkpoint_every else max(1, int(math.ceil(math.sqrt(max(1, n_steps)))))
+        slots = max(1, int(checkpoint_slots))
+        return ("checkpoint", k) if slots >= n_seg(k) else ("checkpoint", k, slots)
     if checkpoint_every:
-        return ("checkpoint", max(1, int(checkpoint_every)))
-    k = max(1, int(math.ceil(math.sqrt(max(1, n_steps)))))
-    if budget is not None:
-        def cost(k_):
-            return plan.snapshot_bytes(n_shots, -(-n_steps // k_), kind) + (k_ + 3) * lvl + extra
+        k = max(1, int(checkpoint_every))
+        if budget is None or cost(k) <= budget:
+            return ("checkpoint", k)
+        ks = [k]
+    else:
+        k = max(1, int(math.ceil(math.sqrt(max(1, n_steps)))))
+        if budget is None or cost(k) <= budget:
+            return ("checkpoint", k)
         best = min(range(1, n_steps + 1), key=cost) if n_steps < 20000 else k
-        if cost(k) > budget:
-            k = best
-        if cost(k) > budget:
-            raise ConfigError(
-                f"checkpointed gradient needs {cost(k) / 2**30:.1f} GiB, above the budget "
-                f"{budget / 2**30:.1f} GiB; lower source_batch or use fp16/bf16 snapshots")
-    return ("checkpoint", k)
+        if cost(best) <= budget:
+            return ("checkpoint", best)
+        ks = range(1, min(n_steps, 4096) + 1)
+    # binomial checkpointing: for each segment length, the slots that fit; keep the fewest steps
+    choice = None
+    for k_ in ks:
+        slots = (budget - (k_ + 3) * lvl - extra) // snap1 if budget is not None else 0
+        if slots < 1:
+            continue
+        steps = binomial_steps(n_steps, k_, int(min(slots, n_seg(k_))))
+        if choice is None or steps < choice[0]:
+            choice = (steps, k_, int(min(slots, n_seg(k_))))
+    if choice is None:
+        raise ConfigError(
+            f"checkpointed gradient needs at least {cost(1, 1) / 2**30:.1f} GiB, above the budget "
+            f"{budget / 2**30:.1f} GiB; lower source_batch or use 16-bit snapshots")
+    _, k, slots = choice
+    return ("checkpoint", k) if slots >= n_seg(k) else ("checkpoint", k, slots)

@@ -165,7 +165,7 @@ def test_fused_misfit_batch_equals_each_problem_alone_and_replays(cuda_device):
     l0 = [float(x) for x in l0]
     g0 = [g.clone() for g in g0]
     for i, op in enumerate(ops):
-        op.snapshot = "fixed16"
+        op.snapshot = bt.snapshot
         op.tuning = tuning
         op._plans.clear()
         l1, g1 = op.misfit_gradient(cs[i], obs[i], misfit=TraceMisfit(1e-3, 40.0, 0.3, True), mask=masks[i])

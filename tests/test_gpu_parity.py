@@ -113,6 +113,31 @@ def test_checkpointed_gradient_is_identical_to_full_history(name, dtype, cuda_de
         assert np.array_equal(got[0], ref[0]) and np.array_equal(got[1], ref[1])
 
 
+@pytest.mark.parametrize("slots", [1, 2, 3])
+@pytest.mark.parametrize("name", ["fwi_o4_sponge", "fwi_o4_pml", "pat3d_o2_sponge"])
+def test_binomial_checkpointing_is_identical_to_full_history(name, slots, cuda_device):
+    """Fewer snapshot slots than segments: the adjoint follows the binomial schedule (restores, advances,
+    new snapshots) and, with exact snapshots, gives bitwise the full-history traces and gradient."""
+    case = load_golden(name)
+    if case["kind"] == "fwi":
+        ref = run_fwi(case, torch.float32, cuda_device)
+        got = run_fwi(case, torch.float32, cuda_device, grad_mode="checkpoint", checkpoint_every=3,
+                      checkpoint_slots=slots)
+    else:
+        ref = run_pat(case, torch.float32, cuda_device)
+        got = run_pat(case, torch.float32, cuda_device, grad_mode="checkpoint", checkpoint_every=3,
+                      checkpoint_slots=slots)
+    assert np.array_equal(got[0], ref[0]) and np.array_equal(got[1], ref[1])
+
+
+def test_binomial_checkpointing_with_16_bit_snapshots(cuda_device):
+    case = load_golden("cfg1_128_o4_sponge")
+    tr, gc = run_fwi(case, torch.float32, cuda_device, grad_mode="checkpoint", checkpoint_every=40,
+                     checkpoint_slots=6, snapshot="delta16")
+    assert rel_l2(tr, case["traces_f64"]) < 1e-5
+    assert rel_l2(gc, case["grad_c_f64"]) < 1e-4
+
+
 @pytest.mark.parametrize("snapshot,tol", [("delta16", 1e-4), ("fixed16", 3e-4), ("fp16", 3e-3), ("bf16", 2.5e-2)])
 def test_reduced_precision_snapshots_error_is_bounded(snapshot, tol, cuda_device):
     """16-bit snapshots perturb only the recomputed forward field, so the traces stay exact and the
@@ -509,3 +534,27 @@ def test_random_geometries_match_the_oracle(seed, dtype, tt, tg, cuda_device):
     print(f"seed {seed} {absorbing} {dtype}: traces {e_tr:.2e} (bound {tt:.1e}), gradient {e_gc:.2e} (bound {tg:.1e})")
     assert e_tr < tt, (absorbing, kw)
     assert e_gc < tg, (absorbing, kw)
+
+
+def test_pat_float64_matches_the_oracle_on_a_96_cube(cuda_device):
+    """The float64 3-D photoacoustic path that the large 3-D configuration's accuracy figure is measured
+    against, checked against the float64 oracle at 96^3 (10-cell sponge, order 2, two instances, a
+    sensor plane on one face, 120 steps): traces, and the gradients w.r.t. p0 and c."""
+    import oracle
+    from nefi_b200.workloads import pat_volume
+
+    w = pat_volume(n=96, batch=2, n_steps=120, seed=1, n_sensors=24)
+    kw = {**w.operator_kwargs(), "absorb_width": 10 * w.h}
+    op = WaveInitialConditionOperatorB200(w.domain, w.sensors, grad_mode="checkpoint", **kw)
+    p0 = torch.tensor(w.p0, dtype=torch.float64, device=cuda_device, requires_grad=True)
+    c = torch.tensor(w.c, dtype=torch.float64, device=cuda_device, requires_grad=True)
+    tr = op.with_speed(p0, c)
+    g = np.random.default_rng(3).standard_normal(tuple(tr.shape))
+    gp, gc = torch.autograd.grad((tr * torch.tensor(g, device=cuda_device)).sum(), (p0, c))
+    okw = {k: v for k, v in kw.items() if k != "c"}
+    orc = oracle.OracleWave(w.domain.shape, w.domain.extent, w.sensors, c_max=float(w.c.max()), **okw)
+    oracle.set_threads(max(1, __import__("os").cpu_count() or 1))
+    otr, ogp, ogc = orc.pat(w.p0, w.c, g, dtype=np.float64)
+    assert rel_l2(tr.detach().cpu().numpy(), otr) < 1e-11
+    assert rel_l2(gp.cpu().numpy(), ogp) < 1e-10
+    assert rel_l2(gc.cpu().numpy(), ogc) < 1e-10
