@@ -449,22 +449,13 @@ void pml_medium(const nw_medium* m, nw::PmlStep<T>& st) {
   st.cz1 = m->pml_core[3];
 }
 
-// The PML cells outside the tiled box (all cells when there is none): 16-byte chunks of a row, a
-// thread per chunk, a CTA of 128 threads per 128 chunks and group of shots; the shot groups are as
-// small as keeps about four CTAs per SM busy, since a CTA reuses its cells' coefficients over its
-// group.
 template <typename T, bool ADJ>
 int launch_pml(const nw_grid* g, const nw::KGrid<T>& kg, const nw::PmlStep<T>& st, int n_shots, cudaStream_t s) {
   const long long cells = (long long)g->n[0] * g->n[1] - (long long)(st.kx1 - st.kx0) * (st.kz1 - st.kz0);
   if (cells <= 0) return NW_OK;
-  nw::PmlChunks<T> ck = nw::pml_chunks<T>(g->n[0], g->n[1], st.kx0, st.kx1, st.kz0, st.kz1, 1);
-  const int per_group = (ck.n_all + 127) / 128;
-  const int groups = std::max(1, std::min(n_shots, (4 * 148 + per_group - 1) / per_group));
-  ck.spc = (n_shots + groups - 1) / groups;
-  const dim3 grid((unsigned)per_group, (unsigned)((n_shots + ck.spc - 1) / ck.spc));
-  if (g->radius == 1)
-    return launch_pdl_b(nw::pml2d_chunk_step<T, 1, ADJ>, grid, dim3(128), 0, s, kg, st, ck, n_shots);
-  return launch_pdl_b(nw::pml2d_chunk_step<T, 2, ADJ>, grid, dim3(128), 0, s, kg, st, ck, n_shots);
+  const dim3 grid((unsigned)((cells + 255) / 256), n_shots);
+  if (g->radius == 1) return launch_pdl(nw::pml2d_step<T, 1, ADJ>, grid, 0, s, kg, st);
+  return launch_pdl(nw::pml2d_step<T, 2, ADJ>, grid, 0, s, kg, st);
 }
 
 // A second stream of the calling thread on the current device, with a fork and a join event: a PML

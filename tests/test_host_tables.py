@@ -490,48 +490,3 @@ def test_padding_and_nearest_cells_match_the_oracle(shape, extent):
     span = [op.grid.padded_shape[ax] * op.grid.spacing[ax] for ax in range(d)]
     pts = np.stack([rng.uniform(lo[ax] - 0.1, lo[ax] + span[ax] + 0.1, 500) for ax in range(d)], 1)
     assert np.array_equal(op.grid.nearest_index(torch.tensor(pts)).numpy(), orc.nearest_cells(pts))
-
-
-def _pml_chunk_cells(n0, n1, kx0, kx1, kz0, kz1, cw):
-    """Python restatement of nw::pml_chunks / the chunk -> cell map of pml2d_chunk_step: the cells
-    each thread writes (in-grid, outside the box) and the element offsets it reads along z."""
-    nch = -(-n1 // cw)
-    ka, kb = kz0 // cw, kz1 // cw
-    n_top, n_mid = kx0 * nch, (kx1 - kx0) * (ka + nch - kb)
-    n_all = n_top + n_mid + (n0 - kx1) * nch
-    owned = []
-    for t in range(n_all):
-        if t < n_top:
-            x, zc = t // nch, (t % nch) * cw
-        elif t < n_top + n_mid:
-            u, w = t - n_top, ka + nch - kb
-            q, r = divmod(u, w)
-            x, zc = kx0 + q, (r if r < ka else kb + (r - ka)) * cw
-        else:
-            u = t - n_top - n_mid
-            x, zc = kx1 + u // nch, (u % nch) * cw
-        for v in range(cw):
-            z = zc + v
-            if z < n1 and (x < kx0 or x >= kx1 or z < kz0 or z >= kz1):
-                owned.append((x, z))
-    return owned
-
-
-@pytest.mark.parametrize("seed", range(12))
-def test_pml_chunks_cover_the_layer_once(seed):
-    """Every cell outside the tiled box is written by exactly one thread of the chunked PML kernel,
-    and no cell inside the box is, for chunk-aligned box starts and arbitrary box ends."""
-    rng = np.random.default_rng(seed)
-    cw = int(rng.choice([2, 4]))
-    n0, n1 = int(rng.integers(8, 70)), int(rng.integers(8, 90))
-    if seed % 3 == 0:
-        kx0 = kx1 = kz0 = kz1 = 0  # no box: every cell
-    else:
-        kx0 = int(rng.integers(1, n0 // 2))
-        kx1 = int(rng.integers(kx0, n0))
-        kz0 = cw * int(rng.integers(0, max(1, n1 // (2 * cw))))
-        kz1 = int(rng.integers(kz0, n1 + 1))
-    owned = _pml_chunk_cells(n0, n1, kx0, kx1, kz0, kz1, cw)
-    assert len(owned) == len(set(owned))
-    expect = {(x, z) for x in range(n0) for z in range(n1) if not (kx0 <= x < kx1 and kz0 <= z < kz1)}
-    assert set(owned) == expect
