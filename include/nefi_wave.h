@@ -89,7 +89,12 @@ typedef struct nw_tuning {
   int32_t adj_vz;            /* the same for the adjoint steps; adj_shots_per_cta shots share */
   int32_t adj_rx;            /*   one gradient accumulator field */
   int32_t adj_shots_per_cta;
-  int32_t reserved[2];
+  int32_t depth;             /* forward steps per launch: 1 (0 = 1) or 2 (2-D without a PML, and a
+                                ring of four levels, nw_storage.ring_levels = 4); two steps per launch
+                                give bitwise the fields of one. With depth 2 the forward tile of
+                                nw_tile_shape is the core a launch stores: (8*rx - 2*radius) rows by
+                                (32*vz - 2*(16 / element size)) columns */
+  int32_t reserved;
 } nw_tuning;
 
 /*
@@ -170,8 +175,9 @@ typedef struct nw_time {
 } nw_time;
 
 /*
- * Wavefield storage. The pressure always advances through `ring`: three levels, level n at
- * ring + ((n+1) % 3) * level_stride (level_stride = n_shots * field_elems). What the gradient
+ * Wavefield storage. The pressure always advances through `ring`: three levels (four with
+ * ring_levels = 4), level n at ring + ((n+1) % levels) * level_stride (level_stride = n_shots *
+ * field_elems). What the gradient
  * needs of the forward run is Lap p^n for n = 0..N-1, the factor of the velocity term
  * mu^{n+1} * Lap p^n; it is kept in one of two ways.
  *  history != NULL: the forward step n stores Lap p^n at history + n*level_stride (N levels,
@@ -213,7 +219,8 @@ typedef struct nw_storage {
                                start, then run its adjoint steps. The segments are reversed last to
                                first, each by one YOUTURN. The batched calls ignore both fields */
   int32_t n_schedule;
-  int32_t reserved;
+  int32_t ring_levels;      /* levels in `ring`: 3 (0 means 3) or 4; level n at ring + ((n+1) % levels) *
+                               level_stride. Four let the forward advance two steps per launch */
 } nw_storage;
 enum { NW_SCHED_RESTORE = 1, NW_SCHED_ADVANCE = 2, NW_SCHED_TAKE = 3, NW_SCHED_YOUTURN = 4 };
 

@@ -41,7 +41,7 @@ class Grid(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("vz", C.c_int32), ("rx", C.c_int32), ("shots_per_cta", C.c_int32),
                 ("adj_vz", C.c_int32), ("adj_rx", C.c_int32), ("adj_shots_per_cta", C.c_int32),
-                ("reserved", C.c_int32 * 2)]
+                ("depth", C.c_int32), ("reserved", C.c_int32)]
 
 
 class Acquisition(C.Structure):
@@ -74,7 +74,7 @@ class Storage(C.Structure):
     _fields_ = [("history", C.c_void_p), ("ring", C.c_void_p), ("snap", C.c_void_p),
                 ("segbuf", C.c_void_p), ("segment", C.c_int32), ("snap_kind", C.c_int32),
                 ("pml_psi", C.c_void_p), ("snap_slot", C.c_void_p), ("schedule", C.c_void_p),
-                ("n_schedule", C.c_int32), ("reserved", C.c_int32)]
+                ("n_schedule", C.c_int32), ("ring_levels", C.c_int32)]
 
 
 class BatchProblem(C.Structure):

@@ -52,7 +52,7 @@ class BatchedFWI:
         n_max = max(op.n_steps for op in ops)
         self.segment = int(segment) if segment else max(1, int(math.ceil(math.sqrt(max(1, n_max)))))
         self.snapshot = snapshot
-        self.tuning = tuple(tuning) if tuning else (0, 0, 0, 0, 0, 0)
+        self.tuning = tuple(tuning)[:6] if tuning else (0, 0, 0, 0, 0, 0)  # one step per launch
         if misfits is not None and len(misfits) != len(ops):
             raise ConfigError("misfits: one per operator")
         if masks is not None and (misfits is None or len(masks) != len(ops)):

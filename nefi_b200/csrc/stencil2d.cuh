@@ -164,6 +164,13 @@ struct Tiled2 {
   // and only cells below (x_end, z_end) are stored; the whole grid is (0, 0, n0, n1), a sub-box is the
   // PML's interior
   int tx_off, tz_off, x_end, z_end;
+  // two steps per launch (fwd2t): the second step's outputs p^{n+2} and Lap p^{n+1}, and its receiver
+  // samples of level n+1 (traces1 non-null on record steps, sample j1); two = 0: the first step only
+  int two;
+  T* __restrict__ next2;
+  T* __restrict__ lap_out1;
+  T* __restrict__ traces1;
+  int j1;
 };
 
 template <typename T, int VZ, int RX, int R>
@@ -205,7 +212,8 @@ __device__ __forceinline__ CopyPlan<Tile2Shape<T, VZ, RX, R>::NCH> plan_halo(con
     const int x = x0 - R + row;
     const int z = z0 - S::HL + ch * S::EPC;
     p.soff[i] = row * S::SW + ch * S::EPC;
-    p.goff[i] = (c < S::HR * CPR && x < g.n0 + R && z < (int)g.s0) ? (int)(g.origin + (long long)x * g.s0 + z) : -1;
+    p.goff[i] = (c < S::HR * CPR && x >= -R && x < g.n0 + R && z < (int)g.s0)
+                    ? (int)(g.origin + (long long)x * g.s0 + z) : -1;
   }
   return p;
 }
@@ -622,6 +630,267 @@ __device__ __forceinline__ void adj2d_body(const KGrid<T>& g, const Tiled2<T>& a
       store_row<T, VZ>(gp + (long long)k * ld, old, zc, a.z_end);
     }
   }
+}
+
+// ------------------------------------------------------------------------------------------
+// Two forward steps per launch (temporal blocking): p^{n+1} and p^{n+2} of every shot of a group over
+// one core tile of TX - 2R rows by TZ - 2 HL columns. The thread layout is fwd2d's over the extended
+// tile E (TX x TZ: the core with R rows and HL columns around it), whose first step p^{n+1} goes to a
+// shared tile; the second step reads it there, with p^n from the staged halo tile. Each cell takes
+// fwd2d's arithmetic in the same order, so the fields, traces and Laplacians are bitwise those of two
+// one-step launches. Cells of E outside the grid hold exact zeros in the shared p^{n+1} tile (the
+// zero padding the second step's Laplacian sees); only core cells are stored. The source stencil and
+// receivers of both steps are applied to the levels they belong to.
+// ------------------------------------------------------------------------------------------
+template <typename T, int VZ, int RX, int R>
+struct Tile2T {  // the core tile of a two-step launch inside fwd2d's tile shape
+  using S = Tile2Shape<T, VZ, RX, R>;
+  static constexpr int CX = S::TX - 2 * R;
+  static constexpr int CZ = S::TZ - 2 * S::HL;
+  static constexpr int NS = (sizeof(T) == 8 || RX >= 4 || VZ >= 4) ? 2 : 3;  // shot buffers of p^n
+};
+
+template <typename T, int R, int VZ, int RX, bool AB>
+__device__ __forceinline__ void fwd2t_body(const KGrid<T>& g, const Tiled2<T>& a, int bx, int by, int bz,
+                                           unsigned char* smem_raw) {
+  using S = Tile2Shape<T, VZ, RX, R>;
+  using U = Tile2T<T, VZ, RX, R>;
+  constexpr int NS = U::NS;
+  T* scc = reinterpret_cast<T*>(smem_raw);  // [QS] C over E
+  T* sa = scc + S::QS;                      // [QS] A (layer tiles)
+  T* sbb = sa + S::QS;                      // [QS] B (layer tiles)
+  T* sq = sbb + S::QS;                      // [PS] p^{n+1} over E, E at (R, HL)
+  T* sp = sq + S::PS;                       // [NS][PS] p^n with halo
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int cz0 = bx * U::CZ, cx0 = by * U::CX;       // core tile origin
+  const int z0 = cz0 - S::HL, x0 = cx0 - R;            // E origin
+  const int tile = by * a.tt.tiles_z + bx;
+  const int sb = bz * a.shots_per_cta;
+  const int se = min(sb + a.shots_per_cta, a.n_shots);
+  const int zc = z0 + lane * VZ;  // first owned column of E
+  const int xr = x0 + warp * RX;  // first owned row of E
+  const int lrow = warp * RX;     // first owned row inside E
+  const int ld = (int)g.s0;
+  const long long cbase = g.origin + (long long)xr * ld + zc;
+  const bool core_cols = lane * VZ >= S::HL && lane * VZ < S::HL + U::CZ;  // lane-uniform
+  bool in_row[RX], core_row[RX];  // row k of the owned cells lies in the grid / in the core
+#pragma unroll
+  for (int k = 0; k < RX; ++k) {
+    const int x = xr + k;
+    in_row[k] = x >= 0 && x < g.n0;
+    core_row[k] = lrow + k >= R && lrow + k < R + U::CX && in_row[k];
+  }
+  bool in_col[VZ];
+#pragma unroll
+  for (int v = 0; v < VZ; ++v) in_col[v] = zc + v >= 0 && zc + v < g.n1;
+  const bool vec_ok = zc >= 0 && zc + VZ <= ld;  // the owned vector lies inside a row of the layout
+
+  const bool layer_tile = AB && (x0 < g.lo0 || x0 + S::TX > g.hi0 || z0 < g.lo1 || z0 + S::TZ > g.hi1);
+  const bool use_b = layer_tile && !a.b_one;  // first step: B = 1 on the first Cerjan step
+  const bool use_b2 = layer_tile;             // second step (n + 1 >= 1)
+  const CopyPlan<S::NCH> ph = plan_halo<T, VZ, RX, R>(g, x0, z0);
+  const CopyPlan<S::NCC> pc = plan_core<T, VZ, RX, R>(g, x0, z0);
+  issue(pc, a.C, scc);  // constants, before the wait (first commit group)
+  if (layer_tile) {
+    issue(pc, a.A, sa);
+    issue(pc, a.B, sbb);
+  }
+  T pv[RX][VZ];  // p^{n-1} of the owned cells of E, one shot ahead
+#pragma unroll
+  for (int k = 0; k < RX; ++k) {
+#pragma unroll
+    for (int v = 0; v < VZ; ++v) pv[k][v] = T(0);
+    if (a.prev_ready && in_row[k] && vec_ok)
+      vldcg<T, VZ>(a.prev + (long long)sb * g.field + cbase + (long long)k * ld, pv[k]);
+  }
+  int e0 = 0, e1 = 0;
+  if (a.traces || a.traces1) { e0 = a.tt.rec_ptr[tile]; e1 = a.tt.rec_ptr[tile + 1]; }
+  int2 scor = make_int2(-1 << 20, -1 << 20);
+  if (a.src_corner) scor = make_int2(a.src_corner[2 * sb], a.src_corner[2 * sb + 1]);
+  wait_previous_grid();
+  allow_next_grid();
+  if (!a.prev_ready) {
+#pragma unroll
+    for (int k = 0; k < RX; ++k)
+      if (in_row[k] && vec_ok) vldg<T, VZ>(a.prev + (long long)sb * g.field + cbase + (long long)k * ld, pv[k]);
+  }
+#pragma unroll
+  for (int i = 0; i < NS - 1; ++i) {
+    if (sb + i < se) issue(ph, a.cur + (long long)(sb + i) * g.field, sp + i * S::PS);
+    cp_async_commit();
+  }
+  const T wc = g.wc, w1x = g.w1a, w1z = g.w1b, w2x = g.w2a, w2z = g.w2b;
+
+  for (int s = sb; s < se; ++s) {
+    const int buf = (s - sb) % NS;
+    cp_async_wait<NS - 2>();
+    __syncthreads();  // shot s landed; every thread is done with shot s-1 (its halo buffer and sq)
+    {
+      const int sn = s + NS - 1, nb = (sn - sb) % NS;
+      if (sn < se) issue(ph, a.cur + (long long)sn * g.field, sp + nb * S::PS);
+      cp_async_commit();
+    }
+    const T* P = sp + buf * S::PS;
+    // receiver samples of level n (corners in the core tile; P holds E with R rows, HL columns of halo)
+    if (a.traces)
+      for (int e = e0 + threadIdx.x; e < e1; e += 256) {
+        const int r = a.tt.rec_list[e];
+        const int row = a.tt.rec_corner[2 * r] - x0 + R, col = a.tt.rec_corner[2 * r + 1] - z0 + S::HL;
+        const T* w = a.rec_w + 4 * r;
+        T acc = mul_rn(w[0], P[row * S::SW + col]);
+        acc = fma_rn(w[1], P[row * S::SW + col + 1], acc);
+        acc = fma_rn(w[2], P[(row + 1) * S::SW + col], acc);
+        acc = fma_rn(w[3], P[(row + 1) * S::SW + col + 1], acc);
+        a.traces[((long long)s * a.n_rec + r) * a.n_t + a.j] = acc;
+      }
+    const int sbx = scor.x, sbz = scor.y;
+    if (a.src_corner && s + 1 < se) scor = make_int2(a.src_corner[2 * (s + 1)], a.src_corner[2 * (s + 1) + 1]);
+    const bool src_tile = a.src_corner && sbx + 1 >= x0 && sbx < x0 + S::TX && sbz + 1 >= z0 && sbz < z0 + S::TZ;
+    T sw0 = 0, sw1 = 0, sw2 = 0, sw3 = 0, tw0 = 0, tw1 = 0, tw2 = 0, tw3 = 0;
+    if (src_tile) {
+      const T wn = a.wavelet[a.n];
+      sw0 = mul_rn(a.src_w[4 * s], wn); sw1 = mul_rn(a.src_w[4 * s + 1], wn);
+      sw2 = mul_rn(a.src_w[4 * s + 2], wn); sw3 = mul_rn(a.src_w[4 * s + 3], wn);
+      if (a.two) {
+        const T wm = a.wavelet[a.n + 1];
+        tw0 = mul_rn(a.src_w[4 * s], wm); tw1 = mul_rn(a.src_w[4 * s + 1], wm);
+        tw2 = mul_rn(a.src_w[4 * s + 2], wm); tw3 = mul_rn(a.src_w[4 * s + 3], wm);
+      }
+    }
+    const bool more = s + 1 < se;
+    const long long so = (long long)s * g.field, sn = so + g.field;
+
+    // ---- step n over E: p^{n+1} into sq (zeros outside the grid), core cells to global
+    {
+      T wv[2 * R + 1][VZ];
+#pragma unroll
+      for (int q = 0; q < 2 * R; ++q) vload<T, VZ>(P + (lrow + q) * S::SW + S::HL + lane * VZ, wv[q]);
+#pragma unroll
+      for (int k = 0; k < RX; ++k) {
+        const int prow = lrow + k + R;
+        vload<T, VZ>(P + (prow + R) * S::SW + S::HL + lane * VZ, wv[2 * R]);
+        Row3<T, VZ> rw;
+        vload<T, VZ>(P + prow * S::SW + S::HL + lane * VZ - VZ, rw.l);
+#pragma unroll
+        for (int v = 0; v < VZ; ++v) rw.c[v] = wv[R][v];
+        vload<T, VZ>(P + prow * S::SW + S::HL + lane * VZ + VZ, rw.r);
+        const int x = xr + k;
+        const int toff = (lrow + k) * S::TZ + lane * VZ;
+        T cc[VZ], ca[VZ], cb[VZ];
+        vload<T, VZ>(scc + toff, cc);
+#pragma unroll
+        for (int v = 0; v < VZ; ++v) { ca[v] = T(1); cb[v] = T(1); }
+        if (layer_tile) vload<T, VZ>(sa + toff, ca);
+        if (use_b) vload<T, VZ>(sbb + toff, cb);
+        T o[VZ], lp[VZ];
+#pragma unroll
+        for (int v = 0; v < VZ; ++v) {
+          lp[v] = lap_at<T, R, VZ>(wv, rw, v, wc, w1x, w1z, w2x, w2z);
+          o[v] = fma_rn(cc[v], lp[v], fma_rn(-cb[v], pv[k][v], add_rn(wv[R][v], wv[R][v])));
+        }
+        if (src_tile) {
+#pragma unroll
+          for (int v = 0; v < VZ; ++v) {
+            const int dx = x - sbx, dz = zc + v - sbz;
+            if (dx >= 0 && dx <= 1 && dz >= 0 && dz <= 1)
+              o[v] = add_rn(o[v], (dx == 0) ? (dz == 0 ? sw0 : sw1) : (dz == 0 ? sw2 : sw3));
+          }
+        }
+        if (layer_tile) {
+#pragma unroll
+          for (int v = 0; v < VZ; ++v) o[v] = mul_rn(ca[v], o[v]);
+        }
+        if (core_row[k] && core_cols) {
+          const long long ro = cbase + (long long)k * ld;
+          store_row<T, VZ>(a.next + so + ro, o, zc, g.n1);
+          if (a.lap_out) store_row<T, VZ>(a.lap_out + so + ro, lp, zc, g.n1);
+        }
+        if (a.two) {
+#pragma unroll
+          for (int v = 0; v < VZ; ++v)
+            if (!(in_row[k] && in_col[v])) o[v] = T(0);  // the grid's zero padding for the next step
+          vstore<T, VZ>(sq + prow * S::SW + S::HL + lane * VZ, o);
+        }
+        if (more && in_row[k] && vec_ok) vldg<T, VZ>(a.prev + sn + cbase + (long long)k * ld, pv[k]);
+#pragma unroll
+        for (int q = 0; q < 2 * R; ++q)
+#pragma unroll
+          for (int v = 0; v < VZ; ++v) wv[q][v] = wv[q + 1][v];
+      }
+    }
+    if (!a.two) continue;
+    __syncthreads();  // p^{n+1} of all of E is in sq
+    if (a.traces1)  // receiver samples of level n+1
+      for (int e = e0 + threadIdx.x; e < e1; e += 256) {
+        const int r = a.tt.rec_list[e];
+        const int row = a.tt.rec_corner[2 * r] - x0 + R, col = a.tt.rec_corner[2 * r + 1] - z0 + S::HL;
+        const T* w = a.rec_w + 4 * r;
+        T acc = mul_rn(w[0], sq[row * S::SW + col]);
+        acc = fma_rn(w[1], sq[row * S::SW + col + 1], acc);
+        acc = fma_rn(w[2], sq[(row + 1) * S::SW + col], acc);
+        acc = fma_rn(w[3], sq[(row + 1) * S::SW + col + 1], acc);
+        a.traces1[((long long)s * a.n_rec + r) * a.n_t + a.j1] = acc;
+      }
+    // ---- step n+1 over E (kept only in the core): p^{n+2} from sq, p^n from the halo tile's centre
+    {
+      T wv[2 * R + 1][VZ];
+#pragma unroll
+      for (int q = 0; q < 2 * R; ++q) vload<T, VZ>(sq + (lrow + q) * S::SW + S::HL + lane * VZ, wv[q]);
+#pragma unroll
+      for (int k = 0; k < RX; ++k) {
+        const int prow = lrow + k + R;
+        vload<T, VZ>(sq + (prow + R) * S::SW + S::HL + lane * VZ, wv[2 * R]);
+        Row3<T, VZ> rw;
+        vload<T, VZ>(sq + prow * S::SW + S::HL + lane * VZ - VZ, rw.l);
+#pragma unroll
+        for (int v = 0; v < VZ; ++v) rw.c[v] = wv[R][v];
+        vload<T, VZ>(sq + prow * S::SW + S::HL + lane * VZ + VZ, rw.r);
+        const int x = xr + k;
+        const int toff = (lrow + k) * S::TZ + lane * VZ;
+        T cc[VZ], ca[VZ], cb[VZ], pn[VZ];
+        vload<T, VZ>(scc + toff, cc);
+        vload<T, VZ>(P + prow * S::SW + S::HL + lane * VZ, pn);  // p^n at the owned cells
+#pragma unroll
+        for (int v = 0; v < VZ; ++v) { ca[v] = T(1); cb[v] = T(1); }
+        if (layer_tile) vload<T, VZ>(sa + toff, ca);
+        if (use_b2) vload<T, VZ>(sbb + toff, cb);
+        T o[VZ], lp[VZ];
+#pragma unroll
+        for (int v = 0; v < VZ; ++v) {
+          lp[v] = lap_at<T, R, VZ>(wv, rw, v, wc, w1x, w1z, w2x, w2z);
+          o[v] = fma_rn(cc[v], lp[v], fma_rn(-cb[v], pn[v], add_rn(wv[R][v], wv[R][v])));
+        }
+        if (src_tile) {
+#pragma unroll
+          for (int v = 0; v < VZ; ++v) {
+            const int dx = x - sbx, dz = zc + v - sbz;
+            if (dx >= 0 && dx <= 1 && dz >= 0 && dz <= 1)
+              o[v] = add_rn(o[v], (dx == 0) ? (dz == 0 ? tw0 : tw1) : (dz == 0 ? tw2 : tw3));
+          }
+        }
+        if (layer_tile) {
+#pragma unroll
+          for (int v = 0; v < VZ; ++v) o[v] = mul_rn(ca[v], o[v]);
+        }
+        if (core_row[k] && core_cols) {
+          const long long ro = cbase + (long long)k * ld;
+          store_row<T, VZ>(a.next2 + so + ro, o, zc, g.n1);
+          if (a.lap_out1) store_row<T, VZ>(a.lap_out1 + so + ro, lp, zc, g.n1);
+        }
+#pragma unroll
+        for (int q = 0; q < 2 * R; ++q)
+#pragma unroll
+          for (int v = 0; v < VZ; ++v) wv[q][v] = wv[q + 1][v];
+      }
+    }
+  }
+}
+
+template <typename T, int R, int VZ, int RX, bool AB>
+__global__ void __launch_bounds__(256, 2) fwd2t(KGrid<T> g, Tiled2<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  fwd2t_body<T, R, VZ, RX, AB>(g, a, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
 }
 
 // The per-CTA launches of one problem: blockIdx = (tile along z, tile along x, shot group).

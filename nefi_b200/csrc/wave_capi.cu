@@ -266,8 +266,10 @@ int snap_load(const nw_grid* g, const nw_storage* st, int n_shots, int j, T* lm1
 // ---- launch shapes ------------------------------------------------------------------------
 struct TileCfg {  // one 2-D step kernel's tile: 8*rx rows by 32*vz columns, spc shots per CTA
   int vz, rx, spc;
-  int tx() const { return 8 * rx; }
-  int tz() const { return 32 * vz; }
+  int depth = 1;   // forward steps per launch; with 2 the tile is the core of that shape (fwd2t)
+  int r = 0, hl = 0;  // stencil radius and halo columns (16 bytes of elements) of the grid
+  int tx() const { return 8 * rx - (depth == 2 ? 2 * r : 0); }
+  int tz() const { return 32 * vz - (depth == 2 ? 2 * hl : 0); }
   int tiles_z(const nw_grid* g) const { return (g->n[1] + tz() - 1) / tz(); }
   int groups(int n_shots) const { return (n_shots + spc - 1) / spc; }
   dim3 grid(const nw_grid* g, int n_shots) const {
@@ -301,6 +303,11 @@ int resolve_tune(const nw_grid* g, const nw_tuning* t, Tune* out) {
   rc = check_tile(g, r.adj, "adj_");
   if (rc) return rc;
   if (g->ndim == 3) r.fwd.spc = r.adj.spc = 1;
+  // two forward steps per launch: 2-D grids without a PML (whose steps run a layer kernel beside the box)
+  r.fwd.depth = (t && t->depth == 2 && g->ndim == 2 && g->absorbing != NW_ABS_PML) ? 2 : 1;
+  if (t && (t->depth < 0 || t->depth > 2)) return fail(NW_ERR_ARG, "tuning.depth must be 0, 1 or 2");
+  r.fwd.r = r.adj.r = g->radius;
+  r.fwd.hl = r.adj.hl = g->dtype == NW_F64 ? 2 : 4;
   *out = r;
   return NW_OK;
 }
@@ -320,6 +327,12 @@ template <typename T, int R, int VZ, int RX, bool ADJ>
 constexpr size_t step2_smem() {
   using S = nw::Tile2Shape<T, VZ, RX, R>;
   return (ADJ ? 6 * S::QS + S::NSA * (S::PS + 2 * S::QS) : 3 * S::QS + S::NS * S::PS) * sizeof(T);
+}
+// fwd2t: C, A, B over the extended tile, the shared p^{n+1} tile and the ring of p^n halo tiles.
+template <typename T, int R, int VZ, int RX>
+constexpr size_t step2t_smem() {
+  using S = nw::Tile2Shape<T, VZ, RX, R>;
+  return (3 * S::QS + (nw::Tile2T<T, VZ, RX, R>::NS + 1) * S::PS) * sizeof(T);
 }
 constexpr size_t kMaxSmem = 227 * 1024;  // opt-in shared memory per CTA on sm_100a
 
@@ -372,6 +385,18 @@ int launch_fwd2_v(const nw::KGrid<T>& kg, const nw::Tiled2<T>& st, dim3 grid, cu
   int rc = allow_smem(nw::fwd2d<T, R, VZ, RX, AB>, smem, &done);
   if (rc) return rc;
   return launch_pdl(nw::fwd2d<T, R, VZ, RX, AB>, grid, smem, s, kg, whole_grid(kg, st));
+}
+template <typename T, int R, int VZ, int RX, bool AB>
+int launch_fwd2t_v(const nw::KGrid<T>& kg, const nw::Tiled2<T>& st, dim3 grid, cudaStream_t s) {
+  constexpr size_t smem = step2t_smem<T, R, VZ, RX>();
+  if constexpr (smem > kMaxSmem) {
+    return fail(NW_ERR_ARG, "two-step tile too large for shared memory (lower tuning rx or vz)");
+  } else {
+    static bool done = false;
+    int rc = allow_smem(nw::fwd2t<T, R, VZ, RX, AB>, smem, &done);
+    if (rc) return rc;
+    return launch_pdl(nw::fwd2t<T, R, VZ, RX, AB>, grid, smem, s, kg, st);
+  }
 }
 template <typename T, int R, int VZ, int RX, bool AB>
 int launch_adj2_v(const nw::KGrid<T>& kg, const nw::Tiled2<T>& st, dim3 grid, cudaStream_t s) {
@@ -542,11 +567,56 @@ dim3 box_tiles(const nw::PmlStep<T>& st, const TileCfg& c, int n_shots, nw::Tile
 }
 
 template <typename T>
-struct Ring {  // time level n (n >= -1) of the pressure field: three rotating levels
+struct Ring {  // time level n (n >= -1) of the pressure field: three (or four) rotating levels
   T* base;
   long long level_elems;
-  T* at(int n) const { return base + (long long)((n + 1) % 3) * level_elems; }
+  int levels = 3;
+  T* at(int n) const { return base + (long long)((n + 1) % levels) * level_elems; }
 };
+int ring_levels(const nw_storage* st) { return st->ring_levels == 4 ? 4 : 3; }
+
+// Two forward steps n, n+1 for all shots in one launch (fwd2t): 2-D without a PML, tuning depth 2,
+// a ring of four levels. Receivers of levels n and n+1 on record steps; Lap p^n and Lap p^{n+1} into
+// lap0 / lap1 when given. two = false: the step n alone with the same tiles.
+template <typename T>
+int forward_pair(const nw_grid* g, const nw::KGrid<T>& kg, const nw_medium* m, const nw_acquisition* a,
+                 const nw_time* t, const Tune& tu, const Ring<T>& L, int n, bool two, T* traces, T* lap0,
+                 T* lap1, cudaStream_t s) {
+  if (two && L.levels != 4) return fail(NW_ERR_ARG, "two steps per launch need a ring of four levels");
+  nw::Tiled2<T> st = {};
+  st.prev = L.at(n - 1);
+  st.cur = L.at(n);
+  st.next = L.at(n + 1);
+  st.next2 = two ? L.at(n + 2) : nullptr;
+  st.lap_out = lap0;
+  st.lap_out1 = two ? lap1 : nullptr;
+  st.two = two ? 1 : 0;
+  st.C = (const T*)m->c2dt2;
+  st.A = (const T*)m->coef_a;
+  st.B = (const T*)m->coef_b;
+  st.b_one = (n == 0 && t->first_b_one) ? 1 : 0;
+  st.prev_ready = 0;  // the previous launch may have written p^{n-1} as its second step
+  st.src_corner = a->has_source ? a->src_corner : nullptr;
+  st.src_w = (const T*)a->src_weight;
+  st.wavelet = (const T*)a->wavelet;
+  st.n = n;
+  st.n_shots = a->n_shots;
+  st.shots_per_cta = tu.fwd.spc;
+  const bool rec0 = traces && a->n_rec > 0 && n % t->substeps == 0;
+  const bool rec1 = two && traces && a->n_rec > 0 && (n + 1) % t->substeps == 0;
+  st.traces = rec0 ? traces : nullptr;
+  st.traces1 = rec1 ? traces : nullptr;
+  st.j = n / t->substeps;
+  st.j1 = (n + 1) / t->substeps;
+  st.rec_w = (const T*)a->rec_weight;
+  st.n_rec = a->n_rec;
+  st.n_t = t->n_t;
+  st.tt = tile_tables(g, a, tu.fwd);
+  st.x_end = g->n[0];
+  st.z_end = g->n[1];
+  return NW_DISPATCH2(launch_fwd2t_v, T, tu.fwd, kg, st, tu.fwd.grid(g, a->n_shots), s);
+}
+
 
 // One forward step n for all shots (traces != NULL: also sample level n if it is a record step;
 // lap_out != NULL: also store Lap p^n there, the factor of the step's velocity gradient term).
@@ -596,6 +666,8 @@ int forward_step(const nw_grid* g, const nw::KGrid<T>& kg, const nw_medium* m, c
         s, true, [&](cudaStream_t t) { return launch_pml<T, false>(g, kg, st, a->n_shots, t); },
         [&](cudaStream_t t) { return NW_DISPATCH2(launch_fwd2_v, T, tu.fwd, kg, tb, grid, t); });
   }
+  if (g->ndim == 2 && tu.fwd.depth == 2)  // the two-step kernel's tiles, one step
+    return forward_pair<T>(g, kg, m, a, t, tu, L, n, false, traces, lap_out, nullptr, s);
   if (g->ndim == 2) {
     nw::Tiled2<T> st = {};
     st.prev = L.at(n - 1);
@@ -651,15 +723,19 @@ int forward_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
   Ring<T> L;
   L.base = (T*)st->ring;
   L.level_elems = LE;
+  L.levels = ring_levels(st);
   const bool ckpt = !st->history && st->snap;
   if (ckpt && st->segment < 1) return fail(NW_ERR_ARG, "segment must be >= 1");
   const bool pml = g->absorbing == NW_ABS_PML;
   if (pml && !st->pml_psi) return fail(NW_ERR_ARG, "a PML run needs storage.pml_psi");
   const nw::KGrid<T> kg = kgrid<T>(g);
-  for (int n = n_begin; n < n_end; ++n) {
-    // a segment start: its snapshot slot (segment j -> slot j, or the binomial schedule's slot, -1: none)
-    const int slot = !(ckpt && n % st->segment == 0) ? -1
-                     : st->snap_slot ? st->snap_slot[n / st->segment] : n / st->segment;
+  // a segment start's snapshot slot (segment j -> slot j, or the binomial schedule's slot; -1: none)
+  auto slot_at = [&](int n) {
+    return !(ckpt && n % st->segment == 0) ? -1 : st->snap_slot ? st->snap_slot[n / st->segment] : n / st->segment;
+  };
+  const bool pairs = g->ndim == 2 && tu.fwd.depth == 2 && L.levels == 4;
+  for (int n = n_begin; n < n_end;) {
+    const int slot = slot_at(n);
     if (slot >= 0) {
       T* faces[2];
       if (pml) pml_faces<T>((T*)st->pml_psi, LE, n, faces);
@@ -667,9 +743,16 @@ int forward_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
       if (rc) return rc;
     }
     T* lap = st->history ? (T*)st->history + (long long)n * LE : nullptr;
+    if (pairs && n + 1 < n_end && slot_at(n + 1) < 0) {  // steps n and n+1 in one launch
+      int rc = forward_pair<T>(g, kg, m, a, t, tu, L, n, true, traces, lap, lap ? lap + LE : nullptr, s);
+      if (rc) return rc;
+      n += 2;
+      continue;
+    }
     // from the second step of the call on, p^{n-1} is the output of a step two launches back
     int rc = forward_step<T>(g, kg, m, a, t, tu, L, n, traces, lap, s, (T*)st->pml_psi, n > n_begin);
     if (rc) return rc;
+    ++n;
   }
   if (traces && n_end == t->n_steps && t->n_steps % t->substeps == 0) {
     int rc = launch_sample<T>(g, a, t->n_t, L.at(n_end), n_end / t->substeps, traces, s);
@@ -705,6 +788,24 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
   Ring<T> L;  // the pressure levels of the segment being recomputed
   L.base = (T*)st->ring;
   L.level_elems = LE;
+  L.levels = ckpt ? ring_levels(st) : 3;
+  const bool pairs = g->ndim == 2 && tu.fwd.depth == 2 && L.levels == 4;
+  // forward steps [k0, k1) of a recompute or an advance; Lap p^k into seg + (k - k0) levels if seg
+  auto recompute = [&](int k0, int k1, T* seg) -> int {
+    for (int k = k0; k < k1;) {
+      T* lp = seg ? seg + (long long)(k - k0) * LE : nullptr;
+      if (pairs && k + 1 < k1) {
+        const int rc = forward_pair<T>(g, kg, m, a, t, tu, L, k, true, nullptr, lp, lp ? lp + LE : nullptr, s);
+        if (rc) return rc;
+        k += 2;
+        continue;
+      }
+      const int rc = forward_step<T>(g, kg, m, a, t, tu, L, k, nullptr, lp, s, (T*)st->pml_psi, k > k0);
+      if (rc) return rc;
+      ++k;
+    }
+    return NW_OK;
+  };
   int seg_n0 = -1;  // first step of the segment whose Lap p levels the segment buffer holds
   const int n_stop = lambda0 ? 0 : 1;
   dim3 ig(((a->n_cells > 0 ? a->n_cells : 1) + 127) / 128, S);
@@ -803,13 +904,12 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
           if (rc) return rc;
           break;
         }
-        case NW_SCHED_ADVANCE:
+        case NW_SCHED_ADVANCE: {
           if (x < 0 || y <= x || (long long)y * K >= N) return fail(NW_ERR_ARG, "schedule: bad advance");
-          for (int k = x * K; k < y * K; ++k) {
-            const int rc = forward_step<T>(g, kg, m, a, t, tu, L, k, nullptr, nullptr, s, (T*)st->pml_psi, k > x * K);
-            if (rc) return rc;
-          }
+          const int rc = recompute(x * K, y * K, nullptr);
+          if (rc) return rc;
           break;
+        }
         case NW_SCHED_YOUTURN:
           if (x != seg) return fail(NW_ERR_ARG, "schedule: segments must be reversed last to first, one YOUTURN each");
           return NW_OK;
@@ -834,11 +934,8 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
         int rc = prog ? run_program(n0 / K)
                       : snap_load<T>(g, st, S, n0 / K, L.at(n0 - 1), L.at(n0), s, pml ? faces : nullptr);
         if (rc) return rc;
-        for (int k = n0; k < n1; ++k) {
-          rc = forward_step<T>(g, kg, m, a, t, tu, L, k, nullptr, (T*)st->segbuf + (long long)(k - n0) * LE, s,
-                               (T*)st->pml_psi, k > n0);
-          if (rc) return rc;
-        }
+        rc = recompute(n0, n1, (T*)st->segbuf);
+        if (rc) return rc;
       }
       lap = (const T*)st->segbuf + (long long)(n - n0) * LE;
     }
@@ -1661,6 +1758,7 @@ int nw_batch_prepare(const nw_batch_problem* problems, int32_t n_problems, const
   if (rc) return rc;
   rc = resolve_tune(&problems[0].grid, tune, &tu);
   if (rc) return rc;
+  tu.fwd.depth = 1;  // batched steps take one step per launch
   rc = check_batch(problems, n_problems, tu);
   if (rc) return rc;
   if (problems[0].grid.dtype == NW_F32)
@@ -1676,6 +1774,7 @@ int nw_batch_forward(const nw_batch_problem* problems, int32_t n_problems, const
   if (rc) return rc;
   rc = resolve_tune(&problems[0].grid, tune, &tu);
   if (rc) return rc;
+  tu.fwd.depth = 1;  // batched steps take one step per launch
   rc = check_batch(problems, n_problems, tu);
   if (rc) return rc;
   if (problems[0].grid.dtype == NW_F32)
@@ -1691,6 +1790,7 @@ int nw_batch_adjoint(const nw_batch_problem* problems, int32_t n_problems, const
   if (rc) return rc;
   rc = resolve_tune(&problems[0].grid, tune, &tu);
   if (rc) return rc;
+  tu.fwd.depth = 1;  // batched steps take one step per launch
   rc = check_batch(problems, n_problems, tu);
   if (rc) return rc;
   if (problems[0].grid.dtype == NW_F32)
@@ -1712,11 +1812,12 @@ int time_reversal_impl(const nw_grid* g, const nw_medium* m, const nw_acquisitio
                        cudaStream_t s) {
   const long long LE = g->field_elems;
   const int N = t->n_steps, M = t->substeps, n_t = t->n_t;
-  NW_CUDA(cudaMemsetAsync(st->ring, 0, 3 * (size_t)LE * sizeof(T), s));
-  if (g->absorbing == NW_ABS_PML) NW_CUDA(cudaMemsetAsync(st->pml_psi, 0, 4 * (size_t)LE * sizeof(T), s));
   Ring<T> L;
   L.base = (T*)st->ring;
   L.level_elems = LE;
+  L.levels = ring_levels(st);
+  NW_CUDA(cudaMemsetAsync(st->ring, 0, L.levels * (size_t)LE * sizeof(T), s));
+  if (g->absorbing == NW_ABS_PML) NW_CUDA(cudaMemsetAsync(st->pml_psi, 0, 4 * (size_t)LE * sizeof(T), s));
   const nw::KGrid<T> kg = kgrid<T>(g);
   auto impose = [&](int n) -> int {  // the traces at reversed time T - n dt on level n
     const double u = (n_t - 1) - (double)n / M;

@@ -180,9 +180,12 @@ class _Run:
         self.kind = mode[0]
         self.storage = _lib.Storage()
         self.history = self.ring = self.snap = self.segbuf = None
-        # the pressure advances through three rotating levels in every mode
-        self.ring = plan.empty_levels(3, n_shots)
+        # the pressure advances through three rotating levels in every mode (four when the forward
+        # takes two steps per launch)
+        self.nl = plan.ring_levels
+        self.ring = plan.empty_levels(self.nl, n_shots)
         self.storage.ring = self.ring.data_ptr()
+        self.storage.ring_levels = self.nl
         self.psi = None
         if plan.pml is not None:  # the PML's face fields, two axes x two step parities, zero at start
             self.psi = plan.empty_levels(4, n_shots)
@@ -214,7 +217,7 @@ class _Run:
 
     def level(self, n: int) -> torch.Tensor:
         """Pressure level ``n`` (``(n_shots, field)``) while it is in the ring."""
-        return self.ring[(n + 1) % 3]
+        return self.ring[(n + 1) % self.nl]
 
     def release(self) -> None:
         self.history = self.ring = self.snap = self.segbuf = self.psi = None

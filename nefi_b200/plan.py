@@ -176,12 +176,16 @@ class DevicePlan:
         self.set_tuning(*(getattr(op, "tuning", None) or ()))
 
     def set_tuning(self, vz: int = 0, rx: int = 0, shots_per_cta: int = 0, adj_vz: int = 0, adj_rx: int = 0,
-                   adj_shots_per_cta: int = 0) -> None:
-        """Choose the 2-D launch shapes (0 = library default) and build the per-tile tables."""
-        t = _lib.Tuning(int(vz), int(rx), int(shots_per_cta), int(adj_vz), int(adj_rx), int(adj_shots_per_cta))
+                   adj_shots_per_cta: int = 0, depth: int = 0) -> None:
+        """Choose the 2-D launch shapes (0 = library default) and the forward steps per launch
+        (``depth`` 2: two, on 2-D grids without a PML), and build the per-tile tables."""
+        t = _lib.Tuning(int(vz), int(rx), int(shots_per_cta), int(adj_vz), int(adj_rx), int(adj_shots_per_cta),
+                        int(depth))
         shape = (C.c_int32 * 4)()
         _lib.check(_lib.load().nw_tile_shape(C.byref(self.g), C.byref(t), shape))
         self.tuning = t
+        # forward steps per launch as the library resolved them (two need a ring of four levels)
+        self.ring_levels = 4 if (int(depth) == 2 and self.g.ndim == 2 and self.pml is None) else 3
         self.tile = (shape[0], shape[1])       # forward steps
         self.adj_tile = (shape[2], shape[3])   # adjoint steps
         self.tiles_z = self.adj_tiles_z = 0

@@ -23,12 +23,16 @@ FWI = golden_names("fwi")
 PAT = golden_names("pat")
 
 
-def make_op(case, **over):
+def make_op(case, tuning=None, **over):
     dom = Domain(tuple(case["shape"]), tuple(tuple(e) for e in case["extent"]))
     kw = {**case["kw"], "grad_mode": "autograd", **over}
     if case["kind"] == "fwi":
-        return WaveOperatorB200(dom, case["sources"], case["receivers"], **kw)
-    return WaveInitialConditionOperatorB200(dom, case["receivers"], c=torch.tensor(case["c"]), **kw)
+        op = WaveOperatorB200(dom, case["sources"], case["receivers"], **kw)
+    else:
+        op = WaveInitialConditionOperatorB200(dom, case["receivers"], c=torch.tensor(case["c"]), **kw)
+    if tuning is not None:
+        op.tuning = tuning
+    return op
 
 
 def run_fwi(case, dtype, dev, **over):
@@ -378,6 +382,51 @@ def test_results_do_not_depend_on_the_launch_shape(dtype, cuda_device):
         tr, g = _layered_grad(op, dtype, cuda_device, shape)
         assert np.array_equal(tr, tr0), shape
         assert rel_l2(g, g0) < (1e-12 if dtype == torch.float64 else 1e-5), shape
+
+
+# (vz, rx, shots_per_cta) of the forward with two steps per launch
+TWO_STEP_SHAPES = [(4, 2, 2), (4, 4, 2), (2, 4, 3), (4, 8, 1), (2, 2, 8)]
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_two_steps_per_launch_are_bitwise_one_step(dtype, cuda_device):
+    """The forward taking two leapfrog steps per launch (temporal blocking) gives bitwise the traces and
+    the gradient of one step per launch, for every tile shape, with an odd step count (a final single
+    step) and on a grid whose tiles straddle the absorbing layer and the grid's edges."""
+    op = _layered_op(n=150, shots=5, n_t=62)
+    tr1, g1 = _layered_grad(op, dtype, cuda_device, (0, 0, 0, 0, 0, 0, 1))
+    assert op.n_steps % 2 == 1
+    for vz, rx, spc in TWO_STEP_SHAPES:
+        if dtype == torch.float64 and vz == 4:
+            continue
+        tr2, g2 = _layered_grad(op, dtype, cuda_device, (vz, rx, spc, 0, 0, 0, 2))
+        assert op._plan(cuda_device, dtype).ring_levels == 4
+        assert np.array_equal(tr2, tr1), (vz, rx, spc)
+        assert np.array_equal(g2, g1), (vz, rx, spc)
+
+
+@pytest.mark.parametrize("name", ["fwi_o4_sponge", "fwi_o2_none", "fwi_o4_cerjan", "fwi_o2_sponge_aniso",
+                                  "cfg1_128_o4_sponge"])
+def test_two_steps_per_launch_match_the_reference(name, cuda_device):
+    """The reference's fixtures through two steps per launch: float64 to rounding, float32 bitwise the
+    one-step results, in full-history and checkpointed (binomial, 16-bit) storage."""
+    case = load_golden(name)
+    tr64, gc64 = run_fwi(case, torch.float64, cuda_device, tuning=(0, 0, 0, 0, 0, 0, 2))
+    assert rel_l2(tr64, case["traces_f64"]) < 1e-11
+    assert rel_l2(gc64, case["grad_c_f64"]) < 1e-10
+    for over in ({}, {"grad_mode": "checkpoint", "checkpoint_every": 7, "checkpoint_slots": 2,
+                      "snapshot": "delta16"}):
+        one = run_fwi(case, torch.float32, cuda_device, tuning=(0, 0, 0, 0, 0, 0, 1), **over)
+        two = run_fwi(case, torch.float32, cuda_device, tuning=(0, 0, 0, 0, 0, 0, 2), **over)
+        assert np.array_equal(one[0], two[0]) and np.array_equal(one[1], two[1]), over
+
+
+def test_two_steps_per_launch_in_the_photoacoustic_operator(cuda_device):
+    case = load_golden("pat2d_o4_sponge")
+    ref = run_pat(case, torch.float32, cuda_device, tuning=(0, 0, 0, 0, 0, 0, 1), with_c=True)
+    got = run_pat(case, torch.float32, cuda_device, tuning=(0, 0, 0, 0, 0, 0, 2), with_c=True)
+    for a, b in zip(ref, got):
+        assert np.array_equal(a, b)
 
 
 def _pml_interior_case():
