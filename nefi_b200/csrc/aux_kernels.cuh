@@ -515,12 +515,30 @@ __global__ void __launch_bounds__(256) snap_encode_d16(const T* __restrict__ lm1
   }
 }
 
+// Whether element e of a field in the ghost layout is a cell of the padded grid, grown by `ex` cells
+// at the high end of axis 0 and `ez` at the high end of the contiguous axis (a face field of the PML:
+// face P of an axis sits in the first ghost row or column).
+template <typename T>
+__device__ __forceinline__ bool grid_element(const KGrid<T>& g, int ndim, long long e, int ex, int ez) {
+  long long u = e - g.origin;
+  if (u < 0) return false;
+  const long long x = u / g.s0;
+  u -= x * g.s0;
+  if (x >= g.n0 + ex) return false;
+  if (ndim == 2) return u < g.n1 + ez;
+  const long long y = u / g.s1;
+  return y < g.n1 && u - y * g.s1 < g.n2 + ez;
+}
+
 // Decodes with one launch: grid.z = 0 decodes slots 0 and 1 of each block together (l0_out = p^{n0},
 // lm1_out = p^{n0} - difference, in T like the separate-slot codecs), grid.z = 1 (PML) the face
-// slots 2 and 3 into f0_out, f1_out.
+// slots 2 and 3 into f0_out, f1_out. Only the elements that hold grid cells (faces) are written: a
+// code relative to the block's anchor returns a zero outside the grid only to within half a step,
+// and the cells outside the grid must stay exact zeros (the Laplacian's zero padding).
 template <typename T>
 __global__ void __launch_bounds__(256) snap_decode_d16(const short* __restrict__ vals, const float* __restrict__ steps,
                                                        const float* __restrict__ anchors, int nblk, long long field,
+                                                       KGrid<T> g, int ndim,
                                                        T* __restrict__ lm1_out, T* __restrict__ l0_out,
                                                        T* __restrict__ f0_out, T* __restrict__ f1_out) {
   const int f = blockIdx.y, pair = blockIdx.z, n_shots = gridDim.y;
@@ -559,12 +577,13 @@ __global__ void __launch_bounds__(256) snap_decode_d16(const short* __restrict__
     if (e >= field) continue;
     const long long i = (long long)f * field + e;
     if (pair == 0) {
+      if (!grid_element(g, ndim, e, 0, 0)) continue;
       const T p0 = (T)va;
       l0_out[i] = p0;
       lm1_out[i] = p0 - (T)vb;
-    } else {
-      f0_out[i] = (T)va;
-      f1_out[i] = (T)vb;
+    } else {  // face slots: the x faces (axis 0) reach the first ghost row, the z faces the first ghost column
+      if (grid_element(g, ndim, e, 1, 0)) f0_out[i] = (T)va;
+      if (grid_element(g, ndim, e, 0, 1)) f1_out[i] = (T)vb;
     }
   }
 }

@@ -200,8 +200,8 @@ int snap_codec_d16(const nw_grid* g, const SnapLayout& L, int n_shots, char* bas
         steps, anchors);
   } else {
     nw::snap_decode_d16<T><<<dim3(gx, n_shots, slots / 2), 256, 0, s>>>(
-        vals, steps, anchors, L.nblk, g->field_elems, lm1_out, l0_out, slots == 4 ? faces_out[0] : nullptr,
-        slots == 4 ? faces_out[1] : nullptr);
+        vals, steps, anchors, L.nblk, g->field_elems, kgrid<T>(g), g->ndim, lm1_out, l0_out,
+        slots == 4 ? faces_out[0] : nullptr, slots == 4 ? faces_out[1] : nullptr);
   }
   NW_LAUNCHED();
   return NW_OK;
