@@ -896,6 +896,8 @@ def main() -> None:
     ap.add_argument("--checkpoint-every", type=int, default=None)
     ap.add_argument("--absorbing", default=None, choices=("sponge", "pml", "cerjan", "none"),
                     help="override the workload's absorbing layer (fwi workloads)")
+    ap.add_argument("--depth", type=int, default=0, choices=(0, 1, 2),
+                    help="fwi workloads: forward steps per launch (0: the library default)")
     ap.add_argument("--pat-n", type=int, default=256, help="pat_256: grid edge (profiling cases)")
     ap.add_argument("--fd-directions", type=int, default=8,
                     help="central finite-difference checks of the float64 gradient (0: none)")
@@ -936,6 +938,8 @@ def main() -> None:
         okw["absorbing"] = args.absorbing
     op = WaveOperatorB200(w.domain, w.sources, w.receivers, grad_mode=args.grad_mode, snapshot=args.snapshot,
                           checkpoint_every=args.checkpoint_every, **okw)
+    if args.depth:
+        op.tuning = (0, 0, 0, 0, 0, 0, args.depth)
     c = torch.tensor(w.c, dtype=torch.float32, device=dev)
     # observed data: traces of a smoothed model (the misfit of a typical early FWI iteration)
     with torch.no_grad():
