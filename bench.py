@@ -28,6 +28,7 @@ from __future__ import annotations
 
 import argparse
 import datetime
+import gc
 import json
 import math
 import os
@@ -968,6 +969,7 @@ def main() -> None:
 
     sampler = ClockSampler(dev.index if "CUDA_VISIBLE_DEVICES" not in os.environ else local)
     times, fwd_ms, adj_ms = [], [], []
+    ev = None
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -983,6 +985,7 @@ def main() -> None:
         fwd_ms.append(ev["fwd0"].elapsed_time(ev["fwd1"]))
         adj_ms.append(ev["adj0"].elapsed_time(ev["adj1"]))
     torch.cuda.synchronize()
+    graph.check()  # encoded snapshots: raises if a decode of the replays met a non-finite value
     if world > 1:
         dist.barrier()
     launches = graph.launches * args.steps
@@ -998,7 +1001,8 @@ def main() -> None:
     cells = w.padded_cells()
     gcells = 2 * cells * w.n_steps * S * world / (ms_per_step / 1000.0) / 1e9
     graph.release()
-    del graph
+    del graph, ev
+    gc.collect()  # the graph's private memory pool returns to the driver only once nothing holds it
     torch.cuda.empty_cache()
 
     # roofline of the dominant stencil kernel: 16 B per cell-update, per launch = cells * shots; the
@@ -1032,15 +1036,18 @@ def main() -> None:
     d_h = d.cpu().pin_memory()
     g_h = torch.empty(c.shape, dtype=torch.float32).pin_memory()
     l_h = torch.empty((), dtype=torch.float64).pin_memory()
-    e2e_ms = []
+    e2e_ms, e2e_storage, e2e_host = [], [], []
     for i in range(2 + args.steps):  # two untimed passes: the pinned copies' first use, allocator growth
         flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
+        t0 = time.perf_counter()
         cd = c_h.to(dev, non_blocking=True).requires_grad_(True)
         dd = d_h.to(dev, non_blocking=True)
         loss = 0.5 * (op({"c": cd}) - dd).double().square().sum()
+        t1 = time.perf_counter()
         loss.backward()
+        t2 = time.perf_counter()
         g = cd.grad
         if world > 1:
             dist.all_reduce(g)
@@ -1051,6 +1058,8 @@ def main() -> None:
         torch.cuda.synchronize()
         if i > 1:
             e2e_ms.append(e0.elapsed_time(e1))
+            e2e_storage.append(op.last_storage[0] if op.last_storage else None)
+            e2e_host.append([round((t1 - t0) * 1e3, 1), round((t2 - t1) * 1e3, 1)])
         del cd, dd, loss, g
     e2e_total = sum(e2e_ms)
     if world > 1:
@@ -1157,7 +1166,9 @@ def main() -> None:
                "gcell_updates_per_s": gcells, "roofline": roofline, "cpu_baseline": cpu,
                "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                        "call": "traces = op({'c': c}); loss = 1/2 ||traces - d||^2 (torch); loss.backward()",
-                       "ms_each": e2e_ms},
+                       "ms_each": e2e_ms, "storage_each": e2e_storage,
+                       "host_ms_each": {"forward_and_loss": [h[0] for h in e2e_host],
+                                        "backward": [h[1] for h in e2e_host]}},
                "e2e_misfit_gradient": {"value": mg_val, "unit": UNIT, "h2d_bytes_per_step": h2d,
                                        "d2h_bytes_per_step": g64_h.numel() * 8 + 8,
                                        "call": "op.misfit_gradient(c, d)", "ms_each": mg_ms},

@@ -18,6 +18,7 @@ from __future__ import annotations
 import ctypes as C
 import logging
 import math
+import threading
 from collections.abc import Callable, Sequence
 
 import torch
@@ -99,6 +100,9 @@ class _LeapfrogB200(Operator):
         # snapshot slots of a checkpointed gradient (None: as the memory budget allows); fewer than the
         # segments selects binomial checkpointing
         self.checkpoint_slots = checkpoint_slots
+        # the wavefield storage the last gradient-carrying call chose: ("history", None),
+        # ("checkpoint", segment) or ("checkpoint", segment, slots); None before the first
+        self.last_storage = None
         self.grid = PaddedGrid(domain, self.absorb_width)
         ta = TimeAxis(self.n_t, self.dt_obs, self.c_max, self.grid.spacing, self.order, self.courant)
         self.substeps, self.dt, self.n_steps = ta.substeps, ta.dt, ta.n_steps
@@ -245,13 +249,29 @@ def _adjoint_sweep(plan: DevicePlan, medium, acq, run: _Run, grad_traces: torch.
                               C.byref(run.storage), C.byref(plan.tuning), grad_traces.data_ptr(),
                               work.data_ptr(), gC.data_ptr(), _lib.ptr(lam0), _lib.ptr(mu1), stream))
     if run.storage.snap and run.storage.snap_kind != _lib.NW_SNAP_EXACT:
-        # encoded snapshots carry a validity check; reading the status synchronises the stream
-        rc = lib.nw_status(stream)
-        if rc == _lib.NW_ERR_NONFINITE:
-            raise SolverError("a wavefield snapshot held a non-finite value: the forward run diverged "
-                              "or the snapshot pool was corrupted")
-        _lib.check(rc)
+        # encoded snapshots carry a validity check; reading the status synchronises the stream, which
+        # a graph capture cannot do: there the graph reads it after each replay
+        if torch.cuda.is_current_stream_capturing():
+            _deferred_status.pending = True
+        else:
+            _check_snapshot_status(stream)
     return gC, lam0, mu1
+
+
+class _Deferred(threading.local):
+    pending = False
+
+
+_deferred_status = _Deferred()  # set while a capture records an adjoint that decodes snapshots
+
+
+def _check_snapshot_status(stream: int) -> None:
+    """Synchronise ``stream`` and raise if a snapshot decode found a non-finite value."""
+    rc = _lib.load().nw_status(stream)
+    if rc == _lib.NW_ERR_NONFINITE:
+        raise SolverError("a wavefield snapshot held a non-finite value: the forward run diverged "
+                          "or the snapshot pool was corrupted")
+    _lib.check(rc)
 
 
 # ------------------------------------------------------------------------------------------------
@@ -273,6 +293,7 @@ class _FWIFunction(torch.autograd.Function):
         needs_grad = ctx.needs_input_grad[0]
         mode = (plan_storage(plan, n_shots, op.n_steps, op.grad_mode, op.checkpoint_every,
                              op.snapshot, op._budget(c.device), op.checkpoint_slots) if needs_grad else ("ring", None))
+        op.last_storage = tuple(mode)
         run = _Run(plan, n_shots, op.n_steps, mode, op.snapshot)
         traces = torch.empty(n_shots, plan.n_rec, op.n_t, device=c.device, dtype=c.dtype)
         _forward_sweep(plan, medium, acq, run, 0, op.n_steps, traces, stream)
@@ -433,6 +454,7 @@ class WaveOperatorB200(_LeapfrogB200):
             S = min(n, s0 + chunk) - s0
             acq = plan.acquisition(S, s0)
             mode = modes[k]
+            self.last_storage = tuple(mode)
             tm = events if (events is not None and s0 == 0) else None
             run = _Run(plan, S, self.n_steps, mode, self.snapshot)
             traces = torch.empty(S, plan.n_rec, self.n_t, device=c.device, dtype=c.dtype)
@@ -612,22 +634,37 @@ class GradientGraph:
         self.events = {} if events else None
         graph = torch.cuda.CUDAGraph()
         n0 = lib.nw_launch_count()
-        with torch.cuda.graph(graph):
-            self.loss, self.grad = op._gradient(self.c, self.observed, self.events, None, None, self._modes)
+        _deferred_status.pending = False
+        try:
+            with torch.cuda.graph(graph):
+                self.loss, self.grad = op._gradient(self.c, self.observed, self.events, None, None, self._modes)
+        finally:
+            # the adjoint decodes encoded snapshots: their status is read after each replay instead
+            self.checks_status = _deferred_status.pending
+            _deferred_status.pending = False
         self.launches = int(lib.nw_launch_count() - n0)  # this library's kernels per replay
         self._graph = graph
         torch.cuda.synchronize(self.device)
 
     def replay(self) -> None:
-        """Recompute ``loss`` and ``grad`` from the current ``c`` and ``observed`` (asynchronous)."""
+        """Recompute ``loss`` and ``grad`` from the current ``c`` and ``observed`` (asynchronous; with
+        encoded snapshots, ``check()`` afterwards raises if a decode met a non-finite value)."""
         self._graph.replay()
 
+    def check(self) -> None:
+        """Synchronise and raise ``SolverError`` if a snapshot decode of the replays since the last
+        check met a non-finite value (no-op without encoded snapshots)."""
+        if self.checks_status:
+            _check_snapshot_status(_lib.stream_handle(self.device))
+
     def run(self, c: torch.Tensor, observed: torch.Tensor):
-        """Check ``c`` like the operator does, copy both inputs in, replay; returns ``(loss, grad)``."""
+        """Check ``c`` like the operator does, copy both inputs in, replay and (with encoded snapshots)
+        check their status; returns ``(loss, grad)``."""
         self.op._validate(c)
         self.c.copy_(c)
         self.observed.copy_(observed)
         self.replay()
+        self.check()
         return self.loss, self.grad
 
     def release(self) -> None:
