@@ -9,6 +9,9 @@
  *
  * Conventions
  *  - Every pointer is a device pointer unless stated otherwise; sizes are element counts.
+ *  - Device buffers holding fields (medium, storage, adjoint work levels, accumulators) start on
+ *    16-byte boundaries: the kernels move fields in 16-byte vectors. nw_forward / nw_adjoint return
+ *    NW_ERR_ARG for a buffer that does not.
  *  - Nothing is allocated by the library: the caller passes every buffer, sized by the
  *    nw_*_bytes() queries. The library never frees caller memory.
  *  - All work is enqueued on `stream` (a cudaStream_t passed as void*); calls are asynchronous

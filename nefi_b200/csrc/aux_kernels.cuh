@@ -406,11 +406,11 @@ __global__ void __launch_bounds__(256) snap_decode(const typename Codec<K>::H* _
 }
 
 // ------------------------------------------------------------------------------------------
-// delta16 snapshot codec: a block of SNAP_BLOCK values x[0..31] (one warp, lane = element) is
-// stored as a float anchor a = x[0], a float step s and 32 int16 codes. Element z decodes to
+// delta16 snapshot codec: a block of SNAP_BLOCK values x[0..31] is stored as a float anchor
+// a = x[0], a float step s and 32 int16 codes. Element z decodes to
 //   fmaf(s, Q[z], a),  Q[z] integer, Q[0] = 0,
 // and the int16 code of element z is the second difference Q[z] - 2 Q[z-1] + Q[z-2] (Q[-1] = 0),
-// so decoding is two warp prefix sums. The encoder takes Q[z] = rint((x[z] - a) / s) with
+// so decoding is two prefix sums. The encoder takes Q[z] = rint((x[z] - a) / s) with
 //   s = max( max(|x[1] - x[0]|, max_z |x[z] - 2 x[z-1] + x[z-2]|) / 32000, max_z |x[z] - a| / 2^22 ):
 // the rounding error |x - decoded| is s/2 (plus one rounding of the fma), i.e. 2^-16 of the
 // block's largest second difference instead of its largest value. Smooth fields (wavefields
@@ -419,173 +419,306 @@ __global__ void __launch_bounds__(256) snap_decode(const typename Codec<K>::H* _
 // Bounds: |x - a| / s <= 2^22, so |Q| and its differences are exact in float and int; each
 // computed ratio (x - a) / s carries at most 0.5 of rounding error, so a code is at most
 // 32000 (1 + 2^-22) + 2 (rint) + 2 (ratio rounding) < 32767 in magnitude.
+//
+// One thread codes one block, sequentially: the max, quantisation and differences are exact or
+// single roundings of the same operands in any order, so the codes do not depend on how the work is
+// split. A CTA covers D16Cta<T>::BLK consecutive blocks of one field and moves them between global
+// and shared memory with coalesced 16-byte accesses; every block is a 128-byte (float) row of a
+// shared tile whose 16-byte chunks are swizzled so that 8 consecutive threads reading one chunk of
+// their own rows, or 8 consecutive chunks of one row, touch distinct banks.
 // ------------------------------------------------------------------------------------------
-__device__ __forceinline__ float warp_max_f(float v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-  return v;
-}
-__device__ __forceinline__ int warp_scan_i(int v, int lane) {  // inclusive prefix sum over the warp
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int t = __shfl_up_sync(0xffffffffu, v, o);
-    if (lane >= o) v += t;
-  }
-  return v;
-}
-
-struct D16Block {  // one encoded block: this lane's code, and the block's step and anchor
-  short code;
-  float step, anchor;
+template <typename T>
+struct D16Cta {
+  static constexpr int BLK = sizeof(T) == 8 ? 128 : 256;  // blocks per CTA (the decode's T tile: 32 KB)
+  static constexpr int CH = 16 / (int)sizeof(T);           // elements of T per 16-byte chunk
 };
 
-// All 32 lanes call this with their element x (0 past the end of the field). Sets the device status
-// word if the block holds a non-finite value (the block then decodes to NaN).
-__device__ __forceinline__ D16Block d16_encode(float x, int lane) {
-  const unsigned full = 0xffffffffu;
-  D16Block b;
-  if (__any_sync(full, !(fabsf(x) <= 3.0e38f))) {
-    if (lane == 0) atomicExch(&g_status, 4);
-    b.code = 0;
-    b.step = __int_as_float(0x7fc00000);
-    b.anchor = b.step;
-    return b;
-  }
-  const float a = __shfl_sync(full, x, 0);
-  const float xm1 = __shfl_up_sync(full, x, 1);
-  const float dx = lane >= 1 ? x - xm1 : 0.f;
-  const float dxm1 = __shfl_up_sync(full, dx, 1);
-  const float d2 = lane >= 2 ? dx - dxm1 : dx;
-  const float m = warp_max_f(fabsf(d2));
-  const float r = warp_max_f(fabsf(x - a));
-  const float s = fmaxf(fmaxf(m * (1.f / 32000.f), r * 0x1p-22f), 1.17549435e-38f);
-  const float inv = 1.f / s;
-  const int q = (int)rintf((x - a) * inv);
-  const int qm1 = __shfl_up_sync(full, q, 1);
-  const int qm2 = __shfl_up_sync(full, q, 2);
-  int d = lane >= 2 ? q - 2 * qm1 + qm2 : (lane == 1 ? q : 0);
-  d = max(-32767, min(32767, d));
-  b.code = (short)d;
-  b.step = s;
-  b.anchor = a;
-  return b;
+// Element offset of chunk k (of `ch` elements) of row t in a tile of 32-element rows.
+__device__ __forceinline__ int d16_chunk(int t, int k, int ch) { return t * SNAP_BLOCK + ((k ^ (t & 7)) * ch); }
+// Byte offset of 16-byte chunk k (0..3) of row t in a tile of 32 int16 codes (64-byte rows).
+__device__ __forceinline__ int d16_code_chunk(int t, int k) { return t * 64 + ((k ^ ((t >> 1) & 3)) << 4); }
+
+// 16-byte loads and stores of CH elements of T through a float4 (aligned by the union).
+template <typename T>
+union D16Vec {
+  float4 v;
+  T e[16 / sizeof(T)];
+};
+template <typename T>
+__device__ __forceinline__ void d16_ld(const T* p, T (&o)[16 / sizeof(T)]) {
+  D16Vec<T> u;
+  u.v = *reinterpret_cast<const float4*>(p);
+#pragma unroll
+  for (int i = 0; i < (int)(16 / sizeof(T)); ++i) o[i] = u.e[i];
+}
+template <typename T>
+__device__ __forceinline__ void d16_st(T* p, const T (&o)[16 / sizeof(T)]) {
+  D16Vec<T> u;
+#pragma unroll
+  for (int i = 0; i < (int)(16 / sizeof(T)); ++i) u.e[i] = o[i];
+  *reinterpret_cast<float4*>(p) = u.v;
 }
 
-__device__ __forceinline__ float d16_decode(short code, float s, float a, int lane) {
-  const int d1 = warp_scan_i((int)code, lane);
-  const int q = warp_scan_i(d1, lane);
-  return fmaf(s, (float)q, a);
+// Sets *step, *anchor and the 32 codes (packed two per word, element 2w in the low half) of the block
+// x; returns false (codes 0, step and anchor NaN) if the block holds a non-finite value.
+__device__ __forceinline__ bool d16_encode_block(const float (&x)[SNAP_BLOCK], unsigned (&code)[SNAP_BLOCK / 2],
+                                                 float* step, float* anchor) {
+  bool finite = true;
+#pragma unroll
+  for (int z = 0; z < SNAP_BLOCK; ++z) finite = finite && fabsf(x[z]) <= 3.0e38f;
+  if (!finite) {
+#pragma unroll
+    for (int w = 0; w < SNAP_BLOCK / 2; ++w) code[w] = 0u;
+    *step = *anchor = __int_as_float(0x7fc00000);
+    return false;
+  }
+  const float a = x[0];
+  float m = 0.f, r = 0.f, dxm1 = 0.f;  // max |second difference|, max |x - a|, x[z-1] - x[z-2]
+#pragma unroll
+  for (int z = 1; z < SNAP_BLOCK; ++z) {
+    const float dx = x[z] - x[z - 1];
+    const float d2 = z >= 2 ? dx - dxm1 : dx;
+    m = fmaxf(m, fabsf(d2));
+    r = fmaxf(r, fabsf(x[z] - a));
+    dxm1 = dx;
+  }
+  const float s = fmaxf(fmaxf(m * (1.f / 32000.f), r * 0x1p-22f), 1.17549435e-38f);
+  const float inv = 1.f / s;
+  int qm1 = 0, qm2 = 0;  // Q[z-1], Q[z-2]
+#pragma unroll
+  for (int z = 0; z < SNAP_BLOCK; ++z) {
+    const int q = z == 0 ? 0 : (int)rintf((x[z] - a) * inv);
+    int d = z >= 2 ? q - 2 * qm1 + qm2 : (z == 1 ? q : 0);
+    d = max(-32767, min(32767, d));
+    const unsigned h = (unsigned)(unsigned short)(short)d;
+    if (z & 1) code[z >> 1] |= h << 16;
+    else code[z >> 1] = h;
+    qm2 = qm1;
+    qm1 = q;
+  }
+  *step = s;
+  *anchor = a;
+  return true;
+}
+
+// The 32 values of a block from its codes, step and anchor (two running sums, exact in int).
+__device__ __forceinline__ void d16_decode_block(const unsigned (&code)[SNAP_BLOCK / 2], float s, float a,
+                                                 float (&v)[SNAP_BLOCK]) {
+  int d1 = 0, q = 0;
+#pragma unroll
+  for (int z = 0; z < SNAP_BLOCK; ++z) {
+    const int c = (int)(short)(unsigned short)(z & 1 ? code[z >> 1] >> 16 : code[z >> 1] & 0xffffu);
+    d1 += c;
+    q += d1;
+    v[z] = fmaf(s, (float)q, a);
+  }
 }
 
 // Encodes snapshot slots with one launch: grid.z = slot (0: l0 = p^{n0}; 1: l0 - lm1; 2, 3: the
-// PML face fields f0, f1), grid.y = shot, SNAP_WARP_BLOCKS blocks per warp with their loads issued
-// together. Slot k of shot f occupies blocks (k * n_shots + f) * nblk of vals / steps / anchors.
+// PML face fields f0, f1), grid.y = shot, grid.x = groups of D16Cta<T>::BLK blocks. Slot k of shot f
+// occupies blocks (k * n_shots + f) * nblk of vals / steps / anchors. Every field holds nblk whole
+// blocks (its length is a multiple of SNAP_BLOCK).
 template <typename T>
 __global__ void __launch_bounds__(256) snap_encode_d16(const T* __restrict__ lm1, const T* __restrict__ l0,
                                                        const T* __restrict__ f0, const T* __restrict__ f1,
                                                        long long field, int nblk, short* __restrict__ vals,
                                                        float* __restrict__ steps, float* __restrict__ anchors) {
+  constexpr int BLK = D16Cta<T>::BLK, CH = D16Cta<T>::CH;
+  __shared__ __align__(16) float tile[BLK * SNAP_BLOCK];  // the values as float; reused for the codes
   const int f = blockIdx.y, slot = blockIdx.z, n_shots = gridDim.y;
-  const long long b0 = ((long long)blockIdx.x * 8 + (threadIdx.x >> 5)) * SNAP_WARP_BLOCKS;
-  if (b0 >= nblk) return;
-  const int lane = threadIdx.x & 31;
+  const long long bb = (long long)blockIdx.x * BLK;  // first block of this CTA within the field
+  const int nb = (int)min((long long)BLK, (long long)nblk - bb);
   const T* src = slot == 0 ? l0 : (slot == 1 ? l0 : (slot == 2 ? f0 : f1));
   const T* sub = slot == 1 ? lm1 : nullptr;
-  float v[SNAP_WARP_BLOCKS];
+  const long long e0 = (long long)f * field + bb * SNAP_BLOCK;  // first element
+  // staging: 16-byte chunks of T in field order, converted to float, into the swizzled tile
+  constexpr int CPR = SNAP_BLOCK / CH;
+  const int n_chunks = nb * CPR;
+#pragma unroll 4
+  for (int c = threadIdx.x; c < n_chunks; c += 256) {
+    const int row = c / CPR, k = c - row * CPR;
+    T v[CH];
+    d16_ld<T>(src + e0 + (long long)c * CH, v);
+    if (sub) {
+      T w[CH];
+      d16_ld<T>(sub + e0 + (long long)c * CH, w);
 #pragma unroll
-  for (int u = 0; u < SNAP_WARP_BLOCKS; ++u) {
-    const long long e = (b0 + u) * SNAP_BLOCK + lane;
-    v[u] = 0.f;
-    if (b0 + u < nblk && e < field) {
-      const long long i = (long long)f * field + e;
-      v[u] = (float)(sub ? src[i] - sub[i] : src[i]);
+      for (int i = 0; i < CH; ++i) v[i] = v[i] - w[i];
     }
-  }
-  const long long blk0 = ((long long)slot * n_shots + f) * nblk;
+    // the chunk's CH floats sit inside one 16-byte float chunk of the row
+    const int z = k * CH;
+    float* dst = tile + d16_chunk(row, z >> 2, 4) + (z & 3);
 #pragma unroll
-  for (int u = 0; u < SNAP_WARP_BLOCKS; ++u) {
-    const long long b = b0 + u;
-    if (b >= nblk) break;  // warp-uniform
-    const D16Block e = d16_encode(v[u], lane);
-    vals[(blk0 + b) * SNAP_BLOCK + lane] = e.code;
-    if (lane == 0) {
-      steps[blk0 + b] = e.step;
-      anchors[blk0 + b] = e.anchor;
-    }
+    for (int i = 0; i < CH; ++i) dst[i] = (float)v[i];
   }
+  __syncthreads();
+  const int t = threadIdx.x;
+  unsigned code[SNAP_BLOCK / 2];
+  if (t < nb) {
+    float x[SNAP_BLOCK];
+#pragma unroll
+    for (int k = 0; k < SNAP_BLOCK / 4; ++k) {
+      const float4 q = *reinterpret_cast<const float4*>(tile + d16_chunk(t, k, 4));
+      x[4 * k] = q.x; x[4 * k + 1] = q.y; x[4 * k + 2] = q.z; x[4 * k + 3] = q.w;
+    }
+    float s, a;
+    if (!d16_encode_block(x, code, &s, &a)) atomicExch(&g_status, 4);
+    const long long blk = ((long long)slot * n_shots + f) * nblk + bb + t;
+    steps[blk] = s;
+    anchors[blk] = a;
+  }
+  __syncthreads();  // every row has been read: the tile takes the codes (64-byte rows)
+  unsigned char* ct = reinterpret_cast<unsigned char*>(tile);
+  if (t < nb) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      *reinterpret_cast<uint4*>(ct + d16_code_chunk(t, k)) =
+          make_uint4(code[4 * k], code[4 * k + 1], code[4 * k + 2], code[4 * k + 3]);
+  }
+  __syncthreads();
+  uint4* out = reinterpret_cast<uint4*>(vals + ((((long long)slot * n_shots + f) * nblk + bb) * SNAP_BLOCK));
+  for (int c = threadIdx.x; c < nb * 4; c += 256)
+    out[c] = *reinterpret_cast<const uint4*>(ct + d16_code_chunk(c >> 2, c & 3));
 }
 
-// Whether element e of a field in the ghost layout is a cell of the padded grid, grown by `ex` cells
-// at the high end of axis 0 and `ez` at the high end of the contiguous axis (a face field of the PML:
-// face P of an axis sits in the first ghost row or column).
+// Number of leading elements of block b (elements 32 b .. 32 b + 31 of a field in the ghost layout)
+// that are cells of the padded grid grown by `ex` cells at the high end of axis 0 and `ez` at the high
+// end of the contiguous axis (a face field of the PML: face P of an axis sits in the first ghost row
+// or column). Rows start on multiples of SNAP_BLOCK elements (the guard and the row pitch are), so a
+// block lies in one row and its grid cells are a prefix of it.
 template <typename T>
-__device__ __forceinline__ bool grid_element(const KGrid<T>& g, int ndim, long long e, int ex, int ez) {
-  long long u = e - g.origin;
-  if (u < 0) return false;
+__device__ __forceinline__ int d16_grid_prefix(const KGrid<T>& g, int ndim, long long b, int ex, int ez) {
+  long long u = b * SNAP_BLOCK - g.origin;
+  if (u < 0) return 0;
   const long long x = u / g.s0;
   u -= x * g.s0;
-  if (x >= g.n0 + ex) return false;
-  if (ndim == 2) return u < g.n1 + ez;
-  const long long y = u / g.s1;
-  return y < g.n1 && u - y * g.s1 < g.n2 + ez;
+  if (x >= g.n0 + ex) return 0;
+  long long n_inner = g.n1 + ez;
+  if (ndim == 3) {
+    const long long y = u / g.s1;
+    if (y >= g.n1) return 0;
+    u -= y * g.s1;
+    n_inner = g.n2 + ez;
+  }
+  return (int)max(0LL, min((long long)SNAP_BLOCK, n_inner - u));
+}
+
+// Writes a CTA's tile of decoded rows (T, swizzled 16-byte chunks) to out, in coalesced chunks, only
+// the first len[row] elements of each row.
+template <typename T>
+__device__ __forceinline__ void d16_store_rows(const T* tile, const int* len, int nb, T* __restrict__ out) {
+  constexpr int CH = D16Cta<T>::CH, CPR = SNAP_BLOCK / CH;
+  for (int c = threadIdx.x; c < nb * CPR; c += 256) {
+    const int row = c / CPR, k = c - row * CPR;
+    const int n = len[row] - k * CH;  // valid elements of this chunk
+    if (n <= 0) continue;
+    const T* src = tile + d16_chunk(row, k, CH);
+    T* dst = out + (long long)row * SNAP_BLOCK + k * CH;
+    if (n >= CH) {
+      T v[CH];
+      d16_ld<T>(src, v);
+      d16_st<T>(dst, v);
+    } else {
+      for (int i = 0; i < n; ++i) dst[i] = src[i];
+    }
+  }
 }
 
 // Decodes with one launch: grid.z = 0 decodes slots 0 and 1 of each block together (l0_out = p^{n0},
 // lm1_out = p^{n0} - difference, in T like the separate-slot codecs), grid.z = 1 (PML) the face
-// slots 2 and 3 into f0_out, f1_out. Only the elements that hold grid cells (faces) are written: a
-// code relative to the block's anchor returns a zero outside the grid only to within half a step,
-// and the cells outside the grid must stay exact zeros (the Laplacian's zero padding).
+// slots 2 and 3 into f0_out, f1_out; grid.y = shot, grid.x = groups of D16Cta<T>::BLK blocks. Only the
+// elements that hold grid cells (faces) are written: a code relative to the block's anchor returns
+// a zero outside the grid only to within half a step, and the cells outside the grid must stay exact
+// zeros (the Laplacian's zero padding).
 template <typename T>
 __global__ void __launch_bounds__(256) snap_decode_d16(const short* __restrict__ vals, const float* __restrict__ steps,
                                                        const float* __restrict__ anchors, int nblk, long long field,
                                                        KGrid<T> g, int ndim,
                                                        T* __restrict__ lm1_out, T* __restrict__ l0_out,
                                                        T* __restrict__ f0_out, T* __restrict__ f1_out) {
+  constexpr int BLK = D16Cta<T>::BLK, CH = D16Cta<T>::CH;
+  // the two slots' codes (64-byte rows), then the decoded rows of one output (T)
+  __shared__ __align__(16) unsigned char smem[BLK * SNAP_BLOCK * sizeof(T)];
+  __shared__ int len0[BLK], len1[BLK];
+  static_assert(2 * BLK * 64 <= BLK * SNAP_BLOCK * (int)sizeof(T), "code tiles fit the row tile");
   const int f = blockIdx.y, pair = blockIdx.z, n_shots = gridDim.y;
-  const long long b0 = ((long long)blockIdx.x * 8 + (threadIdx.x >> 5)) * SNAP_WARP_BLOCKS;
-  if (b0 >= nblk) return;
-  const int lane = threadIdx.x & 31;
-  const long long blkA = ((long long)(2 * pair) * n_shots + f) * nblk;
-  const long long blkB = ((long long)(2 * pair + 1) * n_shots + f) * nblk;
-  short qa[SNAP_WARP_BLOCKS], qb[SNAP_WARP_BLOCKS];
-  float sa[SNAP_WARP_BLOCKS], aa[SNAP_WARP_BLOCKS], sb[SNAP_WARP_BLOCKS], ab[SNAP_WARP_BLOCKS];
-#pragma unroll
-  for (int u = 0; u < SNAP_WARP_BLOCKS; ++u) {
-    const long long b = b0 + u;
-    qa[u] = qb[u] = 0;
-    sa[u] = sb[u] = 1.f;
-    aa[u] = ab[u] = 0.f;
-    if (b < nblk) {
-      qa[u] = vals[(blkA + b) * SNAP_BLOCK + lane];
-      qb[u] = vals[(blkB + b) * SNAP_BLOCK + lane];
-      sa[u] = steps[blkA + b];
-      aa[u] = anchors[blkA + b];
-      sb[u] = steps[blkB + b];
-      ab[u] = anchors[blkB + b];
+  const long long bb = (long long)blockIdx.x * BLK;
+  const int nb = (int)min((long long)BLK, (long long)nblk - bb);
+  const long long blkA = ((long long)(2 * pair) * n_shots + f) * nblk + bb;
+  const long long blkB = ((long long)(2 * pair + 1) * n_shots + f) * nblk + bb;
+  unsigned char* ca = smem;
+  unsigned char* cb = smem + BLK * 64;
+  {
+    const uint4* ga = reinterpret_cast<const uint4*>(vals + blkA * SNAP_BLOCK);
+    const uint4* gb = reinterpret_cast<const uint4*>(vals + blkB * SNAP_BLOCK);
+#pragma unroll 4
+    for (int c = threadIdx.x; c < nb * 4; c += 256) {
+      const uint4 qa = ga[c], qb = gb[c];
+      *reinterpret_cast<uint4*>(ca + d16_code_chunk(c >> 2, c & 3)) = qa;
+      *reinterpret_cast<uint4*>(cb + d16_code_chunk(c >> 2, c & 3)) = qb;
     }
   }
-#pragma unroll
-  for (int u = 0; u < SNAP_WARP_BLOCKS; ++u) {
-    const long long b = b0 + u;
-    if (b >= nblk) break;  // warp-uniform
-    if (lane == 0 && !(sa[u] > 0.f && sa[u] <= 3.0e38f && sb[u] > 0.f && sb[u] <= 3.0e38f &&
-                       fabsf(aa[u]) <= 3.0e38f && fabsf(ab[u]) <= 3.0e38f))
+  const int t = threadIdx.x;
+  float sa = 1.f, aa = 0.f, sb = 1.f, ab = 0.f;
+  if (t < nb) {
+    sa = steps[blkA + t];
+    aa = anchors[blkA + t];
+    sb = steps[blkB + t];
+    ab = anchors[blkB + t];
+    if (!(sa > 0.f && sa <= 3.0e38f && sb > 0.f && sb <= 3.0e38f && fabsf(aa) <= 3.0e38f && fabsf(ab) <= 3.0e38f))
       atomicExch(&g_status, 4);
-    const float va = d16_decode(qa[u], sa[u], aa[u], lane);
-    const float vb = d16_decode(qb[u], sb[u], ab[u], lane);
-    const long long e = b * SNAP_BLOCK + lane;
-    if (e >= field) continue;
-    const long long i = (long long)f * field + e;
+    const long long b = bb + t;
     if (pair == 0) {
-      if (!grid_element(g, ndim, e, 0, 0)) continue;
-      const T p0 = (T)va;
-      l0_out[i] = p0;
-      lm1_out[i] = p0 - (T)vb;
-    } else {  // face slots: the x faces (axis 0) reach the first ghost row, the z faces the first ghost column
-      if (grid_element(g, ndim, e, 1, 0)) f0_out[i] = (T)va;
-      if (grid_element(g, ndim, e, 0, 1)) f1_out[i] = (T)vb;
+      len0[t] = d16_grid_prefix(g, ndim, b, 0, 0);
+    } else {
+      len0[t] = d16_grid_prefix(g, ndim, b, 1, 0);
+      len1[t] = d16_grid_prefix(g, ndim, b, 0, 1);
     }
   }
+  __syncthreads();
+  unsigned qa[SNAP_BLOCK / 2], qb[SNAP_BLOCK / 2];
+  if (t < nb) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const uint4 u = *reinterpret_cast<const uint4*>(ca + d16_code_chunk(t, k));
+      const uint4 w = *reinterpret_cast<const uint4*>(cb + d16_code_chunk(t, k));
+      qa[4 * k] = u.x; qa[4 * k + 1] = u.y; qa[4 * k + 2] = u.z; qa[4 * k + 3] = u.w;
+      qb[4 * k] = w.x; qb[4 * k + 1] = w.y; qb[4 * k + 2] = w.z; qb[4 * k + 3] = w.w;
+    }
+  }
+  __syncthreads();  // the code tiles are read: the smem takes the decoded rows
+  T* tile = reinterpret_cast<T*>(smem);
+  const long long e0 = (long long)f * field + bb * SNAP_BLOCK;
+  float va[SNAP_BLOCK];
+  if (t < nb) {
+    d16_decode_block(qa, sa, aa, va);
+#pragma unroll
+    for (int k = 0; k < SNAP_BLOCK / CH; ++k) {
+      T o[CH];
+#pragma unroll
+      for (int i = 0; i < CH; ++i) o[i] = (T)va[k * CH + i];
+      d16_st<T>(tile + d16_chunk(t, k, CH), o);
+    }
+  }
+  __syncthreads();
+  d16_store_rows<T>(tile, len0, nb, (pair == 0 ? l0_out : f0_out) + e0);
+  __syncthreads();
+  if (t < nb) {
+    float vb[SNAP_BLOCK];
+    d16_decode_block(qb, sb, ab, vb);
+#pragma unroll
+    for (int k = 0; k < SNAP_BLOCK / CH; ++k) {
+      T o[CH];
+#pragma unroll
+      for (int i = 0; i < CH; ++i) {
+        const int z = k * CH + i;
+        o[i] = pair == 0 ? (T)va[z] - (T)vb[z] : (T)vb[z];
+      }
+      d16_st<T>(tile + d16_chunk(t, k, CH), o);
+    }
+  }
+  __syncthreads();
+  d16_store_rows<T>(tile, pair == 0 ? len0 : len1, nb, (pair == 0 ? lm1_out : f1_out) + e0);
 }
 
 }  // namespace nw

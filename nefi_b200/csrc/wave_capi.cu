@@ -193,7 +193,10 @@ int snap_codec_d16(const nw_grid* g, const SnapLayout& L, int n_shots, char* bas
   float* steps = (float*)(base + L.vals_bytes);
   float* anchors = (float*)(base + L.vals_bytes + L.scale_bytes);
   const int slots = g->absorbing == NW_ABS_PML ? 4 : 2;
-  const unsigned gx = (unsigned)((L.nblk + 8 * nw::SNAP_WARP_BLOCKS - 1) / (8 * nw::SNAP_WARP_BLOCKS));
+  if (g->field_elems % nw::SNAP_BLOCK != 0 || g->origin % nw::SNAP_BLOCK != 0)
+    return fail(NW_ERR_UNSUPPORTED, "delta16 snapshots need fields and rows on multiples of 32 elements");
+  constexpr int blk = nw::D16Cta<T>::BLK;
+  const unsigned gx = (unsigned)((L.nblk + blk - 1) / blk);
   if (encode) {
     nw::snap_encode_d16<T><<<dim3(gx, n_shots, slots), 256, 0, s>>>(
         lm1, l0, slots == 4 ? faces[0] : nullptr, slots == 4 ? faces[1] : nullptr, g->field_elems, L.nblk, vals,
@@ -1081,12 +1084,19 @@ int nw_initial_state(const nw_grid* g, const int32_t* n_abs, const nw_medium* m,
   return NW_OK;
 }
 
+// The step kernels and the snapshot codecs move fields in 16-byte vectors.
+static bool misaligned16(const void* p) { return ((uintptr_t)p & 15u) != 0; }
+
 static int check_run(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, const nw_time* t,
                      const nw_storage* st, const Tune& tu) {
   int rc = check_grid(g);
   if (rc) return rc;
   if (!m || !a || !t || !st) return fail(NW_ERR_ARG, "NULL descriptor");
   if (!m->c2dt2) return fail(NW_ERR_ARG, "medium.c2dt2 is NULL");
+  if (misaligned16(m->c2dt2) || misaligned16(m->coef_a) || misaligned16(m->coef_b) ||
+      misaligned16(st->history) || misaligned16(st->ring) || misaligned16(st->snap) ||
+      misaligned16(st->segbuf) || misaligned16(st->pml_psi))
+    return fail(NW_ERR_ARG, "device buffers must start on 16-byte boundaries");
   if ((g->absorbing != NW_ABS_NONE) != (m->coef_a != nullptr) || (m->coef_a == nullptr) != (m->coef_b == nullptr))
     return fail(NW_ERR_ARG, "absorbing coefficients must be given exactly when absorbing != none");
   if (a->n_shots < 1) return fail(NW_ERR_ARG, "n_shots must be >= 1");
@@ -1163,6 +1173,8 @@ int nw_adjoint(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, co
   rc = check_run(g, m, a, t, st, tu);
   if (rc) return rc;
   if (!grad_traces || !work || !grad_acc) return fail(NW_ERR_ARG, "NULL adjoint buffer");
+  if (misaligned16(work) || misaligned16(grad_acc) || misaligned16(lambda0) || misaligned16(mu1))
+    return fail(NW_ERR_ARG, "device buffers must start on 16-byte boundaries");
   if (a->n_cells > 0 && (!a->cell_index || !a->cell_ptr || !a->cell_rec || !a->cell_weight))
     return fail(NW_ERR_ARG, "receiver adjoint table is NULL");
   if (!st->history && st->snap && !st->segbuf) return fail(NW_ERR_ARG, "checkpointing needs segbuf");
