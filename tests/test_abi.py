@@ -144,3 +144,26 @@ def test_grid_validation_runs_before_any_device_call(lib):
              (dict(n=(50000, 50000, 1)), _lib.NW_ERR_ARG)]
     for kw, rc in cases:
         assert lib.nw_tile_shape(C.byref(grid(**kw)), C.byref(t), shape) == rc, kw
+
+
+def test_misaligned_device_buffers_are_refused_on_the_host(lib):
+    """Fields move in 16-byte vectors: a medium or storage buffer off a 16-byte boundary is refused
+    before any launch (the addresses below are never dereferenced)."""
+    g = _lib.Grid()
+    g.ndim, g.order, g.dtype, g.absorbing = 2, 4, _lib.NW_F32, _lib.NW_ABS_SPONGE
+    g.n[0], g.n[1], g.n[2] = 64, 64, 1
+    assert lib.nw_grid_layout(C.byref(g)) == _lib.NW_OK
+    a = _lib.Acquisition()
+    a.n_shots = 1
+    t = _lib.Time()
+    t.substeps, t.n_t, t.n_steps = 1, 2, 1
+    for bad in ("c2dt2", "coef_a", "ring", "segbuf", "snap"):
+        m = _lib.Medium()
+        m.c2dt2, m.coef_a, m.coef_b = 0x10000, 0x20000, 0x30000
+        st = _lib.Storage()
+        st.ring = 0x40000
+        target = m if bad in ("c2dt2", "coef_a") else st
+        setattr(target, bad, 0x50004)
+        rc = lib.nw_forward(C.byref(g), C.byref(m), C.byref(a), C.byref(t), C.byref(st), None, 0, 1, None, None)
+        assert rc == _lib.NW_ERR_ARG, bad
+        assert b"16-byte" in lib.nw_last_error(), bad
