@@ -96,6 +96,16 @@ __device__ __forceinline__ void gather_receivers(const T* __restrict__ lvl, T* _
 // Small kernels: receiver gather, adjoint injection, medium/initial-state preparation,
 // gradient reduction and the snapshot codec.
 // ------------------------------------------------------------------------------------------
+// The sample of receiver r in the field p (its NPTS stencil points, in table order).
+template <typename T, int NPTS>
+__device__ __forceinline__ T sample_point(const T* __restrict__ p, const int64_t* __restrict__ idx,
+                                          const T* __restrict__ w, int r) {
+  T acc = T(0);
+#pragma unroll
+  for (int k = 0; k < NPTS; ++k) acc += w[(long long)r * NPTS + k] * p[idx[(long long)r * NPTS + k]];
+  return acc;
+}
+
 template <typename T, int NPTS>
 __global__ void sample_kernel(const T* __restrict__ lvl, long long field, T* __restrict__ traces,
                               const int64_t* __restrict__ idx, const T* __restrict__ w, int n_rec,
@@ -105,11 +115,7 @@ __global__ void sample_kernel(const T* __restrict__ lvl, long long field, T* __r
   const int s = blockIdx.y;
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n_rec) return;
-  const T* p = lvl + (long long)s * field;
-  T acc = T(0);
-#pragma unroll
-  for (int k = 0; k < NPTS; ++k) acc += w[(long long)r * NPTS + k] * p[idx[(long long)r * NPTS + k]];
-  traces[((long long)s * n_rec + r) * n_t + j] = acc;
+  traces[((long long)s * n_rec + r) * n_t + j] = sample_point<T, NPTS>(lvl + (long long)s * field, idx, w, r);
 }
 
 // out[s][cell] += (apply_a ? A[cell] : 1) * C[cell] * sum_e w_e g[s, rec_e, j], cells in CSR order

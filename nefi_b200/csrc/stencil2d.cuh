@@ -35,9 +35,8 @@
 
 namespace nw {
 
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+__device__ __forceinline__ void cp_async16(unsigned smem, const void* gmem) {  // smem: shared-window address
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
@@ -190,11 +189,11 @@ struct Tile2Shape {
   static constexpr int NSA = (sizeof(T) == 8 || RX >= 4) ? 2 : 3;
 };
 
-// The chunks one thread copies for one tile region: shared and global element offsets (the
-// global offset relative to a field's base; -1 marks a chunk outside the stored rows).
+// The chunks one thread copies for one tile region: the shared byte offset in the destination tile
+// and the global element offset relative to a field's base (-1 marks a chunk outside the stored rows).
 template <int NC>
 struct CopyPlan {
-  int soff[NC];
+  unsigned soff[NC];
   int goff[NC];
 };
 
@@ -211,7 +210,7 @@ __device__ __forceinline__ CopyPlan<Tile2Shape<T, VZ, RX, R>::NCH> plan_halo(con
     const int row = c / CPR, ch = c - row * CPR;
     const int x = x0 - R + row;
     const int z = z0 - S::HL + ch * S::EPC;
-    p.soff[i] = row * S::SW + ch * S::EPC;
+    p.soff[i] = (unsigned)((row * S::SW + ch * S::EPC) * sizeof(T));
     p.goff[i] = (c < S::HR * CPR && x >= -R && x < g.n0 + R && z < (int)g.s0)
                     ? (int)(g.origin + (long long)x * g.s0 + z) : -1;
   }
@@ -229,13 +228,16 @@ __device__ __forceinline__ CopyPlan<Tile2Shape<T, VZ, RX, R>::NCC> plan_core(con
     const int row = c / CPR, ch = c - row * CPR;
     const int x = x0 + row;
     const int z = z0 + ch * S::EPC;
-    p.soff[i] = row * S::TZ + ch * S::EPC;
+    p.soff[i] = (unsigned)((row * S::TZ + ch * S::EPC) * sizeof(T));
     p.goff[i] = (c < S::TX * CPR && x < g.n0 && z < (int)g.s0) ? (int)(g.origin + (long long)x * g.s0 + z) : -1;
   }
   return p;
 }
+// Shared-window address of a shared-memory pointer.
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+// Issues one thread's chunks of a tile: field is the global field, dst the tile's shared-window address.
 template <typename T, int NC>
-__device__ __forceinline__ void issue(const CopyPlan<NC>& p, const T* __restrict__ field, T* dst) {
+__device__ __forceinline__ void issue(const CopyPlan<NC>& p, const T* __restrict__ field, unsigned dst) {
 #pragma unroll
   for (int i = 0; i < NC; ++i)
     if (p.goff[i] >= 0) cp_async16(dst + p.soff[i], field + p.goff[i]);
@@ -314,10 +316,12 @@ __device__ __forceinline__ void fwd2d_body(const KGrid<T>& g, const Tiled2<T>& a
   // first shot's source corner, and p^{n-1}, which the step two launches back wrote (that launch
   // completed before the previous one passed its own wait, which had to happen before this one
   // could start) and which nothing writes until this step has finished reading it.
-  issue(pc, a.C, scc);  // once per CTA, in the first commit group
+  constexpr unsigned PSB = S::PS * sizeof(T);  // bytes of one halo tile of the ring
+  const unsigned sp_s = smem_addr(sp);
+  issue(pc, a.C, smem_addr(scc));  // once per CTA, in the first commit group
   if (layer_tile) {
-    issue(pc, a.A, sa);
-    issue(pc, a.B, sbb);
+    issue(pc, a.A, smem_addr(sa));
+    issue(pc, a.B, smem_addr(sbb));
   }
   T pv[RX][VZ];  // p^{n-1} of the owned cells, one shot ahead
 #pragma unroll
@@ -339,21 +343,30 @@ __device__ __forceinline__ void fwd2d_body(const KGrid<T>& g, const Tiled2<T>& a
   }
 #pragma unroll
   for (int i = 0; i < NS - 1; ++i) {  // one commit group per shot, empty groups included, so that
-    if (sb + i < se) issue(ph, a.cur + (long long)(sb + i) * g.field, sp + i * S::PS);
+    if (sb + i < se) issue(ph, a.cur + (long long)(sb + i) * g.field, sp_s + i * PSB);
     cp_async_commit();                // wait_group<NS-1> in the loop means "shot s has landed"
   }
   const T wc = g.wc, w1x = g.w1a, w1z = g.w1b, w2x = g.w2a, w2z = g.w2b;
 
+  // running per-shot state: the ring buffer of shot s, and the fields of shot s (stores), s + 1
+  // (p^{n-1} prefetch) and s + NS - 1 (the halo copy issued during shot s)
+  const long long fs = g.field;
+  int buf = 0;
+  const T* gcopy = a.cur + (long long)(sb + NS - 1) * fs;
+  T* nxt = a.next + (long long)sb * fs + cbase;
+  T* lpo = a.lap_out ? a.lap_out + (long long)sb * fs + cbase : nullptr;
+  const T* pvn = a.prev + (long long)sb * fs + cbase;  // advanced to shot s + 1 before use
   for (int s = sb; s < se; ++s) {
-    const int buf = (s - sb) % NS;
     cp_async_wait<NS - 2>();  // this thread's copies of shot s have landed
     __syncthreads();          // everyone's have, and every thread is done with shot s-1
     {
-      const int sn = s + NS - 1, nb = (sn - sb) % NS;  // nb: the buffer shot s-1 used
-      if (sn < se) issue(ph, a.cur + (long long)sn * g.field, sp + nb * S::PS);
+      const int nb = buf == 0 ? NS - 1 : buf - 1;  // the buffer shot s-1 used
+      if (s + NS - 1 < se) issue(ph, gcopy, sp_s + nb * PSB);
       cp_async_commit();
+      gcopy += fs;
     }
     const T* P = sp + buf * S::PS;
+    pvn += fs;
 
     for (int e = e0 + threadIdx.x; e < e1; e += 256) {  // receiver samples of p^n
       const int r = a.tt.rec_list[e];
@@ -379,7 +392,6 @@ __device__ __forceinline__ void fwd2d_body(const KGrid<T>& g, const Tiled2<T>& a
       }
     }
     const bool more = s + 1 < se;
-    const long long so = (long long)s * g.field, sn = so + g.field;
 
     // sliding window: wv[q] holds tile row (lrow + k + q - R) (own columns only)
     T wv[2 * R + 1][VZ];
@@ -421,16 +433,18 @@ __device__ __forceinline__ void fwd2d_body(const KGrid<T>& g, const Tiled2<T>& a
         for (int v = 0; v < VZ; ++v) o[v] = mul_rn(ca[v], o[v]);
       }
       if (ok[k]) {
-        const long long ro = cbase + (long long)k * ld;
-        store_row<T, VZ>(a.next + so + ro, o, zc, a.z_end);
-        if (a.lap_out) store_row<T, VZ>(a.lap_out + so + ro, lp, zc, a.z_end);
-        if (more) vldg<T, VZ>(a.prev + sn + ro, pv[k]);  // in flight while the rest of this shot runs
+        store_row<T, VZ>(nxt + k * ld, o, zc, a.z_end);
+        if (lpo) store_row<T, VZ>(lpo + k * ld, lp, zc, a.z_end);
+        if (more) vldg<T, VZ>(pvn + k * ld, pv[k]);  // in flight while the rest of this shot runs
       }
 #pragma unroll
       for (int q = 0; q < 2 * R; ++q)
 #pragma unroll
         for (int v = 0; v < VZ; ++v) wv[q][v] = wv[q + 1][v];
     }
+    nxt += fs;
+    if (lpo) lpo += fs;
+    buf = buf + 1 == NS ? 0 : buf + 1;
   }
 }
 
@@ -470,10 +484,12 @@ __device__ __forceinline__ void adj2d_body(const KGrid<T>& g, const Tiled2<T>& a
   const CopyPlan<S::NCC> pc = plan_core<T, VZ, RX, R>(g, x0, z0);
   // once per CTA, in the first commit group: C, A and B (layer tiles), constant over the sweep, so
   // issued before the wait while the previous step finishes
-  issue(pc, a.C, scc);
+  constexpr unsigned PSB = S::PS * sizeof(T), QSB = S::QS * sizeof(T);  // bytes of a halo / core tile
+  const unsigned sp_s = smem_addr(sp), sq_s = smem_addr(sq), sl_s = smem_addr(sl);
+  issue(pc, a.C, smem_addr(scc));
   if (layer_tile) {
-    issue(pc, a.A, sa);
-    issue(pc, a.B, sbb);
+    issue(pc, a.A, smem_addr(sa));
+    issue(pc, a.B, smem_addr(sbb));
   }
   int c0 = 0, c1 = 0;
   if (a.gtr) { c0 = a.tt.cell_ptr[tile]; c1 = a.tt.cell_ptr[tile + 1]; }
@@ -506,17 +522,17 @@ __device__ __forceinline__ void adj2d_body(const KGrid<T>& g, const Tiled2<T>& a
 #pragma unroll
   for (int i = 0; i < NS - 1; ++i)
     if (sb + i < se) {
-      issue(pc, a.prev + (long long)(sb + i) * g.field, sq + i * S::QS);
-      if (grad && a.lap_ready) issue(pc, a.lap + (long long)(sb + i) * g.field, sl + i * S::QS);
+      issue(pc, a.prev + (long long)(sb + i) * g.field, sq_s + i * QSB);
+      if (grad && a.lap_ready) issue(pc, a.lap + (long long)(sb + i) * g.field, sl_s + i * QSB);
     }
   wait_previous_grid();
   allow_next_grid();
-  if (grad) issue(pc, a.gacc + (long long)bz * g.field, sg);  // the previous step updated it
+  if (grad) issue(pc, a.gacc + (long long)bz * g.field, smem_addr(sg));  // the previous step updated it
 #pragma unroll
   for (int i = 0; i < NS - 1; ++i) {  // one commit group per shot, empty groups included, so that
     if (sb + i < se) {                // wait_group<NS-1> in the loop means "shot s has landed"
-      issue(ph, a.cur + (long long)(sb + i) * g.field, sp + i * S::PS);
-      if (grad && !a.lap_ready) issue(pc, a.lap + (long long)(sb + i) * g.field, sl + i * S::QS);
+      issue(ph, a.cur + (long long)(sb + i) * g.field, sp_s + i * PSB);
+      if (grad && !a.lap_ready) issue(pc, a.lap + (long long)(sb + i) * g.field, sl_s + i * QSB);
     }
     cp_async_commit();
   }
@@ -531,8 +547,19 @@ __device__ __forceinline__ void adj2d_body(const KGrid<T>& g, const Tiled2<T>& a
 #pragma unroll
     for (int v = 0; v < VZ; ++v) gsum[k][v] = T(0);
 
+  // running per-shot state: the ring buffer of shot s, the output of shot s and the fields of shot
+  // s + NS - 1, whose copies are issued during shot s
+  const long long fs = g.field;
+  int buf = 0;
+  const long long cofs = (long long)(sb + NS - 1) * fs;
+  const T* gcur = a.cur + cofs;
+  const T* gprev = a.prev + cofs;
+  const T* glap = grad ? a.lap + cofs : gprev;  // (not read without a gradient)
+  T* ob = a.next + (long long)sb * fs + cbase;
+  bool okr[RX];  // row k of the owned cells lies in the grid
+#pragma unroll
+  for (int k = 0; k < RX; ++k) okr[k] = own_cols && xr + k < a.x_end;
   for (int s = sb; s < se; ++s) {
-    const int buf = (s - sb) % NS;
     // this shot's cotangent half; shot s-2 read it last, and every thread finished shot s-2 before
     // the previous barrier, so it is free; the same thread sets the same cells every shot
     T* sjs = sj + ((s - sb) & 1) * S::QS;
@@ -556,13 +583,16 @@ __device__ __forceinline__ void adj2d_body(const KGrid<T>& g, const Tiled2<T>& a
     }
     __syncthreads();  // every thread's copies and cotangents of shot s are in place; shot s-1 is done
     {
-      const int sn = s + NS - 1, nb = (sn - sb) % NS;  // nb: the buffer shot s-1 used
-      if (sn < se) {
-        issue(ph, a.cur + (long long)sn * g.field, sp + nb * S::PS);
-        issue(pc, a.prev + (long long)sn * g.field, sq + nb * S::QS);
-        if (grad) issue(pc, a.lap + (long long)sn * g.field, sl + nb * S::QS);
+      const int nb = buf == 0 ? NS - 1 : buf - 1;  // the buffer shot s-1 used
+      if (s + NS - 1 < se) {
+        issue(ph, gcur, sp_s + nb * PSB);
+        issue(pc, gprev, sq_s + nb * QSB);
+        if (grad) issue(pc, glap, sl_s + nb * QSB);
       }
       cp_async_commit();
+      gcur += fs;
+      gprev += fs;
+      glap += fs;
     }
     const T* P = sp + buf * S::PS;
     const T* Q = sq + buf * S::QS;
@@ -571,7 +601,6 @@ __device__ __forceinline__ void adj2d_body(const KGrid<T>& g, const Tiled2<T>& a
     T wv[2 * R + 1][VZ];  // sliding window over q^{n+1}, own columns
 #pragma unroll
     for (int q = 0; q < 2 * R; ++q) vload<T, VZ>(P + (lrow + q) * S::SW + S::HL + lane * VZ, wv[q]);
-    T* ob = a.next + (long long)s * g.field + cbase;
 #pragma unroll
     for (int k = 0; k < RX; ++k) {
       const int prow = lrow + k + R;
@@ -585,8 +614,6 @@ __device__ __forceinline__ void adj2d_body(const KGrid<T>& g, const Tiled2<T>& a
       T q2[VZ], cc[VZ];
       vload<T, VZ>(Q + toff, q2);
       vload<T, VZ>(scc + toff, cc);
-      const int x = xr + k;
-      const bool ok = own_cols && x < a.x_end;
       T ca[VZ], cb[VZ], inj[VZ];
 #pragma unroll
       for (int v = 0; v < VZ; ++v) { ca[v] = T(1); cb[v] = T(1); inj[v] = T(0); }
@@ -611,12 +638,14 @@ __device__ __forceinline__ void adj2d_body(const KGrid<T>& g, const Tiled2<T>& a
 #pragma unroll
         for (int v = 0; v < VZ; ++v) gsum[k][v] = fma_rn(wv[R][v], gl[v], gsum[k][v]);
       }
-      if (ok) store_row<T, VZ>(ob + (long long)k * ld, o, zc, a.z_end);
+      if (okr[k]) store_row<T, VZ>(ob + k * ld, o, zc, a.z_end);
 #pragma unroll
       for (int q = 0; q < 2 * R; ++q)
 #pragma unroll
         for (int v = 0; v < VZ; ++v) wv[q][v] = wv[q + 1][v];
     }
+    ob += fs;
+    buf = buf + 1 == NS ? 0 : buf + 1;
   }
   if (grad && own_cols) {  // the accumulator tile landed with the first commit group
     T* gp = a.gacc + (long long)bz * g.field + cbase;
@@ -691,10 +720,10 @@ __device__ __forceinline__ void fwd2t_body(const KGrid<T>& g, const Tiled2<T>& a
   const bool use_b2 = layer_tile;             // second step (n + 1 >= 1)
   const CopyPlan<S::NCH> ph = plan_halo<T, VZ, RX, R>(g, x0, z0);
   const CopyPlan<S::NCC> pc = plan_core<T, VZ, RX, R>(g, x0, z0);
-  issue(pc, a.C, scc);  // constants, before the wait (first commit group)
+  issue(pc, a.C, smem_addr(scc));  // constants, before the wait (first commit group)
   if (layer_tile) {
-    issue(pc, a.A, sa);
-    issue(pc, a.B, sbb);
+    issue(pc, a.A, smem_addr(sa));
+    issue(pc, a.B, smem_addr(sbb));
   }
   T pv[RX][VZ];  // p^{n-1} of the owned cells of E, one shot ahead
 #pragma unroll
@@ -717,7 +746,7 @@ __device__ __forceinline__ void fwd2t_body(const KGrid<T>& g, const Tiled2<T>& a
   }
 #pragma unroll
   for (int i = 0; i < NS - 1; ++i) {
-    if (sb + i < se) issue(ph, a.cur + (long long)(sb + i) * g.field, sp + i * S::PS);
+    if (sb + i < se) issue(ph, a.cur + (long long)(sb + i) * g.field, smem_addr(sp + i * S::PS));
     cp_async_commit();
   }
   const T wc = g.wc, w1x = g.w1a, w1z = g.w1b, w2x = g.w2a, w2z = g.w2b;
@@ -728,7 +757,7 @@ __device__ __forceinline__ void fwd2t_body(const KGrid<T>& g, const Tiled2<T>& a
     __syncthreads();  // shot s landed; every thread is done with shot s-1 (its halo buffer and sq)
     {
       const int sn = s + NS - 1, nb = (sn - sb) % NS;
-      if (sn < se) issue(ph, a.cur + (long long)sn * g.field, sp + nb * S::PS);
+      if (sn < se) issue(ph, a.cur + (long long)sn * g.field, smem_addr(sp + nb * S::PS));
       cp_async_commit();
     }
     const T* P = sp + buf * S::PS;

@@ -45,7 +45,7 @@ __device__ __forceinline__ CopyPlan<Tile3Shape<T, VZ, R>::NCH> plan_plane(const 
     const int row = c / CPR, ch = c - row * CPR;
     const int y = y0 - R + row;
     const int z = z0 - S::HL + ch * S::EPC;
-    p.soff[i] = row * S::SW + ch * S::EPC;
+    p.soff[i] = (unsigned)((row * S::SW + ch * S::EPC) * sizeof(T));
     p.goff[i] = (c < S::HR * CPR && y < g.n1 + R && z < (int)g.s1) ? (int)(g.origin + (long long)y * g.s1 + z) : -1;
   }
   return p;
@@ -57,6 +57,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 3 : 4) step3t(KGrid<T> g
   constexpr int NSP = S::NSP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* ring = reinterpret_cast<T*>(smem_raw);  // [NSP][PS]
+  const unsigned ring_sa = smem_addr(ring);
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int tiles_z = (g.n2 + S::TZ - 1) / S::TZ;
@@ -75,7 +76,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 3 : 4) step3t(KGrid<T> g
   // plane p - R - 1 (NSP = R + 3), the centre of the previous iteration.
   const int xa = x0 - R, xb = x1 + R;
   auto issue_plane = [&](int p) {
-    if (p >= 0 && p < g.n0 && p < xb) issue(pp, cur + (long long)p * g.s0, ring + ((p - xa) % NSP) * S::PS);
+    if (p >= 0 && p < g.n0 && p < xb) issue(pp, cur + (long long)p * g.s0, ring_sa + ((p - xa) % NSP) * (unsigned)(S::PS * sizeof(T)));
   };
   wait_previous_grid();
   allow_next_grid();

@@ -480,10 +480,12 @@ void pml_medium(const nw_medium* m, nw::PmlStep<T>& st) {
 template <typename T, bool ADJ>
 int launch_pml(const nw_grid* g, const nw::KGrid<T>& kg, const nw::PmlStep<T>& st, int n_shots, cudaStream_t s) {
   const long long cells = (long long)g->n[0] * g->n[1] - (long long)(st.kx1 - st.kx0) * (st.kz1 - st.kz0);
-  if (cells <= 0) return NW_OK;
-  const dim3 grid((unsigned)((cells + 255) / 256), n_shots);
-  if (g->radius == 1) return launch_pdl(nw::pml2d_step<T, 1, ADJ>, grid, 0, s, kg, st);
-  return launch_pdl(nw::pml2d_step<T, 2, ADJ>, grid, 0, s, kg, st);
+  if (cells <= 0 && !st.traces) return NW_OK;
+  // a CTA per row and shot, and with st.traces the CTAs that take the receiver samples
+  const int rec_ctas = st.traces ? (st.n_rec + nw::PML_THREADS - 1) / nw::PML_THREADS : 0;
+  const dim3 grid((unsigned)(g->n[0] + rec_ctas), n_shots), block(nw::PML_THREADS);
+  if (g->radius == 1) return launch_pdl_b(nw::pml2d_step<T, 1, ADJ>, grid, block, 0, s, kg, st);
+  return launch_pdl_b(nw::pml2d_step<T, 2, ADJ>, grid, block, 0, s, kg, st);
 }
 
 // A second stream of the calling thread on the current device, with a fork and a join event: a PML
@@ -629,12 +631,16 @@ int forward_step(const nw_grid* g, const nw::KGrid<T>& kg, const nw_medium* m, c
                  cudaStream_t s, T* psi = nullptr, bool prev_ready = false) {
   const bool rec = traces && a->n_rec > 0 && (n % t->substeps) == 0;
   if (g->absorbing == NW_ABS_PML) {  // 2-D with the reference's PML: psi levels 2*axis + parity
-    if (rec) {
-      int rc = launch_sample<T>(g, a, t->n_t, L.at(n), n / t->substeps, traces, s);
-      if (rc) return rc;
-    }
     const long long LE = (long long)a->n_shots * g->field_elems;
     nw::PmlStep<T> st = {};
+    if (rec) {  // the layer kernel's launch also takes the receiver samples of p^n
+      st.traces = traces;
+      st.rec_idx = a->rec_index;
+      st.rec_w = (const T*)a->rec_weight;
+      st.n_rec = (int)a->n_rec;
+      st.n_t = t->n_t;
+      st.j = n / t->substeps;
+    }
     st.prev = L.at(n - 1);
     st.cur = L.at(n);
     st.next = L.at(n + 1);
