@@ -72,19 +72,14 @@ struct Step3 {
   T* __restrict__ grad;                // adjoint: per-shot accumulators of C dJ/dC
 };
 
-__device__ __forceinline__ long long global_thread_in_shot() {
-  return ((long long)blockIdx.y * gridDim.x + blockIdx.x) * (blockDim.x * blockDim.y) +
-         threadIdx.y * blockDim.x + threadIdx.x;
-}
-
-// Receiver gather of one level for shot s: traces[s, r, j] = sum_k w_rk p[idx_rk].
+// Receiver gather of one level for shot s by the `nthr` threads of the launch that work on that shot
+// (this thread is number `thr` of them): traces[s, r, j] = sum_k w_rk p[idx_rk].
 template <typename T, int NPTS>
 __device__ __forceinline__ void gather_receivers(const T* __restrict__ lvl, T* __restrict__ traces,
                                                  const int64_t* __restrict__ idx,
                                                  const T* __restrict__ w, int n_rec, int n_t, int j,
-                                                 int s) {
-  const long long nthr = (long long)gridDim.x * gridDim.y * blockDim.x * blockDim.y;
-  for (long long r = global_thread_in_shot(); r < n_rec; r += nthr) {
+                                                 int s, long long thr, long long nthr) {
+  for (long long r = thr; r < n_rec; r += nthr) {
     T acc = T(0);
 #pragma unroll
     for (int k = 0; k < NPTS; ++k) acc += w[r * NPTS + k] * lvl[idx[r * NPTS + k]];

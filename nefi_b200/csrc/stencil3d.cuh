@@ -52,7 +52,7 @@ __device__ __forceinline__ CopyPlan<Tile3Shape<T, VZ, R>::NCH> plan_plane(const 
 }
 
 template <typename T, int R, int VZ, bool ADJ>
-__global__ void __launch_bounds__(256, sizeof(T) == 8 ? 3 : 4) step3t(KGrid<T> g, Step3<T> a, int xc) {
+__global__ void __launch_bounds__(256, sizeof(T) == 8 ? 3 : 4) step3t(KGrid<T> g, Step3<T> a, int xc, int n_shots) {
   using S = Tile3Shape<T, VZ, R>;
   constexpr int NSP = S::NSP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -60,10 +60,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 3 : 4) step3t(KGrid<T> g
   const unsigned ring_sa = smem_addr(ring);
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // grid.x = tile * n_shots + shot (the shot fastest, so that the CTAs of one tile for all shots run
+  // together and the shot-independent fields C, A, B come from L2 after the first), grid.y = x chunk
   const int tiles_z = (g.n2 + S::TZ - 1) / S::TZ;
-  const int z0 = (blockIdx.x % tiles_z) * S::TZ, y0 = (blockIdx.x / tiles_z) * S::TY;
+  const int s = blockIdx.x % n_shots, tile = blockIdx.x / n_shots;
+  const int z0 = (tile % tiles_z) * S::TZ, y0 = (tile / tiles_z) * S::TY;
   const int x0 = blockIdx.y * xc, x1 = min(x0 + xc, g.n0);
-  const int s = blockIdx.z;
   const long long so = (long long)s * g.field;
   const int y = y0 + warp, zc = z0 + lane * VZ;
   const bool own = y < g.n1 && zc < g.n2;
@@ -80,7 +82,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 3 : 4) step3t(KGrid<T> g
   };
   wait_previous_grid();
   allow_next_grid();
-  if (!ADJ && a.traces) gather_receivers<T, 8>(cur, a.traces, a.rec_idx, a.rec_w, a.n_rec, a.n_t, a.j, s);
+  if (!ADJ && a.traces)
+    gather_receivers<T, 8>(cur, a.traces, a.rec_idx, a.rec_w, a.n_rec, a.n_t, a.j, s,
+                           ((long long)blockIdx.y * (gridDim.x / n_shots) + tile) * blockDim.x + threadIdx.x,
+                           (long long)(gridDim.x / n_shots) * gridDim.y * blockDim.x);
   issue_plane(xa);  // one commit group per plane, empty groups included
   cp_async_commit();
   issue_plane(xa + 1);

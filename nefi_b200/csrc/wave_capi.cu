@@ -418,10 +418,11 @@ template <typename T, int R, bool ADJ>
 int launch_step3_r(const nw_grid* g, const nw::KGrid<T>& kg, const nw::Step3<T>& st, int n_shots, cudaStream_t s) {
   using S = nw::Tile3Shape<T, 2, R>;
   const int tz = (g->n[2] + S::TZ - 1) / S::TZ, ty = (g->n[1] + S::TY - 1) / S::TY;
-  const dim3 grid(tz * ty, (g->n[0] + kXChunk - 1) / kXChunk, n_shots);
+  if ((long long)tz * ty * n_shots > INT_MAX) return fail(NW_ERR_UNSUPPORTED, "3-D grid: too many tiles x shots");
+  const dim3 grid((unsigned)((long long)tz * ty * n_shots), (g->n[0] + kXChunk - 1) / kXChunk);  // shot fastest
   constexpr size_t smem = (size_t)S::NSP * S::PS * sizeof(T);
   static_assert(smem <= 48 * 1024, "plane ring above the default shared-memory limit");
-  return launch_pdl(nw::step3t<T, R, 2, ADJ>, grid, smem, s, kg, st, kXChunk);
+  return launch_pdl(nw::step3t<T, R, 2, ADJ>, grid, smem, s, kg, st, kXChunk, n_shots);
 }
 template <typename T, bool ADJ>
 int launch_step3(const nw_grid* g, const nw::KGrid<T>& kg, const nw::Step3<T>& st, bool ab, int n_shots,

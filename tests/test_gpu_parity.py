@@ -9,6 +9,8 @@ Tolerances (relative L2):
 
 from __future__ import annotations
 
+from pathlib import Path
+
 import numpy as np
 import pytest
 import torch
@@ -536,53 +538,47 @@ def test_pml_forward_captured_in_a_fresh_thread(cuda_device):
 
 @pytest.mark.parametrize("seed", range(8))
 @pytest.mark.parametrize("dtype,tt,tg", [(torch.float64, 1e-11, 1e-10), (torch.float32, 1e-5, 1e-4)])
-def test_random_geometries_match_the_oracle(seed, dtype, tt, tg, cuda_device):
-    """Seeded random 2-D geometries (grid shape and spacing, every layer kind, order, substeps,
-    several shots, receivers anywhere in the domain, long enough for the wave to cross the domain)
-    through the device path against the float64 oracle: traces and the gradient of
-    ``sum(traces * g)``."""
-    import random
-
+def test_random_geometries_match_the_oracle_and_the_reference(seed, dtype, tt, tg, cuda_device):
+    """Seeded random 2-D geometries (tests/random_geometry.py: grid shape and spacing, every layer
+    kind, order, substeps, several shots, receivers anywhere, long enough for the wave to cross the
+    domain) through the device path: traces and the gradient of ``sum(traces * g)`` against the
+    float64 oracle, and in float32 also against the reference's own float32 and float64 runs of the
+    same problems (tests/golden/random/random_<seed>.npz, written by make_random_golden.py)."""
     import oracle
+    from random_geometry import random_geometry
 
-    rnd = random.Random(seed)
-    n0, n1 = rnd.randint(10, 90), rnd.randint(10, 170)
-    h0, h1 = rnd.choice([0.04, 0.05]), rnd.choice([0.04, 0.05])
-    ext = ((0.0, n0 * h0), (0.0, n1 * h1))
-    absorbing = ["none", "sponge", "cerjan", "pml"][seed % 4]
-    width = 0.0 if absorbing == "none" else rnd.choice([0.1, 0.2])
-    lo = 0.5 * max(h0, h1) if absorbing == "none" else 0.0
-
-    def point():
-        return [rnd.uniform(lo, n0 * h0 - lo), rnd.uniform(lo, n1 * h1 - lo)]
-
-    src = [point() for _ in range(rnd.randint(1, 5))]
-    rec = [point() for _ in range(rnd.randint(1, 12))]
-    dt_obs = rnd.choice([0.01, 0.02])  # long enough for the wave to cross the domain once
-    n_t = int((n0 * h0 + n1 * h1) / 1.6 / dt_obs) + 10
-    kw = dict(n_t=n_t, dt_obs=dt_obs, f0=rnd.choice([4.0, 6.0]), c_max=2.5,
-              order=rnd.choice([2, 4]), absorbing=absorbing, absorb_width=width)
-    g = np.random.default_rng(seed)
-    c = np.clip(2.0 + 0.2 * g.standard_normal((n0, n1)), 1.6, 2.4)
-    gt = g.standard_normal((len(src), len(rec), kw["n_t"]))
+    p = random_geometry(seed)
+    (n0, n1), ext, src, rec, kw, c, gt = p["shape"], p["extent"], p["sources"], p["receivers"], p["kw"], p["c"], p["gt"]
     op = WaveOperatorB200(Domain((n0, n1), ext), src, rec, grad_mode="autograd", **kw)
     cd = torch.tensor(c, dtype=dtype, device=cuda_device).requires_grad_(True)
     tr = op({"c": cd})
     (gc,) = torch.autograd.grad((tr * torch.tensor(gt, dtype=dtype, device=cuda_device)).sum(), cd)
+    tr, gc = tr.detach().cpu().numpy(), gc.cpu().numpy()
     orc = oracle.OracleWave((n0, n1), ext, np.asarray(rec), sources=np.asarray(src), **kw)
     tr_o, gc_o = orc.fwi(c, gt, dtype=np.float64)
     assert np.linalg.norm(tr_o) > 0 and np.linalg.norm(gc_o) > 0  # the wave reaches the receivers
+    ref = np.load(Path(__file__).parent / "golden" / "random" / f"random_{seed}.npz")
     if dtype == torch.float32:
         # float32 rounding grows with the step count (up to 1200 steps here): the bound is twice the
-        # error of the same arithmetic in float32 on the host, the reference's own float32 path
-        tr32, gc32 = orc.fwi(c, gt, dtype=np.float32)
-        tt, tg = max(tt, 2.0 * rel_l2(tr32, tr_o)), max(tg, 2.0 * rel_l2(gc32, gc_o))
-        # a fixed ceiling, so that a drifting host error cannot hide a device regression
+        # reference's own float32 error against its float64 run of the same problem
+        r_tr, r_gc = rel_l2(ref["traces_f32"], ref["traces_f64"]), rel_l2(ref["grad_f32"], ref["grad_f64"])
+        tt, tg = max(tt, 2.0 * r_tr), max(tg, 2.0 * r_gc)
+        # a fixed ceiling, so that a drifting reference error cannot hide a device regression
         assert tt <= 1e-4 and tg <= 1e-3, (tt, tg)
-    e_tr, e_gc = rel_l2(tr.detach().cpu().numpy(), tr_o), rel_l2(gc.cpu().numpy(), gc_o)
-    print(f"seed {seed} {absorbing} {dtype}: traces {e_tr:.2e} (bound {tt:.1e}), gradient {e_gc:.2e} (bound {tg:.1e})")
-    assert e_tr < tt, (absorbing, kw)
-    assert e_gc < tg, (absorbing, kw)
+        d_tr, d_gc = rel_l2(tr, ref["traces_f64"]), rel_l2(gc, ref["grad_f64"])
+        v_tr, v_gc = rel_l2(tr, ref["traces_f32"]), rel_l2(gc, ref["grad_f32"])
+        print(f"seed {seed} {kw['absorbing']}: device float32 vs reference float64 traces {d_tr:.2e}, gradient "
+              f"{d_gc:.2e}; vs reference float32 {v_tr:.2e}, {v_gc:.2e}; reference float32 vs float64 "
+              f"{r_tr:.2e}, {r_gc:.2e}")
+        assert d_tr < tt and d_gc < tg, (kw, d_tr, d_gc)
+        assert v_tr < tt and v_gc < tg, (kw, v_tr, v_gc)
+    else:  # the fixtures are stored in float32: agreement to their rounding
+        assert rel_l2(tr, ref["traces_f64"]) < 1e-6 and rel_l2(gc, ref["grad_f64"]) < 1e-6
+    e_tr, e_gc = rel_l2(tr, tr_o), rel_l2(gc, gc_o)
+    print(f"seed {seed} {kw['absorbing']} {dtype}: vs the float64 oracle traces {e_tr:.2e} (bound {tt:.1e}), "
+          f"gradient {e_gc:.2e} (bound {tg:.1e})")
+    assert e_tr < tt, (kw["absorbing"], kw)
+    assert e_gc < tg, (kw["absorbing"], kw)
 
 
 def test_pat_float64_matches_the_oracle_on_a_96_cube(cuda_device):

@@ -146,3 +146,26 @@ def test_oracle_runs_in_shot_chunks_like_one_call():
     orc.HISTORY_BYTES = 1
     chunked = orc.fwi(case["c"], g)
     assert np.array_equal(one[0], chunked[0]) and np.array_equal(one[1], chunked[1])
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_oracle_matches_reference_on_random_geometries(seed):
+    """The float64 oracle against the reference's float64 runs of the seeded random geometries
+    (tests/golden/random/random_<seed>.npz, stored in float32: agreement to that rounding), and the oracle's
+    float32 arithmetic within twice the reference's own float32 error."""
+    from pathlib import Path
+
+    import oracle
+    from random_geometry import random_geometry
+
+    p = random_geometry(seed)
+    ref = np.load(Path(__file__).parent / "golden" / "random" / f"random_{seed}.npz")
+    orc = oracle.OracleWave(p["shape"], p["extent"], np.asarray(p["receivers"]), sources=np.asarray(p["sources"]),
+                            **p["kw"])
+    tr, gc = orc.fwi(p["c"], p["gt"], dtype=np.float64)
+    assert rel_l2(tr, ref["traces_f64"]) < 1e-6 and rel_l2(gc, ref["grad_f64"]) < 1e-6
+    tr32, gc32 = orc.fwi(p["c"], p["gt"], dtype=np.float32)
+    r_tr = rel_l2(ref["traces_f32"], ref["traces_f64"])
+    r_gc = rel_l2(ref["grad_f32"], ref["grad_f64"])
+    assert rel_l2(tr32, ref["traces_f64"]) < max(1e-5, 2 * r_tr)
+    assert rel_l2(gc32, ref["grad_f64"]) < max(1e-4, 2 * r_gc)
