@@ -55,37 +55,53 @@ struct PmlStep {
   T* __restrict__ grad;            // per-shot accumulators of C dJ/dC
 };
 
-// CTA (b, s), b < n0: the layer cells of one row for shot s (b >= n0: receiver samples, see below).
-// Rows entirely outside the tiled box (those above and below it) come first in b, so that their longer CTAs start early; then the rows beside the
-// box, whose layer cells are the strips left and right of it. A thread steps cells t, t + blockDim.x,
-// ... of its row. Offsets inside a field are 32-bit (a field holds fewer than 2^31 elements).
-constexpr int PML_THREADS = 64;
+// Thread t of shot s (grid.y) steps the t-th cell outside the tiled box, row by row: the rows above
+// it, the strips left and right of it, the rows below it. CTAs past the last cell take the receiver
+// samples of p^n on the forward's record steps (p^n is read-only in this step). Offsets inside a field
+// are 32-bit (a field holds fewer than 2^31 elements).
+constexpr int PML_THREADS = 256;
 
 template <typename T, int R, bool ADJ>
 __global__ void __launch_bounds__(PML_THREADS) pml2d_step(KGrid<T> g, PmlStep<T> a) {
   wait_previous_grid();
   allow_next_grid();
   const int s = blockIdx.y;
-  const int b = blockIdx.x;
-  if (b >= g.n0) {  // the receiver samples of p^n (CTAs past the rows; p^n is read-only in this step)
-    const int r = (b - g.n0) * PML_THREADS + threadIdx.x;
+  const int top = a.kx0 * g.n1;
+  const int bw = a.kz0 + (g.n1 - a.kz1);
+  const int mid = (a.kx1 - a.kx0) * bw;
+  const int n_layer = top + mid + (g.n0 - a.kx1) * g.n1;
+  const int cell_ctas = (n_layer + PML_THREADS - 1) / PML_THREADS;
+  if ((int)blockIdx.x >= cell_ctas) {  // the receiver samples
+    const int r = ((int)blockIdx.x - cell_ctas) * PML_THREADS + threadIdx.x;
     if (!ADJ && a.traces && r < a.n_rec)
       a.traces[((long long)s * a.n_rec + r) * a.n_t + a.j] =
           sample_point<T, 4>(a.cur + (long long)s * g.field, a.rec_idx, a.rec_w, r);
     return;
   }
-  const int n_top = a.kx0, n_full = a.kx0 + (g.n0 - a.kx1);
-  const int x = b < n_top ? b : (b < n_full ? a.kx1 + (b - n_top) : a.kx0 + (b - n_full));
-  const bool full = b < n_full;
-  const int n_cells = full ? g.n1 : a.kz0 + (g.n1 - a.kz1);
+  const int t = blockIdx.x * PML_THREADS + threadIdx.x;
+  if (t >= n_layer) return;
+  int x, z;
+  if (t < top) {
+    x = t / g.n1;
+    z = t - x * g.n1;
+  } else if (t < top + mid) {
+    const int u = t - top;
+    const int q = u / bw;
+    const int r = u - q * bw;
+    x = a.kx0 + q;
+    z = r < a.kz0 ? r : a.kz1 + (r - a.kz0);
+  } else {
+    const int u = t - top - mid;
+    x = a.kx1 + u / g.n1;
+    z = u - (x - a.kx1) * g.n1;
+  }
   const long long so = (long long)s * g.field;
   const T* __restrict__ pc = a.cur + so;
   const T* __restrict__ pp = a.prev + so;
   const int ld = (int)g.s0;
   const int row = (int)g.origin + x * ld;
   const bool core_row = x >= a.cx0 && x < a.cx1;
-  for (int u = threadIdx.x; u < n_cells; u += PML_THREADS) {
-    const int z = (full || u < a.kz0) ? u : a.kz1 + (u - a.kz0);
+  {
     const int i = row + z;
     const T c = pc[i];
     // 5- or 9-point Laplacian in the reference's zero-padded convolution (fixed rounding sequence)

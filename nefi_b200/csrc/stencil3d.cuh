@@ -1,8 +1,8 @@
 // stencil3d.cuh — plane-marching 3-D leapfrog step for sm_100a (forward and q-form adjoint).
 //
-// A CTA (8 warps) owns a (y, z) tile of 8 rows by TZ = 32*VZ columns and marches along x over a
-// chunk of XC planes. Warp w owns row y0 + w, lane l the VZ columns z0 + l*VZ. Every plane the
-// march touches passes once through a ring of NSP shared-memory tiles, (8 + 2R) rows by
+// A CTA (8 warps) owns a (y, z) tile of TY = 8 rows by TZ = 32*VZ columns and marches along x over
+// a chunk of XC planes. Warp w owns row y0 + w, lane l the VZ columns z0 + l*VZ. Every plane the
+// march touches passes once through a ring of NSP shared-memory tiles, (TY + 2R) rows by
 // TZ + 2*HL columns (the y/z halo), staged by cp.async two planes ahead of its first use (one
 // barrier per plane: a plane's copy is issued right after the barrier that frees its slot); the
 // x-neighbours of a thread's cells stay in a (2R+1)-plane register window, fed from the ring when a
@@ -19,14 +19,15 @@ namespace nw {
 
 template <typename T, int VZ, int R>
 struct Tile3Shape {
-  static constexpr int TY = 8;
+  static constexpr int NT = 256;                 // threads per CTA: one warp per tile row
+  static constexpr int TY = NT / 32;
   static constexpr int TZ = 32 * VZ;
   static constexpr int HL = 16 / (int)sizeof(T);
   static constexpr int SW = TZ + 2 * HL;
   static constexpr int EPC = 16 / (int)sizeof(T);
   static constexpr int HR = TY + 2 * R;
   static constexpr int PS = HR * SW;                        // elements of a plane tile
-  static constexpr int NCH = (HR * (SW / EPC) + 255) / 256;  // chunks per thread and plane
+  static constexpr int NCH = (HR * (SW / EPC) + NT - 1) / NT;  // chunks per thread and plane
   static constexpr int NSP = R + 3;                          // planes in the ring
 };
 
@@ -41,7 +42,7 @@ __device__ __forceinline__ CopyPlan<Tile3Shape<T, VZ, R>::NCH> plan_plane(const 
   CopyPlan<S::NCH> p;
 #pragma unroll
   for (int i = 0; i < S::NCH; ++i) {
-    const int c = threadIdx.x + 256 * i;
+    const int c = threadIdx.x + S::NT * i;
     const int row = c / CPR, ch = c - row * CPR;
     const int y = y0 - R + row;
     const int z = z0 - S::HL + ch * S::EPC;
@@ -52,7 +53,7 @@ __device__ __forceinline__ CopyPlan<Tile3Shape<T, VZ, R>::NCH> plan_plane(const 
 }
 
 template <typename T, int R, int VZ, bool ADJ>
-__global__ void __launch_bounds__(256, sizeof(T) == 8 ? 3 : 4) step3t(KGrid<T> g, Step3<T> a, int xc, int n_shots) {
+__global__ void __launch_bounds__(Tile3Shape<T, VZ, R>::NT, sizeof(T) == 8 ? 3 : 4) step3t(KGrid<T> g, Step3<T> a, int xc, int n_shots) {
   using S = Tile3Shape<T, VZ, R>;
   constexpr int NSP = S::NSP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
