@@ -185,7 +185,7 @@ def measure_batch(dev, world: int, rank: int, n_problems: int = 64, steps: int =
         obs = [op({"c": torch.nn.functional.avg_pool2d(c[None, None], 9, 1, 4, count_include_pad=False)[0, 0]
                          .contiguous()}) for op, c in zip(ops, cs)]
     t0 = time.perf_counter()
-    tuning, _ = autotune(ops, steps=40, device=dev, repeats=1, snapshot=snapshot)
+    tuning, _ = autotune(ops, steps=200, device=dev, repeats=2, snapshot=snapshot)
     t_tune = time.perf_counter() - t0
     bt = BatchedFWI(ops, device=dev, snapshot=snapshot, tuning=tuning)
     bt.misfit_gradients(cs, obs)

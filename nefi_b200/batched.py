@@ -18,7 +18,6 @@ from __future__ import annotations
 
 import ctypes as C
 import math
-import time
 from collections.abc import Sequence
 
 import torch
@@ -214,11 +213,14 @@ def autotune(ops: Sequence[WaveOperatorB200], *, steps: int = 120, device="cuda"
              snapshot: str = "delta16", fwd_candidates=((4, 2, 2), (2, 4, 2), (4, 2, 1), (2, 2, 2), (4, 4, 1)),
              adj_candidates=((2, 2, 4), (2, 2, 2), (4, 2, 4), (2, 4, 4), (2, 2, 8)), repeats: int = 2):
     """Choose the forward and adjoint tile shapes ``(vz, rx, shots_per_cta)`` for a batch by timing
-    each candidate's sweep on a copy of the batch shortened to ``steps`` time steps (the per-step
-    cost does not depend on the step count). Returns the 6-tuple tuning and the timings."""
+    each candidate's sweep on the device over a copy of the batch shortened in time: the longest
+    problem to ``steps`` samples and every other one in proportion, so that the shortened batch runs
+    the same mix of problems over its steps as the real one (the per-step cost of a problem does
+    not depend on the step count). Returns the 6-tuple tuning and the timings (seconds)."""
     short = []
+    n_t_max = max(op.n_t for op in ops)
     for op in ops:
-        n_t = min(op.n_t, steps + 1)
+        n_t = max(2, min(op.n_t, round(op.n_t * (steps + 1) / n_t_max)))
         short.append(WaveOperatorB200(op.domain, op.sources, op.receivers, f0=op.f0, t0=op.t0,
                                       amplitude=op.amplitude, **{**op._kwargs(), "n_t": n_t}))
     dev = torch.device(device)
@@ -239,13 +241,14 @@ def autotune(ops: Sequence[WaveOperatorB200], *, steps: int = 120, device="cuda"
             _lib.check(lib.nw_batch_forward(bt.problems, n, C.byref(bt.tune), bt.table.data_ptr(), s))
         fn = lib.nw_batch_forward if which == "fwd" else lib.nw_batch_adjoint
         best = float("inf")
-        for r in range(repeats + 1):
-            torch.cuda.synchronize(dev)
-            t0 = time.perf_counter()
+        for r in range(repeats + 1):  # the device time of the sweep, the first run untimed
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
             _lib.check(fn(bt.problems, n, C.byref(bt.tune), bt.table.data_ptr(), s))
+            e1.record()
             torch.cuda.synchronize(dev)
             if r:
-                best = min(best, time.perf_counter() - t0)
+                best = min(best, e0.elapsed_time(e1) * 1e-3)
         bt.check_snapshots()
         del bt
         return best
