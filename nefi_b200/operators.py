@@ -484,6 +484,60 @@ class WaveOperatorB200(_LeapfrogB200):
             loss = j.clone()
         return loss, grad
 
+    FWD_CANDIDATES = ((4, 2, 2, 1), (4, 2, 1, 1), (2, 4, 2, 1), (4, 4, 2, 1), (4, 4, 2, 2), (4, 2, 2, 2))
+    ADJ_CANDIDATES = ((2, 2, 4), (2, 2, 8), (2, 4, 4), (2, 2, 2))
+
+    @_lib.on_device
+    def autotune(self, c: torch.Tensor, steps: int = 200, fwd_candidates=None, adj_candidates=None,
+                 repeats: int = 2) -> tuple:
+        """Choose this operator's 2-D launch shapes and forward steps per launch by timing candidates
+        on the device, on a copy of the operator shortened to about ``steps`` leapfrog steps (the
+        per-step cost does not depend on the step count). The forward candidates ``(vz, rx,
+        shots_per_cta, depth)`` are timed with the default adjoint shape, then the adjoint candidates
+        ``(vz, rx, shots_per_cta)`` with the forward chosen; depth 2 (two steps per launch) applies to
+        2-D grids without a PML and falls back to one step elsewhere. Candidates the library refuses
+        (a shape above the shared-memory limit, a float64 tile of four columns per thread) are
+        skipped. Sets ``self.tuning`` and returns it; ``self.autotune_results`` holds the microseconds
+        per step of each candidate. Traces are bitwise the same under every tuning; the gradient
+        regroups its float sums with the adjoint's shots per CTA."""
+        self._validate(c)
+        if len(self.domain.shape) != 2:
+            return getattr(self, "tuning", None)
+        n_t = max(2, min(self.n_t, steps // self.substeps + 1))
+        short = WaveOperatorB200(self.domain, self.sources, self.receivers, f0=self.f0, t0=self.t0,
+                                 amplitude=self.amplitude, **{**self._kwargs(), "n_t": n_t})
+        short.source_batch = self.source_batch
+        obs = torch.zeros(short.n_sources, short.n_receivers, short.n_t, device=c.device, dtype=c.dtype)
+        results = {}
+
+        def per_step(tuning):  # (forward, adjoint) microseconds per step, best of `repeats`
+            short.tuning = tuning
+            short._plans.clear()
+            fwd = adj = math.inf
+            try:
+                for r in range(repeats + 1):
+                    ev = {}
+                    short.misfit_gradient(c, obs, events=ev)
+                    torch.cuda.synchronize(c.device)
+                    if r:
+                        fwd = min(fwd, ev["fwd0"].elapsed_time(ev["fwd1"]) * 1e3 / short.n_steps)
+                        adj = min(adj, ev["adj0"].elapsed_time(ev["adj1"]) * 1e3 / short.n_steps)
+            except _lib.LibraryError:
+                return math.inf, math.inf
+            results[tuning] = (fwd, adj)
+            return fwd, adj
+
+        fwd_c = fwd_candidates or self.FWD_CANDIDATES
+        adj_c = adj_candidates or self.ADJ_CANDIDATES
+        best_f = min(fwd_c, key=lambda f: per_step((*f[:3], 0, 0, 0, f[3]))[0])
+        best_a = min(adj_c, key=lambda a: per_step((*best_f[:3], *a, best_f[3]))[1])
+        if math.isinf(results.get((*best_f[:3], *best_a, best_f[3]), (math.inf, math.inf))[1]):
+            raise ConfigError("autotune: the library refused every candidate launch shape")
+        self.tuning = (*best_f[:3], *best_a, best_f[3])
+        self._plans.clear()
+        self.autotune_results = results
+        return self.tuning
+
     @_lib.on_device
     def gradient_graph(self, c: torch.Tensor, observed: torch.Tensor, events: bool = False) -> "GradientGraph":
         """``misfit_gradient(c, observed)`` recorded once as a CUDA graph: a :class:`GradientGraph` whose

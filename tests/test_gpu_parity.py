@@ -386,6 +386,24 @@ def test_results_do_not_depend_on_the_launch_shape(dtype, cuda_device):
         assert rel_l2(g, g0) < (1e-12 if dtype == torch.float64 else 1e-5), shape
 
 
+def test_autotune_chooses_the_launch_shape_and_the_depth(cuda_device):
+    """The operator's autotuner times forward shapes with one and two steps per launch and adjoint
+    shapes, keeps the fastest, and the chosen tuning gives the default's traces bitwise and its
+    gradient up to the regrouped sums."""
+    op = _layered_op()
+    tr0, g0 = _layered_grad(op, torch.float32, cuda_device, None)
+    n = op.grid.shape[0]
+    x = torch.linspace(0, 1, n, dtype=torch.float64)
+    c = (2000.0 + 800.0 * x[None, :] + 150.0 * torch.sin(7 * x)[:, None]).to(torch.float32).to(cuda_device)
+    tu = op.autotune(c, steps=60, repeats=1)
+    assert len(tu) == 7 and tu[6] in (1, 2)
+    assert any(k[6] == 2 for k in op.autotune_results), "depth 2 is among the timed candidates"
+    assert all(f > 0 and a > 0 for f, a in op.autotune_results.values())
+    tr, g = _layered_grad(op, torch.float32, cuda_device, tu)
+    assert np.array_equal(tr, tr0)
+    assert rel_l2(g, g0) < 1e-5
+
+
 # (vz, rx, shots_per_cta) of the forward with two steps per launch
 TWO_STEP_SHAPES = [(4, 2, 2), (4, 4, 2), (2, 4, 3), (4, 8, 1), (2, 2, 8)]
 
