@@ -483,11 +483,13 @@ void pml_medium(const nw_medium* m, nw::PmlStep<T>& st) {
 
 template <typename T, bool ADJ>
 int launch_pml(const nw_grid* g, const nw::KGrid<T>& kg, const nw::PmlStep<T>& st, int n_shots, cudaStream_t s) {
-  const long long cells = (long long)g->n[0] * g->n[1] - (long long)(st.kx1 - st.kx0) * (st.kz1 - st.kz0);
-  if (cells <= 0 && !st.traces) return NW_OK;
-  // a thread per layer cell and shot, and with st.traces the CTAs that take the receiver samples
+  const long long vecs =
+      nw::pml_layer_vectors(g->n[0], g->n[1], st.kx0, st.kx1, st.kz0, st.kz1, 16 / (int)sizeof(T));
+  if (vecs <= 0 && !st.traces) return NW_OK;
+  // a thread per 16-byte vector of layer cells and shot, and with st.traces the CTAs that take the
+  // receiver samples
   const int rec_ctas = st.traces ? (st.n_rec + nw::PML_THREADS - 1) / nw::PML_THREADS : 0;
-  const dim3 grid((unsigned)((cells + nw::PML_THREADS - 1) / nw::PML_THREADS + rec_ctas), n_shots),
+  const dim3 grid((unsigned)((vecs + nw::PML_THREADS - 1) / nw::PML_THREADS + rec_ctas), n_shots),
       block(nw::PML_THREADS);
   if (g->radius == 1) return launch_pdl_b(nw::pml2d_step<T, 1, ADJ>, grid, block, 0, s, kg, st);
   return launch_pdl_b(nw::pml2d_step<T, 2, ADJ>, grid, block, 0, s, kg, st);
