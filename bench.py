@@ -277,6 +277,41 @@ def measure_batch(dev, world: int, rank: int, n_problems: int = 64, steps: int =
         plain_ms = max_over_ranks(e0.elapsed_time(e1))
         out["plain"] = {"value": shots / (plain_ms * 1e-3), "unit": UNIT, "ms_per_gradient_of_all_problems": plain_ms,
                         "method": "each problem alone through WaveOperatorB200.misfit_gradient (same storage)"}
+        # the plain single-shot path: one shot per operator call (the full history in HBM where it fits),
+        # on one shot of the first problem of each grid size, scaled to the whole batch by useful
+        # cell-updates
+        for op in ops:
+            op._plans.clear()
+        torch.cuda.empty_cache()
+        firsts = {}
+        for i, w in enumerate(ws):
+            firsts.setdefault(w.n, i)
+        single = []
+        for i in firsts.values():
+            w = ws[i]
+            k = len(w.sources) // 2
+            op1 = WaveOperatorB200(w.domain, [w.sources[k]], w.receivers, **w.operator_kwargs())
+            d1 = obs[i][k:k + 1].contiguous()
+            op1.misfit_gradient(cs[i], d1)  # plan, allocation, kernel loading
+            single.append((op1, cs[i], d1, 2 * w.padded_cells() * w.n_steps,
+                           f"{w.n}^2 x {w.n_steps} steps, 1 shot, {op1.last_storage[0] if op1.last_storage else '?'}"))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for op1, c1, d1, _, _ in single:
+            op1.misfit_gradient(c1, d1)
+        e1.record()
+        torch.cuda.synchronize()
+        single_ms = max_over_ranks(e0.elapsed_time(e1))
+        rate = sum(s[3] for s in single) / (single_ms * 1e-3)  # useful cell-updates/s, one shot per call
+        sample = [s[4] for s in single]
+        del single
+        out["plain_single_shot"] = {
+            "value": shots / (useful / rate), "unit": UNIT, "gcell_updates_per_s": rate / 1e9,
+            "measured_ms": single_ms, "sample": sample,
+            "method": "one shot per WaveOperatorB200.misfit_gradient call (its own storage choice: the full "
+                      "history where it fits); the sample's useful cell-updates/s applied to the whole "
+                      "batch's useful cell-updates"}
     if with_e2e:
         # end to end: models and observed data from pinned host memory in, gradients and losses out
         c_h = [c.cpu().pin_memory() for c in cs]

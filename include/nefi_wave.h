@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define NW_ABI_VERSION 5
+#define NW_ABI_VERSION 6
 
 /* scalar type of a computation */
 enum { NW_F32 = 0, NW_F64 = 1 };
@@ -147,6 +147,18 @@ typedef struct nw_acquisition {
   const int32_t* tile_cell_ptr;    /* (n_adj_tiles + 1): touched cells of the tile */
   const int32_t* tile_cell_local;  /* (x - x0) * adj_tile_cols + (z - z0) */
   const int32_t* tile_cell_gid;    /* row in cell_index / cell_ptr */
+  /* 2-D PML only: 1 when the adjoint tile tables above were built for the tiles of the PML's tiled
+     interior box (the adjoint tile grid starts at cell adj_box_corner = (x, z), the box's corner as
+     the library derives it from medium.pml_core and the adjoint tile shape) and hold the
+     receiver-touched cells inside it, while the n_layer_cells touched cells outside it are listed in
+     layer_cell_index / layer_cell_gid: the box's adjoint launch and the layer's then add the receiver
+     cotangents themselves. 0: the tables cover the whole grid from cell (0, 0), and a separate launch
+     adds the cotangents after each PML step. */
+  int32_t adj_tables_box;
+  int32_t adj_box_corner[2];
+  int32_t n_layer_cells;
+  const int32_t* layer_cell_index; /* (n_layer_cells,) ghost-layout offsets, ascending */
+  const int32_t* layer_cell_gid;   /* row in cell_index / cell_ptr */
 } nw_acquisition;
 
 /* The medium: c^2 dt^2 on the padded grid and the absorbing coefficients. */

@@ -14,7 +14,7 @@ from pathlib import Path
 import torch
 
 LIB_PATH = Path(__file__).resolve().parent / "libnefiwave.so"
-ABI_VERSION = 5
+ABI_VERSION = 6
 
 NW_F32, NW_F64 = 0, 1
 NW_ABS_NONE, NW_ABS_SPONGE, NW_ABS_CERJAN, NW_ABS_PML = 0, 1, 2, 3
@@ -56,6 +56,8 @@ class Acquisition(C.Structure):
         ("rec_corner", C.c_void_p), ("tile_rec_ptr", C.c_void_p), ("tile_rec_list", C.c_void_p),
         ("adj_tiles_z", C.c_int32), ("adj_tile_rows", C.c_int32), ("adj_tile_cols", C.c_int32),
         ("tile_cell_ptr", C.c_void_p), ("tile_cell_local", C.c_void_p), ("tile_cell_gid", C.c_void_p),
+        ("adj_tables_box", C.c_int32), ("adj_box_corner", C.c_int32 * 2),
+        ("n_layer_cells", C.c_int32), ("layer_cell_index", C.c_void_p), ("layer_cell_gid", C.c_void_p),
     ]
 
 

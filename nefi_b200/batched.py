@@ -80,7 +80,7 @@ class BatchedFWI:
             # tensors (and the tuning) alive even if the operator's plan is re-tuned later
             b = {"plan": plan, "S": S, "tune": plan.tuning,
                  "tables": [plan.rec_corner, plan.tile_rec_ptr, plan.tile_rec_list, plan.tile_cell_ptr,
-                            plan.tile_cell_local, plan.tile_cell_gid]}
+                            plan.tile_cell_local, plan.tile_cell_gid, plan.layer_cell_index, plan.layer_cell_gid]}
             b["ring"] = plan.empty_levels(3, S)
             n_snap = -(-op.n_steps // K) if op.n_steps > 0 else 1
             b["snap"] = torch.empty(plan.snapshot_bytes(S, n_snap, kind), dtype=torch.uint8, device=dev)

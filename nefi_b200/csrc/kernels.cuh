@@ -128,10 +128,11 @@ __global__ void inject_kernel(T* __restrict__ out, long long field, const T* __r
   if (c >= n_cells) return;
   T acc = T(0);
   const T* gs = g + (long long)s * n_rec * n_t + j;
-  for (int e = ptr[c]; e < ptr[c + 1]; ++e) acc += w[e] * gs[(long long)rec[e] * n_t];
+  for (int e = ptr[c]; e < ptr[c + 1]; ++e) acc = fma_rn(w[e], gs[(long long)rec[e] * n_t], acc);
   const long long i = cell[c];
   const T av = (apply_a && A) ? A[i] : T(1);
-  out[(long long)s * field + i] += av * (C[i] * acc);
+  T* o = out + (long long)s * field + i;
+  *o = fma_rn(av, mul_rn(C[i], acc), *o);  // the rounding sequence of the PML layer launch's own injection
 }
 
 }  // namespace nw

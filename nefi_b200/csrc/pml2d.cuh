@@ -8,8 +8,9 @@
 // Adjoint, advancing q = C mu like the other adjoint steps (D+^T = -D-, D-^T = -D+):
 //   Psi_k = alpha Psi_{k+1} - (0.5/h) D+(q^{k+1} + q^{k+2})                       (faces)
 //   q^k   = A (2 q^{k+1} - ZZ q^{k+1} - B q^{k+2} + C (Lap q^{k+1} - sum_ax D-(beta Psi_k)))
-// and C dJ/dC += q^{k+1} L_k with L_k stored by the forward step. The receiver cotangents are
-// added by inject_kernel after the step, like the 3-D adjoint.
+// and C dJ/dC += q^{k+1} L_k with L_k stored by the forward step. The receiver cotangents of the
+// cells outside the tiled box are added after the step, q^k += A C R^T g_k: by this launch when the
+// host lists those cells for it, else by inject_kernel after the step, like the 3-D adjoint.
 //
 // Face f of axis ax (between cells f-1 and f, f = 0..P_ax) is stored at the cell index of f in the
 // ghost layout: face P_ax lands in the first ghost row (x) or column (z), which the layout always
@@ -54,6 +55,16 @@ struct PmlStep {
   // adjoint: the gradient
   const T* __restrict__ lap;
   T* __restrict__ grad;            // per-shot accumulators of C dJ/dC
+  // adjoint record steps: the receiver cotangents of the touched cells in the layer (ghost-layout
+  // offsets lc_off, ascending, with their CSR rows lc_gid), added to the cells after the step as
+  // inject_kernel does (NULL gtr: none)
+  const T* __restrict__ gtr;
+  const int* __restrict__ lc_off;
+  const int* __restrict__ lc_gid;
+  int n_lc;
+  const int* __restrict__ gc_ptr;
+  const int* __restrict__ gc_rec;
+  const T* __restrict__ gc_w;
 };
 
 // Thread t of shot s (grid.y) steps the t-th 16-byte vector of W = 16 / sizeof(T) cells of the layer
@@ -249,6 +260,26 @@ __global__ void __launch_bounds__(PML_THREADS) pml2d_step(KGrid<T> g, PmlStep<T>
       o = fma_rn(-B_, PPc[v], fma_rn(cc[v], add_rn(lap, -pml), fma_rn(-Z_, c, add_rn(c, c))));
       out[v] = a.apply_a ? mul_rn(A_, o) : o;
       if (a.lap) lout[v] = fma_rn(c, lp[v], gr[v]);
+    }
+  }
+
+  if (ADJ && a.gtr) {  // the receiver cotangents of this vector's touched cells
+    int lo = 0, hi = a.n_lc;
+    while (lo < hi) {  // the first touched layer cell at or after the vector's first cell
+      const int mid = (lo + hi) >> 1;
+      if (a.lc_off[mid] < i) lo = mid + 1; else hi = mid;
+    }
+    const T* __restrict__ gs = a.gtr + (long long)s * a.n_rec * a.n_t + a.j;
+    for (int e = lo; e < a.n_lc; ++e) {
+      const int v = a.lc_off[e] - i;
+      if (v >= W) break;
+      const int gid = a.lc_gid[e];
+      T acc = T(0);
+      for (int q = a.gc_ptr[gid]; q < a.gc_ptr[gid + 1]; ++q)
+        acc = fma_rn(a.gc_w[q], gs[(long long)a.gc_rec[q] * a.n_t], acc);
+#pragma unroll
+      for (int u = 0; u < W; ++u)
+        if (u == v) out[u] = fma_rn(a.apply_a ? av[u] : T(1), mul_rn(cc[u], acc), out[u]);
     }
   }
 

@@ -578,6 +578,33 @@ dim3 box_tiles(const nw::PmlStep<T>& st, const TileCfg& c, int n_shots, nw::Tile
   return dim3(tb.tt.tiles_z, (st.kx1 - st.kx0 + c.tx() - 1) / c.tx(), c.groups(n_shots));
 }
 
+// The receiver cotangents of step n's touched layer cells, added by the PML layer launch itself.
+template <typename T>
+void layer_inject(const nw_acquisition* a, const T* gtr, int n_t, int j, nw::PmlStep<T>& ps) {
+  if (a->n_layer_cells <= 0) return;
+  ps.gtr = gtr;
+  ps.n_rec = (int)a->n_rec;
+  ps.n_t = n_t;
+  ps.j = j;
+  ps.lc_off = a->layer_cell_index;
+  ps.lc_gid = a->layer_cell_gid;
+  ps.n_lc = a->n_layer_cells;
+  ps.gc_ptr = a->cell_ptr;
+  ps.gc_rec = a->cell_rec;
+  ps.gc_w = (const T*)a->cell_weight;
+}
+
+// Whether the PML's interior box (tiled by `c` from its corner (kx0, kz0), tiles_z tiles along z)
+// adds the receiver cotangents in its own adjoint launch: the acquisition's adjoint tile tables were
+// built for exactly these tiles, and the touched cells outside the box are listed for the layer's
+// launch.
+inline bool box_injects(const nw_acquisition* a, const TileCfg& c, int kx0, int kz0, int tiles_z) {
+  return a->n_cells > 0 && a->adj_tables_box && a->tile_cell_ptr &&
+         (a->n_layer_cells == 0 || (a->layer_cell_index && a->layer_cell_gid)) && a->adj_box_corner[0] == kx0 &&
+         a->adj_box_corner[1] == kz0 && a->adj_tiles_z == tiles_z && a->adj_tile_rows == c.tx() &&
+         a->adj_tile_cols == c.tz();
+}
+
 template <typename T>
 struct Ring {  // time level n (n >= -1) of the pressure field: three (or four) rotating levels
   T* base;
@@ -871,6 +898,7 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
     ps.apply_a = n >= 1 ? 1 : 0;
     ps.lap = lap;
     ps.grad = gacc;
+    bool box_inject = false;
     int rc = pml_tiled_box<T>(g, m, tu.adj, ps);
     if (rc) return rc;
     if (ps.kx1 == ps.kx0) {  // no interior box: the layer kernel over every cell
@@ -888,13 +916,25 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
       tb.apply_a = ps.apply_a;
       tb.lap = lap;
       tb.gacc = gacc;
+      // the receiver cotangents: added by the box's launch itself when the adjoint tile tables were
+      // built for this box's tiles (every touched cell then lies in it), else by inject3 after the step
+      tb.tt = tile_tables(g, a, tu.adj);
       const dim3 grid = box_tiles<T>(ps, tu.adj, S, tb);
+      box_inject = box_injects(a, tu.adj, ps.kx0, ps.kz0, tb.tt.tiles_z);
+      if (box_inject && n % M == 0) {  // the box's cells by the box, the layer's by the layer
+        tb.gtr = gtr;
+        tb.gcell_w = (const T*)a->cell_weight;
+        tb.n_rec = a->n_rec;
+        tb.n_t = t->n_t;
+        tb.j = n / M;
+        layer_inject<T>(a, gtr, t->n_t, n / M, ps);
+      }
       rc = fork_join(
           s, true, [&](cudaStream_t t) { return launch_pml<T, true>(g, kg, ps, S, t); },
           [&](cudaStream_t t) { return NW_DISPATCH2(launch_adj2_v, T, tu.adj, kg, tb, grid, t); });
       if (rc) return rc;
     }
-    return inject3(n);
+    return box_inject ? NW_OK : inject3(n);  // (inject3 itself skips the steps without cotangents)
   };
   if (N >= n_stop) {  // level N: q^N = A C R^T g_N (q^{N+1} = q^{N+2} = 0)
     int rc = pml ? step_pml(N, nullptr) : (g->ndim == 2 ? step2(N, nullptr) : inject3(N));
@@ -1119,9 +1159,13 @@ static int check_run(const nw_grid* g, const nw_medium* m, const nw_acquisition*
   if (a->n_rec > 0 && (!a->rec_index || !a->rec_weight)) return fail(NW_ERR_ARG, "receiver arrays are NULL");
   if (t->substeps < 1 || t->n_t < 1 || t->n_steps != (t->n_t - 1) * t->substeps)
     return fail(NW_ERR_ARG, "inconsistent time axis");
+  if (a->adj_tables_box && (g->ndim != 2 || g->absorbing != NW_ABS_PML))
+    return fail(NW_ERR_ARG, "adjoint tables of a PML's interior box on a grid without a PML");
   if (g->ndim == 2) {
+    // (tables of a PML's interior box count its tiles only; box_injects checks them before use)
     if (a->tile_rows != tu.fwd.tx() || a->tile_cols != tu.fwd.tz() || a->tiles_z != tu.fwd.tiles_z(g) ||
-        a->adj_tile_rows != tu.adj.tx() || a->adj_tile_cols != tu.adj.tz() || a->adj_tiles_z != tu.adj.tiles_z(g))
+        a->adj_tile_rows != tu.adj.tx() || a->adj_tile_cols != tu.adj.tz() ||
+        (!a->adj_tables_box && a->adj_tiles_z != tu.adj.tiles_z(g)))
       return fail(NW_ERR_ARG, "per-tile tables were built for another tile shape (see nw_tile_shape)");
     if (!a->tile_rec_ptr || !a->tile_cell_ptr || !a->rec_corner ||
         (a->n_cells > 0 && (!a->tile_cell_local || !a->tile_cell_gid)) || (a->n_rec > 0 && !a->tile_rec_list))
@@ -1493,6 +1537,10 @@ int batch_prepare_impl(const nw_batch_problem* P, int n, const Tune& tu, void* t
       B.fwd.tt.tiles_z = tf.tt.tiles_z;
       B.adj.tx_off = ta.tx_off; B.adj.tz_off = ta.tz_off; B.adj.x_end = ta.x_end; B.adj.z_end = ta.z_end;
       B.adj.tt.tiles_z = ta.tt.tiles_z;
+      if (box_injects(a, tu.adj, ta.tx_off, ta.tz_off, ta.tt.tiles_z)) {  // the box adds the cotangents
+        B.adj.gtr = (const T*)q.grad_traces;
+        B.adj.n_rec = a->n_rec;
+      }
     }
     const dim3 fg = batch_grid<T>(q, tu.fwd), ag = batch_grid<T>(q, tu.adj);
     B.ftx = (int)fg.y;
@@ -1624,13 +1672,19 @@ int batch_pml_adjoint(const nw_batch_problem& q, const Tune& tu, int n, cudaStre
   ps.grad = (T*)q.grad_acc;
   int rc = pml_tiled_box<T>(g, &q.medium, tu.adj, ps);
   if (rc) return rc;
+  if (ps.kx1 > ps.kx0 && q.acq.n_cells > 0 && n % q.time.substeps == 0) {
+    nw::Tiled2<T> ta = {};
+    box_tiles<T>(ps, tu.adj, q.acq.n_shots, ta);
+    if (box_injects(&q.acq, tu.adj, ta.tx_off, ta.tz_off, ta.tt.tiles_z))  // the layer's touched cells
+      layer_inject<T>(&q.acq, (const T*)q.grad_traces, q.time.n_t, n / q.time.substeps, ps);
+  }
   return launch_pml<T, true>(g, kgrid<T>(g), ps, q.acq.n_shots, s);
 }
 
 // The receiver cotangents of batch problem q at adjoint step n at every cell (a PML problem's
 // batched launch skips them), after its interior box and layer cells.
 template <typename T>
-int batch_pml_inject(const nw_batch_problem& q, int n, cudaStream_t s) {
+int batch_pml_inject(const nw_batch_problem& q, const Tune& tu, int n, cudaStream_t s) {
   const nw_grid* g = &q.grid;
   const long long LE = (long long)q.acq.n_shots * g->field_elems;
   T* work = (T*)q.work;
@@ -1638,6 +1692,14 @@ int batch_pml_inject(const nw_batch_problem& q, int n, cudaStream_t s) {
   const nw_acquisition* a = &q.acq;
   const int M = q.time.substeps;
   if (a->n_cells <= 0 || n % M != 0) return NW_OK;
+  {  // the batched launch of the problem's interior box added them
+    nw::PmlStep<T> sa = {};
+    nw::Tiled2<T> ta = {};
+    if (pml_tiled_box<T>(g, &q.medium, tu.adj, sa) == NW_OK && sa.kx1 > sa.kx0) {
+      box_tiles<T>(sa, tu.adj, a->n_shots, ta);
+      if (box_injects(a, tu.adj, ta.tx_off, ta.tz_off, ta.tt.tiles_z)) return NW_OK;
+    }
+  }
   const dim3 ig((a->n_cells + 127) / 128, a->n_shots);
   return launch_pdl_b(nw::inject_kernel<T>, ig, dim3(128), 0, s, lv(n), (long long)g->field_elems,
                       (const T*)q.medium.c2dt2, (const T*)q.medium.coef_a, n >= 1 ? 1 : 0, (const T*)q.grad_traces,
@@ -1728,7 +1790,7 @@ int batch_adjoint_impl(const nw_batch_problem* P, int n, const Tune& tu, const v
         },
         [&](cudaStream_t t) -> int { return NW_DISPATCH_BATCH(launch_adj_batch, T, tu.adj, R, table, n, na, acta[na], step, 0, K, t); });
     for (int p = 0; p < na && !rc; ++p)  // and their cotangents, once both halves are done
-      if (P[p].grid.absorbing == NW_ABS_PML) rc = batch_pml_inject<T>(P[p], step, s);
+      if (P[p].grid.absorbing == NW_ABS_PML) rc = batch_pml_inject<T>(P[p], tu, step, s);
     return rc;
   };
   int rc = adj_step(Nmax);  // problems with the largest step count start: q^N = A C R^T g_N

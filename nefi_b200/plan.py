@@ -191,6 +191,8 @@ class DevicePlan:
         self.tiles_z = self.adj_tiles_z = 0
         self.rec_corner = self.tile_rec_ptr = self.tile_rec_list = None
         self.tile_cell_ptr = self.tile_cell_local = self.tile_cell_gid = None
+        self.adj_tables_box, self.adj_box_corner = 0, (0, 0)
+        self.layer_cell_index = self.layer_cell_gid = None
         if self.g.ndim == 2:
             self._build_tile_tables()
 
@@ -212,10 +214,25 @@ class DevicePlan:
         rptr = torch.zeros(n_tiles + 1, dtype=torch.int64)
         rptr[1:] = torch.cumsum(torch.bincount(tile_of, minlength=n_tiles), 0)
         AX, AZ = self.adj_tile
-        adj_tiles_z = -(-g.n[1] // AZ)
-        n_adj_tiles = adj_tiles_z * -(-g.n[0] // AX)
         rel = self._cells - int(g.origin)
         x, z = rel // int(g.stride[0]), rel % int(g.stride[0])
+        # the adjoint tile grid: from cell (0, 0) over the whole grid, or, with a PML and a tiled
+        # interior box, from the box's corner over the box, holding the touched cells inside it, the
+        # others listed apart (the box's adjoint launch and the layer's then add the cotangents)
+        ox, oz, ex, ez = 0, 0, int(g.n[0]), int(g.n[1])
+        gid_all = torch.arange(self.n_cells)
+        box = self.pml_tiled_box(AX, AZ)
+        if box is not None and self.n_cells > 0:
+            bx0, bx1, bz0, bz1 = box
+            inside = (x >= bx0) & (x < bx1) & (z >= bz0) & (z < bz1)
+            ox, oz, ex, ez = bx0, bz0, bx1, bz1
+            self.adj_tables_box, self.adj_box_corner = 1, (bx0, bz0)
+            self.layer_cell_index = self._cells[~inside].to(torch.int32).to(self.device)
+            self.layer_cell_gid = gid_all[~inside].to(torch.int32).to(self.device)
+            x, z, gid_all = x[inside], z[inside], gid_all[inside]
+        x, z = x - ox, z - oz
+        adj_tiles_z = -(-(ez - oz) // AZ)
+        n_adj_tiles = adj_tiles_z * -(-(ex - ox) // AX)
         ctile = (x // AX) * adj_tiles_z + z // AZ
         corder = torch.argsort(ctile, stable=True)
         cptr = torch.zeros(n_adj_tiles + 1, dtype=torch.int64)
@@ -228,7 +245,20 @@ class DevicePlan:
         self.tile_rec_list = order.to(i32).to(dev)
         self.tile_cell_ptr = cptr.to(i32).to(dev)
         self.tile_cell_local = local[corder].to(i32).to(dev)
-        self.tile_cell_gid = corder.to(i32).to(dev)
+        self.tile_cell_gid = gid_all[corder].to(i32).to(dev)
+
+    def pml_tiled_box(self, tx: int, tz: int):
+        """The PML's interior box that the tiled kernels of a (tx, tz) tile step, as the library derives
+        it (wave_capi.cu ``pml_tiled_box``): the core box with its first column rounded up to a
+        16-byte chunk, or None when there is no PML or the box is smaller than one tile."""
+        if self.pml is None:
+            return None
+        x0, x1, z0, z1 = (int(v) for v in self.pml["core"])
+        epc = 16 // (torch.finfo(self.dtype).bits // 8)
+        z0 = -(-z0 // epc) * epc
+        if x1 - x0 < tx or z1 - z0 < tz:
+            return None
+        return x0, x1, z0, z1
 
     def n_acc(self, n_shots: int) -> int:
         """Gradient accumulator fields (plan dtype) the adjoint sweep fills for ``n_shots`` shots."""
@@ -282,6 +312,12 @@ class DevicePlan:
             a.tile_cell_ptr = self.tile_cell_ptr.data_ptr()
             a.tile_cell_local = self.tile_cell_local.data_ptr()
             a.tile_cell_gid = self.tile_cell_gid.data_ptr()
+            a.adj_tables_box = self.adj_tables_box
+            a.adj_box_corner[0], a.adj_box_corner[1] = self.adj_box_corner
+            if self.layer_cell_index is not None:
+                a.n_layer_cells = int(self.layer_cell_index.numel())
+                a.layer_cell_index = self.layer_cell_index.data_ptr()
+                a.layer_cell_gid = self.layer_cell_gid.data_ptr()
         return a
 
     def empty_levels(self, n_levels: int, n_shots: int, zero: bool = True) -> torch.Tensor:

@@ -36,7 +36,7 @@ def test_every_declared_symbol_is_exported_and_bound(lib):
 
 
 def test_abi_version_and_arch(lib):
-    assert lib.nw_abi_version() == _lib.ABI_VERSION == 5
+    assert lib.nw_abi_version() == _lib.ABI_VERSION == 6
     assert lib.nw_built_arch() == 1000
 
 

@@ -485,6 +485,8 @@ def test_pml_interior_through_tiled_kernels_matches_the_oracle(dtype, tt, tg, cu
     op = WaveOperatorB200(dom, src, rec, grad_mode="autograd", **kw)
     x0, x1, z0, z1 = op._plan(cuda_device, dtype).pml["core"]
     assert x1 - x0 >= 32 and z1 - z0 >= 128  # larger than the default forward and adjoint tiles
+    # every receiver-touched cell lies in the tiled box: the box's adjoint launch adds the cotangents
+    assert op._plan(cuda_device, dtype).adj_tables_box == 1
     cd = c.to(dtype).to(cuda_device).requires_grad_(True)
     tr = op({"c": cd})
     gt = torch.tensor(cotangent(tr.shape, 22), dtype=dtype, device=cuda_device)

@@ -123,11 +123,26 @@ def _check_tile_tables(plan):
     atz = plan.adj_tiles_z
     cptr = plan.tile_cell_ptr.numpy()
     gid, local = plan.tile_cell_gid.numpy(), plan.tile_cell_local.numpy()
-    assert sorted(gid.tolist()) == list(range(plan.n_cells))
     cells = plan.cell_index.numpy() - plan.g.origin
     ld = plan.g.stride[0]
+    # the adjoint tile grid starts at the PML's tiled box when the tables were built for it; the
+    # touched cells outside the box are then listed apart, ascending, for the layer's launch
+    ox, oz = plan.adj_box_corner if plan.adj_tables_box else (0, 0)
+    box = plan.pml_tiled_box(AX, AZ)
+    if plan.adj_tables_box:
+        assert box is not None and (ox, oz) == (box[0], box[2])
+        assert atz == -(-(box[3] - box[2]) // AZ) and len(cptr) - 1 == atz * -(-(box[1] - box[0]) // AX)
+        off, lgid = plan.layer_cell_index.numpy(), plan.layer_cell_gid.numpy()
+        assert np.all(np.diff(off) > 0)
+        assert np.array_equal(off, plan.cell_index.numpy()[lgid])
+        xs, zs = (off - plan.g.origin) // ld, (off - plan.g.origin) % ld
+        assert not ((xs >= box[0]) & (xs < box[1]) & (zs >= box[2]) & (zs < box[3])).any()
+        assert sorted(gid.tolist() + lgid.tolist()) == list(range(plan.n_cells))
+    else:
+        assert box is None or plan.n_cells == 0
+        assert sorted(gid.tolist()) == list(range(plan.n_cells))
     for t in range(len(cptr) - 1):
-        x0, z0 = (t // atz) * AX, (t % atz) * AZ
+        x0, z0 = ox + (t // atz) * AX, oz + (t % atz) * AZ
         for e in range(cptr[t], cptr[t + 1]):
             x, z = divmod(int(cells[gid[e]]), ld)
             assert x0 <= x < x0 + AX and z0 <= z < z0 + AZ
@@ -490,3 +505,31 @@ def test_padding_and_nearest_cells_match_the_oracle(shape, extent):
     span = [op.grid.padded_shape[ax] * op.grid.spacing[ax] for ax in range(d)]
     pts = np.stack([rng.uniform(lo[ax] - 0.1, lo[ax] + span[ax] + 0.1, 500) for ax in range(d)], 1)
     assert np.array_equal(op.grid.nearest_index(torch.tensor(pts)).numpy(), orc.nearest_cells(pts))
+
+
+
+@pytest.mark.parametrize("edge", [False, True])
+def test_pml_adjoint_tables_follow_the_interior_box(edge):
+    """With a PML and a tiled interior box, the adjoint tile tables are built from the box's corner
+    and hold the receiver-touched cells inside it (the box's adjoint launch adds their cotangents);
+    the cells outside it (a receiver on the domain's face reaches the layer) are listed apart for the
+    layer's launch."""
+    shape, h = (60, 150), 0.01
+    extent = ((0.0, shape[0] * h), (0.0, shape[1] * h))
+    rec = [[0.02, 0.1 + 0.0123 * i] for i in range(100)]
+    if edge:
+        rec.append([0.0, 0.7])  # on the domain's face: the stencil's upper row lies in the layer
+    op = WaveOperatorB200(Domain(shape, extent), [[0.05, 0.4]], rec, n_t=20, dt_obs=0.004, f0=25.0, c_max=2.5,
+                          order=4, absorbing="pml", absorb_width=0.08)
+    for dtype in (torch.float32, torch.float64):
+        plan = op._plan(CPU, dtype)
+        for tuning in [(0, 0, 0), (2, 2, 1, 2, 4, 2), (4, 2, 2, 4, 4, 1)]:
+            if dtype == torch.float64 and 4 in tuning:
+                continue
+            plan.set_tuning(*tuning)
+            assert plan.adj_tables_box == 1
+            assert plan.layer_cell_index.numel() == (2 if edge else 0)
+            a = plan.acquisition(1)
+            assert a.adj_tables_box == 1 and tuple(a.adj_box_corner) == plan.adj_box_corner
+            assert a.n_layer_cells == plan.layer_cell_index.numel()
+            _check_tile_tables(plan)
