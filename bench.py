@@ -178,6 +178,44 @@ def measure_batch(dev, world: int, rank: int, n_problems: int = 64, steps: int =
         t = torch.tensor([x], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t)
+    single_shot = None
+    if with_plain:
+        # the plain single-shot path, measured before the batch allocates its storage: one shot per
+        # operator call (the full history in HBM where it fits), on one shot of the first problem of
+        # each grid size, scaled to the whole batch by useful cell-updates
+        firsts = {}
+        for i, w in enumerate(ws):
+            firsts.setdefault(w.n, i)
+        single = []
+        for i in firsts.values():
+            w = ws[i]
+            k = len(w.sources) // 2
+            op1 = WaveOperatorB200(w.domain, [w.sources[k]], w.receivers, **w.operator_kwargs())
+            c1 = torch.tensor(w.c, dtype=torch.float32, device=dev)
+            with torch.no_grad():
+                d1 = op1({"c": torch.nn.functional.avg_pool2d(c1[None, None], 9, 1, 4, count_include_pad=False)[0, 0]
+                                .contiguous()})
+            op1.misfit_gradient(c1, d1)  # plan, allocation, kernel loading
+            single.append((op1, c1, d1, 2 * w.padded_cells() * w.n_steps,
+                           f"{w.n}^2 x {w.n_steps} steps, 1 shot, {op1.last_storage[0] if op1.last_storage else '?'}"))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for op1, c1, d1, _, _ in single:
+            op1.misfit_gradient(c1, d1)
+        e1.record()
+        torch.cuda.synchronize()
+        single_ms = max_over_ranks(e0.elapsed_time(e1))
+        rate = sum(s[3] for s in single) / (single_ms * 1e-3)  # useful cell-updates/s, one shot per call
+        useful_all = sum(2 * w.padded_cells() * w.n_steps * len(w.sources) for w in ws_all)
+        single_shot = {
+            "value": sum(len(w.sources) for w in ws_all) / (useful_all / rate), "unit": UNIT,
+            "gcell_updates_per_s": rate / 1e9, "measured_ms": single_ms, "sample": [s[4] for s in single],
+            "method": "one shot per WaveOperatorB200.misfit_gradient call (its own storage choice: the full "
+                      "history where it fits), measured before the batch allocates; the sample's useful "
+                      "cell-updates/s applied to the whole batch's useful cell-updates"}
+        del single, op1
+        torch.cuda.empty_cache()
     ops = [WaveOperatorB200(w.domain, w.sources, w.receivers, grad_mode="checkpoint", snapshot=snapshot,
                             **w.operator_kwargs()) for w in ws]
     cs = [torch.tensor(w.c, dtype=torch.float32, device=dev) for w in ws]
@@ -277,41 +315,8 @@ def measure_batch(dev, world: int, rank: int, n_problems: int = 64, steps: int =
         plain_ms = max_over_ranks(e0.elapsed_time(e1))
         out["plain"] = {"value": shots / (plain_ms * 1e-3), "unit": UNIT, "ms_per_gradient_of_all_problems": plain_ms,
                         "method": "each problem alone through WaveOperatorB200.misfit_gradient (same storage)"}
-        # the plain single-shot path: one shot per operator call (the full history in HBM where it fits),
-        # on one shot of the first problem of each grid size, scaled to the whole batch by useful
-        # cell-updates
-        for op in ops:
-            op._plans.clear()
-        torch.cuda.empty_cache()
-        firsts = {}
-        for i, w in enumerate(ws):
-            firsts.setdefault(w.n, i)
-        single = []
-        for i in firsts.values():
-            w = ws[i]
-            k = len(w.sources) // 2
-            op1 = WaveOperatorB200(w.domain, [w.sources[k]], w.receivers, **w.operator_kwargs())
-            d1 = obs[i][k:k + 1].contiguous()
-            op1.misfit_gradient(cs[i], d1)  # plan, allocation, kernel loading
-            single.append((op1, cs[i], d1, 2 * w.padded_cells() * w.n_steps,
-                           f"{w.n}^2 x {w.n_steps} steps, 1 shot, {op1.last_storage[0] if op1.last_storage else '?'}"))
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for op1, c1, d1, _, _ in single:
-            op1.misfit_gradient(c1, d1)
-        e1.record()
-        torch.cuda.synchronize()
-        single_ms = max_over_ranks(e0.elapsed_time(e1))
-        rate = sum(s[3] for s in single) / (single_ms * 1e-3)  # useful cell-updates/s, one shot per call
-        sample = [s[4] for s in single]
-        del single
-        out["plain_single_shot"] = {
-            "value": shots / (useful / rate), "unit": UNIT, "gcell_updates_per_s": rate / 1e9,
-            "measured_ms": single_ms, "sample": sample,
-            "method": "one shot per WaveOperatorB200.misfit_gradient call (its own storage choice: the full "
-                      "history where it fits); the sample's useful cell-updates/s applied to the whole "
-                      "batch's useful cell-updates"}
+        out["plain_single_shot"] = single_shot
+
     if with_e2e:
         # end to end: models and observed data from pinned host memory in, gradients and losses out
         c_h = [c.cpu().pin_memory() for c in cs]
@@ -1150,7 +1155,12 @@ def main() -> None:
         op64 = WaveOperatorB200(w.domain, w.sources[:na], w.receivers, grad_mode="checkpoint", **kw)
         _, g64 = op64.misfit_gradient(c.double(), d[:na].double())
         accuracy = {"grad_rel_l2_fp32_vs_fp64": float((g32 - g64).norm() / g64.norm()), "shots": na,
-                    "fp32_storage": f"{args.grad_mode}, {args.snapshot} snapshots"}
+                    "fp32_storage": f"{args.grad_mode}, {args.snapshot} snapshots",
+                    "fixed_cotangent": fixed_cotangent_error(op64, WaveOperatorB200(
+                        w.domain, w.sources[:na], w.receivers, grad_mode=args.grad_mode, snapshot=args.snapshot,
+                        checkpoint_every=args.checkpoint_every, **kw), c, d[:na]),
+                    "note": "grad_rel_l2_fp32_vs_fp64: each precision's own misfit gradient (its own residual); "
+                            "fixed_cotangent: the float32 adjoint given the float64 residual"}
         if args.fd_directions > 0:
             # central differences of the float64 misfit along seeded unit directions, step scaled to
             # ||c||, against the float64 gradient's directional derivative
