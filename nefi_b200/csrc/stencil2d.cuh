@@ -498,7 +498,7 @@ __device__ __forceinline__ void adj2d_body(const KGrid<T>& g, const Tiled2<T>& a
   // shot-independent and cached here, so a shot only loads the cotangents themselves
   constexpr int kEnt = 4;
   int jl = -1, jn = 0, jrec[kEnt];
-  T jw[kEnt];
+  T jw[kEnt], jv[kEnt];  // jv: the cached entries' cotangents of the current shot, loaded one shot ahead
   bool jslow = false;  // more entries than cached: read the table every shot
   if (inject) {
     for (int i = threadIdx.x; i < 2 * S::QS; i += 256) sj[i] = T(0);
@@ -527,6 +527,11 @@ __device__ __forceinline__ void adj2d_body(const KGrid<T>& g, const Tiled2<T>& a
     }
   wait_previous_grid();
   allow_next_grid();
+  if (jl >= 0 && !jslow) {  // the first shot's cotangents (the launch just before may have written them)
+    const T* gs = a.gtr + (long long)sb * a.n_rec * a.n_t + a.j;
+#pragma unroll
+    for (int m = 0; m < kEnt; ++m) jv[m] = (m < jn) ? gs[(long long)jrec[m] * a.n_t] : T(0);
+  }
   if (grad) issue(pc, a.gacc + (long long)bz * g.field, smem_addr(sg));  // the previous step updated it
 #pragma unroll
   for (int i = 0; i < NS - 1; ++i) {  // one commit group per shot, empty groups included, so that
@@ -570,8 +575,14 @@ __device__ __forceinline__ void adj2d_body(const KGrid<T>& g, const Tiled2<T>& a
         T acc = T(0);
 #pragma unroll
         for (int m = 0; m < kEnt; ++m)
-          if (m < jn) acc = fma_rn(jw[m], gs[(long long)jrec[m] * a.n_t], acc);
+          if (m < jn) acc = fma_rn(jw[m], jv[m], acc);
         sjs[jl] = acc;
+        if (s + 1 < se) {  // the next shot's, in flight while this shot is computed
+          const T* gn = gs + (long long)a.n_rec * a.n_t;
+#pragma unroll
+          for (int m = 0; m < kEnt; ++m)
+            if (m < jn) jv[m] = gn[(long long)jrec[m] * a.n_t];
+        }
       }
       for (int e = c0 + threadIdx.x + (jslow ? 0 : 256); e < c1; e += 256) {  // the uncached cells
         const int gid = a.tt.cell_gid[e];
