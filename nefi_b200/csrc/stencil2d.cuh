@@ -332,6 +332,13 @@ __device__ __forceinline__ void fwd2d_body(const KGrid<T>& g, const Tiled2<T>& a
   }
   int e0 = 0, e1 = 0;
   if (a.traces) { e0 = a.tt.rec_ptr[tile]; e1 = a.tt.rec_ptr[tile + 1]; }
+  // thread t samples the tile's receiver e0 + t: its id and staged-tile offset, read once per CTA
+  // (receivers past the first 256 of the tile read theirs every shot)
+  int rr = -1, roff = 0;
+  if (e0 + (int)threadIdx.x < e1) {
+    rr = a.tt.rec_list[e0 + threadIdx.x];
+    roff = (a.tt.rec_corner[2 * rr] - x0 + R) * S::SW + a.tt.rec_corner[2 * rr + 1] - z0 + S::HL;
+  }
   int2 scor = make_int2(-1 << 20, -1 << 20);  // the next shot's source corner (x, z), one shot ahead
   if (a.src_corner) scor = make_int2(a.src_corner[2 * sb], a.src_corner[2 * sb + 1]);
   wait_previous_grid();
@@ -368,7 +375,15 @@ __device__ __forceinline__ void fwd2d_body(const KGrid<T>& g, const Tiled2<T>& a
     const T* P = sp + buf * S::PS;
     pvn += fs;
 
-    for (int e = e0 + threadIdx.x; e < e1; e += 256) {  // receiver samples of p^n
+    if (rr >= 0) {  // receiver samples of p^n
+      const T* w = a.rec_w + 4 * rr;
+      T acc = mul_rn(w[0], P[roff]);
+      acc = fma_rn(w[1], P[roff + 1], acc);
+      acc = fma_rn(w[2], P[roff + S::SW], acc);
+      acc = fma_rn(w[3], P[roff + S::SW + 1], acc);
+      a.traces[((long long)s * a.n_rec + rr) * a.n_t + a.j] = acc;
+    }
+    for (int e = e0 + threadIdx.x + 256; e < e1; e += 256) {  // the tile's receivers past the first 256
       const int r = a.tt.rec_list[e];
       const int row = a.tt.rec_corner[2 * r] - x0 + R, col = a.tt.rec_corner[2 * r + 1] - z0 + S::HL;
       const T* w = a.rec_w + 4 * r;
