@@ -190,7 +190,8 @@ def measure_batch(dev, world: int, rank: int, n_problems: int = 64, steps: int =
         for i in firsts.values():
             w = ws[i]
             k = len(w.sources) // 2
-            op1 = WaveOperatorB200(w.domain, [w.sources[k]], w.receivers, **w.operator_kwargs())
+            op1 = WaveOperatorB200(w.domain, [w.sources[k]], w.receivers, grad_mode="autograd",
+                                   **w.operator_kwargs())
             c1 = torch.tensor(w.c, dtype=torch.float32, device=dev)
             with torch.no_grad():
                 d1 = op1({"c": torch.nn.functional.avg_pool2d(c1[None, None], 9, 1, 4, count_include_pad=False)[0, 0]
@@ -211,9 +212,9 @@ def measure_batch(dev, world: int, rank: int, n_problems: int = 64, steps: int =
         single_shot = {
             "value": sum(len(w.sources) for w in ws_all) / (useful_all / rate), "unit": UNIT,
             "gcell_updates_per_s": rate / 1e9, "measured_ms": single_ms, "sample": [s[4] for s in single],
-            "method": "one shot per WaveOperatorB200.misfit_gradient call (its own storage choice: the full "
-                      "history where it fits), measured before the batch allocates; the sample's useful "
-                      "cell-updates/s applied to the whole batch's useful cell-updates"}
+            "method": "one shot per WaveOperatorB200.misfit_gradient call, grad_mode='autograd' (the full "
+                      "history in HBM where it fits), measured before the batch allocates; the sample's "
+                      "useful cell-updates/s applied to the whole batch's useful cell-updates"}
         del single, op1
         torch.cuda.empty_cache()
     ops = [WaveOperatorB200(w.domain, w.sources, w.receivers, grad_mode="checkpoint", snapshot=snapshot,
@@ -1191,9 +1192,11 @@ def main() -> None:
     # snapshots, graph-replayed) and the large configuration (checkpointed, 16-bit snapshots), each
     # with its own roofline, accuracy against float64 and clocks; one GPU, default workload only
     extras = {}
+    absorbing = op.absorbing
     if world == 1 and args.workload == "fwi_512" and not args.no_extras and not args.n_steps:
         from nefi_b200 import workloads as _wl
 
+        op._plans.clear()  # the headline operator's device tables, so the next measurements have the device
         torch.cuda.empty_cache()
         extras["batched"] = measure_batch(dev, 1, 0, 64, steps=2, warmup=0, snapshot="delta16",
                                           with_plain=True, with_e2e=False, accuracy_problems=0 if args.no_accuracy else 4)
@@ -1205,7 +1208,7 @@ def main() -> None:
                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "f32",
                "data": "synthetic (seeded layered model; observed data from a smoothed model)",
-               "config": {**workload_desc(w, storage, op.absorbing),
+               "config": {**workload_desc(w, storage, absorbing),
                           "method": f"plain (per-step launches replayed from one CUDA graph, {storage})",
                           "parallelism": f"shots sharded over {world} GPU(s), fp64 gradient and loss all-reduce"},
                "gcell_updates_per_s": gcells, "roofline": roofline, "cpu_baseline": cpu,
