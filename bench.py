@@ -938,6 +938,8 @@ def main() -> None:
     ap.add_argument("--checkpoint-every", type=int, default=None)
     ap.add_argument("--absorbing", default=None, choices=("sponge", "pml", "cerjan", "none"),
                     help="override the workload's absorbing layer (fwi workloads)")
+    ap.add_argument("--tuning", default=None,
+                    help="launch shapes vz,rx,shots_per_cta,adj_vz,adj_rx,adj_shots_per_cta[,depth] (0: default)")
     ap.add_argument("--depth", type=int, default=0, choices=(0, 1, 2),
                     help="fwi workloads: forward steps per launch (0: the library default)")
     ap.add_argument("--pat-n", type=int, default=256, help="pat_256: grid edge (profiling cases)")
@@ -982,6 +984,9 @@ def main() -> None:
                           checkpoint_every=args.checkpoint_every, **okw)
     if args.depth:
         op.tuning = (0, 0, 0, 0, 0, 0, args.depth)
+    if args.tuning:
+        t = [int(v) for v in args.tuning.split(",")]
+        op.tuning = tuple(t + [args.depth or 0] * (7 - len(t)))
     c = torch.tensor(w.c, dtype=torch.float32, device=dev)
     # observed data: traces of a smoothed model (the misfit of a typical early FWI iteration)
     with torch.no_grad():
@@ -1210,6 +1215,7 @@ def main() -> None:
                "data": "synthetic (seeded layered model; observed data from a smoothed model)",
                "config": {**workload_desc(w, storage, absorbing),
                           "method": f"plain (per-step launches replayed from one CUDA graph, {storage})",
+                          "tuning": list(op.tuning) if getattr(op, "tuning", None) else "library defaults",
                           "parallelism": f"shots sharded over {world} GPU(s), fp64 gradient and loss all-reduce"},
                "gcell_updates_per_s": gcells, "roofline": roofline, "cpu_baseline": cpu,
                "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
