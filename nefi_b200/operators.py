@@ -331,9 +331,12 @@ class WaveOperatorB200(_LeapfrogB200):
     """Acoustic FWI forward model on the B200: sound speed ``c(x)`` -> traces of every source.
 
     Same arguments as ``nefi.physics.wave.WaveOperator`` (nefi/physics/wave.py:610-632), plus
-    ``snapshot`` (``"exact"`` | ``"fixed16"`` | ``"fp16"`` | ``"bf16"``: encoding of checkpoint snapshots) and
-    ``memory_budget`` (bytes available for wavefield storage; default 85 % of the device memory that
-    is free or held unused by PyTorch's allocator).
+    ``snapshot`` (encoding of checkpoint snapshots: ``"exact"``; ``"delta16"``, int16 second
+    differences in time with per-block scales, whose float32 gradient stays within 1e-4 of float64;
+    ``"fixed16"``, ``"fp16"`` and ``"bf16"``, block-scaled 16-bit values that do not meet that bound:
+    1.8e-4, 2.0e-3 and 1.7e-2 on a 128^2, 1000-step case) and ``memory_budget`` (bytes available for
+    wavefield storage; default 85 % of the device memory that is free or held unused by PyTorch's
+    allocator).
     Output ``(n_sources, n_receivers, n_t)`` at ``t_j = j dt_obs``; the gradient w.r.t. ``c`` is
     the exact discrete adjoint, reduced over shots in float64.
     """
@@ -740,7 +743,9 @@ class WaveInitialConditionOperatorB200(_LeapfrogB200):
     """Photoacoustic forward model on the B200: initial pressure ``p0`` -> traces.
 
     Same arguments as ``nefi.physics.wave.WaveInitialConditionOperator``
-    (nefi/physics/wave.py:769-787) plus ``snapshot`` and ``memory_budget``. Linear in ``p0``
+    (nefi/physics/wave.py:769-787) plus ``snapshot`` and ``memory_budget`` (as for
+    :class:`WaveOperatorB200`: only ``"exact"`` and ``"delta16"`` snapshots keep the float32 gradient
+    within 1e-4 of float64). Linear in ``p0``
     (``homogeneity = 1``); leading batch dims of ``p0`` are kept. The known sound speed ``c`` is a
     buffer as in the reference; :meth:`with_speed` evaluates the operator for a differentiable
     sound-speed map, giving the gradient w.r.t. ``c`` as well.
