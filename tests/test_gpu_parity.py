@@ -502,6 +502,34 @@ def test_pml_interior_through_tiled_kernels_matches_the_oracle(dtype, tt, tg, cu
     assert torch.equal(gk, gc)
 
 
+@pytest.mark.parametrize("dtype,tt,tg", [(torch.float64, 1e-11, 1e-10), (torch.float32, 1e-5, 1e-4)])
+def test_pml_cotangents_of_layer_cells_match_the_oracle(dtype, tt, tg, cuda_device):
+    """Receivers on the domain's faces reach the first layer row and column: the box's adjoint launch
+    adds the cotangents of the touched cells inside the tiled box and the layer launch those of the
+    listed cells outside it; traces and gradient against the float64 oracle, and checkpointed
+    (exact snapshots) bitwise the history gradient."""
+    import oracle
+
+    shape, extent, c, src, rec, kw = _pml_interior_case()
+    rec = rec + [[0.0, 0.77], [0.33, 0.0], [0.56, 1.3], [0.41, 2.0]]  # on the four faces
+    dom = Domain(shape, extent)
+    op = WaveOperatorB200(dom, src, rec, grad_mode="autograd", **kw)
+    plan = op._plan(cuda_device, dtype)
+    assert plan.adj_tables_box == 1 and plan.layer_cell_index.numel() > 0
+    cd = c.to(dtype).to(cuda_device).requires_grad_(True)
+    tr = op({"c": cd})
+    gt = torch.tensor(cotangent(tr.shape, 23), dtype=dtype, device=cuda_device)
+    (gc,) = torch.autograd.grad((tr * gt).sum(), cd)
+    orc = oracle.OracleWave(shape, extent, np.asarray(rec), sources=np.asarray(src), **kw)
+    tr_o, gc_o = orc.fwi(c.numpy(), cotangent(tr.shape, 23), dtype=np.float64)
+    assert rel_l2(tr.detach().cpu().numpy(), tr_o) < tt
+    assert rel_l2(gc.cpu().numpy(), gc_o) < tg
+    opk = WaveOperatorB200(dom, src, rec, grad_mode="checkpoint", checkpoint_every=7, **kw)
+    cd2 = c.to(dtype).to(cuda_device).requires_grad_(True)
+    (gk,) = torch.autograd.grad((opk({"c": cd2}) * gt).sum(), cd2)
+    assert torch.equal(gk, gc)
+
+
 def test_pml_forward_captured_in_a_fresh_thread(cuda_device):
     """A PML forward sweep (its layer kernel on the calling thread's second stream) captured into a
     CUDA graph by a thread that never ran one: the second stream is created inside the capture, and
