@@ -916,8 +916,9 @@ int adjoint_impl(const nw_grid* g, const nw_medium* m, const nw_acquisition* a, 
       tb.apply_a = ps.apply_a;
       tb.lap = lap;
       tb.gacc = gacc;
-      // the receiver cotangents: added by the box's launch itself when the adjoint tile tables were
-      // built for this box's tiles (every touched cell then lies in it), else by inject3 after the step
+      // the receiver cotangents: added by the box's launch and the layer's when the adjoint tile tables
+      // were built for this box's tiles (the touched cells outside it listed for the layer), else by
+      // inject3 after the step
       tb.tt = tile_tables(g, a, tu.adj);
       const dim3 grid = box_tiles<T>(ps, tu.adj, S, tb);
       box_inject = box_injects(a, tu.adj, ps.kx0, ps.kz0, tb.tt.tiles_z);
