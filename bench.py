@@ -14,14 +14,18 @@ restatement of the reference algorithm (the oracle, float32, all host threads) o
 Other workloads (``--workload``), each printing one line of the same form:
 
 * ``fwi_batch``: 64 uneven 2-D problems in one batched, checkpointed, graph-replayed gradient, with
-  the one-problem-at-a-time path timed beside it (whole problems over the ranks under torchrun);
+  the plain path timed beside it one problem at a time and one shot at a time (whole problems over
+  the ranks under torchrun);
 * ``fwi_2048``: the 2048^2 workload (32 shots, 8000 steps), with ``--grad-mode checkpoint
-  --snapshot fixed16`` for its 16-bit checkpointed gradient;
+  --snapshot delta16`` for its 16-bit checkpointed gradient;
 * ``pat_256``: the 3-D photoacoustic gradient (256^3, 4 instances, 2000 steps, p0 and c);
 * ``datagen_512x2``: float64 data generation from a 2x-refined ground truth;
 * ``misfit_2048``: the fused band-limited misfit and adjoint source at the 2048^2 trace shape.
 
-``--absorbing pml`` switches the 2-D workloads to the reference's default layer.
+``--absorbing pml`` switches the 2-D workloads to the reference's default layer; ``--tuning`` sets the
+launch shapes (``vz,rx,shots_per_cta,adj_vz,adj_rx,adj_shots_per_cta[,depth]``). The default line also
+carries the batch (``batched``) and the checkpointed 2048^2 gradient (``checkpointed_2048``), measured
+in the same run on one GPU.
 """
 
 from __future__ import annotations
