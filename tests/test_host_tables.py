@@ -533,3 +533,65 @@ def test_pml_adjoint_tables_follow_the_interior_box(edge):
             assert a.adj_tables_box == 1 and tuple(a.adj_box_corner) == plan.adj_box_corner
             assert a.n_layer_cells == plan.layer_cell_index.numel()
             _check_tile_tables(plan)
+
+
+def test_pml_layer_vectors_cover_the_layer_once_and_stay_in_bounds():
+    """Replays the PML layer kernel's enumeration (pml2d.cuh: a thread per 16-byte vector of W cells,
+    rows above the tiled box, the vectors left and right of it, rows below it) over random grids and
+    boxes in the library's ghost layout: every layer cell is stored by exactly one lane, and every load
+    and store offset of a vector (rows up to +-R, the neighbouring vectors of the centre row, faces
+    P0 and P1) stays inside one field."""
+    import ctypes as C
+    import random
+
+    from nefi_b200 import _lib
+
+    lib = _lib.load()
+    rnd = random.Random(7)
+    for trial in range(400):
+        r = rnd.choice([1, 2])
+        W = rnd.choice([4, 2])  # float32, float64
+        n0, n1 = rnd.randint(2 * r + 1, 70), rnd.randint(2 * r + 1, 110)
+        g = _lib.Grid(ndim=2, order=2 * r, dtype=_lib.NW_F32 if W == 4 else _lib.NW_F64,
+                      absorbing=_lib.NW_ABS_PML)
+        g.n[0], g.n[1], g.n[2] = n0, n1, 1
+        _lib.check(lib.nw_grid_layout(C.byref(g)))
+        ld, origin, field = int(g.stride[0]), int(g.origin), int(g.field_elems)
+        if trial % 4 == 0:
+            kx0 = kx1 = kz0 = kz1 = 0
+        else:  # a box as pml_tiled_box leaves it: first column rounded up to W, non-empty
+            cx0 = rnd.randint(0, n0 - 1); cx1 = rnd.randint(cx0 + 1, n0)
+            cz0 = rnd.randint(0, n1 - 1); cz1 = rnd.randint(cz0, n1)
+            kz0 = -(-cz0 // W) * W
+            kx0, kx1, kz1 = cx0, cx1, cz1
+            if kz1 <= kz0:
+                kx0 = kx1 = kz0 = kz1 = 0
+        nvr = -(-n1 // W)
+        vl, vr0 = kz0 // W, kz1 // W
+        bw = vl + nvr - vr0
+        top, mid = kx0 * nvr, (kx1 - kx0) * bw
+        n_vec = top + mid + (n0 - kx1) * nvr
+        seen = set()
+        for t in range(n_vec):
+            if t < top:
+                x, m = divmod(t, nvr)
+            elif t < top + mid:
+                q, rr = divmod(t - top, bw)
+                x, m = kx0 + q, (rr if rr < vl else vr0 + rr - vl)
+            else:
+                q, m = divmod(t - top - mid, nvr)
+                x = kx1 + q
+            zb = m * W
+            i = origin + x * ld + zb
+            assert i % W == 0 and ld % W == 0  # aligned 16-byte vectors
+            mid_row = kx0 <= x < kx1
+            for v in range(W):
+                z = zb + v
+                if z < n1 and (not mid_row or z < kz0 or z >= kz1):
+                    assert (x, z) not in seen
+                    seen.add((x, z))
+            lo = min(i - W, i - r * ld, i - 1)
+            hi = max(i + 2 * W - 1, i + r * ld + W - 1, i + ld + W - 1, i + W)
+            assert 0 <= lo and hi < field, (n0, n1, r, W, x, zb)
+        want = {(x, z) for x in range(n0) for z in range(n1) if not (kx0 <= x < kx1 and kz0 <= z < kz1)}
+        assert seen == want, (n0, n1, kx0, kx1, kz0, kz1)
