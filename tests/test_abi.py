@@ -167,3 +167,36 @@ def test_misaligned_device_buffers_are_refused_on_the_host(lib):
         rc = lib.nw_forward(C.byref(g), C.byref(m), C.byref(a), C.byref(t), C.byref(st), None, 0, 1, None, None)
         assert rc == _lib.NW_ERR_ARG, bad
         assert b"16-byte" in lib.nw_last_error(), bad
+
+
+def test_binding_structs_match_the_header_layout(tmp_path):
+    """Every descriptor struct of the ctypes binding has the C header's size and field offsets, as a C
+    compiler lays them out (a binding whose fields drift from the header passes garbage silently)."""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    pairs = {"nw_grid": _lib.Grid, "nw_tuning": _lib.Tuning, "nw_acquisition": _lib.Acquisition,
+             "nw_medium": _lib.Medium, "nw_time": _lib.Time, "nw_storage": _lib.Storage,
+             "nw_batch_problem": _lib.BatchProblem, "nw_traces": _lib.Traces}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "nefi_wave.h"', "int main(void) {"]
+    for cname, cls in pairs.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    include = Path(__file__).resolve().parents[1] / "include"
+    subprocess.run([cc, "-std=c99", f"-I{include}", str(src), "-o", str(exe)], check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines():
+        cname, key, value = line.split()
+        got[(cname, key)] = int(value)
+    for cname, cls in pairs.items():
+        assert got[(cname, "size")] == C.sizeof(cls), cname
+        for fname, _ in cls._fields_:
+            assert got[(cname, fname)] == getattr(cls, fname).offset, (cname, fname)
