@@ -333,6 +333,13 @@ def main():
     fwi_case("fwi_o4_pml_box", (56, 200), ((0.0, 0.56), (0.0, 2.0)), [[0.05, 0.4], [0.3, 1.5]],
              [[0.02, 0.1 + 0.09 * i] for i in range(20)] + [[0.5, 1.0]], cb,
              dict(n_t=50, dt_obs=0.004, f0=25.0, c_max=2.5, order=4, absorbing="pml", absorb_width=0.08), 23)
+    # the same grid with receivers on the domain's four faces: their stencils reach the first layer
+    # row or column, so a propagator that adds the interior's and the layer's cotangents in different
+    # places is checked on both
+    fwi_case("fwi_o4_pml_faces", (56, 200), ((0.0, 0.56), (0.0, 2.0)), [[0.05, 0.4], [0.3, 1.5]],
+             [[0.02, 0.1 + 0.09 * i] for i in range(20)] + [[0.5, 1.0], [0.0, 0.77], [0.33, 0.0], [0.56, 1.3],
+                                                            [0.41, 2.0]], cb,
+             dict(n_t=50, dt_obs=0.004, f0=25.0, c_max=2.5, order=4, absorbing="pml", absorb_width=0.08), 23)
 
 
 if __name__ == "__main__":
